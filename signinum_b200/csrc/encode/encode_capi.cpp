@@ -1,0 +1,47 @@
+// C ABI of the lossless HTJ2K encoder and the synthetic tile generators.
+#include <cstring>
+#include <vector>
+
+#include "../../../include/signinum_j2k_encode.h"
+
+#include "j2k_encode.h"
+
+extern "C" {
+
+int sgn_j2k_encode_lossless(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
+                            uint32_t bit_depth, const sgn_encode_options* o, uint8_t* out, size_t out_cap,
+                            size_t* out_len) {
+  sgn::enc::EncodeParams p;
+  p.width = width;
+  p.height = height;
+  p.comps = components;
+  p.bit_depth = bit_depth;
+  p.levels = o ? o->max_decomposition_levels : 5;
+  p.cbw_exp = o ? o->code_block_width_exp : 4;
+  p.cbh_exp = o ? o->code_block_height_exp : 4;
+  p.mct = o ? o->use_mct != 0 : true;
+  p.progression = o ? (int)o->progression : 0;
+  p.write_tlm = o ? o->write_tlm != 0 : false;
+  p.sop_eph = o ? o->sop_eph != 0 : false;
+  if (p.cbw_exp > 4 || p.cbh_exp > 4 || p.cbw_exp + p.cbh_exp > 8 || p.progression < 0 || p.progression > 4)
+    return -2;
+  std::vector<uint8_t> cs;
+  int rc = sgn::enc::encode(pixels, p, cs);
+  if (rc != 0) return rc;
+  if (out_len) *out_len = cs.size();
+  if (cs.size() > out_cap) return -4;
+  std::memcpy(out, cs.data(), cs.size());
+  return 0;
+}
+
+void sgn_synth_he_rgb8(uint64_t seed, uint32_t w, uint32_t h, double sigma, uint8_t* out) {
+  sgn::synth::he_tile(seed, w, h, sigma, out);
+}
+void sgn_synth_blank_rgb8(uint64_t seed, uint32_t w, uint32_t h, uint8_t* out) {
+  sgn::synth::blank_tile(seed, w, h, out);
+}
+void sgn_synth_fluor_gray16(uint64_t seed, uint32_t w, uint32_t h, uint8_t* out) {
+  sgn::synth::fluor_tile(seed, w, h, out);
+}
+
+}  // extern "C"

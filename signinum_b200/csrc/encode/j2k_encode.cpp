@@ -1,0 +1,654 @@
+// Lossless HTJ2K encoder (host C++): the input side of the decode path.
+//
+// Produces raw J2K codestreams the way the reference's lossless facade does
+// (crates/signinum-j2k/src/encode.rs:166-372 over
+// crates/signinum-j2k-native/src/j2c/encode.rs:265-480): DC level shift,
+// reversible colour transform, forward 5/3 with vertical then horizontal
+// lifting per level, no quantisation (exponents bit_depth + band gain, guard
+// bits raised to 2 with RCT), HT cleanup-only code blocks, one layer, one
+// precinct per resolution, SIZ/CAP/COD/QCD/[TLM]/SOT/SOD/EOC markers.
+//
+// The HT block coder is written here from the HTJ2K cleanup-pass definition
+// (T.814): MEL run coding of quad significance in zero contexts, CxtVLC
+// codewords with UVLC exponent offsets in a backward-growing VLC stream, and
+// magnitude/sign bits in a forward stream, ending in the Scup trailer.  Every
+// context and exponent predictor mirrors what the decoder recomputes.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../ht_tables.h"
+#include "j2k_encode.h"
+
+namespace sgn {
+namespace enc {
+
+static const HtEncodeTables& enc_tables() {
+  static HtEncodeTables* t = [] {
+    auto* p = new HtEncodeTables;
+    build_encode_tables(*p);
+    return p;
+  }();
+  return *t;
+}
+
+// Forward byte stream, bits LSB-first; a byte after 0xFF carries 7 bits.
+struct MagSgnWriter {
+  std::vector<uint8_t> buf;
+  uint64_t tmp = 0;
+  uint32_t used = 0, cap = 8;
+  void put(uint32_t v, uint32_t n) {
+    if (n == 0) return;
+    tmp |= (uint64_t)(v & (n >= 32 ? 0xFFFFFFFFu : ((1u << n) - 1))) << used;
+    used += n;
+    while (used >= cap) {
+      uint8_t b = (uint8_t)(tmp & ((1u << cap) - 1));
+      buf.push_back(b);
+      tmp >>= cap;
+      used -= cap;
+      cap = b == 0xFF ? 7 : 8;
+    }
+  }
+  void terminate() {
+    if (used > 0) {
+      uint8_t b = (uint8_t)((tmp | (0xFFu << used)) & ((1u << cap) - 1));
+      if (cap == 7) b &= 0x7F;
+      if (b != 0xFF) buf.push_back(b);
+    } else if (!buf.empty() && buf.back() == 0xFF) {
+      buf.pop_back();  // the decoder pads the stream with 0xFF anyway
+    }
+    used = 0;
+    tmp = 0;
+  }
+};
+
+// MEL: adaptive run-length coder of binary events, bits MSB-first.
+struct MelWriter {
+  std::vector<uint8_t> buf;
+  uint32_t tmp = 0, remaining = 8;
+  int k = 0;
+  uint32_t run = 0;
+  static int exp_of(int k) {
+    static const int E[13] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5};
+    return E[k];
+  }
+  void emit(uint32_t bit) {
+    tmp = (tmp << 1) | (bit & 1);
+    if (--remaining == 0) {
+      buf.push_back((uint8_t)tmp);
+      remaining = tmp == 0xFF ? 7 : 8;
+      tmp = 0;
+    }
+  }
+  void event(bool one) {
+    if (!one) {
+      if (++run >= (1u << exp_of(k))) {
+        emit(1);
+        run = 0;
+        k = std::min(k + 1, 12);
+      }
+    } else {
+      emit(0);
+      for (int t = exp_of(k) - 1; t >= 0; --t) emit((run >> t) & 1);
+      run = 0;
+      k = std::max(k - 1, 0);
+    }
+  }
+};
+
+// VLC: grows backward from the end of the segment; bits LSB-first within a
+// byte; a byte following (in reading order) one above 0x8F whose low seven
+// bits would all be ones keeps its top bit clear.
+struct VlcWriter {
+  std::vector<uint8_t> rev;  // rev[0] is the last byte of the segment
+  uint32_t tmp, used;
+  bool last_gt_8f;
+  VlcWriter() {
+    rev.push_back(0xFF);  // placeholder for Scup >> 4
+    tmp = 0xF;            // placeholder for Scup & 0xF
+    used = 4;
+    last_gt_8f = true;
+  }
+  void put(uint32_t v, uint32_t n) {
+    while (n > 0) {
+      uint32_t avail = 8 - (last_gt_8f ? 1 : 0) - used;
+      uint32_t t = std::min(avail, n);
+      tmp |= (v & ((1u << t) - 1)) << used;
+      used += t;
+      avail -= t;
+      n -= t;
+      v >>= t;
+      if (avail == 0) {
+        if (last_gt_8f && tmp != 0x7F) {
+          last_gt_8f = false;
+          continue;
+        }
+        rev.push_back((uint8_t)tmp);
+        last_gt_8f = tmp > 0x8F;
+        tmp = 0;
+        used = 0;
+      }
+    }
+  }
+};
+
+static inline uint32_t bitlen(uint32_t v) { return v ? 32 - (uint32_t)__builtin_clz(v) : 0; }
+
+// UVLC code for u >= 1 (no extension bits: u <= 32).
+static void uvlc_code(uint32_t u, uint32_t& pre, uint32_t& plen, uint32_t& suf, uint32_t& slen) {
+  if (u == 1) { pre = 1; plen = 1; suf = 0; slen = 0; }
+  else if (u == 2) { pre = 2; plen = 2; suf = 0; slen = 0; }
+  else if (u <= 4) { pre = 4; plen = 3; suf = u - 3; slen = 1; }
+  else { pre = 0; plen = 3; suf = u - 5; slen = 5; }
+}
+
+struct Quad {
+  uint32_t rho = 0;
+  uint32_t E[4] = {0, 0, 0, 0};
+  uint32_t v[4] = {0, 0, 0, 0};
+  uint32_t emax = 0;
+  uint32_t U = 0, uq = 0, uoff = 0, ek = 0;
+};
+
+// Encodes one code block's cleanup pass with its lowest bit-plane at 0.
+// Returns 0 on success (out empty when every coefficient is zero), or -1 when
+// a magnitude needs more than Mb bits or an exponent needs UVLC extension bits.
+int encode_ht_block(const int32_t* c, size_t stride, uint32_t w, uint32_t h, uint32_t Mb, std::vector<uint8_t>& out) {
+  out.clear();
+  bool any = false;
+  for (uint32_t y = 0; y < h && !any; ++y)
+    for (uint32_t x = 0; x < w; ++x)
+      if (c[y * stride + x] != 0) { any = true; break; }
+  if (!any) return 0;
+  const HtEncodeTables& T = enc_tables();
+  const uint32_t nq = (w + 1) / 2, nqr = (h + 1) / 2;
+  std::vector<Quad> prev(nq + 3), cur(nq + 3);
+  MagSgnWriter ms;
+  MelWriter mel;
+  VlcWriter vlc;
+  auto load = [&](uint32_t qx, uint32_t qy, Quad& q) -> int {
+    q = Quad();
+    for (int i = 0; i < 4; ++i) {
+      uint32_t x = 2 * qx + (i >> 1), y = 2 * qy + (i & 1);
+      if (x >= w || y >= h) continue;
+      int32_t val = c[(size_t)y * stride + x];
+      if (val == 0) continue;
+      uint32_t mu = (uint32_t)(val < 0 ? -(int64_t)val : val);
+      if (Mb < 31 && mu >= (1u << Mb)) return -1;
+      uint32_t s = val < 0 ? 1 : 0;
+      q.rho |= 1u << i;
+      q.v[i] = 2 * (mu - 1) + s;
+      q.E[i] = bitlen(2 * mu - 1);
+      q.emax = std::max(q.emax, q.E[i]);
+    }
+    return 0;
+  };
+  auto emb_of = [](const Quad& q) {
+    uint32_t e = 0;
+    for (int i = 0; i < 4; ++i)
+      if ((q.rho >> i & 1) && q.E[i] == q.U) e |= 1u << i;
+    return e;
+  };
+  auto codeword = [&](int tb, uint32_t ctx, Quad& q) -> int {
+    uint32_t emb = q.uoff ? emb_of(q) : 0;
+    const HtEncodeEntry& e = T.e[tb][ctx][q.rho][q.uoff][emb];
+    if (!e.valid) return -1;
+    vlc.put(e.cwd, e.len);
+    q.ek = e.e_k;
+    return 0;
+  };
+  auto magsgn = [&](const Quad& q) {
+    for (int i = 0; i < 4; ++i) {
+      if (!(q.rho >> i & 1)) continue;
+      uint32_t m = q.U - ((q.ek >> i) & 1);
+      ms.put(q.v[i], m);
+    }
+  };
+  for (uint32_t qy = 0; qy < nqr; ++qy) {
+    const bool initial = qy == 0;
+    for (uint32_t qx = 0; qx < nq; ++qx)
+      if (load(qx, qy, cur[qx]) != 0) return -1;
+    for (uint32_t qx = nq; qx < nq + 3; ++qx) cur[qx] = Quad();
+    // Exponent offsets: kappa is 1 in the initial row; elsewhere it follows
+    // the largest exponent among the four samples above when the quad has
+    // two or more significant samples.
+    for (uint32_t qx = 0; qx < nq; ++qx) {
+      Quad& q = cur[qx];
+      uint32_t kappa = 1;
+      if (!initial && __builtin_popcount(q.rho) >= 2) {
+        uint32_t e = 0;
+        if (qx > 0) e = std::max(e, prev[qx - 1].E[3]);
+        e = std::max(e, prev[qx].E[1]);
+        e = std::max(e, prev[qx].E[3]);
+        e = std::max(e, prev[qx + 1].E[1]);
+        kappa = std::max<uint32_t>(e, 2) - 1;
+      }
+      q.U = std::max(q.emax, kappa);
+      q.uq = q.U - kappa;
+      q.uoff = q.uq > 0 ? 1 : 0;
+      if (q.uq > 32) return -1;
+    }
+    uint32_t c_q = 0;
+    for (uint32_t a = 0; a < nq; a += 2) {
+      Quad& A = cur[a];
+      Quad& B = cur[a + 1];
+      const bool hasB = a + 1 < nq;
+      if (initial) {
+        if (c_q == 0) mel.event(A.rho != 0);
+        if (c_q != 0 || A.rho != 0)
+          if (codeword(0, c_q, A) != 0) return -1;
+        uint32_t tA = A.rho << 4;
+        c_q = ((tA & 0x10) << 3 | (tA & 0xE0) << 2) >> 7;
+        if (hasB) {
+          if (c_q == 0) mel.event(B.rho != 0);
+          if (c_q != 0 || B.rho != 0)
+            if (codeword(0, c_q, B) != 0) return -1;
+          uint32_t tB = B.rho << 4;
+          c_q = ((tB & 0x10) << 3 | (tB & 0xE0) << 2) >> 7;
+        } else {
+          c_q = 0;
+        }
+        uint32_t p0, l0, s0, n0, p1, l1, s1, n1;
+        if (A.uoff && B.uoff) {
+          bool both = A.uq > 2 && B.uq > 2;
+          mel.event(both);
+          if (both) {
+            uvlc_code(A.uq - 2, p0, l0, s0, n0);
+            uvlc_code(B.uq - 2, p1, l1, s1, n1);
+            vlc.put(p0, l0); vlc.put(p1, l1); vlc.put(s0, n0); vlc.put(s1, n1);
+          } else if (A.uq > 2) {
+            uvlc_code(A.uq, p0, l0, s0, n0);
+            vlc.put(p0, l0);
+            vlc.put(B.uq - 1, 1);
+            vlc.put(s0, n0);
+          } else {
+            uvlc_code(A.uq, p0, l0, s0, n0);
+            uvlc_code(B.uq, p1, l1, s1, n1);
+            vlc.put(p0, l0); vlc.put(p1, l1); vlc.put(s0, n0); vlc.put(s1, n1);
+          }
+        } else if (A.uoff) {
+          uvlc_code(A.uq, p0, l0, s0, n0);
+          vlc.put(p0, l0); vlc.put(s0, n0);
+        } else if (B.uoff) {
+          uvlc_code(B.uq, p1, l1, s1, n1);
+          vlc.put(p1, l1); vlc.put(s1, n1);
+        }
+      } else {
+        // Context from the row above (rho of quads a, a+1, a+2) and from the
+        // quad to the left, as the decoder rebuilds it.
+        auto t = [&](uint32_t i) { return prev[i].rho << 4; };
+        uint32_t cq = (c_q << 7);
+        cq |= (t(a) & 0xA0) << 2;
+        cq |= (t(a + 1) & 0x20) << 4;
+        uint32_t ctxA = cq >> 7;
+        if (ctxA == 0) mel.event(A.rho != 0);
+        if (ctxA != 0 || A.rho != 0)
+          if (codeword(1, ctxA, A) != 0) return -1;
+        uint32_t tA = A.rho << 4;
+        cq = ((tA & 0x40) << 2) | ((tA & 0x80) << 1);
+        cq |= t(a) & 0x80;
+        cq |= (t(a + 1) & 0xA0) << 2;
+        cq |= (t(a + 2) & 0x20) << 4;
+        uint32_t ctxB = cq >> 7;
+        uint32_t tB = 0;
+        if (hasB) {
+          if (ctxB == 0) mel.event(B.rho != 0);
+          if (ctxB != 0 || B.rho != 0)
+            if (codeword(1, ctxB, B) != 0) return -1;
+          tB = B.rho << 4;
+        }
+        cq = ((tB & 0x40) << 2) | ((tB & 0x80) << 1);
+        cq |= t(a + 1) & 0x80;
+        c_q = cq >> 7;
+        uint32_t p0 = 0, l0 = 0, s0 = 0, n0 = 0, p1 = 0, l1 = 0, s1 = 0, n1 = 0;
+        if (A.uoff) uvlc_code(A.uq, p0, l0, s0, n0);
+        if (hasB && B.uoff) uvlc_code(B.uq, p1, l1, s1, n1);
+        vlc.put(p0, l0); vlc.put(p1, l1); vlc.put(s0, n0); vlc.put(s1, n1);
+      }
+      magsgn(A);
+      if (hasB) magsgn(B);
+    }
+    std::swap(prev, cur);
+  }
+  // Terminate MEL and VLC, fusing their meeting bytes when the bits allow.
+  if (mel.run > 0) mel.emit(1);
+  uint32_t mel_tmp = (mel.tmp << mel.remaining) & 0xFF;
+  uint32_t mel_mask = (0xFFu << mel.remaining) & 0xFF;
+  uint32_t vlc_mask = (1u << vlc.used) - 1;
+  if ((mel_mask | vlc_mask) != 0) {
+    uint32_t fuse = mel_tmp | vlc.tmp;
+    if (((((fuse ^ mel_tmp) & mel_mask) | ((fuse ^ vlc.tmp) & vlc_mask)) == 0) && fuse != 0xFF && vlc.rev.size() > 1) {
+      mel.buf.push_back((uint8_t)fuse);
+    } else {
+      mel.buf.push_back((uint8_t)mel_tmp);
+      vlc.rev.push_back((uint8_t)vlc.tmp);
+    }
+  }
+  ms.terminate();
+  size_t scup = mel.buf.size() + vlc.rev.size();
+  if (scup < 2 || scup > 4079) return -1;
+  out = ms.buf;
+  out.insert(out.end(), mel.buf.begin(), mel.buf.end());
+  for (size_t i = vlc.rev.size(); i-- > 0;) out.push_back(vlc.rev[i]);
+  size_t L = out.size();
+  out[L - 1] = (uint8_t)(scup >> 4);
+  out[L - 2] = (uint8_t)((out[L - 2] & 0xF0) | (scup & 0xF));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Packet headers: MSB-first bits; after a 0xFF byte the next byte carries 7.
+struct HeaderWriter {
+  std::vector<uint8_t> buf;
+  uint32_t tmp = 0, n = 0, cap = 8;
+  void bit(uint32_t b) {
+    tmp = (tmp << 1) | (b & 1);
+    if (++n == cap) {
+      buf.push_back((uint8_t)tmp);
+      cap = tmp == 0xFF ? 7 : 8;
+      tmp = 0;
+      n = 0;
+    }
+  }
+  void bits(uint32_t v, uint32_t cnt) {
+    for (uint32_t i = cnt; i-- > 0;) bit((v >> i) & 1);
+  }
+  void flush() {
+    if (n > 0) {
+      buf.push_back((uint8_t)(tmp << (cap - n)));
+      n = 0;
+      tmp = 0;
+    }
+    if (!buf.empty() && buf.back() == 0xFF) buf.push_back(0x00);
+  }
+};
+
+// Tag tree over a w x h grid of leaves (standard quad-tree, levels aligned to
+// the origin).
+struct TagTree {
+  std::vector<std::vector<uint32_t>> value, low;
+  std::vector<std::vector<uint8_t>> known;
+  std::vector<uint32_t> lw, lh;
+  TagTree(uint32_t w, uint32_t h, const std::vector<uint32_t>& leaves) {
+    uint32_t cw = w, ch = h;
+    for (;;) {
+      lw.push_back(cw);
+      lh.push_back(ch);
+      value.emplace_back((size_t)cw * ch, UINT32_MAX);
+      low.emplace_back((size_t)cw * ch, 0);
+      known.emplace_back((size_t)cw * ch, 0);
+      if (cw <= 1 && ch <= 1) break;
+      cw = (cw + 1) / 2;
+      ch = (ch + 1) / 2;
+    }
+    value[0] = leaves;
+    for (size_t l = 1; l < value.size(); ++l)
+      for (uint32_t y = 0; y < lh[l - 1]; ++y)
+        for (uint32_t x = 0; x < lw[l - 1]; ++x) {
+          uint32_t& p = value[l][(y / 2) * lw[l] + x / 2];
+          p = std::min(p, value[l - 1][(size_t)y * lw[l - 1] + x]);
+        }
+  }
+  void encode(uint32_t x, uint32_t y, uint32_t threshold, HeaderWriter& hw) {
+    size_t L = value.size();
+    uint32_t lowv = 0;
+    for (size_t l = L; l-- > 0;) {
+      size_t i = (size_t)(y >> l) * lw[l] + (x >> l);
+      if (low[l][i] < lowv) low[l][i] = lowv;
+      else lowv = low[l][i];
+      while (lowv < threshold) {
+        if (lowv >= value[l][i]) {
+          if (!known[l][i]) {
+            hw.bit(1);
+            known[l][i] = 1;
+          }
+          break;
+        }
+        hw.bit(0);
+        ++lowv;
+      }
+      low[l][i] = lowv;
+    }
+  }
+};
+
+struct CodeBlockOut {
+  std::vector<uint8_t> bytes;
+};
+
+struct Band {
+  uint32_t w = 0, h = 0, cbw = 0, cbh = 0, ncx = 0, ncy = 0, mb = 0;
+  std::vector<CodeBlockOut> blocks;
+};
+
+static inline int32_t floor_div(int32_t a, int sh) { return a >> sh; }
+
+// Forward 5/3 lifting of one line (n samples, stride s), origin even.
+static void fwd53(int32_t* x, size_t n, size_t s) {
+  if (n < 2) return;
+  auto at = [&](long i) -> int32_t& {
+    if (i < 0) i = -i;
+    if (i >= (long)n) i = 2 * ((long)n - 1) - i;
+    return x[(size_t)i * s];
+  };
+  for (long i = 1; i < (long)n; i += 2) at(i) -= floor_div(at(i - 1) + at(i + 1), 1);
+  for (long i = 0; i < (long)n; i += 2) at(i) += floor_div(at(i - 1) + at(i + 1) + 2, 2);
+}
+
+
+static void put16(std::vector<uint8_t>& o, uint32_t v) { o.push_back((uint8_t)(v >> 8)); o.push_back((uint8_t)v); }
+static void put32(std::vector<uint8_t>& o, uint32_t v) { put16(o, v >> 16); put16(o, v & 0xFFFF); }
+
+int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& out) {
+  const uint32_t W = P.width, H = P.height, C = P.comps, bd = P.bit_depth;
+  if (W == 0 || H == 0 || C == 0 || C > 4 || bd == 0 || bd > 16) return -2;
+  uint32_t maxl = 0;
+  {
+    uint32_t m = std::min(W, H);
+    while ((2u << maxl) <= m) ++maxl;
+    if (m <= 1) maxl = 0;
+  }
+  const uint32_t L = std::min(P.levels, maxl);
+  const bool mct = P.mct && C >= 3;
+  const uint32_t guard = mct ? 2 : 1;
+  const size_t N = (size_t)W * H;
+  std::vector<std::vector<int32_t>> comp(C, std::vector<int32_t>(N));
+  const int32_t shift = 1 << (bd - 1);
+  for (size_t i = 0; i < N; ++i)
+    for (uint32_t c = 0; c < C; ++c) {
+      int32_t v = bd <= 8 ? pixels[i * C + c] : (int32_t)(pixels[(i * C + c) * 2] | (pixels[(i * C + c) * 2 + 1] << 8));
+      v &= (1 << bd) - 1;
+      comp[c][i] = v - shift;
+    }
+  if (mct) {
+    for (size_t i = 0; i < N; ++i) {
+      int32_t r = comp[0][i], g = comp[1][i], b = comp[2][i];
+      comp[0][i] = floor_div(r + 2 * g + b, 2);
+      comp[1][i] = b - g;
+      comp[2][i] = r - g;
+    }
+  }
+  // Per component: bands[0] = LL, then HL, LH, HH per resolution 1..L.
+  std::vector<std::vector<Band>> bands(C);
+  const uint32_t cbw = 1u << (P.cbw_exp + 2), cbh = 1u << (P.cbh_exp + 2);
+  std::vector<int32_t> tmp;
+  for (uint32_t c = 0; c < C; ++c) {
+    std::vector<int32_t>& img = comp[c];
+    // Dimensions of LL at each level, and the band planes (level 1 = finest).
+    uint32_t cw = W, ch = H;
+    std::vector<std::vector<int32_t>> hl(L + 1), lh(L + 1), hh(L + 1);
+    std::vector<uint32_t> lw(L + 2), lhh(L + 2);
+    lw[0] = W;
+    lhh[0] = H;
+    std::vector<int32_t> cur = img;
+    for (uint32_t d = 1; d <= L; ++d) {
+      // Vertical then horizontal lifting on the current LL (cw x ch).
+      for (uint32_t x = 0; x < cw; ++x) fwd53(&cur[x], ch, cw);
+      for (uint32_t y = 0; y < ch; ++y) fwd53(&cur[(size_t)y * cw], cw, 1);
+      uint32_t lwd = (cw + 1) / 2, hwd = cw / 2, lhd = (ch + 1) / 2, hhd = ch / 2;
+      std::vector<int32_t> ll((size_t)lwd * lhd);
+      hl[d].assign((size_t)hwd * lhd, 0);
+      lh[d].assign((size_t)lwd * hhd, 0);
+      hh[d].assign((size_t)hwd * hhd, 0);
+      for (uint32_t y = 0; y < ch; ++y)
+        for (uint32_t x = 0; x < cw; ++x) {
+          int32_t v = cur[(size_t)y * cw + x];
+          if (y % 2 == 0 && x % 2 == 0) ll[(size_t)(y / 2) * lwd + x / 2] = v;
+          else if (y % 2 == 0) hl[d][(size_t)(y / 2) * hwd + x / 2] = v;
+          else if (x % 2 == 0) lh[d][(size_t)(y / 2) * lwd + x / 2] = v;
+          else hh[d][(size_t)(y / 2) * hwd + x / 2] = v;
+        }
+      cur.swap(ll);
+      cw = lwd;
+      ch = lhd;
+      lw[d] = cw;
+      lhh[d] = ch;
+    }
+    auto make_band = [&](const std::vector<int32_t>& data, uint32_t w, uint32_t h, uint32_t gain) -> int {
+      Band b;
+      b.w = w;
+      b.h = h;
+      b.cbw = cbw;
+      b.cbh = cbh;
+      b.mb = guard + bd + gain - 1;
+      b.ncx = w ? (w + cbw - 1) / cbw : 0;
+      b.ncy = h ? (h + cbh - 1) / cbh : 0;
+      for (uint32_t by = 0; by < b.ncy; ++by)
+        for (uint32_t bx = 0; bx < b.ncx; ++bx) {
+          uint32_t x0 = bx * cbw, y0 = by * cbh, bw = std::min(cbw, w - x0), bh = std::min(cbh, h - y0);
+          CodeBlockOut cb;
+          if (encode_ht_block(&data[(size_t)y0 * w + x0], w, bw, bh, b.mb, cb.bytes) != 0) return -3;
+          b.blocks.push_back(std::move(cb));
+        }
+      bands[c].push_back(std::move(b));
+      return 0;
+    };
+    if (make_band(cur, cw, ch, 0) != 0) return -3;
+    for (uint32_t r = 1; r <= L; ++r) {
+      uint32_t d = L + 1 - r;  // decomposition level of resolution r
+      uint32_t pw = lw[d - 1], ph = lhh[d - 1];
+      uint32_t lwd = (pw + 1) / 2, hwd = pw / 2, lhd = (ph + 1) / 2, hhd = ph / 2;
+      if (make_band(hl[d], hwd, lhd, 1) != 0) return -3;
+      if (make_band(lh[d], lwd, hhd, 1) != 0) return -3;
+      if (make_band(hh[d], hwd, hhd, 2) != 0) return -3;
+    }
+  }
+  // Packets: one layer, one precinct per resolution.
+  std::vector<uint8_t> tile;
+  uint32_t sop_seq = 0;
+  auto packet = [&](uint32_t c, uint32_t r) {
+    size_t b0 = r == 0 ? 0 : 1 + (size_t)(r - 1) * 3, nb = r == 0 ? 1 : 3;
+    bool any = false;
+    for (size_t bi = b0; bi < b0 + nb; ++bi)
+      for (auto& cb : bands[c][bi].blocks) any = any || !cb.bytes.empty();
+    if (P.sop_eph) {
+      tile.push_back(0xFF); tile.push_back(0x91);
+      put16(tile, 4);
+      put16(tile, sop_seq++ & 0xFFFF);
+    }
+    HeaderWriter hw;
+    if (!any) {
+      hw.bit(0);
+    } else {
+      hw.bit(1);
+      for (size_t bi = b0; bi < b0 + nb; ++bi) {
+        Band& b = bands[c][bi];
+        if (b.ncx == 0 || b.ncy == 0) continue;
+        std::vector<uint32_t> incl(b.blocks.size()), zbp(b.blocks.size());
+        for (size_t i = 0; i < b.blocks.size(); ++i) {
+          incl[i] = b.blocks[i].bytes.empty() ? 1 : 0;
+          zbp[i] = b.blocks[i].bytes.empty() ? 0xFFFFu : b.mb - 1;  // empty leaves never coded
+        }
+        TagTree ti(b.ncx, b.ncy, incl), tz(b.ncx, b.ncy, zbp);
+        for (uint32_t y = 0; y < b.ncy; ++y)
+          for (uint32_t x = 0; x < b.ncx; ++x) {
+            const auto& cb = b.blocks[(size_t)y * b.ncx + x];
+            ti.encode(x, y, 1, hw);
+            if (cb.bytes.empty()) continue;
+            tz.encode(x, y, UINT32_MAX, hw);
+            hw.bit(0);  // one coding pass
+            uint32_t len = (uint32_t)cb.bytes.size();
+            uint32_t need = bitlen(len);
+            uint32_t k = need > 3 ? need - 3 : 0;
+            for (uint32_t i = 0; i < k; ++i) hw.bit(1);
+            hw.bit(0);
+            hw.bits(len, 3 + k);
+          }
+      }
+    }
+    hw.flush();
+    tile.insert(tile.end(), hw.buf.begin(), hw.buf.end());
+    if (P.sop_eph) { tile.push_back(0xFF); tile.push_back(0x92); }
+    if (any)
+      for (size_t bi = b0; bi < b0 + nb; ++bi)
+        for (auto& cb : bands[c][bi].blocks) tile.insert(tile.end(), cb.bytes.begin(), cb.bytes.end());
+  };
+  if (P.progression == 3 || P.progression == 4) {
+    for (uint32_t c = 0; c < C; ++c)
+      for (uint32_t r = 0; r <= L; ++r) packet(c, r);
+  } else {
+    for (uint32_t r = 0; r <= L; ++r)
+      for (uint32_t c = 0; c < C; ++c) packet(c, r);
+  }
+  // Codestream.
+  out.clear();
+  out.push_back(0xFF); out.push_back(0x4F);  // SOC
+  out.push_back(0xFF); out.push_back(0x51);  // SIZ
+  put16(out, 38 + 3 * C);
+  put16(out, 0x4000);  // Rsiz: HTJ2K
+  put32(out, W); put32(out, H); put32(out, 0); put32(out, 0);
+  put32(out, W); put32(out, H); put32(out, 0); put32(out, 0);
+  put16(out, C);
+  for (uint32_t c = 0; c < C; ++c) { out.push_back((uint8_t)(bd - 1)); out.push_back(1); out.push_back(1); }
+  out.push_back(0xFF); out.push_back(0x50);  // CAP
+  put16(out, 8);
+  put32(out, 0x00020000);
+  {
+    uint32_t mbits = bd - 1;
+    uint32_t bp = mbits <= 8 ? 0 : (mbits < 28 ? mbits - 8 : 13 + (mbits >> 2));
+    put16(out, bp);
+  }
+  out.push_back(0xFF); out.push_back(0x52);  // COD
+  put16(out, 12);
+  out.push_back(P.sop_eph ? 0x06 : 0x00);
+  out.push_back((uint8_t)P.progression);
+  put16(out, 1);
+  out.push_back(mct ? 1 : 0);
+  out.push_back((uint8_t)L);
+  out.push_back((uint8_t)P.cbw_exp);
+  out.push_back((uint8_t)P.cbh_exp);
+  out.push_back(0x40);
+  out.push_back(1);
+  out.push_back(0xFF); out.push_back(0x5C);  // QCD
+  put16(out, 3 + 1 + 3 * L);
+  out.push_back((uint8_t)(guard << 5));
+  out.push_back((uint8_t)(bd << 3));
+  for (uint32_t l = 0; l < L; ++l) {
+    out.push_back((uint8_t)((bd + 1) << 3));
+    out.push_back((uint8_t)((bd + 1) << 3));
+    out.push_back((uint8_t)((bd + 2) << 3));
+  }
+  uint32_t psot = 12 + 2 + (uint32_t)tile.size();
+  if (P.write_tlm) {
+    out.push_back(0xFF); out.push_back(0x55);
+    put16(out, 10);
+    out.push_back(0);
+    out.push_back(0x22);
+    put16(out, 0);
+    put32(out, psot);
+  }
+  out.push_back(0xFF); out.push_back(0x90);  // SOT
+  put16(out, 10);
+  put16(out, 0);
+  put32(out, psot);
+  out.push_back(0);
+  out.push_back(1);
+  out.push_back(0xFF); out.push_back(0x93);  // SOD
+  out.insert(out.end(), tile.begin(), tile.end());
+  out.push_back(0xFF); out.push_back(0xD9);  // EOC
+  return 0;
+}
+
+}  // namespace enc
+}  // namespace sgn

@@ -1,0 +1,24 @@
+// Internal interface of the lossless HTJ2K encoder and synthetic generators.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace sgn {
+namespace enc {
+struct EncodeParams {
+  uint32_t width, height, comps, bit_depth, levels, cbw_exp, cbh_exp;
+  bool mct;
+  int progression;  // 0 LRCP, 1 RLCP, 2 RPCL, 3 PCRL, 4 CPRL
+  bool write_tlm;
+  bool sop_eph;
+};
+int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& out);
+int encode_ht_block(const int32_t* c, size_t stride, uint32_t w, uint32_t h, uint32_t Mb, std::vector<uint8_t>& out);
+}  // namespace enc
+namespace synth {
+void he_tile(uint64_t seed, uint32_t w, uint32_t h, double sigma, uint8_t* out);
+void blank_tile(uint64_t seed, uint32_t w, uint32_t h, uint8_t* out);
+void fluor_tile(uint64_t seed, uint32_t w, uint32_t h, uint8_t* out_le16);
+}  // namespace synth
+}  // namespace sgn
