@@ -1,0 +1,163 @@
+/* signinum-j2k-cuda drop-in: HTJ2K tile decode into CUDA device memory (sm_100a).
+ *
+ * C ABI of the decode path behind the reference's CUDA adapter
+ * (crates/signinum-j2k-cuda, frames-sg/signinum 0.4.2).  Every entry point
+ * names the reference interface it replaces.  Plain pointers and sizes only;
+ * device memory is this library's own (CUDA runtime, device chosen at
+ * context creation).
+ *
+ * Status codes map one to one onto the reference's Error variants and
+ * predicates (crates/signinum-j2k-cuda/src/error.rs:7-41):
+ *   SGN_ERR_UNSUPPORTED / SGN_ERR_UNSUPPORTED_BACKEND / SGN_ERR_CUDA_UNAVAILABLE
+ *       -> is_unsupported();   SGN_ERR_BUFFER -> is_buffer_error();
+ *   SGN_ERR_TRUNCATED -> is_truncated();  SGN_ERR_REGION -> J2kError::InvalidRegion;
+ *   SGN_ERR_DECODE -> other decode errors;  SGN_ERR_CUDA_RUNTIME -> CudaRuntime{message}.
+ */
+#ifndef SIGNINUM_J2K_CUDA_H
+#define SIGNINUM_J2K_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t sgn_status;
+enum {
+  SGN_OK = 0,
+  SGN_ERR_UNSUPPORTED = 1,
+  SGN_ERR_BUFFER = 2,
+  SGN_ERR_TRUNCATED = 3,
+  SGN_ERR_DECODE = 4,
+  SGN_ERR_REGION = 5,
+  SGN_ERR_CUDA_UNAVAILABLE = 6,
+  SGN_ERR_CUDA_RUNTIME = 7,
+  SGN_ERR_UNSUPPORTED_BACKEND = 8,
+  SGN_ERR_INVALID_ARGUMENT = 9,
+  SGN_ERR_OUT_OF_MEMORY = 10
+};
+
+/* signinum_core::PixelFormat (crates/signinum-core/src/types.rs). */
+typedef enum sgn_pixel_format {
+  SGN_FMT_GRAY8 = 0,
+  SGN_FMT_RGB8 = 1,
+  SGN_FMT_RGBA8 = 2,
+  SGN_FMT_GRAY16 = 3,
+  SGN_FMT_RGB16 = 4,
+  SGN_FMT_RGBA16 = 5 /* rejected as unsupported, as the reference does (decode.rs:358-366) */
+} sgn_pixel_format;
+
+/* signinum_core::BackendRequest (crates/signinum-core/src/backend.rs:15-22).
+ * CUDA and AUTO decode on the GPU; CPU and METAL are rejected with
+ * SGN_ERR_UNSUPPORTED_BACKEND (this library has no host decoder). */
+typedef enum sgn_backend_request {
+  SGN_BACKEND_AUTO = 0,
+  SGN_BACKEND_CPU = 1,
+  SGN_BACKEND_METAL = 2,
+  SGN_BACKEND_CUDA = 3
+} sgn_backend_request;
+
+/* DeviceDecodeRequest (crates/signinum-j2k/src/adapter/device_plan.rs:7-12);
+ * downscale is the Downscale denominator 1, 2, 4 or 8
+ * (crates/signinum-core/src/scale.rs:5-20). */
+typedef enum sgn_request_kind {
+  SGN_REQ_FULL = 0,
+  SGN_REQ_REGION = 1,
+  SGN_REQ_SCALED = 2,
+  SGN_REQ_REGION_SCALED = 3
+} sgn_request_kind;
+
+typedef struct sgn_request {
+  uint32_t kind; /* sgn_request_kind */
+  uint32_t x, y, w, h;
+  uint32_t downscale;
+} sgn_request;
+
+/* Surface + CudaSurface (crates/signinum-j2k-cuda/src/surface.rs:19-127):
+ * tight rows, pitch_bytes = width * bytes_per_pixel. */
+typedef struct sgn_surface {
+  uint64_t device_ptr;
+  uint32_t width, height;
+  uint32_t format;           /* sgn_pixel_format */
+  uint32_t backend;          /* always SGN_BACKEND_CUDA for a decoded surface */
+  uint64_t pitch_bytes;
+  uint64_t kernel_dispatches; /* CudaSurfaceStats::kernel_dispatches */
+} sgn_surface;
+
+/* J2kView::inspect info (crates/signinum-core/src/types.rs Info). */
+typedef struct sgn_info {
+  uint32_t width, height, components, bit_depth, levels, tiles, ht, reversible, mct;
+} sgn_info;
+
+typedef struct sgn_ctx sgn_ctx;
+
+/* Replaces CudaSession + CudaContext::system_default
+ * (crates/signinum-j2k-cuda/src/session.rs:11-39,
+ * crates/signinum-cuda-runtime/src/lib.rs:286-320). */
+sgn_status sgn_ctx_create(int device, sgn_ctx** out);
+void sgn_ctx_destroy(sgn_ctx* ctx);
+/* CudaSession::submissions (session.rs:19-21). */
+uint64_t sgn_ctx_submissions(const sgn_ctx* ctx);
+/* Message of the last failing call on this thread. */
+const char* sgn_last_error_message(void);
+
+/* J2kDecoder::inspect / J2kView::parse (crates/signinum-j2k/src/view.rs:42-58). */
+sgn_status sgn_j2k_inspect(const uint8_t* data, size_t len, sgn_info* out);
+
+/* The plain per-tile drop-in: J2kDecoder::{decode,decode_region,decode_scaled,
+ * decode_region_scaled}_to_device (crates/signinum-j2k-cuda/src/decoder.rs:31-140)
+ * and Codec::submit_tile*_to_device (codec.rs:27-188).  Synchronous; on success
+ * *out owns a device buffer released by sgn_surface_free. */
+sgn_status sgn_j2k_decode_to_device(sgn_ctx* ctx, const uint8_t* data, size_t len, uint32_t format,
+                                    const sgn_request* request, uint32_t backend, sgn_surface* out);
+
+/* The batched form: TileBatchDecodeManyDevice::decode_tiles_to_device
+ * (crates/signinum-j2k-cuda/src/codec.rs:190-209).  One request per tile
+ * (NULL = full decode of every tile).  Order is preserved; per_tile[i] gets
+ * each tile's status; *first_failing gets the lowest failing index or
+ * SIZE_MAX, mirroring TileBatchError (crates/signinum-core/src/batch.rs:41-77).
+ * Returns SGN_OK when every tile decoded, else the status of the first
+ * failing tile; surfaces of successful tiles are valid either way. */
+sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
+                                          uint32_t format, const sgn_request* requests, uint32_t backend,
+                                          sgn_surface* outs, sgn_status* per_tile, size_t* first_failing);
+
+/* Surface::download_into (surface.rs:78-92): tight device-to-host copy into
+ * rows of `stride` bytes (stride >= pitch_bytes). */
+sgn_status sgn_surface_download(sgn_ctx* ctx, const sgn_surface* surface, uint8_t* out, size_t out_len, size_t stride);
+/* Releases the device buffer (CudaDeviceBuffer drop, crates/signinum-cuda-runtime/src/lib.rs:955-964). */
+void sgn_surface_free(sgn_ctx* ctx, sgn_surface* surface);
+
+/* ---- Device-resident batch plans (no counterpart in the reference: the
+ * split of decode_tiles_to_device into host parse + device execute lets a
+ * caller keep codestreams resident and replay decodes). */
+typedef struct sgn_plan sgn_plan;
+/* Parses the batch, uploads codestreams and descriptor tables, allocates the
+ * output surfaces.  Per-tile parse failures are reported like
+ * decode_tiles_to_device. */
+sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t format,
+                           const sgn_request* requests, sgn_plan** out, sgn_status* per_tile);
+/* Enqueues the kernels of the plan on the context stream (no host sync). */
+sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan);
+/* Waits for the plan and gathers per-tile statuses. */
+sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing);
+/* Surfaces of the plan (valid until sgn_plan_destroy). */
+sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n);
+/* Launches issued by one execute of the plan. */
+uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);
+void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan);
+/* The context's CUDA stream (cudaStream_t) for event timing by callers. */
+void* sgn_ctx_stream(sgn_ctx* ctx);
+
+/* Diagnostics (no counterpart in the reference): copies the packed HT lookup
+ * tables the kernels decode with (VLC initial/other rows: 1024 entries each;
+ * UVLC initial row: 320; other rows: 256) so tests can pin them to the
+ * reference's ht_tables.rs. */
+void sgn_ht_lookup_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

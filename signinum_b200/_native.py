@@ -1,0 +1,112 @@
+"""ctypes bindings of the package's native libraries.
+
+The decode path lives in libsigninum_j2k_cuda.so (C ABI in
+include/signinum_j2k_cuda.h); the encoder and synthetic tiles in
+libsigninum_j2k_encode.so (include/signinum_j2k_encode.h).  There is no
+fallback: a missing library raises at load time.
+"""
+import ctypes
+import pathlib
+
+LIB_DIR = pathlib.Path(__file__).resolve().parent / "_lib"
+CUDA_LIB = LIB_DIR / "libsigninum_j2k_cuda.so"
+ENCODE_LIB = LIB_DIR / "libsigninum_j2k_encode.so"
+
+c_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class SgnRequest(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("x", ctypes.c_uint32), ("y", ctypes.c_uint32),
+                ("w", ctypes.c_uint32), ("h", ctypes.c_uint32), ("downscale", ctypes.c_uint32)]
+
+
+class SgnSurface(ctypes.Structure):
+    _fields_ = [("device_ptr", ctypes.c_uint64), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("format", ctypes.c_uint32), ("backend", ctypes.c_uint32), ("pitch_bytes", ctypes.c_uint64),
+                ("kernel_dispatches", ctypes.c_uint64)]
+
+
+class SgnInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in
+                ("width", "height", "components", "bit_depth", "levels", "tiles", "ht", "reversible", "mct")]
+
+
+class SgnEncodeOptions(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in
+                ("max_decomposition_levels", "code_block_width_exp", "code_block_height_exp", "use_mct",
+                 "progression", "write_tlm", "sop_eph")]
+
+
+# Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
+CUDA_SIGNATURES = {
+    "sgn_ctx_create": (ctypes.c_int32, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "sgn_ctx_destroy": (None, [ctypes.c_void_p]),
+    "sgn_ctx_submissions": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "sgn_last_error_message": (ctypes.c_char_p, []),
+    "sgn_j2k_inspect": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(SgnInfo)]),
+    "sgn_j2k_decode_to_device": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32,
+                                                  ctypes.POINTER(SgnRequest), ctypes.c_uint32,
+                                                  ctypes.POINTER(SgnSurface)]),
+    "sgn_j2k_decode_tiles_to_device": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                                        ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t,
+                                                        ctypes.c_uint32, ctypes.POINTER(SgnRequest), ctypes.c_uint32,
+                                                        ctypes.POINTER(SgnSurface), ctypes.POINTER(ctypes.c_int32),
+                                                        ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_surface_download": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnSurface), ctypes.c_void_p,
+                                              ctypes.c_size_t, ctypes.c_size_t]),
+    "sgn_surface_free": (None, [ctypes.c_void_p, ctypes.POINTER(SgnSurface)]),
+    "sgn_plan_create": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t, ctypes.c_uint32,
+                                         ctypes.POINTER(SgnRequest), ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_int32)]),
+    "sgn_plan_execute_async": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
+    "sgn_plan_wait": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_plan_surfaces": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnSurface), ctypes.c_size_t]),
+    "sgn_plan_kernel_launches": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "sgn_plan_destroy": (None, [ctypes.c_void_p, ctypes.c_void_p]),
+    "sgn_ctx_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "sgn_ht_lookup_tables": (None, [ctypes.c_void_p] * 4),
+}
+
+ENCODE_SIGNATURES = {
+    "sgn_j2k_encode_lossless": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                               ctypes.c_uint32, ctypes.POINTER(SgnEncodeOptions), ctypes.c_void_p,
+                                               ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_synth_he_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p]),
+    "sgn_synth_blank_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
+    "sgn_synth_fluor_gray16": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
+}
+
+_cuda = None
+_encode = None
+
+
+def _bind(path, sigs):
+    if not path.exists():
+        raise RuntimeError(f"native library {path.name} is not built; run `python -m signinum_b200.build`")
+    lib = ctypes.CDLL(str(path))
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def cuda_lib():
+    global _cuda
+    if _cuda is None:
+        _cuda = _bind(CUDA_LIB, CUDA_SIGNATURES)
+    return _cuda
+
+
+def encode_lib():
+    global _encode
+    if _encode is None:
+        _encode = _bind(ENCODE_LIB, ENCODE_SIGNATURES)
+    return _encode
+
+
+def last_error():
+    msg = cuda_lib().sgn_last_error_message()
+    return msg.decode() if msg else ""

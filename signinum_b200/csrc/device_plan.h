@@ -1,0 +1,68 @@
+// Device-resident descriptor tables shared by the host plan builder and the
+// sm_100a kernels.
+//
+// One HtJob per code block (the device form of the reference's
+// HtOwnedCodeBlockBatchJob, crates/signinum-j2k-native/src/direct_plan.rs:120-149),
+// one IdwtJob per (tile, component, decomposition level) (cf. J2kDirectIdwtStep,
+// direct_plan.rs:154-177) and one PackJob per tile for the last level fused
+// with inverse RCT, DC shift and pixel packing (cf. J2kDirectStoreStep,
+// direct_plan.rs:182-205).  Offsets are 64-bit so one arena can hold a
+// whole batch.
+#pragma once
+
+#include <cstdint>
+
+namespace sgn {
+
+// Lifting tile of the IDWT kernels (output samples per CTA) and its halo.
+constexpr int kIdwtTileW = 64;
+constexpr int kIdwtTileH = 32;
+constexpr int kIdwtHalo = 2;
+constexpr int kIdwtThreads = 256;
+
+struct HtJob {
+  uint64_t src;      // byte offset of the cleanup segment in the input arena
+  uint64_t dst;      // element offset of the block's first sample in the coefficient arena
+  uint32_t lcup;     // cleanup segment length (refinement follows it)
+  uint32_t tile;     // batch index of the tile (status reporting)
+  uint32_t stride;   // band row stride in elements
+  uint16_t lref;     // refinement segment length
+  uint16_t w, h;
+  uint8_t mmsb;      // missing MSBs after placeholder folding (p = 30 - mmsb)
+  uint8_t passes;    // 0 = all-zero block, 1 = cleanup, 2 = +SigProp, 3 = +MagRef
+  uint8_t nbp;       // magnitude bit-planes of the band (coefficient alignment)
+  uint8_t flags;     // bit 0: vertically causal context
+  uint8_t pad[2];
+};
+static_assert(sizeof(HtJob) == 40, "HtJob layout");
+
+struct IdwtJob {
+  const int32_t* ll;   // ceil(w/2) x ceil(h/2)
+  const int32_t* hl;   // floor(w/2) x ceil(h/2)
+  const int32_t* lh;   // ceil(w/2) x floor(h/2)
+  const int32_t* hh;   // floor(w/2) x floor(h/2)
+  int32_t* out;        // w x h, tight
+  uint32_t w, h;
+  uint32_t tiles_x;
+  uint32_t cta_begin;
+};
+
+enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
+
+struct PackJob {
+  const int32_t* ll[3];
+  const int32_t* hl[3];
+  const int32_t* lh[3];
+  const int32_t* hh[3];
+  uint8_t* out;         // surface (device)
+  uint64_t pitch;       // bytes per output row
+  uint32_t w, h;        // dimensions of the last decoded level (image at that resolution)
+  uint32_t cx, cy, cw, ch;  // crop written to the surface
+  uint32_t lifting;     // 1: inputs are the four bands of the last level; 0: ll holds the image
+  uint32_t ncomp, mct, bit_depth, fmt, region_conv;
+  uint32_t tiles_x;     // CTA tiles across the crop
+  uint32_t cta_begin;
+  uint32_t tile;        // batch index (status)
+};
+
+}  // namespace sgn

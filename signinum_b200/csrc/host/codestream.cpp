@@ -1,0 +1,732 @@
+// Host-side codestream parsing for the CUDA decode path (see codestream.h).
+#include "codestream.h"
+
+#include <algorithm>
+#include <cstring>
+#include <tuple>
+
+namespace sgn {
+namespace {
+
+[[noreturn]] void fail(int32_t s, const char* m) { throw ParseError{s, m}; }
+
+inline uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Byte/bit reader with the packet-header bit-stuffing rule (B.10.1: after a
+// 0xFF byte the next byte carries an extra zero bit in its MSB).
+struct Reader {
+  const uint8_t* d;
+  size_t n, bit = 0;  // bit position
+  Reader(const uint8_t* p, size_t len) : d(p), n(len) {}
+  size_t pos() const { return bit >> 3; }
+  bool end() const { return pos() >= n; }
+  bool u8(uint8_t& v) {
+    if (pos() + 1 > n) return false;
+    v = d[pos()];
+    bit += 8;
+    return true;
+  }
+  bool u16(uint16_t& v) {
+    if (pos() + 2 > n) return false;
+    v = (uint16_t)((d[pos()] << 8) | d[pos() + 1]);
+    bit += 16;
+    return true;
+  }
+  bool u32(uint32_t& v) {
+    if (pos() + 4 > n) return false;
+    const uint8_t* p = d + pos();
+    v = ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3];
+    bit += 32;
+    return true;
+  }
+  bool skip(size_t k) {
+    if (pos() + k < pos() || pos() + k > n) return false;
+    bit += k * 8;
+    return true;
+  }
+  bool marker(uint8_t& m) {
+    if (pos() + 2 > n || d[pos()] != 0xFF) return false;
+    m = d[pos() + 1];
+    bit += 16;
+    return true;
+  }
+  bool peek_marker(uint8_t& m) const {
+    if (pos() + 2 > n || d[pos()] != 0xFF) return false;
+    m = d[pos() + 1];
+    return true;
+  }
+  void align() { bit = (bit + 7) & ~(size_t)7; }
+  bool bits(uint32_t cnt, uint32_t& out) {
+    uint32_t v = 0;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      size_t p = bit >> 3;
+      if (p >= n) return false;
+      uint32_t bp = bit & 7;
+      bool stuff = bp == 7 && d[p] == 0xFF;
+      v = (v << 1) | ((d[p] >> (7 - bp)) & 1);
+      ++bit;
+      if (stuff) {
+        if ((bit >> 3) >= n) return false;
+        if ((d[bit >> 3] >> 7) & 1) return false;
+        ++bit;
+      }
+    }
+    out = v;
+    return true;
+  }
+};
+
+struct CodingStyle {
+  uint8_t flags = 0, ndecomp = 0, cbw = 0, cbh = 0, cbstyle = 0, transform = 1;
+  uint8_t pexp_x[33], pexp_y[33];
+};
+
+struct Quant {
+  uint8_t style = 0, guard = 0;
+  std::vector<uint16_t> exps;  // exponent per band entry
+};
+
+struct Comp {
+  uint8_t precision, xr, yr;
+  CodingStyle cs;
+  Quant q;
+};
+
+bool read_coding_style(Reader& r, uint8_t flags, CodingStyle& cs) {
+  uint8_t cw, ch;
+  if (!r.u8(cs.ndecomp) || cs.ndecomp > 32) return false;
+  if (!r.u8(cw) || !r.u8(ch) || !r.u8(cs.cbstyle) || !r.u8(cs.transform)) return false;
+  if (cw > 8 || ch > 8 || cw + ch > 8 || cs.transform > 1) return false;
+  cs.cbw = (uint8_t)(cw + 2);
+  cs.cbh = (uint8_t)(ch + 2);
+  cs.flags = flags;
+  for (int i = 0; i <= cs.ndecomp; ++i) {
+    if (flags & 1) {
+      uint8_t v;
+      if (!r.u8(v)) return false;
+      cs.pexp_x[i] = v & 0xF;
+      cs.pexp_y[i] = v >> 4;
+    } else {
+      cs.pexp_x[i] = 15;
+      cs.pexp_y[i] = 15;
+    }
+  }
+  return true;
+}
+
+bool read_quant(Reader& r, size_t body, Quant& q) {
+  uint8_t s;
+  if (body < 1 || !r.u8(s)) return false;
+  q.style = s & 0x1F;
+  q.guard = s >> 5;
+  q.exps.clear();
+  if (q.style == 0) {
+    for (size_t i = 0; i + 1 < body; ++i) {
+      uint8_t v;
+      if (!r.u8(v)) return false;
+      q.exps.push_back((uint16_t)(v >> 3));
+    }
+  } else if (q.style == 1 || q.style == 2) {
+    for (size_t i = 0; i + 2 < body + 1; i += 2) {
+      uint16_t v;
+      if (!r.u16(v)) return false;
+      q.exps.push_back((uint16_t)(v >> 11));
+    }
+  } else {
+    return false;
+  }
+  return true;
+}
+
+struct MainHeader {
+  uint32_t gw, gh, ox, oy, tw, th, tox, toy;
+  std::vector<Comp> comps;
+  uint8_t prog = 0;
+  uint16_t layers = 1;
+  bool mct = false;
+  size_t end;  // offset of the first SOT
+};
+
+// Main header: codestream.rs:38-187.
+MainHeader read_main_header(const uint8_t* data, size_t len) {
+  if (len < 4 || data[0] != 0xFF || data[1] != 0x4F || data[2] != 0xFF || data[3] != 0x51)
+    fail(ST_DECODE, "invalid codestream signature");
+  Reader r(data, len);
+  r.skip(4);
+  MainHeader h;
+  uint16_t lsiz, rsiz, csiz;
+  if (!r.u16(lsiz) || !r.u16(rsiz) || !r.u32(h.gw) || !r.u32(h.gh) || !r.u32(h.ox) || !r.u32(h.oy) ||
+      !r.u32(h.tw) || !r.u32(h.th) || !r.u32(h.tox) || !r.u32(h.toy) || !r.u16(csiz))
+    fail(ST_TRUNCATED, "SIZ truncated");
+  if (h.ox >= h.gw || h.oy >= h.gh || csiz == 0 || h.tw == 0 || h.th == 0) fail(ST_DECODE, "invalid SIZ");
+  if (h.tox >= h.gw || h.toy >= h.gh || h.tox > h.ox || h.toy > h.oy) fail(ST_DECODE, "invalid tile offsets");
+  if ((uint64_t)h.tox + h.tw <= h.ox || (uint64_t)h.toy + h.th <= h.oy) fail(ST_DECODE, "invalid tile offsets");
+  for (uint16_t i = 0; i < csiz; ++i) {
+    uint8_t ss, xr, yr;
+    if (!r.u8(ss) || !r.u8(xr) || !r.u8(yr)) fail(ST_TRUNCATED, "SIZ truncated");
+    Comp c;
+    c.precision = (uint8_t)((ss & 0x7F) + 1);
+    c.xr = xr;
+    c.yr = yr;
+    if (c.precision > 32 || xr == 0 || yr == 0) fail(ST_DECODE, "invalid component metadata");
+    h.comps.push_back(c);
+  }
+  bool have_cod = false, have_qcd = false;
+  CodingStyle cod;
+  Quant qcd;
+  std::vector<int> coc_set(csiz, 0), qcc_set(csiz, 0);
+  std::vector<CodingStyle> coc(csiz);
+  std::vector<Quant> qcc(csiz);
+  for (;;) {
+    uint8_t m;
+    if (!r.peek_marker(m)) fail(ST_DECODE, "invalid marker in main header");
+    if (m == 0x90) break;
+    r.marker(m);
+    uint16_t L;
+    if (m >= 0x30 && m <= 0x3F) continue;
+    if (!r.u16(L) || L < 2) fail(ST_TRUNCATED, "marker segment truncated");
+    size_t seg_end = r.pos() + L - 2;
+    if (seg_end > len) fail(ST_TRUNCATED, "marker segment truncated");
+    switch (m) {
+      case 0x52: {  // COD
+        uint8_t flags, prog, mct;
+        uint16_t layers;
+        if (!r.u8(flags) || !r.u8(prog) || !r.u16(layers) || !r.u8(mct) || !read_coding_style(r, flags, cod))
+          fail(ST_DECODE, "COD parse failure");
+        if (prog > 4 || layers == 0 || layers > 32) fail(ST_DECODE, "COD parse failure");
+        h.prog = prog;
+        h.layers = layers;
+        h.mct = mct == 1;
+        have_cod = true;
+        break;
+      }
+      case 0x53: {  // COC
+        uint16_t idx;
+        uint8_t b, flags;
+        if (csiz < 257) {
+          if (!r.u8(b)) fail(ST_DECODE, "COC parse failure");
+          idx = b;
+        } else if (!r.u16(idx)) fail(ST_DECODE, "COC parse failure");
+        if (idx >= csiz || !r.u8(flags) || !read_coding_style(r, flags, coc[idx])) fail(ST_DECODE, "COC parse failure");
+        coc_set[idx] = 1;
+        break;
+      }
+      case 0x5C:  // QCD
+        if (!read_quant(r, L - 2, qcd)) fail(ST_DECODE, "QCD parse failure");
+        have_qcd = true;
+        break;
+      case 0x5D: {  // QCC
+        uint16_t idx;
+        uint8_t b;
+        size_t isz = csiz < 257 ? 1 : 2;
+        if (csiz < 257) {
+          if (!r.u8(b)) fail(ST_DECODE, "QCC parse failure");
+          idx = b;
+        } else if (!r.u16(idx)) fail(ST_DECODE, "QCC parse failure");
+        if (idx >= csiz || L < 2 + isz + 1 || !read_quant(r, L - 2 - isz, qcc[idx])) fail(ST_DECODE, "QCC parse failure");
+        qcc_set[idx] = 1;
+        break;
+      }
+      case 0x60:
+        fail(ST_UNSUPPORTED, "PPM packed packet headers are not supported by the CUDA path");
+      case 0x50: case 0x59: case 0x5E: case 0x55: case 0x64: case 0x63:  // CAP CPF RGN TLM COM CRG
+        break;
+      default:
+        fail(ST_UNSUPPORTED, "unsupported marker in main header");
+    }
+    r.bit = seg_end * 8;
+  }
+  if (!have_cod) fail(ST_DECODE, "missing COD");
+  if (!have_qcd) fail(ST_DECODE, "missing QCD");
+  for (uint16_t i = 0; i < csiz; ++i) {
+    Comp& c = h.comps[i];
+    c.cs = coc_set[i] ? coc[i] : cod;
+    if (coc_set[i]) c.cs.flags |= cod.flags;
+    c.q = qcc_set[i] ? qcc[i] : qcd;
+  }
+  h.end = r.pos();
+  return h;
+}
+
+struct TagTree {
+  uint32_t levels = 0;
+  uint32_t lw[17], lh[17];
+  size_t base[17];
+  std::vector<uint32_t> val;
+  std::vector<uint8_t> known;
+  void init(uint32_t w, uint32_t h) {
+    levels = 0;
+    size_t total = 0;
+    for (;;) {
+      lw[levels] = w;
+      lh[levels] = h;
+      base[levels] = total;
+      total += (size_t)w * h;
+      ++levels;
+      if (w <= 1 && h <= 1) break;
+      w = (w + 1) / 2;
+      h = (h + 1) / 2;
+    }
+    val.assign(total, 0);
+    known.assign(total, 0);
+  }
+  // read_tag_node, tag_tree.rs:118-190, unrolled over levels.
+  bool read(uint32_t x, uint32_t y, uint32_t threshold, Reader& r, uint32_t& out) {
+    uint32_t parent = 0;
+    for (uint32_t l = levels; l-- > 0;) {
+      size_t i = base[l] + (size_t)(y >> l) * lw[l] + (x >> l);
+      if (!known[i]) {
+        uint32_t v = std::max(parent, val[i]);
+        while (v < threshold) {
+          uint32_t b;
+          if (!r.bits(1, b)) return false;
+          if (b == 0) ++v;
+          else {
+            known[i] = 1;
+            break;
+          }
+        }
+        val[i] = v;
+      }
+      if (val[i] >= threshold || l == 0) {
+        out = val[i];
+        return true;
+      }
+      parent = val[i];
+    }
+    out = parent;
+    return true;
+  }
+};
+
+struct PrecinctBand {  // one (precinct, sub-band) pair
+  uint32_t band;
+  uint32_t cb_x0, cb_y0, ncx, ncy, cbw, cbh;
+  uint32_t first_block;  // index into the flat block-state array
+  TagTree incl, zbp;
+};
+
+struct BlockState {
+  uint32_t band, x0, y0, w, h;
+  bool included = false;
+  uint8_t missing = 0, passes = 0;
+  uint32_t lblock = 3;
+  uint32_t lcup = 0, lref = 0;
+  int64_t cleanup_off = -1, ref_off = -1;
+};
+
+struct Packet {  // one (component, resolution, precinct)
+  uint8_t comp, res;
+  uint32_t precinct;
+  uint32_t pb_begin, pb_count;
+  uint64_t sort_py, sort_px;
+};
+
+}  // namespace
+
+Info inspect_codestream(const uint8_t* data, size_t len) {
+  MainHeader h = read_main_header(data, len);
+  Info i;
+  uint32_t xsf = 1, ysf = 1;
+  bool same = true;
+  for (auto& c : h.comps) same = same && c.xr == h.comps[0].xr && c.yr == h.comps[0].yr;
+  if (same) { xsf = h.comps[0].xr; ysf = h.comps[0].yr; }
+  i.width = cdiv(h.gw - h.ox, xsf);
+  i.height = cdiv(h.gh - h.oy, ysf);
+  if (i.width > 60000 || i.height > 60000) fail(ST_DECODE, "image too large");
+  i.components = (uint32_t)h.comps.size();
+  i.bit_depth = h.comps[0].precision;
+  i.levels = h.comps[0].cs.ndecomp;
+  i.tiles = cdiv(h.gw - h.tox, h.tw) * cdiv(h.gh - h.toy, h.th);
+  i.ht = 1;
+  for (auto& c : h.comps) i.ht = i.ht && ((c.cs.cbstyle & 0x40) != 0);
+  i.reversible = h.comps[0].cs.transform == 1;
+  i.mct = h.mct;
+  return i;
+}
+
+void parse_tile(const uint8_t* data, size_t len, const uint32_t* target, TileLayout& T) {
+  MainHeader h = read_main_header(data, len);
+  const uint32_t nc = (uint32_t)h.comps.size();
+  if (h.ox || h.oy || h.tox || h.toy) fail(ST_UNSUPPORTED, "image/tile offsets are not supported by the CUDA path");
+  if (cdiv(h.gw, h.tw) * cdiv(h.gh, h.th) != 1) fail(ST_UNSUPPORTED, "multi-tile codestreams are not supported by the CUDA path");
+  if (nc != 1 && nc != 3) fail(ST_UNSUPPORTED, "only gray and RGB codestreams are supported by the CUDA path");
+  if (h.gw > 60000 || h.gh > 60000) fail(ST_DECODE, "image too large");
+  // Tile-parts (tile.rs:162-306); per-tile COD/COC/QCD/QCC update the components.
+  Reader r(data, len);
+  r.bit = h.end * 8;
+  std::vector<std::pair<size_t, size_t>> parts;
+  bool first_part = true;
+  uint8_t m;
+  while (r.peek_marker(m) && m == 0x90) {
+    r.marker(m);
+    uint16_t lsot, isot;
+    uint32_t psot;
+    uint8_t tp, ntp;
+    if (!r.u16(lsot) || !r.u16(isot) || !r.u32(psot) || !r.u8(tp) || !r.u8(ntp)) fail(ST_TRUNCATED, "SOT truncated");
+    if (isot != 0) fail(ST_DECODE, "invalid tile index");
+    size_t start = r.pos();
+    size_t data_len;
+    if (psot == 0) data_len = len > start ? len - start : 0;
+    else {
+      if (psot < 12) fail(ST_DECODE, "invalid tile-part length");
+      data_len = psot - 12;
+    }
+    bool sod = false;
+    for (;;) {
+      if (!r.peek_marker(m)) break;  // non-strict: a broken tile-part header ends parsing
+      r.marker(m);
+      if (m == 0x93) { sod = true; break; }
+      if (m == 0xD9) break;
+      if (m >= 0x30 && m <= 0x3F) continue;
+      uint16_t L;
+      if (!r.u16(L) || L < 2 || r.pos() + L - 2 > len) fail(ST_TRUNCATED, "marker segment truncated");
+      size_t seg_end = r.pos() + L - 2;
+      if (m == 0x52) {
+        uint8_t flags, prog, mct;
+        uint16_t layers;
+        CodingStyle cs;
+        if (!r.u8(flags) || !r.u8(prog) || !r.u16(layers) || !r.u8(mct) || !read_coding_style(r, flags, cs) ||
+            prog > 4 || layers == 0 || layers > 32)
+          fail(ST_DECODE, "COD parse failure");
+        h.prog = prog;
+        h.layers = layers;
+        h.mct = mct == 1;
+        for (auto& c : h.comps) {
+          uint8_t f = (uint8_t)(c.cs.flags | cs.flags);
+          c.cs = cs;
+          c.cs.flags = f;
+        }
+      } else if (m == 0x53) {
+        uint16_t idx;
+        uint8_t b, flags;
+        CodingStyle cs;
+        if (nc < 257) {
+          if (!r.u8(b)) fail(ST_DECODE, "COC parse failure");
+          idx = b;
+        } else if (!r.u16(idx)) fail(ST_DECODE, "COC parse failure");
+        if (idx >= nc || !r.u8(flags) || !read_coding_style(r, flags, cs)) fail(ST_DECODE, "COC parse failure");
+        uint8_t f = (uint8_t)(h.comps[idx].cs.flags | flags);
+        h.comps[idx].cs = cs;
+        h.comps[idx].cs.flags = f;
+      } else if (m == 0x5C) {
+        Quant q;
+        if (!read_quant(r, L - 2, q)) fail(ST_DECODE, "QCD parse failure");
+        for (auto& c : h.comps) c.q = q;
+      } else if (m == 0x5D) {
+        uint16_t idx;
+        uint8_t b;
+        size_t isz = nc < 257 ? 1 : 2;
+        Quant q;
+        if (nc < 257) {
+          if (!r.u8(b)) fail(ST_DECODE, "QCC parse failure");
+          idx = b;
+        } else if (!r.u16(idx)) fail(ST_DECODE, "QCC parse failure");
+        if (idx >= nc || L < 2 + isz + 1 || !read_quant(r, L - 2 - isz, q)) fail(ST_DECODE, "QCC parse failure");
+        h.comps[idx].q = q;
+      } else if (m == 0x61) {
+        fail(ST_UNSUPPORTED, "PPT packed packet headers are not supported by the CUDA path");
+      } else if (m != 0x58 && m != 0x64) {
+        fail(ST_UNSUPPORTED, "unsupported marker in tile-part header");
+      }
+      r.bit = seg_end * 8;
+    }
+    (void)first_part;
+    first_part = false;
+    if (!sod) break;
+    size_t used = r.pos() - start;
+    if (used > data_len) break;
+    size_t body = data_len - used;
+    if (r.pos() + body > len) fail(ST_TRUNCATED, "tile-part data truncated");
+    parts.push_back({r.pos(), body});
+    r.skip(body);
+  }
+  if (parts.empty()) fail(ST_DECODE, "no tile-part data");
+  // Component checks for this path.
+  const Comp& c0 = h.comps[0];
+  for (auto& c : h.comps) {
+    if (c.xr != 1 || c.yr != 1) fail(ST_UNSUPPORTED, "sub-sampled components are not supported by the CUDA path");
+    if (!(c.cs.cbstyle & 0x40)) fail(ST_UNSUPPORTED, "classic (non-HT) block coding is not supported by the CUDA path");
+    if (c.cs.transform != 1) fail(ST_UNSUPPORTED, "the irreversible 9/7 transform is not supported by the CUDA path");
+    if (c.q.style != 0) fail(ST_UNSUPPORTED, "quantized coding is not supported by the CUDA path");
+    if (c.cs.ndecomp != c0.cs.ndecomp) fail(ST_UNSUPPORTED, "components with different level counts");
+    if (c.precision != c0.precision || c.precision > 16) fail(ST_UNSUPPORTED, "component precision not supported by the CUDA path");
+    if ((c.cs.cbstyle & 0x08) != (c0.cs.cbstyle & 0x08)) fail(ST_UNSUPPORTED, "mixed code-block styles");
+    size_t max_res = c.cs.ndecomp, n = c.q.exps.size();
+    if (n == 0) fail(ST_DECODE, "missing step sizes");
+    if (max_res != 0 && 1 + (max_res - 1) * 3 + 2 >= n) fail(ST_DECODE, "insufficient exponents");
+  }
+  if (h.layers > 1) fail(ST_UNSUPPORTED, "multi-layer HTJ2K packet assembly");
+  const uint32_t W = h.gw, H = h.gh, L = c0.cs.ndecomp;
+  T = TileLayout();
+  T.width = W;
+  T.height = H;
+  T.ncomp = nc;
+  T.bit_depth = c0.precision;
+  T.levels = L;
+  T.mct = h.mct;
+  T.causal = (c0.cs.cbstyle & 0x08) != 0;
+  uint32_t skipped = 0;
+  if (target) {
+    uint32_t wr = W / target[0], hr = H / target[1];
+    uint32_t wl = wr ? 31 - (uint32_t)__builtin_clz(wr) : 0, hl = hr ? 31 - (uint32_t)__builtin_clz(hr) : 0;
+    skipped = std::min(std::min(wl, hl), L);
+  }
+  T.skipped = skipped;
+  T.out_w = cdiv(W, 1ull << skipped);
+  T.out_h = cdiv(H, 1ull << skipped);
+  const uint32_t nres_dec = L + 1 - skipped;
+  // Bands: LL (resolution 0), then HL, LH, HH per resolution (build.rs:18-111).
+  std::vector<Packet> packets;
+  std::vector<PrecinctBand> pbs;
+  std::vector<BlockState> blocks;
+  T.comp_band_begin.resize(nc);
+  for (uint32_t c = 0; c < nc; ++c) {
+    const CodingStyle& cs = h.comps[c].cs;
+    T.comp_band_begin[c] = (uint32_t)T.bands.size();
+    uint64_t off = 0;
+    for (uint32_t res = 0; res <= L; ++res) {
+      uint32_t d = res == 0 ? L : L - res + 1;  // decomposition level
+      uint64_t den = 1ull << d, half = d ? 1ull << (d - 1) : 0;
+      auto span = [&](uint32_t full, bool high) -> uint32_t {
+        uint64_t n = high ? (full > half ? full - half : 0) : full;
+        return (uint32_t)((n + den - 1) / den);
+      };
+      uint8_t types[3] = {BAND_HL, BAND_LH, BAND_HH};
+      uint32_t nb = res == 0 ? 1 : 3;
+      uint32_t band_first = (uint32_t)T.bands.size();
+      for (uint32_t k = 0; k < nb; ++k) {
+        Band b;
+        b.comp = (uint8_t)c;
+        b.res = (uint8_t)res;
+        b.type = res == 0 ? BAND_LL : types[k];
+        bool hx = b.type == BAND_HL || b.type == BAND_HH, hy = b.type == BAND_LH || b.type == BAND_HH;
+        b.w = span(W, hx);
+        b.h = span(H, hy);
+        size_t ei = res == 0 ? 0 : 1 + (size_t)(res - 1) * 3 + (b.type - 1);
+        if (ei >= h.comps[c].q.exps.size()) fail(ST_DECODE, "missing step size");
+        int nbp = (int)h.comps[c].q.guard + (int)h.comps[c].q.exps[ei] - 1;
+        if (nbp < 0) fail(ST_DECODE, "invalid bitplane count");
+        if (nbp > 32 && res < nres_dec) fail(ST_DECODE, "too many bitplanes");
+        b.nbp = (uint8_t)std::min(nbp, 255);
+        b.coef_off = off;
+        if (res < nres_dec) off += (uint64_t)b.w * b.h;
+        T.bands.push_back(b);
+      }
+      // Precincts of this resolution (tile.rs:487-629): the resolution rect
+      // is [0, ceil(W/2^(L-res))) x [0, ceil(H/2^(L-res))).
+      uint32_t rw = cdiv(W, 1ull << (L - res)), rh = cdiv(H, 1ull << (L - res));
+      uint32_t ppx = cs.pexp_x[res], ppy = cs.pexp_y[res];
+      if (res > 0 && (ppx == 0 || ppy == 0)) fail(ST_DECODE, "invalid precinct");
+      uint32_t npx = rw == 0 ? 0 : cdiv(rw, 1ull << ppx), npy = rh == 0 ? 0 : cdiv(rh, 1ull << ppy);
+      uint32_t sx = res > 0 ? ppx - 1 : ppx, sy = res > 0 ? ppy - 1 : ppy;  // precinct size in band coordinates
+      uint32_t xcb = std::min<uint32_t>(cs.cbw, sx), ycb = std::min<uint32_t>(cs.cbh, sy);
+      uint32_t cbw = 1u << xcb, cbh = 1u << ycb;
+      uint64_t xstep = 1ull << std::min<uint32_t>(ppx + (L - res), 63), ystep = 1ull << std::min<uint32_t>(ppy + (L - res), 63);
+      for (uint32_t py = 0; py < npy; ++py)
+        for (uint32_t px = 0; px < npx; ++px) {
+          Packet pk;
+          pk.comp = (uint8_t)c;
+          pk.res = (uint8_t)res;
+          pk.precinct = py * npx + px;
+          pk.pb_begin = (uint32_t)pbs.size();
+          pk.pb_count = nb;
+          pk.sort_px = px * xstep;
+          pk.sort_py = py * ystep;
+          for (uint32_t k = 0; k < nb; ++k) {
+            const Band& b = T.bands[band_first + k];
+            PrecinctBand pbd;
+            pbd.band = band_first + k;
+            uint64_t prx0 = (uint64_t)px << sx, pry0 = (uint64_t)py << sy;
+            uint64_t prx1 = prx0 + (1ull << sx), pry1 = pry0 + (1ull << sy);
+            uint64_t ax0 = (prx0 / cbw) * cbw, ay0 = (pry0 / cbh) * cbh;
+            uint64_t ax1 = ((std::min<uint64_t>(prx1, b.w) + cbw - 1) / cbw) * cbw;
+            uint64_t ay1 = ((std::min<uint64_t>(pry1, b.h) + cbh - 1) / cbh) * cbh;
+            pbd.cb_x0 = (uint32_t)ax0;
+            pbd.cb_y0 = (uint32_t)ay0;
+            pbd.ncx = (b.w == 0 || ax1 <= ax0) ? 0 : (uint32_t)((ax1 - ax0) / cbw);
+            pbd.ncy = (b.h == 0 || ay1 <= ay0) ? 0 : (uint32_t)((ay1 - ay0) / cbh);
+            pbd.cbw = cbw;
+            pbd.cbh = cbh;
+            pbd.first_block = (uint32_t)blocks.size();
+            if ((uint64_t)pbd.ncx * pbd.ncy > (1u << 24)) fail(ST_DECODE, "too many code blocks");
+            for (uint32_t yi = 0; yi < pbd.ncy; ++yi)
+              for (uint32_t xi = 0; xi < pbd.ncx; ++xi) {
+                BlockState bs;
+                bs.band = pbd.band;
+                bs.x0 = pbd.cb_x0 + xi * cbw;
+                bs.y0 = pbd.cb_y0 + yi * cbh;
+                bs.w = std::min<uint32_t>(bs.x0 + cbw, b.w) - bs.x0;
+                bs.h = std::min<uint32_t>(bs.y0 + cbh, b.h) - bs.y0;
+                blocks.push_back(bs);
+              }
+            pbd.incl.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1));
+            pbd.zbp.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1));
+            pbs.push_back(std::move(pbd));
+          }
+          packets.push_back(pk);
+        }
+    }
+    T.coef_per_comp = off;
+  }
+  // Packet order (progression.rs:114-338), one layer.
+  std::vector<uint32_t> order(packets.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (uint32_t)i;
+  auto key = [&](const Packet& p) {
+    switch (h.prog) {
+      case 0: case 1:  // LRCP / RLCP with one layer: resolution, component, precinct
+        return std::make_tuple((uint64_t)p.res, (uint64_t)p.comp, (uint64_t)0, (uint64_t)0, (uint64_t)p.precinct);
+      case 2:  // RPCL
+        return std::make_tuple((uint64_t)p.res, p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.precinct);
+      case 3:  // PCRL
+        return std::make_tuple(p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.res, (uint64_t)p.precinct);
+      default:  // CPRL
+        return std::make_tuple((uint64_t)p.comp, p.sort_py, p.sort_px, (uint64_t)p.res, (uint64_t)p.precinct);
+    }
+  };
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key(packets[a]) < key(packets[b]); });
+  // Packet headers and bodies (segment.rs:53-148, :304-394, :409-479, :508-581).
+  size_t next_packet = 0;
+  for (auto& part : parts) {
+    Reader pr(data + part.first, part.second);
+    bool ok = true;
+    while (ok && !pr.end()) {
+      if (next_packet >= order.size()) { ok = false; break; }
+      const Packet& pk = packets[order[next_packet++]];
+      const CodingStyle& cs = h.comps[pk.comp].cs;
+      uint8_t mk;
+      if ((cs.flags & 2) && pr.peek_marker(mk) && mk == 0x91) {
+        pr.marker(mk);
+        if (!pr.skip(4)) { ok = false; break; }
+      }
+      uint32_t nz;
+      if (!pr.bits(1, nz)) { ok = false; break; }
+      for (uint32_t k = 0; nz && ok && k < pk.pb_count; ++k) {
+        PrecinctBand& pb = pbs[pk.pb_begin + k];
+        for (uint32_t yi = 0; ok && yi < pb.ncy; ++yi)
+          for (uint32_t xi = 0; ok && xi < pb.ncx; ++xi) {
+            BlockState& bs = blocks[pb.first_block + yi * pb.ncx + xi];
+            bool first = !bs.included;
+            uint32_t v;
+            bool inc;
+            if (bs.included) {
+              if (!pr.bits(1, v)) { ok = false; break; }
+              inc = v == 1;
+            } else {
+              if (!pb.incl.read(xi, yi, 1, pr, v)) { ok = false; break; }
+              inc = v == 0;
+            }
+            if (!inc) continue;
+            if (first) {
+              if (!pb.zbp.read(xi, yi, UINT32_MAX, pr, v)) { ok = false; break; }
+              bs.missing = (uint8_t)v;
+            }
+            bs.included = true;
+            if (!first || bs.passes != 0) { ok = false; break; }
+            uint32_t np = 1, b;
+            if (!pr.bits(1, b)) { ok = false; break; }
+            if (b) {
+              np = 2;
+              if (!pr.bits(1, b)) { ok = false; break; }
+              if (b) {
+                uint32_t e;
+                if (!pr.bits(2, e)) { ok = false; break; }
+                np = 3 + e;
+                if (e == 3) {
+                  if (!pr.bits(5, e)) { ok = false; break; }
+                  np = 6 + e;
+                  if (e == 31) {
+                    if (!pr.bits(7, e)) { ok = false; break; }
+                    np = 37 + e;
+                  }
+                }
+              }
+            }
+            if (np > 94) { ok = false; break; }
+            uint32_t groups = (np - 1) / 3;
+            if ((uint32_t)bs.missing + groups > 255) { ok = false; break; }
+            uint32_t ph = groups * 3, actual = np - ph;
+            uint32_t incr = 0;
+            for (;;) {
+              if (!pr.bits(1, b)) { ok = false; break; }
+              if (!b) break;
+              ++incr;
+            }
+            if (!ok) break;
+            bs.lblock += incr;
+            uint32_t nbits = bs.lblock + (31 - (uint32_t)__builtin_clz(ph + 1));
+            uint32_t lcup;
+            if (nbits > 255 || !pr.bits(nbits, lcup) || lcup < 2 || lcup >= 65535) { ok = false; break; }
+            uint32_t lref = 0;
+            if (actual > 1) {
+              uint32_t rb = bs.lblock + (actual > 2 ? 1 : 0);
+              if (rb > 255 || !pr.bits(rb, lref) || lref >= 2047) { ok = false; break; }
+            }
+            bs.missing = (uint8_t)(bs.missing + groups);
+            bs.passes = (uint8_t)actual;
+            bs.lcup = lcup;
+            bs.lref = lref;
+          }
+      }
+      if (!ok) break;
+      pr.align();
+      if (cs.flags & 4) {
+        if (!pr.marker(mk) || mk != 0x92) { ok = false; break; }
+      }
+      for (uint32_t k = 0; nz && ok && k < pk.pb_count; ++k) {
+        PrecinctBand& pb = pbs[pk.pb_begin + k];
+        for (uint32_t i = 0; ok && i < pb.ncx * pb.ncy; ++i) {
+          BlockState& bs = blocks[pb.first_block + i];
+          if (bs.passes == 0 || bs.cleanup_off >= 0) continue;
+          size_t at = part.first + pr.pos();
+          if (!pr.skip(bs.lcup)) { ok = false; break; }
+          bs.cleanup_off = (int64_t)at;
+          if (bs.passes > 1) {
+            size_t at2 = part.first + pr.pos();
+            if (!pr.skip(bs.lref)) { ok = false; break; }
+            bs.ref_off = (int64_t)at2;
+          }
+        }
+      }
+    }
+  }
+  // Segment table for the decoded resolutions (decode.rs:1554-1718 checks).
+  for (const BlockState& bs : blocks) {
+    const Band& b = T.bands[bs.band];
+    if (b.res >= nres_dec || bs.w == 0 || bs.h == 0) continue;
+    CodeBlock cb;
+    cb.band = bs.band;
+    cb.x0 = bs.x0;
+    cb.y0 = bs.y0;
+    cb.w = (uint16_t)bs.w;
+    cb.h = (uint16_t)bs.h;
+    cb.missing_msbs = bs.missing;
+    cb.passes = bs.passes;
+    cb.cleanup_off = 0;
+    cb.lcup = 0;
+    cb.ref_off = 0;
+    cb.lref = 0;
+    uint32_t nbp = b.nbp;
+    uint32_t actual = nbp > bs.missing ? nbp - bs.missing : 0;
+    if (nbp > 31) fail(ST_DECODE, "too many bitplanes");
+    if (nbp == 0 || bs.passes == 0 || actual == 0) {
+      cb.passes = 0;  // all-zero block
+    } else {
+      uint32_t passes = bs.passes;
+      if (passes > 1 && (bs.ref_off < 0 || bs.lref == 0)) passes = 1;
+      if (bs.cleanup_off < 0) fail(ST_DECODE, "code-block decode failure: missing cleanup segment data");
+      if (passes > 3 || bs.missing >= 30 || bs.lcup < 2) fail(ST_DECODE, "code-block decode failure");
+      if (bs.missing == 29 && passes > 1) passes = 1;
+      cb.passes = (uint8_t)passes;
+      cb.cleanup_off = (uint32_t)bs.cleanup_off;
+      cb.lcup = bs.lcup;
+      if (passes > 1) {
+        cb.ref_off = (uint32_t)bs.ref_off;
+        cb.lref = bs.lref;
+      }
+    }
+    T.blocks.push_back(cb);
+  }
+}
+
+}  // namespace sgn

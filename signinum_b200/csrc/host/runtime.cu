@@ -1,0 +1,740 @@
+// Context, device plans and the C ABI of the CUDA decode path.
+//
+// A plan is the device form of one decode call: the codestreams copied once
+// into a device arena, one HtJob per code block (ordered by coded length),
+// the IDWT level jobs of every tile grouped into rounds (coarse to fine) and
+// one fused last-level/pack job per tile writing straight into the output
+// surfaces.  Executing a plan is a fixed sequence of launches on the context
+// stream, so a plan can be replayed and captured in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#include "../../../include/signinum_j2k_cuda.h"
+#include "../device_plan.h"
+#include "../ht_tables.h"
+#include "../kernels/kernels.h"
+#include "codestream.h"
+
+using namespace sgn;
+
+namespace {
+
+thread_local char g_msg[512];
+
+sgn_status set_error(sgn_status s, const char* msg) {
+  std::snprintf(g_msg, sizeof(g_msg), "%s", msg ? msg : "");
+  return s;
+}
+
+sgn_status cuda_status(cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return SGN_OK;
+  char buf[400];
+  std::snprintf(buf, sizeof(buf), "CUDA runtime error in %s: %s", where, cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return set_error(SGN_ERR_OUT_OF_MEMORY, buf);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return set_error(SGN_ERR_CUDA_UNAVAILABLE, buf);
+  return set_error(SGN_ERR_CUDA_RUNTIME, buf);
+}
+
+int bytes_per_pixel(uint32_t fmt) {
+  static const int b[] = {1, 3, 4, 2, 6, 8};
+  return fmt < 6 ? b[fmt] : 0;
+}
+
+// Minimal fixed pool for host-side parsing of large batches.
+class Workers {
+ public:
+  explicit Workers(unsigned n) {
+    for (unsigned i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
+  }
+  ~Workers() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+  size_t size() const { return threads_.size(); }
+  // Runs f(i) for i in [0, n) over the pool plus the calling thread.
+  void parallel_for(size_t n, const std::function<void(size_t)>& f) {
+    if (n == 0) return;
+    if (threads_.empty() || n < 4) {
+      for (size_t i = 0; i < n; ++i) f(i);
+      return;
+    }
+    std::atomic<size_t> next{0};
+    std::atomic<size_t> done_workers{0};
+    size_t nw = std::min(threads_.size(), n);
+    auto body = [&] {
+      for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    };
+    {
+      std::lock_guard<std::mutex> g(m_);
+      for (size_t k = 0; k < nw; ++k)
+        tasks_.push_back([&] {
+          body();
+          done_workers.fetch_add(1);
+          cv_done_.notify_all();
+        });
+    }
+    cv_.notify_all();
+    body();
+    std::unique_lock<std::mutex> lk(m_);
+    cv_done_.wait(lk, [&] { return done_workers.load() == nw; });
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void()> t;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+        if (stop_ && tasks_.empty()) return;
+        t = std::move(tasks_.back());
+        tasks_.pop_back();
+      }
+      t();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::vector<std::function<void()>> tasks_;
+  std::mutex m_;
+  std::condition_variable cv_, cv_done_;
+  bool stop_ = false;
+};
+
+struct PinnedBuffer {
+  uint8_t* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t c = std::max<size_t>(n, cap * 2);
+    cudaError_t e = cudaMallocHost((void**)&p, c);
+    if (e == cudaSuccess) cap = c;
+    return e;
+  }
+  ~PinnedBuffer() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+}  // namespace
+
+struct sgn_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  std::atomic<uint64_t> submissions{0};
+  std::mutex mu;
+  PinnedBuffer staging;
+  Workers* workers = nullptr;
+};
+
+struct RoundInfo {
+  uint32_t job_begin, njobs, ctas;
+};
+
+struct sgn_plan {
+  size_t n = 0;
+  uint32_t format = 0;
+  std::vector<sgn_status> status;  // host-side (parse/request) status per tile
+  std::vector<sgn_surface> surfaces;
+  // Device allocations (stream-ordered pool).
+  uint8_t* d_input = nullptr;
+  int32_t* d_coef = nullptr;
+  int32_t* d_levels = nullptr;
+  HtJob* d_ht = nullptr;
+  uint32_t* d_refine = nullptr;
+  IdwtJob* d_idwt = nullptr;
+  PackJob* d_pack = nullptr;
+  uint32_t* d_status = nullptr;
+  uint32_t nht = 0, max_nq = 1, nref = 0, npack = 0, pack_ctas = 0;
+  std::vector<RoundInfo> rounds;
+  uint64_t launches = 0;
+  std::vector<uint32_t> h_status;
+};
+
+namespace {
+
+struct TileWork {
+  TileLayout layout;
+  sgn_status status = SGN_OK;
+  uint32_t crop_x = 0, crop_y = 0, crop_w = 0, crop_h = 0;
+  uint32_t region_conv = 0;
+};
+
+// Request semantics: DeviceDecodePlan::for_image (device_plan.rs:23-51) for
+// the output rectangle, decode_scaled_from_info / decode_region_scaled_from_info
+// (crates/signinum-j2k/src/decode.rs:12-71) for the reduced resolution.
+void prepare_tile(const uint8_t* data, size_t len, uint32_t fmt, const sgn_request* req, TileWork& tw) {
+  try {
+    if (fmt == SGN_FMT_RGBA16) throw ParseError{SGN_ERR_UNSUPPORTED, "Rgba16 output is not supported"};
+    if (fmt > SGN_FMT_RGBA16) throw ParseError{SGN_ERR_INVALID_ARGUMENT, "unknown pixel format"};
+    Info info = inspect_codestream(data, len);
+    uint32_t kind = req ? req->kind : SGN_REQ_FULL;
+    uint32_t sx = 0, sy = 0, sw = info.width, sh = info.height, d = 1;
+    if (kind == SGN_REQ_REGION || kind == SGN_REQ_REGION_SCALED) {
+      sx = req->x;
+      sy = req->y;
+      sw = req->w;
+      sh = req->h;
+    }
+    if (kind == SGN_REQ_SCALED || kind == SGN_REQ_REGION_SCALED) d = req->downscale;
+    if (kind > SGN_REQ_REGION_SCALED) throw ParseError{SGN_ERR_INVALID_ARGUMENT, "unknown request kind"};
+    if (d != 1 && d != 2 && d != 4 && d != 8) throw ParseError{SGN_ERR_UNSUPPORTED, "unknown downscale"};
+    if ((uint64_t)sx + sw > info.width || (uint64_t)sy + sh > info.height)
+      throw ParseError{SGN_ERR_REGION, "region outside the image"};
+    uint32_t ox0 = sx / d, oy0 = sy / d;
+    uint32_t ox1 = (uint32_t)(((uint64_t)sx + sw + d - 1) / d), oy1 = (uint32_t)(((uint64_t)sy + sh + d - 1) / d);
+    uint32_t target[2] = {(info.width + d - 1) / d, (info.height + d - 1) / d};
+    parse_tile(data, len, d == 1 ? nullptr : target, tw.layout);
+    const TileLayout& L = tw.layout;
+    bool gray = L.ncomp == 1;
+    bool ok_map = (gray && (fmt == SGN_FMT_GRAY8 || fmt == SGN_FMT_GRAY16)) ||
+                  (!gray && (fmt == SGN_FMT_RGB8 || fmt == SGN_FMT_RGBA8 || fmt == SGN_FMT_RGB16));
+    if (!ok_map) throw ParseError{SGN_ERR_UNSUPPORTED, "backend color space cannot be mapped to requested pixel format"};
+    if (kind == SGN_REQ_SCALED) {
+      if (L.out_w != ox1 - ox0 || L.out_h != oy1 - oy0)
+        throw ParseError{SGN_ERR_BUFFER, "output buffer does not match the reduced image"};
+    } else if (kind == SGN_REQ_REGION_SCALED && d > 1) {
+      if (ox1 > L.out_w || oy1 > L.out_h) throw ParseError{SGN_ERR_REGION, "scaled region outside the reduced image"};
+    }
+    tw.crop_x = ox0;
+    tw.crop_y = oy0;
+    tw.crop_w = ox1 - ox0;
+    tw.crop_h = oy1 - oy0;
+    tw.region_conv = (kind == SGN_REQ_REGION || kind == SGN_REQ_REGION_SCALED) ? 1 : 0;
+    tw.status = SGN_OK;
+  } catch (const ParseError& e) {
+    tw.status = e.status;
+  }
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count, cudaStream_t s) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMallocAsync((void**)p, count * sizeof(T), s);
+}
+
+void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
+  void* ptrs[] = {p->d_input, p->d_coef, p->d_levels, p->d_ht, p->d_refine, p->d_idwt, p->d_pack, p->d_status};
+  for (void* q : ptrs)
+    if (q) cudaFreeAsync(q, s);
+  p->d_input = nullptr;
+  p->d_coef = p->d_levels = nullptr;
+  p->d_ht = nullptr;
+  p->d_refine = nullptr;
+  p->d_idwt = nullptr;
+  p->d_pack = nullptr;
+  p->d_status = nullptr;
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t fmt,
+                      const sgn_request* reqs, sgn_plan* plan) {
+  plan->n = n;
+  plan->format = fmt;
+  plan->status.assign(n, SGN_OK);
+  plan->surfaces.assign(n, sgn_surface{});
+  std::vector<TileWork> work(n);
+  ctx->workers->parallel_for(n, [&](size_t i) {
+    if (!datas[i] && lens[i]) {
+      work[i].status = SGN_ERR_INVALID_ARGUMENT;
+      return;
+    }
+    prepare_tile(datas[i], lens[i], fmt, reqs ? &reqs[i] : nullptr, work[i]);
+  });
+  // Arena layout.
+  std::vector<uint64_t> in_off(n, 0), coef_off(n, 0), lvl_off(n, 0), lvl_size(n, 0);
+  uint64_t in_total = 0, coef_total = 0, lvl_total = 0;
+  size_t nblocks = 0, nlevel_jobs = 0;
+  uint32_t max_rounds = 0;
+  for (size_t i = 0; i < n; ++i) {
+    plan->status[i] = work[i].status;
+    if (work[i].status != SGN_OK) continue;
+    const TileLayout& L = work[i].layout;
+    in_off[i] = in_total;
+    in_total += (lens[i] + 15) & ~(size_t)15;
+    coef_off[i] = coef_total;
+    coef_total += L.coef_per_comp * L.ncomp;
+    uint32_t R = L.levels - L.skipped;  // last decoded resolution
+    if (R >= 2) {
+      uint32_t d = L.skipped + 1;
+      uint64_t w = (L.width + (1ull << d) - 1) >> d, h = (L.height + (1ull << d) - 1) >> d;
+      lvl_size[i] = w * h;
+      lvl_off[i] = lvl_total;
+      lvl_total += 2 * w * h * L.ncomp;
+      nlevel_jobs += (size_t)(R - 1) * L.ncomp;
+      max_rounds = std::max(max_rounds, R - 1);
+    }
+    nblocks += L.blocks.size();
+  }
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  if ((e = dalloc(&plan->d_input, in_total, s)) != cudaSuccess) return cuda_status(e, "input arena");
+  if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
+  if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
+  if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
+  // HT jobs, longest segments first.
+  std::vector<HtJob> ht;
+  ht.reserve(nblocks);
+  std::vector<uint32_t> refine;
+  uint32_t max_nq = 1;
+  for (size_t i = 0; i < n; ++i) {
+    if (plan->status[i] != SGN_OK) continue;
+    const TileLayout& L = work[i].layout;
+    for (const CodeBlock& cb : L.blocks) {
+      const Band& b = L.bands[cb.band];
+      HtJob j;
+      std::memset(&j, 0, sizeof(j));
+      j.src = in_off[i] + cb.cleanup_off;
+      j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+      j.lcup = cb.lcup;
+      j.tile = (uint32_t)i;
+      j.stride = b.w;
+      j.lref = (uint16_t)cb.lref;
+      j.w = cb.w;
+      j.h = cb.h;
+      j.mmsb = cb.missing_msbs;
+      j.passes = cb.passes;
+      j.nbp = b.nbp;
+      j.flags = L.causal ? 1 : 0;
+      max_nq = std::max<uint32_t>(max_nq, (cb.w + 1) / 2);
+      ht.push_back(j);
+    }
+  }
+  std::stable_sort(ht.begin(), ht.end(), [](const HtJob& a, const HtJob& b) { return a.lcup > b.lcup; });
+  for (size_t k = 0; k < ht.size(); ++k)
+    if (ht[k].passes > 1) refine.push_back((uint32_t)k);
+  plan->nht = (uint32_t)ht.size();
+  plan->max_nq = max_nq;
+  plan->nref = (uint32_t)refine.size();
+  // IDWT rounds: round r-1 holds resolution r of every tile that has it.
+  std::vector<std::vector<IdwtJob>> rounds(max_rounds);
+  std::vector<PackJob> packs;
+  auto band_ptr = [&](size_t i, uint32_t c, uint32_t bi) -> int32_t* {
+    const TileLayout& L = work[i].layout;
+    return plan->d_coef + coef_off[i] + (uint64_t)c * L.coef_per_comp + L.bands[bi].coef_off;
+  };
+  for (size_t i = 0; i < n; ++i) {
+    if (plan->status[i] != SGN_OK) continue;
+    const TileLayout& L = work[i].layout;
+    const uint32_t R = L.levels - L.skipped;
+    auto lvl = [&](uint32_t c, uint32_t r) {
+      return plan->d_levels + lvl_off[i] + ((uint64_t)c * 2 + (r & 1)) * lvl_size[i];
+    };
+    auto res_dim = [&](uint32_t r, bool wdim) {
+      uint32_t sh = L.levels - r;
+      uint64_t v = wdim ? L.width : L.height;
+      return (uint32_t)((v + (1ull << sh) - 1) >> sh);
+    };
+    for (uint32_t c = 0; c < L.ncomp; ++c) {
+      uint32_t b0 = L.comp_band_begin[c];
+      for (uint32_t r = 1; r < R; ++r) {
+        IdwtJob j;
+        j.ll = r == 1 ? band_ptr(i, c, b0) : lvl(c, r - 1);
+        j.hl = band_ptr(i, c, b0 + 1 + (r - 1) * 3);
+        j.lh = band_ptr(i, c, b0 + 2 + (r - 1) * 3);
+        j.hh = band_ptr(i, c, b0 + 3 + (r - 1) * 3);
+        j.out = lvl(c, r);
+        j.w = res_dim(r, true);
+        j.h = res_dim(r, false);
+        j.tiles_x = (j.w + kIdwtTileW - 1) / kIdwtTileW;
+        j.cta_begin = 0;
+        if (j.w == 0 || j.h == 0) continue;
+        rounds[r - 1].push_back(j);
+      }
+    }
+    // Output surface.
+    const TileWork& tw = work[i];
+    sgn_surface& sf = plan->surfaces[i];
+    sf.width = tw.crop_w;
+    sf.height = tw.crop_h;
+    sf.format = fmt;
+    sf.backend = SGN_BACKEND_CUDA;
+    sf.pitch_bytes = (uint64_t)tw.crop_w * bytes_per_pixel(fmt);
+    size_t bytes = std::max<size_t>((size_t)sf.pitch_bytes * sf.height, 1);
+    void* outp = nullptr;
+    if ((e = cudaMallocAsync(&outp, bytes, s)) != cudaSuccess) return cuda_status(e, "surface");
+    sf.device_ptr = (uint64_t)(uintptr_t)outp;
+    if (tw.crop_w == 0 || tw.crop_h == 0) continue;
+    PackJob pj;
+    std::memset(&pj, 0, sizeof(pj));
+    for (uint32_t c = 0; c < L.ncomp && c < 3; ++c) {
+      uint32_t b0 = L.comp_band_begin[c];
+      if (R == 0) {
+        pj.ll[c] = band_ptr(i, c, b0);
+      } else {
+        pj.ll[c] = R == 1 ? band_ptr(i, c, b0) : lvl(c, R - 1);
+        pj.hl[c] = band_ptr(i, c, b0 + 1 + (R - 1) * 3);
+        pj.lh[c] = band_ptr(i, c, b0 + 2 + (R - 1) * 3);
+        pj.hh[c] = band_ptr(i, c, b0 + 3 + (R - 1) * 3);
+      }
+    }
+    pj.out = (uint8_t*)outp;
+    pj.pitch = sf.pitch_bytes;
+    pj.w = L.out_w;
+    pj.h = L.out_h;
+    pj.cx = tw.crop_x;
+    pj.cy = tw.crop_y;
+    pj.cw = tw.crop_w;
+    pj.ch = tw.crop_h;
+    pj.lifting = R > 0 ? 1 : 0;
+    pj.ncomp = L.ncomp;
+    pj.mct = (L.mct && L.ncomp >= 3) ? 1 : 0;
+    pj.bit_depth = L.bit_depth;
+    pj.fmt = fmt;
+    pj.region_conv = tw.region_conv;
+    uint32_t ax = tw.crop_x & ~1u, ay = tw.crop_y & ~1u;
+    pj.tiles_x = (tw.crop_x + tw.crop_w - ax + kIdwtTileW - 1) / kIdwtTileW;
+    uint32_t tiles_y = (tw.crop_y + tw.crop_h - ay + kIdwtTileH - 1) / kIdwtTileH;
+    pj.cta_begin = plan->pack_ctas;
+    pj.tile = (uint32_t)i;
+    plan->pack_ctas += pj.tiles_x * tiles_y;
+    packs.push_back(pj);
+  }
+  // Flatten the rounds.
+  std::vector<IdwtJob> idwt;
+  for (auto& rj : rounds) {
+    RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0};
+    for (IdwtJob& j : rj) {
+      j.cta_begin = ri.ctas;
+      ri.ctas += j.tiles_x * ((j.h + kIdwtTileH - 1) / kIdwtTileH);
+      idwt.push_back(j);
+    }
+    if (ri.njobs) plan->rounds.push_back(ri);
+  }
+  plan->npack = (uint32_t)packs.size();
+  if ((e = dalloc(&plan->d_ht, ht.size(), s)) != cudaSuccess) return cuda_status(e, "ht jobs");
+  if ((e = dalloc(&plan->d_refine, refine.size(), s)) != cudaSuccess) return cuda_status(e, "refine list");
+  if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
+  if ((e = dalloc(&plan->d_pack, packs.size(), s)) != cudaSuccess) return cuda_status(e, "pack jobs");
+  // Uploads: codestreams (one copy when the caller's buffers are pinned and
+  // contiguous, else through the pinned staging buffer) and the tables.
+  size_t tables = ht.size() * sizeof(HtJob) + refine.size() * 4 + idwt.size() * sizeof(IdwtJob) +
+                  packs.size() * sizeof(PackJob) + 64;
+  bool direct = n > 0 && in_total > 0;
+  // Contiguity in arena order (16-byte padded) is needed for a single copy.
+  for (size_t i = 0; direct && i + 1 < n; ++i)
+    direct = plan->status[i] == SGN_OK && plan->status[i + 1] == SGN_OK &&
+             datas[i + 1] == datas[i] + ((lens[i] + 15) & ~(size_t)15);
+  direct = direct && plan->status[0] == SGN_OK && is_pinned(datas[0]);
+  size_t stage_bytes = tables + (direct ? 0 : in_total);
+  if ((e = ctx->staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
+  uint8_t* st = ctx->staging.p;
+  size_t at = 0;
+  auto stage = [&](const void* src, size_t bytes) {
+    uint8_t* p = st + at;
+    if (bytes) std::memcpy(p, src, bytes);
+    at += (bytes + 15) & ~(size_t)15;
+    return p;
+  };
+  if (direct) {
+    if ((e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_status(e, "input upload");
+  } else if (in_total) {
+    uint8_t* dst = st;
+    ctx->workers->parallel_for(n, [&](size_t i) {
+      if (plan->status[i] == SGN_OK) std::memcpy(dst + in_off[i], datas[i], lens[i]);
+    });
+    at = (in_total + 15) & ~(size_t)15;
+    if ((e = cudaMemcpyAsync(plan->d_input, st, in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_status(e, "input upload");
+  }
+  struct Up {
+    void* d;
+    const void* h;
+    size_t bytes;
+  } ups[] = {{plan->d_ht, ht.data(), ht.size() * sizeof(HtJob)},
+             {plan->d_refine, refine.data(), refine.size() * 4},
+             {plan->d_idwt, idwt.data(), idwt.size() * sizeof(IdwtJob)},
+             {plan->d_pack, packs.data(), packs.size() * sizeof(PackJob)}};
+  for (auto& u : ups) {
+    if (!u.bytes) continue;
+    void* p = stage(u.h, u.bytes);
+    if ((e = cudaMemcpyAsync(u.d, p, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_status(e, "table upload");
+  }
+  // The staging buffer is reused by the next call: finish the copies now.
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
+  plan->launches = 1 + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0);
+  for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
+  return SGN_OK;
+}
+
+sgn_status execute(sgn_ctx* ctx, sgn_plan* p) {
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  if (p->n && (e = cudaMemsetAsync(p->d_status, 0, p->n * sizeof(uint32_t), s)) != cudaSuccess)
+    return cuda_status(e, "status reset");
+  if ((e = launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_coef, p->d_status, p->max_nq, s)) != cudaSuccess)
+    return cuda_status(e, "HT cleanup launch");
+  if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
+    return cuda_status(e, "HT refinement launch");
+  for (const RoundInfo& r : p->rounds)
+    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s)) != cudaSuccess)
+      return cuda_status(e, "IDWT launch");
+  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, s)) != cudaSuccess) return cuda_status(e, "pack launch");
+  return SGN_OK;
+}
+
+sgn_status wait_plan(sgn_ctx* ctx, sgn_plan* p, sgn_status* per_tile, size_t* first_failing) {
+  cudaError_t e;
+  p->h_status.assign(p->n, 0);
+  if (p->n && (e = cudaMemcpyAsync(p->h_status.data(), p->d_status, p->n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
+                  cudaSuccess)
+    return cuda_status(e, "status download");
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(e, "decode");
+  size_t first = SIZE_MAX;
+  sgn_status first_status = SGN_OK;
+  for (size_t i = 0; i < p->n; ++i) {
+    sgn_status st = p->status[i];
+    if (st == SGN_OK && p->h_status[i] != 0) st = SGN_ERR_DECODE;
+    if (per_tile) per_tile[i] = st;
+    if (st != SGN_OK && first == SIZE_MAX) {
+      first = i;
+      first_status = st;
+    }
+  }
+  if (first_failing) *first_failing = first;
+  if (first_status != SGN_OK) set_error(first_status, "tile decode failed");
+  return first_status;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sgn_last_error_message(void) { return g_msg; }
+
+sgn_status sgn_ctx_create(int device, sgn_ctx** out) {
+  if (!out) return set_error(SGN_ERR_INVALID_ARGUMENT, "null output");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return set_error(SGN_ERR_CUDA_UNAVAILABLE, "CUDA is unavailable on this host");
+  }
+  if (device < 0 || device >= count) return set_error(SGN_ERR_INVALID_ARGUMENT, "device index out of range");
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+  sgn_ctx* c = new sgn_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete c;
+    return cuda_status(e, "cudaStreamCreate");
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  static std::once_flag tables_once;
+  static cudaError_t tables_err = cudaSuccess;
+  std::call_once(tables_once, [] {
+    HtDecodeTables t;
+    build_decode_tables(t);
+    tables_err = upload_ht_tables(t);
+    if (tables_err == cudaSuccess) tables_err = ht_kernels_init();
+  });
+  if (tables_err != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return cuda_status(tables_err, "HT table upload");
+  }
+  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  c->workers = new Workers(std::min(hw, 32u) - 1);
+  *out = c;
+  return SGN_OK;
+}
+
+void sgn_ctx_destroy(sgn_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx->workers;
+  delete ctx;
+}
+
+uint64_t sgn_ctx_submissions(const sgn_ctx* ctx) { return ctx ? ctx->submissions.load() : 0; }
+
+void* sgn_ctx_stream(sgn_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+void sgn_ht_lookup_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1) {
+  HtDecodeTables t;
+  build_decode_tables(t);
+  if (vlc0) std::memcpy(vlc0, t.vlc[0], sizeof(t.vlc[0]));
+  if (vlc1) std::memcpy(vlc1, t.vlc[1], sizeof(t.vlc[1]));
+  if (uvlc0) std::memcpy(uvlc0, t.uvlc0, sizeof(t.uvlc0));
+  if (uvlc1) std::memcpy(uvlc1, t.uvlc1, sizeof(t.uvlc1));
+}
+
+sgn_status sgn_j2k_inspect(const uint8_t* data, size_t len, sgn_info* out) {
+  if (!data || !out) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    Info i = inspect_codestream(data, len);
+    *out = {i.width, i.height, i.components, i.bit_depth, i.levels, i.tiles, i.ht, i.reversible, i.mct};
+    return SGN_OK;
+  } catch (const ParseError& e) {
+    return set_error(e.status, e.message.c_str());
+  }
+}
+
+static sgn_status check_backend(uint32_t backend) {
+  if (backend == SGN_BACKEND_CUDA || backend == SGN_BACKEND_AUTO) return SGN_OK;
+  if (backend == SGN_BACKEND_CPU || backend == SGN_BACKEND_METAL)
+    return set_error(SGN_ERR_UNSUPPORTED_BACKEND, "backend request is not supported by this CUDA decoder");
+  return set_error(SGN_ERR_INVALID_ARGUMENT, "unknown backend request");
+}
+
+sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t format,
+                           const sgn_request* requests, sgn_plan** out, sgn_status* per_tile) {
+  if (!ctx || !out || (n && (!datas || !lens))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  sgn_plan* p = new sgn_plan();
+  sgn_status st;
+  try {
+    st = build_plan(ctx, datas, lens, n, format, requests, p);
+  } catch (const std::bad_alloc&) {
+    st = set_error(SGN_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+  if (st != SGN_OK) {
+    for (auto& sf : p->surfaces)
+      if (sf.device_ptr) cudaFreeAsync((void*)(uintptr_t)sf.device_ptr, ctx->stream);
+    free_plan_buffers(p, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    delete p;
+    return st;
+  }
+  if (per_tile)
+    for (size_t i = 0; i < n; ++i) per_tile[i] = p->status[i];
+  *out = p;
+  return SGN_OK;
+}
+
+sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan) {
+  if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  cudaSetDevice(ctx->device);
+  return execute(ctx, plan);
+}
+
+sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing) {
+  if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  cudaSetDevice(ctx->device);
+  return wait_plan(ctx, plan, per_tile, first_failing);
+}
+
+sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n) {
+  if (!plan || (n && !outs) || n > plan->n) return set_error(SGN_ERR_INVALID_ARGUMENT, "bad arguments");
+  for (size_t i = 0; i < n; ++i) outs[i] = plan->surfaces[i];
+  return SGN_OK;
+}
+
+uint64_t sgn_plan_kernel_launches(const sgn_plan* plan) { return plan ? plan->launches : 0; }
+
+void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan) {
+  if (!ctx || !plan) return;
+  cudaSetDevice(ctx->device);
+  for (auto& sf : plan->surfaces)
+    if (sf.device_ptr) cudaFreeAsync((void*)(uintptr_t)sf.device_ptr, ctx->stream);
+  free_plan_buffers(plan, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  delete plan;
+}
+
+sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
+                                          uint32_t format, const sgn_request* requests, uint32_t backend,
+                                          sgn_surface* outs, sgn_status* per_tile, size_t* first_failing) {
+  if (!ctx || (n && (!datas || !lens || !outs))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  sgn_status bs = check_backend(backend);
+  if (bs != SGN_OK) return bs;
+  if (first_failing) *first_failing = SIZE_MAX;
+  for (size_t i = 0; i < n; ++i) outs[i] = sgn_surface{};
+  if (n == 0) return SGN_OK;
+  sgn_plan* p = nullptr;
+  sgn_status st = sgn_plan_create(ctx, datas, lens, n, format, requests, &p, nullptr);
+  if (st != SGN_OK) return st;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->submissions.fetch_add(1);
+  st = execute(ctx, p);
+  std::vector<sgn_status> statuses(n);
+  sgn_status wst = st == SGN_OK ? wait_plan(ctx, p, statuses.data(), first_failing) : st;
+  for (size_t i = 0; i < n; ++i) {
+    if (per_tile) per_tile[i] = st == SGN_OK ? statuses[i] : st;
+    if (st == SGN_OK && statuses[i] == SGN_OK) {
+      outs[i] = p->surfaces[i];
+      p->surfaces[i].device_ptr = 0;  // ownership moves to the caller
+    }
+  }
+  for (auto& sf : p->surfaces)
+    if (sf.device_ptr) cudaFreeAsync((void*)(uintptr_t)sf.device_ptr, ctx->stream);
+  p->surfaces.clear();
+  free_plan_buffers(p, ctx->stream);
+  delete p;
+  return wst;
+}
+
+sgn_status sgn_j2k_decode_to_device(sgn_ctx* ctx, const uint8_t* data, size_t len, uint32_t format,
+                                    const sgn_request* request, uint32_t backend, sgn_surface* out) {
+  if (!ctx || !data || !out) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  sgn_status tile_status = SGN_OK;
+  size_t first = 0;
+  sgn_status st = sgn_j2k_decode_tiles_to_device(ctx, &data, &len, 1, format, request, backend, out, &tile_status,
+                                                 &first);
+  if (st != SGN_OK) return st;
+  return tile_status;
+}
+
+sgn_status sgn_surface_download(sgn_ctx* ctx, const sgn_surface* sf, uint8_t* out, size_t out_len, size_t stride) {
+  if (!ctx || !sf || (!out && out_len)) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  size_t row = (size_t)sf->pitch_bytes;
+  if (sf->height == 0 || row == 0) return SGN_OK;
+  // validate_strided_output_buffer: stride covers a row and the buffer covers
+  // (h - 1) strides plus one row.
+  if (stride < row || out_len < stride * (sf->height - 1) + row)
+    return set_error(SGN_ERR_BUFFER, "output buffer too small for the surface");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaMemcpy2DAsync(out, stride, (const void*)(uintptr_t)sf->device_ptr, row, row, sf->height,
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_status(e, "surface download");
+}
+
+void sgn_surface_free(sgn_ctx* ctx, sgn_surface* sf) {
+  if (!ctx || !sf || !sf->device_ptr) return;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaFreeAsync((void*)(uintptr_t)sf->device_ptr, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  sf->device_ptr = 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,24 @@
+// Launchers of the sm_100a decode kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../device_plan.h"
+#include "../ht_tables.h"
+
+namespace sgn {
+
+cudaError_t ht_kernels_init();
+cudaError_t upload_ht_tables(const HtDecodeTables& host);
+size_t ht_cleanup_smem_bytes(uint32_t max_nq, uint32_t threads);
+cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, int32_t* coef,
+                              uint32_t* tile_status, uint32_t max_nq, cudaStream_t stream);
+cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,
+                             uint32_t* tile_status, cudaStream_t stream);
+cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream);
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream);
+
+}  // namespace sgn
