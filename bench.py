@@ -1,0 +1,401 @@
+"""Benchmark: decoded Mpixel/s of the HTJ2K tile-batch decode path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c3] [--impl ours|reference]
+
+A step is one decode of the whole workload batch.  Default workload: 256
+tiles of 512x512 RGB8 (H&E-like, 5 levels, 64x64 code blocks, RCT), seeded
+synthetic data.  Prints one JSON line (rank 0):
+
+  value        batched decode, codestreams resident in HBM (one plan: HT
+               cleanup over all code blocks ordered by coded length, IDWT
+               rounds, fused last level + RCT + pack), timed with CUDA events
+               on the library's stream;
+  plain_*      the plain per-tile path (one tile per call) on the same tiles;
+  e2e          sgn_j2k_decode_tiles_to_device from pinned host codestreams:
+               host parse, H2D copy, kernels, status read-back;
+  roofline     dominant kernel: (codestream + output bytes) / its duration;
+  cpu_baseline the oracle (C++ restatement of the reference CPU tile batch)
+               on the host cores, bounded sample.
+
+With --gpus N > 1 (torchrun) every rank decodes its own replica of the
+workload (independent tiles, no data-path collective) and rank 0 reports the
+total over the max per-rank time.
+"""
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def build_workload(name):
+    from signinum_b200 import encode
+
+    if name == "c1":
+        return encode.config1(), "rgb8"
+    if name == "c2":
+        return encode.config2(), "rgb8"
+    return encode.config3(), "gray16"
+
+
+WORKLOAD_CONFIG = {
+    "c1": {"workload": "uniform batch: 256 tiles 512x512 RGB8, HTJ2K lossless 5/3, 5 levels, 64x64 code blocks, RCT",
+           "tiles": 256},
+    "c2": {"workload": "uneven batch: 1024 RGB8 tiles, sides 128..1024, 3..6 levels, 32x32/64x64 blocks, 20% near-blank",
+           "tiles": 1024},
+    "c3": {"workload": "high bit depth: 128 tiles 2048x2048 u16 gray, 6 levels, 64x64 code blocks",
+           "tiles": 128},
+}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(tiles, fmt, budget_s=20.0):
+    """The oracle's CPU tile batch (all host threads) over a bounded sample."""
+    from oracle import oracle
+
+    # One single-threaded probe decode sizes the sample to ~budget_s of CPU work.
+    t0 = time.perf_counter()
+    oracle.decode(tiles[0].codestream, fmt)
+    per_tile = max(time.perf_counter() - t0, 1e-4)
+    k = int(max(1, min(len(tiles), budget_s / per_tile)))
+    sample = tiles[:k]
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    outs, first = oracle.decode_batch([t.codestream for t in sample], fmt, workers=cores)
+    dt = time.perf_counter() - t0
+    px = sum(t.width * t.height for t in sample)
+    return {"value": px / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": "port",
+            "sample": f"first {k} of {len(tiles)} tiles of the workload, one pass, {cores} threads",
+            "seconds": dt, "ok": first == -1}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference's tile batch."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w, kind = build_workload(args.workload)
+    fmt = 1 if kind == "rgb8" else 3
+    from oracle import oracle
+
+    cores = os.cpu_count() or 1
+    # Each step: a bounded sample (~2 s of CPU work per step at one thread).
+    t0 = time.perf_counter()
+    oracle.decode(w.tiles[0].codestream, fmt)
+    per_tile = max(time.perf_counter() - t0, 1e-4)
+    k = int(max(1, min(len(w.tiles), 2.0 * cores / per_tile / max(args.steps, 1))))
+    sample = [t.codestream for t in w.tiles[:k]]
+    px = sum(t.width * t.height for t in w.tiles[:k])
+    for _ in range(args.warmup):
+        oracle.decode_batch(sample, fmt, workers=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, first = oracle.decode_batch(sample, fmt, workers=cores)
+        times.append(time.perf_counter() - t0)
+    ms = 1000.0 * float(np.mean(times))
+    v = px / (ms / 1000.0) / 1e6
+    line = {"impl": "reference", "metric": "decoded Mpixel/s", "value": v, "unit": "Mpixel/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded)", "config": dict(WORKLOAD_CONFIG[args.workload], sample_tiles=k),
+            "cpu_baseline": {"value": v, "unit": "Mpixel/s", "cores": cores, "kind": "port",
+                             "sample": f"first {k} tiles of the workload per step, {cores} threads; C++ "
+                                       "restatement of the reference CPU tile batch (Rust toolchain absent)"},
+            "e2e": {"value": v, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def traffic_for(workload, kernel):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    p = ROOT / "profiles" / "dram_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
+            return float(parts[2])
+    return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from signinum_b200 import j2k_cuda
+    from signinum_b200.plan import Plan
+
+    ctx = j2k_cuda._Context.open(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    w, kind = build_workload(args.workload)
+    fmt = 1 if kind == "rgb8" else 3
+    bpp = 3 if kind == "rgb8" else 2
+    tiles = w.tiles
+    n = len(tiles)
+    pixels = w.pixels()
+    coded = w.coded_bytes()
+    out_bytes = sum(t.width * t.height * bpp for t in tiles)
+    # Pinned, contiguous codestreams (16-byte aligned) for the H2D path.
+    offs, pos = [], 0
+    for t in tiles:
+        offs.append(pos)
+        pos += (len(t.codestream) + 15) & ~15
+    pinned = torch.empty(pos, dtype=torch.uint8, pin_memory=True)
+    host = pinned.numpy()
+    for o, t in zip(offs, tiles):
+        host[o:o + len(t.codestream)] = np.frombuffer(t.codestream, np.uint8)
+    lens = [len(t.codestream) for t in tiles]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    # ---- Batched, device-resident (value).
+    plan = Plan(lens, fmt, ctx=ctx, contiguous=host, offsets=offs)
+    for _ in range(args.warmup):
+        plan.execute_timed()
+    st, per = plan.wait()
+    assert st == 0, f"decode failed: {st}"
+    stages = []
+    barrier()
+    with Clocks(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stages.append(plan.execute_timed())
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    batched_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    stage = np.mean(np.array(stages), axis=0)  # HT, refine, IDWT, pack, total
+    launches = plan.launches * args.steps
+    value = world * pixels / (batched_ms / 1000.0) / 1e6
+    # Parity spot check of the benchmark output against the oracle.
+    check = None
+    if rank == 0:
+        from oracle import oracle
+
+        idx = [0, n // 2, n - 1]
+        check = all(plan.download(i) == oracle.decode(tiles[i].codestream, fmt)[0] for i in idx)
+
+    # ---- Plain per-tile path (one tile per call), device-resident and e2e.
+    plain = {}
+    if not args.no_plain:
+        tplans = [Plan([lens[i]], fmt, ctx=ctx, contiguous=host[offs[i]:offs[i] + ((lens[i] + 15) & ~15)],
+                       offsets=[0]) for i in range(n)]
+        for p in tplans[: min(8, n)]:
+            p.execute_async()
+            p.wait()
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for p, (e0, e1) in zip(tplans, evs):
+            e0.record(stream)
+            p.execute_async()
+            e1.record(stream)
+            p.wait()
+        a1.record(stream)
+        a1.synchronize()
+        lat = [e0.elapsed_time(e1) for e0, e1 in evs]
+        plain_ms = max_over_ranks(a0.elapsed_time(a1))
+        for p in tplans:
+            p.destroy()
+        # e2e plain: the drop-in call from pinned host memory, one tile per call.
+        import ctypes
+
+        from signinum_b200 import _native
+        from signinum_b200._native import SgnRequest, SgnSurface
+
+        lib = _native.cuda_lib()
+        req = SgnRequest(0, 0, 0, 0, 0, 1)
+        barrier()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        e2e_lat = []
+        b0.record(stream)
+        for i in range(n):
+            s = SgnSurface()
+            t0 = time.perf_counter()
+            rc = lib.sgn_j2k_decode_to_device(ctx.handle, host.ctypes.data + offs[i], lens[i], fmt,
+                                              ctypes.byref(req), 3, ctypes.byref(s))
+            e2e_lat.append((time.perf_counter() - t0) * 1000.0)
+            assert rc == 0
+            lib.sgn_surface_free(ctx.handle, ctypes.byref(s))
+        b1.record(stream)
+        b1.synchronize()
+        plain_e2e_ms = max_over_ranks(b0.elapsed_time(b1))
+        plain = {"plain_mpix_s": world * pixels / (plain_ms / 1000.0) / 1e6,
+                 "plain_tile_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                 "plain_e2e_mpix_s": world * pixels / (plain_e2e_ms / 1000.0) / 1e6,
+                 "plain_e2e_tile_latency_ms": {"p50": float(np.percentile(e2e_lat, 50)),
+                                               "p99": float(np.percentile(e2e_lat, 99))}}
+        plain["batched_over_plain"] = value / plain["plain_mpix_s"]
+
+    # ---- e2e batched: decode_tiles_to_device from pinned host buffers.
+    import ctypes
+
+    from signinum_b200 import _native
+    from signinum_b200._native import SgnSurface
+
+    lib = _native.cuda_lib()
+    ptrs = (ctypes.c_void_p * n)(*[host.ctypes.data + o for o in offs])
+    clens = (ctypes.c_size_t * n)(*lens)
+    per_tile = (ctypes.c_int32 * n)()
+    first = ctypes.c_size_t()
+
+    def e2e_step():
+        outs = (SgnSurface * n)()
+        rc = lib.sgn_j2k_decode_tiles_to_device(ctx.handle, ptrs, clens, n, fmt, None, 3, outs, per_tile,
+                                                ctypes.byref(first))
+        assert rc == 0, rc
+        return outs
+
+    for _ in range(min(args.warmup, 2)):
+        outs = e2e_step()
+        for i in range(n):
+            lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
+    barrier()
+    e2e_ms_list = []
+    for _ in range(max(1, min(args.steps, 5))):
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        outs = e2e_step()
+        c1.record(stream)
+        c1.synchronize()
+        e2e_ms_list.append(c0.elapsed_time(c1))
+        for i in range(n):
+            lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
+    e2e_ms = max_over_ranks(float(np.mean(e2e_ms_list)))
+    e2e_val = world * pixels / (e2e_ms / 1000.0) / 1e6
+
+    if rank == 0:
+        names = ["ht_cleanup_kernel", "ht_refine_kernel", "idwt_level_kernel", "pack_kernel"]
+        dom = int(np.argmax(stage[:4]))
+        peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+        peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+        algo = coded + out_bytes
+        achieved = algo / (stage[dom] / 1000.0) / 1e9
+        traffic = traffic_for(args.workload, names[dom])
+        cpu = None if args.no_cpu else cpu_baseline(tiles, fmt)
+        line = {
+            "metric": "decoded Mpixel/s (batched persistent form; plain per-tile beside it)",
+            "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic (seeded)",
+            "config": dict(WORKLOAD_CONFIG[args.workload], parallelism=f"replicas{world}",
+                           l2="inputs larger than L2 (coded + coefficient arenas), no flush",
+                           coded_bytes=coded, output_bytes=out_bytes, pixels=pixels),
+            "compressed_MB_s": world * coded / (batched_ms / 1000.0) / 1e6,
+            "hbm_roofline_frac_path": (world * algo / (batched_ms / 1000.0) / 1e9) / peak,
+            "stage_ms": {"ht_cleanup": stage[0], "ht_refine": stage[1], "idwt_levels": stage[2],
+                         "last_level_pack": stage[3], "total": stage[4]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": names[dom],
+                         "peak_source": "measured" if PEAKS.exists() else "fallback",
+                         "algorithmic_bytes_per_launch": algo},
+            "e2e": {"value": e2e_val, "unit": "Mpixel/s", "h2d_bytes_per_step": pos,
+                    "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "parity_spot_check": check,
+        }
+        line.update(plain)
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    plan.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -64,6 +64,7 @@ CUDA_SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_plan_surfaces": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnSurface), ctypes.c_size_t]),
     "sgn_plan_kernel_launches": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "sgn_plan_execute_timed": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "sgn_plan_destroy": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgn_ctx_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "sgn_ht_lookup_tables": (None, [ctypes.c_void_p] * 4),

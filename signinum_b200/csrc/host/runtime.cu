@@ -645,6 +645,35 @@ sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan) {
   return execute(ctx, plan);
 }
 
+sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
+  if (!ctx || !p || !stage_ms) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  chk(cudaMemsetAsync(p->d_status, 0, std::max<size_t>(p->n, 1) * sizeof(uint32_t), s));
+  chk(cudaEventRecord(ev[0], s));
+  chk(launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_coef, p->d_status, p->max_nq, s));
+  chk(cudaEventRecord(ev[1], s));
+  chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
+  chk(cudaEventRecord(ev[2], s));
+  for (const RoundInfo& r : p->rounds) chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s));
+  chk(cudaEventRecord(ev[3], s));
+  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, s));
+  chk(cudaEventRecord(ev[4], s));
+  chk(cudaEventSynchronize(ev[4]));
+  if (e == cudaSuccess) {
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+    cudaEventElapsedTime(&stage_ms[4], ev[0], ev[4]);
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  return cuda_status(e, "timed execute");
+}
+
 sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing) {
   if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
