@@ -23,6 +23,7 @@ constexpr int kIdwtThreads = 256;
 struct HtJob {
   uint64_t src;      // byte offset of the cleanup segment in the input arena
   uint64_t dst;      // element offset of the block's first sample in the coefficient arena
+  uint64_t sym;      // element offset of the block's quad-symbol table in the symbol scratch
   uint32_t lcup;     // cleanup segment length (refinement follows it)
   uint32_t tile;     // batch index of the tile (status reporting)
   uint32_t stride;   // band row stride in elements
@@ -34,7 +35,12 @@ struct HtJob {
   uint8_t flags;     // bit 0: vertically causal context
   uint8_t pad[2];
 };
-static_assert(sizeof(HtJob) == 40, "HtJob layout");
+static_assert(sizeof(HtJob) == 48, "HtJob layout");
+
+// Quad symbol written by the VLC pass: bits 0-15 the CxtVLC entry (rho,
+// u_off, e_k, e_1), bits 16-23 u_q (initial row: u_q + 1).  A block whose
+// cleanup VLC/MEL decode failed has kSymFailed in its first entry.
+constexpr uint32_t kSymFailed = 0xFFFFFFFFu;
 
 struct IdwtJob {
   const int32_t* ll;   // ceil(w/2) x ceil(h/2)

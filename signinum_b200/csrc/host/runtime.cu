@@ -157,12 +157,13 @@ struct sgn_plan {
   uint8_t* d_input = nullptr;
   int32_t* d_coef = nullptr;
   int32_t* d_levels = nullptr;
+  uint32_t* d_symbols = nullptr;
   HtJob* d_ht = nullptr;
   uint32_t* d_refine = nullptr;
   IdwtJob* d_idwt = nullptr;
   PackJob* d_pack = nullptr;
   uint32_t* d_status = nullptr;
-  uint32_t nht = 0, max_nq = 1, nref = 0, npack = 0, pack_ctas = 0;
+  uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
   std::vector<RoundInfo> rounds;
   uint64_t launches = 0;
   std::vector<uint32_t> h_status;
@@ -232,11 +233,13 @@ cudaError_t dalloc(T** p, size_t count, cudaStream_t s) {
 }
 
 void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
-  void* ptrs[] = {p->d_input, p->d_coef, p->d_levels, p->d_ht, p->d_refine, p->d_idwt, p->d_pack, p->d_status};
+  void* ptrs[] = {p->d_input,  p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
+                  p->d_refine, p->d_idwt, p->d_pack,   p->d_status};
   for (void* q : ptrs)
     if (q) cudaFreeAsync(q, s);
   p->d_input = nullptr;
   p->d_coef = p->d_levels = nullptr;
+  p->d_symbols = nullptr;
   p->d_ht = nullptr;
   p->d_refine = nullptr;
   p->d_idwt = nullptr;
@@ -298,11 +301,13 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
   if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
   if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
-  // HT jobs, longest segments first.
+  // HT jobs, longest segments first.  Each coded block gets a quad-symbol
+  // table (ceil(w/2) x ceil(h/2) words) in the symbol scratch.
   std::vector<HtJob> ht;
   ht.reserve(nblocks);
   std::vector<uint32_t> refine;
-  uint32_t max_nq = 1;
+  uint32_t ms_words = 8, max_w = 1;
+  uint64_t sym_total = 0;
   for (size_t i = 0; i < n; ++i) {
     if (plan->status[i] != SGN_OK) continue;
     const TileLayout& L = work[i].layout;
@@ -322,7 +327,16 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
       j.passes = cb.passes;
       j.nbp = b.nbp;
       j.flags = L.causal ? 1 : 0;
-      max_nq = std::max<uint32_t>(max_nq, (cb.w + 1) / 2);
+      max_w = std::max<uint32_t>(max_w, cb.w);
+      if (cb.passes) {
+        j.sym = sym_total;
+        sym_total += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
+        if (cb.lcup >= 2) {
+          const uint8_t* seg = datas[i] + cb.cleanup_off;
+          uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
+          if (scup <= cb.lcup) ms_words = std::max<uint32_t>(ms_words, (cb.lcup - scup + 15) / 4 + 2);
+        }
+      }
       ht.push_back(j);
     }
   }
@@ -330,7 +344,12 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   for (size_t k = 0; k < ht.size(); ++k)
     if (ht[k].passes > 1) refine.push_back((uint32_t)k);
   plan->nht = (uint32_t)ht.size();
-  plan->max_nq = max_nq;
+  plan->ms_words = ms_words;
+  plan->max_w = max_w;
+  if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
+    return cuda_status(e, "symbol scratch");
+  if (ht_magsgn_smem_bytes(ms_words, max_w) > 227 * 1024)
+    return set_error(SGN_ERR_UNSUPPORTED, "code-block segment too long for the MagSgn staging buffer");
   plan->nref = (uint32_t)refine.size();
   // IDWT rounds: round r-1 holds resolution r of every tile that has it.
   std::vector<std::vector<IdwtJob>> rounds(max_rounds);
@@ -490,7 +509,7 @@ sgn_status execute(sgn_ctx* ctx, sgn_plan* p) {
   cudaError_t e;
   if (p->n && (e = cudaMemsetAsync(p->d_status, 0, p->n * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "status reset");
-  if ((e = launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_coef, p->d_status, p->max_nq, s)) != cudaSuccess)
+  if ((e = launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s)) != cudaSuccess)
     return cuda_status(e, "HT cleanup launch");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
@@ -657,7 +676,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   };
   chk(cudaMemsetAsync(p->d_status, 0, std::max<size_t>(p->n, 1) * sizeof(uint32_t), s));
   chk(cudaEventRecord(ev[0], s));
-  chk(launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_coef, p->d_status, p->max_nq, s));
+  chk(launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s));
   chk(cudaEventRecord(ev[1], s));
   chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
   chk(cudaEventRecord(ev[2], s));

@@ -5,12 +5,15 @@
 // decode_impl (crates/signinum-j2k-native/src/j2c/ht_block_decode.rs:1563-1683)
 // followed by coefficient_to_i32 (:225-234).
 //
-// Work mapping: one thread decodes one code block; the blocks of a launch are
-// ordered by coded length on the host so the 32 blocks of a warp carry
-// similar work.  The cleanup pass is fused row by row: for each quad row the
-// thread runs the MEL/VLC/UVLC chain (the serial part) and immediately the
-// magnitude/sign pass of that row, so the only per-block state is one row of
-// quad symbols and exponents, kept in shared memory (no global scratch).
+// Work mapping, in two passes over the blocks of a launch (ordered by coded
+// length on the host, so neighbouring blocks carry similar work):
+//  1. ht_vlc_kernel: one lane per code block runs the MEL / CxtVLC / UVLC
+//     chain, the only inherently serial part of the cleanup pass, and writes
+//     one 32-bit symbol per quad to a scratch table;
+//  2. ht_magsgn_kernel: one warp per code block decodes magnitudes and signs,
+//     a quad per lane, with a warp prefix scan of per-quad bit counts over the
+//     block's unstuffed MagSgn stream staged in shared memory, and writes
+//     whole rows with coalesced stores.
 // Refinement passes (SigProp/MagRef) run in ht_refine_kernel for the few
 // blocks that carry them.
 #include <cstdint>
@@ -177,144 +180,58 @@ struct Fwd {
   }
 };
 
-__device__ __forceinline__ uint32_t bitlen(uint32_t v) { return 32 - __clz(v); }
-
 __device__ __forceinline__ int32_t to_i32(uint32_t v, uint32_t nbp) {
   uint32_t shift = nbp >= 31 ? 0 : 31 - nbp;
   int32_t m = (int32_t)((v & 0x7FFFFFFFu) >> shift);
   return (v & 0x80000000u) ? -m : m;
 }
 
-// decode_mag_sgn_sample_with_vn (ht_block_decode.rs:1010-1032).
-__device__ __forceinline__ uint32_t magsgn_sample(Fwd<0xFF>& ms, uint32_t inf, uint32_t bit, uint32_t uq, uint32_t p,
-                                                  uint32_t& vn) {
-  if ((inf & (1u << (4 + bit))) == 0) {
-    vn = 0;
-    return 0;
-  }
-  uint32_t msv = ms.fetch();
-  uint32_t m_n = uq - ((inf >> (12 + bit)) & 1);
-  ms.advance(m_n);
-  uint32_t value = msv << 31;
-  uint32_t mask = m_n == 0 ? 0 : (m_n >= 32 ? 0xFFFFFFFFu : ((1u << m_n) - 1));
-  uint32_t v = msv & mask;
-  v |= ((inf >> (8 + bit)) & 1) << m_n;
-  v |= 1;
-  value |= (v + 2) << (p - 1);
-  vn = v;
-  return value;
-}
-
-// Per-thread row state in shared memory, interleaved by thread so that the
-// threads of a warp hit distinct banks.
-struct RowState {
-  uint16_t* prevT;  // quad symbols of the previous quad row
-  uint16_t* curT;   // quad symbols of this row
-  uint8_t* curU;    // u_q of this row (initial row: u_q + 1)
-  uint8_t* vE;      // exponent bound from the row above, per quad boundary
-  uint32_t step;    // element stride between consecutive entries of one thread
-  __device__ __forceinline__ uint16_t& pt(uint32_t i) { return prevT[i * step]; }
-  __device__ __forceinline__ uint16_t& ct(uint32_t i) { return curT[i * step]; }
-  __device__ __forceinline__ uint8_t& cu(uint32_t i) { return curU[i * step]; }
-  __device__ __forceinline__ uint8_t& ve(uint32_t i) { return vE[i * step]; }
-};
-
-__device__ void zero_block(int32_t* dst, uint32_t stride, uint32_t w, uint32_t h) {
-  for (uint32_t y = 0; y < h; ++y)
-    for (uint32_t x = 0; x < w; ++x) dst[(size_t)y * stride + x] = 0;
-}
-
-// Cleanup + magnitude/sign decode of one block (decode_cleanup_symbols,
-// ht_block_decode.rs:1056-1205, and decode_magnitude_sign_phase, :1435-1561,
-// fused per quad row).  Returns false where the reference returns None.
-__device__ bool decode_cleanup(const HtJob& job, const uint8_t* src, int32_t* dst, RowState& st,
-                               const SmemTables& T) {
-  const uint32_t lcup = job.lcup, w = job.w, h = job.h, stride = job.stride;
+// CxtVLC / MEL / UVLC pass of one block (decode_cleanup_symbols,
+// ht_block_decode.rs:1056-1205): the serial chain of the cleanup pass.  Writes
+// one 32-bit symbol per quad (entry | u << 16) into the block's symbol table,
+// quad rows of nq entries; the previous row's entries give the context.
+__device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T) {
+  const uint32_t lcup = job.lcup, w = job.w, h = job.h;
   if (lcup < 2) return false;
   uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
   if (scup < 2 || scup > lcup || scup > 4079) return false;
-  const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2;
-  const bool raw = job.passes > 1;  // keep sign-magnitude words for the refinement kernel
-  const uint32_t nbp = job.nbp;
   Mel mel;
   mel.init(src, lcup, scup);
   Vlc vlc;
   vlc.init(src, lcup, scup);
-  Fwd<0xFF> ms;
-  ms.init(src, lcup - scup);
   int run = mel.get_run();
   const uint32_t nq = (w + 1) / 2;
-  for (uint32_t i = 0; i < nq + 3; ++i) st.pt(i) = 0;
-  for (uint32_t i = 0; i < nq + 2; ++i) st.ve(i) = 0;
-  for (uint32_t y = 0; y < h; y += 2) {
-    const bool initial = y == 0;
-    // ---- CxtVLC / MEL / UVLC for this quad row.
+  uint32_t* row = sym;
+  // Initial quad row.
+  {
     uint32_t c_q = 0;
-    uint32_t q = 0;
-    for (uint32_t x = 0; x < w; q += 2) {
-      uint32_t t0, t1, ue;
+    for (uint32_t q = 0; q < nq; q += 2) {
       uint32_t v = vlc.fetch();
-      if (initial) {
-        t0 = T.vlc0[c_q + (v & 0x7F)];
-        if (c_q == 0) {
-          run -= 2;
-          t0 = run == -1 ? t0 : 0;
-          if (run < 0) run = mel.get_run();
-        }
-        st.ct(q) = (uint16_t)t0;
-        x += 2;
-        c_q = ((t0 & 0x10) << 3) | ((t0 & 0xE0) << 2);
-        v = vlc.advance(t0 & 7);
-        t1 = T.vlc0[c_q + (v & 0x7F)];
-        if (c_q == 0 && x < w) {
-          run -= 2;
-          t1 = run == -1 ? t1 : 0;
-          if (run < 0) run = mel.get_run();
-        }
-        if (x >= w) t1 = 0;
-        st.ct(q + 1) = (uint16_t)t1;
-        x += 2;
-        c_q = ((t1 & 0x10) << 3) | ((t1 & 0xE0) << 2);
-        v = vlc.advance(t1 & 7);
-        uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
-        if (mode == 0xC0) {
-          run -= 2;
-          if (run == -1) mode += 0x40;
-          if (run < 0) run = mel.get_run();
-        }
-        ue = T.uvlc0[mode + (v & 0x3F)];
-      } else {
-        uint32_t pq0 = st.pt(q), pq1 = st.pt(q + 1), pq2 = st.pt(q + 2);
-        c_q |= (pq0 & 0xA0) << 2;
-        c_q |= (pq1 & 0x20) << 4;
-        t0 = T.vlc1[c_q + (v & 0x7F)];
-        if (c_q == 0) {
-          run -= 2;
-          t0 = run == -1 ? t0 : 0;
-          if (run < 0) run = mel.get_run();
-        }
-        st.ct(q) = (uint16_t)t0;
-        x += 2;
-        c_q = ((t0 & 0x40) << 2) | ((t0 & 0x80) << 1);
-        c_q |= pq0 & 0x80;
-        c_q |= (pq1 & 0xA0) << 2;
-        c_q |= (pq2 & 0x20) << 4;
-        v = vlc.advance(t0 & 7);
-        t1 = T.vlc1[c_q + (v & 0x7F)];
-        if (c_q == 0 && x < w) {
-          run -= 2;
-          t1 = run == -1 ? t1 : 0;
-          if (run < 0) run = mel.get_run();
-        }
-        if (x >= w) t1 = 0;
-        st.ct(q + 1) = (uint16_t)t1;
-        x += 2;
-        c_q = ((t1 & 0x40) << 2) | ((t1 & 0x80) << 1);
-        c_q |= pq1 & 0x80;
-        v = vlc.advance(t1 & 7);
-        uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
-        ue = T.uvlc1[mode + (v & 0x3F)];
+      uint32_t t0 = T.vlc0[c_q + (v & 0x7F)];
+      if (c_q == 0) {
+        run -= 2;
+        t0 = run == -1 ? t0 : 0;
+        if (run < 0) run = mel.get_run();
       }
+      c_q = ((t0 & 0x10) << 3) | ((t0 & 0xE0) << 2);
+      v = vlc.advance(t0 & 7);
+      const bool hasB = q + 1 < nq;
+      uint32_t t1 = T.vlc0[c_q + (v & 0x7F)];
+      if (c_q == 0 && hasB) {
+        run -= 2;
+        t1 = run == -1 ? t1 : 0;
+        if (run < 0) run = mel.get_run();
+      }
+      if (!hasB) t1 = 0;
+      c_q = ((t1 & 0x10) << 3) | ((t1 & 0xE0) << 2);
+      v = vlc.advance(t1 & 7);
+      uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
+      if (mode == 0xC0) {
+        run -= 2;
+        if (run == -1) mode += 0x40;
+        if (run < 0) run = mel.get_run();
+      }
+      uint32_t ue = T.uvlc0[mode + (v & 0x3F)];
       v = vlc.advance(ue & 7);
       ue >>= 3;
       uint32_t len = ue & 0xF;
@@ -323,100 +240,270 @@ __device__ bool decode_cleanup(const HtJob& job, const uint8_t* src, int32_t* ds
       ue >>= 4;
       len = ue & 7;
       ue >>= 3;
-      uint32_t add = initial ? 1 : 0;
-      st.cu(q) = (uint8_t)(add + (ue & 7) + (tmp & ~(0xFFu << len)));
-      st.cu(q + 1) = (uint8_t)(add + (ue >> 3) + (tmp >> len));
+      row[q] = t0 | ((1 + (ue & 7) + (tmp & ~(0xFFu << len))) << 16);
+      if (hasB) row[q + 1] = t1 | ((1 + (ue >> 3) + (tmp >> len)) << 16);
     }
-    st.ct(q) = 0;
-    st.ct(q + 1) = 0;
-    st.ct(q + 2) = 0;
-    // ---- Magnitude/sign for this quad row.
-    const bool second = y + 1 < h;
-    int32_t* row0 = dst + (size_t)y * stride;
-    int32_t* row1 = row0 + stride;
-    uint32_t prev_v3 = 0;
-    uint32_t x = 0;
-    for (uint32_t qi = 0; x < w; ++qi) {
-      uint32_t inf = st.ct(qi);
-      uint32_t uq = st.cu(qi);
-      if (!initial) {
-        uint32_t gamma = inf & 0xF0;
-        gamma &= gamma - 0x10;
-        uint32_t e = max((uint32_t)st.ve(qi), (uint32_t)st.ve(qi + 1));
-        uint32_t emax = max(e, 2u) - 1;
-        uq += gamma != 0 ? emax : 1;
+  }
+  // Other quad rows: context from the row above (quads q, q+1, q+2).
+  for (uint32_t y = 2; y < h; y += 2) {
+    const uint32_t* prev = row;
+    row += nq;
+    uint32_t c_q = 0;
+    uint32_t pq0 = prev[0] & 0xFFFF;
+    uint32_t pq1 = nq > 1 ? prev[1] & 0xFFFF : 0;
+    for (uint32_t q = 0; q < nq; q += 2) {
+      uint32_t pq2 = q + 2 < nq ? prev[q + 2] & 0xFFFF : 0;
+      uint32_t pq3 = q + 3 < nq ? prev[q + 3] & 0xFFFF : 0;
+      c_q |= (pq0 & 0xA0) << 2;
+      c_q |= (pq1 & 0x20) << 4;
+      uint32_t v = vlc.fetch();
+      uint32_t t0 = T.vlc1[c_q + (v & 0x7F)];
+      if (c_q == 0) {
+        run -= 2;
+        t0 = run == -1 ? t0 : 0;
+        if (run < 0) run = mel.get_run();
       }
-      if (uq > mmsbp2) return false;
-      uint32_t v0, v1, v2, v3;
-      uint32_t a0 = magsgn_sample(ms, inf, 0, uq, p, v0);
-      uint32_t a1 = magsgn_sample(ms, inf, 1, uq, p, v1);
-      if (raw) {
-        row0[x] = (int32_t)a0;
-        if (second) row1[x] = (int32_t)a1;
-      } else {
-        row0[x] = to_i32(a0, nbp);
-        if (second) row1[x] = to_i32(a1, nbp);
+      c_q = ((t0 & 0x40) << 2) | ((t0 & 0x80) << 1);
+      c_q |= pq0 & 0x80;
+      c_q |= (pq1 & 0xA0) << 2;
+      c_q |= (pq2 & 0x20) << 4;
+      v = vlc.advance(t0 & 7);
+      const bool hasB = q + 1 < nq;
+      uint32_t t1 = T.vlc1[c_q + (v & 0x7F)];
+      if (c_q == 0 && hasB) {
+        run -= 2;
+        t1 = run == -1 ? t1 : 0;
+        if (run < 0) run = mel.get_run();
       }
-      st.ve(qi) = (uint8_t)bitlen(prev_v3 | v1);
-      prev_v3 = 0;
-      ++x;
-      if (x >= w) {
-        st.ve(qi + 1) = 0;
-        break;
-      }
-      uint32_t a2 = magsgn_sample(ms, inf, 2, uq, p, v2);
-      uint32_t a3 = magsgn_sample(ms, inf, 3, uq, p, v3);
-      if (raw) {
-        row0[x] = (int32_t)a2;
-        if (second) row1[x] = (int32_t)a3;
-      } else {
-        row0[x] = to_i32(a2, nbp);
-        if (second) row1[x] = to_i32(a3, nbp);
-      }
-      prev_v3 = v3;
-      ++x;
-      if (x >= w) st.ve(qi + 1) = (uint8_t)bitlen(prev_v3);
+      if (!hasB) t1 = 0;
+      c_q = ((t1 & 0x40) << 2) | ((t1 & 0x80) << 1);
+      c_q |= pq1 & 0x80;
+      v = vlc.advance(t1 & 7);
+      uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
+      uint32_t ue = T.uvlc1[mode + (v & 0x3F)];
+      v = vlc.advance(ue & 7);
+      ue >>= 3;
+      uint32_t len = ue & 0xF;
+      uint32_t tmp = v & ((1u << len) - 1);
+      vlc.advance(len);
+      ue >>= 4;
+      len = ue & 7;
+      ue >>= 3;
+      row[q] = t0 | (((ue & 7) + (tmp & ~(0xFFu << len))) << 16);
+      if (hasB) row[q + 1] = t1 | (((ue >> 3) + (tmp >> len)) << 16);
+      pq0 = pq2;
+      pq1 = pq3;
     }
-    // This row's symbols become the context of the next row.
-    for (uint32_t i = 0; i < nq + 3; ++i) st.pt(i) = st.ct(i);
   }
   return true;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kHtThreads) ht_cleanup_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
-                                                                 const uint8_t* __restrict__ arena,
-                                                                 int32_t* __restrict__ coef,
-                                                                 uint32_t* __restrict__ tile_status, uint32_t max_nq) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  SmemTables& T = *reinterpret_cast<SmemTables*>(smem);
+// Pass 1: one lane per code block runs the VLC chain.
+__global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
+                                                            const uint8_t* __restrict__ arena,
+                                                            uint32_t* __restrict__ symbols) {
+  __shared__ SmemTables T;
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&g_ht_tables);
-    uint32_t* dstw = reinterpret_cast<uint32_t*>(smem);
-    for (uint32_t i = threadIdx.x; i < sizeof(SmemTables) / 4; i += blockDim.x) dstw[i] = src[i];
+    uint32_t* d = reinterpret_cast<uint32_t*>(&T);
+    for (uint32_t i = threadIdx.x; i < sizeof(SmemTables) / 4; i += blockDim.x) d[i] = src[i];
   }
   __syncthreads();
-  const uint32_t rows = max_nq + 4;
-  uint8_t* base = smem + sizeof(SmemTables);
-  RowState st;
-  st.step = blockDim.x;
-  st.prevT = reinterpret_cast<uint16_t*>(base) + threadIdx.x;
-  st.curT = reinterpret_cast<uint16_t*>(base) + (size_t)rows * blockDim.x + threadIdx.x;
-  uint8_t* b8 = base + (size_t)rows * blockDim.x * 4;
-  st.curU = b8 + threadIdx.x;
-  st.vE = b8 + (size_t)rows * blockDim.x + threadIdx.x;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) {
-    const HtJob job = jobs[j];
-    int32_t* dst = coef + job.dst;
-    if (job.passes == 0) {
-      zero_block(dst, job.stride, job.w, job.h);
-      continue;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const HtJob job = jobs[j];
+  if (job.passes == 0) return;
+  uint32_t* sym = symbols + job.sym;
+  if (!decode_vlc(job, arena + job.src, sym, T)) sym[0] = kSymFailed;
+}
+
+namespace {
+
+constexpr int kMsWarps = 8;  // warps (code blocks in flight) per CTA of the MagSgn pass
+
+// Unstuffs the forward MagSgn byte stream [0, len) into a bit array W
+// (bit k of the stream = bit k%32 of W[k/32]): each byte contributes 8 bits,
+// or 7 after a 0xFF byte, ORed in at its offset exactly as the reference's
+// ForwardBitReader accumulates it (ht_block_decode.rs:888-930).  Bits past
+// the end read as ones (the reader pads with 0xFF).  Returns the number of
+// real bits.
+__device__ uint32_t unstuff_magsgn(const uint8_t* src, uint32_t len, uint32_t* W, uint32_t nwords) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t i = lane; i < nwords; i += 32) W[i] = 0;
+  __syncwarp();
+  uint32_t carry = 0, last_ff = 0, end_bits = 0;
+  for (uint32_t base = 0; base < len; base += 32) {
+    const uint32_t i = base + lane;
+    const bool valid = i < len;
+    const uint32_t b = valid ? (uint32_t)ld8(src + i) : 0;
+    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, valid && b == 0xFF);
+    // FF bytes among [0, i - 1): they shorten byte i's predecessors.
+    uint32_t ff_before = lane == 0 ? carry - last_ff : carry + __popc(mask & ((1u << (lane - 1)) - 1));
+    const uint32_t off = 8 * i - ff_before;
+    if (valid) {
+      atomicOr(&W[off >> 5], b << (off & 31));
+      if ((off & 31) > 24) atomicOr(&W[(off >> 5) + 1], b >> (32 - (off & 31)));
     }
-    if ((uint32_t)((job.w + 1) / 2) > max_nq || !decode_cleanup(job, arena + job.src, dst, st, T)) {
-      zero_block(dst, job.stride, job.w, job.h);
-      atomicOr(&tile_status[job.tile], kStatusDecode);
+    const uint32_t nvalid = min(32u, len - base);
+    carry += __popc(mask);
+    last_ff = (mask >> (nvalid - 1)) & 1;
+  }
+  // Real bits: 8 per byte minus one per byte that follows a 0xFF.
+  end_bits = len ? 8 * len - (carry - last_ff) : 0;
+  __syncwarp();
+  // Padding: every bit from end_bits on is one.
+  for (uint32_t wi = lane; wi < nwords; wi += 32) {
+    uint32_t lo = wi * 32;
+    if (lo >= end_bits) W[wi] = 0xFFFFFFFFu;
+    else if (lo + 32 > end_bits) W[wi] |= 0xFFFFFFFFu << (end_bits - lo);
+  }
+  __syncwarp();
+  return end_bits;
+}
+
+__device__ __forceinline__ uint32_t bits_at(const uint32_t* W, uint32_t nwords, uint32_t off) {
+  uint32_t wi = off >> 5, sh = off & 31;
+  uint32_t lo = wi < nwords ? W[wi] : 0xFFFFFFFFu;
+  uint32_t hi = wi + 1 < nwords ? W[wi + 1] : 0xFFFFFFFFu;
+  return __funnelshift_r(lo, hi, sh);
+}
+
+}  // namespace
+
+// Pass 2: one warp per code block decodes magnitudes and signs
+// (decode_magnitude_sign_phase, ht_block_decode.rs:1435-1561).  Per quad row
+// the lanes take one quad each: the exponent bound kappa comes from the four
+// samples above (bit lengths of the previous row's v_n, kept per column in
+// shared memory), each lane sums its samples' m_n, a warp prefix scan turns
+// the sums into bit offsets inside the unstuffed MagSgn stream, and the row
+// is written with coalesced stores.
+__global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
+                                                                  const uint8_t* __restrict__ arena,
+                                                                  const uint32_t* __restrict__ symbols,
+                                                                  int32_t* __restrict__ coef,
+                                                                  uint32_t* __restrict__ tile_status,
+                                                                  uint32_t ms_words, uint32_t max_w) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t cols = max_w + 4;
+  uint32_t* W = reinterpret_cast<uint32_t*>(smem) + (size_t)warp * ms_words;
+  uint8_t* Ebase = smem + (size_t)kMsWarps * ms_words * 4 + (size_t)warp * 2 * cols;
+  const uint32_t j = blockIdx.x * kMsWarps + warp;
+  if (j >= njobs) return;
+  const HtJob job = jobs[j];
+  int32_t* dst = coef + job.dst;
+  const uint32_t w = job.w, h = job.h, stride = job.stride;
+  if (job.passes == 0) {
+    for (uint32_t y = 0; y < h; ++y)
+      for (uint32_t x = lane; x < w; x += 32) dst[(size_t)y * stride + x] = 0;
+    return;
+  }
+  const uint32_t* sym = symbols + job.sym;
+  const uint8_t* src = arena + job.src;
+  bool ok = sym[0] != kSymFailed;
+  uint32_t lcup = job.lcup, scup = 0;
+  if (ok) {
+    scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
+    ok = (lcup - scup + 15) / 4 + 2 <= ms_words;
+  }
+  if (ok) {
+    const uint32_t ms_len = lcup - scup;
+    unstuff_magsgn(src, ms_len, W, ms_words);
+    const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
+    const bool raw = job.passes > 1;
+    const uint32_t nq = (w + 1) / 2;
+    uint8_t* Eprev = Ebase;  // bit lengths of v_n, bottom row of the previous quad row, per column + 2
+    uint8_t* Ecur = Ebase + cols;
+    for (uint32_t c = lane; c < cols; c += 32) Eprev[c] = 0;
+    __syncwarp();
+    uint32_t rowbase = 0;
+    bool bad = false;
+    for (uint32_t y = 0, r = 0; y < h; y += 2, ++r) {
+      const bool initial = y == 0, second = y + 1 < h;
+      int32_t* row0 = dst + (size_t)y * stride;
+      int32_t* row1 = row0 + stride;
+      for (uint32_t c0 = 0; c0 < nq; c0 += 32) {
+        const uint32_t q = c0 + lane;
+        const bool active = q < nq;
+        const uint32_t s = active ? sym[(size_t)r * nq + q] : 0;
+        const uint32_t inf = s & 0xFFFF;
+        uint32_t U = s >> 16;
+        if (!initial) {
+          uint32_t gamma = inf & 0xF0;
+          gamma &= gamma - 0x10;
+          // Columns 2q-1 .. 2q+2 of the row above live at Eprev[col + 1].
+          uint32_t e = max(max((uint32_t)Eprev[2 * q], (uint32_t)Eprev[2 * q + 1]),
+                           max((uint32_t)Eprev[2 * q + 2], (uint32_t)Eprev[2 * q + 3]));
+          U += gamma != 0 ? max(e, 2u) - 1 : 1;
+        }
+        bad |= active && U > mmsbp2;
+        // m_n per sample (0 when insignificant) and the quad's bit count.
+        uint32_t m[4], tot = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
+          tot += m[i];
+        }
+        // Warp inclusive scan of the bit counts.
+        uint32_t inc = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+          if (lane >= (uint32_t)d) inc += v;
+        }
+        const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        uint32_t off = rowbase + inc - tot;
+        rowbase += chunk_bits;
+        uint32_t val[4], E[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          val[i] = 0;
+          E[i] = 0;
+          if ((inf >> (4 + i)) & 1) {
+            uint32_t msv = bits_at(W, ms_words, off);
+            uint32_t mn = m[i];
+            off += mn;
+            uint32_t mask = mn == 0 ? 0 : (mn >= 32 ? 0xFFFFFFFFu : ((1u << mn) - 1));
+            uint32_t v = (msv & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
+            val[i] = (msv << 31) | ((v + 2) << (p - 1));
+            E[i] = 32 - __clz(v);
+          }
+        }
+        if (active) {
+          const uint32_t x = 2 * q;
+          auto put = [&](int32_t* rp, uint32_t xx, uint32_t vv) { rp[xx] = raw ? (int32_t)vv : to_i32(vv, nbp); };
+          put(row0, x, val[0]);
+          if (second) put(row1, x, val[1]);
+          if (x + 1 < w) {
+            put(row0, x + 1, val[2]);
+            if (second) put(row1, x + 1, val[3]);
+          }
+          // Bottom-row exponents of this quad for the next quad row.
+          Ecur[x + 1] = (uint8_t)E[1];
+          Ecur[x + 2] = x + 1 < w ? (uint8_t)E[3] : 0;
+        }
+      }
+      __syncwarp();
+      // Columns outside [0, w) stay zero in both buffers.
+      if (lane == 0) {
+        Ecur[0] = 0;
+        Ecur[w + 1] = 0;
+        Ecur[w + 2] = 0;
+      }
+      __syncwarp();
+      uint8_t* t = Eprev;
+      Eprev = Ecur;
+      Ecur = t;
     }
+    ok = !__any_sync(0xFFFFFFFFu, bad);
+  }
+  if (!ok) {
+    __syncwarp();
+    for (uint32_t y = 0; y < h; ++y)
+      for (uint32_t x = lane; x < w; x += 32) dst[(size_t)y * stride + x] = 0;
+    if (lane == 0) atomicOr(&tile_status[job.tile], kStatusDecode);
   }
 }
 
@@ -435,7 +522,7 @@ __device__ const uint32_t kSpread[16] = {0x33,   0x76,   0xEC,   0xC8,   0x330, 
 }  // namespace
 
 // One thread per refinement block.  The block's cleanup result (raw
-// sign-magnitude words written by ht_cleanup_kernel) gives the significance
+// sign-magnitude words written by ht_magsgn_kernel) gives the significance
 // map; SigProp (ht_block_decode.rs:1254-1375) and MagRef (:1377-1433) then
 // update the words in place, and the block is converted to int32.
 __global__ void ht_refine_kernel(const HtJob* __restrict__ jobs, const uint32_t* __restrict__ list, uint32_t n,
@@ -606,26 +693,25 @@ __global__ void ht_refine_kernel(const HtJob* __restrict__ jobs, const uint32_t*
   }
 }
 
-size_t ht_cleanup_smem_bytes(uint32_t max_nq, uint32_t threads) {
-  size_t rows = max_nq + 4;
-  return sizeof(SmemTables) + rows * threads * 6;
+size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w) {
+  return (size_t)kMsWarps * ms_words * 4 + (size_t)kMsWarps * 2 * (max_w + 4);
 }
 
 cudaError_t ht_kernels_init() {
-  cudaError_t e = cudaFuncSetAttribute(ht_cleanup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  return e;
+  return cudaFuncSetAttribute(ht_magsgn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
-cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, int32_t* coef,
-                              uint32_t* tile_status, uint32_t max_nq, cudaStream_t stream) {
+cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
+                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
+                              cudaStream_t stream) {
   if (njobs == 0) return cudaSuccess;
-  // Wide code blocks need more row state per thread: shrink the CTA so the
-  // row state stays within the shared-memory budget.
-  uint32_t threads = kHtThreads;
-  while (threads > 32 && ht_cleanup_smem_bytes(max_nq, threads) > 200 * 1024) threads /= 2;
-  size_t smem = ht_cleanup_smem_bytes(max_nq, threads);
-  uint32_t blocks = (njobs + threads - 1) / threads;
-  ht_cleanup_kernel<<<blocks, threads, smem, stream>>>(jobs, njobs, arena, coef, tile_status, max_nq);
+  ht_vlc_kernel<<<(njobs + kHtThreads - 1) / kHtThreads, kHtThreads, 0, stream>>>(jobs, njobs, arena, symbols);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t smem = ht_magsgn_smem_bytes(ms_words, max_w);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  ht_magsgn_kernel<<<(njobs + kMsWarps - 1) / kMsWarps, kMsWarps * 32, smem, stream>>>(
+      jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w);
   return cudaGetLastError();
 }
 

@@ -13,9 +13,13 @@ namespace sgn {
 
 cudaError_t ht_kernels_init();
 cudaError_t upload_ht_tables(const HtDecodeTables& host);
-size_t ht_cleanup_smem_bytes(uint32_t max_nq, uint32_t threads);
-cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, int32_t* coef,
-                              uint32_t* tile_status, uint32_t max_nq, cudaStream_t stream);
+size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w);
+// HT cleanup: the VLC pass (one lane per block) then the MagSgn pass (one
+// warp per block).  ms_words: unstuffed MagSgn capacity per block in 32-bit
+// words; max_w: widest code block of the launch.
+cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
+                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
+                              cudaStream_t stream);
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,
                              uint32_t* tile_status, cudaStream_t stream);
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream);
