@@ -430,10 +430,11 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
         const uint32_t s = active ? sym[(size_t)r * nq + q] : 0;
         const uint32_t inf = s & 0xFFFF;
         uint32_t U = s >> 16;
-        if (!initial) {
+        if (!initial && active) {
           uint32_t gamma = inf & 0xF0;
           gamma &= gamma - 0x10;
-          // Columns 2q-1 .. 2q+2 of the row above live at Eprev[col + 1].
+          // Columns 2q-1 .. 2q+2 of the row above live at Eprev[col + 1]
+          // (index <= 2*nq + 1 <= w + 2 < max_w + 4 for an active lane).
           uint32_t e = max(max((uint32_t)Eprev[2 * q], (uint32_t)Eprev[2 * q + 1]),
                            max((uint32_t)Eprev[2 * q + 2], (uint32_t)Eprev[2 * q + 3]));
           U += gamma != 0 ? max(e, 2u) - 1 : 1;
