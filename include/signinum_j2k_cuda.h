@@ -161,6 +161,66 @@ void* sgn_ctx_stream(sgn_ctx* ctx);
  * reference's ht_tables.rs. */
 void sgn_ht_lookup_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1);
 
+/* One HT code block for the block-level entry points below: where its
+ * cleanup segment starts in a segment buffer (the refinement segment, if
+ * any, follows it), where its first sample goes in an int32 coefficient
+ * buffer and how rows are strided there. */
+typedef struct sgn_ht_block {
+  uint64_t src;           /* byte offset of the cleanup segment */
+  uint64_t dst;           /* element offset of sample (0, 0) */
+  uint64_t reserved;      /* filled by the library */
+  uint32_t lcup;          /* cleanup segment length */
+  uint32_t tile;          /* index into the status array */
+  uint32_t stride;        /* row stride in elements */
+  uint16_t lref;          /* refinement segment length */
+  uint16_t w, h;          /* block size, at most 4096 samples */
+  uint8_t missing_msbs;   /* missing MSBs after placeholder passes are folded in */
+  uint8_t passes;         /* 0 = all-zero block, 1 cleanup, 2 + SigProp, 3 + MagRef */
+  uint8_t num_bitplanes;  /* magnitude bit-planes of the band */
+  uint8_t flags;          /* bit 0: vertically causal context */
+  uint8_t pad[2];
+} sgn_ht_block;
+
+/* Diagnostics (no counterpart in the reference): the code-block table of a
+ * full-resolution decode of one codestream, as the decode path builds it,
+ * with src relative to the codestream and dst into one tight int32 buffer of
+ * *coef_elems elements (per component: LL, then HL/LH/HH per resolution).
+ * *count receives the number of blocks (also when cap is too small:
+ * SGN_ERR_BUFFER). */
+sgn_status sgn_j2k_ht_block_table(const uint8_t* data, size_t len, sgn_ht_block* out, size_t cap, size_t* count,
+                                  uint64_t* coef_elems);
+/* Diagnostics: copies tile `tile`'s sub-band coefficients (the HT stage
+ * output, same layout as sgn_j2k_ht_block_table) of an executed plan to host
+ * memory; *count receives the element count. */
+sgn_status sgn_plan_tile_coefficients(sgn_ctx* ctx, const sgn_plan* plan, size_t tile, int32_t* out, size_t cap,
+                                      size_t* count);
+
+/* HT code-block decode that allocates nothing (no counterpart in the
+ * reference).
+ *
+ * For callers that cannot call cudaMalloc: code running inside CUDA graph
+ * capture or an externally owned device memory arena, real-time loops that
+ * must not allocate (nor synchronise the device through the allocator) once
+ * they run, and frameworks whose own allocator owns all device memory.  The
+ * caller passes device memory for the inputs (`segments`, the buffer the
+ * blocks' src offsets point into) and the outputs (`coefficients`, and
+ * `tile_status` with n_tiles words, set to nonzero for tiles with a block that
+ * failed to decode); `blocks` is a host array.  The scratch the HT kernels
+ * need lives in a fixed static device array (16 MiB of quad symbols; 4096
+ * blocks of at most 4096 samples per call; cleanup segments up to about 27 KB),
+ * and larger requests are rejected with SGN_ERR_INVALID_ARGUMENT or
+ * SGN_ERR_UNSUPPORTED before any device work.
+ *
+ * Runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) on the current device.  The first call on a device looks up the
+ * static arrays' device addresses; make that first call before any stream
+ * capture.  All calls on a device share the static arrays and leave the last
+ * call's contents there: calls that overlap on the GPU race and must be
+ * serialised by the caller.  tile_status is cleared by the call. */
+sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, const uint8_t* segments,
+                                        int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
+                                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

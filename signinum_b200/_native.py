@@ -31,6 +31,14 @@ class SgnInfo(ctypes.Structure):
                 ("width", "height", "components", "bit_depth", "levels", "tiles", "ht", "reversible", "mct")]
 
 
+class SgnHtBlock(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_uint64), ("dst", ctypes.c_uint64), ("reserved", ctypes.c_uint64),
+                ("lcup", ctypes.c_uint32), ("tile", ctypes.c_uint32), ("stride", ctypes.c_uint32),
+                ("lref", ctypes.c_uint16), ("w", ctypes.c_uint16), ("h", ctypes.c_uint16),
+                ("missing_msbs", ctypes.c_uint8), ("passes", ctypes.c_uint8), ("num_bitplanes", ctypes.c_uint8),
+                ("flags", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 2)]
+
+
 class SgnEncodeOptions(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("max_decomposition_levels", "code_block_width_exp", "code_block_height_exp", "use_mct",
@@ -68,6 +76,14 @@ CUDA_SIGNATURES = {
     "sgn_plan_destroy": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgn_ctx_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "sgn_ht_lookup_tables": (None, [ctypes.c_void_p] * 4),
+    "sgn_j2k_ht_block_table": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                                ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_uint64)]),
+    "sgn_plan_tile_coefficients": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                                    ctypes.c_void_p, ctypes.c_size_t,
+                                                    ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_ht_decode_blocks_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                      ctypes.c_void_p]),
 }
 
 ENCODE_SIGNATURES = {

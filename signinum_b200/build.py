@@ -26,6 +26,7 @@ CUDA_SOURCES = [
     CSRC / "kernels" / "ht_decode.cu",
     CSRC / "kernels" / "idwt_pack.cu",
     CSRC / "host" / "runtime.cu",
+    CSRC / "host" / "noalloc.cu",
     CSRC / "host" / "codestream.cpp",
 ]
 ENCODE_SOURCES = [

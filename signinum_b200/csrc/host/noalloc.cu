@@ -1,0 +1,166 @@
+// HT code-block decode that allocates nothing.
+//
+// For callers that cannot call cudaMalloc: code that runs inside CUDA graph
+// capture or an externally owned memory arena, real-time decode loops that
+// must not allocate (or synchronise the device through the allocator) once
+// running, and host frameworks whose allocator owns all device memory.  They
+// hand in device inputs and outputs; the scratch the HT kernels need (one
+// 32-bit symbol per quad, written by the VLC pass and read by the MagSgn
+// pass), the device copy of the block descriptors and the refinement list
+// live in file-scope static device arrays of fixed size, so this entry point
+// calls no cudaMalloc, cudaFree or allocating library routine.
+//
+// The arrays are shared by every call on a device and keep the last call's
+// contents; calls that overlap on the GPU (different streams, or host
+// threads racing) race on them and must be serialised by the caller.
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstring>
+#include <mutex>
+
+#include "../../../include/signinum_j2k_cuda.h"
+#include "../device_plan.h"
+#include "../kernels/kernels.h"
+
+using namespace sgn;
+
+// Shared with the rest of the C ABI (sgn_last_error_message).
+void sgn_set_last_error_message(const char* msg);
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxBlocks = 4096;
+// ceil(w/2) * ceil(h/2) <= 1024 for any code block of at most 4096 samples
+// with power-of-two sides (edge blocks are smaller).
+constexpr uint32_t kNoAllocSymbolsPerBlock = 1024;
+constexpr int kMaxDevices = 64;
+
+// 16 MiB of quad symbols: the scratch of the HT cleanup pass.
+static __device__ __align__(256) uint32_t g_noalloc_symbols[kNoAllocMaxBlocks * kNoAllocSymbolsPerBlock];
+static __device__ __align__(256) HtJob g_noalloc_jobs[kNoAllocMaxBlocks];
+static __device__ __align__(256) uint32_t g_noalloc_refine[kNoAllocMaxBlocks];
+static __device__ __align__(256) uint32_t g_noalloc_refine_count;
+
+static_assert(sizeof(sgn_ht_block) == sizeof(HtJob), "sgn_ht_block must match the device job layout");
+static_assert(offsetof(sgn_ht_block, src) == offsetof(HtJob, src), "layout");
+static_assert(offsetof(sgn_ht_block, dst) == offsetof(HtJob, dst), "layout");
+static_assert(offsetof(sgn_ht_block, reserved) == offsetof(HtJob, sym), "layout");
+static_assert(offsetof(sgn_ht_block, lcup) == offsetof(HtJob, lcup), "layout");
+static_assert(offsetof(sgn_ht_block, tile) == offsetof(HtJob, tile), "layout");
+static_assert(offsetof(sgn_ht_block, stride) == offsetof(HtJob, stride), "layout");
+static_assert(offsetof(sgn_ht_block, lref) == offsetof(HtJob, lref), "layout");
+static_assert(offsetof(sgn_ht_block, w) == offsetof(HtJob, w), "layout");
+static_assert(offsetof(sgn_ht_block, h) == offsetof(HtJob, h), "layout");
+static_assert(offsetof(sgn_ht_block, missing_msbs) == offsetof(HtJob, mmsb), "layout");
+static_assert(offsetof(sgn_ht_block, passes) == offsetof(HtJob, passes), "layout");
+static_assert(offsetof(sgn_ht_block, num_bitplanes) == offsetof(HtJob, nbp), "layout");
+static_assert(offsetof(sgn_ht_block, flags) == offsetof(HtJob, flags), "layout");
+
+struct DeviceArrays {
+  bool ready = false;
+  uint32_t* symbols = nullptr;
+  HtJob* jobs = nullptr;
+  uint32_t* refine = nullptr;
+  uint32_t* refine_count = nullptr;
+};
+
+DeviceArrays g_arrays[kMaxDevices];
+std::mutex g_setup_mu;
+
+sgn_status fail(sgn_status s, const char* m) {
+  sgn_set_last_error_message(m);
+  return s;
+}
+
+// Device addresses of the static arrays for the current device: taken once
+// per device with cudaGetSymbolAddress (host code must not use the arrays'
+// names as device addresses).
+sgn_status setup(int device, DeviceArrays** out) {
+  if (device < 0 || device >= kMaxDevices) return fail(SGN_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(g_setup_mu);
+  DeviceArrays& a = g_arrays[device];
+  if (!a.ready) {
+    if (ensure_device_init(device) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(SGN_ERR_CUDA_RUNTIME, "HT table set-up failed");
+    }
+    if (cudaGetSymbolAddress((void**)&a.symbols, g_noalloc_symbols) != cudaSuccess ||
+        cudaGetSymbolAddress((void**)&a.jobs, g_noalloc_jobs) != cudaSuccess ||
+        cudaGetSymbolAddress((void**)&a.refine, g_noalloc_refine) != cudaSuccess ||
+        cudaGetSymbolAddress((void**)&a.refine_count, g_noalloc_refine_count) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(SGN_ERR_CUDA_RUNTIME, "cudaGetSymbolAddress failed for the no-allocation scratch");
+    }
+    a.ready = true;
+  }
+  *out = &a;
+  return SGN_OK;
+}
+
+// Gives every block its slice of the symbol scratch and lists the blocks
+// that carry refinement passes.
+__global__ void noalloc_prepare_kernel(HtJob* jobs, uint32_t n, uint32_t* refine, uint32_t* refine_count) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  jobs[j].sym = (uint64_t)j * kNoAllocSymbolsPerBlock;
+  if (jobs[j].passes > 1) refine[atomicAdd(refine_count, 1u)] = j;
+}
+
+}  // namespace
+
+extern "C" {
+
+sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, const uint8_t* segments,
+                                        int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
+                                        void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n > kNoAllocMaxBlocks) return fail(SGN_ERR_INVALID_ARGUMENT, "more than 4096 code blocks in one call");
+  if ((n && (!blocks || !segments || !coefficients)) || (n_tiles && !tile_status))
+    return fail(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  // Validate the descriptors on the host before any device work.
+  uint32_t max_w = 1, max_lcup = 0, nref = 0;
+  for (uint32_t j = 0; j < n; ++j) {
+    const sgn_ht_block& b = blocks[j];
+    if (b.w == 0 || b.h == 0 || (uint32_t)b.w * b.h > 4096 ||
+        (uint32_t)((b.w + 1) / 2) * ((b.h + 1) / 2) > kNoAllocSymbolsPerBlock)
+      return fail(SGN_ERR_INVALID_ARGUMENT, "code block larger than 4096 samples");
+    if (b.passes > 3 || (b.passes && (b.lcup < 2 || b.missing_msbs >= 30)) || b.tile >= n_tiles ||
+        b.stride < b.w)
+      return fail(SGN_ERR_INVALID_ARGUMENT, "invalid code-block descriptor");
+    if (b.w > max_w) max_w = b.w;
+    if (b.passes && b.lcup > max_lcup) max_lcup = b.lcup;
+    if (b.passes > 1) ++nref;
+  }
+  uint32_t ms_words = (max_lcup + 15) / 4 + 2;
+  if (ht_magsgn_smem_bytes(ms_words, max_w) > 227 * 1024)
+    return fail(SGN_ERR_UNSUPPORTED, "cleanup segment too long for the MagSgn staging buffer");
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SGN_ERR_CUDA_UNAVAILABLE, "no current CUDA device");
+  }
+  DeviceArrays* a = nullptr;
+  sgn_status st = setup(device, &a);
+  if (st != SGN_OK) return st;
+  cudaError_t e = cudaSuccess;
+  // What must start at zero: the status words the kernels OR into and the
+  // refinement-list counter.  The symbol scratch is written before it is read.
+  if (n_tiles) e = cudaMemsetAsync(tile_status, 0, (size_t)n_tiles * sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a->refine_count, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess && n) e = cudaMemcpyAsync(a->jobs, blocks, (size_t)n * sizeof(HtJob), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && n) {
+    noalloc_prepare_kernel<<<(n + 127) / 128, 128, 0, s>>>(a->jobs, n, a->refine, a->refine_count);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = launch_ht_cleanup(a->jobs, n, segments, a->symbols, coefficients, tile_status, ms_words, max_w, s);
+  if (e == cudaSuccess) e = launch_ht_refine(a->jobs, a->refine, nref, segments, coefficients, tile_status, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SGN_ERR_CUDA_RUNTIME, cudaGetErrorString(e));
+  }
+  return SGN_OK;
+}
+
+}  // extern "C"

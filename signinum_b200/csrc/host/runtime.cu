@@ -36,6 +36,37 @@ sgn_status set_error(sgn_status s, const char* msg) {
   return s;
 }
 
+}  // namespace
+
+void sgn_set_last_error_message(const char* msg) { set_error(0, msg); }
+
+namespace sgn {
+
+// Per-device set-up of the decode kernels: the HT lookup tables in device
+// memory and the shared-memory opt-in of the MagSgn pass.  Done once per
+// device, with that device current.
+cudaError_t ensure_device_init(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  static cudaError_t err[64] = {};
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(mu);
+  if (!done[device]) {
+    HtDecodeTables t;
+    build_decode_tables(t);
+    cudaError_t e = upload_ht_tables(t);
+    if (e == cudaSuccess) e = ht_kernels_init();
+    err[device] = e;
+    done[device] = e == cudaSuccess;
+    return e;
+  }
+  return err[device];
+}
+
+}  // namespace sgn
+
+namespace {
+
 sgn_status cuda_status(cudaError_t e, const char* where) {
   if (e == cudaSuccess) return SGN_OK;
   char buf[400];
@@ -167,6 +198,7 @@ struct sgn_plan {
   std::vector<RoundInfo> rounds;
   uint64_t launches = 0;
   std::vector<uint32_t> h_status;
+  std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
 };
 
 namespace {
@@ -301,6 +333,10 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
   if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
   if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
+  plan->tile_coef_off = coef_off;
+  plan->tile_coef_elems.assign(n, 0);
+  for (size_t i = 0; i < n; ++i)
+    if (plan->status[i] == SGN_OK) plan->tile_coef_elems[i] = work[i].layout.coef_per_comp * work[i].layout.ncomp;
   // HT jobs, longest segments first.  Each coded block gets a quad-symbol
   // table (ceil(w/2) x ceil(h/2) words) in the symbol scratch.
   std::vector<HtJob> ht;
@@ -572,14 +608,7 @@ sgn_status sgn_ctx_create(int device, sgn_ctx** out) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  static std::once_flag tables_once;
-  static cudaError_t tables_err = cudaSuccess;
-  std::call_once(tables_once, [] {
-    HtDecodeTables t;
-    build_decode_tables(t);
-    tables_err = upload_ht_tables(t);
-    if (tables_err == cudaSuccess) tables_err = ht_kernels_init();
-  });
+  cudaError_t tables_err = sgn::ensure_device_init(device);
   if (tables_err != cudaSuccess) {
     cudaStreamDestroy(c->stream);
     delete c;
@@ -706,6 +735,53 @@ sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n) 
 }
 
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan) { return plan ? plan->launches : 0; }
+
+sgn_status sgn_plan_tile_coefficients(sgn_ctx* ctx, const sgn_plan* plan, size_t tile, int32_t* out, size_t cap,
+                                      size_t* count) {
+  if (!ctx || !plan || tile >= plan->n || (!out && cap)) return set_error(SGN_ERR_INVALID_ARGUMENT, "bad arguments");
+  size_t elems = plan->tile_coef_elems[tile];
+  if (count) *count = elems;
+  if (elems > cap) return set_error(SGN_ERR_BUFFER, "output buffer too small");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaMemcpyAsync(out, plan->d_coef + plan->tile_coef_off[tile], elems * sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_status(e, "coefficient download");
+}
+
+sgn_status sgn_j2k_ht_block_table(const uint8_t* data, size_t len, sgn_ht_block* out, size_t cap, size_t* count,
+                                  uint64_t* coef_elems) {
+  if (!data || (!out && cap)) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    TileLayout L;
+    parse_tile(data, len, nullptr, L);
+    if (count) *count = L.blocks.size();
+    if (coef_elems) *coef_elems = L.coef_per_comp * L.ncomp;
+    if (L.blocks.size() > cap) return set_error(SGN_ERR_BUFFER, "block table buffer too small");
+    for (size_t k = 0; k < L.blocks.size(); ++k) {
+      const CodeBlock& cb = L.blocks[k];
+      const Band& b = L.bands[cb.band];
+      sgn_ht_block& o = out[k];
+      std::memset(&o, 0, sizeof(o));
+      o.src = cb.cleanup_off;
+      o.dst = (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+      o.lcup = cb.lcup;
+      o.tile = 0;
+      o.stride = b.w;
+      o.lref = (uint16_t)cb.lref;
+      o.w = cb.w;
+      o.h = cb.h;
+      o.missing_msbs = cb.missing_msbs;
+      o.passes = cb.passes;
+      o.num_bitplanes = b.nbp;
+      o.flags = L.causal ? 1 : 0;
+    }
+    return SGN_OK;
+  } catch (const ParseError& e) {
+    return set_error(e.status, e.message.c_str());
+  }
+}
 
 void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan) {
   if (!ctx || !plan) return;

@@ -12,6 +12,8 @@
 namespace sgn {
 
 cudaError_t ht_kernels_init();
+// Uploads the HT tables and sets kernel attributes on `device` (current) once.
+cudaError_t ensure_device_init(int device);
 cudaError_t upload_ht_tables(const HtDecodeTables& host);
 size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w);
 // HT cleanup: the VLC pass (one lane per block) then the MagSgn pass (one
