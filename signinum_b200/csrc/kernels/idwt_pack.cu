@@ -30,13 +30,14 @@ namespace {
 constexpr int TW = kIdwtTileW, TH = kIdwtTileH, HALO = kIdwtHalo;
 constexpr int SW = TW + 2 * HALO, SH = TH + 2 * HALO;
 
-// Periodic symmetric extension of index i into [0, n).
+// Periodic symmetric extension of index i into [0, n): reflect about the
+// first and last samples until inside (the staged halo overshoots by at most
+// two samples, so one or two reflections suffice).
 __device__ __forceinline__ int fold(int i, int n) {
   if (n == 1) return 0;
-  int p = 2 * (n - 1);
-  int m = i % p;
-  if (m < 0) m += p;
-  return m >= n ? p - m : m;
+#pragma unroll 1
+  for (int k = 0; k < 8 && (i < 0 || i >= n); ++k) i = i < 0 ? -i : 2 * (n - 1) - i;
+  return i;
 }
 
 // Sample (gx, gy) of the interleaved level image (origin 0: even columns come
@@ -54,6 +55,31 @@ __device__ __forceinline__ int32_t interleaved(const int32_t* ll, const int32_t*
     if ((gx & 1) == 0) { b = lh; s = lw; } else { b = hh; s = hw; }
   }
   return __ldg(b + (size_t)(gy >> 1) * s + (gx >> 1));
+}
+
+// Stages the tile at (x0, y0) plus its halo into S.  Interior tiles (halo
+// inside the image) load each band as a block of rows, coalesced along the
+// band row; edge tiles fold every index.
+__device__ __forceinline__ void stage_tile(int32_t (*S)[SW], const int32_t* ll, const int32_t* hl, const int32_t* lh,
+                                           const int32_t* hh, int x0, int y0, int w, int h) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (x0 >= HALO && y0 >= HALO && x0 + TW + HALO <= w && y0 + TH + HALO <= h) {
+    constexpr int BW = SW / 2, BH = SH / 2;  // band samples per staged tile
+    const int lw = (w + 1) >> 1, hw = w >> 1;
+    const int bx0 = (x0 - HALO) >> 1, by0 = (y0 - HALO) >> 1;
+    for (int i = tid; i < 4 * BH * BW; i += nt) {
+      const int band = i / (BH * BW), r = i - band * (BH * BW);
+      const int by = r / BW, bx = r - by * BW;
+      const int32_t* b = band == 0 ? ll : band == 1 ? hl : band == 2 ? lh : hh;
+      const int s = (band & 1) ? hw : lw;
+      S[2 * by + (band >> 1)][2 * bx + (band & 1)] = __ldg(b + (size_t)(by0 + by) * s + bx0 + bx);
+    }
+  } else {
+    for (int i = tid; i < SH * SW; i += nt) {
+      const int ly = i / SW, lx = i - ly * SW;
+      S[ly][lx] = interleaved(ll, hl, lh, hh, x0 - HALO + lx, y0 - HALO + ly, w, h);
+    }
+  }
 }
 
 // Both lifting passes on one staged tile.  The tile origin is even, so the
@@ -105,10 +131,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_level_kernel(const IdwtJob*
   const uint32_t local = blockIdx.x - job.cta_begin;
   const int x0 = (int)(local % job.tiles_x) * TW, y0 = (int)(local / job.tiles_x) * TH;
   const int w = (int)job.w, h = (int)job.h;
-  for (int i = threadIdx.x; i < SH * SW; i += blockDim.x) {
-    int ly = i / SW, lx = i % SW;
-    S[ly][lx] = interleaved(job.ll, job.hl, job.lh, job.hh, x0 - HALO + lx, y0 - HALO + ly, w, h);
-  }
+  stage_tile(S, job.ll, job.hl, job.lh, job.hh, x0, y0, w, h);
   __syncthreads();
   lift_tile(S, w, h);
   for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
@@ -149,6 +172,7 @@ __device__ __forceinline__ uint16_t to_u16(int32_t v, uint32_t bd) {
 
 __global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs) {
   __shared__ int32_t S[3][SH][SW];
+  __shared__ __align__(16) uint8_t O[TH][TW * 8 + 16];
   const PackJob& job = find_job(jobs, njobs);
   const uint32_t local = blockIdx.x - job.cta_begin;
   const int ax = (int)(job.cx & ~1u);
@@ -157,10 +181,7 @@ __global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __res
   const int nc = (int)job.ncomp;
   for (int c = 0; c < nc; ++c) {
     if (job.lifting) {
-      for (int i = threadIdx.x; i < SH * SW; i += blockDim.x) {
-        int ly = i / SW, lx = i % SW;
-        S[c][ly][lx] = interleaved(job.ll[c], job.hl[c], job.lh[c], job.hh[c], x0 - HALO + lx, y0 - HALO + ly, w, h);
-      }
+      stage_tile(S[c], job.ll[c], job.hl[c], job.lh[c], job.hh[c], x0, y0, w, h);
     } else {
       for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
         int ly = i / TW, lx = i % TW;
@@ -175,6 +196,11 @@ __global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __res
   const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
   const int32_t shift = 1 << (job.bit_depth - 1);
   const uint32_t fmt = job.fmt, bd = job.bit_depth, reg = job.region_conv;
+  const int bpp = fmt == PACK_GRAY8 ? 1 : fmt == PACK_RGB8 ? 3 : fmt == PACK_RGBA8 ? 4 : fmt == PACK_GRAY16 ? 2 : 6;
+  // Packed pixels of each tile row, staged at the same offset modulo 16 as
+  // their destination so the copy-out can use 16-byte stores.
+  const int xs = max(x0, cx0), xe = min(x0 + TW, cx1);
+  const int npix = xe - xs;
   for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
     int ly = i / TW, lx = i % TW;
     int gx = x0 + lx, gy = y0 + ly;
@@ -194,30 +220,60 @@ __global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __res
       v2 += shift;
     }
     v0 += shift;
-    uint8_t* o = job.out + (size_t)(gy - cy0) * job.pitch;
-    const int ox = gx - cx0;
+    const uint64_t gbase = (uint64_t)(gy - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
+    uint8_t* o = &O[ly][(gbase & 15) + (size_t)(gx - xs) * bpp];
     switch (fmt) {
-      case PACK_GRAY8: o[ox] = to_u8(v0, bd, reg); break;
+      case PACK_GRAY8: o[0] = to_u8(v0, bd, reg); break;
       case PACK_RGB8:
-        o[3 * ox] = to_u8(v0, bd, reg);
-        o[3 * ox + 1] = to_u8(v1, bd, reg);
-        o[3 * ox + 2] = to_u8(v2, bd, reg);
+        o[0] = to_u8(v0, bd, reg);
+        o[1] = to_u8(v1, bd, reg);
+        o[2] = to_u8(v2, bd, reg);
         break;
       case PACK_RGBA8:
-        o[4 * ox] = to_u8(v0, bd, reg);
-        o[4 * ox + 1] = to_u8(v1, bd, reg);
-        o[4 * ox + 2] = to_u8(v2, bd, reg);
-        o[4 * ox + 3] = 255;
+        o[0] = to_u8(v0, bd, reg);
+        o[1] = to_u8(v1, bd, reg);
+        o[2] = to_u8(v2, bd, reg);
+        o[3] = 255;
         break;
-      case PACK_GRAY16: reinterpret_cast<uint16_t*>(o)[ox] = to_u16(v0, bd); break;
+      case PACK_GRAY16: {
+        uint16_t a = to_u16(v0, bd);
+        o[0] = (uint8_t)a;
+        o[1] = (uint8_t)(a >> 8);
+        break;
+      }
       case PACK_RGB16: {
-        uint16_t* p = reinterpret_cast<uint16_t*>(o) + 3 * ox;
-        p[0] = to_u16(v0, bd);
-        p[1] = to_u16(v1, bd);
-        p[2] = to_u16(v2, bd);
+        uint16_t a = to_u16(v0, bd), g = to_u16(v1, bd), c = to_u16(v2, bd);
+        o[0] = (uint8_t)a;
+        o[1] = (uint8_t)(a >> 8);
+        o[2] = (uint8_t)g;
+        o[3] = (uint8_t)(g >> 8);
+        o[4] = (uint8_t)c;
+        o[5] = (uint8_t)(c >> 8);
         break;
       }
     }
+  }
+  __syncthreads();
+  if (npix <= 0) return;
+  // Copy-out: one warp per row; bytes up to the first 16-byte boundary, then
+  // 16-byte vectors, then the tail.
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int nbytes = npix * bpp;
+  for (int ly = warp; ly < TH; ly += nwarps) {
+    const int gy = y0 + ly;
+    if (gy < cy0 || gy >= cy1) continue;
+    const uint64_t gbase = (uint64_t)(gy - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
+    uint8_t* g = job.out + gbase;
+    const uint8_t* src = &O[ly][gbase & 15];
+    int head = (int)((16 - ((uintptr_t)g & 15)) & 15);
+    if (head > nbytes) head = nbytes;
+    if (lane < head) g[lane] = src[lane];
+    const int nvec = (nbytes - head) >> 4;
+    const uint4* sv = reinterpret_cast<const uint4*>(src + head);
+    uint4* gv = reinterpret_cast<uint4*>(g + head);
+    for (int k = lane; k < nvec; k += 32) gv[k] = sv[k];
+    const int done = head + (nvec << 4);
+    if (lane < nbytes - done) g[done + lane] = src[done + lane];
   }
 }
 
