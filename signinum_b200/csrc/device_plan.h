@@ -14,11 +14,11 @@
 
 namespace sgn {
 
-// Lifting tile of the IDWT kernels (output samples per CTA) and its halo.
-constexpr int kIdwtTileW = 64;
-constexpr int kIdwtTileH = 32;
-constexpr int kIdwtHalo = 2;
-constexpr int kIdwtThreads = 256;
+// Work unit of the IDWT kernels: one warp decodes a strip of kIdwtStripW
+// columns (two per lane) over kIdwtSegRows rows of one level.
+constexpr int kIdwtStripW = 64;
+constexpr int kIdwtSegRows = 64;
+constexpr int kIdwtWarps = 8;  // warps (units) per CTA
 
 struct HtJob {
   uint64_t src;      // byte offset of the cleanup segment in the input arena
@@ -49,8 +49,8 @@ struct IdwtJob {
   const int32_t* hh;   // floor(w/2) x floor(h/2)
   int32_t* out;        // w x h, tight
   uint32_t w, h;
-  uint32_t tiles_x;
-  uint32_t cta_begin;
+  uint32_t strips;      // strips across the level
+  uint32_t unit_begin;  // first work unit of this job in its launch
 };
 
 enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
@@ -66,8 +66,8 @@ struct PackJob {
   uint32_t cx, cy, cw, ch;  // crop written to the surface
   uint32_t lifting;     // 1: inputs are the four bands of the last level; 0: ll holds the image
   uint32_t ncomp, mct, bit_depth, fmt, region_conv;
-  uint32_t tiles_x;     // CTA tiles across the crop
-  uint32_t cta_begin;
+  uint32_t strips;      // strips across the crop (from cx rounded down to kIdwtStripW)
+  uint32_t unit_begin;  // first work unit of this job in its launch
   uint32_t tile;        // batch index (status)
 };
 

@@ -417,8 +417,8 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
         j.out = lvl(c, r);
         j.w = res_dim(r, true);
         j.h = res_dim(r, false);
-        j.tiles_x = (j.w + kIdwtTileW - 1) / kIdwtTileW;
-        j.cta_begin = 0;
+        j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
+        j.unit_begin = 0;
         if (j.w == 0 || j.h == 0) continue;
         rounds[r - 1].push_back(j);
       }
@@ -463,12 +463,12 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
     pj.bit_depth = L.bit_depth;
     pj.fmt = fmt;
     pj.region_conv = tw.region_conv;
-    uint32_t ax = tw.crop_x & ~1u, ay = tw.crop_y & ~1u;
-    pj.tiles_x = (tw.crop_x + tw.crop_w - ax + kIdwtTileW - 1) / kIdwtTileW;
-    uint32_t tiles_y = (tw.crop_y + tw.crop_h - ay + kIdwtTileH - 1) / kIdwtTileH;
-    pj.cta_begin = plan->pack_ctas;
+    uint32_t ax = tw.crop_x & ~(uint32_t)(kIdwtStripW - 1), ay = tw.crop_y & ~1u;
+    pj.strips = (tw.crop_x + tw.crop_w - ax + kIdwtStripW - 1) / kIdwtStripW;
+    uint32_t segs = (tw.crop_y + tw.crop_h - ay + kIdwtSegRows - 1) / kIdwtSegRows;
+    pj.unit_begin = plan->pack_ctas;
     pj.tile = (uint32_t)i;
-    plan->pack_ctas += pj.tiles_x * tiles_y;
+    plan->pack_ctas += pj.strips * segs;
     packs.push_back(pj);
   }
   // Flatten the rounds.
@@ -476,8 +476,8 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   for (auto& rj : rounds) {
     RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0};
     for (IdwtJob& j : rj) {
-      j.cta_begin = ri.ctas;
-      ri.ctas += j.tiles_x * ((j.h + kIdwtTileH - 1) / kIdwtTileH);
+      j.unit_begin = ri.ctas;
+      ri.ctas += j.strips * ((j.h + kIdwtSegRows - 1) / kIdwtSegRows);
       idwt.push_back(j);
     }
     if (ri.njobs) plan->rounds.push_back(ri);

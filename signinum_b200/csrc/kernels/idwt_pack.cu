@@ -9,16 +9,23 @@
 // (:908-925).  All values are integers, so int32 with arithmetic shifts gives
 // the reference's f32 floors bit for bit.
 //
-// Memory mapping: each CTA produces a 64x32 tile of one level.  It stages the
-// tile plus a 2-sample halo from the four bands into shared memory (mirrored
-// loads at the image edges; symmetric extension commutes with the lifting
-// steps), runs both lifting passes there and writes the tile once, so every
-// level reads its inputs and writes its output exactly once from HBM.  The
-// last level keeps all components of the tile in shared memory and finishes
-// the pixels in the same kernel: inverse RCT (mct.rs:117-150), +2^(bd-1)
-// (decode.rs:1720-1729, :1748-1752) and the conversion to the requested
-// pixel format (crates/signinum-j2k-native/src/lib.rs:1772-1840, :2202-2294;
-// crates/signinum-j2k/src/decode.rs:345-356, :517-545).
+// Mapping: one warp per unit = a strip of 64 columns x 64 rows of one level.
+// Lane k owns image columns (2k, 2k+1) of the strip, i.e. band column k of
+// the low and high bands, so every band load and every row store is
+// coalesced.  Horizontal lifting of a row needs the odd neighbour on the left
+// and the updated even neighbour on the right: both come from warp shuffles
+// (the strip's edge lanes load the one extra band sample they need).  The
+// vertical pass streams down the rows keeping the previous odd row and the
+// previous updated even row in registers.  Symmetric extension is done by
+// reflecting row/column indices (it commutes with the lifting steps), so the
+// edges need no special arithmetic.  No shared memory, no barriers.
+//
+// The last level keeps the streams of all components of a pixel in the same
+// lane and finishes the pixels there: inverse RCT (mct.rs:117-150),
+// +2^(bd-1) (decode.rs:1720-1729, :1748-1752) and the conversion to the
+// requested pixel format (crates/signinum-j2k-native/src/lib.rs:1772-1840,
+// :2202-2294; crates/signinum-j2k/src/decode.rs:345-356, :517-545); packed
+// rows are staged per warp in shared memory and written with 16-byte stores.
 #include <cstdint>
 
 #include "../device_plan.h"
@@ -27,12 +34,10 @@
 namespace sgn {
 namespace {
 
-constexpr int TW = kIdwtTileW, TH = kIdwtTileH, HALO = kIdwtHalo;
-constexpr int SW = TW + 2 * HALO, SH = TH + 2 * HALO;
+constexpr int kLanes = 32;
 
-// Periodic symmetric extension of index i into [0, n): reflect about the
-// first and last samples until inside (the staged halo overshoots by at most
-// two samples, so one or two reflections suffice).
+// Periodic symmetric extension of index i into [0, n) (reflections about the
+// first and last samples; the streams overshoot by at most a few samples).
 __device__ __forceinline__ int fold(int i, int n) {
   if (n == 1) return 0;
 #pragma unroll 1
@@ -40,84 +45,94 @@ __device__ __forceinline__ int fold(int i, int n) {
   return i;
 }
 
-// Sample (gx, gy) of the interleaved level image (origin 0: even columns come
-// from the low bands, even rows from LL/HL).
-__device__ __forceinline__ int32_t interleaved(const int32_t* ll, const int32_t* hl, const int32_t* lh,
-                                               const int32_t* hh, int gx, int gy, int w, int h) {
-  gx = fold(gx, w);
-  gy = fold(gy, h);
-  const int lw = (w + 1) >> 1, hw = w >> 1;
-  const int32_t* b;
-  int s;
-  if ((gy & 1) == 0) {
-    if ((gx & 1) == 0) { b = ll; s = lw; } else { b = hl; s = hw; }
-  } else {
-    if ((gx & 1) == 0) { b = lh; s = lw; } else { b = hh; s = hw; }
+struct Bands {
+  const int32_t* ll;
+  const int32_t* hl;
+  const int32_t* lh;
+  const int32_t* hh;
+  int w, h;
+};
+
+// Horizontally lifted row y of the interleaved level, at this lane's columns
+// (col, col + 1) with col = 2b.  Lanes past the right edge return garbage.
+__device__ __forceinline__ int2 hrow(const Bands& B, int y, int b, int lane) {
+  y = fold(y, B.h);
+  const int r = y >> 1;
+  const int lw = (B.w + 1) >> 1, hw = B.w >> 1;
+  const int32_t* L = (y & 1) ? B.lh : B.ll;
+  const int32_t* H = (y & 1) ? B.hh : B.hl;
+  const int col = 2 * b;
+  const int32_t* Lr = L + (size_t)r * lw;
+  const int32_t* Hr = H + (size_t)r * hw;
+  int lo = col < B.w ? __ldg(Lr + b) : 0;
+  if (B.w == 1) return make_int2(lo, 0);
+  int hi = col + 1 < B.w ? __ldg(Hr + b) : 0;
+  int hiL = __shfl_up_sync(0xFFFFFFFFu, hi, 1);
+  if (lane == 0) hiL = b == 0 ? hi : __ldg(Hr + b - 1);  // column -1 mirrors column 1
+  if (col + 1 >= B.w) hi = hiL;                          // column w mirrors column w - 2
+  const int E = lo - ((hiL + hi + 2) >> 2);
+  int ER = __shfl_down_sync(0xFFFFFFFFu, E, 1);
+  if (lane == kLanes - 1 && col + 2 < B.w) {
+    const int lo2 = __ldg(Lr + b + 1);
+    const int hi2 = col + 3 < B.w ? __ldg(Hr + b + 1) : hi;
+    ER = lo2 - ((hi + hi2 + 2) >> 2);
   }
-  return __ldg(b + (size_t)(gy >> 1) * s + (gx >> 1));
+  if (col + 2 >= B.w) ER = E;  // column w mirrors column w - 2
+  return make_int2(E, hi + ((E + ER) >> 1));
 }
 
-// Stages the tile at (x0, y0) plus its halo into S.  Interior tiles (halo
-// inside the image) load each band as a block of rows, coalesced along the
-// band row; edge tiles fold every index.
-__device__ __forceinline__ void stage_tile(int32_t (*S)[SW], const int32_t* ll, const int32_t* hl, const int32_t* lh,
-                                           const int32_t* hh, int x0, int y0, int w, int h) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  if (x0 >= HALO && y0 >= HALO && x0 + TW + HALO <= w && y0 + TH + HALO <= h) {
-    constexpr int BW = SW / 2, BH = SH / 2;  // band samples per staged tile
-    const int lw = (w + 1) >> 1, hw = w >> 1;
-    const int bx0 = (x0 - HALO) >> 1, by0 = (y0 - HALO) >> 1;
-    for (int i = tid; i < 4 * BH * BW; i += nt) {
-      const int band = i / (BH * BW), r = i - band * (BH * BW);
-      const int by = r / BW, bx = r - by * BW;
-      const int32_t* b = band == 0 ? ll : band == 1 ? hl : band == 2 ? lh : hh;
-      const int s = (band & 1) ? hw : lw;
-      S[2 * by + (band >> 1)][2 * bx + (band & 1)] = __ldg(b + (size_t)(by0 + by) * s + bx0 + bx);
-    }
-  } else {
-    for (int i = tid; i < SH * SW; i += nt) {
-      const int ly = i / SW, lx = i - ly * SW;
-      S[ly][lx] = interleaved(ll, hl, lh, hh, x0 - HALO + lx, y0 - HALO + ly, w, h);
-    }
+// Vertical 5/3 stream over output rows [ys, ye) (ys even) of NC level
+// images at once; emit(y, v[NC]) receives each finished row.
+template <int NC, typename Emit>
+__device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int ys, int ye, Emit emit) {
+  const int h = B[0].h;
+  int2 v[NC];
+  if (h == 1) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) v[c] = hrow(B[c], 0, b, lane);
+    emit(0, v);
+    return;
   }
-}
-
-// Both lifting passes on one staged tile.  The tile origin is even, so the
-// parity of a shared-memory column equals the parity of its image column.
-__device__ __forceinline__ void lift_tile(int32_t (*S)[SW], int w, int h) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  if (w > 1) {
-    for (int i = tid; i < SH * (SW / 2 - 1); i += nt) {
-      int ly = i / (SW / 2 - 1), lx = 2 + 2 * (i % (SW / 2 - 1));  // even columns 2..SW-2
-      S[ly][lx] -= (S[ly][lx - 1] + S[ly][lx + 1] + 2) >> 2;
-    }
-    __syncthreads();
-    for (int i = tid; i < SH * (SW / 2 - 1); i += nt) {
-      int ly = i / (SW / 2 - 1), lx = 1 + 2 * (i % (SW / 2 - 1));  // odd columns 1..SW-3
-      S[ly][lx] += (S[ly][lx - 1] + S[ly][lx + 1]) >> 1;
-    }
-    __syncthreads();
+  int2 xo_prev[NC], ev_prev[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    xo_prev[c] = hrow(B[c], ys - 1, b, lane);
+    ev_prev[c] = make_int2(0, 0);
   }
-  if (h > 1) {
-    for (int i = tid; i < (SH / 2 - 1) * SW; i += nt) {
-      int ly = 2 + 2 * (i / SW), lx = i % SW;  // even rows 2..SH-2
-      S[ly][lx] -= (S[ly - 1][lx] + S[ly + 1][lx] + 2) >> 2;
+  for (int m = ys >> 1;; ++m) {
+    const int ye_row = 2 * m, yo_row = 2 * m + 1;
+    int2 ev[NC], xo[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const int2 xe = hrow(B[c], ye_row, b, lane);
+      xo[c] = hrow(B[c], yo_row, b, lane);
+      ev[c].x = xe.x - ((xo_prev[c].x + xo[c].x + 2) >> 2);
+      ev[c].y = xe.y - ((xo_prev[c].y + xo[c].y + 2) >> 2);
     }
-    __syncthreads();
-    for (int i = tid; i < (SH / 2 - 1) * SW; i += nt) {
-      int ly = 1 + 2 * (i / SW), lx = i % SW;  // odd rows 1..SH-3
-      S[ly][lx] += (S[ly - 1][lx] + S[ly + 1][lx]) >> 1;
+    if (ye_row - 1 >= ys && ye_row - 1 < ye) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        v[c].x = xo_prev[c].x + ((ev_prev[c].x + ev[c].x) >> 1);
+        v[c].y = xo_prev[c].y + ((ev_prev[c].y + ev[c].y) >> 1);
+      }
+      emit(ye_row - 1, v);
     }
-    __syncthreads();
+    if (ye_row < ye) emit(ye_row, ev);
+    if (yo_row >= ye) break;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      xo_prev[c] = xo[c];
+      ev_prev[c] = ev[c];
+    }
   }
 }
 
 template <typename Job>
-__device__ __forceinline__ const Job& find_job(const Job* jobs, uint32_t njobs) {
+__device__ __forceinline__ const Job& find_job(const Job* jobs, uint32_t njobs, uint32_t unit) {
   uint32_t lo = 0, hi = njobs - 1;
   while (lo < hi) {
     uint32_t mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].cta_begin <= blockIdx.x) lo = mid;
+    if (jobs[mid].unit_begin <= unit) lo = mid;
     else hi = mid - 1;
   }
   return jobs[lo];
@@ -125,20 +140,25 @@ __device__ __forceinline__ const Job& find_job(const Job* jobs, uint32_t njobs) 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kIdwtThreads) idwt_level_kernel(const IdwtJob* __restrict__ jobs, uint32_t njobs) {
-  __shared__ int32_t S[SH][SW];
-  const IdwtJob& job = find_job(jobs, njobs);
-  const uint32_t local = blockIdx.x - job.cta_begin;
-  const int x0 = (int)(local % job.tiles_x) * TW, y0 = (int)(local / job.tiles_x) * TH;
+__global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJob* __restrict__ jobs,
+                                                                     uint32_t njobs, uint32_t nunits) {
+  const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
+  if (unit >= nunits) return;
+  const int lane = threadIdx.x & 31;
+  const IdwtJob& job = find_job(jobs, njobs, unit);
+  const uint32_t local = unit - job.unit_begin;
+  const int x0 = (int)(local % job.strips) * kIdwtStripW;
+  const int ys = (int)(local / job.strips) * kIdwtSegRows;
   const int w = (int)job.w, h = (int)job.h;
-  stage_tile(S, job.ll, job.hl, job.lh, job.hh, x0, y0, w, h);
-  __syncthreads();
-  lift_tile(S, w, h);
-  for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
-    int ly = i / TW, lx = i % TW;
-    int gx = x0 + lx, gy = y0 + ly;
-    if (gx < w && gy < h) job.out[(size_t)gy * w + gx] = S[ly + HALO][lx + HALO];
-  }
+  const int ye = min(ys + kIdwtSegRows, h);
+  Bands B{job.ll, job.hl, job.lh, job.hh, w, h};
+  const int b = (x0 >> 1) + lane, col = 2 * b;
+  int32_t* out = job.out;
+  stream_rows<1>(&B, b, lane, ys, ye, [&](int y, const int2* v) {
+    int32_t* row = out + (size_t)y * w;
+    if (col < w) row[col] = v[0].x;
+    if (col + 1 < w) row[col + 1] = v[0].y;
+  });
 }
 
 namespace {
@@ -168,103 +188,83 @@ __device__ __forceinline__ uint16_t to_u16(int32_t v, uint32_t bd) {
   return (uint16_t)c;
 }
 
-}  // namespace
+constexpr int kRowBytes = kIdwtStripW * 8 + 16;
 
-__global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs) {
-  __shared__ int32_t S[3][SH][SW];
-  __shared__ __align__(16) uint8_t O[TH][TW * 8 + 16];
-  const PackJob& job = find_job(jobs, njobs);
-  const uint32_t local = blockIdx.x - job.cta_begin;
-  const int ax = (int)(job.cx & ~1u);
-  const int x0 = ax + (int)(local % job.tiles_x) * TW, y0 = (int)(job.cy & ~1u) + (int)(local / job.tiles_x) * TH;
-  const int w = (int)job.w, h = (int)job.h;
-  const int nc = (int)job.ncomp;
-  for (int c = 0; c < nc; ++c) {
-    if (job.lifting) {
-      stage_tile(S[c], job.ll[c], job.hl[c], job.lh[c], job.hh[c], x0, y0, w, h);
-    } else {
-      for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
-        int ly = i / TW, lx = i % TW;
-        int gx = x0 + lx, gy = y0 + ly;
-        S[c][ly + HALO][lx + HALO] = (gx < w && gy < h) ? __ldg(job.ll[c] + (size_t)gy * w + gx) : 0;
-      }
+// Packs one pixel (components v0..v2 after the inverse RCT) into o.
+__device__ __forceinline__ void put_pixel(uint8_t* o, uint32_t fmt, int32_t v0, int32_t v1, int32_t v2, uint32_t bd,
+                                          uint32_t reg) {
+  switch (fmt) {
+    case PACK_GRAY8: o[0] = to_u8(v0, bd, reg); break;
+    case PACK_RGB8:
+      o[0] = to_u8(v0, bd, reg);
+      o[1] = to_u8(v1, bd, reg);
+      o[2] = to_u8(v2, bd, reg);
+      break;
+    case PACK_RGBA8:
+      o[0] = to_u8(v0, bd, reg);
+      o[1] = to_u8(v1, bd, reg);
+      o[2] = to_u8(v2, bd, reg);
+      o[3] = 255;
+      break;
+    case PACK_GRAY16: {
+      uint16_t a = to_u16(v0, bd);
+      o[0] = (uint8_t)a;
+      o[1] = (uint8_t)(a >> 8);
+      break;
+    }
+    default: {
+      uint16_t a = to_u16(v0, bd), g = to_u16(v1, bd), c = to_u16(v2, bd);
+      o[0] = (uint8_t)a;
+      o[1] = (uint8_t)(a >> 8);
+      o[2] = (uint8_t)g;
+      o[3] = (uint8_t)(g >> 8);
+      o[4] = (uint8_t)c;
+      o[5] = (uint8_t)(c >> 8);
+      break;
     }
   }
-  __syncthreads();
-  if (job.lifting)
-    for (int c = 0; c < nc; ++c) lift_tile(S[c], w, h);
-  const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
-  const int32_t shift = 1 << (job.bit_depth - 1);
+}
+
+template <int NC>
+__device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint8_t* rowbuf) {
+  const int w = (int)job.w;
+  const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw;
   const uint32_t fmt = job.fmt, bd = job.bit_depth, reg = job.region_conv;
   const int bpp = fmt == PACK_GRAY8 ? 1 : fmt == PACK_RGB8 ? 3 : fmt == PACK_RGBA8 ? 4 : fmt == PACK_GRAY16 ? 2 : 6;
-  // Packed pixels of each tile row, staged at the same offset modulo 16 as
-  // their destination so the copy-out can use 16-byte stores.
-  const int xs = max(x0, cx0), xe = min(x0 + TW, cx1);
-  const int npix = xe - xs;
-  for (int i = threadIdx.x; i < TH * TW; i += blockDim.x) {
-    int ly = i / TW, lx = i % TW;
-    int gx = x0 + lx, gy = y0 + ly;
-    if (gx < cx0 || gx >= cx1 || gy < cy0 || gy >= cy1) continue;
-    int32_t v0 = S[0][ly + HALO][lx + HALO], v1 = 0, v2 = 0;
-    if (nc >= 3) {
-      v1 = S[1][ly + HALO][lx + HALO];
-      v2 = S[2][ly + HALO][lx + HALO];
-      if (job.mct) {
-        int32_t g = v0 - ((v2 + v1) >> 2);
-        int32_t r = v2 + g, b = v1 + g;
-        v0 = r;
-        v1 = g;
-        v2 = b;
+  const int32_t shift = 1 << (bd - 1);
+  const bool mct = NC == 3 && job.mct;
+  const int b = (x0 >> 1) + lane, col = 2 * b;
+  const int xs = max(x0, cx0), xe = min(x0 + kIdwtStripW, cx1);
+  const int nbytes = (xe - xs) * bpp;
+  auto emit = [&](int y, const int2* v) {
+    if (y < cy0 || y >= cy0 + (int)job.ch) return;  // warp-uniform
+    const uint64_t gbase = (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
+    const int off = (int)(gbase & 15);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int px = col + k;
+      if (px < xs || px >= xe) continue;
+      int32_t c0 = k ? v[0].y : v[0].x, c1 = 0, c2 = 0;
+      if (NC == 3) {
+        c1 = k ? v[1].y : v[1].x;
+        c2 = k ? v[2].y : v[2].x;
+        if (mct) {
+          const int32_t g = c0 - ((c2 + c1) >> 2);
+          const int32_t r = c2 + g, bl = c1 + g;
+          c0 = r;
+          c1 = g;
+          c2 = bl;
+        }
+        c1 += shift;
+        c2 += shift;
       }
-      v1 += shift;
-      v2 += shift;
+      c0 += shift;
+      put_pixel(rowbuf + off + (px - xs) * bpp, fmt, c0, c1, c2, bd, reg);
     }
-    v0 += shift;
-    const uint64_t gbase = (uint64_t)(gy - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
-    uint8_t* o = &O[ly][(gbase & 15) + (size_t)(gx - xs) * bpp];
-    switch (fmt) {
-      case PACK_GRAY8: o[0] = to_u8(v0, bd, reg); break;
-      case PACK_RGB8:
-        o[0] = to_u8(v0, bd, reg);
-        o[1] = to_u8(v1, bd, reg);
-        o[2] = to_u8(v2, bd, reg);
-        break;
-      case PACK_RGBA8:
-        o[0] = to_u8(v0, bd, reg);
-        o[1] = to_u8(v1, bd, reg);
-        o[2] = to_u8(v2, bd, reg);
-        o[3] = 255;
-        break;
-      case PACK_GRAY16: {
-        uint16_t a = to_u16(v0, bd);
-        o[0] = (uint8_t)a;
-        o[1] = (uint8_t)(a >> 8);
-        break;
-      }
-      case PACK_RGB16: {
-        uint16_t a = to_u16(v0, bd), g = to_u16(v1, bd), c = to_u16(v2, bd);
-        o[0] = (uint8_t)a;
-        o[1] = (uint8_t)(a >> 8);
-        o[2] = (uint8_t)g;
-        o[3] = (uint8_t)(g >> 8);
-        o[4] = (uint8_t)c;
-        o[5] = (uint8_t)(c >> 8);
-        break;
-      }
-    }
-  }
-  __syncthreads();
-  if (npix <= 0) return;
-  // Copy-out: one warp per row; bytes up to the first 16-byte boundary, then
-  // 16-byte vectors, then the tail.
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int nbytes = npix * bpp;
-  for (int ly = warp; ly < TH; ly += nwarps) {
-    const int gy = y0 + ly;
-    if (gy < cy0 || gy >= cy1) continue;
-    const uint64_t gbase = (uint64_t)(gy - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
+    __syncwarp();
+    // Copy-out: bytes up to the first 16-byte boundary, 16-byte vectors, tail.
     uint8_t* g = job.out + gbase;
-    const uint8_t* src = &O[ly][gbase & 15];
+    const uint8_t* src = rowbuf + off;
     int head = (int)((16 - ((uintptr_t)g & 15)) & 15);
     if (head > nbytes) head = nbytes;
     if (lane < head) g[lane] = src[lane];
@@ -274,18 +274,55 @@ __global__ void __launch_bounds__(kIdwtThreads) pack_kernel(const PackJob* __res
     for (int k = lane; k < nvec; k += 32) gv[k] = sv[k];
     const int done = head + (nvec << 4);
     if (lane < nbytes - done) g[done + lane] = src[done + lane];
+    __syncwarp();
+  };
+  if (job.lifting) {
+    Bands B[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) B[c] = Bands{job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, (int)job.h};
+    stream_rows<NC>(B, b, lane, ys, ye, emit);
+  } else {
+    // Nothing left to lift: the image is the LL band itself.
+    for (int y = ys; y < ye; ++y) {
+      int2 v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int32_t* row = job.ll[c] + (size_t)y * w;
+        v[c].x = col < w ? __ldg(row + col) : 0;
+        v[c].y = col + 1 < w ? __ldg(row + col + 1) : 0;
+      }
+      emit(y, v);
+    }
   }
 }
 
-cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream) {
-  if (njobs == 0 || total_ctas == 0) return cudaSuccess;
-  idwt_level_kernel<<<total_ctas, kIdwtThreads, 0, stream>>>(jobs, njobs);
+}  // namespace
+
+__global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+                                                               uint32_t nunits) {
+  __shared__ __align__(16) uint8_t rowbufs[kIdwtWarps][kRowBytes];
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t unit = blockIdx.x * kIdwtWarps + warp;
+  if (unit >= nunits) return;
+  const int lane = threadIdx.x & 31;
+  const PackJob& job = find_job(jobs, njobs, unit);
+  const uint32_t local = unit - job.unit_begin;
+  const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
+  const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * kIdwtSegRows;
+  const int ye = min(ys + kIdwtSegRows, (int)(job.cy + job.ch));
+  if (job.ncomp >= 3) pack_unit<3>(job, x0, ys, ye, lane, rowbufs[warp]);
+  else pack_unit<1>(job, x0, ys, ye, lane, rowbufs[warp]);
+}
+
+cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
+  if (njobs == 0 || nunits == 0) return cudaSuccess;
+  idwt_level_kernel<<<(nunits + kIdwtWarps - 1) / kIdwtWarps, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits);
   return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream) {
-  if (njobs == 0 || total_ctas == 0) return cudaSuccess;
-  pack_kernel<<<total_ctas, kIdwtThreads, 0, stream>>>(jobs, njobs);
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
+  if (njobs == 0 || nunits == 0) return cudaSuccess;
+  pack_kernel<<<(nunits + kIdwtWarps - 1) / kIdwtWarps, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits);
   return cudaGetLastError();
 }
 

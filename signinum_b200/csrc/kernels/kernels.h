@@ -24,7 +24,8 @@ cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* 
                               cudaStream_t stream);
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,
                              uint32_t* tile_status, cudaStream_t stream);
-cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream);
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t total_ctas, cudaStream_t stream);
+// nunits: work units (strip x row segment) of all jobs of the launch.
+cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream);
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream);
 
 }  // namespace sgn
