@@ -15,9 +15,12 @@
 namespace sgn {
 
 // Work unit of the IDWT kernels: one warp decodes a strip of kIdwtStripW
-// columns (two per lane) over kIdwtSegRows rows of one level.
+// columns (two per lane) over `seg` rows of one level (even, chosen per job).
 constexpr int kIdwtStripW = 64;
-constexpr int kIdwtSegRows = 64;
+
+// Rows per work unit: long segments for big levels (less halo re-reading),
+// short ones for small levels (more warps in flight).
+inline uint32_t idwt_segment_rows(uint32_t h) { return h >= 256 ? 64 : (h >= 64 ? 32 : 16); }
 constexpr int kIdwtWarps = 8;  // warps (units) per CTA
 
 struct HtJob {
@@ -51,6 +54,8 @@ struct IdwtJob {
   uint32_t w, h;
   uint32_t strips;      // strips across the level
   uint32_t unit_begin;  // first work unit of this job in its launch
+  uint32_t seg;         // output rows per work unit (even)
+  uint32_t pad;
 };
 
 enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
@@ -68,6 +73,7 @@ struct PackJob {
   uint32_t ncomp, mct, bit_depth, fmt, region_conv;
   uint32_t strips;      // strips across the crop (from cx rounded down to kIdwtStripW)
   uint32_t unit_begin;  // first work unit of this job in its launch
+  uint32_t seg;         // output rows per work unit (even)
   uint32_t tile;        // batch index (status)
 };
 

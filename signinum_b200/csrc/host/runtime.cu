@@ -419,6 +419,8 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
         j.h = res_dim(r, false);
         j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
         j.unit_begin = 0;
+        j.seg = idwt_segment_rows(j.h);
+        j.pad = 0;
         if (j.w == 0 || j.h == 0) continue;
         rounds[r - 1].push_back(j);
       }
@@ -465,7 +467,8 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
     pj.region_conv = tw.region_conv;
     uint32_t ax = tw.crop_x & ~(uint32_t)(kIdwtStripW - 1), ay = tw.crop_y & ~1u;
     pj.strips = (tw.crop_x + tw.crop_w - ax + kIdwtStripW - 1) / kIdwtStripW;
-    uint32_t segs = (tw.crop_y + tw.crop_h - ay + kIdwtSegRows - 1) / kIdwtSegRows;
+    pj.seg = idwt_segment_rows(tw.crop_h);
+    uint32_t segs = (tw.crop_y + tw.crop_h - ay + pj.seg - 1) / pj.seg;
     pj.unit_begin = plan->pack_ctas;
     pj.tile = (uint32_t)i;
     plan->pack_ctas += pj.strips * segs;
@@ -477,7 +480,7 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
     RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0};
     for (IdwtJob& j : rj) {
       j.unit_begin = ri.ctas;
-      ri.ctas += j.strips * ((j.h + kIdwtSegRows - 1) / kIdwtSegRows);
+      ri.ctas += j.strips * ((j.h + j.seg - 1) / j.seg);
       idwt.push_back(j);
     }
     if (ri.njobs) plan->rounds.push_back(ri);

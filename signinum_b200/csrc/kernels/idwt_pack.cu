@@ -9,7 +9,7 @@
 // (:908-925).  All values are integers, so int32 with arithmetic shifts gives
 // the reference's f32 floors bit for bit.
 //
-// Mapping: one warp per unit = a strip of 64 columns x 64 rows of one level.
+// Mapping: one warp per unit = a strip of 64 columns x `seg` rows of a level.
 // Lane k owns image columns (2k, 2k+1) of the strip, i.e. band column k of
 // the low and high bands, so every band load and every row store is
 // coalesced.  Horizontal lifting of a row needs the odd neighbour on the left
@@ -39,6 +39,7 @@ constexpr int kLanes = 32;
 // Periodic symmetric extension of index i into [0, n) (reflections about the
 // first and last samples; the streams overshoot by at most a few samples).
 __device__ __forceinline__ int fold(int i, int n) {
+  if ((unsigned)i < (unsigned)n) return i;
   if (n == 1) return 0;
 #pragma unroll 1
   for (int k = 0; k < 8 && (i < 0 || i >= n); ++k) i = i < 0 ? -i : 2 * (n - 1) - i;
@@ -53,39 +54,61 @@ struct Bands {
   int w, h;
 };
 
-// Horizontally lifted row y of the interleaved level, at this lane's columns
-// (col, col + 1) with col = 2b.  Lanes past the right edge return garbage.
-__device__ __forceinline__ int2 hrow(const Bands& B, int y, int b, int lane) {
+// Band samples of one interleaved row at this lane's columns (col, col + 1),
+// col = 2b, plus the extra samples the strip's edge lanes need.  Loads only:
+// the lifting happens in lift_row, so a caller can keep the next rows' loads
+// in flight while it lifts the current ones.
+struct RawRow {
+  int lo, hi;     // low band (column col), high band (column col + 1)
+  int hi_left;    // lane 0: high band at column col - 1
+  int lo_r, hi_r; // lane 31: low / high band at columns col + 2, col + 3
+};
+
+__device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lane) {
   y = fold(y, B.h);
   const int r = y >> 1;
   const int lw = (B.w + 1) >> 1, hw = B.w >> 1;
-  const int32_t* L = (y & 1) ? B.lh : B.ll;
-  const int32_t* H = (y & 1) ? B.hh : B.hl;
+  const int32_t* Lr = ((y & 1) ? B.lh : B.ll) + (size_t)r * lw;
+  const int32_t* Hr = ((y & 1) ? B.hh : B.hl) + (size_t)r * hw;
   const int col = 2 * b;
-  const int32_t* Lr = L + (size_t)r * lw;
-  const int32_t* Hr = H + (size_t)r * hw;
-  int lo = col < B.w ? __ldg(Lr + b) : 0;
-  if (B.w == 1) return make_int2(lo, 0);
-  int hi = col + 1 < B.w ? __ldg(Hr + b) : 0;
+  RawRow R;
+  R.lo = col < B.w ? __ldg(Lr + b) : 0;
+  R.hi = col + 1 < B.w ? __ldg(Hr + b) : 0;
+  R.hi_left = (lane == 0 && b > 0) ? __ldg(Hr + b - 1) : 0;
+  R.lo_r = (lane == kLanes - 1 && col + 2 < B.w) ? __ldg(Lr + b + 1) : 0;
+  R.hi_r = (lane == kLanes - 1 && col + 3 < B.w) ? __ldg(Hr + b + 1) : 0;
+  return R;
+}
+
+// Horizontal lifting of a loaded row: (even, odd) samples of this lane.
+// Lanes past the right edge return garbage.
+__device__ __forceinline__ int2 lift_row(const RawRow& R, int w, int b, int lane) {
+  if (w == 1) return make_int2(R.lo, 0);
+  const int col = 2 * b;
+  int hi = R.hi;
   int hiL = __shfl_up_sync(0xFFFFFFFFu, hi, 1);
-  if (lane == 0) hiL = b == 0 ? hi : __ldg(Hr + b - 1);  // column -1 mirrors column 1
-  if (col + 1 >= B.w) hi = hiL;                          // column w mirrors column w - 2
-  const int E = lo - ((hiL + hi + 2) >> 2);
+  if (lane == 0) hiL = b == 0 ? hi : R.hi_left;  // column -1 mirrors column 1
+  if (col + 1 >= w) hi = hiL;                     // column w mirrors column w - 2
+  const int E = R.lo - ((hiL + hi + 2) >> 2);
   int ER = __shfl_down_sync(0xFFFFFFFFu, E, 1);
-  if (lane == kLanes - 1 && col + 2 < B.w) {
-    const int lo2 = __ldg(Lr + b + 1);
-    const int hi2 = col + 3 < B.w ? __ldg(Hr + b + 1) : hi;
-    ER = lo2 - ((hi + hi2 + 2) >> 2);
+  if (lane == kLanes - 1 && col + 2 < w) {
+    const int hi2 = col + 3 < w ? R.hi_r : hi;
+    ER = R.lo_r - ((hi + hi2 + 2) >> 2);
   }
-  if (col + 2 >= B.w) ER = E;  // column w mirrors column w - 2
+  if (col + 2 >= w) ER = E;  // column w mirrors column w - 2
   return make_int2(E, hi + ((E + ER) >> 1));
 }
 
+__device__ __forceinline__ int2 hrow(const Bands& B, int y, int b, int lane) {
+  return lift_row(load_row(B, y, b, lane), B.w, b, lane);
+}
+
 // Vertical 5/3 stream over output rows [ys, ye) (ys even) of NC level
-// images at once; emit(y, v[NC]) receives each finished row.
+// images at once; emit(y, v[NC]) receives each finished row.  The loads of
+// row pair m + 1 are issued before row pair m is lifted.
 template <int NC, typename Emit>
 __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int ys, int ye, Emit emit) {
-  const int h = B[0].h;
+  const int h = B[0].h, w = B[0].w;
   int2 v[NC];
   if (h == 1) {
 #pragma unroll
@@ -94,18 +117,27 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
     return;
   }
   int2 xo_prev[NC], ev_prev[NC];
+  RawRow re[NC], ro[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
+    re[c] = load_row(B[c], ys, b, lane);
+    ro[c] = load_row(B[c], ys + 1, b, lane);
     xo_prev[c] = hrow(B[c], ys - 1, b, lane);
     ev_prev[c] = make_int2(0, 0);
   }
   for (int m = ys >> 1;; ++m) {
     const int ye_row = 2 * m, yo_row = 2 * m + 1;
+    const bool more = yo_row < ye;
+    RawRow ne[NC], no[NC];
     int2 ev[NC], xo[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      const int2 xe = hrow(B[c], ye_row, b, lane);
-      xo[c] = hrow(B[c], yo_row, b, lane);
+      if (more) {
+        ne[c] = load_row(B[c], ye_row + 2, b, lane);
+        no[c] = load_row(B[c], yo_row + 2, b, lane);
+      }
+      const int2 xe = lift_row(re[c], w, b, lane);
+      xo[c] = lift_row(ro[c], w, b, lane);
       ev[c].x = xe.x - ((xo_prev[c].x + xo[c].x + 2) >> 2);
       ev[c].y = xe.y - ((xo_prev[c].y + xo[c].y + 2) >> 2);
     }
@@ -118,11 +150,13 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
       emit(ye_row - 1, v);
     }
     if (ye_row < ye) emit(ye_row, ev);
-    if (yo_row >= ye) break;
+    if (!more) break;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       xo_prev[c] = xo[c];
       ev_prev[c] = ev[c];
+      re[c] = ne[c];
+      ro[c] = no[c];
     }
   }
 }
@@ -148,9 +182,9 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJ
   const IdwtJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
   const int x0 = (int)(local % job.strips) * kIdwtStripW;
-  const int ys = (int)(local / job.strips) * kIdwtSegRows;
+  const int ys = (int)(local / job.strips) * (int)job.seg;
   const int w = (int)job.w, h = (int)job.h;
-  const int ye = min(ys + kIdwtSegRows, h);
+  const int ye = min(ys + (int)job.seg, h);
   Bands B{job.ll, job.hl, job.lh, job.hh, w, h};
   const int b = (x0 >> 1) + lane, col = 2 * b;
   int32_t* out = job.out;
@@ -308,8 +342,8 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __
   const PackJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
   const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
-  const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * kIdwtSegRows;
-  const int ye = min(ys + kIdwtSegRows, (int)(job.cy + job.ch));
+  const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
+  const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
   if (job.ncomp >= 3) pack_unit<3>(job, x0, ys, ye, lane, rowbufs[warp]);
   else pack_unit<1>(job, x0, ys, ye, lane, rowbufs[warp]);
 }
