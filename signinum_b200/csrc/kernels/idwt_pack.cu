@@ -104,9 +104,10 @@ __device__ __forceinline__ int2 hrow(const Bands& B, int y, int b, int lane) {
 }
 
 // Vertical 5/3 stream over output rows [ys, ye) (ys even) of NC level
-// images at once; emit(y, v[NC]) receives each finished row.  The loads of
-// row pair m + 1 are issued before row pair m is lifted.
-template <int NC, typename Emit>
+// images at once; emit(y, v[NC]) receives each finished row.  With PREFETCH
+// the loads of row pair m + 1 are issued before row pair m is lifted (more
+// registers; used where a warp streams one component).
+template <int NC, bool PREFETCH, typename Emit>
 __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int ys, int ye, Emit emit) {
   const int h = B[0].h, w = B[0].w;
   int2 v[NC];
@@ -128,11 +129,18 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
   for (int m = ys >> 1;; ++m) {
     const int ye_row = 2 * m, yo_row = 2 * m + 1;
     const bool more = yo_row < ye;
+    if (!PREFETCH && m != (ys >> 1)) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        re[c] = load_row(B[c], ye_row, b, lane);
+        ro[c] = load_row(B[c], yo_row, b, lane);
+      }
+    }
     RawRow ne[NC], no[NC];
     int2 ev[NC], xo[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      if (more) {
+      if (PREFETCH && more) {
         ne[c] = load_row(B[c], ye_row + 2, b, lane);
         no[c] = load_row(B[c], yo_row + 2, b, lane);
       }
@@ -155,8 +163,10 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
     for (int c = 0; c < NC; ++c) {
       xo_prev[c] = xo[c];
       ev_prev[c] = ev[c];
-      re[c] = ne[c];
-      ro[c] = no[c];
+      if (PREFETCH) {
+        re[c] = ne[c];
+        ro[c] = no[c];
+      }
     }
   }
 }
@@ -188,7 +198,7 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJ
   Bands B{job.ll, job.hl, job.lh, job.hh, w, h};
   const int b = (x0 >> 1) + lane, col = 2 * b;
   int32_t* out = job.out;
-  stream_rows<1>(&B, b, lane, ys, ye, [&](int y, const int2* v) {
+  stream_rows<1, true>(&B, b, lane, ys, ye, [&](int y, const int2* v) {
     int32_t* row = out + (size_t)y * w;
     if (col < w) row[col] = v[0].x;
     if (col + 1 < w) row[col + 1] = v[0].y;
@@ -314,7 +324,7 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
     Bands B[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) B[c] = Bands{job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, (int)job.h};
-    stream_rows<NC>(B, b, lane, ys, ye, emit);
+    stream_rows<NC, NC == 1>(B, b, lane, ys, ye, emit);
   } else {
     // Nothing left to lift: the image is the LL band itself.
     for (int y = ys; y < ye; ++y) {
