@@ -555,7 +555,7 @@ sgn_status execute(sgn_ctx* ctx, sgn_plan* p) {
   for (const RoundInfo& r : p->rounds)
     if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s)) != cudaSuccess)
       return cuda_status(e, "IDWT launch");
-  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, s)) != cudaSuccess) return cuda_status(e, "pack launch");
+  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s)) != cudaSuccess) return cuda_status(e, "pack launch");
   return SGN_OK;
 }
 
@@ -714,7 +714,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   chk(cudaEventRecord(ev[2], s));
   for (const RoundInfo& r : p->rounds) chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s));
   chk(cudaEventRecord(ev[3], s));
-  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, s));
+  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s));
   chk(cudaEventRecord(ev[4], s));
   chk(cudaEventSynchronize(ev[4]));
   if (e == cudaSuccess) {

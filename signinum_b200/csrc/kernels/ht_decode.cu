@@ -186,10 +186,19 @@ __device__ __forceinline__ int32_t to_i32(uint32_t v, uint32_t nbp) {
   return (v & 0x80000000u) ? -m : m;
 }
 
+// Significance of the two bottom samples of a quad (entry bits 5 and 7), the
+// only part of a quad the row below takes its context from, as two bits.
+__device__ __forceinline__ uint32_t ctx_bits(uint32_t t) { return ((t >> 5) & 1) | ((t >> 6) & 2); }
+// The same two bits spread back to their entry positions.
+__device__ __forceinline__ uint32_t ctx_entry(uint32_t b) { return ((b & 1) << 5) | ((b & 2) << 6); }
+
 // CxtVLC / MEL / UVLC pass of one block (decode_cleanup_symbols,
 // ht_block_decode.rs:1056-1205): the serial chain of the cleanup pass.  Writes
 // one 32-bit symbol per quad (entry | u << 16) into the block's symbol table,
-// quad rows of nq entries; the previous row's entries give the context.
+// quad rows of nq entries.  The row above gives the context: with REG (blocks
+// at most 64 wide, nq <= 32) its two context bits per quad live in a 64-bit
+// register, otherwise they are read back from the symbol table.
+template <bool REG>
 __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T) {
   const uint32_t lcup = job.lcup, w = job.w, h = job.h;
   if (lcup < 2) return false;
@@ -202,6 +211,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
   int run = mel.get_run();
   const uint32_t nq = (w + 1) / 2;
   uint32_t* row = sym;
+  uint64_t ctx = 0;  // REG: context bits of the row above, 2 per quad
   // Initial quad row.
   {
     uint32_t c_q = 0;
@@ -242,6 +252,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       ue >>= 3;
       row[q] = t0 | ((1 + (ue & 7) + (tmp & ~(0xFFu << len))) << 16);
       if (hasB) row[q + 1] = t1 | ((1 + (ue >> 3) + (tmp >> len)) << 16);
+      if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
     }
   }
   // Other quad rows: context from the row above (quads q, q+1, q+2).
@@ -249,11 +260,27 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
     const uint32_t* prev = row;
     row += nq;
     uint32_t c_q = 0;
-    uint32_t pq0 = prev[0] & 0xFFFF;
-    uint32_t pq1 = nq > 1 ? prev[1] & 0xFFFF : 0;
+    const uint64_t above = ctx;
+    ctx = 0;
+    uint32_t pq0, pq1;
+    if (REG) {
+      pq0 = ctx_entry((uint32_t)above);
+      pq1 = ctx_entry((uint32_t)above >> 2);
+    } else {
+      pq0 = prev[0] & 0xFFFF;
+      pq1 = nq > 1 ? prev[1] & 0xFFFF : 0;
+    }
     for (uint32_t q = 0; q < nq; q += 2) {
-      uint32_t pq2 = q + 2 < nq ? prev[q + 2] & 0xFFFF : 0;
-      uint32_t pq3 = q + 3 < nq ? prev[q + 3] & 0xFFFF : 0;
+      uint32_t pq2, pq3;
+      if (REG) {
+        // Bits past the row's last quad are zero.
+        const uint32_t a = (uint32_t)(above >> (2 * q)) >> 4;  // 2q <= 60
+        pq2 = ctx_entry(a);
+        pq3 = ctx_entry(a >> 2);
+      } else {
+        pq2 = q + 2 < nq ? prev[q + 2] & 0xFFFF : 0;
+        pq3 = q + 3 < nq ? prev[q + 3] & 0xFFFF : 0;
+      }
       c_q |= (pq0 & 0xA0) << 2;
       c_q |= (pq1 & 0x20) << 4;
       uint32_t v = vlc.fetch();
@@ -291,6 +318,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       ue >>= 3;
       row[q] = t0 | (((ue & 7) + (tmp & ~(0xFFu << len))) << 16);
       if (hasB) row[q + 1] = t1 | (((ue >> 3) + (tmp >> len)) << 16);
+      if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
       pq0 = pq2;
       pq1 = pq3;
     }
@@ -316,7 +344,9 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
   const HtJob job = jobs[j];
   if (job.passes == 0) return;
   uint32_t* sym = symbols + job.sym;
-  if (!decode_vlc(job, arena + job.src, sym, T)) sym[0] = kSymFailed;
+  const bool ok = job.w <= 64 ? decode_vlc<true>(job, arena + job.src, sym, T)
+                              : decode_vlc<false>(job, arena + job.src, sym, T);
+  if (!ok) sym[0] = kSymFailed;
 }
 
 namespace {
@@ -370,6 +400,150 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t* W, uint32_t nwords, 
   return __funnelshift_r(lo, hi, sh);
 }
 
+
+// The magnitude/sign rows of one block (decode_magnitude_sign_phase,
+// ht_block_decode.rs:1435-1561) for the calling warp.  Per quad row the lanes
+// take one quad each; a warp prefix scan of the per-quad bit counts gives each
+// lane its bit offset in the unstuffed stream W, and the lane reads its bits
+// through one 64-bit window.  The exponent bound kappa needs the bit lengths
+// of v_n of the four samples above the quad: with NARROW (blocks at most 64
+// wide, one quad per lane per row) they stay in registers and come from the
+// neighbouring lanes by shuffles, otherwise they are kept per column in
+// shared memory (Ebase, two rows of `cols` bytes).  Returns true (on every
+// lane) when the stream is invalid.
+template <bool NARROW>
+__device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_words, uint8_t* Ebase, uint32_t cols,
+                            const uint32_t* __restrict__ sym, int32_t* __restrict__ dst) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t w = job.w, h = job.h, stride = job.stride;
+  const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
+  const bool raw = job.passes > 1;
+  const bool pairs = ((job.dst | stride) & 1) == 0;  // 8-byte aligned sample pairs
+  const uint32_t nq = (w + 1) / 2;
+  uint8_t* Eprev = Ebase;  // wide blocks: bit lengths of v_n per column + 1, row above
+  uint8_t* Ecur = Ebase + cols;
+  if (!NARROW) {
+    for (uint32_t c = lane; c < cols; c += 32) Eprev[c] = 0;
+    __syncwarp();
+  }
+  uint32_t e_left = 0, e_right = 0;  // NARROW: bottom-row bit lengths of this lane's quad
+  uint32_t rowbase = 0;
+  bool bad = false;
+  for (uint32_t y = 0, r = 0; y < h; y += 2, ++r) {
+    const bool initial = y == 0, second = y + 1 < h;
+    int32_t* row0 = dst + (size_t)y * stride;
+    int32_t* row1 = row0 + stride;
+    for (uint32_t c0 = 0; c0 < nq; c0 += 32) {
+      const uint32_t q = c0 + lane;
+      const bool active = q < nq;
+      const uint32_t s = active ? sym[(size_t)r * nq + q] : 0;
+      const uint32_t inf = s & 0xFFFF;
+      uint32_t U = s >> 16;
+      if (!initial) {
+        uint32_t e;
+        if (NARROW) {
+          // Columns 2q-1 and 2q+2 belong to the neighbouring lanes' quads;
+          // outside the block they are zero (lanes past nq hold zeros).
+          uint32_t l = __shfl_up_sync(0xFFFFFFFFu, e_right, 1);
+          uint32_t rr = __shfl_down_sync(0xFFFFFFFFu, e_left, 1);
+          if (lane == 0) l = 0;
+          if (lane == 31) rr = 0;
+          e = max(max(l, e_left), max(e_right, rr));
+        } else {
+          // Columns 2q-1 .. 2q+2 of the row above live at Eprev[col + 1]
+          // (index <= 2*nq + 1 <= w + 2 < max_w + 4 for an active lane).
+          e = active ? max(max((uint32_t)Eprev[2 * q], (uint32_t)Eprev[2 * q + 1]),
+                           max((uint32_t)Eprev[2 * q + 2], (uint32_t)Eprev[2 * q + 3]))
+                     : 0;
+        }
+        uint32_t gamma = inf & 0xF0;
+        gamma &= gamma - 0x10;
+        if (active) U += gamma != 0 ? max(e, 2u) - 1 : 1;
+      }
+      bad |= active && U > mmsbp2;
+      // m_n per sample (0 when insignificant) and the quad's bit count.
+      uint32_t m[4], tot = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
+        tot += m[i];
+      }
+      // Warp inclusive scan of the bit counts.
+      uint32_t inc = tot;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+        if (lane >= (uint32_t)d) inc += v;
+      }
+      const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 31);
+      uint32_t off = rowbase + inc - tot;
+      rowbase += chunk_bits;
+      // This quad's bits: one 64-bit window when they fit, else per sample.
+      const bool window = tot < 64;
+      uint64_t win = 0;
+      if (window && (inf & 0xF0)) win = (uint64_t)bits_at(W, ms_words, off) | ((uint64_t)bits_at(W, ms_words, off + 32) << 32);
+      uint32_t val[4], E[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        val[i] = 0;
+        E[i] = 0;
+        if ((inf >> (4 + i)) & 1) {
+          const uint32_t mn = m[i];
+          uint32_t msv;
+          if (window) {
+            msv = (uint32_t)win;
+            win >>= mn;
+          } else {
+            msv = bits_at(W, ms_words, off);
+            off += mn;
+          }
+          uint32_t mask = mn == 0 ? 0 : (mn >= 32 ? 0xFFFFFFFFu : ((1u << mn) - 1));
+          uint32_t v = (msv & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
+          val[i] = (msv << 31) | ((v + 2) << (p - 1));
+          E[i] = 32 - __clz(v);
+        }
+      }
+      if (active) {
+        const uint32_t x = 2 * q;
+        auto cv = [&](uint32_t vv) { return raw ? (int32_t)vv : to_i32(vv, nbp); };
+        if (pairs && x + 1 < w) {
+          *reinterpret_cast<int2*>(row0 + x) = make_int2(cv(val[0]), cv(val[2]));
+          if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(cv(val[1]), cv(val[3]));
+        } else {
+          row0[x] = cv(val[0]);
+          if (second) row1[x] = cv(val[1]);
+          if (x + 1 < w) {
+            row0[x + 1] = cv(val[2]);
+            if (second) row1[x + 1] = cv(val[3]);
+          }
+        }
+        if (!NARROW) {
+          // Bottom-row exponents of this quad for the next quad row.
+          Ecur[x + 1] = (uint8_t)E[1];
+          Ecur[x + 2] = x + 1 < w ? (uint8_t)E[3] : 0;
+        }
+      }
+      if (NARROW) {
+        e_left = active ? E[1] : 0;
+        e_right = active && 2 * q + 1 < w ? E[3] : 0;
+      }
+    }
+    if (!NARROW) {
+      __syncwarp();
+      // Columns outside [0, w) stay zero in both buffers.
+      if (lane == 0) {
+        Ecur[0] = 0;
+        Ecur[w + 1] = 0;
+        Ecur[w + 2] = 0;
+      }
+      __syncwarp();
+      uint8_t* t = Eprev;
+      Eprev = Ecur;
+      Ecur = t;
+    }
+  }
+  return __any_sync(0xFFFFFFFFu, bad);
+}
 }  // namespace
 
 // Pass 2: one warp per code block decodes magnitudes and signs
@@ -411,94 +585,9 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
   if (ok) {
     const uint32_t ms_len = lcup - scup;
     unstuff_magsgn(src, ms_len, W, ms_words);
-    const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
-    const bool raw = job.passes > 1;
-    const uint32_t nq = (w + 1) / 2;
-    uint8_t* Eprev = Ebase;  // bit lengths of v_n, bottom row of the previous quad row, per column + 2
-    uint8_t* Ecur = Ebase + cols;
-    for (uint32_t c = lane; c < cols; c += 32) Eprev[c] = 0;
-    __syncwarp();
-    uint32_t rowbase = 0;
-    bool bad = false;
-    for (uint32_t y = 0, r = 0; y < h; y += 2, ++r) {
-      const bool initial = y == 0, second = y + 1 < h;
-      int32_t* row0 = dst + (size_t)y * stride;
-      int32_t* row1 = row0 + stride;
-      for (uint32_t c0 = 0; c0 < nq; c0 += 32) {
-        const uint32_t q = c0 + lane;
-        const bool active = q < nq;
-        const uint32_t s = active ? sym[(size_t)r * nq + q] : 0;
-        const uint32_t inf = s & 0xFFFF;
-        uint32_t U = s >> 16;
-        if (!initial && active) {
-          uint32_t gamma = inf & 0xF0;
-          gamma &= gamma - 0x10;
-          // Columns 2q-1 .. 2q+2 of the row above live at Eprev[col + 1]
-          // (index <= 2*nq + 1 <= w + 2 < max_w + 4 for an active lane).
-          uint32_t e = max(max((uint32_t)Eprev[2 * q], (uint32_t)Eprev[2 * q + 1]),
-                           max((uint32_t)Eprev[2 * q + 2], (uint32_t)Eprev[2 * q + 3]));
-          U += gamma != 0 ? max(e, 2u) - 1 : 1;
-        }
-        bad |= active && U > mmsbp2;
-        // m_n per sample (0 when insignificant) and the quad's bit count.
-        uint32_t m[4], tot = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
-          tot += m[i];
-        }
-        // Warp inclusive scan of the bit counts.
-        uint32_t inc = tot;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-          if (lane >= (uint32_t)d) inc += v;
-        }
-        const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 31);
-        uint32_t off = rowbase + inc - tot;
-        rowbase += chunk_bits;
-        uint32_t val[4], E[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          val[i] = 0;
-          E[i] = 0;
-          if ((inf >> (4 + i)) & 1) {
-            uint32_t msv = bits_at(W, ms_words, off);
-            uint32_t mn = m[i];
-            off += mn;
-            uint32_t mask = mn == 0 ? 0 : (mn >= 32 ? 0xFFFFFFFFu : ((1u << mn) - 1));
-            uint32_t v = (msv & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
-            val[i] = (msv << 31) | ((v + 2) << (p - 1));
-            E[i] = 32 - __clz(v);
-          }
-        }
-        if (active) {
-          const uint32_t x = 2 * q;
-          auto put = [&](int32_t* rp, uint32_t xx, uint32_t vv) { rp[xx] = raw ? (int32_t)vv : to_i32(vv, nbp); };
-          put(row0, x, val[0]);
-          if (second) put(row1, x, val[1]);
-          if (x + 1 < w) {
-            put(row0, x + 1, val[2]);
-            if (second) put(row1, x + 1, val[3]);
-          }
-          // Bottom-row exponents of this quad for the next quad row.
-          Ecur[x + 1] = (uint8_t)E[1];
-          Ecur[x + 2] = x + 1 < w ? (uint8_t)E[3] : 0;
-        }
-      }
-      __syncwarp();
-      // Columns outside [0, w) stay zero in both buffers.
-      if (lane == 0) {
-        Ecur[0] = 0;
-        Ecur[w + 1] = 0;
-        Ecur[w + 2] = 0;
-      }
-      __syncwarp();
-      uint8_t* t = Eprev;
-      Eprev = Ecur;
-      Ecur = t;
-    }
-    ok = !__any_sync(0xFFFFFFFFu, bad);
+    const bool bad = job.w <= 64 ? magsgn_rows<true>(job, W, ms_words, Ebase, cols, sym, dst)
+                                 : magsgn_rows<false>(job, W, ms_words, Ebase, cols, sym, dst);
+    ok = !bad;
   }
   if (!ok) {
     __syncwarp();

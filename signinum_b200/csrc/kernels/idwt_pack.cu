@@ -235,9 +235,9 @@ __device__ __forceinline__ uint16_t to_u16(int32_t v, uint32_t bd) {
 constexpr int kRowBytes = kIdwtStripW * 8 + 16;
 
 // Packs one pixel (components v0..v2 after the inverse RCT) into o.
-__device__ __forceinline__ void put_pixel(uint8_t* o, uint32_t fmt, int32_t v0, int32_t v1, int32_t v2, uint32_t bd,
-                                          uint32_t reg) {
-  switch (fmt) {
+template <int FMT>
+__device__ __forceinline__ void put_pixel(uint8_t* o, int32_t v0, int32_t v1, int32_t v2, uint32_t bd, uint32_t reg) {
+  switch (FMT) {
     case PACK_GRAY8: o[0] = to_u8(v0, bd, reg); break;
     case PACK_RGB8:
       o[0] = to_u8(v0, bd, reg);
@@ -269,12 +269,17 @@ __device__ __forceinline__ void put_pixel(uint8_t* o, uint32_t fmt, int32_t v0, 
   }
 }
 
-template <int NC>
+template <int FMT>
+__host__ __device__ constexpr int pack_bpp() {
+  return FMT == PACK_GRAY8 ? 1 : FMT == PACK_RGB8 ? 3 : FMT == PACK_RGBA8 ? 4 : FMT == PACK_GRAY16 ? 2 : 6;
+}
+
+template <int NC, int FMT>
 __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint8_t* rowbuf) {
   const int w = (int)job.w;
   const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw;
-  const uint32_t fmt = job.fmt, bd = job.bit_depth, reg = job.region_conv;
-  const int bpp = fmt == PACK_GRAY8 ? 1 : fmt == PACK_RGB8 ? 3 : fmt == PACK_RGBA8 ? 4 : fmt == PACK_GRAY16 ? 2 : 6;
+  const uint32_t bd = job.bit_depth, reg = job.region_conv;
+  constexpr int bpp = pack_bpp<FMT>();
   const int32_t shift = 1 << (bd - 1);
   const bool mct = NC == 3 && job.mct;
   const int b = (x0 >> 1) + lane, col = 2 * b;
@@ -303,7 +308,7 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
         c2 += shift;
       }
       c0 += shift;
-      put_pixel(rowbuf + off + (px - xs) * bpp, fmt, c0, c1, c2, bd, reg);
+      put_pixel<FMT>(rowbuf + off + (px - xs) * bpp, c0, c1, c2, bd, reg);
     }
     __syncwarp();
     // Copy-out: bytes up to the first 16-byte boundary, 16-byte vectors, tail.
@@ -342,6 +347,7 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
 
 }  // namespace
 
+template <int FMT>
 __global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
                                                                uint32_t nunits) {
   __shared__ __align__(16) uint8_t rowbufs[kIdwtWarps][kRowBytes];
@@ -354,8 +360,8 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __
   const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
   const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
   const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
-  if (job.ncomp >= 3) pack_unit<3>(job, x0, ys, ye, lane, rowbufs[warp]);
-  else pack_unit<1>(job, x0, ys, ye, lane, rowbufs[warp]);
+  if (job.ncomp >= 3) pack_unit<3, FMT>(job, x0, ys, ye, lane, rowbufs[warp]);
+  else pack_unit<1, FMT>(job, x0, ys, ye, lane, rowbufs[warp]);
 }
 
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
@@ -364,9 +370,17 @@ cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nuni
   return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream) {
   if (njobs == 0 || nunits == 0) return cudaSuccess;
-  pack_kernel<<<(nunits + kIdwtWarps - 1) / kIdwtWarps, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits);
+  const dim3 grid((nunits + kIdwtWarps - 1) / kIdwtWarps), block(kIdwtWarps * 32);
+  switch (fmt) {
+    case PACK_GRAY8: pack_kernel<PACK_GRAY8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    case PACK_RGB8: pack_kernel<PACK_RGB8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    case PACK_RGBA8: pack_kernel<PACK_RGBA8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    case PACK_GRAY16: pack_kernel<PACK_GRAY16><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    case PACK_RGB16: pack_kernel<PACK_RGB16><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

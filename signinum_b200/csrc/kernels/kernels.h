@@ -26,6 +26,7 @@ cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n
                              uint32_t* tile_status, cudaStream_t stream);
 // nunits: work units (strip x row segment) of all jobs of the launch.
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream);
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream);
+// All jobs of one launch share the pixel format fmt (a PackFormat).
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream);
 
 }  // namespace sgn
