@@ -252,7 +252,7 @@ def main():
         ev1.synchronize()
     barrier()
     batched_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-    stage = np.mean(np.array(stages), axis=0)  # HT, refine, IDWT, pack, total
+    stage = np.mean(np.array(stages), axis=0)  # VLC, MagSgn, refine, IDWT, pack, total
     launches = plan.launches * args.steps
     value = world * pixels / (batched_ms / 1000.0) / 1e6
     # Parity spot check of the benchmark output against the oracle.
@@ -357,8 +357,8 @@ def main():
     e2e_val = world * pixels / (e2e_ms / 1000.0) / 1e6
 
     if rank == 0:
-        names = ["ht_cleanup_kernel", "ht_refine_kernel", "idwt_level_kernel", "pack_kernel"]
-        dom = int(np.argmax(stage[:4]))
+        names = ["ht_vlc_kernel", "ht_magsgn_kernel", "ht_refine_kernel", "idwt_level_kernel", "pack_kernel"]
+        dom = int(np.argmax(stage[:5]))
         peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
         peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
         algo = coded + out_bytes
@@ -375,8 +375,8 @@ def main():
                            coded_bytes=coded, output_bytes=out_bytes, pixels=pixels),
             "compressed_MB_s": world * coded / (batched_ms / 1000.0) / 1e6,
             "hbm_roofline_frac_path": (world * algo / (batched_ms / 1000.0) / 1e9) / peak,
-            "stage_ms": {"ht_cleanup": stage[0], "ht_refine": stage[1], "idwt_levels": stage[2],
-                         "last_level_pack": stage[3], "total": stage[4]},
+            "stage_ms": {"ht_vlc": stage[0], "ht_magsgn": stage[1], "ht_refine": stage[2], "idwt_levels": stage[3],
+                         "last_level_pack": stage[4], "total": stage[5]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": names[dom],
                          "peak_source": "measured" if PEAKS.exists() else "fallback",

@@ -145,9 +145,9 @@ sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, siz
 /* Surfaces of the plan (valid until sgn_plan_destroy). */
 sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n);
 /* Executes the plan with CUDA events around each stage on the launching
- * stream and waits; stage_ms receives {HT cleanup, HT refinement, IDWT
- * levels, last level + pack, total} in milliseconds (no counterpart in the
- * reference: measurement). */
+ * stream and waits; stage_ms (6 entries) receives {HT cleanup VLC pass, HT
+ * cleanup MagSgn pass, HT refinement, IDWT levels, last level + pack, total}
+ * in milliseconds (no counterpart in the reference: measurement). */
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms);
 /* Launches issued by one execute of the plan. */
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);

@@ -95,7 +95,6 @@ class Workers {
     cv_.notify_all();
     for (auto& t : threads_) t.join();
   }
-  size_t size() const { return threads_.size(); }
   // Runs f(i) for i in [0, n) over the pool plus the calling thread.
   void parallel_for(size_t n, const std::function<void(size_t)>& f) {
     if (n == 0) return;
@@ -114,7 +113,12 @@ class Workers {
       for (size_t k = 0; k < nw; ++k)
         tasks_.push_back([&] {
           body();
-          done_workers.fetch_add(1);
+          // Under the mutex: the waiter checks the count and blocks
+          // atomically with respect to it, so the wake-up cannot be lost.
+          {
+            std::lock_guard<std::mutex> g(m_);
+            done_workers.fetch_add(1);
+          }
           cv_done_.notify_all();
         });
     }
@@ -288,6 +292,12 @@ bool is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Coded-length bucket of a block: the HT job table is ordered by bucket,
+// longest segments first (64-byte steps), which is the order the HT kernels
+// take blocks in.  Exact order inside a bucket does not matter.
+constexpr uint32_t kLenBuckets = 64;
+inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<uint32_t>(lcup >> 6, kLenBuckets - 1); }
+
 sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t fmt,
                       const sgn_request* reqs, sgn_plan* plan) {
   plan->n = n;
@@ -305,7 +315,6 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   // Arena layout.
   std::vector<uint64_t> in_off(n, 0), coef_off(n, 0), lvl_off(n, 0), lvl_size(n, 0);
   uint64_t in_total = 0, coef_total = 0, lvl_total = 0;
-  size_t nblocks = 0, nlevel_jobs = 0;
   uint32_t max_rounds = 0;
   for (size_t i = 0; i < n; ++i) {
     plan->status[i] = work[i].status;
@@ -322,14 +331,21 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
       lvl_size[i] = w * h;
       lvl_off[i] = lvl_total;
       lvl_total += 2 * w * h * L.ncomp;
-      nlevel_jobs += (size_t)(R - 1) * L.ncomp;
       max_rounds = std::max(max_rounds, R - 1);
     }
-    nblocks += L.blocks.size();
   }
   cudaStream_t s = ctx->stream;
   cudaError_t e = cudaSuccess;
   if ((e = dalloc(&plan->d_input, in_total, s)) != cudaSuccess) return cuda_status(e, "input arena");
+  // When the caller's codestreams are pinned and contiguous in arena order
+  // (16-byte padded), they go up in one copy, issued now so that it overlaps
+  // the rest of the plan build.
+  bool direct = n > 0 && in_total > 0 && plan->status[0] == SGN_OK;
+  for (size_t i = 0; direct && i + 1 < n; ++i)
+    direct = plan->status[i + 1] == SGN_OK && datas[i + 1] == datas[i] + ((lens[i] + 15) & ~(size_t)15);
+  direct = direct && is_pinned(datas[0]);
+  if (direct && (e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e, "input upload");
   if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
   if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
   if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
@@ -337,56 +353,61 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   plan->tile_coef_elems.assign(n, 0);
   for (size_t i = 0; i < n; ++i)
     if (plan->status[i] == SGN_OK) plan->tile_coef_elems[i] = work[i].layout.coef_per_comp * work[i].layout.ncomp;
-  // HT jobs, longest segments first.  Each coded block gets a quad-symbol
-  // table (ceil(w/2) x ceil(h/2) words) in the symbol scratch.
-  std::vector<HtJob> ht;
-  ht.reserve(nblocks);
-  std::vector<uint32_t> refine;
-  uint32_t ms_words = 8, max_w = 1;
-  uint64_t sym_total = 0;
-  for (size_t i = 0; i < n; ++i) {
-    if (plan->status[i] != SGN_OK) continue;
-    const TileLayout& L = work[i].layout;
-    for (const CodeBlock& cb : L.blocks) {
-      const Band& b = L.bands[cb.band];
-      HtJob j;
-      std::memset(&j, 0, sizeof(j));
-      j.src = in_off[i] + cb.cleanup_off;
-      j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
-      j.lcup = cb.lcup;
-      j.tile = (uint32_t)i;
-      j.stride = b.w;
-      j.lref = (uint16_t)cb.lref;
-      j.w = cb.w;
-      j.h = cb.h;
-      j.mmsb = cb.missing_msbs;
-      j.passes = cb.passes;
-      j.nbp = b.nbp;
-      j.flags = L.causal ? 1 : 0;
-      max_w = std::max<uint32_t>(max_w, cb.w);
-      if (cb.passes) {
-        j.sym = sym_total;
-        sym_total += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
-        if (cb.lcup >= 2) {
-          const uint8_t* seg = datas[i] + cb.cleanup_off;
-          uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
-          if (scup <= cb.lcup) ms_words = std::max<uint32_t>(ms_words, (cb.lcup - scup + 15) / 4 + 2);
-        }
+
+  // HT job table, pass A (per tile, in parallel): block counts per
+  // coded-length bucket, symbol scratch, refinement blocks and the MagSgn
+  // staging bound.  Each coded block gets a quad-symbol table of
+  // ceil(w/2) x ceil(h/2) words in the symbol scratch.
+  struct TileHt {
+    uint64_t sym = 0;
+    uint32_t nref = 0, ms_words = 8, max_w = 1;
+    uint32_t hist[kLenBuckets];
+  };
+  std::vector<TileHt> th(n);
+  ctx->workers->parallel_for(n, [&](size_t i) {
+    TileHt& t = th[i];
+    std::fill(t.hist, t.hist + kLenBuckets, 0u);
+    if (plan->status[i] != SGN_OK) return;
+    for (const CodeBlock& cb : work[i].layout.blocks) {
+      ++t.hist[len_bucket(cb.lcup)];
+      t.max_w = std::max<uint32_t>(t.max_w, cb.w);
+      if (!cb.passes) continue;
+      t.sym += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
+      if (cb.passes > 1) ++t.nref;
+      if (cb.lcup >= 2) {
+        const uint8_t* seg = datas[i] + cb.cleanup_off;
+        uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
+        if (scup <= cb.lcup) t.ms_words = std::max<uint32_t>(t.ms_words, (cb.lcup - scup + 15) / 4 + 2);
       }
-      ht.push_back(j);
     }
+  });
+  // Bucket-major, tile-minor start positions; symbol and refinement offsets.
+  std::vector<uint64_t> sym_off(n, 0);
+  std::vector<uint32_t> ref_off(n, 0), start((size_t)kLenBuckets * n, 0);
+  uint64_t sym_total = 0;
+  uint32_t nht = 0, nref = 0, ms_words = 8, max_w = 1;
+  for (size_t i = 0; i < n; ++i) {
+    sym_off[i] = sym_total;
+    sym_total += th[i].sym;
+    ref_off[i] = nref;
+    nref += th[i].nref;
+    ms_words = std::max(ms_words, th[i].ms_words);
+    max_w = std::max(max_w, th[i].max_w);
   }
-  std::stable_sort(ht.begin(), ht.end(), [](const HtJob& a, const HtJob& b) { return a.lcup > b.lcup; });
-  for (size_t k = 0; k < ht.size(); ++k)
-    if (ht[k].passes > 1) refine.push_back((uint32_t)k);
-  plan->nht = (uint32_t)ht.size();
+  for (uint32_t b = 0; b < kLenBuckets; ++b)
+    for (size_t i = 0; i < n; ++i) {
+      start[(size_t)b * n + i] = nht;
+      nht += th[i].hist[b];
+    }
+  plan->nht = nht;
   plan->ms_words = ms_words;
   plan->max_w = max_w;
-  if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
-    return cuda_status(e, "symbol scratch");
+  plan->nref = nref;
   if (ht_magsgn_smem_bytes(ms_words, max_w) > 227 * 1024)
     return set_error(SGN_ERR_UNSUPPORTED, "code-block segment too long for the MagSgn staging buffer");
-  plan->nref = (uint32_t)refine.size();
+  if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
+    return cuda_status(e, "symbol scratch");
+
   // IDWT rounds: round r-1 holds resolution r of every tile that has it.
   std::vector<std::vector<IdwtJob>> rounds(max_rounds);
   std::vector<PackJob> packs;
@@ -486,55 +507,70 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
     if (ri.njobs) plan->rounds.push_back(ri);
   }
   plan->npack = (uint32_t)packs.size();
-  if ((e = dalloc(&plan->d_ht, ht.size(), s)) != cudaSuccess) return cuda_status(e, "ht jobs");
-  if ((e = dalloc(&plan->d_refine, refine.size(), s)) != cudaSuccess) return cuda_status(e, "refine list");
+  if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
+  if ((e = dalloc(&plan->d_refine, nref, s)) != cudaSuccess) return cuda_status(e, "refine list");
   if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
   if ((e = dalloc(&plan->d_pack, packs.size(), s)) != cudaSuccess) return cuda_status(e, "pack jobs");
-  // Uploads: codestreams (one copy when the caller's buffers are pinned and
-  // contiguous, else through the pinned staging buffer) and the tables.
-  size_t tables = ht.size() * sizeof(HtJob) + refine.size() * 4 + idwt.size() * sizeof(IdwtJob) +
-                  packs.size() * sizeof(PackJob) + 64;
-  bool direct = n > 0 && in_total > 0;
-  // Contiguity in arena order (16-byte padded) is needed for a single copy.
-  for (size_t i = 0; direct && i + 1 < n; ++i)
-    direct = plan->status[i] == SGN_OK && plan->status[i + 1] == SGN_OK &&
-             datas[i + 1] == datas[i] + ((lens[i] + 15) & ~(size_t)15);
-  direct = direct && plan->status[0] == SGN_OK && is_pinned(datas[0]);
-  size_t stage_bytes = tables + (direct ? 0 : in_total);
+
+  // Pinned staging: [codestreams unless direct] [HT jobs] [refine] [IDWT] [pack].
+  auto up16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+  const size_t at_ht = direct ? 0 : up16(in_total);
+  const size_t at_ref = at_ht + up16((size_t)nht * sizeof(HtJob));
+  const size_t at_idwt = at_ref + up16((size_t)nref * 4);
+  const size_t at_pack = at_idwt + up16(idwt.size() * sizeof(IdwtJob));
+  const size_t stage_bytes = at_pack + up16(packs.size() * sizeof(PackJob));
   if ((e = ctx->staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
   uint8_t* st = ctx->staging.p;
-  size_t at = 0;
-  auto stage = [&](const void* src, size_t bytes) {
-    uint8_t* p = st + at;
-    if (bytes) std::memcpy(p, src, bytes);
-    at += (bytes + 15) & ~(size_t)15;
-    return p;
-  };
-  if (direct) {
-    if ((e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_status(e, "input upload");
-  } else if (in_total) {
-    uint8_t* dst = st;
-    ctx->workers->parallel_for(n, [&](size_t i) {
-      if (plan->status[i] == SGN_OK) std::memcpy(dst + in_off[i], datas[i], lens[i]);
-    });
-    at = (in_total + 15) & ~(size_t)15;
-    if ((e = cudaMemcpyAsync(plan->d_input, st, in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_status(e, "input upload");
-  }
+  HtJob* ht = reinterpret_cast<HtJob*>(st + at_ht);
+  uint32_t* refine = reinterpret_cast<uint32_t*>(st + at_ref);
+  // HT job table, pass B (per tile, in parallel): each tile writes its jobs
+  // at its cursors in the buckets, and the codestream into staging.
+  ctx->workers->parallel_for(n, [&](size_t i) {
+    if (plan->status[i] != SGN_OK) return;
+    if (!direct) std::memcpy(st + in_off[i], datas[i], lens[i]);
+    const TileLayout& L = work[i].layout;
+    uint32_t cursor[kLenBuckets];
+    for (uint32_t b = 0; b < kLenBuckets; ++b) cursor[b] = start[(size_t)b * n + i];
+    uint64_t sym = sym_off[i];
+    uint32_t rk = ref_off[i];
+    for (const CodeBlock& cb : L.blocks) {
+      const Band& b = L.bands[cb.band];
+      const uint32_t pos = cursor[len_bucket(cb.lcup)]++;
+      HtJob& j = ht[pos];
+      std::memset(&j, 0, sizeof(j));
+      j.src = in_off[i] + cb.cleanup_off;
+      j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+      j.lcup = cb.lcup;
+      j.tile = (uint32_t)i;
+      j.stride = b.w;
+      j.lref = (uint16_t)cb.lref;
+      j.w = cb.w;
+      j.h = cb.h;
+      j.mmsb = cb.missing_msbs;
+      j.passes = cb.passes;
+      j.nbp = b.nbp;
+      j.flags = L.causal ? 1 : 0;
+      if (cb.passes) {
+        j.sym = sym;
+        sym += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
+      }
+      if (cb.passes > 1) refine[rk++] = pos;
+    }
+  });
+  if (!idwt.empty()) std::memcpy(st + at_idwt, idwt.data(), idwt.size() * sizeof(IdwtJob));
+  if (!packs.empty()) std::memcpy(st + at_pack, packs.data(), packs.size() * sizeof(PackJob));
   struct Up {
     void* d;
-    const void* h;
-    size_t bytes;
-  } ups[] = {{plan->d_ht, ht.data(), ht.size() * sizeof(HtJob)},
-             {plan->d_refine, refine.data(), refine.size() * 4},
-             {plan->d_idwt, idwt.data(), idwt.size() * sizeof(IdwtJob)},
-             {plan->d_pack, packs.data(), packs.size() * sizeof(PackJob)}};
+    size_t at, bytes;
+  } ups[] = {{plan->d_input, 0, direct ? 0 : in_total},
+             {plan->d_ht, at_ht, (size_t)nht * sizeof(HtJob)},
+             {plan->d_refine, at_ref, (size_t)nref * 4},
+             {plan->d_idwt, at_idwt, idwt.size() * sizeof(IdwtJob)},
+             {plan->d_pack, at_pack, packs.size() * sizeof(PackJob)}};
   for (auto& u : ups) {
     if (!u.bytes) continue;
-    void* p = stage(u.h, u.bytes);
-    if ((e = cudaMemcpyAsync(u.d, p, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_status(e, "table upload");
+    if ((e = cudaMemcpyAsync(u.d, st + u.at, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_status(e, "plan upload");
   }
   // The staging buffer is reused by the next call: finish the copies now.
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
@@ -700,7 +736,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   if (!ctx || !p || !stage_ms) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[6];
   for (auto& e : ev) cudaEventCreate(&e);
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) {
@@ -708,18 +744,20 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   };
   chk(cudaMemsetAsync(p->d_status, 0, std::max<size_t>(p->n, 1) * sizeof(uint32_t), s));
   chk(cudaEventRecord(ev[0], s));
-  chk(launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s));
+  chk(launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s));
   chk(cudaEventRecord(ev[1], s));
-  chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
+  chk(launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s));
   chk(cudaEventRecord(ev[2], s));
-  for (const RoundInfo& r : p->rounds) chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s));
+  chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
   chk(cudaEventRecord(ev[3], s));
-  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s));
+  for (const RoundInfo& r : p->rounds) chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s));
   chk(cudaEventRecord(ev[4], s));
-  chk(cudaEventSynchronize(ev[4]));
+  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s));
+  chk(cudaEventRecord(ev[5], s));
+  chk(cudaEventSynchronize(ev[5]));
   if (e == cudaSuccess) {
-    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
-    cudaEventElapsedTime(&stage_ms[4], ev[0], ev[4]);
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+    cudaEventElapsedTime(&stage_ms[5], ev[0], ev[5]);
   }
   for (auto& x : ev) cudaEventDestroy(x);
   return cuda_status(e, "timed execute");

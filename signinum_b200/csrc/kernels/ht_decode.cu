@@ -40,26 +40,30 @@ struct SmemTables {
 
 __device__ __forceinline__ uint8_t ld8(const uint8_t* p) { return __ldg(p); }
 
-// MEL run decoder (ht_block_decode.rs:782-880).
+// MEL run decoder (ht_block_decode.rs:782-880).  The reference decodes runs
+// into a small queue; here each run is decoded when it is needed, from a
+// 64-bit buffer of unstuffed MEL bits (most significant bit first), with no
+// inner loop: lanes of a warp decode different blocks, so a short fixed
+// sequence per run diverges far less than a queue refill.
 struct Mel {
   const uint8_t* data;
-  uint32_t pos, remaining;
-  uint32_t unstuff, cur, bits_left;
-  int k, num_runs;
-  uint64_t runs;
+  uint32_t pos, remaining, unstuff;
+  uint64_t buf;  // unread bits, left-aligned
+  int bits, k;
   __device__ void init(const uint8_t* d, uint32_t lcup, uint32_t scup) {
     data = d;
     pos = lcup - scup;
     remaining = scup - 1;
     unstuff = 0;
-    cur = 0;
-    bits_left = 0;
+    buf = 0;
+    bits = 0;
     k = 0;
-    num_runs = 0;
-    runs = 0;
   }
-  __device__ __forceinline__ uint32_t bit() {
-    if (bits_left == 0) {
+  // Appends bytes until more than 56 bits are buffered.  After a 0xFF byte
+  // the next byte carries 7 bits; the last byte is ORed with 0x0F and the
+  // stream continues with 0xFF bytes.
+  __device__ void refill() {
+    while (bits <= 56) {
       uint32_t b;
       if (remaining > 0) {
         b = ld8(data + pos);
@@ -69,39 +73,26 @@ struct Mel {
         b = 0xFF;
       }
       if (remaining == 0) b |= 0x0F;
-      cur = b;
-      bits_left = 8 - unstuff;
+      const int nb = 8 - (int)unstuff;
+      buf |= (uint64_t)(b & ((1u << nb) - 1)) << (64 - bits - nb);
+      bits += nb;
       unstuff = b == 0xFF;
-    }
-    --bits_left;
-    return (cur >> bits_left) & 1;
-  }
-  __device__ void more() {
-    while (num_runs < 8) {
-      // MEL exponent table {0,0,0,1,1,1,2,2,2,3,3,4,5}.
-      int e = (k < 3) ? 0 : (k < 6) ? 1 : (k < 9) ? 2 : (k < 11) ? 3 : (k == 11) ? 4 : 5;
-      uint32_t first = bit();
-      uint64_t run;
-      if (first) {
-        k = k + 1 < 12 ? k + 1 : 12;
-        run = ((1ull << e) - 1) << 1;
-      } else {
-        k = k > 0 ? k - 1 : 0;
-        uint32_t v = 0;
-        for (int i = 0; i < e; ++i) v = (v << 1) | bit();
-        run = ((uint64_t)v << 1) | 1;
-      }
-      runs |= run << (num_runs * 7);
-      ++num_runs;
-      if (e == 5 && first == 0 && num_runs >= 8) break;
     }
   }
   __device__ __forceinline__ int get_run() {
-    if (num_runs == 0) more();
-    int r = (int)(runs & 0x7F);
-    runs >>= 7;
-    --num_runs;
-    return r;
+    if (bits < 6) refill();
+    // MEL exponent table {0,0,0,1,1,1,2,2,2,3,3,4,5}, 3 bits per state.
+    constexpr uint64_t kExp = (0ull << 0) | (0ull << 3) | (0ull << 6) | (1ull << 9) | (1ull << 12) | (1ull << 15) |
+                              (2ull << 18) | (2ull << 21) | (2ull << 24) | (3ull << 27) | (3ull << 30) |
+                              (4ull << 33) | (5ull << 36);
+    const int e = (int)((kExp >> (3 * k)) & 7);
+    const bool first = (buf >> 63) != 0;
+    const uint32_t v = e ? (uint32_t)((buf << 1) >> (64 - e)) : 0u;
+    const int used = first ? 1 : 1 + e;
+    k = first ? min(k + 1, 12) : max(k - 1, 0);
+    buf <<= used;
+    bits -= used;
+    return first ? ((1 << e) - 1) << 1 : (int)((v << 1) | 1);
   }
 };
 
@@ -121,18 +112,37 @@ struct Vlc {
     remaining = scup - 2;
     unstuff = (b | 0x0F) > 0x8F;
   }
+  __device__ __forceinline__ void push(uint32_t b) {
+    const uint32_t db = 8 - ((unstuff && (b & 0x7F) == 0x7F) ? 1 : 0);
+    tmp |= (uint64_t)b << bits;
+    bits += db;
+    unstuff = b > 0x8F;
+  }
+  // Appends bytes (walking backwards) until more than 32 bits are buffered;
+  // past the segment the reader supplies zero bytes.  Four bytes at a time
+  // come from one unaligned 32-bit read (two aligned loads inside the
+  // segment), so the byte steps do not wait on one load each.
   __device__ __forceinline__ void fill() {
     while (bits <= 32) {
-      uint32_t b = 0;
-      if (remaining > 0) {
-        b = ld8(data + pos);
-        --pos;
-        --remaining;
+      if (remaining >= 4) {
+        const uintptr_t addr = (uintptr_t)(data + pos - 3);
+        const uint32_t* a = reinterpret_cast<const uint32_t*>(addr & ~(uintptr_t)3);
+        const uint32_t wv = __funnelshift_r(__ldg(a), __ldg(a + 1), (uint32_t)(addr & 3) * 8);
+        pos -= 4;
+        remaining -= 4;
+        push(wv >> 24);
+        push((wv >> 16) & 0xFF);
+        push((wv >> 8) & 0xFF);
+        push(wv & 0xFF);
+      } else {
+        uint32_t b = 0;
+        if (remaining > 0) {
+          b = ld8(data + pos);
+          --pos;
+          --remaining;
+        }
+        push(b);
       }
-      uint32_t db = 8 - ((unstuff && (b & 0x7F) == 0x7F) ? 1 : 0);
-      tmp |= (uint64_t)b << bits;
-      bits += db;
-      unstuff = b > 0x8F;
     }
   }
   __device__ __forceinline__ uint32_t fetch() {
@@ -791,18 +801,30 @@ cudaError_t ht_kernels_init() {
   return cudaFuncSetAttribute(ht_magsgn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
-cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
-                              cudaStream_t stream) {
+cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
+                          cudaStream_t stream) {
   if (njobs == 0) return cudaSuccess;
   ht_vlc_kernel<<<(njobs + kHtThreads - 1) / kHtThreads, kHtThreads, 0, stream>>>(jobs, njobs, arena, symbols);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
+                             int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
+                             cudaStream_t stream) {
+  if (njobs == 0) return cudaSuccess;
   size_t smem = ht_magsgn_smem_bytes(ms_words, max_w);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   ht_magsgn_kernel<<<(njobs + kMsWarps - 1) / kMsWarps, kMsWarps * 32, smem, stream>>>(
       jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w);
   return cudaGetLastError();
+}
+
+cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
+                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
+                              cudaStream_t stream) {
+  cudaError_t e = launch_ht_vlc(jobs, njobs, arena, symbols, stream);
+  if (e != cudaSuccess) return e;
+  return launch_ht_magsgn(jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w, stream);
 }
 
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,

@@ -19,6 +19,11 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w);
 // HT cleanup: the VLC pass (one lane per block) then the MagSgn pass (one
 // warp per block).  ms_words: unstuffed MagSgn capacity per block in 32-bit
 // words; max_w: widest code block of the launch.
+cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
+                          cudaStream_t stream);
+cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
+                             int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
+                             cudaStream_t stream);
 cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                               int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                               cudaStream_t stream);

@@ -54,8 +54,9 @@ class Plan:
         return st, list(per)
 
     def execute_timed(self):
-        """Per-stage milliseconds: HT cleanup, HT refinement, IDWT levels, last level + pack, total."""
-        ms = (ctypes.c_float * 5)()
+        """Per-stage milliseconds: HT VLC pass, HT MagSgn pass, HT refinement, IDWT levels,
+        last level + pack, total."""
+        ms = (ctypes.c_float * 6)()
         _check(_native.cuda_lib().sgn_plan_execute_timed(self.ctx.handle, self.handle, ms))
         return list(ms)
 
