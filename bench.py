@@ -25,7 +25,6 @@ import argparse
 import json
 import os
 import pathlib
-import subprocess
 import sys
 import time
 
@@ -71,45 +70,99 @@ WORKLOAD_CONFIG = {
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and clock-event reasons sampled from NVML (read-only
+    queries) every millisecond during the timed region; each sample is also
+    written to gpurun_out/clocks_<pid>.csv."""
+
+    REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap")]
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
+        self.rows = []
         self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.stop = None
+        self.thread = None
+
+    def _handle(self, nv):
+        import torch
+
+        try:
+            prop = torch.cuda.get_device_properties(self.index)
+            bus = f"{prop.pci_domain_id:08X}:{prop.pci_bus_id:02X}:{prop.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        try:
+            power = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+        except Exception:
+            power = float("nan")
+        active = [name for name, attr in self.REASONS if reasons & getattr(nv, attr, 0)]
+        self.rows.append((time.perf_counter(), sm, mx, power, active))
 
     def __enter__(self):
+        import threading
+
         try:
-            self.path.parent.mkdir(exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index),
-                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._handle(nv)
+            self._sample()
         except Exception:
-            self.proc = None
+            self.nv = None
+            return self
+        self.stop = threading.Event()
+
+        def loop():
+            while not self.stop.is_set():
+                try:
+                    self._sample()
+                except Exception:
+                    pass
+                self.stop.wait(0.001)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            self.proc.wait()
-            self.f.close()
+        if self.thread:
+            self.stop.set()
+            self.thread.join()
+        if self.nv:
+            try:
+                self._sample()
+            except Exception:
+                pass
+            try:
+                self.path.parent.mkdir(exist_ok=True)
+                with open(self.path, "w") as f:
+                    f.write("t_s,sm_mhz,sm_max_mhz,power_w,reasons\n")
+                    for t, sm, mx, pw, act in self.rows:
+                        f.write(f"{t:.6f},{sm},{mx},{pw:.1f},{'|'.join(act)}\n")
+            except Exception:
+                pass
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
-        except Exception:
-            rows = []
-        if not rows:
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows]
-        mx = max(float(r[2]) for r in rows)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip().lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        sm = [r[1] for r in self.rows]
+        reasons = sorted({x for r in self.rows for x in r[4]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[2] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "source": "NVML, 1 ms polling during the timed region"}
 
 
 def cpu_baseline(tiles, fmt, budget_s=20.0):
