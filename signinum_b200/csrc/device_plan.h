@@ -15,8 +15,8 @@
 namespace sgn {
 
 // Work unit of the IDWT kernels: one warp decodes a strip of kIdwtStripW
-// columns (two per lane) over `seg` rows of one level (even, chosen per job).
-constexpr int kIdwtStripW = 64;
+// columns (four per lane) over `seg` rows of one level (even, chosen per job).
+constexpr int kIdwtStripW = 128;
 
 // Rows per work unit: long segments for big levels (less halo re-reading),
 // short ones for small levels (more warps in flight).

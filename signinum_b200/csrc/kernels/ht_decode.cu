@@ -369,29 +369,72 @@ constexpr int kMsWarps = 8;  // warps (code blocks in flight) per CTA of the Mag
 // ForwardBitReader accumulates it (ht_block_decode.rs:888-930).  Bits past
 // the end read as ones (the reader pads with 0xFF).  Returns the number of
 // real bits.
+//
+// The warp takes 128 bytes per step, four per lane.  A step with no 0xFF
+// byte (and none just before it) is a plain bit shift of the input: each
+// lane stores one whole output word built from its word and its right
+// neighbour's.  Other steps place every byte at its own offset.
 __device__ uint32_t unstuff_magsgn(const uint8_t* src, uint32_t len, uint32_t* W, uint32_t nwords) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t i = lane; i < nwords; i += 32) W[i] = 0;
   __syncwarp();
-  uint32_t carry = 0, last_ff = 0, end_bits = 0;
-  for (uint32_t base = 0; base < len; base += 32) {
-    const uint32_t i = base + lane;
-    const bool valid = i < len;
-    const uint32_t b = valid ? (uint32_t)ld8(src + i) : 0;
-    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, valid && b == 0xFF);
-    // FF bytes among [0, i - 1): they shorten byte i's predecessors.
-    uint32_t ff_before = lane == 0 ? carry - last_ff : carry + __popc(mask & ((1u << (lane - 1)) - 1));
-    const uint32_t off = 8 * i - ff_before;
-    if (valid) {
-      atomicOr(&W[off >> 5], b << (off & 31));
-      if ((off & 31) > 24) atomicOr(&W[(off >> 5) + 1], b >> (32 - (off & 31)));
+  uint32_t ff_total = 0;  // 0xFF bytes among bytes [0, base)
+  uint32_t prev_ff = 0;   // byte base - 1 is 0xFF
+  for (uint32_t base = 0; base < len; base += 128) {
+    const uint32_t i0 = base + 4 * lane;
+    // Bytes i0 .. i0+3 (zero past len), little-endian.  Both aligned words
+    // hold a byte of the segment, so they lie inside its allocation.
+    uint32_t x = 0;
+    if (i0 < len) {
+      const uintptr_t addr = (uintptr_t)(src + i0);
+      const uint32_t* wp = reinterpret_cast<const uint32_t*>(addr & ~(uintptr_t)3);
+      const uint32_t sh = (uint32_t)(addr & 3);
+      const uint32_t nvalid = min(4u, len - i0);
+      const uint32_t lo = __ldg(wp);
+      const uint32_t hi = sh + nvalid > 4 ? __ldg(wp + 1) : 0u;
+      x = __funnelshift_r(lo, hi, 8 * sh);
+      if (nvalid < 4) x &= 0xFFFFFFFFu >> (8 * (4 - nvalid));
     }
-    const uint32_t nvalid = min(32u, len - base);
-    carry += __popc(mask);
-    last_ff = (mask >> (nvalid - 1)) & 1;
+    const uint32_t fm = i0 < len ? __vcmpeq4(x, 0xFFFFFFFFu) : 0u;  // 0xFF per 0xFF byte
+    // Padding bytes beyond len are zero, never 0xFF.
+    const bool full = base + 128 <= len;
+    if (full && !prev_ff && !__any_sync(0xFFFFFFFFu, fm != 0)) {
+      // Stream bit of byte base: 8 * base minus one per 0xFF before it.
+      const uint32_t P = 8 * base - ff_total;
+      const uint32_t s = P & 31, wb = P >> 5;
+      const uint32_t xn = __shfl_down_sync(0xFFFFFFFFu, x, 1);
+      if (lane < 31) W[wb + lane + 1] = __funnelshift_l(x, xn, s);
+      if (lane == 0) atomicOr(&W[wb], x << s);
+      if (lane == 31 && s) atomicOr(&W[wb + 32], x >> (32 - s));
+      continue;
+    }
+    const uint32_t f0 = fm & 1, f1 = (fm >> 8) & 1, f2 = (fm >> 16) & 1, f3 = (fm >> 24) & 1;
+    const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, f0), b1 = __ballot_sync(0xFFFFFFFFu, f1);
+    const uint32_t b2 = __ballot_sync(0xFFFFFFFFu, f2), b3 = __ballot_sync(0xFFFFFFFFu, f3);
+    const uint32_t lt = (1u << lane) - 1;
+    // 0xFF bytes among [0, i0) and whether byte i0 - 1 is one.
+    const uint32_t F = ff_total + __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+    uint32_t pf = __shfl_up_sync(0xFFFFFFFFu, f3, 1);
+    if (lane == 0) pf = prev_ff;
+    // Byte i0 + j is shortened by the 0xFF bytes among [0, i0 + j - 1).
+    const uint32_t ffb[4] = {F - pf, F, F + f0, F + f0 + f1};
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      if (i0 + j < len) {
+        const uint32_t pos = 8 * (i0 + j) - ffb[j];
+        const uint32_t byte = (x >> (8 * j)) & 0xFF;
+        atomicOr(&W[pos >> 5], byte << (pos & 31));
+        if ((pos & 31) > 24) atomicOr(&W[(pos >> 5) + 1], byte >> (32 - (pos & 31)));
+      }
+    }
+    ff_total += __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+    const uint32_t last = min(base + 128, len) - 1 - base;  // last byte of the step
+    const uint32_t lb = last >> 2, lj = last & 3;
+    const uint32_t lf = lj == 0 ? b0 : lj == 1 ? b1 : lj == 2 ? b2 : b3;
+    prev_ff = (lf >> lb) & 1;
   }
   // Real bits: 8 per byte minus one per byte that follows a 0xFF.
-  end_bits = len ? 8 * len - (carry - last_ff) : 0;
+  const uint32_t end_bits = len ? 8 * len - (ff_total - prev_ff) : 0;
   __syncwarp();
   // Padding: every bit from end_bits on is one.
   for (uint32_t wi = lane; wi < nwords; wi += 32) {
@@ -488,30 +531,33 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
       const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 31);
       uint32_t off = rowbase + inc - tot;
       rowbase += chunk_bits;
-      // This quad's bits: one 64-bit window when they fit, else per sample.
-      const bool window = tot < 64;
-      uint64_t win = 0;
-      if (window && (inf & 0xF0)) win = (uint64_t)bits_at(W, ms_words, off) | ((uint64_t)bits_at(W, ms_words, off + 32) << 32);
+      // Sample i's bits start at off + c_i, c_i = m_0 + .. + m_{i-1}.  When the
+      // quad holds fewer than 64 bits one 64-bit window read serves all four
+      // samples (independent funnel shifts); otherwise each sample reads its
+      // own 32 bits.
+      const uint32_t cs[4] = {0u, m[0], m[0] + m[1], m[0] + m[1] + m[2]};
+      uint32_t lo = 0, hi = 0;
+      if (inf & 0xF0) {
+        lo = bits_at(W, ms_words, off);
+        hi = bits_at(W, ms_words, off + 32);
+      }
+      uint32_t msv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) msv[i] = cs[i] < 32 ? __funnelshift_r(lo, hi, cs[i]) : hi >> (cs[i] - 32);
+      if (tot >= 64) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) msv[i] = bits_at(W, ms_words, off + cs[i]);
+      }
       uint32_t val[4], E[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        val[i] = 0;
-        E[i] = 0;
-        if ((inf >> (4 + i)) & 1) {
-          const uint32_t mn = m[i];
-          uint32_t msv;
-          if (window) {
-            msv = (uint32_t)win;
-            win >>= mn;
-          } else {
-            msv = bits_at(W, ms_words, off);
-            off += mn;
-          }
-          uint32_t mask = mn == 0 ? 0 : (mn >= 32 ? 0xFFFFFFFFu : ((1u << mn) - 1));
-          uint32_t v = (msv & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
-          val[i] = (msv << 31) | ((v + 2) << (p - 1));
-          E[i] = 32 - __clz(v);
-        }
+        const bool sig = (inf >> (4 + i)) & 1;
+        const uint32_t mn = m[i];
+        // (1 << mn) - 1, saturating at 32 bits.
+        const uint32_t mask = __funnelshift_lc(0xFFFFFFFFu, 0u, mn);
+        const uint32_t v = (msv[i] & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
+        val[i] = sig ? (msv[i] << 31) | ((v + 2) << (p - 1)) : 0u;
+        E[i] = sig ? 32 - __clz(v) : 0u;
       }
       if (active) {
         const uint32_t x = 2 * q;

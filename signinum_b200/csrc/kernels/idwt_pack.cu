@@ -9,23 +9,24 @@
 // (:908-925).  All values are integers, so int32 with arithmetic shifts gives
 // the reference's f32 floors bit for bit.
 //
-// Mapping: one warp per unit = a strip of 64 columns x `seg` rows of a level.
-// Lane k owns image columns (2k, 2k+1) of the strip, i.e. band column k of
-// the low and high bands, so every band load and every row store is
-// coalesced.  Horizontal lifting of a row needs the odd neighbour on the left
-// and the updated even neighbour on the right: both come from warp shuffles
-// (the strip's edge lanes load the one extra band sample they need).  The
-// vertical pass streams down the rows keeping the previous odd row and the
-// previous updated even row in registers.  Symmetric extension is done by
-// reflecting row/column indices (it commutes with the lifting steps), so the
-// edges need no special arithmetic.  No shared memory, no barriers.
+// Mapping: one warp per unit = a strip of 128 columns x `seg` rows of a level.
+// Lane k owns image columns 4k .. 4k+3 of the strip, i.e. band columns 2k and
+// 2k+1 of the low and high bands, read as 8-byte pairs, so every band load
+// and every row store is coalesced.  Horizontal lifting of a row needs the
+// odd neighbour on the left and the updated even neighbour on the right: both
+// come from warp shuffles (the strip's edge lanes load the extra band samples
+// they need).  The vertical pass streams down the rows keeping the previous
+// odd row and the previous updated even row in registers.  Symmetric
+// extension is done by reflecting row/column indices (it commutes with the
+// lifting steps), so the edges need no special arithmetic.  No barriers.
 //
 // The last level keeps the streams of all components of a pixel in the same
 // lane and finishes the pixels there: inverse RCT (mct.rs:117-150),
 // +2^(bd-1) (decode.rs:1720-1729, :1748-1752) and the conversion to the
 // requested pixel format (crates/signinum-j2k-native/src/lib.rs:1772-1840,
-// :2202-2294; crates/signinum-j2k/src/decode.rs:345-356, :517-545); packed
-// rows are staged per warp in shared memory and written with 16-byte stores.
+// :2202-2294; crates/signinum-j2k/src/decode.rs:345-356, :517-545); each lane
+// packs its four pixels into 32-bit words, the words of a row are staged per
+// warp in shared memory and the row is written with 16-byte stores.
 #include <cstdint>
 
 #include "../device_plan.h"
@@ -35,6 +36,7 @@ namespace sgn {
 namespace {
 
 constexpr int kLanes = 32;
+static_assert(kIdwtStripW == 4 * kLanes, "one strip is four columns per lane");
 
 // Periodic symmetric extension of index i into [0, n) (reflections about the
 // first and last samples; the streams overshoot by at most a few samples).
@@ -52,16 +54,23 @@ struct Bands {
   const int32_t* lh;
   const int32_t* hh;
   int w, h;
+  bool vec;  // w % 4 == 0 and 8-byte aligned bases: every band row starts 8-byte aligned
 };
 
-// Band samples of one interleaved row at this lane's columns (col, col + 1),
-// col = 2b, plus the extra samples the strip's edge lanes need.  Loads only:
-// the lifting happens in lift_row, so a caller can keep the next rows' loads
-// in flight while it lifts the current ones.
+__device__ __forceinline__ Bands make_bands(const int32_t* ll, const int32_t* hl, const int32_t* lh,
+                                            const int32_t* hh, int w, int h) {
+  const uintptr_t a = (uintptr_t)ll | (uintptr_t)hl | (uintptr_t)lh | (uintptr_t)hh;
+  return Bands{ll, hl, lh, hh, w, h, (w & 3) == 0 && (a & 7) == 0};
+}
+
+// Band samples of one interleaved row at this lane's band columns b, b + 1
+// (image columns 2b .. 2b+3), plus the extra samples the strip's edge lanes
+// need.  Loads only: lifting happens in lift_row, so a caller can keep the
+// next rows' loads in flight while it lifts the current ones.
 struct RawRow {
-  int lo, hi;     // low band (column col), high band (column col + 1)
-  int hi_left;    // lane 0: high band at column col - 1
-  int lo_r, hi_r; // lane 31: low / high band at columns col + 2, col + 3
+  int lo0, lo1, hi0, hi1;  // low / high band at columns b, b + 1
+  int x1;                  // lane 0: high band at column b - 1; lane 31: low band at column b + 2
+  int x2;                  // lane 31: high band at column b + 2
 };
 
 __device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lane) {
@@ -70,91 +79,108 @@ __device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lan
   const int lw = (B.w + 1) >> 1, hw = B.w >> 1;
   const int32_t* Lr = ((y & 1) ? B.lh : B.ll) + (size_t)r * lw;
   const int32_t* Hr = ((y & 1) ? B.hh : B.hl) + (size_t)r * hw;
-  const int col = 2 * b;
   RawRow R;
-  R.lo = col < B.w ? __ldg(Lr + b) : 0;
-  R.hi = col + 1 < B.w ? __ldg(Hr + b) : 0;
-  R.hi_left = (lane == 0 && b > 0) ? __ldg(Hr + b - 1) : 0;
-  R.lo_r = (lane == kLanes - 1 && col + 2 < B.w) ? __ldg(Lr + b + 1) : 0;
-  R.hi_r = (lane == kLanes - 1 && col + 3 < B.w) ? __ldg(Hr + b + 1) : 0;
+  if (B.vec && b + 1 < hw) {
+    // b is even and both band widths are even: one 8-byte load per band.
+    const int2 l = __ldg(reinterpret_cast<const int2*>(Lr + b));
+    const int2 h = __ldg(reinterpret_cast<const int2*>(Hr + b));
+    R.lo0 = l.x;
+    R.lo1 = l.y;
+    R.hi0 = h.x;
+    R.hi1 = h.y;
+  } else {
+    R.lo0 = b < lw ? __ldg(Lr + b) : 0;
+    R.lo1 = b + 1 < lw ? __ldg(Lr + b + 1) : 0;
+    R.hi0 = b < hw ? __ldg(Hr + b) : 0;
+    R.hi1 = b + 1 < hw ? __ldg(Hr + b + 1) : 0;
+  }
+  R.x1 = (lane == 0 && b > 0) ? __ldg(Hr + b - 1) : (lane == kLanes - 1 && b + 2 < lw) ? __ldg(Lr + b + 2) : 0;
+  R.x2 = (lane == kLanes - 1 && b + 2 < hw) ? __ldg(Hr + b + 2) : 0;
   return R;
 }
 
-// Horizontal lifting of a loaded row: (even, odd) samples of this lane.
-// Lanes past the right edge return garbage.
-__device__ __forceinline__ int2 lift_row(const RawRow& R, int w, int b, int lane) {
-  if (w == 1) return make_int2(R.lo, 0);
-  const int col = 2 * b;
-  int hi = R.hi;
-  int hiL = __shfl_up_sync(0xFFFFFFFFu, hi, 1);
-  if (lane == 0) hiL = b == 0 ? hi : R.hi_left;  // column -1 mirrors column 1
-  if (col + 1 >= w) hi = hiL;                     // column w mirrors column w - 2
-  const int E = R.lo - ((hiL + hi + 2) >> 2);
-  int ER = __shfl_down_sync(0xFFFFFFFFu, E, 1);
-  if (lane == kLanes - 1 && col + 2 < w) {
-    const int hi2 = col + 3 < w ? R.hi_r : hi;
-    ER = R.lo_r - ((hi + hi2 + 2) >> 2);
+// Horizontal lifting of a loaded row: samples of image columns 2b .. 2b+3
+// (x: 2b, y: 2b+1, z: 2b+2, w: 2b+3).  Columns past the right edge return
+// garbage.  X[-1] mirrors X[1] and X[w] mirrors X[w-2].
+__device__ __forceinline__ int4 lift_row(const RawRow& R, int w, int b, int lane) {
+  if (w == 1) return make_int4(R.lo0, 0, 0, 0);
+  const int c = 2 * b;
+  int hm1 = __shfl_up_sync(0xFFFFFFFFu, R.hi1, 1);  // X[c-1]
+  if (lane == 0) hm1 = b == 0 ? R.hi0 : R.x1;
+  const int h0 = c + 1 < w ? R.hi0 : hm1;              // X[c+1]
+  const int h1 = c + 3 < w ? R.hi1 : h0;               // X[c+3]
+  const int e0 = R.lo0 - ((hm1 + h0 + 2) >> 2);        // X[c]
+  int e1 = R.lo1 - ((h0 + h1 + 2) >> 2);               // X[c+2]
+  int e2 = __shfl_down_sync(0xFFFFFFFFu, e0, 1);       // X[c+4]
+  if (lane == kLanes - 1 && c + 4 < w) {
+    const int h2 = c + 5 < w ? R.x2 : h1;
+    e2 = R.x1 - ((h1 + h2 + 2) >> 2);
   }
-  if (col + 2 >= w) ER = E;  // column w mirrors column w - 2
-  return make_int2(E, hi + ((E + ER) >> 1));
+  if (c + 2 >= w) e1 = e0;  // column w mirrors column w - 2
+  if (c + 4 >= w) e2 = e1;
+  return make_int4(e0, h0 + ((e0 + e1) >> 1), e1, h1 + ((e1 + e2) >> 1));
 }
 
-__device__ __forceinline__ int2 hrow(const Bands& B, int y, int b, int lane) {
+__device__ __forceinline__ int4 hrow(const Bands& B, int y, int b, int lane) {
   return lift_row(load_row(B, y, b, lane), B.w, b, lane);
 }
 
-// Vertical 5/3 stream over output rows [ys, ye) (ys even) of NC level
-// images at once; emit(y, v[NC]) receives each finished row.  With PREFETCH
-// the loads of row pair m + 1 are issued before row pair m is lifted (more
-// registers; used where a warp streams one component).
+__device__ __forceinline__ int4 vupdate(int4 xe, int4 a, int4 c) {
+  return make_int4(xe.x - ((a.x + c.x + 2) >> 2), xe.y - ((a.y + c.y + 2) >> 2), xe.z - ((a.z + c.z + 2) >> 2),
+                   xe.w - ((a.w + c.w + 2) >> 2));
+}
+__device__ __forceinline__ int4 vpredict(int4 xo, int4 a, int4 c) {
+  return make_int4(xo.x + ((a.x + c.x) >> 1), xo.y + ((a.y + c.y) >> 1), xo.z + ((a.z + c.z) >> 1),
+                   xo.w + ((a.w + c.w) >> 1));
+}
+
+// Vertical 5/3 stream over output rows [ys, ye) (ys even) of NC level images
+// at once; emit(y, v[NC]) receives each finished row (four columns per lane).
+// With PREFETCH the loads of row pair m + 1 are issued before row pair m is
+// lifted (more registers; used where a warp streams one component).
 template <int NC, bool PREFETCH, typename Emit>
 __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int ys, int ye, Emit emit) {
   const int h = B[0].h, w = B[0].w;
-  int2 v[NC];
+  int4 v[NC];
   if (h == 1) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) v[c] = hrow(B[c], 0, b, lane);
     emit(0, v);
     return;
   }
-  int2 xo_prev[NC], ev_prev[NC];
+  int4 xo_prev[NC], ev_prev[NC];
   RawRow re[NC], ro[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     re[c] = load_row(B[c], ys, b, lane);
     ro[c] = load_row(B[c], ys + 1, b, lane);
     xo_prev[c] = hrow(B[c], ys - 1, b, lane);
-    ev_prev[c] = make_int2(0, 0);
+    ev_prev[c] = make_int4(0, 0, 0, 0);
   }
   for (int m = ys >> 1;; ++m) {
     const int ye_row = 2 * m, yo_row = 2 * m + 1;
     const bool more = yo_row < ye;
-    if (!PREFETCH && m != (ys >> 1)) {
+    const bool first = m == (ys >> 1);
+    RawRow ne[NC], no[NC];
+    int4 ev[NC], xo[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
+    for (int c = 0; c < NC; ++c) {
+      // Without PREFETCH one component's rows are loaded at a time.
+      if (!PREFETCH && !first) {
         re[c] = load_row(B[c], ye_row, b, lane);
         ro[c] = load_row(B[c], yo_row, b, lane);
       }
-    }
-    RawRow ne[NC], no[NC];
-    int2 ev[NC], xo[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
       if (PREFETCH && more) {
         ne[c] = load_row(B[c], ye_row + 2, b, lane);
         no[c] = load_row(B[c], yo_row + 2, b, lane);
       }
-      const int2 xe = lift_row(re[c], w, b, lane);
+      const int4 xe = lift_row(re[c], w, b, lane);
       xo[c] = lift_row(ro[c], w, b, lane);
-      ev[c].x = xe.x - ((xo_prev[c].x + xo[c].x + 2) >> 2);
-      ev[c].y = xe.y - ((xo_prev[c].y + xo[c].y + 2) >> 2);
+      ev[c] = vupdate(xe, xo_prev[c], xo[c]);
     }
     if (ye_row - 1 >= ys && ye_row - 1 < ye) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        v[c].x = xo_prev[c].x + ((ev_prev[c].x + ev[c].x) >> 1);
-        v[c].y = xo_prev[c].y + ((ev_prev[c].y + ev[c].y) >> 1);
-      }
+      for (int c = 0; c < NC; ++c) v[c] = vpredict(xo_prev[c], ev_prev[c], ev[c]);
       emit(ye_row - 1, v);
     }
     if (ye_row < ye) emit(ye_row, ev);
@@ -195,22 +221,34 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJ
   const int ys = (int)(local / job.strips) * (int)job.seg;
   const int w = (int)job.w, h = (int)job.h;
   const int ye = min(ys + (int)job.seg, h);
-  Bands B{job.ll, job.hl, job.lh, job.hh, w, h};
-  const int b = (x0 >> 1) + lane, col = 2 * b;
+  const Bands B = make_bands(job.ll, job.hl, job.lh, job.hh, w, h);
+  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
   int32_t* out = job.out;
-  stream_rows<1, true>(&B, b, lane, ys, ye, [&](int y, const int2* v) {
+  // Rows of w int32 from a 16-byte aligned base: 16-byte stores when w % 4 == 0.
+  const bool vec_out = (w & 3) == 0 && (((uintptr_t)out) & 15) == 0;
+  stream_rows<1, true>(&B, b, lane, ys, ye, [&](int y, const int4* v) {
     int32_t* row = out + (size_t)y * w;
-    if (col < w) row[col] = v[0].x;
-    if (col + 1 < w) row[col + 1] = v[0].y;
+    if (vec_out && col + 3 < w) {
+      *reinterpret_cast<int4*>(row + col) = v[0];
+    } else {
+      if (col < w) row[col] = v[0].x;
+      if (col + 1 < w) row[col + 1] = v[0].y;
+      if (col + 2 < w) row[col + 2] = v[0].z;
+      if (col + 3 < w) row[col + 3] = v[0].w;
+    }
   });
 }
 
 namespace {
 
-__device__ __forceinline__ uint8_t sat_u8f(float r) { return (uint8_t)fminf(fmaxf(r, 0.0f), 255.0f); }
+__device__ __forceinline__ uint32_t sat_u8f(float r) { return (uint32_t)fminf(fmaxf(r, 0.0f), 255.0f); }
 
-__device__ __forceinline__ uint8_t to_u8(int32_t v, uint32_t bd, uint32_t region) {
-  if (bd == 8) return (uint8_t)min(max(v, 0), 255);
+// DIRECT: the sample needs only a clamp (8-bit samples to u8, or samples of
+// more than 8 bits to u16); chosen per unit so the hot loop holds no float or
+// division path.
+template <bool DIRECT>
+__device__ __forceinline__ uint32_t to_u8(int32_t v, uint32_t bd, uint32_t region) {
+  if (DIRECT || bd == 8) return (uint32_t)min(max(v, 0), 255);
   if (region) {
     // sample_as_u8: round, clamp to the depth's maximum, rescale to 8 bits.
     float maxv = bd >= 16 ? 65535.0f : (float)max((1 << bd) - 1, 1);
@@ -222,51 +260,15 @@ __device__ __forceinline__ uint8_t to_u8(int32_t v, uint32_t bd, uint32_t region
   return sat_u8f(roundf(__fmul_rn(__fdiv_rn((float)v, d), 255.0f)));
 }
 
-__device__ __forceinline__ uint16_t to_u16(int32_t v, uint32_t bd) {
+template <bool DIRECT>
+__device__ __forceinline__ uint32_t to_u16(int32_t v, uint32_t bd) {
   int32_t maxv = (int32_t)((1u << bd) - 1);
   int32_t c = min(max(v, 0), maxv);
-  if (bd <= 8) {
+  if (!DIRECT && bd <= 8) {
     uint32_t mx = max((1u << bd) - 1, 1u);
-    return (uint16_t)(((uint32_t)c * 65535u + mx / 2) / mx);
+    return ((uint32_t)c * 65535u + mx / 2) / mx;
   }
-  return (uint16_t)c;
-}
-
-constexpr int kRowBytes = kIdwtStripW * 8 + 16;
-
-// Packs one pixel (components v0..v2 after the inverse RCT) into o.
-template <int FMT>
-__device__ __forceinline__ void put_pixel(uint8_t* o, int32_t v0, int32_t v1, int32_t v2, uint32_t bd, uint32_t reg) {
-  switch (FMT) {
-    case PACK_GRAY8: o[0] = to_u8(v0, bd, reg); break;
-    case PACK_RGB8:
-      o[0] = to_u8(v0, bd, reg);
-      o[1] = to_u8(v1, bd, reg);
-      o[2] = to_u8(v2, bd, reg);
-      break;
-    case PACK_RGBA8:
-      o[0] = to_u8(v0, bd, reg);
-      o[1] = to_u8(v1, bd, reg);
-      o[2] = to_u8(v2, bd, reg);
-      o[3] = 255;
-      break;
-    case PACK_GRAY16: {
-      uint16_t a = to_u16(v0, bd);
-      o[0] = (uint8_t)a;
-      o[1] = (uint8_t)(a >> 8);
-      break;
-    }
-    default: {
-      uint16_t a = to_u16(v0, bd), g = to_u16(v1, bd), c = to_u16(v2, bd);
-      o[0] = (uint8_t)a;
-      o[1] = (uint8_t)(a >> 8);
-      o[2] = (uint8_t)g;
-      o[3] = (uint8_t)(g >> 8);
-      o[4] = (uint8_t)c;
-      o[5] = (uint8_t)(c >> 8);
-      break;
-    }
-  }
+  return (uint32_t)c;
 }
 
 template <int FMT>
@@ -274,46 +276,95 @@ __host__ __device__ constexpr int pack_bpp() {
   return FMT == PACK_GRAY8 ? 1 : FMT == PACK_RGB8 ? 3 : FMT == PACK_RGBA8 ? 4 : FMT == PACK_GRAY16 ? 2 : 6;
 }
 
-template <int NC, int FMT>
-__device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint8_t* rowbuf) {
+// Byte q (a compile-time constant after unrolling) of a lane's packed words.
+__device__ __forceinline__ void put_byte(uint32_t* wds, int q, uint32_t byte) { wds[q >> 2] |= byte << (8 * (q & 3)); }
+
+// Packs pixel p (components c0..c2 after the inverse RCT and DC shift) at
+// byte p * bpp of the lane's four-pixel group.
+template <int FMT, bool DIRECT>
+__device__ __forceinline__ void put_pixel(uint32_t* wds, int p, int32_t c0, int32_t c1, int32_t c2, uint32_t bd,
+                                          uint32_t reg) {
+  constexpr int B = pack_bpp<FMT>();
+  const int q = p * B;
+  if (FMT == PACK_GRAY8) {
+    put_byte(wds, q, to_u8<DIRECT>(c0, bd, reg));
+  } else if (FMT == PACK_RGB8 || FMT == PACK_RGBA8) {
+    put_byte(wds, q, to_u8<DIRECT>(c0, bd, reg));
+    put_byte(wds, q + 1, to_u8<DIRECT>(c1, bd, reg));
+    put_byte(wds, q + 2, to_u8<DIRECT>(c2, bd, reg));
+    if (FMT == PACK_RGBA8) put_byte(wds, q + 3, 255u);
+  } else if (FMT == PACK_GRAY16) {
+    const uint32_t a = to_u16<DIRECT>(c0, bd);
+    put_byte(wds, q, a & 0xFF);
+    put_byte(wds, q + 1, a >> 8);
+  } else {
+    const uint32_t a = to_u16<DIRECT>(c0, bd), g = to_u16<DIRECT>(c1, bd), c = to_u16<DIRECT>(c2, bd);
+    put_byte(wds, q, a & 0xFF);
+    put_byte(wds, q + 1, a >> 8);
+    put_byte(wds, q + 2, g & 0xFF);
+    put_byte(wds, q + 3, g >> 8);
+    put_byte(wds, q + 4, c & 0xFF);
+    put_byte(wds, q + 5, c >> 8);
+  }
+}
+
+__device__ __forceinline__ int lane_comp(const int4& v, int p) { return p == 0 ? v.x : p == 1 ? v.y : p == 2 ? v.z : v.w; }
+
+// Row buffer per warp: up to 15 bytes of alignment shift + 128 pixels x 6 bytes.
+constexpr int kRowWords = (16 + kIdwtStripW * 6) / 4;
+
+template <int NC, int FMT, bool DIRECT>
+__device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf) {
+  constexpr int BPP = pack_bpp<FMT>();
   const int w = (int)job.w;
-  const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw;
+  const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
   const uint32_t bd = job.bit_depth, reg = job.region_conv;
-  constexpr int bpp = pack_bpp<FMT>();
   const int32_t shift = 1 << (bd - 1);
   const bool mct = NC == 3 && job.mct;
-  const int b = (x0 >> 1) + lane, col = 2 * b;
+  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
   const int xs = max(x0, cx0), xe = min(x0 + kIdwtStripW, cx1);
-  const int nbytes = (xe - xs) * bpp;
-  auto emit = [&](int y, const int2* v) {
-    if (y < cy0 || y >= cy0 + (int)job.ch) return;  // warp-uniform
-    const uint64_t gbase = (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * bpp;
-    const int off = (int)(gbase & 15);
+  const int nbytes = (xe - xs) * BPP;
+  uint8_t* rowbytes = reinterpret_cast<uint8_t*>(rowbuf);
+  auto emit = [&](int y, const int4* v) {
+    if (y < cy0 || y >= cy1) return;  // warp-uniform
+    uint8_t* g = job.out + (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * BPP;
+    // Stage so that the copied range has the destination's alignment mod 16.
+    const int sh = (int)(((uintptr_t)g - (uintptr_t)((xs - x0) * BPP)) & 15);
+    uint32_t wds[BPP];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int px = col + k;
-      if (px < xs || px >= xe) continue;
-      int32_t c0 = k ? v[0].y : v[0].x, c1 = 0, c2 = 0;
+    for (int k = 0; k < BPP; ++k) wds[k] = 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      int32_t c0 = lane_comp(v[0], p), c1 = 0, c2 = 0;
       if (NC == 3) {
-        c1 = k ? v[1].y : v[1].x;
-        c2 = k ? v[2].y : v[2].x;
+        c1 = lane_comp(v[1], p);
+        c2 = lane_comp(v[2], p);
         if (mct) {
-          const int32_t g = c0 - ((c2 + c1) >> 2);
-          const int32_t r = c2 + g, bl = c1 + g;
+          const int32_t gg = c0 - ((c2 + c1) >> 2);
+          const int32_t r = c2 + gg, bl = c1 + gg;
           c0 = r;
-          c1 = g;
+          c1 = gg;
           c2 = bl;
         }
         c1 += shift;
         c2 += shift;
       }
       c0 += shift;
-      put_pixel<FMT>(rowbuf + off + (px - xs) * bpp, c0, c1, c2, bd, reg);
+      put_pixel<FMT, DIRECT>(wds, p, c0, c1, c2, bd, reg);
+    }
+    if ((sh & 3) == 0) {
+      uint32_t* dst = rowbuf + (sh >> 2) + lane * BPP;
+#pragma unroll
+      for (int k = 0; k < BPP; ++k) dst[k] = wds[k];
+    } else {
+      uint8_t* dst = rowbytes + sh + lane * 4 * BPP;
+#pragma unroll
+      for (int q = 0; q < 4 * BPP; ++q) dst[q] = (uint8_t)(wds[q >> 2] >> (8 * (q & 3)));
     }
     __syncwarp();
-    // Copy-out: bytes up to the first 16-byte boundary, 16-byte vectors, tail.
-    uint8_t* g = job.out + gbase;
-    const uint8_t* src = rowbuf + off;
+    // Copy-out of columns [xs, xe): bytes up to the first 16-byte boundary,
+    // 16-byte vectors, tail.
+    const uint8_t* src = rowbytes + sh + (xs - x0) * BPP;
     int head = (int)((16 - ((uintptr_t)g & 15)) & 15);
     if (head > nbytes) head = nbytes;
     if (lane < head) g[lane] = src[lane];
@@ -328,17 +379,19 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
   if (job.lifting) {
     Bands B[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) B[c] = Bands{job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, (int)job.h};
+    for (int c = 0; c < NC; ++c) B[c] = make_bands(job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, (int)job.h);
     stream_rows<NC, NC == 1>(B, b, lane, ys, ye, emit);
   } else {
     // Nothing left to lift: the image is the LL band itself.
     for (int y = ys; y < ye; ++y) {
-      int2 v[NC];
+      int4 v[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const int32_t* row = job.ll[c] + (size_t)y * w;
         v[c].x = col < w ? __ldg(row + col) : 0;
         v[c].y = col + 1 < w ? __ldg(row + col + 1) : 0;
+        v[c].z = col + 2 < w ? __ldg(row + col + 2) : 0;
+        v[c].w = col + 3 < w ? __ldg(row + col + 3) : 0;
       }
       emit(y, v);
     }
@@ -348,9 +401,9 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
 }  // namespace
 
 template <int FMT>
-__global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kIdwtWarps * 32, 2) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
                                                                uint32_t nunits) {
-  __shared__ __align__(16) uint8_t rowbufs[kIdwtWarps][kRowBytes];
+  __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
   const uint32_t warp = threadIdx.x >> 5;
   const uint32_t unit = blockIdx.x * kIdwtWarps + warp;
   if (unit >= nunits) return;
@@ -360,8 +413,15 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) pack_kernel(const PackJob* __
   const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
   const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
   const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
-  if (job.ncomp >= 3) pack_unit<3, FMT>(job, x0, ys, ye, lane, rowbufs[warp]);
-  else pack_unit<1, FMT>(job, x0, ys, ye, lane, rowbufs[warp]);
+  constexpr bool kU8 = FMT == PACK_GRAY8 || FMT == PACK_RGB8 || FMT == PACK_RGBA8;
+  const bool direct = kU8 ? job.bit_depth == 8 : job.bit_depth > 8;
+  if (job.ncomp >= 3) {
+    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbufs[warp]);
+    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbufs[warp]);
+  } else {
+    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbufs[warp]);
+    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbufs[warp]);
+  }
 }
 
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
