@@ -221,6 +221,61 @@ sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, 
                                         int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
                                         void* stream);
 
+/* ---- Serving loop: continuous batching of tile requests (sgn_server_submit /
+ * sgn_server_poll stand beside the drop-in calls; the reference has no
+ * serving loop, its adapter decodes one call at a time).
+ *
+ * Codestreams are registered once and stay resident in device memory.
+ * Requests (full, region, reduced resolution, region at reduced resolution,
+ * any pixel format the plain call accepts) are queued as they arrive; a
+ * dispatcher thread forms a batch from the queue whenever one of `slots`
+ * CUDA streams is free and the batch's estimated device memory fits in
+ * `device_budget_bytes` beside the batches already on the GPU, so requests
+ * that arrive while others decode are admitted as slots and memory free up
+ * and their work overlaps on the device.  A completion thread publishes each
+ * request's surface, status and latency (submit to publication, host clock)
+ * as its batch finishes. */
+typedef struct sgn_server sgn_server;
+
+typedef struct sgn_server_config {
+  uint64_t device_budget_bytes;     /* admission budget for in-flight batches (0: 16 GiB) */
+  uint64_t resident_capacity_bytes; /* device arena for registered codestreams (0: 1 GiB) */
+  uint32_t max_batch_tiles;         /* requests per batch (0: 512) */
+  uint32_t slots;                   /* batches in flight at once, one CUDA stream each (0: 3) */
+} sgn_server_config;
+
+typedef struct sgn_server_result {
+  uint64_t ticket;
+  sgn_status status;       /* per request, as sgn_j2k_decode_to_device reports it */
+  uint32_t batch_tiles;    /* requests in the batch that carried this one */
+  sgn_surface surface;     /* owned by the caller when status is SGN_OK: sgn_server_surface_free */
+  double latency_ms;       /* submit -> result published */
+  double queue_ms;         /* submit -> batch launched */
+} sgn_server_result;
+
+typedef struct sgn_server_stats {
+  uint64_t submitted, completed, batches, rejected;
+  uint64_t bytes_in_use, peak_bytes_in_use;
+  uint32_t max_batch_seen, max_inflight_seen;
+} sgn_server_stats;
+
+sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_server** out);
+/* Copies a codestream into the resident arena; *tile_id names it in requests. */
+sgn_status sgn_server_register(sgn_server* server, const uint8_t* data, size_t len, uint32_t* tile_id);
+/* Queues a request (request NULL = full image); validation that needs no
+ * parse (format, request kind, region bounds, budget) fails here. */
+sgn_status sgn_server_submit(sgn_server* server, uint32_t tile_id, uint32_t format, const sgn_request* request,
+                             uint64_t* ticket);
+/* Moves up to cap published results into out (*count of them), waiting up to
+ * timeout_ms for the first one (0: no wait). */
+sgn_status sgn_server_poll(sgn_server* server, sgn_server_result* out, size_t cap, size_t* count, uint32_t timeout_ms);
+sgn_status sgn_server_stats_get(sgn_server* server, sgn_server_stats* out);
+/* Frees a result surface without synchronising the device. */
+void sgn_server_surface_free(sgn_server* server, sgn_surface* surface);
+/* Finishes every queued and in-flight request, then releases the server;
+ * results not yet polled are freed. */
+void sgn_server_destroy(sgn_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,8 +45,35 @@ class SgnEncodeOptions(ctypes.Structure):
                  "progression", "write_tlm", "sop_eph")]
 
 
+class SgnServerConfig(ctypes.Structure):
+    _fields_ = [("device_budget_bytes", ctypes.c_uint64), ("resident_capacity_bytes", ctypes.c_uint64),
+                ("max_batch_tiles", ctypes.c_uint32), ("slots", ctypes.c_uint32)]
+
+
+class SgnServerResult(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("status", ctypes.c_int32), ("batch_tiles", ctypes.c_uint32),
+                ("surface", SgnSurface), ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+
+
+class SgnServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "batches", "rejected", "bytes_in_use",
+                                               "peak_bytes_in_use")] + \
+               [("max_batch_seen", ctypes.c_uint32), ("max_inflight_seen", ctypes.c_uint32)]
+
+
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
 CUDA_SIGNATURES = {
+    "sgn_server_create": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerConfig),
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "sgn_server_register": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                             ctypes.POINTER(ctypes.c_uint32)]),
+    "sgn_server_submit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(SgnRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "sgn_server_poll": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerResult), ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_size_t), ctypes.c_uint32]),
+    "sgn_server_stats_get": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerStats)]),
+    "sgn_server_surface_free": (None, [ctypes.c_void_p, ctypes.POINTER(SgnSurface)]),
+    "sgn_server_destroy": (None, [ctypes.c_void_p]),
     "sgn_ctx_create": (ctypes.c_int32, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "sgn_ctx_destroy": (None, [ctypes.c_void_p]),
     "sgn_ctx_submissions": (ctypes.c_uint64, [ctypes.c_void_p]),

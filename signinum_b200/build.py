@@ -27,6 +27,7 @@ CUDA_SOURCES = [
     CSRC / "kernels" / "idwt_pack.cu",
     CSRC / "host" / "runtime.cu",
     CSRC / "host" / "noalloc.cu",
+    CSRC / "host" / "server.cu",
     CSRC / "host" / "codestream.cpp",
 ]
 ENCODE_SOURCES = [

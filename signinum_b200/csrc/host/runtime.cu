@@ -24,10 +24,12 @@
 #include "../ht_tables.h"
 #include "../kernels/kernels.h"
 #include "codestream.h"
+#include "runtime_internal.h"
 
 using namespace sgn;
 
-namespace {
+namespace sgn {
+namespace rt {
 
 thread_local char g_msg[512];
 
@@ -36,7 +38,10 @@ sgn_status set_error(sgn_status s, const char* msg) {
   return s;
 }
 
-}  // namespace
+}  // namespace rt
+}  // namespace sgn
+
+using namespace sgn::rt;
 
 void sgn_set_last_error_message(const char* msg) { set_error(0, msg); }
 
@@ -65,7 +70,8 @@ cudaError_t ensure_device_init(int device) {
 
 }  // namespace sgn
 
-namespace {
+namespace sgn {
+namespace rt {
 
 sgn_status cuda_status(cudaError_t e, const char* where) {
   if (e == cudaSuccess) return SGN_OK;
@@ -80,130 +86,6 @@ int bytes_per_pixel(uint32_t fmt) {
   static const int b[] = {1, 3, 4, 2, 6, 8};
   return fmt < 6 ? b[fmt] : 0;
 }
-
-// Minimal fixed pool for host-side parsing of large batches.
-class Workers {
- public:
-  explicit Workers(unsigned n) {
-    for (unsigned i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
-  }
-  ~Workers() {
-    {
-      std::lock_guard<std::mutex> g(m_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (auto& t : threads_) t.join();
-  }
-  // Runs f(i) for i in [0, n) over the pool plus the calling thread.
-  void parallel_for(size_t n, const std::function<void(size_t)>& f) {
-    if (n == 0) return;
-    if (threads_.empty() || n < 4) {
-      for (size_t i = 0; i < n; ++i) f(i);
-      return;
-    }
-    std::atomic<size_t> next{0};
-    std::atomic<size_t> done_workers{0};
-    size_t nw = std::min(threads_.size(), n);
-    auto body = [&] {
-      for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
-    };
-    {
-      std::lock_guard<std::mutex> g(m_);
-      for (size_t k = 0; k < nw; ++k)
-        tasks_.push_back([&] {
-          body();
-          // Under the mutex: the waiter checks the count and blocks
-          // atomically with respect to it, so the wake-up cannot be lost.
-          {
-            std::lock_guard<std::mutex> g(m_);
-            done_workers.fetch_add(1);
-          }
-          cv_done_.notify_all();
-        });
-    }
-    cv_.notify_all();
-    body();
-    std::unique_lock<std::mutex> lk(m_);
-    cv_done_.wait(lk, [&] { return done_workers.load() == nw; });
-  }
-
- private:
-  void loop() {
-    for (;;) {
-      std::function<void()> t;
-      {
-        std::unique_lock<std::mutex> lk(m_);
-        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
-        if (stop_ && tasks_.empty()) return;
-        t = std::move(tasks_.back());
-        tasks_.pop_back();
-      }
-      t();
-    }
-  }
-  std::vector<std::thread> threads_;
-  std::vector<std::function<void()>> tasks_;
-  std::mutex m_;
-  std::condition_variable cv_, cv_done_;
-  bool stop_ = false;
-};
-
-struct PinnedBuffer {
-  uint8_t* p = nullptr;
-  size_t cap = 0;
-  cudaError_t ensure(size_t n) {
-    if (n <= cap) return cudaSuccess;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-    size_t c = std::max<size_t>(n, cap * 2);
-    cudaError_t e = cudaMallocHost((void**)&p, c);
-    if (e == cudaSuccess) cap = c;
-    return e;
-  }
-  ~PinnedBuffer() {
-    if (p) cudaFreeHost(p);
-  }
-};
-
-}  // namespace
-
-struct sgn_ctx {
-  int device = 0;
-  int sm_count = 0;
-  cudaStream_t stream = nullptr;
-  std::atomic<uint64_t> submissions{0};
-  std::mutex mu;
-  PinnedBuffer staging;
-  Workers* workers = nullptr;
-};
-
-struct RoundInfo {
-  uint32_t job_begin, njobs, ctas;
-};
-
-struct sgn_plan {
-  size_t n = 0;
-  uint32_t format = 0;
-  std::vector<sgn_status> status;  // host-side (parse/request) status per tile
-  std::vector<sgn_surface> surfaces;
-  // Device allocations (stream-ordered pool).
-  uint8_t* d_input = nullptr;
-  int32_t* d_coef = nullptr;
-  int32_t* d_levels = nullptr;
-  uint32_t* d_symbols = nullptr;
-  HtJob* d_ht = nullptr;
-  uint32_t* d_refine = nullptr;
-  IdwtJob* d_idwt = nullptr;
-  PackJob* d_pack = nullptr;
-  uint32_t* d_status = nullptr;
-  uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
-  std::vector<RoundInfo> rounds;
-  uint64_t launches = 0;
-  std::vector<uint32_t> h_status;
-  std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
-};
 
 namespace {
 
@@ -268,21 +150,6 @@ cudaError_t dalloc(T** p, size_t count, cudaStream_t s) {
   return cudaMallocAsync((void**)p, count * sizeof(T), s);
 }
 
-void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
-  void* ptrs[] = {p->d_input,  p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
-                  p->d_refine, p->d_idwt, p->d_pack,   p->d_status};
-  for (void* q : ptrs)
-    if (q) cudaFreeAsync(q, s);
-  p->d_input = nullptr;
-  p->d_coef = p->d_levels = nullptr;
-  p->d_symbols = nullptr;
-  p->d_ht = nullptr;
-  p->d_refine = nullptr;
-  p->d_idwt = nullptr;
-  p->d_pack = nullptr;
-  p->d_status = nullptr;
-}
-
 bool is_pinned(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -298,8 +165,9 @@ bool is_pinned(const void* p) {
 constexpr uint32_t kLenBuckets = 64;
 inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<uint32_t>(lcup >> 6, kLenBuckets - 1); }
 
-sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t fmt,
-                      const sgn_request* reqs, sgn_plan* plan) {
+sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
+                           const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
+                           const uint8_t* resident_arena, const uint64_t* resident_off) {
   plan->n = n;
   plan->format = fmt;
   plan->status.assign(n, SGN_OK);
@@ -320,8 +188,12 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
     plan->status[i] = work[i].status;
     if (work[i].status != SGN_OK) continue;
     const TileLayout& L = work[i].layout;
-    in_off[i] = in_total;
-    in_total += (lens[i] + 15) & ~(size_t)15;
+    if (resident_arena) {
+      in_off[i] = resident_off[i];
+    } else {
+      in_off[i] = in_total;
+      in_total += (lens[i] + 15) & ~(size_t)15;
+    }
     coef_off[i] = coef_total;
     coef_total += L.coef_per_comp * L.ncomp;
     uint32_t R = L.levels - L.skipped;  // last decoded resolution
@@ -334,18 +206,23 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
       max_rounds = std::max(max_rounds, R - 1);
     }
   }
-  cudaStream_t s = ctx->stream;
   cudaError_t e = cudaSuccess;
-  if ((e = dalloc(&plan->d_input, in_total, s)) != cudaSuccess) return cuda_status(e, "input arena");
-  // When the caller's codestreams are pinned and contiguous in arena order
-  // (16-byte padded), they go up in one copy, issued now so that it overlaps
-  // the rest of the plan build.
-  bool direct = n > 0 && in_total > 0 && plan->status[0] == SGN_OK;
-  for (size_t i = 0; direct && i + 1 < n; ++i)
-    direct = plan->status[i + 1] == SGN_OK && datas[i + 1] == datas[i] + ((lens[i] + 15) & ~(size_t)15);
-  direct = direct && is_pinned(datas[0]);
-  if (direct && (e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-    return cuda_status(e, "input upload");
+  bool direct = true;  // codestreams need no staging copy
+  if (resident_arena) {
+    plan->d_input = const_cast<uint8_t*>(resident_arena);
+    plan->owns_input = false;
+  } else {
+    if ((e = dalloc(&plan->d_input, in_total, s)) != cudaSuccess) return cuda_status(e, "input arena");
+    // When the caller's codestreams are pinned and contiguous in arena order
+    // (16-byte padded), they go up in one copy, issued now so that it
+    // overlaps the rest of the plan build.
+    direct = n > 0 && in_total > 0 && plan->status[0] == SGN_OK;
+    for (size_t i = 0; direct && i + 1 < n; ++i)
+      direct = plan->status[i + 1] == SGN_OK && datas[i + 1] == datas[i] + ((lens[i] + 15) & ~(size_t)15);
+    direct = direct && is_pinned(datas[0]);
+    if (direct && (e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_status(e, "input upload");
+  }
   if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
   if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
   if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
@@ -519,8 +396,8 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   const size_t at_idwt = at_ref + up16((size_t)nref * 4);
   const size_t at_pack = at_idwt + up16(idwt.size() * sizeof(IdwtJob));
   const size_t stage_bytes = at_pack + up16(packs.size() * sizeof(PackJob));
-  if ((e = ctx->staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
-  uint8_t* st = ctx->staging.p;
+  if ((e = staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
+  uint8_t* st = staging.p;
   HtJob* ht = reinterpret_cast<HtJob*>(st + at_ht);
   uint32_t* refine = reinterpret_cast<uint32_t*>(st + at_ref);
   // HT job table, pass B (per tile, in parallel): each tile writes its jobs
@@ -579,8 +456,31 @@ sgn_status build_plan(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* l
   return SGN_OK;
 }
 
-sgn_status execute(sgn_ctx* ctx, sgn_plan* p) {
-  cudaStream_t s = ctx->stream;
+}  // namespace
+
+void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
+  void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
+                  p->d_refine, p->d_idwt, p->d_pack, p->d_status};
+  for (void* q : ptrs)
+    if (q) cudaFreeAsync(q, s);
+  p->d_input = nullptr;
+  p->d_coef = p->d_levels = nullptr;
+  p->d_symbols = nullptr;
+  p->d_ht = nullptr;
+  p->d_refine = nullptr;
+  p->d_idwt = nullptr;
+  p->d_pack = nullptr;
+  p->d_status = nullptr;
+}
+
+void release_plan(sgn_plan* p, cudaStream_t s) {
+  for (auto& sf : p->surfaces)
+    if (sf.device_ptr) cudaFreeAsync((void*)(uintptr_t)sf.device_ptr, s);
+  p->surfaces.clear();
+  free_plan_buffers(p, s);
+}
+
+sgn_status execute(sgn_plan* p, cudaStream_t s) {
   cudaError_t e;
   if (p->n && (e = cudaMemsetAsync(p->d_status, 0, p->n * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "status reset");
@@ -595,13 +495,13 @@ sgn_status execute(sgn_ctx* ctx, sgn_plan* p) {
   return SGN_OK;
 }
 
-sgn_status wait_plan(sgn_ctx* ctx, sgn_plan* p, sgn_status* per_tile, size_t* first_failing) {
+sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* first_failing) {
   cudaError_t e;
   p->h_status.assign(p->n, 0);
-  if (p->n && (e = cudaMemcpyAsync(p->h_status.data(), p->d_status, p->n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
+  if (p->n && (e = cudaMemcpyAsync(p->h_status.data(), p->d_status, p->n * 4, cudaMemcpyDeviceToHost, s)) !=
                   cudaSuccess)
     return cuda_status(e, "status download");
-  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(e, "decode");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "decode");
   size_t first = SIZE_MAX;
   sgn_status first_status = SGN_OK;
   for (size_t i = 0; i < p->n; ++i) {
@@ -618,7 +518,14 @@ sgn_status wait_plan(sgn_ctx* ctx, sgn_plan* p, sgn_status* per_tile, size_t* fi
   return first_status;
 }
 
-}  // namespace
+sgn_status build_plan(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
+                      const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
+                      const uint8_t* resident_arena, const uint64_t* resident_off) {
+  return build_plan_impl(ctx, s, staging, datas, lens, n, fmt, reqs, plan, resident_arena, resident_off);
+}
+
+}  // namespace rt
+}  // namespace sgn
 
 extern "C" {
 
@@ -708,7 +615,7 @@ sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size
   sgn_plan* p = new sgn_plan();
   sgn_status st;
   try {
-    st = build_plan(ctx, datas, lens, n, format, requests, p);
+    st = build_plan(ctx, ctx->stream, ctx->staging, datas, lens, n, format, requests, p);
   } catch (const std::bad_alloc&) {
     st = set_error(SGN_ERR_OUT_OF_MEMORY, "host allocation failed");
   }
@@ -729,7 +636,7 @@ sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size
 sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan) {
   if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
-  return execute(ctx, plan);
+  return execute(plan, ctx->stream);
 }
 
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
@@ -766,7 +673,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
 sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing) {
   if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
-  return wait_plan(ctx, plan, per_tile, first_failing);
+  return wait_plan(plan, ctx->stream, per_tile, first_failing);
 }
 
 sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n) {
@@ -848,9 +755,9 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
   if (st != SGN_OK) return st;
   std::lock_guard<std::mutex> g(ctx->mu);
   ctx->submissions.fetch_add(1);
-  st = execute(ctx, p);
+  st = execute(p, ctx->stream);
   std::vector<sgn_status> statuses(n);
-  sgn_status wst = st == SGN_OK ? wait_plan(ctx, p, statuses.data(), first_failing) : st;
+  sgn_status wst = st == SGN_OK ? wait_plan(p, ctx->stream, statuses.data(), first_failing) : st;
   for (size_t i = 0; i < n; ++i) {
     if (per_tile) per_tile[i] = st == SGN_OK ? statuses[i] : st;
     if (st == SGN_OK && statuses[i] == SGN_OK) {

@@ -1,0 +1,178 @@
+// Internals of the CUDA decode runtime shared by the C ABI (runtime.cu) and
+// the serving loop (server.cu): the context and plan structures and the plan
+// builder.  Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <functional>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../../include/signinum_j2k_cuda.h"
+#include "../device_plan.h"
+
+namespace sgn {
+namespace rt {
+
+// Minimal fixed pool for host-side parsing of large batches.
+class Workers {
+ public:
+  explicit Workers(unsigned n) {
+    for (unsigned i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
+  }
+  ~Workers() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+  // Runs f(i) for i in [0, n) over the pool plus the calling thread.
+  void parallel_for(size_t n, const std::function<void(size_t)>& f) {
+    if (n == 0) return;
+    if (threads_.empty() || n < 4) {
+      for (size_t i = 0; i < n; ++i) f(i);
+      return;
+    }
+    std::atomic<size_t> next{0};
+    std::atomic<size_t> done_workers{0};
+    size_t nw = std::min(threads_.size(), n);
+    auto body = [&] {
+      for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    };
+    {
+      std::lock_guard<std::mutex> g(m_);
+      for (size_t k = 0; k < nw; ++k)
+        tasks_.push_back([&] {
+          body();
+          // Under the mutex: the waiter checks the count and blocks
+          // atomically with respect to it, so the wake-up cannot be lost.
+          {
+            std::lock_guard<std::mutex> g(m_);
+            done_workers.fetch_add(1);
+          }
+          cv_done_.notify_all();
+        });
+    }
+    cv_.notify_all();
+    body();
+    std::unique_lock<std::mutex> lk(m_);
+    cv_done_.wait(lk, [&] { return done_workers.load() == nw; });
+  }
+
+ private:
+  void loop() {
+    for (;;) {
+      std::function<void()> t;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+        if (stop_ && tasks_.empty()) return;
+        t = std::move(tasks_.back());
+        tasks_.pop_back();
+      }
+      t();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::vector<std::function<void()>> tasks_;
+  std::mutex m_;
+  std::condition_variable cv_, cv_done_;
+  bool stop_ = false;
+};
+
+struct PinnedBuffer {
+  uint8_t* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t c = std::max<size_t>(n, cap * 2);
+    cudaError_t e = cudaMallocHost((void**)&p, c);
+    if (e == cudaSuccess) cap = c;
+    return e;
+  }
+  ~PinnedBuffer() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+}  // namespace rt
+}  // namespace sgn
+
+struct sgn_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  std::atomic<uint64_t> submissions{0};
+  std::mutex mu;
+  sgn::rt::PinnedBuffer staging;
+  sgn::rt::Workers* workers = nullptr;
+};
+
+struct RoundInfo {
+  uint32_t job_begin, njobs, ctas;
+};
+
+struct sgn_plan {
+  using HtJob = sgn::HtJob;
+  using IdwtJob = sgn::IdwtJob;
+  using PackJob = sgn::PackJob;
+  using RoundInfo = ::RoundInfo;
+  size_t n = 0;
+  uint32_t format = 0;
+  std::vector<sgn_status> status;  // host-side (parse/request) status per tile
+  std::vector<sgn_surface> surfaces;
+  // Device allocations (stream-ordered pool).
+  uint8_t* d_input = nullptr;
+  bool owns_input = true;  // false: codestreams live in a caller-owned resident arena
+  int32_t* d_coef = nullptr;
+  int32_t* d_levels = nullptr;
+  uint32_t* d_symbols = nullptr;
+  HtJob* d_ht = nullptr;
+  uint32_t* d_refine = nullptr;
+  IdwtJob* d_idwt = nullptr;
+  PackJob* d_pack = nullptr;
+  uint32_t* d_status = nullptr;
+  uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
+  std::vector<RoundInfo> rounds;
+  uint64_t launches = 0;
+  std::vector<uint32_t> h_status;
+  std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
+};
+
+
+namespace sgn {
+namespace rt {
+
+sgn_status set_error(sgn_status s, const char* msg);
+sgn_status cuda_status(cudaError_t e, const char* where);
+int bytes_per_pixel(uint32_t fmt);
+
+// Builds a plan for n codestreams on stream s, using `staging` for the
+// uploads (the copies are finished when it returns).  With resident_arena,
+// the codestreams already sit in that device buffer at byte offsets
+// resident_off[i] (16-byte aligned) and are not copied; datas still give the
+// host bytes for parsing.
+sgn_status build_plan(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
+                      const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
+                      const uint8_t* resident_arena = nullptr, const uint64_t* resident_off = nullptr);
+// Enqueues the plan's kernels on s.
+sgn_status execute(sgn_plan* p, cudaStream_t s);
+// Reads the per-tile device status (synchronising s) and merges host statuses.
+sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* first_failing);
+void free_plan_buffers(sgn_plan* p, cudaStream_t s);
+// Frees the plan's surfaces that are still owned by it, then its buffers.
+void release_plan(sgn_plan* p, cudaStream_t s);
+
+}  // namespace rt
+}  // namespace sgn
