@@ -49,6 +49,9 @@ def parse_args():
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
     ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000", help="c4: arrival rates, tiles/s")
     ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate")
+    ap.add_argument("--slots", type=int, default=3, help="c4: batches in flight")
+    ap.add_argument("--max-batch", type=int, default=512, help="c4: requests per batch")
+    ap.add_argument("--max-batch-samples", type=int, default=0, help="c4: decoded samples per batch (0: unbounded)")
     return ap.parse_args()
 
 
@@ -247,7 +250,7 @@ def run_serving(args):
 
     ctx = j2k_cuda._Context.open(local)
     server = Server(ctx, device_budget_bytes=16 << 30, resident_capacity_bytes=coded + 64 * len(pool) + (1 << 20),
-                    max_batch_tiles=512, slots=3)
+                    max_batch_tiles=args.max_batch, slots=args.slots, max_batch_samples=args.max_batch_samples)
     ids = [server.register(t.codestream) for t in pool]
     lib = _native.cuda_lib()
     h = server._h
@@ -275,63 +278,75 @@ def run_serving(args):
         return reqs, px
 
     def run(reqs, gaps, check=0):
-        """Submits reqs at the given inter-arrival gaps (seconds); returns
-        latencies (ms), wall seconds from first submit to last result, and the
-        parity of `check` sampled results against the oracle."""
+        """Submits reqs at the given inter-arrival gaps (seconds), every request
+        whose arrival time has passed going in with one sgn_server_submit_many
+        call; returns latencies (ms), wall seconds from first submit to last
+        result, and the parity of `check` sampled results against the oracle."""
         n = len(reqs)
         got = {}
         done = threading.Event()
         keep = set(range(0, n, max(1, n // check))) if check else set()
         kept = {}
-        tick_of = {}
+        first = []
 
         def poller():
+            from signinum_b200._native import SgnSurface
+
             buf = (SgnServerResult * 4096)()
             cnt = ctypes.c_size_t()
             while len(got) < n:
                 lib.sgn_server_poll(h, buf, 4096, ctypes.byref(cnt), 20)
                 for r in buf[: cnt.value]:
                     got[r.ticket] = (r.status, r.latency_ms)
-                    k = tick_of.get(r.ticket)
-                    if k in keep and r.status == 0:
-                        from signinum_b200._native import SgnSurface
-
-                        s = SgnSurface()
-                        ctypes.pointer(s)[0] = r.surface
+                    if not r.surface.device_ptr:
+                        continue
+                    s = SgnSurface()
+                    ctypes.pointer(s)[0] = r.surface
+                    while not first:
+                        pass
+                    k = r.ticket - first[0]
+                    if k in keep:
                         out = np.zeros(max(1, s.pitch_bytes * s.height), np.uint8)
                         lib.sgn_surface_download(ctx.handle, ctypes.byref(s), out.ctypes.data, out.nbytes,
                                                  s.pitch_bytes)
                         kept[k] = out.tobytes()
-                        lib.sgn_server_surface_free(h, ctypes.byref(s))
-                    elif r.surface.device_ptr:
-                        s = r.surface
-                        lib.sgn_server_surface_free(h, ctypes.byref(s))
+                    lib.sgn_server_surface_free(h, ctypes.byref(s))
             done.set()
 
+        ids_arr = (ctypes.c_uint32 * n)(*[q[0] for q in reqs])
+        req_arr = (SgnRequest * n)(*[q[1] for q in reqs])
+        tick_arr = (ctypes.c_uint64 * n)()
+        sub = ctypes.c_size_t()
+        rsz = ctypes.sizeof(SgnRequest)
         th = threading.Thread(target=poller, daemon=True)
         th.start()
-        t_ticket = ctypes.c_uint64()
         sched = np.cumsum(gaps)
+        k = 0
         t0 = time.perf_counter()
-        for k, (tid, r, _) in enumerate(reqs):
-            target = t0 + sched[k]
-            while time.perf_counter() < target:
-                pass
-            rc = lib.sgn_server_submit(h, tid, 1, ctypes.byref(r), ctypes.byref(t_ticket))
-            assert rc == 0, rc
-            tick_of[t_ticket.value] = k
+        while k < n:
+            j = int(np.searchsorted(sched, time.perf_counter() - t0, side="right"))
+            if j <= k:
+                continue
+            rc = lib.sgn_server_submit_many(
+                h, j - k, ctypes.cast(ctypes.addressof(ids_arr) + 4 * k, ctypes.POINTER(ctypes.c_uint32)), 1,
+                ctypes.cast(ctypes.addressof(req_arr) + rsz * k, ctypes.POINTER(SgnRequest)),
+                ctypes.cast(ctypes.addressof(tick_arr) + 8 * k, ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(sub))
+            assert rc == 0 and sub.value == j - k, rc
+            if not first:
+                first.append(tick_arr[0])
+            k = j
         done.wait(120)
         wall = time.perf_counter() - t0
         th.join(5)
         lat = np.array([got[t][1] for t in got])
-        assert all(v[0] == 0 for v in got.values()), "a request failed"
+        assert len(got) == n and all(v[0] == 0 for v in got.values()), "a request failed"
         ok = None
         if check:
             from oracle import oracle
 
-            ok = True
-            for k, b in kept.items():
-                tid, r, i = reqs[k]
+            ok = len(kept) > 0
+            for kk, b in kept.items():
+                tid, r, i = reqs[kk]
                 want, _, _ = oracle.decode(pool[i].codestream, 1, r.kind, (r.x, r.y, r.w, r.h), r.downscale)
                 ok = ok and (want == b)
         return lat, wall, ok
@@ -369,7 +384,8 @@ def run_serving(args):
             "config": {"workload": f"serving pool of {len(pool)} uneven RGB8 tiles (sides 128..1024), requests 60% "
                                    "full RGB8 / 25% quarter resolution / 15% 256x256 region, Poisson arrivals, "
                                    "16 GiB admission budget, codestreams resident on the device",
-                       "pool_coded_bytes": coded, "slots": 3, "max_batch_tiles": 512},
+                       "pool_coded_bytes": coded, "slots": args.slots, "max_batch_tiles": args.max_batch,
+                       "max_batch_samples": args.max_batch_samples},
             "peak_closed_loop": {"throughput_tiles_s": peak_tps, "throughput_mpix_s": sum(peak_px) / peak_wall / 1e6,
                                  "requests": len(peak_reqs), "parity_sample_ok": ok_peak,
                                  "clocks": clk_peak.summary()},

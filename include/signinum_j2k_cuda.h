@@ -242,6 +242,8 @@ typedef struct sgn_server_config {
   uint64_t resident_capacity_bytes; /* device arena for registered codestreams (0: 1 GiB) */
   uint32_t max_batch_tiles;         /* requests per batch (0: 512) */
   uint32_t slots;                   /* batches in flight at once, one CUDA stream each (0: 3) */
+  uint32_t reserved;
+  uint64_t max_batch_samples;       /* decoded samples per batch, bounds a batch's GPU time (0: no bound) */
 } sgn_server_config;
 
 typedef struct sgn_server_result {
@@ -257,6 +259,7 @@ typedef struct sgn_server_stats {
   uint64_t submitted, completed, batches, rejected;
   uint64_t bytes_in_use, peak_bytes_in_use;
   uint32_t max_batch_seen, max_inflight_seen;
+  uint64_t build_us_total;  /* dispatcher time spent building and launching batches */
 } sgn_server_stats;
 
 sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_server** out);
@@ -266,6 +269,11 @@ sgn_status sgn_server_register(sgn_server* server, const uint8_t* data, size_t l
  * parse (format, request kind, region bounds, budget) fails here. */
 sgn_status sgn_server_submit(sgn_server* server, uint32_t tile_id, uint32_t format, const sgn_request* request,
                              uint64_t* ticket);
+/* Queues n requests in one call (requests NULL = all full images), in order;
+ * stops at the first invalid one and returns its status, *submitted telling
+ * how many went in. */
+sgn_status sgn_server_submit_many(sgn_server* server, size_t n, const uint32_t* tile_ids, uint32_t format,
+                                  const sgn_request* requests, uint64_t* tickets, size_t* submitted);
 /* Moves up to cap published results into out (*count of them), waiting up to
  * timeout_ms for the first one (0: no wait). */
 sgn_status sgn_server_poll(sgn_server* server, sgn_server_result* out, size_t cap, size_t* count, uint32_t timeout_ms);

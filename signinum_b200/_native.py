@@ -47,7 +47,8 @@ class SgnEncodeOptions(ctypes.Structure):
 
 class SgnServerConfig(ctypes.Structure):
     _fields_ = [("device_budget_bytes", ctypes.c_uint64), ("resident_capacity_bytes", ctypes.c_uint64),
-                ("max_batch_tiles", ctypes.c_uint32), ("slots", ctypes.c_uint32)]
+                ("max_batch_tiles", ctypes.c_uint32), ("slots", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("max_batch_samples", ctypes.c_uint64)]
 
 
 class SgnServerResult(ctypes.Structure):
@@ -58,7 +59,8 @@ class SgnServerResult(ctypes.Structure):
 class SgnServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "batches", "rejected", "bytes_in_use",
                                                "peak_bytes_in_use")] + \
-               [("max_batch_seen", ctypes.c_uint32), ("max_inflight_seen", ctypes.c_uint32)]
+               [("max_batch_seen", ctypes.c_uint32), ("max_inflight_seen", ctypes.c_uint32),
+                ("build_us_total", ctypes.c_uint64)]
 
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
@@ -69,6 +71,9 @@ CUDA_SIGNATURES = {
                                              ctypes.POINTER(ctypes.c_uint32)]),
     "sgn_server_submit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.POINTER(SgnRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "sgn_server_submit_many": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.c_uint32, ctypes.POINTER(SgnRequest),
+                                                ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_server_poll": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerResult), ctypes.c_size_t,
                                          ctypes.POINTER(ctypes.c_size_t), ctypes.c_uint32]),
     "sgn_server_stats_get": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerStats)]),

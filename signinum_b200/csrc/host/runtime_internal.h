@@ -9,7 +9,9 @@
 #include <atomic>
 #include <condition_variable>
 #include <cstdint>
+#include <deque>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -35,36 +37,46 @@ class Workers {
     for (auto& t : threads_) t.join();
   }
   // Runs f(i) for i in [0, n) over the pool plus the calling thread.
+  // Runs f(i) for i in [0, n) over the pool plus the calling thread and
+  // returns once every item is done.  Completion counts items, not helper
+  // tasks: a helper that starts late (its thread descheduled) finds no work
+  // left and the caller does not wait for it.  Helpers hold the shared state
+  // by reference count, never the caller's stack.
   void parallel_for(size_t n, const std::function<void(size_t)>& f) {
     if (n == 0) return;
     if (threads_.empty() || n < 4) {
       for (size_t i = 0; i < n; ++i) f(i);
       return;
     }
-    std::atomic<size_t> next{0};
-    std::atomic<size_t> done_workers{0};
-    size_t nw = std::min(threads_.size(), n);
-    auto body = [&] {
-      for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    struct Shared {
+      std::atomic<size_t> next{0}, done{0};
+      size_t n = 0;
+      const std::function<void(size_t)>* f = nullptr;
     };
+    auto sh = std::make_shared<Shared>();
+    sh->n = n;
+    sh->f = &f;
+    auto body = [this](const std::shared_ptr<Shared>& s) {
+      size_t mine = 0;
+      for (size_t i; (i = s->next.fetch_add(1)) < s->n;) {
+        (*s->f)(i);
+        ++mine;
+      }
+      if (mine && s->done.fetch_add(mine) + mine == s->n) {
+        // Under the mutex, so the waiter cannot miss it between its check and its wait.
+        std::lock_guard<std::mutex> g(m_);
+        cv_done_.notify_all();
+      }
+    };
+    const size_t nw = std::min(threads_.size(), (n + 1) / 2);
     {
       std::lock_guard<std::mutex> g(m_);
-      for (size_t k = 0; k < nw; ++k)
-        tasks_.push_back([&] {
-          body();
-          // Under the mutex: the waiter checks the count and blocks
-          // atomically with respect to it, so the wake-up cannot be lost.
-          {
-            std::lock_guard<std::mutex> g(m_);
-            done_workers.fetch_add(1);
-          }
-          cv_done_.notify_all();
-        });
+      for (size_t k = 0; k < nw; ++k) tasks_.push_back([body, sh] { body(sh); });
     }
     cv_.notify_all();
-    body();
+    body(sh);
     std::unique_lock<std::mutex> lk(m_);
-    cv_done_.wait(lk, [&] { return done_workers.load() == nw; });
+    cv_done_.wait(lk, [&] { return sh->done.load() == n; });
   }
 
  private:
@@ -75,14 +87,14 @@ class Workers {
         std::unique_lock<std::mutex> lk(m_);
         cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
         if (stop_ && tasks_.empty()) return;
-        t = std::move(tasks_.back());
-        tasks_.pop_back();
+        t = std::move(tasks_.front());
+        tasks_.pop_front();
       }
       t();
     }
   }
   std::vector<std::thread> threads_;
-  std::vector<std::function<void()>> tasks_;
+  std::deque<std::function<void()>> tasks_;
   std::mutex m_;
   std::condition_variable cv_, cv_done_;
   bool stop_ = false;

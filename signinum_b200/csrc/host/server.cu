@@ -42,7 +42,8 @@ struct Request {
   uint32_t tile;
   uint32_t format;
   sgn_request req;
-  uint64_t bytes;  // admission estimate
+  uint64_t bytes;    // admission estimate
+  uint64_t samples;  // decoded samples (batch bound)
   Clock::time_point submitted;
 };
 
@@ -72,6 +73,11 @@ uint64_t estimate_bytes(const ResidentTile& t, uint32_t format, const sgn_reques
   }
   const uint64_t coef = samples * 4, levels = samples * 2, symbols = samples, jobs = samples / 64 + 4096;
   return coef + levels + symbols + jobs + out_w * out_h * bytes_per_pixel(format) + 4096;
+}
+
+uint64_t decoded_samples(const ResidentTile& t, const sgn_request& r) {
+  const uint64_t d = (r.kind == SGN_REQ_SCALED || r.kind == SGN_REQ_REGION_SCALED) ? std::max(1u, r.downscale) : 1;
+  return ((t.width + d - 1) / d) * ((t.height + d - 1) / d) * t.ncomp;
 }
 
 }  // namespace
@@ -129,9 +135,12 @@ void sgn_server::dispatch_loop() {
         cv_work.wait(lk);
       }
       const uint32_t fmt = pending.front().format;
+      uint64_t samples = 0;
       while (!pending.empty() && batch.size() < cfg.max_batch_tiles && pending.front().format == fmt &&
-             (batch.empty() || stats.bytes_in_use + bytes + pending.front().bytes <= cfg.device_budget_bytes)) {
+             (batch.empty() || ((stats.bytes_in_use + bytes + pending.front().bytes <= cfg.device_budget_bytes) &&
+                                (!cfg.max_batch_samples || samples + pending.front().samples <= cfg.max_batch_samples)))) {
         bytes += pending.front().bytes;
+        samples += pending.front().samples;
         batch.push_back(pending.front());
         pending.pop_front();
       }
@@ -143,6 +152,7 @@ void sgn_server::dispatch_loop() {
       stats.batches += 1;
     }
     Slot& sl = slots[si];
+    const auto t_build = Clock::now();
     const size_t n = batch.size();
     std::vector<const uint8_t*> datas(n);
     std::vector<size_t> lens(n);
@@ -165,6 +175,7 @@ void sgn_server::dispatch_loop() {
     sl.launched = Clock::now();
     {
       std::lock_guard<std::mutex> g(mu);
+      stats.build_us_total += (uint64_t)(ms_between(t_build, sl.launched) * 1000.0);
       inflight.push_back(si);
       stats.max_inflight_seen = std::max<uint32_t>(stats.max_inflight_seen, (uint32_t)inflight.size());
     }
@@ -282,9 +293,13 @@ sgn_status sgn_server_register(sgn_server* sv, const uint8_t* data, size_t len, 
   return SGN_OK;
 }
 
-sgn_status sgn_server_submit(sgn_server* sv, uint32_t tile_id, uint32_t format, const sgn_request* request,
-                             uint64_t* ticket) {
-  if (!sv || !ticket) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+}  // extern "C"
+
+namespace {
+
+// Validates and queues one request; sv->mu is held by the caller.
+sgn_status submit_locked(sgn_server* sv, uint32_t tile_id, uint32_t format, const sgn_request* request,
+                         uint64_t* ticket) {
   sgn_request r{};
   r.kind = SGN_REQ_FULL;
   r.downscale = 1;
@@ -294,13 +309,13 @@ sgn_status sgn_server_submit(sgn_server* sv, uint32_t tile_id, uint32_t format, 
     return set_error(SGN_ERR_INVALID_ARGUMENT, "unknown pixel format or request kind");
   Request q;
   {
-    std::lock_guard<std::mutex> g(sv->mu);
     if (tile_id >= sv->tiles.size()) return set_error(SGN_ERR_INVALID_ARGUMENT, "unknown tile id");
     const ResidentTile& t = *sv->tiles[tile_id];
     if ((r.kind == SGN_REQ_REGION || r.kind == SGN_REQ_REGION_SCALED) &&
         ((uint64_t)r.x + r.w > t.width || (uint64_t)r.y + r.h > t.height))
       return set_error(SGN_ERR_REGION, "region outside the image");
     q.bytes = estimate_bytes(t, format, r);
+    q.samples = decoded_samples(t, r);
     if (q.bytes > sv->cfg.device_budget_bytes) {
       sv->stats.rejected += 1;
       return set_error(SGN_ERR_OUT_OF_MEMORY, "request exceeds the server's device-memory budget");
@@ -313,9 +328,41 @@ sgn_status sgn_server_submit(sgn_server* sv, uint32_t tile_id, uint32_t format, 
     sv->pending.push_back(q);
     sv->stats.submitted += 1;
   }
-  sv->cv_work.notify_all();
   *ticket = q.ticket;
   return SGN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sgn_status sgn_server_submit(sgn_server* sv, uint32_t tile_id, uint32_t format, const sgn_request* request,
+                             uint64_t* ticket) {
+  if (!sv || !ticket) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  sgn_status st;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    st = submit_locked(sv, tile_id, format, request, ticket);
+  }
+  if (st == SGN_OK) sv->cv_work.notify_all();
+  return st;
+}
+
+sgn_status sgn_server_submit_many(sgn_server* sv, size_t n, const uint32_t* tile_ids, uint32_t format,
+                                  const sgn_request* requests, uint64_t* tickets, size_t* submitted) {
+  if (!sv || (n && (!tile_ids || !tickets))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  sgn_status st = SGN_OK;
+  size_t k = 0;
+  {
+    std::lock_guard<std::mutex> g(sv->mu);
+    for (; k < n; ++k) {
+      st = submit_locked(sv, tile_ids[k], format, requests ? &requests[k] : nullptr, &tickets[k]);
+      if (st != SGN_OK) break;
+    }
+  }
+  if (submitted) *submitted = k;
+  if (k) sv->cv_work.notify_all();
+  return st;
 }
 
 sgn_status sgn_server_poll(sgn_server* sv, sgn_server_result* out, size_t cap, size_t* count, uint32_t timeout_ms) {

@@ -46,9 +46,11 @@ class Result:
 
 class Server:
     def __init__(self, ctx: Optional[_Context] = None, device_budget_bytes: int = 16 << 30,
-                 resident_capacity_bytes: int = 1 << 30, max_batch_tiles: int = 512, slots: int = 3):
+                 resident_capacity_bytes: int = 1 << 30, max_batch_tiles: int = 512, slots: int = 3,
+                 max_batch_samples: int = 0):
         self.ctx = ctx or _Context.default(0)
-        cfg = SgnServerConfig(device_budget_bytes, resident_capacity_bytes, max_batch_tiles, slots)
+        cfg = SgnServerConfig(device_budget_bytes, resident_capacity_bytes, max_batch_tiles, slots, 0,
+                              max_batch_samples)
         h = ctypes.c_void_p()
         _check(_native.cuda_lib().sgn_server_create(self.ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
