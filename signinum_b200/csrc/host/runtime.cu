@@ -90,7 +90,8 @@ int bytes_per_pixel(uint32_t fmt) {
 namespace {
 
 struct TileWork {
-  TileLayout layout;
+  const TileLayout* L = nullptr;  // the parse below, or a caller's cached one
+  TileLayout own;
   sgn_status status = SGN_OK;
   uint32_t crop_x = 0, crop_y = 0, crop_w = 0, crop_h = 0;
   uint32_t region_conv = 0;
@@ -99,7 +100,8 @@ struct TileWork {
 // Request semantics: DeviceDecodePlan::for_image (device_plan.rs:23-51) for
 // the output rectangle, decode_scaled_from_info / decode_region_scaled_from_info
 // (crates/signinum-j2k/src/decode.rs:12-71) for the reduced resolution.
-void prepare_tile(const uint8_t* data, size_t len, uint32_t fmt, const sgn_request* req, TileWork& tw) {
+void prepare_tile(const uint8_t* data, size_t len, uint32_t fmt, const sgn_request* req, TileWork& tw,
+                  const TileLayout* cached) {
   try {
     if (fmt == SGN_FMT_RGBA16) throw ParseError{SGN_ERR_UNSUPPORTED, "Rgba16 output is not supported"};
     if (fmt > SGN_FMT_RGBA16) throw ParseError{SGN_ERR_INVALID_ARGUMENT, "unknown pixel format"};
@@ -120,8 +122,13 @@ void prepare_tile(const uint8_t* data, size_t len, uint32_t fmt, const sgn_reque
     uint32_t ox0 = sx / d, oy0 = sy / d;
     uint32_t ox1 = (uint32_t)(((uint64_t)sx + sw + d - 1) / d), oy1 = (uint32_t)(((uint64_t)sy + sh + d - 1) / d);
     uint32_t target[2] = {(info.width + d - 1) / d, (info.height + d - 1) / d};
-    parse_tile(data, len, d == 1 ? nullptr : target, tw.layout);
-    const TileLayout& L = tw.layout;
+    if (cached) {
+      tw.L = cached;
+    } else {
+      parse_tile(data, len, d == 1 ? nullptr : target, tw.own);
+      tw.L = &tw.own;
+    }
+    const TileLayout& L = *tw.L;
     bool gray = L.ncomp == 1;
     bool ok_map = (gray && (fmt == SGN_FMT_GRAY8 || fmt == SGN_FMT_GRAY16)) ||
                   (!gray && (fmt == SGN_FMT_RGB8 || fmt == SGN_FMT_RGBA8 || fmt == SGN_FMT_RGB16));
@@ -167,7 +174,8 @@ inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<ui
 
 sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
                            const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
-                           const uint8_t* resident_arena, const uint64_t* resident_off) {
+                           const uint8_t* resident_arena, const uint64_t* resident_off,
+                           const TileLayout* const* layouts, bool sync_uploads) {
   plan->n = n;
   plan->format = fmt;
   plan->status.assign(n, SGN_OK);
@@ -178,7 +186,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       work[i].status = SGN_ERR_INVALID_ARGUMENT;
       return;
     }
-    prepare_tile(datas[i], lens[i], fmt, reqs ? &reqs[i] : nullptr, work[i]);
+    prepare_tile(datas[i], lens[i], fmt, reqs ? &reqs[i] : nullptr, work[i], layouts ? layouts[i] : nullptr);
   });
   // Arena layout.
   std::vector<uint64_t> in_off(n, 0), coef_off(n, 0), lvl_off(n, 0), lvl_size(n, 0);
@@ -187,7 +195,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   for (size_t i = 0; i < n; ++i) {
     plan->status[i] = work[i].status;
     if (work[i].status != SGN_OK) continue;
-    const TileLayout& L = work[i].layout;
+    const TileLayout& L = *work[i].L;
     if (resident_arena) {
       in_off[i] = resident_off[i];
     } else {
@@ -229,7 +237,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   plan->tile_coef_off = coef_off;
   plan->tile_coef_elems.assign(n, 0);
   for (size_t i = 0; i < n; ++i)
-    if (plan->status[i] == SGN_OK) plan->tile_coef_elems[i] = work[i].layout.coef_per_comp * work[i].layout.ncomp;
+    if (plan->status[i] == SGN_OK) plan->tile_coef_elems[i] = work[i].L->coef_per_comp * work[i].L->ncomp;
 
   // HT job table, pass A (per tile, in parallel): block counts per
   // coded-length bucket, symbol scratch, refinement blocks and the MagSgn
@@ -245,7 +253,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     TileHt& t = th[i];
     std::fill(t.hist, t.hist + kLenBuckets, 0u);
     if (plan->status[i] != SGN_OK) return;
-    for (const CodeBlock& cb : work[i].layout.blocks) {
+    for (const CodeBlock& cb : work[i].L->blocks) {
       ++t.hist[len_bucket(cb.lcup)];
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
       if (!cb.passes) continue;
@@ -289,12 +297,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   std::vector<std::vector<IdwtJob>> rounds(max_rounds);
   std::vector<PackJob> packs;
   auto band_ptr = [&](size_t i, uint32_t c, uint32_t bi) -> int32_t* {
-    const TileLayout& L = work[i].layout;
+    const TileLayout& L = *work[i].L;
     return plan->d_coef + coef_off[i] + (uint64_t)c * L.coef_per_comp + L.bands[bi].coef_off;
   };
   for (size_t i = 0; i < n; ++i) {
     if (plan->status[i] != SGN_OK) continue;
-    const TileLayout& L = work[i].layout;
+    const TileLayout& L = *work[i].L;
     const uint32_t R = L.levels - L.skipped;
     auto lvl = [&](uint32_t c, uint32_t r) {
       return plan->d_levels + lvl_off[i] + ((uint64_t)c * 2 + (r & 1)) * lvl_size[i];
@@ -405,7 +413,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   ctx->workers->parallel_for(n, [&](size_t i) {
     if (plan->status[i] != SGN_OK) return;
     if (!direct) std::memcpy(st + in_off[i], datas[i], lens[i]);
-    const TileLayout& L = work[i].layout;
+    const TileLayout& L = *work[i].L;
     uint32_t cursor[kLenBuckets];
     for (uint32_t b = 0; b < kLenBuckets; ++b) cursor[b] = start[(size_t)b * n + i];
     uint64_t sym = sym_off[i];
@@ -449,8 +457,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if ((e = cudaMemcpyAsync(u.d, st + u.at, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
       return cuda_status(e, "plan upload");
   }
-  // The staging buffer is reused by the next call: finish the copies now.
-  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
+  // The staging buffer is reused by the next call: finish the copies now
+  // (callers that reuse it only after the plan has run pass sync_uploads false).
+  if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
   plan->launches = 1 + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0);
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
   return SGN_OK;
@@ -520,8 +529,10 @@ sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* 
 
 sgn_status build_plan(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
                       const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
-                      const uint8_t* resident_arena, const uint64_t* resident_off) {
-  return build_plan_impl(ctx, s, staging, datas, lens, n, fmt, reqs, plan, resident_arena, resident_off);
+                      const uint8_t* resident_arena, const uint64_t* resident_off,
+                      const TileLayout* const* layouts, bool sync_uploads) {
+  return build_plan_impl(ctx, s, staging, datas, lens, n, fmt, reqs, plan, resident_arena, resident_off, layouts,
+                         sync_uploads);
 }
 
 }  // namespace rt

@@ -18,6 +18,7 @@
 
 #include "../../../include/signinum_j2k_cuda.h"
 #include "../device_plan.h"
+#include "codestream.h"
 
 namespace sgn {
 namespace rt {
@@ -175,9 +176,14 @@ int bytes_per_pixel(uint32_t fmt);
 // the codestreams already sit in that device buffer at byte offsets
 // resident_off[i] (16-byte aligned) and are not copied; datas still give the
 // host bytes for parsing.
+// layouts (optional, entries may be null) hands in tile layouts parsed
+// earlier for the same codestream and resolution (parse_tile with the target
+// the request implies); sync_uploads false leaves the copies in flight (the
+// caller must not reuse `staging` before the plan has run).
 sgn_status build_plan(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
                       const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
-                      const uint8_t* resident_arena = nullptr, const uint64_t* resident_off = nullptr);
+                      const uint8_t* resident_arena = nullptr, const uint64_t* resident_off = nullptr,
+                      const TileLayout* const* layouts = nullptr, bool sync_uploads = true);
 // Enqueues the plan's kernels on s.
 sgn_status execute(sgn_plan* p, cudaStream_t s);
 // Reads the per-tile device status (synchronising s) and merges host statuses.

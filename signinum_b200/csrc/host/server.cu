@@ -35,7 +35,22 @@ struct ResidentTile {
   std::vector<uint8_t> host;  // for header parsing
   uint64_t offset = 0;        // in the device arena (16-byte aligned)
   uint32_t width = 0, height = 0, ncomp = 0;
+  // Packet-header parse per resolution (downscale 1, 2, 4, 8), made by the
+  // dispatcher the first time a request needs it and reused afterwards.
+  std::unique_ptr<TileLayout> layout[4];
+  bool parse_failed[4] = {};
 };
+
+int scale_index(const sgn_request& r) {
+  if (r.kind != SGN_REQ_SCALED && r.kind != SGN_REQ_REGION_SCALED) return 0;
+  switch (r.downscale) {
+    case 1: return 0;
+    case 2: return 1;
+    case 4: return 2;
+    case 8: return 3;
+    default: return -1;  // rejected by the plan builder
+  }
+}
 
 struct Request {
   uint64_t ticket;
@@ -110,7 +125,7 @@ void sgn_server::dispatch_loop() {
   for (;;) {
     int si = -1;
     std::vector<Request> batch;
-    std::vector<const ResidentTile*> batch_tiles;  // stable: tiles are never removed
+    std::vector<ResidentTile*> batch_tiles;  // stable: tiles are never removed
     uint64_t bytes = 0;
     {
       std::unique_lock<std::mutex> lk(mu);
@@ -158,16 +173,41 @@ void sgn_server::dispatch_loop() {
     std::vector<size_t> lens(n);
     std::vector<uint64_t> offs(n);
     std::vector<sgn_request> reqs(n);
+    std::vector<const TileLayout*> layouts(n, nullptr);
+    std::vector<std::pair<ResidentTile*, int>> misses;
     for (size_t i = 0; i < n; ++i) {
-      const ResidentTile& t = *batch_tiles[i];
+      ResidentTile& t = *batch_tiles[i];
       datas[i] = t.host.data();
       lens[i] = t.host.size();
       offs[i] = t.offset;
       reqs[i] = batch[i].req;
+      const int si_ = scale_index(reqs[i]);
+      if (si_ >= 0 && !t.layout[si_] && !t.parse_failed[si_]) {
+        t.layout[si_].reset(new TileLayout());
+        misses.emplace_back(&t, si_);
+      }
+    }
+    // First use of a tile at a resolution: parse its packet headers once.
+    ctx->workers->parallel_for(misses.size(), [&](size_t k) {
+      ResidentTile& t = *misses[k].first;
+      const int d = 1 << misses[k].second;
+      const uint32_t target[2] = {(t.width + d - 1) / d, (t.height + d - 1) / d};
+      try {
+        parse_tile(t.host.data(), t.host.size(), d == 1 ? nullptr : target, *t.layout[misses[k].second]);
+      } catch (const ParseError&) {
+        t.parse_failed[misses[k].second] = true;
+      }
+    });
+    for (auto& m : misses)
+      if (m.first->parse_failed[m.second]) m.first->layout[m.second].reset();
+    for (size_t i = 0; i < n; ++i) {
+      const int si_ = scale_index(reqs[i]);
+      if (si_ >= 0) layouts[i] = batch_tiles[i]->layout[si_].get();
     }
     sl.plan = new sgn_plan();
+    // No upload sync: the slot's staging is reused only after this batch ran.
     sl.launch_status = build_plan(ctx, sl.stream, sl.staging, datas.data(), lens.data(), n, batch[0].format,
-                                  reqs.data(), sl.plan, arena, offs.data());
+                                  reqs.data(), sl.plan, arena, offs.data(), layouts.data(), false);
     if (sl.launch_status == SGN_OK) sl.launch_status = execute(sl.plan, sl.stream);
     cudaEventRecord(sl.done, sl.stream);
     sl.reqs = std::move(batch);
