@@ -280,6 +280,9 @@ sgn_status sgn_server_poll(sgn_server* server, sgn_server_result* out, size_t ca
 sgn_status sgn_server_stats_get(sgn_server* server, sgn_server_stats* out);
 /* Frees a result surface without synchronising the device. */
 void sgn_server_surface_free(sgn_server* server, sgn_surface* surface);
+/* Frees the surfaces of n polled results at once (entries already freed or
+ * failed are skipped). */
+void sgn_server_results_release(sgn_server* server, sgn_server_result* results, size_t n);
 /* Finishes every queued and in-flight request, then releases the server;
  * results not yet polled are freed. */
 void sgn_server_destroy(sgn_server* server);

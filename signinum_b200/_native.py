@@ -78,6 +78,7 @@ CUDA_SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_size_t), ctypes.c_uint32]),
     "sgn_server_stats_get": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerStats)]),
     "sgn_server_surface_free": (None, [ctypes.c_void_p, ctypes.POINTER(SgnSurface)]),
+    "sgn_server_results_release": (None, [ctypes.c_void_p, ctypes.POINTER(SgnServerResult), ctypes.c_size_t]),
     "sgn_server_destroy": (None, [ctypes.c_void_p]),
     "sgn_ctx_create": (ctypes.c_int32, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "sgn_ctx_destroy": (None, [ctypes.c_void_p]),

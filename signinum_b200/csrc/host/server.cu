@@ -434,6 +434,16 @@ void sgn_server_surface_free(sgn_server* sv, sgn_surface* sf) {
   sf->device_ptr = 0;
 }
 
+void sgn_server_results_release(sgn_server* sv, sgn_server_result* results, size_t n) {
+  if (!sv || !results) return;
+  cudaSetDevice(sv->ctx->device);
+  for (size_t i = 0; i < n; ++i)
+    if (results[i].surface.device_ptr) {
+      cudaFreeAsync((void*)(uintptr_t)results[i].surface.device_ptr, sv->free_stream);
+      results[i].surface.device_ptr = 0;
+    }
+}
+
 void sgn_server_destroy(sgn_server* sv) {
   if (!sv) return;
   {
