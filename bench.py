@@ -370,9 +370,19 @@ def run_serving(args):
     warm, _ = make_requests(2000, 11)
     run(warm, np.zeros(len(warm)))
     peak_reqs, peak_px = make_requests(20000, 12)
+    s0 = server.stats()
     with Clocks(local) as clk_peak:
         _, peak_wall, ok_peak = run(peak_reqs, np.zeros(len(peak_reqs)), check=16)
     peak_tps = len(peak_reqs) / peak_wall
+    s1 = server.stats()
+
+    def per_batch(a, b):
+        nb = max(1, b["batches"] - a["batches"])
+        return {"batches": b["batches"] - a["batches"], "tiles_per_batch": (b["completed"] - a["completed"]) / nb,
+                "build_us": (b["build_us_total"] - a["build_us_total"]) / nb,
+                "gpu_us": (b["gpu_us_total"] - a["gpu_us_total"]) / nb,
+                "flight_us": (b["flight_us_total"] - a["flight_us_total"]) / nb}
+
     rates = [float(x) for x in args.rates.split(",") if x]
     per_rate = []
     for k, lam in enumerate(rates):
@@ -380,13 +390,16 @@ def run_serving(args):
         reqs, px = make_requests(n, 100 + k)
         gaps = np.random.default_rng(200 + k).exponential(1.0 / lam, size=n)
         gaps[0] = 0.0
+        sa = server.stats()
         with Clocks(local) as clk:
             lat, wall, ok = run(reqs, gaps, check=8)
+        sb = server.stats()
         tps = n / wall
         per_rate.append({"rate_tiles_s": lam, "requests": n, "throughput_tiles_s": tps,
                          "throughput_mpix_s": sum(px) / wall / 1e6,
                          "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "max_ms": float(lat.max()), "parity_sample_ok": ok, "clocks": clk.summary()})
+                         "max_ms": float(lat.max()), "parity_sample_ok": ok, "clocks": clk.summary(),
+                         "per_batch": per_batch(sa, sb)})
     # Peak batched throughput: the larger of the closed-loop run and the best
     # rate the open-loop sweep sustained.
     peak_ref = max([peak_tps] + [r["throughput_tiles_s"] for r in per_rate])
@@ -409,6 +422,7 @@ def run_serving(args):
             "peak_tiles_s": peak_ref,
             "peak_closed_loop": {"throughput_tiles_s": peak_tps, "throughput_mpix_s": sum(peak_px) / peak_wall / 1e6,
                                  "requests": len(peak_reqs), "parity_sample_ok": ok_peak,
+                                 "per_batch": per_batch(s0, s1),
                                  "clocks": clk_peak.summary()},
             "per_rate": per_rate,
             "server_stats": st,

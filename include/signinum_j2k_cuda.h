@@ -260,6 +260,8 @@ typedef struct sgn_server_stats {
   uint64_t bytes_in_use, peak_bytes_in_use;
   uint32_t max_batch_seen, max_inflight_seen;
   uint64_t build_us_total;  /* dispatcher time spent building and launching batches */
+  uint64_t gpu_us_total;    /* device time of the batches' kernels (CUDA events) */
+  uint64_t flight_us_total; /* batch launched -> batch results published */
 } sgn_server_stats;
 
 sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_server** out);

@@ -60,7 +60,8 @@ class SgnServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "batches", "rejected", "bytes_in_use",
                                                "peak_bytes_in_use")] + \
                [("max_batch_seen", ctypes.c_uint32), ("max_inflight_seen", ctypes.c_uint32),
-                ("build_us_total", ctypes.c_uint64)]
+                ("build_us_total", ctypes.c_uint64), ("gpu_us_total", ctypes.c_uint64),
+                ("flight_us_total", ctypes.c_uint64)]
 
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.

@@ -64,7 +64,7 @@ struct Request {
 
 struct Slot {
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr, done = nullptr;
   PinnedBuffer staging;
   sgn_plan* plan = nullptr;
   std::vector<Request> reqs;
@@ -208,6 +208,7 @@ void sgn_server::dispatch_loop() {
     // No upload sync: the slot's staging is reused only after this batch ran.
     sl.launch_status = build_plan(ctx, sl.stream, sl.staging, datas.data(), lens.data(), n, batch[0].format,
                                   reqs.data(), sl.plan, arena, offs.data(), layouts.data(), false);
+    cudaEventRecord(sl.start, sl.stream);
     if (sl.launch_status == SGN_OK) sl.launch_status = execute(sl.plan, sl.stream);
     cudaEventRecord(sl.done, sl.stream);
     sl.reqs = std::move(batch);
@@ -235,6 +236,8 @@ void sgn_server::complete_loop() {
     }
     Slot& sl = slots[si];
     cudaEventSynchronize(sl.done);
+    float gpu_ms = 0.f;
+    cudaEventElapsedTime(&gpu_ms, sl.start, sl.done);
     const size_t n = sl.reqs.size();
     std::vector<sgn_status> per(n, sl.launch_status);
     if (sl.launch_status == SGN_OK) wait_plan(sl.plan, sl.stream, per.data(), nullptr);
@@ -261,6 +264,8 @@ void sgn_server::complete_loop() {
       std::lock_guard<std::mutex> g(mu);
       for (auto& r : out) results.push_back(r);
       stats.completed += n;
+      stats.gpu_us_total += (uint64_t)(gpu_ms * 1000.0f);
+      stats.flight_us_total += (uint64_t)(ms_between(sl.launched, now) * 1000.0);
       stats.bytes_in_use -= sl.bytes;
       sl.busy = false;
       inflight.pop_front();
@@ -288,12 +293,14 @@ sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_
   sv->slots.resize(sv->cfg.slots);
   for (auto& sl : sv->slots) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&sl.start);
+    if (e == cudaSuccess) e = cudaEventCreate(&sl.done);
   }
   if (e != cudaSuccess) {
     sgn_status st = cuda_status(e, "server set-up");
     for (auto& sl : sv->slots) {
       if (sl.stream) cudaStreamDestroy(sl.stream);
+      if (sl.start) cudaEventDestroy(sl.start);
       if (sl.done) cudaEventDestroy(sl.done);
     }
     if (sv->free_stream) cudaStreamDestroy(sv->free_stream);
@@ -460,6 +467,7 @@ void sgn_server_destroy(sgn_server* sv) {
   for (auto& sl : sv->slots) {
     cudaStreamSynchronize(sl.stream);
     cudaStreamDestroy(sl.stream);
+    cudaEventDestroy(sl.start);
     cudaEventDestroy(sl.done);
   }
   cudaStreamDestroy(sv->free_stream);
