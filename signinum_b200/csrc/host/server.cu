@@ -296,6 +296,15 @@ sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_
     if (e == cudaSuccess) e = cudaEventCreate(&sl.start);
     if (e == cudaSuccess) e = cudaEventCreate(&sl.done);
   }
+  // Grow the stream-ordered pool to the admission budget once, so batches
+  // never wait on the pool reserving memory (the context keeps what the pool
+  // holds: its release threshold is unbounded).
+  if (e == cudaSuccess) {
+    void* warm = nullptr;
+    e = cudaMallocAsync(&warm, sv->cfg.device_budget_bytes, sv->free_stream);
+    if (e == cudaSuccess) e = cudaFreeAsync(warm, sv->free_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sv->free_stream);
+  }
   if (e != cudaSuccess) {
     sgn_status st = cuda_status(e, "server set-up");
     for (auto& sl : sv->slots) {
@@ -324,6 +333,16 @@ sgn_status sgn_server_register(sgn_server* sv, const uint8_t* data, size_t len, 
     t->ncomp = info.components;
   } catch (const ParseError& pe) {
     return set_error(pe.status, pe.message.c_str());
+  }
+  // Full-resolution packet headers are parsed here, once; other resolutions
+  // on first use.  A codestream that fails to parse is still registered: its
+  // requests report the error like the plain call does.
+  t->layout[0].reset(new TileLayout());
+  try {
+    parse_tile(data, len, nullptr, *t->layout[0]);
+  } catch (const ParseError&) {
+    t->layout[0].reset();
+    t->parse_failed[0] = true;
   }
   std::lock_guard<std::mutex> g(sv->mu);
   const uint64_t off = (sv->arena_used + 15) & ~(uint64_t)15;
