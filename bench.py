@@ -47,11 +47,13 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
-    ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000", help="c4: arrival rates, tiles/s")
+    ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000",
+                    help="c4: arrival rates, tiles/s")
     ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate")
-    ap.add_argument("--slots", type=int, default=3, help="c4: batches in flight")
+    ap.add_argument("--slots", type=int, default=4, help="c4: batches in flight")
     ap.add_argument("--max-batch", type=int, default=512, help="c4: requests per batch")
-    ap.add_argument("--max-batch-samples", type=int, default=0, help="c4: decoded samples per batch (0: unbounded)")
+    ap.add_argument("--max-batch-samples", type=int, default=96000000,
+                    help="c4: decoded samples per batch (0: unbounded)")
     return ap.parse_args()
 
 
