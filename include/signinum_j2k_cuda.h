@@ -138,7 +138,8 @@ typedef struct sgn_plan sgn_plan;
  * decode_tiles_to_device. */
 sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n, uint32_t format,
                            const sgn_request* requests, sgn_plan** out, sgn_status* per_tile);
-/* Enqueues the kernels of the plan on the context stream (no host sync). */
+/* Enqueues the kernels of the plan on the context stream (no host sync).
+ * From the second execution on, the plan runs as one captured CUDA graph. */
 sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan);
 /* Waits for the plan and gathers per-tile statuses. */
 sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing);
@@ -149,6 +150,23 @@ sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n);
  * cleanup MagSgn pass, HT refinement, IDWT levels, last level + pack, total}
  * in milliseconds (no counterpart in the reference: measurement). */
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms);
+/* Autotuner (no counterpart in the reference).  Times the plan's stages on
+ * its own data over `reps` runs each (0: 5) for every candidate launch shape
+ * (VLC lanes per CTA; MagSgn warps per CTA, one block per warp or persistent
+ * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
+ * pack one unit per warp or persistent on a queue), keeps the fastest per
+ * stage for the plan and for later plans of the same shape on this context,
+ * and re-executes the plan so its surfaces hold the decode.  Synchronous. */
+typedef struct sgn_tune_report {
+  uint32_t vlc_threads, ms_warps, ms_blocks_per_grab, dwt_queue;  /* chosen shape */
+  float vlc_ms, ms_ms, dwt_ms;                                     /* its stage times */
+  float vlc_ms_default, ms_ms_default, dwt_ms_default;             /* the default shape's */
+} sgn_tune_report;
+sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
+/* Sets the launch shape by hand (the fields of sgn_tune_report's first row;
+ * vlc_threads 32..128 in steps of 32, ms_warps 1..8). */
+sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_threads, uint32_t ms_warps,
+                                     uint32_t ms_blocks_per_grab, uint32_t dwt_queue);
 /* Launches issued by one execute of the plan. */
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);
 void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan);

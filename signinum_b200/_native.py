@@ -64,8 +64,18 @@ class SgnServerStats(ctypes.Structure):
                 ("flight_us_total", ctypes.c_uint64)]
 
 
+class SgnTuneReport(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("vlc_threads", "ms_warps", "ms_blocks_per_grab", "dwt_queue")] + \
+               [(n, ctypes.c_float) for n in ("vlc_ms", "ms_ms", "dwt_ms", "vlc_ms_default", "ms_ms_default",
+                                              "dwt_ms_default")]
+
+
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
 CUDA_SIGNATURES = {
+    "sgn_plan_set_launch_shape": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
+    "sgn_plan_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                           ctypes.POINTER(SgnTuneReport)]),
     "sgn_server_create": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(SgnServerConfig),
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "sgn_server_register": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,

@@ -460,14 +460,61 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // The staging buffer is reused by the next call: finish the copies now
   // (callers that reuse it only after the plan has run pass sync_uploads false).
   if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
-  plan->launches = 1 + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0);
+  plan->launches = (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0);
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
-  return SGN_OK;
+  // Work-queue counters and the launch shape (an autotuned one when this
+  // context has tuned a plan of the same signature).
+  plan->nqueues = (uint32_t)plan->rounds.size() + 2;
+  if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
+  LaunchConfig cfg;
+  {
+    const uint64_t sig = plan_signature(plan);
+    std::lock_guard<std::mutex> g(ctx->tune_mu);
+    for (auto& t : ctx->tuned)
+      if (t.first == sig) cfg = t.second;
+  }
+  return apply_config(ctx, plan, cfg);
 }
 
 }  // namespace
 
+uint64_t plan_signature(const sgn_plan* p) {
+  auto lg = [](uint64_t v) {
+    uint64_t k = 0;
+    while (v > 1) {
+      v >>= 1;
+      ++k;
+    }
+    return k;
+  };
+  return (uint64_t)p->format | (lg(p->nht + 1) << 4) | (lg(p->max_w) << 10) | (lg(p->ms_words) << 14) |
+         (lg(p->pack_ctas + 1) << 20) | ((uint64_t)p->rounds.size() << 26) | ((uint64_t)(p->nref > 0) << 31);
+}
+
+sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
+  LaunchConfig c = in;
+  int ms = 0, idwt = 0, pack = 0;
+  cudaError_t e = ht_magsgn_occupancy(p->ms_words, p->max_w, c.ms_warps ? c.ms_warps : 8, &ms);
+  if (e == cudaSuccess) e = idwt_pack_occupancy(p->format < 5 ? p->format : 1, &idwt, &pack);
+  if (e != cudaSuccess) return cuda_status(e, "occupancy query");
+  c.ms_ctas = (uint32_t)std::max(1, ms * ctx->sm_count);
+  c.idwt_ctas = (uint32_t)std::max(1, idwt * ctx->sm_count);
+  c.pack_ctas = (uint32_t)std::max(1, pack * ctx->sm_count);
+  p->cfg = c;
+  if (p->graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+  }
+  return SGN_OK;
+}
+
 void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
+  if (p->graph) {
+    cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+  }
+  if (p->d_queue) cudaFreeAsync(p->d_queue, s);
+  p->d_queue = nullptr;
   void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
                   p->d_refine, p->d_idwt, p->d_pack, p->d_status};
   for (void* q : ptrs)
@@ -491,17 +538,54 @@ void release_plan(sgn_plan* p, cudaStream_t s) {
 
 sgn_status execute(sgn_plan* p, cudaStream_t s) {
   cudaError_t e;
+  const LaunchConfig& c = p->cfg;
   if (p->n && (e = cudaMemsetAsync(p->d_status, 0, p->n * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "status reset");
-  if ((e = launch_ht_cleanup(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s)) != cudaSuccess)
-    return cuda_status(e, "HT cleanup launch");
+  if (p->d_queue && (e = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s)) != cudaSuccess)
+    return cuda_status(e, "work queue reset");
+  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads)) != cudaSuccess)
+    return cuda_status(e, "HT VLC launch");
+  if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
+                            s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas)) != cudaSuccess)
+    return cuda_status(e, "HT MagSgn launch");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
-  for (const RoundInfo& r : p->rounds)
-    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s)) != cudaSuccess)
+  for (size_t k = 0; k < p->rounds.size(); ++k) {
+    const RoundInfo& r = p->rounds[k];
+    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.dwt_queue ? p->d_queue + 1 + k : nullptr,
+                               c.idwt_ctas)) != cudaSuccess)
       return cuda_status(e, "IDWT launch");
-  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s)) != cudaSuccess) return cuda_status(e, "pack launch");
+  }
+  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
+                       c.dwt_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas)) != cudaSuccess)
+    return cuda_status(e, "pack launch");
   return SGN_OK;
+}
+
+// Re-executions replay the plan as one CUDA graph, captured on the second
+// execution (the first one runs eagerly: one-shot plans never pay for a
+// capture).
+sgn_status execute_graph(sgn_plan* p, cudaStream_t s) {
+  ++p->executions;
+  if (!p->graph && p->executions >= 2) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e, "graph capture");
+    sgn_status st = execute(p, s);
+    e = cudaStreamEndCapture(s, &g);
+    if (st != SGN_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      p->graph = nullptr;
+      return cuda_status(e, "graph instantiate");
+    }
+  }
+  if (p->graph) return cuda_status(cudaGraphLaunch(p->graph, s), "graph launch");
+  return execute(p, s);
 }
 
 sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* first_failing) {
@@ -647,7 +731,7 @@ sgn_status sgn_plan_create(sgn_ctx* ctx, const uint8_t* const* datas, const size
 sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan) {
   if (!ctx || !plan) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
-  return execute(plan, ctx->stream);
+  return execute_graph(plan, ctx->stream);
 }
 
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
@@ -660,17 +744,25 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   auto chk = [&](cudaError_t x) {
     if (e == cudaSuccess) e = x;
   };
+  const LaunchConfig& c = p->cfg;
   chk(cudaMemsetAsync(p->d_status, 0, std::max<size_t>(p->n, 1) * sizeof(uint32_t), s));
+  if (p->d_queue) chk(cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s));
   chk(cudaEventRecord(ev[0], s));
-  chk(launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s));
+  chk(launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads));
   chk(cudaEventRecord(ev[1], s));
-  chk(launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s));
+  chk(launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s,
+                       c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas));
   chk(cudaEventRecord(ev[2], s));
   chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
   chk(cudaEventRecord(ev[3], s));
-  for (const RoundInfo& r : p->rounds) chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s));
+  for (size_t k = 0; k < p->rounds.size(); ++k) {
+    const RoundInfo& r = p->rounds[k];
+    chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.dwt_queue ? p->d_queue + 1 + k : nullptr,
+                          c.idwt_ctas));
+  }
   chk(cudaEventRecord(ev[4], s));
-  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s));
+  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
+                  c.dwt_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas));
   chk(cudaEventRecord(ev[5], s));
   chk(cudaEventSynchronize(ev[5]));
   if (e == cudaSuccess) {
@@ -679,6 +771,142 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   }
   for (auto& x : ev) cudaEventDestroy(x);
   return cuda_status(e, "timed execute");
+}
+
+}  // extern "C"
+
+namespace {
+
+// Mean device time (ms) of `reps` runs of one stage, CUDA events on s.
+template <typename F>
+float time_stage(cudaStream_t s, uint32_t reps, F launch, cudaError_t& err) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float ms = 0.f;
+  if (err == cudaSuccess) err = launch();  // warm-up
+  if (err == cudaSuccess) err = cudaEventRecord(a, s);
+  for (uint32_t r = 0; r < reps && err == cudaSuccess; ++r) err = launch();
+  if (err == cudaSuccess) err = cudaEventRecord(b, s);
+  if (err == cudaSuccess) err = cudaEventSynchronize(b);
+  if (err == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return reps ? ms / reps : ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_threads, uint32_t ms_warps,
+                                     uint32_t ms_blocks_per_grab, uint32_t dwt_queue) {
+  if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  if (vlc_threads < 32 || vlc_threads > 128 || vlc_threads % 32 || ms_warps < 1 || ms_warps > 8 || dwt_queue > 1)
+    return set_error(SGN_ERR_INVALID_ARGUMENT, "launch shape out of range");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  LaunchConfig c;
+  c.vlc_threads = vlc_threads;
+  c.ms_warps = ms_warps;
+  c.ms_gran = ms_blocks_per_grab;
+  c.dwt_queue = dwt_queue;
+  return apply_config(ctx, p, c);
+}
+
+sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_report* out) {
+  if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (reps == 0) reps = 5;
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  // Inputs of every stage in place: one full execution with the current shape.
+  sgn_status st = execute(p, s);
+  if (st != SGN_OK) return st;
+  const LaunchConfig base = p->cfg;
+  sgn_tune_report rep;
+  std::memset(&rep, 0, sizeof(rep));
+  // VLC pass: lanes per CTA.
+  const uint32_t vlc_c[] = {64, 128};
+  float best_vlc = 1e30f;
+  uint32_t vlc_threads = base.vlc_threads;
+  for (uint32_t t : vlc_c) {
+    float ms = time_stage(s, reps, [&] { return launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, t); }, e);
+    if (t == 128) rep.vlc_ms_default = ms;
+    if (e == cudaSuccess && ms < best_vlc) best_vlc = ms, vlc_threads = t;
+  }
+  // MagSgn pass: warps per CTA, grid or queue (blocks per grab).
+  struct MsC {
+    uint32_t warps, gran;
+  } ms_c[] = {{8, 0}, {4, 0}, {8, 1}, {8, 4}, {4, 1}};
+  float best_ms = 1e30f;
+  LaunchConfig cfg = base;
+  uint32_t ms_warps = base.ms_warps, ms_gran = base.ms_gran;
+  for (const MsC& m : ms_c) {
+    LaunchConfig tc = base;
+    tc.ms_warps = m.warps;
+    if (apply_config(ctx, p, tc) != SGN_OK) continue;
+    const uint32_t ctas = p->cfg.ms_ctas;
+    float ms = time_stage(s, reps, [&] {
+      cudaError_t x = cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
+      if (x != cudaSuccess) return x;
+      return launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words,
+                              p->max_w, s, m.warps, m.gran ? p->d_queue : nullptr, m.gran, ctas);
+    }, e);
+    if (m.warps == 8 && m.gran == 0) rep.ms_ms_default = ms;
+    if (e == cudaSuccess && ms < best_ms) best_ms = ms, ms_warps = m.warps, ms_gran = m.gran;
+  }
+  // IDWT levels + pack: one unit per warp, or persistent warps on a queue.
+  float best_dwt = 1e30f;
+  uint32_t dwt_queue = 0;
+  for (uint32_t q = 0; q < 2; ++q) {
+    const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
+    float ms = time_stage(s, reps, [&] {
+      cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
+      for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) {
+        const RoundInfo& r = p->rounds[k];
+        x = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q ? p->d_queue + 1 + k : nullptr, ictas);
+      }
+      if (x == cudaSuccess)
+        x = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s, q ? p->d_queue + 1 + p->rounds.size() : nullptr,
+                        pctas);
+      return x;
+    }, e);
+    if (q == 0) rep.dwt_ms_default = ms;
+    if (e == cudaSuccess && ms < best_dwt) best_dwt = ms, dwt_queue = q;
+  }
+  if (e != cudaSuccess) {
+    apply_config(ctx, p, base);
+    return cuda_status(e, "autotune");
+  }
+  cfg.vlc_threads = vlc_threads;
+  cfg.ms_warps = ms_warps;
+  cfg.ms_gran = ms_gran;
+  cfg.dwt_queue = dwt_queue;
+  st = apply_config(ctx, p, cfg);
+  if (st != SGN_OK) return st;
+  // Leave the plan's outputs consistent (the refinement pass is not
+  // idempotent when a stage runs alone).
+  st = execute(p, s);
+  if (st == SGN_OK) st = cuda_status(cudaStreamSynchronize(s), "autotune");
+  {
+    const uint64_t sig = plan_signature(p);
+    std::lock_guard<std::mutex> tg(ctx->tune_mu);
+    bool found = false;
+    for (auto& t : ctx->tuned)
+      if (t.first == sig) t.second = p->cfg, found = true;
+    if (!found) ctx->tuned.emplace_back(sig, p->cfg);
+  }
+  rep.vlc_threads = cfg.vlc_threads;
+  rep.ms_warps = cfg.ms_warps;
+  rep.ms_blocks_per_grab = cfg.ms_gran;
+  rep.dwt_queue = cfg.dwt_queue;
+  rep.vlc_ms = best_vlc;
+  rep.ms_ms = best_ms;
+  rep.dwt_ms = best_dwt;
+  if (out) *out = rep;
+  return st;
 }
 
 sgn_status sgn_plan_wait(sgn_ctx* ctx, sgn_plan* plan, sgn_status* per_tile, size_t* first_failing) {

@@ -122,6 +122,16 @@ struct PinnedBuffer {
 }  // namespace rt
 }  // namespace sgn
 
+// Launch shape of a plan's kernels, chosen by the autotuner.
+struct LaunchConfig {
+  uint32_t vlc_threads = 128;  // lanes (code blocks) per CTA of the VLC pass
+  uint32_t ms_warps = 8;       // warps (code blocks in flight) per CTA of the MagSgn pass
+  uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
+  uint32_t dwt_queue = 0;      // 0: one unit per warp; 1: persistent warps take IDWT/pack units from a queue
+  // Persistent grid sizes (SMs x resident CTAs), derived from the above.
+  uint32_t ms_ctas = 0, idwt_ctas = 0, pack_ctas = 0;
+};
+
 struct sgn_ctx {
   int device = 0;
   int sm_count = 0;
@@ -130,6 +140,9 @@ struct sgn_ctx {
   std::mutex mu;
   sgn::rt::PinnedBuffer staging;
   sgn::rt::Workers* workers = nullptr;
+  // Autotuned launch shapes by workload signature (see plan_signature).
+  std::mutex tune_mu;
+  std::vector<std::pair<uint64_t, LaunchConfig>> tuned;
 };
 
 struct RoundInfo {
@@ -161,6 +174,14 @@ struct sgn_plan {
   uint64_t launches = 0;
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
+  // Launch shape and the device work-queue counters (one per queued launch:
+  // MagSgn, each IDWT round, pack), zeroed at the start of every execution.
+  LaunchConfig cfg;
+  uint32_t* d_queue = nullptr;
+  uint32_t nqueues = 0;
+  // The execution captured as a CUDA graph (made on the second execution).
+  cudaGraphExec_t graph = nullptr;
+  uint64_t executions = 0;
 };
 
 
@@ -189,6 +210,12 @@ sgn_status execute(sgn_plan* p, cudaStream_t s);
 // Reads the per-tile device status (synchronising s) and merges host statuses.
 sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* first_failing);
 void free_plan_buffers(sgn_plan* p, cudaStream_t s);
+// Fills in the persistent grid sizes of cfg for the plan's kernels and
+// device, and makes it the plan's launch shape (dropping any captured graph).
+sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& cfg);
+// Workload signature for the autotuner cache: pixel format, job counts and
+// block shape classes.
+uint64_t plan_signature(const sgn_plan* p);
 // Frees the plan's surfaces that are still owned by it, then its buffers.
 void release_plan(sgn_plan* p, cudaStream_t s);
 

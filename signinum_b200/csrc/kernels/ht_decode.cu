@@ -16,6 +16,7 @@
 //     whole rows with coalesced stores.
 // Refinement passes (SigProp/MagRef) run in ht_refine_kernel for the few
 // blocks that carry them.
+#include <algorithm>
 #include <cstdint>
 
 #include "../device_plan.h"
@@ -609,20 +610,15 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
 // shared memory), each lane sums its samples' m_n, a warp prefix scan turns
 // the sums into bit offsets inside the unstuffed MagSgn stream, and the row
 // is written with coalesced stores.
-__global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
-                                                                  const uint8_t* __restrict__ arena,
-                                                                  const uint32_t* __restrict__ symbols,
-                                                                  int32_t* __restrict__ coef,
-                                                                  uint32_t* __restrict__ tile_status,
-                                                                  uint32_t ms_words, uint32_t max_w) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t cols = max_w + 4;
-  uint32_t* W = reinterpret_cast<uint32_t*>(smem) + (size_t)warp * ms_words;
-  uint8_t* Ebase = smem + (size_t)kMsWarps * ms_words * 4 + (size_t)warp * 2 * cols;
-  const uint32_t j = blockIdx.x * kMsWarps + warp;
-  if (j >= njobs) return;
-  const HtJob job = jobs[j];
+namespace {
+
+// Magnitudes and signs of one code block by the calling warp; W and Ebase
+// are the warp's shared-memory bit array and exponent rows.
+__device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena,
+                             const uint32_t* __restrict__ symbols, int32_t* __restrict__ coef,
+                             uint32_t* __restrict__ tile_status, uint32_t ms_words, uint32_t cols, uint32_t* W,
+                             uint8_t* Ebase) {
+  const uint32_t lane = threadIdx.x & 31;
   int32_t* dst = coef + job.dst;
   const uint32_t w = job.w, h = job.h, stride = job.stride;
   if (job.passes == 0) {
@@ -650,6 +646,43 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
     for (uint32_t y = 0; y < h; ++y)
       for (uint32_t x = lane; x < w; x += 32) dst[(size_t)y * stride + x] = 0;
     if (lane == 0) atomicOr(&tile_status[job.tile], kStatusDecode);
+  }
+  __syncwarp();  // the warp's shared buffers are reused by its next block
+}
+
+}  // namespace
+
+// Pass 2: one warp per code block decodes magnitudes and signs
+// (decode_magnitude_sign_phase, ht_block_decode.rs:1435-1561).  Grid form
+// (queue == nullptr): warp k of CTA c takes block c * warps + k.  Queue form:
+// a persistent grid whose warps take `gran` consecutive blocks at a time
+// from the device work queue (an atomic counter over the job table, which is
+// ordered by coded length, longest first).
+__global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
+                                                                  const uint8_t* __restrict__ arena,
+                                                                  const uint32_t* __restrict__ symbols,
+                                                                  int32_t* __restrict__ coef,
+                                                                  uint32_t* __restrict__ tile_status,
+                                                                  uint32_t ms_words, uint32_t max_w, uint32_t* queue,
+                                                                  uint32_t gran) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const uint32_t nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t cols = max_w + 4;
+  uint32_t* W = reinterpret_cast<uint32_t*>(smem) + (size_t)warp * ms_words;
+  uint8_t* Ebase = smem + (size_t)nw * ms_words * 4 + (size_t)warp * 2 * cols;
+  if (!queue) {
+    const uint32_t j = blockIdx.x * nw + warp;
+    if (j < njobs) magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+    return;
+  }
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(queue, gran);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= njobs) break;
+    const uint32_t end = min(base + gran, njobs);
+    for (uint32_t j = base; j < end; ++j)
+      magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
   }
 }
 
@@ -839,8 +872,8 @@ __global__ void ht_refine_kernel(const HtJob* __restrict__ jobs, const uint32_t*
   }
 }
 
-size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w) {
-  return (size_t)kMsWarps * ms_words * 4 + (size_t)kMsWarps * 2 * (max_w + 4);
+size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps) {
+  return (size_t)warps * ms_words * 4 + (size_t)warps * 2 * (max_w + 4);
 }
 
 cudaError_t ht_kernels_init() {
@@ -848,29 +881,44 @@ cudaError_t ht_kernels_init() {
 }
 
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, uint32_t threads) {
   if (njobs == 0) return cudaSuccess;
-  ht_vlc_kernel<<<(njobs + kHtThreads - 1) / kHtThreads, kHtThreads, 0, stream>>>(jobs, njobs, arena, symbols);
+  if (threads == 0 || threads > kHtThreads || threads % 32) threads = kHtThreads;
+  ht_vlc_kernel<<<(njobs + threads - 1) / threads, threads, 0, stream>>>(jobs, njobs, arena, symbols);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, uint32_t warps, uint32_t* queue, uint32_t gran,
+                             uint32_t persistent_ctas) {
   if (njobs == 0) return cudaSuccess;
-  size_t smem = ht_magsgn_smem_bytes(ms_words, max_w);
+  if (warps == 0 || warps > kMsWarps) warps = kMsWarps;
+  size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, warps);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  ht_magsgn_kernel<<<(njobs + kMsWarps - 1) / kMsWarps, kMsWarps * 32, smem, stream>>>(
-      jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w);
+  uint32_t ctas = (njobs + warps - 1) / warps;
+  if (queue) {
+    if (gran == 0) gran = 1;
+    ctas = std::max(1u, std::min(ctas, persistent_ctas));
+  }
+  ht_magsgn_kernel<<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status, ms_words,
+                                                        max_w, queue, gran);
   return cudaGetLastError();
+}
+
+cudaError_t ht_magsgn_occupancy(uint32_t ms_words, uint32_t max_w, uint32_t warps, int* ctas_per_sm) {
+  if (warps == 0 || warps > kMsWarps) warps = kMsWarps;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, ht_magsgn_kernel, warps * 32,
+                                                       ht_magsgn_smem_bytes(ms_words, max_w, warps));
 }
 
 cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                               int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                               cudaStream_t stream) {
-  cudaError_t e = launch_ht_vlc(jobs, njobs, arena, symbols, stream);
+  cudaError_t e = launch_ht_vlc(jobs, njobs, arena, symbols, stream, kHtThreads);
   if (e != cudaSuccess) return e;
-  return launch_ht_magsgn(jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w, stream);
+  return launch_ht_magsgn(jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w, stream, kMsWarps, nullptr,
+                          0, 0);
 }
 
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,

@@ -27,6 +27,7 @@
 // :2202-2294; crates/signinum-j2k/src/decode.rs:345-356, :517-545); each lane
 // packs its four pixels into 32-bit words, the words of a row are staged per
 // warp in shared memory and the row is written with 16-byte stores.
+#include <algorithm>
 #include <cstdint>
 
 #include "../device_plan.h"
@@ -210,10 +211,25 @@ __device__ __forceinline__ const Job& find_job(const Job* jobs, uint32_t njobs, 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJob* __restrict__ jobs,
-                                                                     uint32_t njobs, uint32_t nunits) {
-  const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
-  if (unit >= nunits) return;
+namespace {
+
+// Next work unit of the calling warp: the grid form takes one unit per warp;
+// the queue form (persistent grid) takes units from a device counter until
+// they run out.  Returns false when the warp is done.
+__device__ __forceinline__ bool next_unit(uint32_t* queue, uint32_t nunits, bool& first, uint32_t& unit) {
+  if (!queue) {
+    unit = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const bool go = first && unit < nunits;
+    first = false;
+    return go;
+  }
+  uint32_t u = 0;
+  if ((threadIdx.x & 31) == 0) u = atomicAdd(queue, 1u);
+  unit = __shfl_sync(0xFFFFFFFFu, u, 0);
+  return unit < nunits;
+}
+
+__device__ __forceinline__ void idwt_unit(const IdwtJob* __restrict__ jobs, uint32_t njobs, uint32_t unit) {
   const int lane = threadIdx.x & 31;
   const IdwtJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
@@ -237,6 +253,23 @@ __global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJ
       if (col + 3 < w) row[col + 3] = v[0].w;
     }
   });
+}
+
+}  // namespace
+
+// QUEUE: persistent grid taking units from the device counter `queue`;
+// otherwise one unit per warp.
+template <bool QUEUE>
+__global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJob* __restrict__ jobs,
+                                                                     uint32_t njobs, uint32_t nunits,
+                                                                     uint32_t* queue) {
+  if (!QUEUE) {
+    const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
+    if (unit < nunits) idwt_unit(jobs, njobs, unit);
+    return;
+  }
+  bool first = true;
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);) idwt_unit(jobs, njobs, unit);
 }
 
 namespace {
@@ -401,12 +434,8 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
 }  // namespace
 
 template <int FMT>
-__global__ void __launch_bounds__(kIdwtWarps * 32, 2) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
-                                                               uint32_t nunits) {
-  __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
-  const uint32_t warp = threadIdx.x >> 5;
-  const uint32_t unit = blockIdx.x * kIdwtWarps + warp;
-  if (unit >= nunits) return;
+__device__ __forceinline__ void pack_one(const PackJob* __restrict__ jobs, uint32_t njobs, uint32_t unit,
+                                         uint32_t* rowbuf) {
   const int lane = threadIdx.x & 31;
   const PackJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
@@ -416,32 +445,78 @@ __global__ void __launch_bounds__(kIdwtWarps * 32, 2) pack_kernel(const PackJob*
   constexpr bool kU8 = FMT == PACK_GRAY8 || FMT == PACK_RGB8 || FMT == PACK_RGBA8;
   const bool direct = kU8 ? job.bit_depth == 8 : job.bit_depth > 8;
   if (job.ncomp >= 3) {
-    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbufs[warp]);
-    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbufs[warp]);
+    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbuf);
+    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbuf);
   } else {
-    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbufs[warp]);
-    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbufs[warp]);
+    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbuf);
+    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbuf);
   }
 }
 
-cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream) {
+template <int FMT, bool QUEUE>
+__global__ void __launch_bounds__(kIdwtWarps * 32, 2) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+                                                               uint32_t nunits, uint32_t* queue) {
+  __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
+  uint32_t* rowbuf = rowbufs[threadIdx.x >> 5];
+  if (!QUEUE) {
+    const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
+    if (unit < nunits) pack_one<FMT>(jobs, njobs, unit, rowbuf);
+    return;
+  }
+  bool first = true;
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);) pack_one<FMT>(jobs, njobs, unit, rowbuf);
+}
+
+cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
+                              uint32_t* queue, uint32_t persistent_ctas) {
   if (njobs == 0 || nunits == 0) return cudaSuccess;
-  idwt_level_kernel<<<(nunits + kIdwtWarps - 1) / kIdwtWarps, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits);
+  uint32_t ctas = (nunits + kIdwtWarps - 1) / kIdwtWarps;
+  if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
+  if (queue) idwt_level_kernel<true><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, queue);
+  else idwt_level_kernel<false><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, nullptr);
   return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream) {
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
+                        uint32_t* queue, uint32_t persistent_ctas) {
   if (njobs == 0 || nunits == 0) return cudaSuccess;
-  const dim3 grid((nunits + kIdwtWarps - 1) / kIdwtWarps), block(kIdwtWarps * 32);
+  uint32_t ctas = (nunits + kIdwtWarps - 1) / kIdwtWarps;
+  if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
+  const dim3 grid(ctas), block(kIdwtWarps * 32);
+#define SGN_PACK_LAUNCH(F)                                                                   \
+  case F:                                                                                     \
+    if (queue) pack_kernel<F, true><<<grid, block, 0, stream>>>(jobs, njobs, nunits, queue); \
+    else pack_kernel<F, false><<<grid, block, 0, stream>>>(jobs, njobs, nunits, nullptr);    \
+    break;
   switch (fmt) {
-    case PACK_GRAY8: pack_kernel<PACK_GRAY8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
-    case PACK_RGB8: pack_kernel<PACK_RGB8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
-    case PACK_RGBA8: pack_kernel<PACK_RGBA8><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
-    case PACK_GRAY16: pack_kernel<PACK_GRAY16><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
-    case PACK_RGB16: pack_kernel<PACK_RGB16><<<grid, block, 0, stream>>>(jobs, njobs, nunits); break;
+    SGN_PACK_LAUNCH(PACK_GRAY8)
+    SGN_PACK_LAUNCH(PACK_RGB8)
+    SGN_PACK_LAUNCH(PACK_RGBA8)
+    SGN_PACK_LAUNCH(PACK_GRAY16)
+    SGN_PACK_LAUNCH(PACK_RGB16)
     default: return cudaErrorInvalidValue;
   }
+#undef SGN_PACK_LAUNCH
   return cudaGetLastError();
+}
+
+cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm) {
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(idwt_ctas_per_sm, idwt_level_kernel<true>,
+                                                                kIdwtWarps * 32, 0);
+  if (e != cudaSuccess) return e;
+  switch (fmt) {
+    case PACK_GRAY8:
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_GRAY8, true>, kIdwtWarps * 32, 0);
+    case PACK_RGB8:
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGB8, true>, kIdwtWarps * 32, 0);
+    case PACK_RGBA8:
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGBA8, true>, kIdwtWarps * 32, 0);
+    case PACK_GRAY16:
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_GRAY16, true>, kIdwtWarps * 32, 0);
+    case PACK_RGB16:
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGB16, true>, kIdwtWarps * 32, 0);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace sgn

@@ -15,23 +15,33 @@ cudaError_t ht_kernels_init();
 // Uploads the HT tables and sets kernel attributes on `device` (current) once.
 cudaError_t ensure_device_init(int device);
 cudaError_t upload_ht_tables(const HtDecodeTables& host);
-size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w);
-// HT cleanup: the VLC pass (one lane per block) then the MagSgn pass (one
-// warp per block).  ms_words: unstuffed MagSgn capacity per block in 32-bit
-// words; max_w: widest code block of the launch.
+size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps = 8);
+// HT cleanup: the VLC pass (one lane per block, `threads` lanes per CTA) then
+// the MagSgn pass (one warp per block, `warps` warps per CTA).  ms_words:
+// unstuffed MagSgn capacity per block in 32-bit words; max_w: widest code
+// block of the launch.  With `queue` (a zeroed device counter) the MagSgn pass
+// runs as a persistent grid of at most persistent_ctas CTAs whose warps take
+// `gran` blocks per grab.
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                          cudaStream_t stream);
+                          cudaStream_t stream, uint32_t threads = 128);
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
-                             cudaStream_t stream);
+                             cudaStream_t stream, uint32_t warps = 8, uint32_t* queue = nullptr, uint32_t gran = 0,
+                             uint32_t persistent_ctas = 0);
+cudaError_t ht_magsgn_occupancy(uint32_t ms_words, uint32_t max_w, uint32_t warps, int* ctas_per_sm);
 cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                               int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                               cudaStream_t stream);
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,
                              uint32_t* tile_status, cudaStream_t stream);
-// nunits: work units (strip x row segment) of all jobs of the launch.
-cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream);
+// nunits: work units (strip x row segment) of all jobs of the launch.  With
+// `queue` (a zeroed device counter) the kernels run as a persistent grid of
+// at most persistent_ctas CTAs whose warps take units from the counter.
+cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
+                              uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
 // All jobs of one launch share the pixel format fmt (a PackFormat).
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream);
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
+                        uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
+cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm);
 
 }  // namespace sgn

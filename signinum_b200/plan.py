@@ -53,6 +53,19 @@ class Plan:
         st = _native.cuda_lib().sgn_plan_wait(self.ctx.handle, self.handle, per, ctypes.byref(first))
         return st, list(per)
 
+    def autotune(self, reps: int = 5) -> dict:
+        """Times candidate launch shapes on this plan's data and keeps the fastest
+        (sgn_plan_autotune); returns the chosen shape and stage times."""
+        from ._native import SgnTuneReport
+
+        r = SgnTuneReport()
+        _check(_native.cuda_lib().sgn_plan_autotune(self.ctx.handle, self.handle, reps, ctypes.byref(r)))
+        return {n: getattr(r, n) for n, _ in SgnTuneReport._fields_}
+
+    def set_launch_shape(self, vlc_threads=128, ms_warps=8, ms_blocks_per_grab=0, dwt_queue=0):
+        _check(_native.cuda_lib().sgn_plan_set_launch_shape(self.ctx.handle, self.handle, vlc_threads, ms_warps,
+                                                            ms_blocks_per_grab, dwt_queue))
+
     def execute_timed(self):
         """Per-stage milliseconds: HT VLC pass, HT MagSgn pass, HT refinement, IDWT levels,
         last level + pack, total."""

@@ -1,0 +1,56 @@
+"""GPU: every launch shape of a batch plan (grid or persistent work-queue
+kernels), graph replay and the autotuner's choice decode bit-exactly."""
+import pytest
+
+from oracle import oracle
+from signinum_b200 import PixelFormat, encode
+from signinum_b200.plan import Plan
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [
+    (128, 8, 0, 0),  # default: one block / unit per warp
+    (64, 4, 0, 0),
+    (128, 8, 1, 1),  # persistent MagSgn (1 block per grab) and IDWT/pack queues
+    (96, 4, 4, 1),   # persistent MagSgn, 4 blocks per grab
+    (32, 1, 2, 0),
+]
+
+
+@pytest.fixture(scope="module")
+def batch():
+    # Uneven tiles (sizes, block sizes, near-blank) to exercise the queues.
+    return encode.config2(n=10).tiles
+
+
+def _want(tiles):
+    return [oracle.decode(t.codestream, int(PixelFormat.Rgb8))[0] for t in tiles]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=[f"vlc{a}_ms{b}x{c}_dwtq{d}" for a, b, c, d in SHAPES])
+def test_launch_shapes_are_bit_exact(batch, shape):
+    want = _want(batch)
+    plan = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
+    plan.set_launch_shape(*shape)
+    for rep in range(3):  # eager, graph capture, graph replay
+        plan.execute_async()
+        st, per = plan.wait()
+        assert st == 0 and per == [0] * len(batch)
+        for i in (0, len(batch) // 2, len(batch) - 1):
+            assert plan.download(i) == want[i], f"tile {i}, execution {rep}"
+    assert [plan.download(i) for i in range(len(batch))] == want
+    plan.destroy()
+
+
+def test_autotune_keeps_output_and_is_reused(batch):
+    want = _want(batch)
+    plan = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
+    rep = plan.autotune(2)
+    assert rep["vlc_threads"] in (64, 128) and rep["ms_warps"] in (4, 8) and rep["dwt_queue"] in (0, 1)
+    assert rep["vlc_ms"] > 0 and rep["ms_ms"] > 0 and rep["dwt_ms"] > 0
+    assert [plan.download(i) for i in range(len(batch))] == want
+    for _ in range(3):
+        plan.execute_async()
+    st, _ = plan.wait()
+    assert st == 0 and [plan.download(i) for i in range(len(batch))] == want
+    plan.destroy()
