@@ -432,6 +432,24 @@ def run_serving(args):
         print(json.dumps(line), flush=True)
 
 
+def reduce_max(dist, x, device):
+    """Max of a per-rank scalar over all ranks (the timed region's duration is
+    the slowest replica's); identity without a process group."""
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, ms):
+    """Whole-job rate (units/s, in millions) of `world` replicas that each
+    processed units_per_rank in `ms` milliseconds (max over ranks)."""
+    return world * units_per_rank / (ms / 1000.0) / 1e6
+
+
 def traffic_for(workload, kernel):
     """dram bytes per launch of `kernel` from the committed ncu summary."""
     p = ROOT / "profiles" / "dram_traffic.txt"
@@ -493,11 +511,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        tt = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return reduce_max(dist, x, "cuda")
 
     # ---- Batched, device-resident (value).
     plan = Plan(lens, fmt, ctx=ctx, contiguous=host, offsets=offs)
@@ -524,7 +538,7 @@ def main():
     batched_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     stage = np.mean(np.array(stages), axis=0)  # VLC, MagSgn, refine, IDWT, pack, total
     launches = plan.launches * args.steps
-    value = world * pixels / (batched_ms / 1000.0) / 1e6
+    value = replica_throughput(world, pixels, batched_ms)
     # Parity spot check of the benchmark output against the oracle.
     check = None
     if rank == 0:
