@@ -655,6 +655,14 @@ sgn_status sgn_ctx_create(int device, sgn_ctx** out) {
     delete c;
     return cuda_status(tables_err, "HT table upload");
   }
+  for (auto& l : c->lanes)
+    if ((e = cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking)) != cudaSuccess) {
+      for (auto& x : c->lanes)
+        if (x) cudaStreamDestroy(x);
+      cudaStreamDestroy(c->stream);
+      delete c;
+      return cuda_status(e, "cudaStreamCreate");
+    }
   unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   c->workers = new Workers(std::min(hw, 32u) - 1);
   *out = c;
@@ -666,6 +674,10 @@ void sgn_ctx_destroy(sgn_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaStreamDestroy(ctx->stream);
+  for (auto& l : ctx->lanes) {
+    cudaStreamSynchronize(l);
+    cudaStreamDestroy(l);
+  }
   delete ctx->workers;
   delete ctx;
 }
@@ -980,6 +992,20 @@ void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan) {
   delete plan;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Frees a surface on the context stream; ctx->mu is held by the caller.
+void sgn_surface_free_locked(sgn_ctx* ctx, sgn_surface* sf) {
+  cudaFreeAsync((void*)(uintptr_t)sf->device_ptr, ctx->stream);
+  sf->device_ptr = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
 sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
                                           uint32_t format, const sgn_request* requests, uint32_t backend,
                                           sgn_surface* outs, sgn_status* per_tile, size_t* first_failing) {
@@ -989,26 +1015,75 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
   if (first_failing) *first_failing = SIZE_MAX;
   for (size_t i = 0; i < n; ++i) outs[i] = sgn_surface{};
   if (n == 0) return SGN_OK;
-  sgn_plan* p = nullptr;
-  sgn_status st = sgn_plan_create(ctx, datas, lens, n, format, requests, &p, nullptr);
-  if (st != SGN_OK) return st;
   std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
   ctx->submissions.fetch_add(1);
-  st = execute(p, ctx->stream);
-  std::vector<sgn_status> statuses(n);
-  sgn_status wst = st == SGN_OK ? wait_plan(p, ctx->stream, statuses.data(), first_failing) : st;
-  for (size_t i = 0; i < n; ++i) {
-    if (per_tile) per_tile[i] = st == SGN_OK ? statuses[i] : st;
-    if (st == SGN_OK && statuses[i] == SGN_OK) {
-      outs[i] = p->surfaces[i];
-      p->surfaces[i].device_ptr = 0;  // ownership moves to the caller
+  // Pipelined: large batches are cut into up to four chunks of about equal
+  // coded bytes, each a plan on its own stream with its own staging, built
+  // and launched in turn, so the upload of chunk c overlaps the kernels of
+  // chunk c - 1 and the host parse of chunk c + 1.
+  uint64_t total = 0;
+  for (size_t i = 0; i < n; ++i) total += lens[i];
+  const size_t K = std::min<size_t>(total >= (48ull << 20) ? 4 : total >= (12ull << 20) ? 2 : 1, std::max<size_t>(1, n / 2));
+  std::vector<size_t> cut(K + 1, n);
+  cut[0] = 0;
+  {
+    uint64_t acc = 0;
+    size_t c = 1;
+    for (size_t i = 0; i < n && c < K; ++i) {
+      acc += lens[i];
+      if (acc * K >= total * c) cut[c++] = i + 1;
     }
   }
-  for (auto& sf : p->surfaces)
-    if (sf.device_ptr) cudaFreeAsync((void*)(uintptr_t)sf.device_ptr, ctx->stream);
-  p->surfaces.clear();
-  free_plan_buffers(p, ctx->stream);
-  delete p;
+  std::vector<sgn_plan*> plans(K, nullptr);
+  std::vector<sgn_status> statuses(n, SGN_OK);
+  sgn_status st = SGN_OK;
+  for (size_t c = 0; c < K && st == SGN_OK; ++c) {
+    const size_t b = cut[c], m = cut[c + 1] - b;
+    if (m == 0) continue;
+    plans[c] = new sgn_plan();
+    try {
+      st = build_plan(ctx, ctx->lanes[c], ctx->lane_staging[c], datas + b, lens + b, m, format,
+                      requests ? requests + b : nullptr, plans[c], nullptr, nullptr, nullptr, false);
+    } catch (const std::bad_alloc&) {
+      st = set_error(SGN_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    if (st == SGN_OK) st = execute(plans[c], ctx->lanes[c]);
+  }
+  sgn_status wst = SGN_OK;
+  size_t first = SIZE_MAX;
+  for (size_t c = 0; c < K; ++c) {
+    if (!plans[c]) continue;
+    const size_t b = cut[c];
+    size_t f = SIZE_MAX;
+    if (st == SGN_OK) {
+      wait_plan(plans[c], ctx->lanes[c], statuses.data() + b, &f);
+      if (f != SIZE_MAX && first == SIZE_MAX) {
+        first = b + f;
+        wst = statuses[b + f];
+      }
+      for (size_t i = 0; i < plans[c]->n; ++i)
+        if (statuses[b + i] == SGN_OK) {
+          outs[b + i] = plans[c]->surfaces[i];
+          plans[c]->surfaces[i].device_ptr = 0;  // ownership moves to the caller
+        }
+    } else {
+      cudaStreamSynchronize(ctx->lanes[c]);
+    }
+    release_plan(plans[c], ctx->lanes[c]);
+    delete plans[c];
+  }
+  if (st != SGN_OK) {
+    for (size_t i = 0; i < n; ++i) {
+      if (outs[i].device_ptr) sgn_surface_free_locked(ctx, &outs[i]);
+      if (per_tile) per_tile[i] = st;
+    }
+    return st;
+  }
+  if (per_tile)
+    for (size_t i = 0; i < n; ++i) per_tile[i] = statuses[i];
+  if (first_failing) *first_failing = first;
+  if (wst != SGN_OK) set_error(wst, "tile decode failed");
   return wst;
 }
 

@@ -140,6 +140,11 @@ struct sgn_ctx {
   std::mutex mu;
   sgn::rt::PinnedBuffer staging;
   sgn::rt::Workers* workers = nullptr;
+  // Streams and pinned staging of the pipelined batch call (one per chunk):
+  // chunk c's codestream upload overlaps the kernels of chunk c - 1.
+  static constexpr int kLanes = 4;
+  cudaStream_t lanes[kLanes] = {};
+  sgn::rt::PinnedBuffer lane_staging[kLanes];
   // Autotuned launch shapes by workload signature (see plan_signature).
   std::mutex tune_mu;
   std::vector<std::pair<uint64_t, LaunchConfig>> tuned;
