@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <array>
 #include <cstdio>
+#include <string>
 #include <tuple>
 #include <cmath>
 #include <cstring>
@@ -1322,7 +1323,115 @@ static void convert(const Planes& p, int fmt, bool region, uint32_t rx, uint32_t
     }
 }
 
+// JP2 container: parse_image_info / parse_jp2 / parse_jp2h / parse_colr /
+// read_box_header (crates/signinum-j2k/src/parse/mod.rs:17-31,
+// parse/boxes.rs:10-245).  Returns the codestream range; raw codestreams
+// are passed through.
+struct Jp2 {
+  size_t off = 0, len = 0;
+  bool jp2 = false;
+  int colr = -1;         // enumerated colour space; -2 ICC / other method
+  bool channels = false; // pclr / cmap / cdef in jp2h
+};
+
+static uint32_t rd_be32(const uint8_t* p) {
+  return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | (uint32_t)p[3];
+}
+
+static void read_box(const uint8_t* d, size_t n, size_t at, char type[5], size_t& body, size_t& end) {
+  if (at + 8 > n) fail(ERR_TRUNCATED, "box header truncated");
+  uint32_t l = rd_be32(d + at);
+  std::memcpy(type, d + at + 4, 4);
+  type[4] = 0;
+  body = at + 8;
+  if (l == 0) {
+    end = n;
+  } else if (l == 1) {
+    if (at + 16 > n) fail(ERR_TRUNCATED, "extended box header truncated");
+    uint64_t x = ((uint64_t)rd_be32(d + at + 8) << 32) | rd_be32(d + at + 12);
+    if (x < 16) fail(ERR_DECODE, "extended box length smaller than header");
+    body = at + 16;
+    end = at + (size_t)x;
+  } else if (l < 8) {
+    fail(ERR_DECODE, "box length smaller than header");
+  } else {
+    end = at + l;
+  }
+}
+
+static Jp2 container(const uint8_t* d, size_t n) {
+  static const uint8_t sig[12] = {0, 0, 0, 12, 'j', 'P', ' ', ' ', 0x0D, 0x0A, 0x87, 0x0A};
+  Jp2 j;
+  if (n >= 8 && std::memcmp(d, sig, 8) == 0) {
+    if (n < 12) fail(ERR_TRUNCATED, "too short for the JP2 signature");
+    bool have_sig = false, have_ftyp = false, have_jp2h = false, have_ihdr = false, have_jp2c = false;
+    size_t at = 0;
+    while (at < n) {
+      char t[5];
+      size_t body, end;
+      read_box(d, n, at, t, body, end);
+      if (end > n) fail(ERR_TRUNCATED, "box payload truncated");
+      const std::string type(t);
+      if (type == "jP  ") {
+        if (have_sig || at != 0) fail(ERR_DECODE, "signature box must appear exactly once at the start");
+        if (end - body != 4 || std::memcmp(d + body, sig + 8, 4) != 0) fail(ERR_DECODE, "invalid JP2 signature");
+        have_sig = true;
+      } else if (type == "ftyp") {
+        if (!have_sig || have_ftyp || have_jp2h || have_jp2c) fail(ERR_DECODE, "misplaced ftyp");
+        if (end - body < 8) fail(ERR_DECODE, "ftyp payload shorter than 8 bytes");
+        have_ftyp = true;
+      } else if (type == "jp2h") {
+        if (!have_ftyp || have_jp2h || have_jp2c) fail(ERR_DECODE, "misplaced jp2h");
+        const uint8_t* h = d + body;
+        const size_t hn = end - body;
+        size_t ia = 0;
+        while (ia < hn) {
+          char it[5];
+          size_t ib, ie;
+          read_box(h, hn, ia, it, ib, ie);
+          if (ie > hn) ie = hn;
+          const std::string itype(it);
+          const size_t len = ie > ib ? ie - ib : 0;
+          if (itype == "ihdr") {
+            if (len < 14) fail(ERR_DECODE, "ihdr payload shorter than 14 bytes");
+            have_ihdr = true;
+          } else if (itype == "colr" && len >= 3) {
+            if (h[ib] == 1 && len >= 7) j.colr = (int)rd_be32(h + ib + 3);
+            else if (h[ib] == 2) j.colr = -2;
+          } else if (itype == "pclr" || itype == "cmap" || itype == "cdef") {
+            j.channels = true;
+          }
+          ia = ie;
+        }
+        have_jp2h = true;
+      } else if (type == "jp2c") {
+        if (!have_jp2h || have_jp2c) fail(ERR_DECODE, "misplaced jp2c");
+        j.off = body;
+        j.len = end - body;
+        have_jp2c = true;
+      }
+      at = end;
+    }
+    if (!have_ftyp || !have_jp2h || !have_ihdr || !have_jp2c) fail(ERR_DECODE, "missing required JP2 box");
+    j.jp2 = true;
+    return j;
+  }
+  if (n >= 4 && d[0] == 0xFF && d[1] == 0x4F && d[2] == 0xFF && d[3] == 0x51) {
+    j.len = n;
+    return j;
+  }
+  fail(ERR_UNSUPPORTED, "input is not a JP2 container or raw JPEG 2000 codestream");
+  return j;
+}
+
+static Info inspect_raw(const uint8_t* data, size_t len);
+
 Info inspect(const uint8_t* data, size_t len) {
+  const Jp2 j = container(data, len);
+  return inspect_raw(data + j.off, j.len);
+}
+
+static Info inspect_raw(const uint8_t* data, size_t len) {
   BitReader r(data, len);
   uint8_t m;
   if (len < 4 || data[0] != 0xFF || data[1] != 0x4F || data[2] != 0xFF || data[3] != 0x51)
@@ -1347,7 +1456,10 @@ void decode(const uint8_t* data, size_t len, int fmt, const Request& req, std::v
             uint32_t& out_w, uint32_t& out_h) {
   if (fmt == FMT_RGBA16) fail(ERR_UNSUPPORTED, "Rgba16 output is not supported");
   if (fmt < 0 || fmt > FMT_RGBA16) fail(ERR_UNSUPPORTED, "unknown pixel format");
-  Info info = inspect(data, len);
+  const Jp2 j = container(data, len);
+  data += j.off;
+  len = j.len;
+  Info info = inspect_raw(data, len);
   uint32_t W = info.width, H = info.height;
   // DeviceDecodePlan::for_image, crates/signinum-j2k/src/adapter/device_plan.rs:23-51.
   uint32_t sx = 0, sy = 0, sw = W, sh = H, d = 1;
@@ -1361,6 +1473,13 @@ void decode(const uint8_t* data, size_t len, int fmt, const Request& req, std::v
   uint32_t ox0 = sx / d, oy0 = sy / d, ox1 = div_ceil(sx + sw, d), oy1 = div_ceil(sy + sh, d);
   out_w = ox1 - ox0;
   out_h = oy1 - oy0;
+  // write_components_u8_output / write_u16_output (crates/signinum-j2k/src/
+  // decode.rs:235-273, :430-470): the decoded colour space must map onto the
+  // format; from a JP2 colr box only sRGB (3 components) and greyscale (1)
+  // map here.
+  if (j.jp2 && (j.channels || (j.colr != -1 && !((j.colr == 16 && info.components == 3) ||
+                                                  (j.colr == 17 && info.components == 1)))))
+    fail(ERR_UNSUPPORTED, "backend color space cannot be mapped to the requested pixel format");
   Planes p;
   if (d == 1) {
     decode_codestream(data, len, nullptr, p);

@@ -324,7 +324,147 @@ struct Packet {  // one (component, resolution, precinct)
 
 }  // namespace
 
+namespace {
+
+Info inspect_raw(const uint8_t* data, size_t len);
+void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, TileLayout& T);
+
+// ---------------------------------------------------------------------------
+// JP2 container (crates/signinum-j2k/src/parse/boxes.rs:10-245,
+// parse/mod.rs:17-31): the box order rules, and what of the colour
+// specification the decode path can honour.
+
+struct Container {
+  size_t off = 0, len = 0;  // the codestream inside the input
+  bool jp2 = false;
+  int colr = -1;            // enumerated colour space of the colr box, -1 none, -2 ICC / other method
+  bool channel_boxes = false;  // pclr / cmap / cdef present in jp2h
+};
+
+struct BoxHeader {
+  uint32_t type;
+  size_t payload, end;
+};
+
+uint32_t be32(const uint8_t* p) { return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3]; }
+constexpr uint32_t fourcc(char a, char b, char c, char d) {
+  return ((uint32_t)(uint8_t)a << 24) | ((uint32_t)(uint8_t)b << 16) | ((uint32_t)(uint8_t)c << 8) | (uint8_t)d;
+}
+
+BoxHeader box_header(const uint8_t* d, size_t len, size_t off) {
+  if (off + 8 > len) fail(ST_TRUNCATED, "box header truncated");
+  const uint32_t lbox = be32(d + off);
+  BoxHeader h{be32(d + off + 4), off + 8, 0};
+  if (lbox == 0) {
+    h.end = len;
+  } else if (lbox == 1) {
+    if (off + 16 > len) fail(ST_TRUNCATED, "extended box header truncated");
+    const uint64_t xl = ((uint64_t)be32(d + off + 8) << 32) | be32(d + off + 12);
+    if (xl < 16) fail(ST_DECODE, "extended box length smaller than header");
+    if (xl > (uint64_t)SIZE_MAX - off) fail(ST_DECODE, "extended box length overflow");
+    h.payload = off + 16;
+    h.end = off + (size_t)xl;
+  } else if (lbox < 8) {
+    fail(ST_DECODE, "box length smaller than header");
+  } else {
+    h.end = off + lbox;
+  }
+  return h;
+}
+
+Container locate(const uint8_t* d, size_t len) {
+  static const uint8_t kSig[12] = {0, 0, 0, 12, 'j', 'P', ' ', ' ', 0x0D, 0x0A, 0x87, 0x0A};
+  Container c;
+  if (len >= 8 && std::memcmp(d, kSig, 8) == 0) {
+    if (len < 12) fail(ST_TRUNCATED, "input shorter than the JP2 signature");
+    bool sig = false, ftyp = false, jp2h = false, ihdr = false, jp2c = false;
+    for (size_t off = 0; off < len;) {
+      const BoxHeader b = box_header(d, len, off);
+      if (b.end > len) fail(ST_TRUNCATED, "box payload truncated");
+      const uint8_t* pl = d + b.payload;
+      const size_t pn = b.end - b.payload;
+      if (b.type == fourcc('j', 'P', ' ', ' ')) {
+        if (sig || off != 0) fail(ST_DECODE, "signature box must appear exactly once at the start of the file");
+        if (pn != 4 || std::memcmp(pl, kSig + 8, 4) != 0) fail(ST_DECODE, "invalid JP2 signature payload");
+        sig = true;
+      } else if (b.type == fourcc('f', 't', 'y', 'p')) {
+        if (!sig || ftyp || jp2h || jp2c) fail(ST_DECODE, "file type box must appear exactly once before jp2h and jp2c");
+        if (pn < 8) fail(ST_DECODE, "ftyp payload shorter than 8 bytes");
+        ftyp = true;
+      } else if (b.type == fourcc('j', 'p', '2', 'h')) {
+        if (!ftyp || jp2h || jp2c) fail(ST_DECODE, "jp2h must appear exactly once after ftyp and before jp2c");
+        for (size_t o = 0; o < pn;) {
+          const BoxHeader ib = box_header(pl, pn, o);
+          const size_t iend = std::min(ib.end, pn);  // inner boxes are bounded by jp2h
+          const uint8_t* ip = pl + ib.payload;
+          const size_t in = iend > ib.payload ? iend - ib.payload : 0;
+          if (ib.type == fourcc('i', 'h', 'd', 'r')) {
+            if (in < 14) fail(ST_DECODE, "ihdr payload shorter than 14 bytes");
+            ihdr = true;
+          } else if (ib.type == fourcc('c', 'o', 'l', 'r')) {
+            if (in >= 3) {
+              if (ip[0] == 1 && in >= 7) c.colr = (int)be32(ip + 3);
+              else if (ip[0] == 2) c.colr = -2;
+            }
+          } else if (ib.type == fourcc('p', 'c', 'l', 'r') || ib.type == fourcc('c', 'm', 'a', 'p') ||
+                     ib.type == fourcc('c', 'd', 'e', 'f')) {
+            c.channel_boxes = true;
+          }
+          o = ib.end;
+        }
+        jp2h = true;
+      } else if (b.type == fourcc('j', 'p', '2', 'c')) {
+        if (!jp2h || jp2c) fail(ST_DECODE, "jp2c must appear exactly once after jp2h");
+        c.off = b.payload;
+        c.len = pn;
+        jp2c = true;
+      }
+      off = b.end;
+    }
+    if (!ftyp) fail(ST_DECODE, "missing required box ftyp");
+    if (!jp2h) fail(ST_DECODE, "missing required box jp2h");
+    if (!ihdr) fail(ST_DECODE, "missing required box ihdr");
+    if (!jp2c) fail(ST_DECODE, "missing required box jp2c");
+    c.jp2 = true;
+    return c;
+  }
+  if (len >= 4 && d[0] == 0xFF && d[1] == 0x4F && d[2] == 0xFF && d[3] == 0x51) {
+    c.len = len;
+    return c;
+  }
+  fail(ST_UNSUPPORTED, "input is not a JP2 container or raw JPEG 2000 codestream");
+  return c;
+}
+
+}  // namespace
+
 Info inspect_codestream(const uint8_t* data, size_t len) {
+  const Container c = locate(data, len);
+  return inspect_raw(data + c.off, c.len);
+}
+
+void parse_tile(const uint8_t* data, size_t len, const uint32_t* target, TileLayout& T) {
+  const Container c = locate(data, len);
+  parse_tile_raw(data + c.off, c.len, target, T);
+  // The pixel formats map the decoded components as the reference's output
+  // writers do (crates/signinum-j2k/src/decode.rs:235-273, :430-470): an
+  // enumerated sRGB / greyscale colour specification must agree with the
+  // component count; palettes, channel definitions, sYCC and ICC profiles
+  // are not mapped by this path.
+  if (c.jp2) {
+    if (c.channel_boxes) fail(ST_UNSUPPORTED, "JP2 palette / channel definition boxes are not supported by the CUDA path");
+    if (c.colr != -1 && !((c.colr == 16 && T.ncomp == 3) || (c.colr == 17 && T.ncomp == 1)))
+      fail(ST_UNSUPPORTED, "backend color space cannot be mapped to the requested pixel format");
+  }
+  for (CodeBlock& cb : T.blocks) {
+    cb.cleanup_off += (uint32_t)c.off;
+    if (cb.passes > 1) cb.ref_off += (uint32_t)c.off;
+  }
+}
+
+namespace {
+
+Info inspect_raw(const uint8_t* data, size_t len) {
   MainHeader h = read_main_header(data, len);
   Info i;
   uint32_t xsf = 1, ysf = 1;
@@ -345,7 +485,7 @@ Info inspect_codestream(const uint8_t* data, size_t len) {
   return i;
 }
 
-void parse_tile(const uint8_t* data, size_t len, const uint32_t* target, TileLayout& T) {
+void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, TileLayout& T) {
   MainHeader h = read_main_header(data, len);
   const uint32_t nc = (uint32_t)h.comps.size();
   if (h.ox || h.oy || h.tox || h.toy) fail(ST_UNSUPPORTED, "image/tile offsets are not supported by the CUDA path");
@@ -728,5 +868,7 @@ void parse_tile(const uint8_t* data, size_t len, const uint32_t* target, TileLay
     T.blocks.push_back(cb);
   }
 }
+
+}  // namespace
 
 }  // namespace sgn

@@ -35,3 +35,35 @@ def random_codestream(rng, max_side=80):
                                 cb_exp=cbw, cb_exp_h=cbh, progression=int(rng.choice([0, 1, 2, 3, 4])),
                                 sop_eph=bool(rng.integers(0, 2)))
     return cs, px, w, h, comps, bd
+
+
+def _box(btype: bytes, payload: bytes, form: str = "short") -> bytes:
+    """One JP2 box: 'short' (32-bit length), 'long' (extended 64-bit length)
+    or 'to_end' (length 0: the box runs to the end of the file)."""
+    import struct
+
+    if form == "long":
+        return struct.pack(">I", 1) + btype + struct.pack(">Q", 16 + len(payload)) + payload
+    if form == "to_end":
+        return struct.pack(">I", 0) + btype + payload
+    return struct.pack(">I", 8 + len(payload)) + btype + payload
+
+
+def jp2_wrap(codestream: bytes, width: int, height: int, comps: int, bit_depth: int = 8, colr_enum=None,
+             icc: bool = False, extra_jp2h: bytes = b"", jp2c_form: str = "short", with_ihdr: bool = True,
+             order=("jP", "ftyp", "jp2h", "jp2c")) -> bytes:
+    """A JP2 file around a raw codestream (ISO/IEC 15444-1 Annex I boxes)."""
+    import struct
+
+    if colr_enum is None:
+        colr_enum = 16 if comps == 3 else 17
+    ihdr = _box(b"ihdr", struct.pack(">IIHBBBB", height, width, comps, bit_depth - 1, 7, 0, 0))
+    colr = _box(b"colr", bytes([2, 0, 0]) + b"\x00" * 8) if icc else \
+        _box(b"colr", bytes([1, 0, 0]) + struct.pack(">I", colr_enum))
+    parts = {
+        "jP": _box(b"jP  ", b"\x0d\x0a\x87\x0a"),
+        "ftyp": _box(b"ftyp", b"jp2 " + struct.pack(">I", 0) + b"jp2 "),
+        "jp2h": _box(b"jp2h", (ihdr if with_ihdr else b"") + colr + extra_jp2h),
+        "jp2c": _box(b"jp2c", codestream, jp2c_form),
+    }
+    return b"".join(parts[k] for k in order)
