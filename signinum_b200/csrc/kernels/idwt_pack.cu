@@ -198,6 +198,61 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
   }
 }
 
+// Per-lane shared-memory slots (int4 each) of the three-component stream:
+// 0..2 previous odd row (horizontally lifted), 3..5 previous updated even
+// row (also the finished row 2m), 6..8 the finished row 2m - 1.
+constexpr int kStreamSlots = 9;
+
+// Vertical 5/3 stream over rows [ys, ye) of three level images, one
+// component at a time: the lifting state lives in the lane's own
+// shared-memory slots `st` (slot k at st[k * 32 + lane]), so only one
+// component's rows are in registers at once.  emit(y, v[3]) as stream_rows.
+template <typename Emit>
+__device__ __forceinline__ void stream_rows3(const PackJob& job, int w, int h, int b, int lane, int ys, int ye,
+                                             int4* st, Emit emit) {
+  auto bands = [&](int c) { return make_bands(job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, h); };
+  auto slot = [&](int k) -> int4& { return st[k * kLanes + lane]; };
+  int4 v[3];
+  if (h == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = hrow(bands(c), 0, b, lane);
+    emit(0, v);
+    return;
+  }
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    slot(c) = hrow(bands(c), ys - 1, b, lane);
+    slot(3 + c) = make_int4(0, 0, 0, 0);
+  }
+  for (int m = ys >> 1;; ++m) {
+    const int ye_row = 2 * m, yo_row = 2 * m + 1;
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      const Bands B = bands(c);
+      const RawRow re = load_row(B, ye_row, b, lane);
+      const RawRow ro = load_row(B, yo_row, b, lane);
+      const int4 xe = lift_row(re, w, b, lane);
+      const int4 xo = lift_row(ro, w, b, lane);
+      const int4 xo_prev = slot(c), ev_prev = slot(3 + c);
+      const int4 ev = vupdate(xe, xo_prev, xo);
+      slot(6 + c) = vpredict(xo_prev, ev_prev, ev);
+      slot(c) = xo;
+      slot(3 + c) = ev;
+    }
+    if (ye_row - 1 >= ys && ye_row - 1 < ye) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[c] = slot(6 + c);
+      emit(ye_row - 1, v);
+    }
+    if (ye_row < ye) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[c] = slot(3 + c);
+      emit(ye_row, v);
+    }
+    if (yo_row >= ye) break;
+  }
+}
+
 template <typename Job>
 __device__ __forceinline__ const Job& find_job(const Job* jobs, uint32_t njobs, uint32_t unit) {
   uint32_t lo = 0, hi = njobs - 1;
@@ -347,7 +402,8 @@ __device__ __forceinline__ int lane_comp(const int4& v, int p) { return p == 0 ?
 constexpr int kRowWords = (16 + kIdwtStripW * 6) / 4;
 
 template <int NC, int FMT, bool DIRECT>
-__device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf) {
+__device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
+                                          int4* st) {
   constexpr int BPP = pack_bpp<FMT>();
   const int w = (int)job.w;
   const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
@@ -410,10 +466,12 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
     __syncwarp();
   };
   if (job.lifting) {
-    Bands B[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) B[c] = make_bands(job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, (int)job.h);
-    stream_rows<NC, NC == 1>(B, b, lane, ys, ye, emit);
+    if (NC == 3) {
+      stream_rows3(job, w, (int)job.h, b, lane, ys, ye, st, emit);
+    } else {
+      const Bands B = make_bands(job.ll[0], job.hl[0], job.lh[0], job.hh[0], w, (int)job.h);
+      stream_rows<1, true>(&B, b, lane, ys, ye, emit);
+    }
   } else {
     // Nothing left to lift: the image is the LL band itself.
     for (int y = ys; y < ye; ++y) {
@@ -435,7 +493,7 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
 
 template <int FMT>
 __device__ __forceinline__ void pack_one(const PackJob* __restrict__ jobs, uint32_t njobs, uint32_t unit,
-                                         uint32_t* rowbuf) {
+                                         uint32_t* rowbuf, int4* st) {
   const int lane = threadIdx.x & 31;
   const PackJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
@@ -445,26 +503,28 @@ __device__ __forceinline__ void pack_one(const PackJob* __restrict__ jobs, uint3
   constexpr bool kU8 = FMT == PACK_GRAY8 || FMT == PACK_RGB8 || FMT == PACK_RGBA8;
   const bool direct = kU8 ? job.bit_depth == 8 : job.bit_depth > 8;
   if (job.ncomp >= 3) {
-    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbuf);
-    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbuf);
+    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbuf, st);
+    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbuf, st);
   } else {
-    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbuf);
-    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbuf);
+    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbuf, st);
+    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbuf, st);
   }
 }
 
 template <int FMT, bool QUEUE>
-__global__ void __launch_bounds__(kIdwtWarps * 32, 2) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kIdwtWarps * 32, 3) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
                                                                uint32_t nunits, uint32_t* queue) {
   __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
+  __shared__ int4 states[kIdwtWarps][kStreamSlots * kLanes];
   uint32_t* rowbuf = rowbufs[threadIdx.x >> 5];
+  int4* st = states[threadIdx.x >> 5];
   if (!QUEUE) {
     const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
-    if (unit < nunits) pack_one<FMT>(jobs, njobs, unit, rowbuf);
+    if (unit < nunits) pack_one<FMT>(jobs, njobs, unit, rowbuf, st);
     return;
   }
   bool first = true;
-  for (uint32_t unit; next_unit(queue, nunits, first, unit);) pack_one<FMT>(jobs, njobs, unit, rowbuf);
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);) pack_one<FMT>(jobs, njobs, unit, rowbuf, st);
 }
 
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
