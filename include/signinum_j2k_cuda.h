@@ -154,7 +154,8 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms)
  * its own data over `reps` runs each (0: 5) for every candidate launch shape
  * (VLC lanes per CTA; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
- * pack one unit per warp or persistent on a queue), keeps the fastest per
+ * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
+ * IDWT levels, bit 1 = pack), keeps the fastest per
  * stage for the plan and for later plans of the same shape on this context,
  * and re-executes the plan so its surfaces hold the decode.  Synchronous. */
 typedef struct sgn_tune_report {
@@ -164,7 +165,7 @@ typedef struct sgn_tune_report {
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;
- * vlc_threads 32..128 in steps of 32, ms_warps 1..8). */
+ * vlc_threads 32..128 in steps of 32, ms_warps 1..8, dwt_queue 0..3). */
 sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_threads, uint32_t ms_warps,
                                      uint32_t ms_blocks_per_grab, uint32_t dwt_queue);
 /* Launches issued by one execute of the plan. */

@@ -552,12 +552,12 @@ sgn_status execute(sgn_plan* p, cudaStream_t s) {
     return cuda_status(e, "HT refinement launch");
   for (size_t k = 0; k < p->rounds.size(); ++k) {
     const RoundInfo& r = p->rounds[k];
-    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.dwt_queue ? p->d_queue + 1 + k : nullptr,
+    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.idwt_queue ? p->d_queue + 1 + k : nullptr,
                                c.idwt_ctas)) != cudaSuccess)
       return cuda_status(e, "IDWT launch");
   }
   if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
-                       c.dwt_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas)) != cudaSuccess)
+                       c.pack_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas)) != cudaSuccess)
     return cuda_status(e, "pack launch");
   return SGN_OK;
 }
@@ -769,12 +769,12 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   chk(cudaEventRecord(ev[3], s));
   for (size_t k = 0; k < p->rounds.size(); ++k) {
     const RoundInfo& r = p->rounds[k];
-    chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.dwt_queue ? p->d_queue + 1 + k : nullptr,
+    chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.idwt_queue ? p->d_queue + 1 + k : nullptr,
                           c.idwt_ctas));
   }
   chk(cudaEventRecord(ev[4], s));
   chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
-                  c.dwt_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas));
+                  c.pack_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas));
   chk(cudaEventRecord(ev[5], s));
   chk(cudaEventSynchronize(ev[5]));
   if (e == cudaSuccess) {
@@ -814,7 +814,7 @@ extern "C" {
 sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_threads, uint32_t ms_warps,
                                      uint32_t ms_blocks_per_grab, uint32_t dwt_queue) {
   if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
-  if (vlc_threads < 32 || vlc_threads > 128 || vlc_threads % 32 || ms_warps < 1 || ms_warps > 8 || dwt_queue > 1)
+  if (vlc_threads < 32 || vlc_threads > 128 || vlc_threads % 32 || ms_warps < 1 || ms_warps > 8 || dwt_queue > 3)
     return set_error(SGN_ERR_INVALID_ARGUMENT, "launch shape out of range");
   std::lock_guard<std::mutex> g(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -822,7 +822,8 @@ sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_thr
   c.vlc_threads = vlc_threads;
   c.ms_warps = ms_warps;
   c.ms_gran = ms_blocks_per_grab;
-  c.dwt_queue = dwt_queue;
+  c.idwt_queue = dwt_queue & 1;
+  c.pack_queue = (dwt_queue >> 1) & 1;
   return apply_config(ctx, p, c);
 }
 
@@ -869,9 +870,9 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     if (m.warps == 8 && m.gran == 0) rep.ms_ms_default = ms;
     if (e == cudaSuccess && ms < best_ms) best_ms = ms, ms_warps = m.warps, ms_gran = m.gran;
   }
-  // IDWT levels + pack: one unit per warp, or persistent warps on a queue.
-  float best_dwt = 1e30f;
-  uint32_t dwt_queue = 0;
+  // IDWT levels and pack, each: one unit per warp, or persistent warps on a queue.
+  float best_idwt = 1e30f, best_pack = 1e30f, idwt_default = 0.f, pack_default = 0.f;
+  uint32_t idwt_queue = 0, pack_queue = 0;
   for (uint32_t q = 0; q < 2; ++q) {
     const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
     float ms = time_stage(s, reps, [&] {
@@ -880,14 +881,22 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
         const RoundInfo& r = p->rounds[k];
         x = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q ? p->d_queue + 1 + k : nullptr, ictas);
       }
+      return x;
+    }, e);
+    if (q == 0) idwt_default = ms;
+    if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q;
+    ms = time_stage(s, reps, [&] {
+      cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
       if (x == cudaSuccess)
         x = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s, q ? p->d_queue + 1 + p->rounds.size() : nullptr,
                         pctas);
       return x;
     }, e);
-    if (q == 0) rep.dwt_ms_default = ms;
-    if (e == cudaSuccess && ms < best_dwt) best_dwt = ms, dwt_queue = q;
+    if (q == 0) pack_default = ms;
+    if (e == cudaSuccess && ms < best_pack) best_pack = ms, pack_queue = q;
   }
+  rep.dwt_ms_default = idwt_default + pack_default;
+  const float best_dwt = best_idwt + best_pack;
   if (e != cudaSuccess) {
     apply_config(ctx, p, base);
     return cuda_status(e, "autotune");
@@ -895,7 +904,8 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   cfg.vlc_threads = vlc_threads;
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
-  cfg.dwt_queue = dwt_queue;
+  cfg.idwt_queue = idwt_queue;
+  cfg.pack_queue = pack_queue;
   st = apply_config(ctx, p, cfg);
   if (st != SGN_OK) return st;
   // Leave the plan's outputs consistent (the refinement pass is not
@@ -913,7 +923,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   rep.vlc_threads = cfg.vlc_threads;
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
-  rep.dwt_queue = cfg.dwt_queue;
+  rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);
   rep.vlc_ms = best_vlc;
   rep.ms_ms = best_ms;
   rep.dwt_ms = best_dwt;

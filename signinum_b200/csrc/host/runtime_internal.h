@@ -127,7 +127,8 @@ struct LaunchConfig {
   uint32_t vlc_threads = 128;  // lanes (code blocks) per CTA of the VLC pass
   uint32_t ms_warps = 8;       // warps (code blocks in flight) per CTA of the MagSgn pass
   uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
-  uint32_t dwt_queue = 0;      // 0: one unit per warp; 1: persistent warps take IDWT/pack units from a queue
+  uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue
+  uint32_t pack_queue = 0;     // the same for the last level + pack
   // Persistent grid sizes (SMs x resident CTAs), derived from the above.
   uint32_t ms_ctas = 0, idwt_ctas = 0, pack_ctas = 0;
 };

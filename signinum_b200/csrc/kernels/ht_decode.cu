@@ -131,10 +131,18 @@ struct Vlc {
         const uint32_t wv = __funnelshift_r(__ldg(a), __ldg(a + 1), (uint32_t)(addr & 3) * 8);
         pos -= 4;
         remaining -= 4;
-        push(wv >> 24);
-        push((wv >> 16) & 0xFF);
-        push((wv >> 8) & 0xFF);
-        push(wv & 0xFF);
+        if (__vcmpeq4(wv | 0x80808080u, 0xFFFFFFFFu) == 0) {
+          // No byte has its low 7 bits all ones, so none loses a bit to
+          // stuffing: the four bytes (highest address first) go in whole.
+          tmp |= (uint64_t)__byte_perm(wv, 0, 0x0123) << bits;
+          bits += 32;
+          unstuff = (wv & 0xFF) > 0x8F;
+        } else {
+          push(wv >> 24);
+          push((wv >> 16) & 0xFF);
+          push((wv >> 8) & 0xFF);
+          push(wv & 0xFF);
+        }
       } else {
         uint32_t b = 0;
         if (remaining > 0) {
@@ -658,6 +666,7 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
 // a persistent grid whose warps take `gran` consecutive blocks at a time
 // from the device work queue (an atomic counter over the job table, which is
 // ordered by coded length, longest first).
+template <bool QUEUE>
 __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
                                                                   const uint8_t* __restrict__ arena,
                                                                   const uint32_t* __restrict__ symbols,
@@ -670,19 +679,19 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
   const uint32_t cols = max_w + 4;
   uint32_t* W = reinterpret_cast<uint32_t*>(smem) + (size_t)warp * ms_words;
   uint8_t* Ebase = smem + (size_t)nw * ms_words * 4 + (size_t)warp * 2 * cols;
-  if (!queue) {
+  if constexpr (!QUEUE) {
     const uint32_t j = blockIdx.x * nw + warp;
     if (j < njobs) magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
-    return;
-  }
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(queue, gran);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= njobs) break;
-    const uint32_t end = min(base + gran, njobs);
-    for (uint32_t j = base; j < end; ++j)
-      magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+  } else {
+    for (;;) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(queue, gran);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base >= njobs) break;
+      const uint32_t end = min(base + gran, njobs);
+      for (uint32_t j = base; j < end; ++j)
+        magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+    }
   }
 }
 
@@ -877,7 +886,9 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps) {
 }
 
 cudaError_t ht_kernels_init() {
-  return cudaFuncSetAttribute(ht_magsgn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(ht_magsgn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(ht_magsgn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
@@ -901,14 +912,18 @@ cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* a
     if (gran == 0) gran = 1;
     ctas = std::max(1u, std::min(ctas, persistent_ctas));
   }
-  ht_magsgn_kernel<<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status, ms_words,
-                                                        max_w, queue, gran);
+  if (queue)
+    ht_magsgn_kernel<true><<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status,
+                                                               ms_words, max_w, queue, gran);
+  else
+    ht_magsgn_kernel<false><<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status,
+                                                                ms_words, max_w, nullptr, 0);
   return cudaGetLastError();
 }
 
 cudaError_t ht_magsgn_occupancy(uint32_t ms_words, uint32_t max_w, uint32_t warps, int* ctas_per_sm) {
   if (warps == 0 || warps > kMsWarps) warps = kMsWarps;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, ht_magsgn_kernel, warps * 32,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, ht_magsgn_kernel<true>, warps * 32,
                                                        ht_magsgn_smem_bytes(ms_words, max_w, warps));
 }
 

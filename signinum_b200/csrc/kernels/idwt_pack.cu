@@ -512,7 +512,7 @@ __device__ __forceinline__ void pack_one(const PackJob* __restrict__ jobs, uint3
 }
 
 template <int FMT, bool QUEUE>
-__global__ void __launch_bounds__(kIdwtWarps * 32, 3) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kIdwtWarps * 32, 4) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
                                                                uint32_t nunits, uint32_t* queue) {
   __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
   __shared__ int4 states[kIdwtWarps][kStreamSlots * kLanes];

@@ -11,9 +11,9 @@ pytestmark = pytest.mark.gpu
 SHAPES = [
     (128, 8, 0, 0),  # default: one block / unit per warp
     (64, 4, 0, 0),
-    (128, 8, 1, 1),  # persistent MagSgn (1 block per grab) and IDWT/pack queues
-    (96, 4, 4, 1),   # persistent MagSgn, 4 blocks per grab
-    (32, 1, 2, 0),
+    (128, 8, 1, 3),  # persistent MagSgn (1 block per grab), IDWT and pack queues
+    (96, 4, 4, 1),   # persistent MagSgn, 4 blocks per grab, IDWT queue
+    (32, 1, 2, 2),   # pack queue
 ]
 
 
@@ -46,7 +46,7 @@ def test_autotune_keeps_output_and_is_reused(batch):
     want = _want(batch)
     plan = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
     rep = plan.autotune(2)
-    assert rep["vlc_threads"] in (64, 128) and rep["ms_warps"] in (4, 8) and rep["dwt_queue"] in (0, 1)
+    assert rep["vlc_threads"] in (64, 128) and rep["ms_warps"] in (4, 8) and rep["dwt_queue"] in (0, 1, 2, 3)
     assert rep["vlc_ms"] > 0 and rep["ms_ms"] > 0 and rep["dwt_ms"] > 0
     assert [plan.download(i) for i in range(len(batch))] == want
     for _ in range(3):
