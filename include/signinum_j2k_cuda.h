@@ -240,6 +240,21 @@ sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, 
                                         int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
                                         void* stream);
 
+/* ---- DICOM input: extract_dicom_encapsulated_frames_with_limit
+ * (crates/signinum-j2k-metal/src/dicom.rs:22-95).  Extracts up to `limit`
+ * frames (SIZE_MAX: all) of the encapsulated Pixel Data of a DICOM file:
+ * grouped by the Basic Offset Table, else by the Extended Offset Table (its
+ * Lengths trim padded frames), else one frame per fragment.  Call once with
+ * out == NULL for *nframes and *out_bytes, then with buffers of that size:
+ * the frames are written back to back into `out`, each 16-byte aligned, at
+ * frame_offsets[i] with frame_lens[i] bytes, ready for
+ * sgn_j2k_decode_tiles_to_device.  Errors: SGN_ERR_TRUNCATED, SGN_ERR_DECODE
+ * (malformed / no Pixel Data), SGN_ERR_UNSUPPORTED (native Pixel Data),
+ * SGN_ERR_BUFFER (buffers too small).  Host only. */
+sgn_status sgn_dicom_frames(const uint8_t* data, size_t len, size_t limit, uint8_t* out, size_t out_cap,
+                            uint64_t* frame_offsets, uint64_t* frame_lens, size_t frames_cap, size_t* nframes,
+                            size_t* out_bytes);
+
 /* ---- Serving loop: continuous batching of tile requests (sgn_server_submit /
  * sgn_server_poll stand beside the drop-in calls; the reference has no
  * serving loop, its adapter decodes one call at a time).

@@ -6,7 +6,7 @@ mirrors the reference's signinum-j2k-cuda adapter; j2k_cuda is its Python
 face.
 """
 from .j2k_cuda import (BackendKind, BackendRequest, Codec, CudaSession, CudaSurface, Downscale, Error, J2kDecoder,
-                       PixelFormat, Rect, Surface, TileBatchError, inspect)
+                       PixelFormat, Rect, Surface, TileBatchError, dicom_frames, inspect)
 
 __all__ = ["BackendKind", "BackendRequest", "Codec", "CudaSession", "CudaSurface", "Downscale", "Error",
-           "J2kDecoder", "PixelFormat", "Rect", "Surface", "TileBatchError", "inspect"]
+           "J2kDecoder", "PixelFormat", "Rect", "Surface", "TileBatchError", "dicom_frames", "inspect"]

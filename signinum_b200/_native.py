@@ -72,6 +72,10 @@ class SgnTuneReport(ctypes.Structure):
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
 CUDA_SIGNATURES = {
+    "sgn_dicom_frames": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p,
+                                          ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_plan_set_launch_shape": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                                    ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
     "sgn_plan_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,

@@ -28,6 +28,7 @@ CUDA_SOURCES = [
     CSRC / "host" / "runtime.cu",
     CSRC / "host" / "noalloc.cu",
     CSRC / "host" / "server.cu",
+    CSRC / "host" / "dicom.cpp",
     CSRC / "host" / "codestream.cpp",
 ]
 ENCODE_SOURCES = [

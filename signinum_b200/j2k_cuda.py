@@ -387,3 +387,21 @@ class Codec:
             idx = first.value if first.value < n else 0
             raise TileBatchError(idx, per[idx] if n else st, _native.last_error())
         return surfaces
+
+
+def dicom_frames(data, limit: Optional[int] = None):
+    """JPEG 2000 frames of a DICOM file's encapsulated Pixel Data
+    (extract_dicom_encapsulated_frames, crates/signinum-j2k-metal/src/dicom.rs:22-95),
+    as a list of bytes."""
+    arr = _as_u8(data)
+    lim = ctypes.c_size_t(-1).value if limit is None else limit
+    n, total = ctypes.c_size_t(), ctypes.c_size_t()
+    lib = _native.cuda_lib()
+    _check(lib.sgn_dicom_frames(arr.ctypes.data, arr.nbytes, lim, None, 0, None, None, 0, ctypes.byref(n),
+                                ctypes.byref(total)))
+    out = np.zeros(max(1, total.value), np.uint8)
+    offs = (ctypes.c_uint64 * max(1, n.value))()
+    lens = (ctypes.c_uint64 * max(1, n.value))()
+    _check(lib.sgn_dicom_frames(arr.ctypes.data, arr.nbytes, lim, out.ctypes.data, out.nbytes, offs, lens, n.value,
+                                ctypes.byref(n), ctypes.byref(total)))
+    return [out[offs[i]:offs[i] + lens[i]].tobytes() for i in range(n.value)]
