@@ -46,6 +46,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
     ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000",
                     help="c4: arrival rates, tiles/s")
@@ -516,7 +517,7 @@ def main():
     # ---- Batched, device-resident (value).
     plan = Plan(lens, fmt, ctx=ctx, contiguous=host, offsets=offs)
     # Launch shape chosen by the autotuner on this plan's data (untimed).
-    tune = plan.autotune(5)
+    tune = None if args.no_autotune else plan.autotune(5)
     # Per-stage breakdown with the tuned shape (events between stages; untimed).
     stages = [plan.execute_timed() for _ in range(3)]
     # Warm-up: the first execution runs eagerly, the second captures the plan
