@@ -174,24 +174,30 @@ class Clocks:
                 "samples": len(self.rows), "source": "NVML, 1 ms polling during the timed region"}
 
 
-def cpu_baseline(tiles, fmt, budget_s=20.0):
-    """The oracle's CPU tile batch (all host threads) over a bounded sample."""
+def cpu_baseline(tiles, fmt, budget_s=12.0):
+    """The oracle's CPU tile batch (all host threads) over a bounded sample of
+    the workload: whole passes over its tiles until about budget_s seconds."""
     from oracle import oracle
 
-    # One single-threaded probe decode sizes the sample to ~budget_s of CPU work.
+    cores = os.cpu_count() or 1
+    # One single-threaded probe decode sizes the sample.
     t0 = time.perf_counter()
     oracle.decode(tiles[0].codestream, fmt)
     per_tile = max(time.perf_counter() - t0, 1e-4)
-    k = int(max(1, min(len(tiles), budget_s / per_tile)))
-    sample = tiles[:k]
-    cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    outs, first = oracle.decode_batch([t.codestream for t in sample], fmt, workers=cores)
-    dt = time.perf_counter() - t0
-    px = sum(t.width * t.height for t in sample)
-    return {"value": px / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": "port",
-            "sample": f"first {k} of {len(tiles)} tiles of the workload, one pass, {cores} threads",
-            "seconds": dt, "ok": first == -1}
+    k = int(max(1, min(len(tiles), budget_s * cores / per_tile)))
+    sample = [t.codestream for t in tiles[:k]]
+    px = sum(t.width * t.height for t in tiles[:k])
+    passes, dt, ok = 0, 0.0, True
+    while passes == 0 or dt < budget_s:
+        t0 = time.perf_counter()
+        outs, first = oracle.decode_batch(sample, fmt, workers=cores)
+        dt += time.perf_counter() - t0
+        ok = ok and first == -1
+        passes += 1
+    return {"value": passes * px / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": "port",
+            "sample": f"first {k} of {len(tiles)} tiles of the workload, {passes} passes, {cores} threads; C++ "
+                      "restatement of the reference CPU tile batch (Rust toolchain absent)",
+            "seconds": dt, "ok": ok}
 
 
 def run_reference(args):
