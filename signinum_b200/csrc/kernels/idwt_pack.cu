@@ -224,15 +224,28 @@ __device__ __forceinline__ void stream_rows3(const PackJob& job, int w, int h, i
     slot(c) = hrow(bands(c), ys - 1, b, lane);
     slot(3 + c) = make_int4(0, 0, 0, 0);
   }
+  // The rows of the next component (or of the next row pair's first
+  // component) are loaded while the current one is lifted.
+  RawRow re = load_row(bands(0), ys, b, lane), ro = load_row(bands(0), ys + 1, b, lane);
   for (int m = ys >> 1;; ++m) {
     const int ye_row = 2 * m, yo_row = 2 * m + 1;
+    const bool more = yo_row < ye;
 #pragma unroll 1
     for (int c = 0; c < 3; ++c) {
-      const Bands B = bands(c);
-      const RawRow re = load_row(B, ye_row, b, lane);
-      const RawRow ro = load_row(B, yo_row, b, lane);
+      RawRow ne = re, no = ro;
+      if (c < 2) {
+        const Bands N = bands(c + 1);
+        ne = load_row(N, ye_row, b, lane);
+        no = load_row(N, yo_row, b, lane);
+      } else if (more) {
+        const Bands N = bands(0);
+        ne = load_row(N, ye_row + 2, b, lane);
+        no = load_row(N, yo_row + 2, b, lane);
+      }
       const int4 xe = lift_row(re, w, b, lane);
       const int4 xo = lift_row(ro, w, b, lane);
+      re = ne;
+      ro = no;
       const int4 xo_prev = slot(c), ev_prev = slot(3 + c);
       const int4 ev = vupdate(xe, xo_prev, xo);
       slot(6 + c) = vpredict(xo_prev, ev_prev, ev);
