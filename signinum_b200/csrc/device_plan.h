@@ -45,6 +45,20 @@ static_assert(sizeof(HtJob) == 48, "HtJob layout");
 // cleanup VLC/MEL decode failed has kSymFailed in its first entry.
 constexpr uint32_t kSymFailed = 0xFFFFFFFFu;
 
+// Quad-symbol table of a code block: ceil(h/2) rows of ceil(w/2) symbols,
+// each row padded to an even count so a quad pair's two symbols form one
+// 8-byte store; tables are padded to a multiple of 4 words, so they start
+// 16-byte aligned (rows of a multiple of 4 symbols are written 16 bytes at
+// a time).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline uint32_t sym_row_stride(uint32_t w) { return (((w + 1) / 2) + 1) & ~1u; }
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline uint32_t sym_words(uint32_t w, uint32_t h) { return (sym_row_stride(w) * ((h + 1) / 2) + 3) & ~3u; }
+
 struct IdwtJob {
   const int32_t* ll;   // ceil(w/2) x ceil(h/2)
   const int32_t* hl;   // floor(w/2) x ceil(h/2)

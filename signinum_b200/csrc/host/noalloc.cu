@@ -31,8 +31,8 @@ void sgn_set_last_error_message(const char* msg);
 namespace {
 
 constexpr uint32_t kNoAllocMaxBlocks = 4096;
-// ceil(w/2) * ceil(h/2) <= 1024 for any code block of at most 4096 samples
-// with power-of-two sides (edge blocks are smaller).
+// The quad-symbol table of any code block of at most 4096 samples and at
+// most 1024 rows fits in 1024 words (rows padded to an even quad count).
 constexpr uint32_t kNoAllocSymbolsPerBlock = 1024;
 constexpr int kMaxDevices = 64;
 
@@ -123,7 +123,7 @@ sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, 
   for (uint32_t j = 0; j < n; ++j) {
     const sgn_ht_block& b = blocks[j];
     if (b.w == 0 || b.h == 0 || (uint32_t)b.w * b.h > 4096 ||
-        (uint32_t)((b.w + 1) / 2) * ((b.h + 1) / 2) > kNoAllocSymbolsPerBlock)
+        sym_words(b.w, b.h) > kNoAllocSymbolsPerBlock)
       return fail(SGN_ERR_INVALID_ARGUMENT, "code block larger than 4096 samples");
     if (b.passes > 3 || (b.passes && (b.lcup < 2 || b.missing_msbs >= 30)) || b.tile >= n_tiles ||
         b.stride < b.w)

@@ -257,7 +257,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       ++t.hist[len_bucket(cb.lcup)];
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
       if (!cb.passes) continue;
-      t.sym += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
+      t.sym += sym_words(cb.w, cb.h);
       if (cb.passes > 1) ++t.nref;
       if (cb.lcup >= 2) {
         const uint8_t* seg = datas[i] + cb.cleanup_off;
@@ -437,7 +437,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       j.flags = L.causal ? 1 : 0;
       if (cb.passes) {
         j.sym = sym;
-        sym += (uint64_t)((cb.w + 1) / 2) * ((cb.h + 1) / 2);
+        sym += sym_words(cb.w, cb.h);
       }
       if (cb.passes > 1) refine[rk++] = pos;
     }

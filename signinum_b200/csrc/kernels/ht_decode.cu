@@ -104,6 +104,11 @@ struct Vlc {
   uint32_t remaining;
   uint64_t tmp;
   uint32_t bits, unstuff;
+  // Word refills walk down 4 bytes at a time, so their two aligned words
+  // are the previous refill's low word and the word below it: that one is
+  // loaded a refill ahead (w_lo) and the refill itself never waits on memory.
+  const uint32_t* wp;  // aligned word of the next refill's low half
+  uint32_t w_lo, w_hi, sh8;
   __device__ void init(const uint8_t* d, uint32_t lcup, uint32_t scup) {
     data = d;
     uint32_t b = ld8(d + lcup - 2);
@@ -112,6 +117,17 @@ struct Vlc {
     pos = (int)lcup - 3;
     remaining = scup - 2;
     unstuff = (b | 0x0F) > 0x8F;
+    w_lo = w_hi = 0;
+    wp = nullptr;
+    sh8 = 0;
+    if (remaining >= 4) {
+      // Both words hold bytes of the segment (pos - 3 .. pos).
+      const uintptr_t addr = (uintptr_t)(data + pos - 3);
+      wp = reinterpret_cast<const uint32_t*>(addr & ~(uintptr_t)3);
+      sh8 = (uint32_t)(addr & 3) * 8;
+      w_lo = __ldg(wp);
+      w_hi = sh8 ? __ldg(wp + 1) : 0u;
+    }
   }
   __device__ __forceinline__ void push(uint32_t b) {
     const uint32_t db = 8 - ((unstuff && (b & 0x7F) == 0x7F) ? 1 : 0);
@@ -126,9 +142,12 @@ struct Vlc {
   __device__ __forceinline__ void fill() {
     while (bits <= 32) {
       if (remaining >= 4) {
-        const uintptr_t addr = (uintptr_t)(data + pos - 3);
-        const uint32_t* a = reinterpret_cast<const uint32_t*>(addr & ~(uintptr_t)3);
-        const uint32_t wv = __funnelshift_r(__ldg(a), __ldg(a + 1), (uint32_t)(addr & 3) * 8);
+        const uint32_t wv = __funnelshift_r(w_lo, w_hi, sh8);
+        w_hi = w_lo;
+        --wp;
+        // The next word refill (when 4 more bytes remain) reads bytes down to
+        // pos - 7, all inside the segment, so its low word is one of them.
+        w_lo = remaining >= 8 ? __ldg(wp) : 0u;
         pos -= 4;
         remaining -= 4;
         if (__vcmpeq4(wv | 0x80808080u, 0xFFFFFFFFu) == 0) {
@@ -218,7 +237,8 @@ __device__ __forceinline__ uint32_t ctx_entry(uint32_t b) { return ((b & 1) << 5
 // at most 64 wide, nq <= 32) its two context bits per quad live in a 64-bit
 // register, otherwise they are read back from the symbol table.
 template <bool REG>
-__device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T) {
+__device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T,
+                           uint2* __restrict__ stage) {
   const uint32_t lcup = job.lcup, w = job.w, h = job.h;
   if (lcup < 2) return false;
   uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
@@ -228,8 +248,27 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
   Vlc vlc;
   vlc.init(src, lcup, scup);
   int run = mel.get_run();
-  const uint32_t nq = (w + 1) / 2;
+  const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
   uint32_t* row = sym;
+  // REG blocks whose rows hold a multiple of 4 symbols stage each row's
+  // pairs in the lane's shared-memory column and write the row with 16-byte
+  // stores (far fewer scattered store requests than one per pair).
+  const bool staged = REG && (qs & 3) == 0;
+  const uint32_t lanes = blockDim.x, tid = threadIdx.x;
+  auto put = [&](uint32_t q, uint32_t a, uint32_t b) {
+    if (staged) stage[(q >> 1) * lanes + tid] = make_uint2(a, b);
+    else *reinterpret_cast<uint2*>(row + q) = make_uint2(a, b);  // q even, rows padded to even
+  };
+  auto flush = [&]() {
+    if constexpr (REG) {
+      if (!staged) return;
+      for (uint32_t k = 0; 2 * k < nq; k += 2) {
+        const uint2 a = stage[k * lanes + tid];
+        const uint2 b = 2 * (k + 1) < nq ? stage[(k + 1) * lanes + tid] : make_uint2(0, 0);
+        *reinterpret_cast<uint4*>(row + 2 * k) = make_uint4(a.x, a.y, b.x, b.y);
+      }
+    }
+  };
   uint64_t ctx = 0;  // REG: context bits of the row above, 2 per quad
   // Initial quad row.
   {
@@ -243,7 +282,10 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
         if (run < 0) run = mel.get_run();
       }
       c_q = ((t0 & 0x10) << 3) | ((t0 & 0xE0) << 2);
-      v = vlc.advance(t0 & 7);
+      // The pair's bits (at most 30) are read from the 32-bit window v with
+      // 32-bit shifts; the reader advances once, by their sum, at the end.
+      const uint32_t l0 = t0 & 7;
+      v >>= l0;
       const bool hasB = q + 1 < nq;
       uint32_t t1 = T.vlc0[c_q + (v & 0x7F)];
       if (c_q == 0 && hasB) {
@@ -253,7 +295,8 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       }
       if (!hasB) t1 = 0;
       c_q = ((t1 & 0x10) << 3) | ((t1 & 0xE0) << 2);
-      v = vlc.advance(t1 & 7);
+      const uint32_t l1 = t1 & 7;
+      v >>= l1;
       uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
       if (mode == 0xC0) {
         run -= 2;
@@ -261,23 +304,24 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
         if (run < 0) run = mel.get_run();
       }
       uint32_t ue = T.uvlc0[mode + (v & 0x3F)];
-      v = vlc.advance(ue & 7);
+      const uint32_t lp = ue & 7;
+      v >>= lp;
       ue >>= 3;
       uint32_t len = ue & 0xF;
       uint32_t tmp = v & ((1u << len) - 1);
-      vlc.advance(len);
+      vlc.advance(l0 + l1 + lp + len);
       ue >>= 4;
       len = ue & 7;
       ue >>= 3;
-      row[q] = t0 | ((1 + (ue & 7) + (tmp & ~(0xFFu << len))) << 16);
-      if (hasB) row[q + 1] = t1 | ((1 + (ue >> 3) + (tmp >> len)) << 16);
+      put(q, t0 | ((1 + (ue & 7) + (tmp & ~(0xFFu << len))) << 16), t1 | ((1 + (ue >> 3) + (tmp >> len)) << 16));
       if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
     }
+    flush();
   }
   // Other quad rows: context from the row above (quads q, q+1, q+2).
   for (uint32_t y = 2; y < h; y += 2) {
     const uint32_t* prev = row;
-    row += nq;
+    row += qs;
     uint32_t c_q = 0;
     const uint64_t above = ctx;
     ctx = 0;
@@ -313,7 +357,8 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       c_q |= pq0 & 0x80;
       c_q |= (pq1 & 0xA0) << 2;
       c_q |= (pq2 & 0x20) << 4;
-      v = vlc.advance(t0 & 7);
+      const uint32_t l0 = t0 & 7;
+      v >>= l0;
       const bool hasB = q + 1 < nq;
       uint32_t t1 = T.vlc1[c_q + (v & 0x7F)];
       if (c_q == 0 && hasB) {
@@ -324,23 +369,25 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       if (!hasB) t1 = 0;
       c_q = ((t1 & 0x40) << 2) | ((t1 & 0x80) << 1);
       c_q |= pq1 & 0x80;
-      v = vlc.advance(t1 & 7);
+      const uint32_t l1 = t1 & 7;
+      v >>= l1;
       uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
       uint32_t ue = T.uvlc1[mode + (v & 0x3F)];
-      v = vlc.advance(ue & 7);
+      const uint32_t lp = ue & 7;
+      v >>= lp;
       ue >>= 3;
       uint32_t len = ue & 0xF;
       uint32_t tmp = v & ((1u << len) - 1);
-      vlc.advance(len);
+      vlc.advance(l0 + l1 + lp + len);
       ue >>= 4;
       len = ue & 7;
       ue >>= 3;
-      row[q] = t0 | (((ue & 7) + (tmp & ~(0xFFu << len))) << 16);
-      if (hasB) row[q + 1] = t1 | (((ue >> 3) + (tmp >> len)) << 16);
+      put(q, t0 | (((ue & 7) + (tmp & ~(0xFFu << len))) << 16), t1 | (((ue >> 3) + (tmp >> len)) << 16));
       if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
       pq0 = pq2;
       pq1 = pq3;
     }
+    flush();
   }
   return true;
 }
@@ -352,6 +399,7 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
                                                             const uint8_t* __restrict__ arena,
                                                             uint32_t* __restrict__ symbols) {
   __shared__ SmemTables T;
+  __shared__ uint2 stage[16 * kHtThreads];  // per lane: the pairs of one row of a 64-wide block
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&g_ht_tables);
     uint32_t* d = reinterpret_cast<uint32_t*>(&T);
@@ -363,8 +411,8 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
   const HtJob job = jobs[j];
   if (job.passes == 0) return;
   uint32_t* sym = symbols + job.sym;
-  const bool ok = job.w <= 64 ? decode_vlc<true>(job, arena + job.src, sym, T)
-                              : decode_vlc<false>(job, arena + job.src, sym, T);
+  const bool ok = job.w <= 64 ? decode_vlc<true>(job, arena + job.src, sym, T, stage)
+                              : decode_vlc<false>(job, arena + job.src, sym, T, stage);
   if (!ok) sym[0] = kSymFailed;
 }
 
@@ -481,7 +529,7 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
   const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
   const bool raw = job.passes > 1;
   const bool pairs = ((job.dst | stride) & 1) == 0;  // 8-byte aligned sample pairs
-  const uint32_t nq = (w + 1) / 2;
+  const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
   uint8_t* Eprev = Ebase;  // wide blocks: bit lengths of v_n per column + 1, row above
   uint8_t* Ecur = Ebase + cols;
   if (!NARROW) {
@@ -498,7 +546,7 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
     for (uint32_t c0 = 0; c0 < nq; c0 += 32) {
       const uint32_t q = c0 + lane;
       const bool active = q < nq;
-      const uint32_t s = active ? sym[(size_t)r * nq + q] : 0;
+      const uint32_t s = active ? sym[(size_t)r * qs + q] : 0;
       const uint32_t inf = s & 0xFFFF;
       uint32_t U = s >> 16;
       if (!initial) {
