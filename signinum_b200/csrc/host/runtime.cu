@@ -1048,13 +1048,36 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
   std::vector<sgn_plan*> plans(K, nullptr);
   std::vector<sgn_status> statuses(n, SGN_OK);
   sgn_status st = SGN_OK;
+  // Pinned codestreams laid out back to back (16-byte padded): every chunk's
+  // upload is issued up front, into an arena per chunk, so the host link
+  // streams from the start of the call while the chunks are parsed and built
+  // (their plans then read the arenas in place).
+  auto pad16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+  bool up_front = K > 1 && datas[0] != nullptr;
+  for (size_t i = 0; up_front && i + 1 < n; ++i) up_front = datas[i + 1] == datas[i] + pad16(lens[i]);
+  up_front = up_front && is_pinned(datas[0]);
+  std::vector<uint8_t*> arenas(K, nullptr);
+  std::vector<std::vector<uint64_t>> roffs(K);
+  if (up_front) {
+    for (size_t c = 0; c < K && st == SGN_OK; ++c) {
+      const size_t b = cut[c], e = cut[c + 1];
+      if (e == b) continue;
+      const size_t bytes = (size_t)(datas[e - 1] - datas[b]) + pad16(lens[e - 1]);
+      cudaError_t ce = cudaMallocAsync((void**)&arenas[c], bytes, ctx->lanes[c]);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(arenas[c], datas[b], bytes, cudaMemcpyHostToDevice, ctx->lanes[c]);
+      if (ce != cudaSuccess) st = cuda_status(ce, "input upload");
+      roffs[c].resize(e - b);
+      for (size_t i = b; i < e; ++i) roffs[c][i - b] = (uint64_t)(datas[i] - datas[b]);
+    }
+  }
   for (size_t c = 0; c < K && st == SGN_OK; ++c) {
     const size_t b = cut[c], m = cut[c + 1] - b;
     if (m == 0) continue;
     plans[c] = new sgn_plan();
     try {
       st = build_plan(ctx, ctx->lanes[c], ctx->lane_staging[c], datas + b, lens + b, m, format,
-                      requests ? requests + b : nullptr, plans[c], nullptr, nullptr, nullptr, false);
+                      requests ? requests + b : nullptr, plans[c], arenas[c], up_front ? roffs[c].data() : nullptr,
+                      nullptr, false);
     } catch (const std::bad_alloc&) {
       st = set_error(SGN_ERR_OUT_OF_MEMORY, "host allocation failed");
     }
@@ -1083,6 +1106,11 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     release_plan(plans[c], ctx->lanes[c]);
     delete plans[c];
   }
+  for (size_t c = 0; c < K; ++c)
+    if (arenas[c]) {
+      if (st != SGN_OK) cudaStreamSynchronize(ctx->lanes[c]);
+      cudaFreeAsync(arenas[c], ctx->lanes[c]);
+    }
   if (st != SGN_OK) {
     for (size_t i = 0; i < n; ++i) {
       if (outs[i].device_ptr) sgn_surface_free_locked(ctx, &outs[i]);
