@@ -1057,9 +1057,70 @@ static void filter_cols(float* s, size_t w, size_t h, size_t y0) {
   }
 }
 
+// Irreversible 9/7: irreversible_filter_97i / irreversible_filter_97i_simd,
+// idwt.rs:767-836, :1016-1140 (Table F.4 constants; math::mul_add is fused on
+// an FMA host, as the B200 host is).
+static const float kNegAlpha = 1.5861343f, kNegBeta = 0.052980117f, kNegGamma = -0.8829111f,
+                   kNegDelta = -0.44350687f, kKappa = 1.2301741f;
+
+static void filter_row97(float* s, size_t w, size_t x0) {
+  if (w == 1) {
+    if (x0 % 2) s[0] *= 0.5f;
+    return;
+  }
+  size_t fe = x0 % 2, fo = 1 - fe;
+  const float inv_k = 1.0f / kKappa;
+  const float k0 = fe == 0 ? kKappa : inv_k, k1 = fe == 0 ? inv_k : kKappa;
+  for (size_t i = 0; i + 1 < w; i += 2) {
+    s[i] *= k0;
+    s[i + 1] *= k1;
+  }
+  if (w % 2 == 1) s[w - 1] *= k0;
+  auto step = [&](size_t first, float c) {
+    auto f = [&](float v, float l, float r) { return std::fma(l + r, c, v); };
+    if (first == 0) s[0] = f(s[0], s[pse_left(0, 1)], s[pse_right(0, 1, w)]);
+    size_t ms = first == 0 ? 2 : 1;
+    for (size_t i = ms; i + 1 < w; i += 2) s[i] = f(s[i], s[i - 1], s[i + 1]);
+    if ((w - 1) % 2 == first) {
+      size_t i = w - 1;
+      s[i] = f(s[i], s[pse_left(i, 1)], s[pse_right(i, 1, w)]);
+    }
+  };
+  step(fe, kNegDelta);
+  step(fo, kNegGamma);
+  step(fe, kNegBeta);
+  step(fo, kNegAlpha);
+}
+
+static void filter_cols97(float* s, size_t w, size_t h, size_t y0) {
+  if (h == 1) {
+    if (y0 % 2)
+      for (size_t c = 0; c < w; ++c) s[c] *= 0.5f;
+    return;
+  }
+  size_t fe = y0 % 2, fo = 1 - fe;
+  const float inv_k = 1.0f / kKappa;
+  const float k0 = fe == 0 ? kKappa : inv_k, k1 = fe == 0 ? inv_k : kKappa;
+  for (size_t row = 0; row + 1 < h; row += 2)
+    for (size_t c = 0; c < w; ++c) {
+      s[row * w + c] *= k0;
+      s[(row + 1) * w + c] *= k1;
+    }
+  if (h % 2 == 1)
+    for (size_t c = 0; c < w; ++c) s[(h - 1) * w + c] *= k0;
+  const size_t firsts[4] = {fe, fo, fe, fo};
+  const float cs[4] = {kNegDelta, kNegGamma, kNegBeta, kNegAlpha};
+  for (int k = 0; k < 4; ++k)
+    for (size_t row = firsts[k]; row < h; row += 2) {
+      size_t ra = pse_left(row, 1), rb = pse_right(row, 1, h);
+      for (size_t c = 0; c < w; ++c)
+        s[row * w + c] = std::fma(s[ra * w + c] + s[rb * w + c], cs[k], s[row * w + c]);
+    }
+}
+
 // filter_2d with interleave_samples, idwt.rs:535-712.
 static void idwt_level(const std::vector<float>& ll, const SubBand& hl, const SubBand& lh, const SubBand& hh,
-                       const IntRect& rect, std::vector<float>& out) {
+                       const IntRect& rect, std::vector<float>& out, bool reversible) {
   size_t w = rect.width(), h = rect.height();
   out.assign(w * h, 0.0f);
   uint32_t u0 = rect.x0, u1 = rect.x1, v0 = rect.y0, v1 = rect.y1;
@@ -1088,8 +1149,13 @@ static void idwt_level(const std::vector<float>& ll, const SubBand& hl, const Su
   if (u0 % 2 == 0) rows(lh.coef.data(), hh.coef.data(), orr, nvh);
   else rows(hh.coef.data(), lh.coef.data(), orr, nvh);
   if (w > 0 && h > 0) {
-    for (size_t y = 0; y < h; ++y) filter_row(out.data() + y * w, w, rect.x0);
-    filter_cols(out.data(), w, h, rect.y0);
+    if (reversible) {
+      for (size_t y = 0; y < h; ++y) filter_row(out.data() + y * w, w, rect.x0);
+      filter_cols(out.data(), w, h, rect.y0);
+    } else {
+      for (size_t y = 0; y < h; ++y) filter_row97(out.data() + y * w, w, rect.x0);
+      filter_cols97(out.data(), w, h, rect.y0);
+    }
   }
 }
 
@@ -1112,9 +1178,16 @@ static int32_t coefficient_to_i32(uint32_t v, uint8_t kmax) {
 static void decode_band(Storage& st, size_t bi, uint8_t res, const CompInfo& ci, const Header& h) {
   SubBand& sb = st.bands[bi];
   if (!ci.ht()) fail(ERR_UNSUPPORTED, "classic block coding is outside the oracle's scope");
-  float step = 1.0f;
-  if (ci.q.style != QNONE) fail(ERR_UNSUPPORTED, "quantized (irreversible) coding is outside the oracle's scope");
   auto em = ci.exponent_mantissa(sb.type, res);
+  // Dequantisation step (decode.rs:1130-1151): 2^(R_b - exponent) * (1 + mantissa / 2048),
+  // R_b = precision + log2 gain of the band (LL 0, HL/LH 1, HH 2); pow2i, math.rs:550-556.
+  float step = 1.0f;
+  if (ci.q.style != QNONE) {
+    int gain = sb.type == LL ? 0 : sb.type == HH ? 2 : 1;
+    int e = (int)ci.size.precision + gain - (int)em.first;
+    float p2 = e >= 0 ? (float)(1u << e) : 1.0f / (float)(1u << -e);
+    step = p2 * (1.0f + (float)em.second / 2048.0f);
+  }
   int nb = (int)ci.q.guard + (int)em.first - 1;
   if (nb < 0) fail(ERR_DECODE, "invalid bitplane count");
   if (nb > 32) fail(ERR_DECODE, "too many bitplanes");
@@ -1167,7 +1240,6 @@ static void decode_codestream(const uint8_t* data, size_t len, const uint32_t* t
   if (hdr_out) *hdr_out = h;
   for (auto& c : h.comps) {
     if (c.size.xr != 1 || c.size.yr != 1) fail(ERR_UNSUPPORTED, "sub-sampled components are outside the oracle's scope");
-    if (!c.cp.reversible) fail(ERR_UNSUPPORTED, "the 9/7 transform is outside the oracle's scope");
   }
   BitReader body(data + r.byte_pos(), len - r.byte_pos());
   std::vector<Tile> tiles = parse_tiles(body, h);
@@ -1208,7 +1280,7 @@ static void decode_codestream(const uint8_t* data, size_t len, const uint32_t* t
       IntRect rect = st.bands[cb.ll].rect;
       for (size_t d = 0; d < nd; ++d) {
         const auto& ids = cb.decomp[d];
-        idwt_level(cur, st.bands[ids[0]], st.bands[ids[1]], st.bands[ids[2]], cb.decomp_rect[d], nxt);
+        idwt_level(cur, st.bands[ids[0]], st.bands[ids[1]], st.bands[ids[2]], cb.decomp_rect[d], nxt, c.cp.reversible);
         std::swap(cur, nxt);
         rect = cb.decomp_rect[d];
       }
@@ -1238,12 +1310,22 @@ static void decode_codestream(const uint8_t* data, size_t len, const uint32_t* t
       if (c[0].cp.reversible != c[1].cp.reversible || c[1].cp.reversible != c[2].cp.reversible)
         fail(ERR_DECODE, "mct");
       float *y0 = planes.data[0].data(), *y1 = planes.data[1].data(), *y2 = planes.data[2].data();
-      for (size_t i = 0; i < planes.data[0].size(); ++i) {
-        float a = y0[i], b = y1[i], cc = y2[i];
-        float i1 = a - std::floor((cc + b) * 0.25f);
-        y0[i] = cc + i1;
-        y1[i] = i1;
-        y2[i] = b + i1;
+      if (c[0].cp.reversible) {
+        for (size_t i = 0; i < planes.data[0].size(); ++i) {
+          float a = y0[i], b = y1[i], cc = y2[i];
+          float i1 = a - std::floor((cc + b) * 0.25f);
+          y0[i] = cc + i1;
+          y1[i] = i1;
+          y2[i] = b + i1;
+        }
+      } else {
+        // Irreversible ICT (mct.rs:80-115), fused multiply-adds as on the SIMD path.
+        for (size_t i = 0; i < planes.data[0].size(); ++i) {
+          float a = y0[i], b = y1[i], cc = y2[i];
+          y0[i] = std::fma(cc, 1.402f, a);
+          y1[i] = std::fma(cc, -0.71414f, std::fma(b, -0.34413f, a));
+          y2[i] = std::fma(b, 1.772f, a);
+        }
       }
     }
     for (size_t ci = 0; ci < planes.data.size(); ++ci) {

@@ -28,11 +28,14 @@ def test_openhtj2k_ds0_ht_12_known_answer():
     assert got == bytes.fromhex(fx["gray_hex"])
 
 
-def test_irreversible_fixture_is_out_of_scope():
+def test_openhtj2k_ds0_ht_09_known_answer():
+    # crates/signinum-j2k-native/src/lib.rs:2941-2947,3474-3481: irreversible
+    # 9/7 with scalar-expounded quantisation, 17x37 gray, decoded samples by
+    # OpenJPH.  Exact: the oracle's float lifting rounds the same way here.
     fx = _fixtures()["openhtj2k_ds0_ht_09_b11"]
-    with pytest.raises(oracle.OracleError) as e:
-        oracle.decode(bytes.fromhex(fx["j2k_hex"]), 0)
-    assert e.value.status == 1
+    got, w, h = oracle.decode(bytes.fromhex(fx["j2k_hex"]), 0)
+    assert (w, h) == (17, 37)
+    assert got == bytes.fromhex(fx["gray_hex"])
 
 
 def _sha(arr):
