@@ -46,6 +46,18 @@ int sgn_j2k_encode_lossless(const uint8_t* pixels, uint32_t width, uint32_t heig
                             uint32_t bit_depth, const sgn_encode_options* options, uint8_t* out, size_t out_cap,
                             size_t* out_len);
 
+/* Irreversible HTJ2K encode, the lossy input of the 9/7 decode path: DC
+ * shift, ICT when options->use_mct and components >= 3, forward 9/7 and
+ * scalar expounded quantisation with the same relative step for every band
+ * (step_b = relative_step * 2^(bit_depth + gain_b), rounded to the
+ * 5-bit exponent / 11-bit mantissa form).  This mode has no counterpart in
+ * the reference (its encoder is lossless only); it exists to produce
+ * irreversible codestreams of any size for the decode path's parity tests.
+ * Returns as sgn_j2k_encode_lossless; -2 also for relative_step outside (0, 1). */
+int sgn_j2k_encode_irreversible(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
+                                uint32_t bit_depth, const sgn_encode_options* options, double relative_step,
+                                uint8_t* out, size_t out_cap, size_t* out_len);
+
 /* Seeded synthetic tiles (tight, interleaved). */
 void sgn_synth_he_rgb8(uint64_t seed, uint32_t width, uint32_t height, double noise_sigma, uint8_t* out);
 void sgn_synth_blank_rgb8(uint64_t seed, uint32_t width, uint32_t height, uint8_t* out);

@@ -59,6 +59,9 @@ __host__ __device__
 #endif
 inline uint32_t sym_words(uint32_t w, uint32_t h) { return (sym_row_stride(w) * ((h + 1) / 2) + 3) & ~3u; }
 
+// Irreversible (9/7) levels use the same tables: band pointers hold int32
+// coefficients that the kernel dequantises with `step`, level images (the
+// ll input after the first level, and `out`) hold f32 samples.
 struct IdwtJob {
   const int32_t* ll;   // ceil(w/2) x ceil(h/2)
   const int32_t* hl;   // floor(w/2) x ceil(h/2)
@@ -69,7 +72,8 @@ struct IdwtJob {
   uint32_t strips;      // strips across the level
   uint32_t unit_begin;  // first work unit of this job in its launch
   uint32_t seg;         // output rows per work unit (even)
-  uint32_t pad;
+  uint32_t ll_band;     // 9/7: ll is the LL band (dequantise) rather than a level image
+  float step[4];        // 9/7: dequantisation steps of ll, hl, lh, hh
 };
 
 enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
@@ -89,6 +93,8 @@ struct PackJob {
   uint32_t unit_begin;  // first work unit of this job in its launch
   uint32_t seg;         // output rows per work unit (even)
   uint32_t tile;        // batch index (status)
+  uint32_t ll_band;     // 9/7: ll[c] are LL bands (dequantise) rather than level images
+  float step[3][4];     // 9/7: dequantisation steps of ll, hl, lh, hh per component
 };
 
 }  // namespace sgn

@@ -1,4 +1,5 @@
-// C ABI of the lossless HTJ2K encoder and the synthetic tile generators.
+// C ABI of the HTJ2K encoder (lossless; irreversible for test inputs) and the
+// synthetic tile generators.
 #include <cstring>
 #include <vector>
 
@@ -8,10 +9,12 @@
 
 extern "C" {
 
-int sgn_j2k_encode_lossless(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
-                            uint32_t bit_depth, const sgn_encode_options* o, uint8_t* out, size_t out_cap,
-                            size_t* out_len) {
+static int encode_with(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
+                       uint32_t bit_depth, const sgn_encode_options* o, bool irreversible, double rel_step,
+                       uint8_t* out, size_t out_cap, size_t* out_len) {
   sgn::enc::EncodeParams p;
+  p.irreversible = irreversible;
+  p.rel_step = rel_step;
   p.width = width;
   p.height = height;
   p.comps = components;
@@ -32,6 +35,18 @@ int sgn_j2k_encode_lossless(const uint8_t* pixels, uint32_t width, uint32_t heig
   if (cs.size() > out_cap) return -4;
   std::memcpy(out, cs.data(), cs.size());
   return 0;
+}
+
+int sgn_j2k_encode_lossless(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
+                            uint32_t bit_depth, const sgn_encode_options* o, uint8_t* out, size_t out_cap,
+                            size_t* out_len) {
+  return encode_with(pixels, width, height, components, bit_depth, o, false, 0.0, out, out_cap, out_len);
+}
+
+int sgn_j2k_encode_irreversible(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
+                                uint32_t bit_depth, const sgn_encode_options* o, double relative_step,
+                                uint8_t* out, size_t out_cap, size_t* out_len) {
+  return encode_with(pixels, width, height, components, bit_depth, o, true, relative_step, out, out_cap, out_len);
 }
 
 void sgn_synth_he_rgb8(uint64_t seed, uint32_t w, uint32_t h, double sigma, uint8_t* out) {

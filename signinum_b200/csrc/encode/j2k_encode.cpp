@@ -8,12 +8,20 @@
 // bits raised to 2 with RCT), HT cleanup-only code blocks, one layer, one
 // precinct per resolution, SIZ/CAP/COD/QCD/[TLM]/SOT/SOD/EOC markers.
 //
+// The irreversible mode produces lossy inputs for the 9/7 decode path (it
+// has no counterpart in the reference, which encodes losslessly only): DC
+// shift, ICT, forward 9/7 lifting (Table F.4 factors) with vertical then
+// horizontal passes, and scalar expounded quantisation with one relative
+// step for every band, q = sign(y) floor(|y| / step_b),
+// step_b = 2^(bit_depth + gain_b - eps) (1 + mu / 2048).
+//
 // The HT block coder is written here from the HTJ2K cleanup-pass definition
 // (T.814): MEL run coding of quad significance in zero contexts, CxtVLC
 // codewords with UVLC exponent offsets in a backward-growing VLC stream, and
 // magnitude/sign bits in a forward stream, ending in the Scup trailer.  Every
 // context and exponent predictor mirrors what the decoder recomputes.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -424,18 +432,87 @@ struct Band {
 
 static inline int32_t floor_div(int32_t a, int sh) { return a >> sh; }
 
+// Whole-sample symmetric extension of a line of n samples with stride s.
+template <typename T>
+static T& ext(T* x, long i, size_t n, size_t s) {
+  if (i < 0) i = -i;
+  if (i >= (long)n) i = 2 * ((long)n - 1) - i;
+  return x[(size_t)i * s];
+}
+
 // Forward 5/3 lifting of one line (n samples, stride s), origin even.
 static void fwd53(int32_t* x, size_t n, size_t s) {
   if (n < 2) return;
-  auto at = [&](long i) -> int32_t& {
-    if (i < 0) i = -i;
-    if (i >= (long)n) i = 2 * ((long)n - 1) - i;
-    return x[(size_t)i * s];
-  };
+  auto at = [&](long i) -> int32_t& { return ext(x, i, n, s); };
   for (long i = 1; i < (long)n; i += 2) at(i) -= floor_div(at(i - 1) + at(i + 1), 1);
   for (long i = 0; i < (long)n; i += 2) at(i) += floor_div(at(i - 1) + at(i + 1) + 2, 2);
 }
 
+// Forward 9/7 lifting of one line, origin even: predict/update steps with
+// alpha, beta, gamma, delta, then low samples scaled by 1/K, high by K.
+static void fwd97(double* x, size_t n, size_t s) {
+  if (n < 2) return;
+  auto at = [&](long i) -> double& { return ext(x, i, n, s); };
+  const double a = -1.586134342059924, b = -0.052980118572961, g = 0.882911075530934, d = 0.443506852043971;
+  const double k = 1.230174104914001;
+  for (long i = 1; i < (long)n; i += 2) at(i) += a * (at(i - 1) + at(i + 1));
+  for (long i = 0; i < (long)n; i += 2) at(i) += b * (at(i - 1) + at(i + 1));
+  for (long i = 1; i < (long)n; i += 2) at(i) += g * (at(i - 1) + at(i + 1));
+  for (long i = 0; i < (long)n; i += 2) at(i) += d * (at(i - 1) + at(i + 1));
+  for (long i = 0; i < (long)n; ++i) at(i) *= (i % 2 == 0) ? 1.0 / k : k;
+}
+
+// L levels of a separable decomposition of a w x h plane: vertical then
+// horizontal lifting of the current LL, then de-interleaving.  hl/lh/hh[d]
+// hold level d (1 = finest); lw/lh_[d] the LL size after level d.
+template <typename T, typename Lift>
+static void decompose(std::vector<T> cur, uint32_t W, uint32_t H, uint32_t L, Lift lift, std::vector<T>& ll_out,
+                      std::vector<std::vector<T>>& hl, std::vector<std::vector<T>>& lh,
+                      std::vector<std::vector<T>>& hh, std::vector<uint32_t>& lw, std::vector<uint32_t>& lhh) {
+  uint32_t cw = W, ch = H;
+  hl.assign(L + 1, {});
+  lh.assign(L + 1, {});
+  hh.assign(L + 1, {});
+  lw.assign(L + 2, 0);
+  lhh.assign(L + 2, 0);
+  lw[0] = W;
+  lhh[0] = H;
+  for (uint32_t d = 1; d <= L; ++d) {
+    for (uint32_t x = 0; x < cw; ++x) lift(&cur[x], ch, cw);
+    for (uint32_t y = 0; y < ch; ++y) lift(&cur[(size_t)y * cw], cw, 1);
+    uint32_t lwd = (cw + 1) / 2, hwd = cw / 2, lhd = (ch + 1) / 2, hhd = ch / 2;
+    std::vector<T> ll((size_t)lwd * lhd);
+    hl[d].assign((size_t)hwd * lhd, 0);
+    lh[d].assign((size_t)lwd * hhd, 0);
+    hh[d].assign((size_t)hwd * hhd, 0);
+    for (uint32_t y = 0; y < ch; ++y)
+      for (uint32_t x = 0; x < cw; ++x) {
+        T v = cur[(size_t)y * cw + x];
+        if (y % 2 == 0 && x % 2 == 0) ll[(size_t)(y / 2) * lwd + x / 2] = v;
+        else if (y % 2 == 0) hl[d][(size_t)(y / 2) * hwd + x / 2] = v;
+        else if (x % 2 == 0) lh[d][(size_t)(y / 2) * lwd + x / 2] = v;
+        else hh[d][(size_t)(y / 2) * hwd + x / 2] = v;
+      }
+    cur.swap(ll);
+    cw = lwd;
+    ch = lhd;
+    lw[d] = cw;
+    lhh[d] = ch;
+  }
+  ll_out.swap(cur);
+}
+
+// Scalar quantisation of a band: sign(y) floor(|y| / step), magnitudes
+// clamped to the band's mb bit-planes.
+static std::vector<int32_t> quantize(const std::vector<double>& y, double step, uint32_t mb) {
+  std::vector<int32_t> q(y.size());
+  const double maxq = (double)((1u << std::min<uint32_t>(mb, 30)) - 1);
+  for (size_t i = 0; i < y.size(); ++i) {
+    double m = std::min(std::floor(std::fabs(y[i]) / step), maxq);
+    q[i] = y[i] < 0 ? -(int32_t)m : (int32_t)m;
+  }
+  return q;
+}
 
 static void put16(std::vector<uint8_t>& o, uint32_t v) { o.push_back((uint8_t)(v >> 8)); o.push_back((uint8_t)v); }
 static void put32(std::vector<uint8_t>& o, uint32_t v) { put16(o, v >> 16); put16(o, v & 0xFFFF); }
@@ -451,67 +528,81 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   }
   const uint32_t L = std::min(P.levels, maxl);
   const bool mct = P.mct && C >= 3;
-  const uint32_t guard = mct ? 2 : 1;
+  const bool irr = P.irreversible;
+  const uint32_t guard = (mct || irr) ? 2 : 1;
+  // Relative step of the irreversible path as 2^-eps (1 + mu / 2048).
+  uint32_t q_eps = 0, q_mu = 0;
+  if (irr) {
+    if (!(P.rel_step > 0.0) || P.rel_step >= 1.0) return -2;
+    while (q_eps < 24 && std::ldexp(1.0, -(int)q_eps) > P.rel_step) ++q_eps;
+    double m = std::round((P.rel_step * std::ldexp(1.0, (int)q_eps) - 1.0) * 2048.0);
+    q_mu = (uint32_t)std::min(std::max(m, 0.0), 2047.0);
+    if (q_eps < 1) return -2;
+  }
   const size_t N = (size_t)W * H;
-  std::vector<std::vector<int32_t>> comp(C, std::vector<int32_t>(N));
   const int32_t shift = 1 << (bd - 1);
-  for (size_t i = 0; i < N; ++i)
-    for (uint32_t c = 0; c < C; ++c) {
-      int32_t v = bd <= 8 ? pixels[i * C + c] : (int32_t)(pixels[(i * C + c) * 2] | (pixels[(i * C + c) * 2 + 1] << 8));
-      v &= (1 << bd) - 1;
-      comp[c][i] = v - shift;
+  auto sample = [&](size_t i, uint32_t c) -> int32_t {
+    int32_t v = bd <= 8 ? pixels[i * C + c] : (int32_t)(pixels[(i * C + c) * 2] | (pixels[(i * C + c) * 2 + 1] << 8));
+    return (v & ((1 << bd) - 1)) - shift;
+  };
+  std::vector<std::vector<int32_t>> comp(irr ? 0 : C, std::vector<int32_t>(N));
+  std::vector<std::vector<double>> compf(irr ? C : 0, std::vector<double>(N));
+  if (!irr) {
+    for (size_t i = 0; i < N; ++i)
+      for (uint32_t c = 0; c < C; ++c) comp[c][i] = sample(i, c);
+    if (mct) {
+      for (size_t i = 0; i < N; ++i) {
+        int32_t r = comp[0][i], g = comp[1][i], b = comp[2][i];
+        comp[0][i] = floor_div(r + 2 * g + b, 2);
+        comp[1][i] = b - g;
+        comp[2][i] = r - g;
+      }
     }
-  if (mct) {
-    for (size_t i = 0; i < N; ++i) {
-      int32_t r = comp[0][i], g = comp[1][i], b = comp[2][i];
-      comp[0][i] = floor_div(r + 2 * g + b, 2);
-      comp[1][i] = b - g;
-      comp[2][i] = r - g;
+  } else {
+    for (size_t i = 0; i < N; ++i)
+      for (uint32_t c = 0; c < C; ++c) compf[c][i] = sample(i, c);
+    if (mct) {
+      for (size_t i = 0; i < N; ++i) {
+        double r = compf[0][i], g = compf[1][i], b = compf[2][i];
+        compf[0][i] = 0.299 * r + 0.587 * g + 0.114 * b;
+        compf[1][i] = -0.168736 * r - 0.331264 * g + 0.5 * b;
+        compf[2][i] = 0.5 * r - 0.418688 * g - 0.081312 * b;
+      }
     }
   }
   // Per component: bands[0] = LL, then HL, LH, HH per resolution 1..L.
   std::vector<std::vector<Band>> bands(C);
   const uint32_t cbw = 1u << (P.cbw_exp + 2), cbh = 1u << (P.cbh_exp + 2);
-  std::vector<int32_t> tmp;
+  auto band_mb = [&](uint32_t gain) { return irr ? guard + q_eps - 1 : guard + bd + gain - 1; };
   for (uint32_t c = 0; c < C; ++c) {
-    std::vector<int32_t>& img = comp[c];
-    // Dimensions of LL at each level, and the band planes (level 1 = finest).
-    uint32_t cw = W, ch = H;
-    std::vector<std::vector<int32_t>> hl(L + 1), lh(L + 1), hh(L + 1);
-    std::vector<uint32_t> lw(L + 2), lhh(L + 2);
-    lw[0] = W;
-    lhh[0] = H;
-    std::vector<int32_t> cur = img;
-    for (uint32_t d = 1; d <= L; ++d) {
-      // Vertical then horizontal lifting on the current LL (cw x ch).
-      for (uint32_t x = 0; x < cw; ++x) fwd53(&cur[x], ch, cw);
-      for (uint32_t y = 0; y < ch; ++y) fwd53(&cur[(size_t)y * cw], cw, 1);
-      uint32_t lwd = (cw + 1) / 2, hwd = cw / 2, lhd = (ch + 1) / 2, hhd = ch / 2;
-      std::vector<int32_t> ll((size_t)lwd * lhd);
-      hl[d].assign((size_t)hwd * lhd, 0);
-      lh[d].assign((size_t)lwd * hhd, 0);
-      hh[d].assign((size_t)hwd * hhd, 0);
-      for (uint32_t y = 0; y < ch; ++y)
-        for (uint32_t x = 0; x < cw; ++x) {
-          int32_t v = cur[(size_t)y * cw + x];
-          if (y % 2 == 0 && x % 2 == 0) ll[(size_t)(y / 2) * lwd + x / 2] = v;
-          else if (y % 2 == 0) hl[d][(size_t)(y / 2) * hwd + x / 2] = v;
-          else if (x % 2 == 0) lh[d][(size_t)(y / 2) * lwd + x / 2] = v;
-          else hh[d][(size_t)(y / 2) * hwd + x / 2] = v;
-        }
-      cur.swap(ll);
-      cw = lwd;
-      ch = lhd;
-      lw[d] = cw;
-      lhh[d] = ch;
+    std::vector<int32_t> cur;
+    std::vector<std::vector<int32_t>> hl, lh, hh;
+    std::vector<uint32_t> lw, lhh;
+    if (!irr) {
+      decompose(std::move(comp[c]), W, H, L, fwd53, cur, hl, lh, hh, lw, lhh);
+    } else {
+      std::vector<double> llf;
+      std::vector<std::vector<double>> hlf, lhf, hhf;
+      decompose(std::move(compf[c]), W, H, L, fwd97, llf, hlf, lhf, hhf, lw, lhh);
+      auto step = [&](uint32_t gain) { return std::ldexp(1.0 + q_mu / 2048.0, (int)(bd + gain) - (int)q_eps); };
+      cur = quantize(llf, step(0), band_mb(0));
+      hl.assign(L + 1, {});
+      lh.assign(L + 1, {});
+      hh.assign(L + 1, {});
+      for (uint32_t d = 1; d <= L; ++d) {
+        hl[d] = quantize(hlf[d], step(1), band_mb(1));
+        lh[d] = quantize(lhf[d], step(1), band_mb(1));
+        hh[d] = quantize(hhf[d], step(2), band_mb(2));
+      }
     }
+    const uint32_t cw = lw[L], ch = lhh[L];
     auto make_band = [&](const std::vector<int32_t>& data, uint32_t w, uint32_t h, uint32_t gain) -> int {
       Band b;
       b.w = w;
       b.h = h;
       b.cbw = cbw;
       b.cbh = cbh;
-      b.mb = guard + bd + gain - 1;
+      b.mb = band_mb(gain);
       b.ncx = w ? (w + cbw - 1) / cbw : 0;
       b.ncy = h ? (h + cbh - 1) / cbh : 0;
       for (uint32_t by = 0; by < b.ncy; ++by)
@@ -619,15 +710,21 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   out.push_back((uint8_t)P.cbw_exp);
   out.push_back((uint8_t)P.cbh_exp);
   out.push_back(0x40);
-  out.push_back(1);
+  out.push_back(irr ? 0 : 1);  // wavelet: 0 = 9/7 irreversible, 1 = 5/3 reversible
   out.push_back(0xFF); out.push_back(0x5C);  // QCD
-  put16(out, 3 + 1 + 3 * L);
-  out.push_back((uint8_t)(guard << 5));
-  out.push_back((uint8_t)(bd << 3));
-  for (uint32_t l = 0; l < L; ++l) {
-    out.push_back((uint8_t)((bd + 1) << 3));
-    out.push_back((uint8_t)((bd + 1) << 3));
-    out.push_back((uint8_t)((bd + 2) << 3));
+  if (irr) {
+    put16(out, 3 + 2 * (1 + 3 * L));
+    out.push_back((uint8_t)((guard << 5) | 2));  // scalar expounded
+    for (uint32_t k = 0; k < 1 + 3 * L; ++k) put16(out, (q_eps << 11) | q_mu);
+  } else {
+    put16(out, 3 + 1 + 3 * L);
+    out.push_back((uint8_t)(guard << 5));
+    out.push_back((uint8_t)(bd << 3));
+    for (uint32_t l = 0; l < L; ++l) {
+      out.push_back((uint8_t)((bd + 1) << 3));
+      out.push_back((uint8_t)((bd + 1) << 3));
+      out.push_back((uint8_t)((bd + 2) << 3));
+    }
   }
   uint32_t psot = 12 + 2 + (uint32_t)tile.size();
   if (P.write_tlm) {

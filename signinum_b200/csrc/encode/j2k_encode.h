@@ -1,4 +1,5 @@
-// Internal interface of the lossless HTJ2K encoder and synthetic generators.
+// Internal interface of the HTJ2K encoder (lossless, and irreversible 9/7
+// for test inputs) and the synthetic generators.
 #pragma once
 
 #include <cstdint>
@@ -12,6 +13,10 @@ struct EncodeParams {
   int progression;  // 0 LRCP, 1 RLCP, 2 RPCL, 3 PCRL, 4 CPRL
   bool write_tlm;
   bool sop_eph;
+  // Irreversible path: ICT (with mct), 9/7, scalar expounded quantisation
+  // with relative step rel_step of every band's nominal range.
+  bool irreversible = false;
+  double rel_step = 1.0 / 256;
 };
 int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& out);
 int encode_ht_block(const int32_t* c, size_t stride, uint32_t w, uint32_t h, uint32_t Mb, std::vector<uint8_t>& out);

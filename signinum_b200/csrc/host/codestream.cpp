@@ -2,6 +2,7 @@
 #include "codestream.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <tuple>
 
@@ -83,7 +84,8 @@ struct CodingStyle {
 
 struct Quant {
   uint8_t style = 0, guard = 0;
-  std::vector<uint16_t> exps;  // exponent per band entry
+  std::vector<uint16_t> exps;   // exponent per band entry
+  std::vector<uint16_t> mants;  // mantissa per band entry (0 without quantisation)
 };
 
 struct Comp {
@@ -120,17 +122,20 @@ bool read_quant(Reader& r, size_t body, Quant& q) {
   q.style = s & 0x1F;
   q.guard = s >> 5;
   q.exps.clear();
+  q.mants.clear();
   if (q.style == 0) {
     for (size_t i = 0; i + 1 < body; ++i) {
       uint8_t v;
       if (!r.u8(v)) return false;
       q.exps.push_back((uint16_t)(v >> 3));
+      q.mants.push_back(0);
     }
   } else if (q.style == 1 || q.style == 2) {
     for (size_t i = 0; i + 2 < body + 1; i += 2) {
       uint16_t v;
       if (!r.u16(v)) return false;
       q.exps.push_back((uint16_t)(v >> 11));
+      q.mants.push_back((uint16_t)(v & 0x7FF));
     }
   } else {
     return false;
@@ -587,14 +592,16 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   for (auto& c : h.comps) {
     if (c.xr != 1 || c.yr != 1) fail(ST_UNSUPPORTED, "sub-sampled components are not supported by the CUDA path");
     if (!(c.cs.cbstyle & 0x40)) fail(ST_UNSUPPORTED, "classic (non-HT) block coding is not supported by the CUDA path");
-    if (c.cs.transform != 1) fail(ST_UNSUPPORTED, "the irreversible 9/7 transform is not supported by the CUDA path");
-    if (c.q.style != 0) fail(ST_UNSUPPORTED, "quantized coding is not supported by the CUDA path");
+    if (c.cs.transform != c0.cs.transform) fail(ST_UNSUPPORTED, "components with different wavelet transforms");
+    // The reversible path is integer arithmetic: a quantised 5/3 codestream
+    // (non-integer dequantised samples) is outside it.
+    if (c.cs.transform == 1 && c.q.style != 0) fail(ST_UNSUPPORTED, "quantized reversible coding is not supported by the CUDA path");
     if (c.cs.ndecomp != c0.cs.ndecomp) fail(ST_UNSUPPORTED, "components with different level counts");
     if (c.precision != c0.precision || c.precision > 16) fail(ST_UNSUPPORTED, "component precision not supported by the CUDA path");
     if ((c.cs.cbstyle & 0x08) != (c0.cs.cbstyle & 0x08)) fail(ST_UNSUPPORTED, "mixed code-block styles");
     size_t max_res = c.cs.ndecomp, n = c.q.exps.size();
     if (n == 0) fail(ST_DECODE, "missing step sizes");
-    if (max_res != 0 && 1 + (max_res - 1) * 3 + 2 >= n) fail(ST_DECODE, "insufficient exponents");
+    if (c.q.style != 1 && max_res != 0 && 1 + (max_res - 1) * 3 + 2 >= n) fail(ST_DECODE, "insufficient exponents");
   }
   if (h.layers > 1) fail(ST_UNSUPPORTED, "multi-layer HTJ2K packet assembly");
   const uint32_t W = h.gw, H = h.gh, L = c0.cs.ndecomp;
@@ -605,6 +612,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   T.bit_depth = c0.precision;
   T.levels = L;
   T.mct = h.mct;
+  T.reversible = c0.cs.transform == 1;
   T.causal = (c0.cs.cbstyle & 0x08) != 0;
   uint32_t skipped = 0;
   if (target) {
@@ -643,9 +651,31 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
         bool hx = b.type == BAND_HL || b.type == BAND_HH, hy = b.type == BAND_LH || b.type == BAND_HH;
         b.w = span(W, hx);
         b.h = span(H, hy);
-        size_t ei = res == 0 ? 0 : 1 + (size_t)(res - 1) * 3 + (b.type - 1);
-        if (ei >= h.comps[c].q.exps.size()) fail(ST_DECODE, "missing step size");
-        int nbp = (int)h.comps[c].q.guard + (int)h.comps[c].q.exps[ei] - 1;
+        // ComponentInfo::exponent_mantissa (codestream.rs:224-268): one entry
+        // per band, or, derived, the LL entry with the exponent moved by the
+        // band's level.
+        const Quant& q = h.comps[c].q;
+        int expo, mant;
+        if (q.style == 1) {
+          int e = (int)q.exps[0] - (int)L;
+          if (e < 0) fail(ST_DECODE, "invalid exponents");
+          expo = e + (int)(res == 0 ? L : L + 1 - res);
+          mant = q.mants[0];
+        } else {
+          size_t ei = res == 0 ? 0 : 1 + (size_t)(res - 1) * 3 + (b.type - 1);
+          if (ei >= q.exps.size()) fail(ST_DECODE, "missing step size");
+          expo = q.exps[ei];
+          mant = q.mants[ei];
+        }
+        // Dequantisation step (decode.rs:1130-1151): 2^(R_b - exponent) *
+        // (1 + mantissa / 2048), R_b = precision + log2 gain (LL 0, HL/LH 1,
+        // HH 2); exact in float.
+        b.step = 1.0f;
+        if (q.style != 0) {
+          const int gain = b.type == BAND_LL ? 0 : b.type == BAND_HH ? 2 : 1;
+          b.step = std::ldexp(1.0f + (float)mant / 2048.0f, (int)h.comps[c].precision + gain - expo);
+        }
+        int nbp = (int)q.guard + expo - 1;
         if (nbp < 0) fail(ST_DECODE, "invalid bitplane count");
         if (nbp > 32 && res < nres_dec) fail(ST_DECODE, "too many bitplanes");
         b.nbp = (uint8_t)std::min(nbp, 255);

@@ -37,6 +37,7 @@ enum BandType : uint8_t { BAND_LL = 0, BAND_HL = 1, BAND_LH = 2, BAND_HH = 3 };
 struct Band {
   uint8_t comp, res, type, nbp;  // nbp: number of magnitude bit-planes (E-2)
   uint32_t w, h;                 // sub-band dimensions (origin 0)
+  float step;                    // dequantisation step (1 without quantisation)
   uint64_t coef_off;             // element offset within the tile's coefficient block
 };
 
@@ -57,6 +58,7 @@ struct TileLayout {
   uint32_t bit_depth = 0;          // component 0 precision (all components equal)
   uint32_t levels = 0;             // decomposition levels
   bool mct = false;
+  bool reversible = true;          // 5/3 (integer path); false: 9/7 with dequantisation
   bool causal = false;             // vertically causal context (code-block style bit 3)
   uint32_t skipped = 0;            // resolution levels dropped for a reduced decode
   uint32_t out_w = 0, out_h = 0;   // dimensions of the decoded (possibly reduced) image

@@ -294,8 +294,10 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     return cuda_status(e, "symbol scratch");
 
   // IDWT rounds: round r-1 holds resolution r of every tile that has it.
-  std::vector<std::vector<IdwtJob>> rounds(max_rounds);
-  std::vector<PackJob> packs;
+  // Rounds 0 .. max_rounds-1 hold 5/3 levels, the next max_rounds the 9/7
+  // levels (each round is one launch of the kernel of its transform).
+  std::vector<std::vector<IdwtJob>> rounds(2 * (size_t)max_rounds);
+  std::vector<PackJob> packs, packs97;
   auto band_ptr = [&](size_t i, uint32_t c, uint32_t bi) -> int32_t* {
     const TileLayout& L = *work[i].L;
     return plan->d_coef + coef_off[i] + (uint64_t)c * L.coef_per_comp + L.bands[bi].coef_off;
@@ -326,9 +328,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
         j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
         j.unit_begin = 0;
         j.seg = idwt_segment_rows(j.h);
-        j.pad = 0;
+        j.ll_band = r == 1 ? 1 : 0;
+        j.step[0] = L.bands[b0].step;
+        for (uint32_t k = 0; k < 3; ++k) j.step[1 + k] = L.bands[b0 + 1 + (r - 1) * 3 + k].step;
+        if (!L.reversible) j.seg *= 2;  // 9/7 units re-read seven rows: longer segments
         if (j.w == 0 || j.h == 0) continue;
-        rounds[r - 1].push_back(j);
+        rounds[L.reversible ? r - 1 : max_rounds + r - 1].push_back(j);
       }
     }
     // Output surface.
@@ -348,6 +353,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     std::memset(&pj, 0, sizeof(pj));
     for (uint32_t c = 0; c < L.ncomp && c < 3; ++c) {
       uint32_t b0 = L.comp_band_begin[c];
+      pj.step[c][0] = L.bands[b0].step;
+      if (R > 0)
+        for (uint32_t k = 0; k < 3; ++k) pj.step[c][1 + k] = L.bands[b0 + 1 + (R - 1) * 3 + k].step;
       if (R == 0) {
         pj.ll[c] = band_ptr(i, c, b0);
       } else {
@@ -373,17 +381,20 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     pj.region_conv = tw.region_conv;
     uint32_t ax = tw.crop_x & ~(uint32_t)(kIdwtStripW - 1), ay = tw.crop_y & ~1u;
     pj.strips = (tw.crop_x + tw.crop_w - ax + kIdwtStripW - 1) / kIdwtStripW;
-    pj.seg = idwt_segment_rows(tw.crop_h);
+    pj.seg = idwt_segment_rows(tw.crop_h) * (L.reversible ? 1 : 2);
+    pj.ll_band = R <= 1 ? 1 : 0;
     uint32_t segs = (tw.crop_y + tw.crop_h - ay + pj.seg - 1) / pj.seg;
-    pj.unit_begin = plan->pack_ctas;
+    uint32_t& units = L.reversible ? plan->pack_ctas : plan->pack97_ctas;
+    pj.unit_begin = units;
     pj.tile = (uint32_t)i;
-    plan->pack_ctas += pj.strips * segs;
-    packs.push_back(pj);
+    units += pj.strips * segs;
+    (L.reversible ? packs : packs97).push_back(pj);
   }
   // Flatten the rounds.
   std::vector<IdwtJob> idwt;
-  for (auto& rj : rounds) {
-    RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0};
+  for (size_t k = 0; k < rounds.size(); ++k) {
+    auto& rj = rounds[k];
+    RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0, k >= max_rounds ? 1u : 0u};
     for (IdwtJob& j : rj) {
       j.unit_begin = ri.ctas;
       ri.ctas += j.strips * ((j.h + j.seg - 1) / j.seg);
@@ -392,6 +403,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (ri.njobs) plan->rounds.push_back(ri);
   }
   plan->npack = (uint32_t)packs.size();
+  plan->npack97 = (uint32_t)packs97.size();
+  packs.insert(packs.end(), packs97.begin(), packs97.end());
   if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
   if ((e = dalloc(&plan->d_refine, nref, s)) != cudaSuccess) return cuda_status(e, "refine list");
   if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
@@ -460,11 +473,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // The staging buffer is reused by the next call: finish the copies now
   // (callers that reuse it only after the plan has run pass sync_uploads false).
   if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
-  plan->launches = (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0);
+  plan->launches =
+      (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0) + (plan->npack97 ? 1 : 0);
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
   // Work-queue counters and the launch shape (an autotuned one when this
   // context has tuned a plan of the same signature).
-  plan->nqueues = (uint32_t)plan->rounds.size() + 2;
+  plan->nqueues = (uint32_t)plan->rounds.size() + 3;
   if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
   LaunchConfig cfg;
   {
@@ -488,7 +502,8 @@ uint64_t plan_signature(const sgn_plan* p) {
     return k;
   };
   return (uint64_t)p->format | (lg(p->nht + 1) << 4) | (lg(p->max_w) << 10) | (lg(p->ms_words) << 14) |
-         (lg(p->pack_ctas + 1) << 20) | ((uint64_t)p->rounds.size() << 26) | ((uint64_t)(p->nref > 0) << 31);
+         (lg(p->pack_ctas + 1) << 20) | ((uint64_t)p->rounds.size() << 26) | ((uint64_t)(p->nref > 0) << 31) |
+         ((uint64_t)lg(p->pack97_ctas + 1) << 32);
 }
 
 sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
@@ -506,6 +521,21 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
     p->graph = nullptr;
   }
   return SGN_OK;
+}
+
+cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas) {
+  const RoundInfo& r = p->rounds[k];
+  uint32_t* q = queued ? p->d_queue + 1 + k : nullptr;
+  return r.irreversible ? launch_idwt97_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q, ctas)
+                        : launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q, ctas);
+}
+
+cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas) {
+  uint32_t* q = queued ? p->d_queue + 1 + p->rounds.size() : nullptr;
+  cudaError_t e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s, q, ctas);
+  if (e == cudaSuccess)
+    e = launch_pack97(p->d_pack + p->npack, p->npack97, p->pack97_ctas, p->format, s, q ? q + 1 : nullptr, ctas);
+  return e;
 }
 
 void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
@@ -550,15 +580,9 @@ sgn_status execute(sgn_plan* p, cudaStream_t s) {
     return cuda_status(e, "HT MagSgn launch");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
-  for (size_t k = 0; k < p->rounds.size(); ++k) {
-    const RoundInfo& r = p->rounds[k];
-    if ((e = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.idwt_queue ? p->d_queue + 1 + k : nullptr,
-                               c.idwt_ctas)) != cudaSuccess)
-      return cuda_status(e, "IDWT launch");
-  }
-  if ((e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
-                       c.pack_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas)) != cudaSuccess)
-    return cuda_status(e, "pack launch");
+  for (size_t k = 0; k < p->rounds.size(); ++k)
+    if ((e = launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas)) != cudaSuccess) return cuda_status(e, "IDWT launch");
+  if ((e = launch_packs(p, s, c.pack_queue != 0, c.pack_ctas)) != cudaSuccess) return cuda_status(e, "pack launch");
   return SGN_OK;
 }
 
@@ -767,14 +791,9 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   chk(cudaEventRecord(ev[2], s));
   chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
   chk(cudaEventRecord(ev[3], s));
-  for (size_t k = 0; k < p->rounds.size(); ++k) {
-    const RoundInfo& r = p->rounds[k];
-    chk(launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, c.idwt_queue ? p->d_queue + 1 + k : nullptr,
-                          c.idwt_ctas));
-  }
+  for (size_t k = 0; k < p->rounds.size(); ++k) chk(launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas));
   chk(cudaEventRecord(ev[4], s));
-  chk(launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s,
-                  c.pack_queue ? p->d_queue + 1 + p->rounds.size() : nullptr, c.pack_ctas));
+  chk(launch_packs(p, s, c.pack_queue != 0, c.pack_ctas));
   chk(cudaEventRecord(ev[5], s));
   chk(cudaEventSynchronize(ev[5]));
   if (e == cudaSuccess) {
@@ -877,19 +896,14 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
     float ms = time_stage(s, reps, [&] {
       cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
-      for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) {
-        const RoundInfo& r = p->rounds[k];
-        x = launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q ? p->d_queue + 1 + k : nullptr, ictas);
-      }
+      for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, q != 0, ictas);
       return x;
     }, e);
     if (q == 0) idwt_default = ms;
     if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q;
     ms = time_stage(s, reps, [&] {
       cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
-      if (x == cudaSuccess)
-        x = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s, q ? p->d_queue + 1 + p->rounds.size() : nullptr,
-                        pctas);
+      if (x == cudaSuccess) x = launch_packs(p, s, q != 0, pctas);
       return x;
     }, e);
     if (q == 0) pack_default = ms;

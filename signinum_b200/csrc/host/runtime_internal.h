@@ -153,6 +153,7 @@ struct sgn_ctx {
 
 struct RoundInfo {
   uint32_t job_begin, njobs, ctas;
+  uint32_t irreversible;  // 9/7 jobs (launched by the f32 kernel)
 };
 
 struct sgn_plan {
@@ -176,12 +177,15 @@ struct sgn_plan {
   PackJob* d_pack = nullptr;
   uint32_t* d_status = nullptr;
   uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
+  // Pack jobs of irreversible tiles follow the npack reversible ones.
+  uint32_t npack97 = 0, pack97_ctas = 0;
   std::vector<RoundInfo> rounds;
   uint64_t launches = 0;
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
   // Launch shape and the device work-queue counters (one per queued launch:
-  // MagSgn, each IDWT round, pack), zeroed at the start of every execution.
+  // MagSgn, each IDWT round, pack, 9/7 pack), zeroed at the start of every
+  // execution.
   LaunchConfig cfg;
   uint32_t* d_queue = nullptr;
   uint32_t nqueues = 0;
@@ -219,6 +223,10 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s);
 // Fills in the persistent grid sizes of cfg for the plan's kernels and
 // device, and makes it the plan's launch shape (dropping any captured graph).
 sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& cfg);
+// IDWT round k (the 5/3 or the 9/7 kernel) and the pack launches, with the
+// plan's work-queue counters when `queued`, on persistent grids of `ctas`.
+cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas);
+cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas);
 // Workload signature for the autotuner cache: pixel format, job counts and
 // block shape classes.
 uint64_t plan_signature(const sgn_plan* p);

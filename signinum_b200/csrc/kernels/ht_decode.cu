@@ -117,6 +117,22 @@ struct Vlc {
     pos = (int)lcup - 3;
     remaining = scup - 2;
     unstuff = (b | 0x0F) > 0x8F;
+    init_words();
+  }
+  // The MagRef reader (new_mrp, ht_block_decode.rs:1377-1433): the whole
+  // refinement segment of n bytes from its last byte down, stuffing from the
+  // start.
+  __device__ void init_mrp(const uint8_t* d, uint32_t n) {
+    data = d;
+    tmp = 0;
+    bits = 0;
+    pos = (int)n - 1;
+    remaining = n;
+    unstuff = 1;
+    init_words();
+  }
+  // Word-refill state for bytes pos - 3 .. pos; every initialiser calls it.
+  __device__ __forceinline__ void init_words() {
     w_lo = w_hi = 0;
     wp = nullptr;
     sh8 = 0;
@@ -878,12 +894,7 @@ __global__ void ht_refine_kernel(const HtJob* __restrict__ jobs, const uint32_t*
         } else {
           // Backward reader over the refinement segment (new_mrp).
           Vlc mr;
-          mr.data = ref;
-          mr.pos = (int)lref - 1;
-          mr.remaining = lref;
-          mr.tmp = 0;
-          mr.bits = 0;
-          mr.unstuff = 1;
+          mr.init_mrp(ref, lref);
           uint32_t half = 1u << (p - 2);
           for (uint32_t y = 0; y < h; y += 4) {
             uint32_t csi = (y >> 2) * mstr;

@@ -414,6 +414,39 @@ __device__ __forceinline__ int lane_comp(const int4& v, int p) { return p == 0 ?
 // Row buffer per warp: up to 15 bytes of alignment shift + 128 pixels x 6 bytes.
 constexpr int kRowWords = (16 + kIdwtStripW * 6) / 4;
 
+// Writes one output row of a warp's strip: each lane's packed words (four
+// pixels of BPP bytes) are staged in the warp's row buffer so that the copied
+// range has the destination's alignment mod 16, then columns [xs, xe) go out
+// as the bytes up to the first 16-byte boundary, 16-byte vectors and a tail.
+template <int BPP>
+__device__ __forceinline__ void store_row(const PackJob& job, int y, int x0, int xs, int nbytes, int lane,
+                                          uint32_t* rowbuf, const uint32_t* wds) {
+  uint8_t* rowbytes = reinterpret_cast<uint8_t*>(rowbuf);
+  uint8_t* g = job.out + (uint64_t)(y - (int)job.cy) * job.pitch + (uint64_t)(xs - (int)job.cx) * BPP;
+  const int sh = (int)(((uintptr_t)g - (uintptr_t)((xs - x0) * BPP)) & 15);
+  if ((sh & 3) == 0) {
+    uint32_t* dst = rowbuf + (sh >> 2) + lane * BPP;
+#pragma unroll
+    for (int k = 0; k < BPP; ++k) dst[k] = wds[k];
+  } else {
+    uint8_t* dst = rowbytes + sh + lane * 4 * BPP;
+#pragma unroll
+    for (int q = 0; q < 4 * BPP; ++q) dst[q] = (uint8_t)(wds[q >> 2] >> (8 * (q & 3)));
+  }
+  __syncwarp();
+  const uint8_t* src = rowbytes + sh + (xs - x0) * BPP;
+  int head = (int)((16 - ((uintptr_t)g & 15)) & 15);
+  if (head > nbytes) head = nbytes;
+  if (lane < head) g[lane] = src[lane];
+  const int nvec = (nbytes - head) >> 4;
+  const uint4* sv = reinterpret_cast<const uint4*>(src + head);
+  uint4* gv = reinterpret_cast<uint4*>(g + head);
+  for (int k = lane; k < nvec; k += 32) gv[k] = sv[k];
+  const int done = head + (nvec << 4);
+  if (lane < nbytes - done) g[done + lane] = src[done + lane];
+  __syncwarp();
+}
+
 template <int NC, int FMT, bool DIRECT>
 __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
                                           int4* st) {
@@ -426,12 +459,8 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
   const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
   const int xs = max(x0, cx0), xe = min(x0 + kIdwtStripW, cx1);
   const int nbytes = (xe - xs) * BPP;
-  uint8_t* rowbytes = reinterpret_cast<uint8_t*>(rowbuf);
   auto emit = [&](int y, const int4* v) {
     if (y < cy0 || y >= cy1) return;  // warp-uniform
-    uint8_t* g = job.out + (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * BPP;
-    // Stage so that the copied range has the destination's alignment mod 16.
-    const int sh = (int)(((uintptr_t)g - (uintptr_t)((xs - x0) * BPP)) & 15);
     uint32_t wds[BPP];
 #pragma unroll
     for (int k = 0; k < BPP; ++k) wds[k] = 0;
@@ -454,29 +483,7 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
       c0 += shift;
       put_pixel<FMT, DIRECT>(wds, p, c0, c1, c2, bd, reg);
     }
-    if ((sh & 3) == 0) {
-      uint32_t* dst = rowbuf + (sh >> 2) + lane * BPP;
-#pragma unroll
-      for (int k = 0; k < BPP; ++k) dst[k] = wds[k];
-    } else {
-      uint8_t* dst = rowbytes + sh + lane * 4 * BPP;
-#pragma unroll
-      for (int q = 0; q < 4 * BPP; ++q) dst[q] = (uint8_t)(wds[q >> 2] >> (8 * (q & 3)));
-    }
-    __syncwarp();
-    // Copy-out of columns [xs, xe): bytes up to the first 16-byte boundary,
-    // 16-byte vectors, tail.
-    const uint8_t* src = rowbytes + sh + (xs - x0) * BPP;
-    int head = (int)((16 - ((uintptr_t)g & 15)) & 15);
-    if (head > nbytes) head = nbytes;
-    if (lane < head) g[lane] = src[lane];
-    const int nvec = (nbytes - head) >> 4;
-    const uint4* sv = reinterpret_cast<const uint4*>(src + head);
-    uint4* gv = reinterpret_cast<uint4*>(g + head);
-    for (int k = lane; k < nvec; k += 32) gv[k] = sv[k];
-    const int done = head + (nvec << 4);
-    if (lane < nbytes - done) g[done + lane] = src[done + lane];
-    __syncwarp();
+    store_row<BPP>(job, y, x0, xs, nbytes, lane, rowbuf, wds);
   };
   if (job.lifting) {
     if (NC == 3) {
@@ -538,6 +545,450 @@ __global__ void __launch_bounds__(kIdwtWarps * 32, 4) pack_kernel(const PackJob*
   }
   bool first = true;
   for (uint32_t unit; next_unit(queue, nunits, first, unit);) pack_one<FMT>(jobs, njobs, unit, rowbuf, st);
+}
+
+// ---------------------------------------------------------------------------
+// Irreversible 9/7 levels and the fused last level + inverse ICT + DC shift +
+// pack (crates/signinum-j2k-native/src/j2c/idwt.rs:767-836, :1016-1140;
+// mct.rs:80-115; decode.rs:1130-1151 for the dequantisation).
+//
+// Same mapping as the 5/3 kernels (a warp per 128-column strip of `seg`
+// rows, four columns per lane), in f32.  Every sample goes through the
+// reference's own sequence of roundings: band coefficient x step, then per
+// level the horizontal pass (even columns x K, odd x 1/K, then the four
+// lifting steps delta, gamma, beta, alpha as fma(left + right, c, x)), then
+// the same vertical pass.  Only __fmul_rn / __fadd_rn / fmaf are used, so no
+// multiply is contracted into a neighbouring add and results match the
+// reference's f32 arithmetic bit for bit.  Symmetric extension is done by
+// reflecting indices, which commutes with the lifting steps (reflected
+// positions compute the same sums in the other order, and f32 addition is
+// commutative).
+//
+// Horizontal: lane k holds columns c .. c+3 (c = 2b); each step needs one
+// neighbour from the adjacent lane (shuffles); the strip's edge lanes
+// compute the values outside the strip from halo samples (three on the
+// left, four on the right).  Vertical: a four-stage pipeline down the rows,
+// loading rows 2m+2 and 2m+3 per step and finishing rows 2m (after beta)
+// and 2m-1 (after alpha); a unit starting at row ys primes from row ys-3.
+
+constexpr float kNegAlpha97 = 1.5861343f, kNegBeta97 = 0.052980117f, kNegGamma97 = -0.8829111f,
+                kNegDelta97 = -0.44350687f, kKappa97 = 1.2301741f;
+constexpr int kWarps97 = 4;  // warps per CTA of the 9/7 pack kernel (its shared state is larger)
+
+namespace {
+
+// Whole-sample symmetric extension of any index into [0, n).
+__device__ __forceinline__ int fold97(int i, int n) {
+  if ((unsigned)i < (unsigned)n) return i;
+  if (n == 1) return 0;
+  const int p = 2 * (n - 1);
+  i = abs(i) % p;
+  return i < n ? i : p - i;
+}
+
+struct Src97 {
+  const int32_t* ll;
+  const int32_t* hl;
+  const int32_t* lh;
+  const int32_t* hh;
+  float q[4];    // dequantisation steps of ll, hl, lh, hh
+  int w, h;
+  bool ll_band;  // ll is the LL band; otherwise the previous level's f32 image
+  bool vec;
+};
+
+__device__ __forceinline__ Src97 make_src97(const int32_t* ll, const int32_t* hl, const int32_t* lh,
+                                            const int32_t* hh, const float* q, bool ll_band, int w, int h) {
+  const uintptr_t a = (uintptr_t)ll | (uintptr_t)hl | (uintptr_t)lh | (uintptr_t)hh;
+  return Src97{ll, hl, lh, hh, {q[0], q[1], q[2], q[3]}, w, h, ll_band, (w & 3) == 0 && (a & 7) == 0};
+}
+
+// Image columns c .. c+3 of one interleaved row (dequantised), and the edge
+// lanes' halo: lane 0 columns c-3, c-2, c-1; lane 31 columns c+4 .. c+7.
+struct Raw97 {
+  float e0, o0, e1, o1;
+  float h0, h1, h2, h3;
+};
+
+__device__ __forceinline__ Raw97 load97(const Src97& S, int y, int b, int lane) {
+  const int w = S.w;
+  y = fold97(y, S.h);
+  const int r = y >> 1;
+  const bool odd = y & 1;
+  const int lw = (w + 1) >> 1, hw = w >> 1;
+  const int32_t* Lr = (odd ? S.lh : S.ll) + (size_t)r * lw;
+  const int32_t* Hr = (odd ? S.hh : S.hl) + (size_t)r * hw;
+  const float ql = odd ? S.q[2] : S.q[0], qh = odd ? S.q[3] : S.q[1];
+  const bool lraw = !odd && !S.ll_band;
+  auto lo_of = [&](int32_t v) { return lraw ? __int_as_float(v) : __fmul_rn(__int2float_rn(v), ql); };
+  auto hi_of = [&](int32_t v) { return __fmul_rn(__int2float_rn(v), qh); };
+  auto at = [&](int j) {
+    j = fold97(j, w);
+    return (j & 1) ? hi_of(__ldg(Hr + (j >> 1))) : lo_of(__ldg(Lr + (j >> 1)));
+  };
+  const int c = 2 * b;
+  Raw97 R;
+  if (S.vec && c + 3 < w) {
+    const int2 l = __ldg(reinterpret_cast<const int2*>(Lr + b));
+    const int2 h = __ldg(reinterpret_cast<const int2*>(Hr + b));
+    R.e0 = lo_of(l.x);
+    R.o0 = hi_of(h.x);
+    R.e1 = lo_of(l.y);
+    R.o1 = hi_of(h.y);
+  } else {
+    R.e0 = at(c);
+    R.o0 = at(c + 1);
+    R.e1 = at(c + 2);
+    R.o1 = at(c + 3);
+  }
+  R.h0 = R.h1 = R.h2 = R.h3 = 0.0f;
+  if (lane == 0) {
+    R.h0 = at(c - 3);
+    R.h1 = at(c - 2);
+    R.h2 = at(c - 1);
+  } else if (lane == kLanes - 1) {
+    R.h0 = at(c + 4);
+    R.h1 = at(c + 5);
+    R.h2 = at(c + 6);
+    R.h3 = at(c + 7);
+  }
+  return R;
+}
+
+__device__ __forceinline__ float lstep(float l, float r, float c, float x) { return fmaf(__fadd_rn(l, r), c, x); }
+
+// Horizontal 9/7 synthesis of a loaded row: columns c .. c+3.
+__device__ __forceinline__ float4 lift97(const Raw97& R, int w, int lane, float K, float IK) {
+  if (w == 1) return make_float4(R.e0, 0.0f, 0.0f, 0.0f);
+  const float e0 = __fmul_rn(R.e0, K), o0 = __fmul_rn(R.o0, IK), e1 = __fmul_rn(R.e1, K), o1 = __fmul_rn(R.o1, IK);
+  // Halo, scaled by the parity of its columns.
+  const bool left = lane == 0;
+  const float h0 = __fmul_rn(R.h0, left ? IK : K), h1 = __fmul_rn(R.h1, left ? K : IK);
+  const float h2 = __fmul_rn(R.h2, left ? IK : K), h3 = __fmul_rn(R.h3, IK);
+  // delta: even columns.
+  float om1 = __shfl_up_sync(0xFFFFFFFFu, o1, 1);  // X[c-1]
+  if (left) om1 = h2;
+  const float e0a = lstep(om1, o0, kNegDelta97, e0);
+  const float e1a = lstep(o0, o1, kNegDelta97, e1);
+  // gamma: odd columns.
+  float ep4a = __shfl_down_sync(0xFFFFFFFFu, e0a, 1);  // E[c+4]
+  if (lane == kLanes - 1) ep4a = lstep(o1, h1, kNegDelta97, h0);
+  const float o0b = lstep(e0a, e1a, kNegGamma97, o0);
+  const float o1b = lstep(e1a, ep4a, kNegGamma97, o1);
+  // beta: even columns.
+  float om1b = __shfl_up_sync(0xFFFFFFFFu, o1b, 1);  // O[c-1]
+  if (left) {
+    const float em2a = lstep(h0, h2, kNegDelta97, h1);  // E[c-2] after delta
+    om1b = lstep(em2a, e0a, kNegGamma97, h2);
+  }
+  const float e0c = lstep(om1b, o0b, kNegBeta97, e0a);
+  const float e1c = lstep(o0b, o1b, kNegBeta97, e1a);
+  // alpha: odd columns.
+  float ep4c = __shfl_down_sync(0xFFFFFFFFu, e0c, 1);  // E[c+4]
+  if (lane == kLanes - 1) {
+    const float ep6a = lstep(h1, h3, kNegDelta97, h2);   // E[c+6] after delta
+    const float op5b = lstep(ep4a, ep6a, kNegGamma97, h1);  // O[c+5] after gamma
+    ep4c = lstep(o1b, op5b, kNegBeta97, ep4a);
+  }
+  const float o0d = lstep(e0c, e1c, kNegAlpha97, o0b);
+  const float o1d = lstep(e1c, ep4c, kNegAlpha97, o1b);
+  return make_float4(e0c, o0d, e1c, o1d);
+}
+
+__device__ __forceinline__ float4 scale4(float4 v, float k) {
+  return make_float4(__fmul_rn(v.x, k), __fmul_rn(v.y, k), __fmul_rn(v.z, k), __fmul_rn(v.w, k));
+}
+__device__ __forceinline__ float4 lstep4(float4 a, float4 b, float c, float4 x) {
+  return make_float4(lstep(a.x, b.x, c, x.x), lstep(a.y, b.y, c, x.y), lstep(a.z, b.z, c, x.z),
+                     lstep(a.w, b.w, c, x.w));
+}
+
+// Vertical 9/7 stream over rows [ys, ye) (ys even) of NC level images.
+// row(c, y) returns the horizontally lifted row y of component c (any y,
+// reflected inside); st(c, k) is the component's lifting state k (0 the
+// last odd input row, 1..3 the last rows after delta, gamma, beta);
+// emit(y, v[NC]) receives each finished row.
+template <int NC, typename Row, typename State, typename Emit>
+__device__ __forceinline__ void stream97(Row row, int h, int ys, int ye, float K, float IK, State st, Emit emit) {
+  float4 od[NC], ev[NC];
+  if (h == 1) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) ev[c] = row(c, 0);
+    emit(0, ev);
+    return;
+  }
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    st(c, 0) = scale4(row(c, ys - 3), IK);
+    st(c, 1) = zero;
+    st(c, 2) = zero;
+    st(c, 3) = zero;
+  }
+  for (int m = (ys >> 1) - 2; m <= (ye >> 1); ++m) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const float4 xe = scale4(row(c, 2 * m + 2), K), xo = scale4(row(c, 2 * m + 3), IK);
+      const float4 xp = st(c, 0), s1p = st(c, 1), s2p = st(c, 2), s3p = st(c, 3);
+      const float4 s1 = lstep4(xp, xo, kNegDelta97, xe);    // row 2m+2
+      const float4 s2 = lstep4(s1p, s1, kNegGamma97, xp);   // row 2m+1
+      const float4 s3 = lstep4(s2p, s2, kNegBeta97, s1p);   // row 2m, final
+      od[c] = lstep4(s3p, s3, kNegAlpha97, s2p);            // row 2m-1, final
+      ev[c] = s3;
+      st(c, 0) = xo;
+      st(c, 1) = s1;
+      st(c, 2) = s2;
+      st(c, 3) = s3;
+    }
+    const int yo = 2 * m - 1, yv = 2 * m;
+    if (yo >= ys && yo < ye) emit(yo, od);
+    if (yv >= ys && yv < ye) emit(yv, ev);
+  }
+}
+
+__device__ __forceinline__ void idwt97_unit(const IdwtJob* __restrict__ jobs, uint32_t njobs, uint32_t unit, float IK) {
+  const int lane = threadIdx.x & 31;
+  const IdwtJob& job = find_job(jobs, njobs, unit);
+  const uint32_t local = unit - job.unit_begin;
+  const int x0 = (int)(local % job.strips) * kIdwtStripW;
+  const int ys = (int)(local / job.strips) * (int)job.seg;
+  const int w = (int)job.w, h = (int)job.h;
+  const int ye = min(ys + (int)job.seg, h);
+  const Src97 S = make_src97(job.ll, job.hl, job.lh, job.hh, job.step, job.ll_band != 0, w, h);
+  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
+  float* out = reinterpret_cast<float*>(job.out);
+  const bool vec_out = (w & 3) == 0 && (((uintptr_t)out) & 15) == 0;
+  float4 state[4];
+  stream97<1>([&](int, int y) { return lift97(load97(S, y, b, lane), w, lane, kKappa97, IK); }, h, ys, ye,
+              kKappa97, IK, [&](int, int k) -> float4& { return state[k]; },
+              [&](int y, const float4* v) {
+                float* rowp = out + (size_t)y * w;
+                if (vec_out && col + 3 < w) {
+                  *reinterpret_cast<float4*>(rowp + col) = v[0];
+                } else {
+                  if (col < w) rowp[col] = v[0].x;
+                  if (col + 1 < w) rowp[col + 1] = v[0].y;
+                  if (col + 2 < w) rowp[col + 2] = v[0].z;
+                  if (col + 3 < w) rowp[col + 3] = v[0].w;
+                }
+              });
+}
+
+}  // namespace
+
+template <bool QUEUE>
+__global__ void __launch_bounds__(kIdwtWarps * 32) idwt97_level_kernel(const IdwtJob* __restrict__ jobs,
+                                                                       uint32_t njobs, uint32_t nunits,
+                                                                       uint32_t* queue) {
+  const float IK = __fdiv_rn(1.0f, kKappa97);
+  if (!QUEUE) {
+    const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
+    if (unit < nunits) idwt97_unit(jobs, njobs, unit, IK);
+    return;
+  }
+  bool first = true;
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);) idwt97_unit(jobs, njobs, unit, IK);
+}
+
+namespace {
+
+__device__ __forceinline__ float lane_compf(const float4& v, int p) {
+  return p == 0 ? v.x : p == 1 ? v.y : p == 2 ? v.z : v.w;
+}
+
+// `as u8` of a rounded f32: NaN and negatives 0, saturating at 255.
+__device__ __forceinline__ uint32_t sat_u8_round(float r) {
+  if (!(r > 0.0f)) return 0u;
+  if (r >= 255.0f) return 255u;
+  return (uint32_t)r;
+}
+
+// Sample conversions of the f32 path (crates/signinum-j2k-native/src/lib.rs:1772-1840,
+// :2202-2294; crates/signinum-j2k/src/decode.rs:345-356, :517-545).
+__device__ __forceinline__ uint32_t f_to_u8(float v, uint32_t bd, uint32_t region) {
+  const float r = roundf(v);
+  if (region) {
+    // sample_as_u8: round, clamp to the depth's maximum, rescale to 8 bits.
+    if (bd == 8) return (uint32_t)fminf(fmaxf(r, 0.0f), 255.0f);
+    const float maxv = bd >= 16 ? 65535.0f : (float)max((1 << bd) - 1, 1);
+    const float c = fminf(fmaxf(r, 0.0f), maxv);
+    return sat_u8_round(roundf(__fmul_rn(__fdiv_rn(c, maxv), 255.0f)));
+  }
+  // interleave_and_convert: rounded as u8 at 8 bits, else rescaled.
+  if (bd == 8) return sat_u8_round(r);
+  return sat_u8_round(roundf(__fmul_rn(__fdiv_rn(v, (float)((1u << bd) - 1)), 255.0f)));
+}
+
+// decode_native: round, clamp to [0, 2^bd - 1], widen depths <= 8 to 16 bits.
+__device__ __forceinline__ uint32_t f_to_u16(float v, uint32_t bd) {
+  const float maxv = (float)((1u << bd) - 1);
+  const float r = roundf(v);
+  const float c = r < 0.0f ? 0.0f : (r > maxv ? maxv : r);
+  if (bd <= 8) {
+    const uint32_t s = (uint32_t)(uint8_t)c, mx = max((1u << bd) - 1, 1u);
+    return (s * 65535u + mx / 2) / mx;
+  }
+  return (uint32_t)c;
+}
+
+template <int FMT>
+__device__ __forceinline__ void put_pixel97(uint32_t* wds, int p, float c0, float c1, float c2, uint32_t bd,
+                                            uint32_t reg) {
+  constexpr int B = pack_bpp<FMT>();
+  const int q = p * B;
+  if (FMT == PACK_GRAY8) {
+    put_byte(wds, q, f_to_u8(c0, bd, reg));
+  } else if (FMT == PACK_RGB8 || FMT == PACK_RGBA8) {
+    put_byte(wds, q, f_to_u8(c0, bd, reg));
+    put_byte(wds, q + 1, f_to_u8(c1, bd, reg));
+    put_byte(wds, q + 2, f_to_u8(c2, bd, reg));
+    if (FMT == PACK_RGBA8) put_byte(wds, q + 3, 255u);
+  } else if (FMT == PACK_GRAY16) {
+    const uint32_t a = f_to_u16(c0, bd);
+    put_byte(wds, q, a & 0xFF);
+    put_byte(wds, q + 1, a >> 8);
+  } else {
+    const uint32_t a = f_to_u16(c0, bd), g = f_to_u16(c1, bd), c = f_to_u16(c2, bd);
+    put_byte(wds, q, a & 0xFF);
+    put_byte(wds, q + 1, a >> 8);
+    put_byte(wds, q + 2, g & 0xFF);
+    put_byte(wds, q + 3, g >> 8);
+    put_byte(wds, q + 4, c & 0xFF);
+    put_byte(wds, q + 5, c >> 8);
+  }
+}
+
+// Slots of a lane's 9/7 lifting state in shared memory: 4 per component.
+constexpr int kSlots97 = 4 * 3;
+
+template <int NC, int FMT>
+__device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
+                                            float4* st, float IK) {
+  constexpr int BPP = pack_bpp<FMT>();
+  const int w = (int)job.w, h = (int)job.h;
+  const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
+  const uint32_t bd = job.bit_depth, reg = job.region_conv;
+  const float shift = (float)(1u << (bd - 1));
+  const bool ict = NC == 3 && job.mct;
+  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
+  const int xs = max(x0, cx0), xe = min(x0 + kIdwtStripW, cx1);
+  const int nbytes = (xe - xs) * BPP;
+  auto emit = [&](int y, const float4* v) {
+    if (y < cy0 || y >= cy1) return;  // warp-uniform
+    uint32_t wds[BPP];
+#pragma unroll
+    for (int k = 0; k < BPP; ++k) wds[k] = 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      float c0 = lane_compf(v[0], p), c1 = 0.0f, c2 = 0.0f;
+      if (NC == 3) {
+        c1 = lane_compf(v[1], p);
+        c2 = lane_compf(v[2], p);
+        if (ict) {
+          // mct.rs:80-115 with fused multiply-adds.
+          const float r = fmaf(c2, 1.402f, c0);
+          const float g = fmaf(c2, -0.71414f, fmaf(c1, -0.34413f, c0));
+          const float bl = fmaf(c1, 1.772f, c0);
+          c0 = r;
+          c1 = g;
+          c2 = bl;
+        }
+        c1 = __fadd_rn(c1, shift);
+        c2 = __fadd_rn(c2, shift);
+      }
+      c0 = __fadd_rn(c0, shift);
+      put_pixel97<FMT>(wds, p, c0, c1, c2, bd, reg);
+    }
+    store_row<BPP>(job, y, x0, xs, nbytes, lane, rowbuf, wds);
+  };
+  auto src = [&](int c) {
+    return make_src97(job.ll[c], job.hl[c], job.lh[c], job.hh[c], job.step[c], job.ll_band != 0, w, h);
+  };
+  if (job.lifting) {
+    auto row = [&](int c, int y) { return lift97(load97(src(c), y, b, lane), w, lane, kKappa97, IK); };
+    if (NC == 3) {
+      stream97<3>(row, h, ys, ye, kKappa97, IK, [&](int c, int k) -> float4& { return st[(c * 4 + k) * kLanes + lane]; },
+                  emit);
+    } else {
+      float4 state[4];
+      stream97<1>(row, h, ys, ye, kKappa97, IK, [&](int, int k) -> float4& { return state[k]; }, emit);
+    }
+  } else {
+    // Nothing to lift: the image is the LL band itself (dequantised).
+    for (int y = ys; y < ye; ++y) {
+      float4 v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int32_t* rowp = job.ll[c] + (size_t)y * w;
+        const float q = job.step[c][0];
+        auto at = [&](int k) { return col + k < w ? __fmul_rn(__int2float_rn(__ldg(rowp + col + k)), q) : 0.0f; };
+        v[c] = make_float4(at(0), at(1), at(2), at(3));
+      }
+      emit(y, v);
+    }
+  }
+}
+
+}  // namespace
+
+template <int FMT, bool QUEUE>
+__global__ void __launch_bounds__(kWarps97 * 32) pack97_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+                                                               uint32_t nunits, uint32_t* queue) {
+  __shared__ __align__(16) uint32_t rowbufs[kWarps97][kRowWords];
+  __shared__ float4 states[kWarps97][kSlots97 * kLanes];
+  const float IK = __fdiv_rn(1.0f, kKappa97);
+  uint32_t* rowbuf = rowbufs[threadIdx.x >> 5];
+  float4* st = states[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  auto one = [&](uint32_t unit) {
+    const PackJob& job = find_job(jobs, njobs, unit);
+    const uint32_t local = unit - job.unit_begin;
+    const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
+    const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
+    const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
+    if (job.ncomp >= 3) pack97_unit<3, FMT>(job, x0, ys, ye, lane, rowbuf, st, IK);
+    else pack97_unit<1, FMT>(job, x0, ys, ye, lane, rowbuf, st, IK);
+  };
+  if (!QUEUE) {
+    const uint32_t unit = blockIdx.x * kWarps97 + (threadIdx.x >> 5);
+    if (unit < nunits) one(unit);
+    return;
+  }
+  bool first = true;
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);) one(unit);
+}
+
+cudaError_t launch_idwt97_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
+                                uint32_t* queue, uint32_t persistent_ctas) {
+  if (njobs == 0 || nunits == 0) return cudaSuccess;
+  uint32_t ctas = (nunits + kIdwtWarps - 1) / kIdwtWarps;
+  if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
+  if (queue) idwt97_level_kernel<true><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, queue);
+  else idwt97_level_kernel<false><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack97(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
+                          uint32_t* queue, uint32_t persistent_ctas) {
+  if (njobs == 0 || nunits == 0) return cudaSuccess;
+  uint32_t ctas = (nunits + kWarps97 - 1) / kWarps97;
+  if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
+  const dim3 grid(ctas), block(kWarps97 * 32);
+#define SGN_PACK97_LAUNCH(F)                                                                   \
+  case F:                                                                                       \
+    if (queue) pack97_kernel<F, true><<<grid, block, 0, stream>>>(jobs, njobs, nunits, queue); \
+    else pack97_kernel<F, false><<<grid, block, 0, stream>>>(jobs, njobs, nunits, nullptr);    \
+    break;
+  switch (fmt) {
+    SGN_PACK97_LAUNCH(PACK_GRAY8)
+    SGN_PACK97_LAUNCH(PACK_RGB8)
+    SGN_PACK97_LAUNCH(PACK_RGBA8)
+    SGN_PACK97_LAUNCH(PACK_GRAY16)
+    SGN_PACK97_LAUNCH(PACK_RGB16)
+    default: return cudaErrorInvalidValue;
+  }
+#undef SGN_PACK97_LAUNCH
+  return cudaGetLastError();
 }
 
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,

@@ -43,5 +43,11 @@ cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nuni
 cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
                         uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
 cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm);
+// Irreversible (9/7) forms of the two launches above, same arguments; the
+// pack units of launch_pack97 run four warps per CTA.
+cudaError_t launch_idwt97_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
+                                uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
+cudaError_t launch_pack97(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
+                          uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
 
 }  // namespace sgn

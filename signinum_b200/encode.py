@@ -51,6 +51,24 @@ def encode_lossless(pixels: np.ndarray, width: int, height: int, components: int
     return out[: n.value].tobytes()
 
 
+def encode_irreversible(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int,
+                        relative_step: float = 1.0 / 256, levels: int = 5, cb_exp: int = 4, use_mct: bool = True,
+                        progression: int = 0, cb_exp_h: int | None = None) -> bytes:
+    """Lossy 9/7 codestream (ICT, scalar expounded quantisation) for the
+    irreversible decode path's tests; same sample layout as encode_lossless."""
+    px = np.ascontiguousarray(pixels)
+    opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression, 0, 0)
+    cap = px.nbytes * 2 + 65536
+    out = np.zeros(cap, np.uint8)
+    n = ctypes.c_size_t()
+    rc = _native.encode_lib().sgn_j2k_encode_irreversible(px.ctypes.data, width, height, components, bit_depth,
+                                                          ctypes.byref(opts), relative_step, out.ctypes.data, cap,
+                                                          ctypes.byref(n))
+    if rc != 0:
+        raise ValueError(f"encode failed ({rc})")
+    return out[: n.value].tobytes()
+
+
 def he_rgb8(seed: int, width: int, height: int, sigma: float = 6.0) -> np.ndarray:
     out = np.zeros(width * height * 3, np.uint8)
     _native.encode_lib().sgn_synth_he_rgb8(seed, width, height, sigma, out.ctypes.data)

@@ -67,3 +67,19 @@ def jp2_wrap(codestream: bytes, width: int, height: int, comps: int, bit_depth: 
         "jp2c": _box(b"jp2c", codestream, jp2c_form),
     }
     return b"".join(parts[k] for k in order)
+
+
+def random_irreversible(rng, max_side=80):
+    """A seeded lossy 9/7 codestream (ICT for RGB, expounded quantisation)."""
+    w = int(rng.integers(1, max_side))
+    h = int(rng.integers(1, max_side))
+    comps = int(rng.choice([1, 3]))
+    bd = int(rng.choice([8, 8, 12, 16])) if comps == 1 else int(rng.choice([8, 8, 8, 10]))
+    px = random_tile(rng, w, h, comps, bd, int(rng.integers(0, 3)))
+    cbw = int(rng.integers(0, 5))
+    cbh = min(int(rng.integers(0, 5)), 8 - cbw)
+    step = float(rng.choice([1 / 16, 1 / 100, 1 / 256, 1 / 1000, 3 / 4096]))
+    cs = encode.encode_irreversible(px.reshape(-1).view(np.uint8), w, h, comps, bd, step,
+                                    levels=int(rng.integers(0, 7)), cb_exp=cbw, cb_exp_h=cbh,
+                                    use_mct=bool(rng.integers(0, 4)), progression=int(rng.choice([0, 1, 2, 3, 4])))
+    return cs, px, w, h, comps, bd
