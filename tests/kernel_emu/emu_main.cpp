@@ -1,0 +1,251 @@
+// CPU emulation driver (test infrastructure): decodes each codestream given
+// on the command line through every decode kernel (HT VLC, MagSgn,
+// refinement, IDWT levels, pack), compiled for the host with cuda_shim.h and
+// run on CPU threads, with the job tables the runtime builds for one tile at
+// full resolution (build_plan_impl in host/runtime.cu: HT jobs with symbol
+// offsets and the refinement list, one IDWT job per component and level,
+// one pack job).  The coefficients after the HT kernels are compared with
+// the oracle's block decoder, the pixels with the oracle's decode.  Usage:
+// emu <pixel formats, e.g. 134> <codestream>...; prints one line per codestream and
+// exits non-zero on any difference.
+#include <fstream>
+#include <iterator>
+#include <memory>
+#include <thread>
+#include <vector>
+#include "cuda_shim.h"
+#include "device_plan.h"
+#include "host/codestream.h"
+#include "oracle_internal.h"
+
+thread_local dim3e threadIdx, blockIdx;
+dim3e blockDim, gridDim;
+thread_local WarpEmu* g_warp;
+thread_local std::barrier<>* g_block;
+alignas(16) uint8_t g_dyn_smem[232448];
+
+namespace sgn {
+void emu_tables();
+void emu_vlc(const HtJob*, uint32_t, const uint8_t*, uint32_t*);
+void emu_magsgn(const HtJob*, uint32_t, const uint8_t*, const uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t);
+void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t*, uint32_t*);
+void emu_idwt(bool, const IdwtJob*, uint32_t, uint32_t);
+void emu_pack(bool, int, const PackJob*, uint32_t, uint32_t);
+int emu_pack_warps(bool);
+size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps);
+}
+extern "C" int oracle_decode(const uint8_t*, size_t, int, int, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
+                             uint8_t*, size_t, uint32_t*, uint32_t*);
+
+// One launch: blockDim threads run every CTA of the grid in turn (a CTA
+// barrier between CTAs, since static shared memory is reused).
+template <class F> void launch(unsigned grid, unsigned block, F kernel) {
+  if (grid == 0) return;
+  blockDim.x = block;
+  gridDim.x = grid;
+  std::barrier<> bb(block);
+  std::vector<std::unique_ptr<WarpEmu>> warps;
+  for (unsigned w = 0; w < block / 32; ++w) warps.emplace_back(new WarpEmu);
+  std::vector<std::thread> ts;
+  for (unsigned t = 0; t < block; ++t)
+    ts.emplace_back([&, t] {
+      threadIdx.x = t;
+      g_warp = warps[t / 32].get();
+      g_block = &bb;
+      for (unsigned b = 0; b < grid; ++b) {
+        blockIdx.x = b;
+        kernel();
+        bb.arrive_and_wait();
+      }
+    });
+  for (auto& t : ts) t.join();
+}
+
+static int32_t to_i32(uint32_t v, uint32_t nbp) {
+  uint32_t shift = nbp >= 31 ? 0 : 31 - nbp;
+  int32_t m = (int32_t)((v & 0x7FFFFFFFu) >> shift);
+  return (v & 0x80000000u) ? -m : m;
+}
+static int bpp_of(int f) { return f == 0 ? 1 : f == 1 ? 3 : f == 2 ? 4 : f == 3 ? 2 : 6; }
+
+int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
+  using namespace sgn;
+  TileLayout T;
+  try {
+    parse_tile(d.data(), d.size(), nullptr, T);
+  } catch (ParseError& e) {
+    printf("parse error %d %s\n", e.status, e.message.c_str());
+    return 2;
+  }
+  const uint32_t nc = T.ncomp;
+  const bool irr = !T.reversible;
+  // Arena: the codestream, 16-byte padded as in the runtime.
+  std::vector<uint8_t> arena((d.size() + 15) & ~(size_t)15, 0);
+  std::memcpy(arena.data(), d.data(), d.size());
+  std::vector<int32_t> coef(T.coef_per_comp * nc, 0x7F7F7F7F), ref(T.coef_per_comp * nc, 0);
+  // HT jobs (runtime passes A/B for one tile).
+  std::vector<HtJob> jobs;
+  std::vector<uint32_t> refine;
+  uint64_t sym = 0;
+  uint32_t ms_words = 8, max_w = 1;
+  for (const CodeBlock& cb : T.blocks) {
+    const Band& b = T.bands[cb.band];
+    max_w = std::max<uint32_t>(max_w, cb.w);
+    HtJob j;
+    std::memset(&j, 0, sizeof(j));
+    j.src = cb.cleanup_off;
+    j.dst = (uint64_t)b.comp * T.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+    j.lcup = cb.lcup;
+    j.stride = b.w;
+    j.lref = (uint16_t)cb.lref;
+    j.w = cb.w;
+    j.h = cb.h;
+    j.mmsb = cb.missing_msbs;
+    j.passes = cb.passes;
+    j.nbp = b.nbp;
+    j.flags = T.causal ? 1 : 0;
+    if (cb.passes) {
+      j.sym = sym;
+      sym += sym_words(cb.w, cb.h);
+    }
+    if (cb.passes > 1) refine.push_back((uint32_t)jobs.size());
+    if (cb.passes && cb.lcup >= 2) {
+      const uint8_t* seg = d.data() + cb.cleanup_off;
+      uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
+      if (scup <= cb.lcup) ms_words = std::max<uint32_t>(ms_words, (cb.lcup - scup + 15) / 4 + 2);
+    }
+    if (cb.passes && cb.lref && cb.ref_off != cb.cleanup_off + cb.lcup) printf("refinement not contiguous\n");
+    jobs.push_back(j);
+    // Oracle block decode.
+    if (!cb.passes || b.nbp <= cb.missing_msbs) {
+      for (uint32_t y = 0; y < cb.h; ++y)
+        for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = 0;
+      continue;
+    }
+    std::vector<uint32_t> buf((size_t)cb.w * cb.h);
+    static const uint8_t empty = 0;
+    if (!oracle::ht_block_decode(cb.lcup ? d.data() + cb.cleanup_off : &empty, cb.lcup,
+                                 cb.lref ? d.data() + cb.ref_off : &empty, cb.lref, cb.missing_msbs, cb.passes, cb.w,
+                                 cb.h, cb.w, T.causal, buf.data()))
+      printf("oracle block decode failure\n");
+    for (uint32_t y = 0; y < cb.h; ++y)
+      for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = to_i32(buf[(size_t)y * cb.w + x], b.nbp);
+  }
+  std::vector<uint32_t> symbols(std::max<uint64_t>(sym, 1), 0xDEADBEEF);
+  std::vector<uint32_t> status(1, 0);
+  const uint32_t n = (uint32_t)jobs.size();
+  launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols.data()); });
+  const size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, 8);
+  if (smem > sizeof(g_dyn_smem)) { printf("smem too large\n"); return 2; }
+  launch((n + 7) / 8, 256, [&] {
+    emu_magsgn(jobs.data(), n, arena.data(), symbols.data(), coef.data(), status.data(), ms_words, max_w);
+  });
+  const uint32_t nr = (uint32_t)refine.size();
+  if (nr) launch((nr + 63) / 64, 64, [&] { emu_refine(jobs.data(), refine.data(), nr, arena.data(), coef.data(), status.data()); });
+  size_t cdiff = 0;
+  for (size_t i = 0; i < coef.size(); ++i) cdiff += coef[i] != ref[i];
+  // IDWT levels and pack (runtime plan for one tile, full image).
+  const uint32_t L = T.levels, R = L;
+  auto res_dim = [&](uint32_t r, bool wd) {
+    uint32_t sh = L - r;
+    uint64_t v = wd ? T.width : T.height;
+    return (uint32_t)((v + (1ull << sh) - 1) >> sh);
+  };
+  size_t lvl_size = R >= 2 ? (size_t)res_dim(R - 1, true) * res_dim(R - 1, false) : 0;
+  std::vector<std::vector<int32_t>> lvl(nc * 2);
+  for (auto& v : lvl) v.assign(lvl_size, 0);
+  auto band_ptr = [&](uint32_t c, uint32_t bi) { return coef.data() + (size_t)c * T.coef_per_comp + T.bands[bi].coef_off; };
+  for (uint32_t r = 1; r < R; ++r) {
+    std::vector<IdwtJob> ij;
+    uint32_t units = 0;
+    for (uint32_t c = 0; c < nc; ++c) {
+      uint32_t b0 = T.comp_band_begin[c];
+      IdwtJob j;
+      j.ll = r == 1 ? band_ptr(c, b0) : lvl[c * 2 + ((r - 1) & 1)].data();
+      j.hl = band_ptr(c, b0 + 1 + (r - 1) * 3);
+      j.lh = band_ptr(c, b0 + 2 + (r - 1) * 3);
+      j.hh = band_ptr(c, b0 + 3 + (r - 1) * 3);
+      j.out = lvl[c * 2 + (r & 1)].data();
+      j.w = res_dim(r, true);
+      j.h = res_dim(r, false);
+      j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
+      j.seg = idwt_segment_rows(j.h) * (irr ? 2 : 1);
+      j.ll_band = r == 1;
+      j.step[0] = T.bands[b0].step;
+      for (int k = 0; k < 3; ++k) j.step[1 + k] = T.bands[b0 + 1 + (r - 1) * 3 + k].step;
+      j.unit_begin = units;
+      if (j.w == 0 || j.h == 0) continue;
+      units += j.strips * ((j.h + j.seg - 1) / j.seg);
+      ij.push_back(j);
+    }
+    if (!ij.empty())
+      launch((units + kIdwtWarps - 1) / kIdwtWarps, kIdwtWarps * 32, [&] { emu_idwt(irr, ij.data(), (uint32_t)ij.size(), units); });
+  }
+  size_t nd_total = 0;
+  for (int fmt : fmts) {
+    const int bpp = bpp_of(fmt);
+    const uint32_t W = T.width, H = T.height;
+    std::vector<uint8_t> out((size_t)W * H * bpp + 1, 0xCD);
+    PackJob pj;
+    std::memset(&pj, 0, sizeof(pj));
+    for (uint32_t c = 0; c < nc && c < 3; ++c) {
+      uint32_t b0 = T.comp_band_begin[c];
+      pj.step[c][0] = T.bands[b0].step;
+      if (R == 0) {
+        pj.ll[c] = band_ptr(c, b0);
+      } else {
+        for (int k = 0; k < 3; ++k) pj.step[c][1 + k] = T.bands[b0 + 1 + (R - 1) * 3 + k].step;
+        pj.ll[c] = R == 1 ? band_ptr(c, b0) : lvl[c * 2 + ((R - 1) & 1)].data();
+        pj.hl[c] = band_ptr(c, b0 + 1 + (R - 1) * 3);
+        pj.lh[c] = band_ptr(c, b0 + 2 + (R - 1) * 3);
+        pj.hh[c] = band_ptr(c, b0 + 3 + (R - 1) * 3);
+      }
+    }
+    pj.out = out.data();
+    pj.pitch = (uint64_t)W * bpp;
+    pj.w = W;
+    pj.h = H;
+    pj.cw = W;
+    pj.ch = H;
+    pj.lifting = R > 0;
+    pj.ncomp = nc;
+    pj.mct = T.mct && nc >= 3;
+    pj.bit_depth = T.bit_depth;
+    pj.fmt = fmt;
+    pj.strips = (W + kIdwtStripW - 1) / kIdwtStripW;
+    pj.seg = idwt_segment_rows(H) * (irr ? 2 : 1);
+    pj.ll_band = R <= 1;
+    const uint32_t units = pj.strips * ((H + pj.seg - 1) / pj.seg);
+    const int pw = emu_pack_warps(irr);
+    launch((units + pw - 1) / pw, pw * 32, [&] { emu_pack(irr, fmt, &pj, 1, units); });
+    if (out.back() != 0xCD) printf("guard byte overwritten\n");
+    std::vector<uint8_t> want((size_t)W * H * bpp + 16);
+    uint32_t ow, oh;
+    int rc = oracle_decode(d.data(), d.size(), fmt, 0, 0, 0, 0, 0, 1, want.data(), want.size(), &ow, &oh);
+    if (rc) { printf("oracle error %d\n", rc); return 2; }
+    size_t nd = 0, first = SIZE_MAX;
+    for (size_t i = 0; i < (size_t)W * H * bpp; ++i)
+      if (out[i] != want[i]) { ++nd; if (first == SIZE_MAX) first = i; }
+    printf("%ux%u nc %u bd %u L %u %s fmt %d blocks %u refine %u status %u: coef diffs %zu, pixel diffs %zu", W, H, nc,
+           T.bit_depth, L, irr ? "9/7" : "5/3", fmt, n, nr, status[0], cdiff, nd);
+    if (nd) printf(" (first at %zu: got %u want %u)", first, out[first], want[first]);
+    printf("\n");
+    nd_total += nd;
+  }
+  return (nd_total || cdiff) ? 1 : 0;
+}
+
+int main(int argc, char** argv) {
+  sgn::emu_tables();
+  std::vector<int> fmts;
+  for (const char* c = argv[1]; *c; ++c)
+    if (*c >= '0' && *c <= '4') fmts.push_back(*c - '0');
+  int fails = 0;
+  for (int i = 2; i < argc; ++i) {
+    std::ifstream f(argv[i], std::ios::binary);
+    std::vector<uint8_t> d((std::istreambuf_iterator<char>(f)), {});
+    fails += run(d, fmts) != 0;
+  }
+  printf("fails %d\n", fails);
+  return fails != 0;
+}

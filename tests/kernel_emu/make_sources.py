@@ -1,0 +1,79 @@
+"""Writes host-compilable copies of the decode kernels for the CPU emulation
+test: the include paths point back at the package, the launchers (which
+use the <<<>>> syntax) are dropped, dynamic shared memory becomes a static
+buffer, and small wrappers expose each kernel to the driver."""
+import pathlib
+import re
+import sys
+
+CSRC = pathlib.Path(__file__).resolve().parents[2] / "signinum_b200" / "csrc"
+
+HT_WRAPPERS = """
+namespace sgn {
+void emu_tables() { build_decode_tables(g_ht_tables); }
+void emu_vlc(const HtJob* jobs, uint32_t n, const uint8_t* arena, uint32_t* sym) { ht_vlc_kernel(jobs, n, arena, sym); }
+void emu_magsgn(const HtJob* jobs, uint32_t n, const uint8_t* arena, const uint32_t* sym, int32_t* coef,
+                uint32_t* status, uint32_t ms_words, uint32_t max_w) {
+  ht_magsgn_kernel<false>(jobs, n, arena, sym, coef, status, ms_words, max_w, nullptr, 0);
+}
+void emu_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,
+                uint32_t* status) {
+  ht_refine_kernel(jobs, list, n, arena, coef, status);
+}
+}  // namespace sgn
+"""
+
+IP_WRAPPERS = """
+namespace sgn {
+void emu_idwt(bool irr, const IdwtJob* jobs, uint32_t n, uint32_t units) {
+  if (irr) idwt97_level_kernel<false>(jobs, n, units, nullptr);
+  else idwt_level_kernel<false>(jobs, n, units, nullptr);
+}
+void emu_pack(bool irr, int fmt, const PackJob* jobs, uint32_t n, uint32_t units) {
+#define K(F) case F: if (irr) pack97_kernel<F, false>(jobs, n, units, nullptr); else pack_kernel<F, false>(jobs, n, units, nullptr); break;
+  switch (fmt) { K(PACK_GRAY8) K(PACK_RGB8) K(PACK_RGBA8) K(PACK_GRAY16) K(PACK_RGB16) }
+#undef K
+}
+int emu_pack_warps(bool irr) { return irr ? kWarps97 : kIdwtWarps; }
+}  // namespace sgn
+"""
+
+
+def strip_functions(src, names):
+    out, i = [], 0
+    pat = re.compile(r"^(cudaError_t|size_t) (%s)\(" % names, re.M)
+    while True:
+        m = pat.search(src, i)
+        if not m:
+            out.append(src[i:])
+            return "".join(out)
+        out.append(src[i:m.start()])
+        j, depth = src.index("{", m.start()), 0
+        while True:
+            depth += {"{": 1, "}": -1}.get(src[j], 0)
+            if depth == 0 and src[j] == "}":
+                break
+            j += 1
+        i = j + 1
+
+
+def main(out_dir):
+    out = pathlib.Path(out_dir)
+    inc = lambda name: '#include "%s"' % (CSRC / name)
+    src = (CSRC / "kernels" / "ht_decode.cu").read_text()
+    src = src.replace('#include "../device_plan.h"', inc("device_plan.h"))
+    src = src.replace('#include "../ht_tables.h"', inc("ht_tables.h"))
+    src = src.replace('#include "kernels.h"', '#include "cuda_shim.h"\nnamespace sgn { size_t '
+                      'ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps = 8); }')
+    src = src.replace("extern __shared__ __align__(16) uint8_t smem[];", "uint8_t* smem = g_dyn_smem;")
+    src = strip_functions(src, r"launch_\w+|ht_kernels_init|ht_magsgn_occupancy|upload_ht_tables")
+    (out / "ht_decode_emu.cpp").write_text(src + HT_WRAPPERS)
+    src = (CSRC / "kernels" / "idwt_pack.cu").read_text()
+    src = src.replace('#include "../device_plan.h"', inc("device_plan.h")).replace('#include "kernels.h"',
+                                                                                   '#include "cuda_shim.h"')
+    src = strip_functions(src, r"launch_\w+|idwt_pack_occupancy")
+    (out / "idwt_pack_emu.cpp").write_text(src + IP_WRAPPERS)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

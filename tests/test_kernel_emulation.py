@@ -1,0 +1,64 @@
+"""The decode kernels' CUDA source run on CPU threads (tests/kernel_emu):
+every HT, IDWT and pack kernel on the golden fixtures and on seeded random
+reversible and irreversible codestreams, built with AddressSanitizer, and
+compared with the oracle (coefficients per code block, then pixels, exact).
+Out-of-bounds accesses and parity breaks show up here without a GPU."""
+import json
+import pathlib
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from tests.helpers import random_codestream, random_irreversible
+
+EMU = pathlib.Path(__file__).parent / "kernel_emu"
+ROOT = EMU.parents[1]
+CSRC = ROOT / "signinum_b200" / "csrc"
+
+pytestmark = pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    out = tmp_path_factory.mktemp("kernel_emu")
+    subprocess.run([sys.executable, str(EMU / "make_sources.py"), str(out)], check=True)
+    flags = ["g++", "-std=c++20", "-O1", "-fsanitize=address", "-ffp-contract=off", f"-I{EMU}", f"-I{CSRC}",
+             f"-I{ROOT / 'oracle'}"]
+    units = [out / "ht_decode_emu.cpp", out / "idwt_pack_emu.cpp", EMU / "emu_main.cpp", CSRC / "host" / "codestream.cpp",
+             ROOT / "oracle" / "oracle.cpp", ROOT / "oracle" / "oracle_ht.cpp", ROOT / "oracle" / "oracle_capi.cpp"]
+    procs = [subprocess.Popen(flags + ["-c", str(u), "-o", str(out / (u.stem + ".o"))]) for u in units]
+    assert all(p.wait() == 0 for p in procs)
+    subprocess.run(flags + ["-o", str(out / "emu")] + [str(out / (u.stem + ".o")) for u in units] + ["-lpthread"],
+                   check=True)
+    return out
+
+
+def run(emu, fmts, codestreams):
+    paths = []
+    for k, cs in enumerate(codestreams):
+        p = emu / f"case_{fmts}_{k}.j2k"
+        p.write_bytes(cs)
+        paths.append(str(p))
+    r = subprocess.run([str(emu / "emu"), fmts] + paths, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    assert r.stdout.strip().endswith("fails 0")
+
+
+def test_golden_fixtures_through_emulated_kernels(emu):
+    fx = json.loads((pathlib.Path(__file__).parent / "golden" / "openhtj2k.json").read_text())["fixtures"]
+    run(emu, "03", [bytes.fromhex(f["j2k_hex"]) for f in fx.values()])
+
+
+@pytest.mark.parametrize("kind", ["reversible", "irreversible"])
+def test_random_codestreams_through_emulated_kernels(emu, kind):
+    rng = np.random.default_rng(31 if kind == "reversible" else 97)
+    make = random_codestream if kind == "reversible" else random_irreversible
+    by_comps = {1: [], 3: []}
+    while len(by_comps[1]) < 4 or len(by_comps[3]) < 4:
+        cs, _, _, _, comps, _ = make(rng, max_side=100)
+        by_comps[comps].append(cs)
+    run(emu, "03", by_comps[1])  # Gray8, Gray16
+    run(emu, "124", by_comps[3])  # Rgb8, Rgba8, Rgb16
