@@ -1,10 +1,11 @@
 """Benchmark: decoded Mpixel/s of the HTJ2K tile-batch decode path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c3] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c1i|c2|c3|c4] [--impl ours|reference]
 
 A step is one decode of the whole workload batch.  Default workload: 256
 tiles of 512x512 RGB8 (H&E-like, 5 levels, 64x64 code blocks, RCT), seeded
-synthetic data.  Prints one JSON line (rank 0):
+synthetic data; c1i is the same batch coded lossy (9/7, ICT, quantised).
+Prints one JSON line (rank 0):
 
   value        batched decode, codestreams resident in HBM (one plan: HT
                cleanup over all code blocks ordered by coded length, IDWT
@@ -42,7 +43,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c1i", "c2", "c3", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -63,6 +64,8 @@ def build_workload(name):
 
     if name == "c1":
         return encode.config1(), "rgb8"
+    if name == "c1i":
+        return encode.config1_irreversible(), "rgb8"
     if name == "c2":
         return encode.config2(), "rgb8"
     return encode.config3(), "gray16"
@@ -71,6 +74,8 @@ def build_workload(name):
 WORKLOAD_CONFIG = {
     "c1": {"workload": "uniform batch: 256 tiles 512x512 RGB8, HTJ2K lossless 5/3, 5 levels, 64x64 code blocks, RCT",
            "tiles": 256},
+    "c1i": {"workload": "uniform batch, lossy: 256 tiles 512x512 RGB8, HTJ2K irreversible 9/7 + ICT, scalar "
+                    "expounded quantisation (relative step 1/256), 5 levels, 64x64 code blocks", "tiles": 256},
     "c2": {"workload": "uneven batch: 1024 RGB8 tiles, sides 128..1024, 3..6 levels, 32x32/64x64 blocks, 20% near-blank",
            "tiles": 1024},
     "c3": {"workload": "high bit depth: 128 tiles 2048x2048 u16 gray, 6 levels, 64x64 code blocks",
@@ -649,6 +654,8 @@ def main():
 
     if rank == 0:
         names = ["ht_vlc_kernel", "ht_magsgn_kernel", "ht_refine_kernel", "idwt_level_kernel", "pack_kernel"]
+        if args.workload == "c1i":
+            names[3:] = ["idwt97_level_kernel", "pack97_kernel"]
         dom = int(np.argmax(stage[:5]))
         peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
         peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
@@ -660,7 +667,7 @@ def main():
             "metric": "decoded Mpixel/s (batched persistent form; plain per-tile beside it)",
             "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int32", "data": "synthetic (seeded)",
+            "dtype": "int32 (HT), f32 (9/7, ICT)" if args.workload == "c1i" else "int32", "data": "synthetic (seeded)",
             "config": dict(WORKLOAD_CONFIG[args.workload], parallelism=f"replicas{world}",
                            l2="inputs larger than L2 (coded + coefficient arenas), no flush",
                            coded_bytes=coded, output_bytes=out_bytes, pixels=pixels),

@@ -17,6 +17,9 @@ namespace sgn {
 // Work unit of the IDWT kernels: one warp decodes a strip of kIdwtStripW
 // columns (four per lane) over `seg` rows of one level (even, chosen per job).
 constexpr int kIdwtStripW = 128;
+// The 9/7 kernels' strips: 120 output columns (lanes 1..30; lanes 0 and 31
+// carry the four columns on either side).
+constexpr int kStrip97 = 120;
 
 // Rows per work unit: long segments for big levels (less halo re-reading),
 // short ones for small levels (more warps in flight).

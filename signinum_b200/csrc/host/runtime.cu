@@ -325,7 +325,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
         j.out = lvl(c, r);
         j.w = res_dim(r, true);
         j.h = res_dim(r, false);
-        j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
+        const uint32_t sw = L.reversible ? kIdwtStripW : kStrip97;
+        j.strips = (j.w + sw - 1) / sw;
         j.unit_begin = 0;
         j.seg = idwt_segment_rows(j.h);
         j.ll_band = r == 1 ? 1 : 0;
@@ -379,8 +380,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     pj.bit_depth = L.bit_depth;
     pj.fmt = fmt;
     pj.region_conv = tw.region_conv;
-    uint32_t ax = tw.crop_x & ~(uint32_t)(kIdwtStripW - 1), ay = tw.crop_y & ~1u;
-    pj.strips = (tw.crop_x + tw.crop_w - ax + kIdwtStripW - 1) / kIdwtStripW;
+    const uint32_t sw = L.reversible ? kIdwtStripW : kStrip97;
+    uint32_t ax = tw.crop_x - tw.crop_x % sw, ay = tw.crop_y & ~1u;
+    pj.strips = (tw.crop_x + tw.crop_w - ax + sw - 1) / sw;
     pj.seg = idwt_segment_rows(tw.crop_h) * (L.reversible ? 1 : 2);
     pj.ll_band = R <= 1 ? 1 : 0;
     uint32_t segs = (tw.crop_y + tw.crop_h - ay + pj.seg - 1) / pj.seg;

@@ -552,38 +552,48 @@ __global__ void __launch_bounds__(kIdwtWarps * 32, 4) pack_kernel(const PackJob*
 // pack (crates/signinum-j2k-native/src/j2c/idwt.rs:767-836, :1016-1140;
 // mct.rs:80-115; decode.rs:1130-1151 for the dequantisation).
 //
-// Same mapping as the 5/3 kernels (a warp per 128-column strip of `seg`
-// rows, four columns per lane), in f32.  Every sample goes through the
-// reference's own sequence of roundings: band coefficient x step, then per
-// level the horizontal pass (even columns x K, odd x 1/K, then the four
-// lifting steps delta, gamma, beta, alpha as fma(left + right, c, x)), then
-// the same vertical pass.  Only __fmul_rn / __fadd_rn / fmaf are used, so no
-// multiply is contracted into a neighbouring add and results match the
-// reference's f32 arithmetic bit for bit.  Symmetric extension is done by
-// reflecting indices, which commutes with the lifting steps (reflected
-// positions compute the same sums in the other order, and f32 addition is
-// commutative).
+// Every sample goes through the reference's own sequence of f32 roundings:
+// band coefficient x step, then per level the horizontal pass (even columns
+// x K, odd x 1/K, then the four lifting steps delta, gamma, beta, alpha as
+// fma(left + right, c, x)), then the same vertical pass.  Only __fmul_rn /
+// __fadd_rn / fmaf are used, so no multiply is contracted into a
+// neighbouring add and the results match the reference's f32 arithmetic bit
+// for bit.  Symmetric extension is done by reflecting indices, which
+// commutes with the lifting steps (reflected positions compute the same sums
+// in the other order, and f32 addition is commutative).
 //
-// Horizontal: lane k holds columns c .. c+3 (c = 2b); each step needs one
-// neighbour from the adjacent lane (shuffles); the strip's edge lanes
-// compute the values outside the strip from halo samples (three on the
-// left, four on the right).  Vertical: a four-stage pipeline down the rows,
-// loading rows 2m+2 and 2m+3 per step and finishing rows 2m (after beta)
-// and 2m-1 (after alpha); a unit starting at row ys primes from row ys-3.
+// Mapping: a warp per strip of kStrip97 = 120 output columns x `seg` rows.
+// Lane k holds the four columns x0 - 4 + 4k .. x0 - 1 + 4k, so lanes 0 and
+// 31 hold the four columns on either side of the strip: a sample after the
+// four lifting steps depends on the samples within four columns of it, so
+// lanes 1..30 finish exact values while every lane runs the same code (each
+// step takes one neighbour from the adjacent lane by a shuffle; the edge
+// lanes' own results are not used).  Vertically a four-stage pipeline runs
+// down the rows, loading rows 2m+2 and 2m+3 per step and finishing rows 2m
+// (after beta) and 2m-1 (after alpha); a unit starting at row ys primes from
+// row ys-3.  The next rows' raw samples are loaded one step (or, for three
+// components, one component) ahead.
 
 constexpr float kNegAlpha97 = 1.5861343f, kNegBeta97 = 0.052980117f, kNegGamma97 = -0.8829111f,
                 kNegDelta97 = -0.44350687f, kKappa97 = 1.2301741f;
 constexpr int kWarps97 = 4;  // warps per CTA of the 9/7 pack kernel (its shared state is larger)
+static_assert(kStrip97 == 4 * (kLanes - 2), "lanes 1..30 hold a strip's output columns");
 
 namespace {
 
-// Whole-sample symmetric extension of any index into [0, n).
+// Whole-sample symmetric extension into [0, n) of an index at most four
+// samples outside it (every sample an exact output depends on).  Indices
+// further out (columns of lanes whose results are unused) end at the nearest
+// in-range index of the same parity, so the band they select (low for even,
+// high for odd) and the row inside it stay in bounds.
 __device__ __forceinline__ int fold97(int i, int n) {
   if ((unsigned)i < (unsigned)n) return i;
   if (n == 1) return 0;
-  const int p = 2 * (n - 1);
-  i = abs(i) % p;
-  return i < n ? i : p - i;
+#pragma unroll 1
+  for (int k = 0; k < 4 && (unsigned)i >= (unsigned)n; ++k) i = i < 0 ? -i : 2 * (n - 1) - i;
+  if (i < 0) return i & 1;
+  if (i >= n) return (n - 1) - (((n - 1) ^ i) & 1);
+  return i;
 }
 
 struct Src97 {
@@ -594,105 +604,74 @@ struct Src97 {
   float q[4];    // dequantisation steps of ll, hl, lh, hh
   int w, h;
   bool ll_band;  // ll is the LL band; otherwise the previous level's f32 image
-  bool vec;
+  bool fast;     // the strip's 128 columns lie inside the level and rows are 8-byte aligned
 };
 
 __device__ __forceinline__ Src97 make_src97(const int32_t* ll, const int32_t* hl, const int32_t* lh,
-                                            const int32_t* hh, const float* q, bool ll_band, int w, int h) {
+                                            const int32_t* hh, const float* q, bool ll_band, int w, int h, int c0) {
   const uintptr_t a = (uintptr_t)ll | (uintptr_t)hl | (uintptr_t)lh | (uintptr_t)hh;
-  return Src97{ll, hl, lh, hh, {q[0], q[1], q[2], q[3]}, w, h, ll_band, (w & 3) == 0 && (a & 7) == 0};
+  const bool fast = (w & 3) == 0 && (a & 7) == 0 && c0 >= 0 && c0 + 4 * kLanes <= w;
+  return Src97{ll, hl, lh, hh, {q[0], q[1], q[2], q[3]}, w, h, ll_band, fast};
 }
 
-// Image columns c .. c+3 of one interleaved row (dequantised), and the edge
-// lanes' halo: lane 0 columns c-3, c-2, c-1; lane 31 columns c+4 .. c+7.
+// The raw words of a lane's four columns of one interleaved row (low band at
+// the even columns, high band at the odd ones), loaded ahead of their use.
 struct Raw97 {
-  float e0, o0, e1, o1;
-  float h0, h1, h2, h3;
+  int32_t e0, o0, e1, o1;
 };
 
-__device__ __forceinline__ Raw97 load97(const Src97& S, int y, int b, int lane) {
-  const int w = S.w;
+__device__ __forceinline__ void row_bands(const Src97& S, int y, const int32_t*& lo, const int32_t*& hi) {
   y = fold97(y, S.h);
   const int r = y >> 1;
-  const bool odd = y & 1;
-  const int lw = (w + 1) >> 1, hw = w >> 1;
-  const int32_t* Lr = (odd ? S.lh : S.ll) + (size_t)r * lw;
-  const int32_t* Hr = (odd ? S.hh : S.hl) + (size_t)r * hw;
-  const float ql = odd ? S.q[2] : S.q[0], qh = odd ? S.q[3] : S.q[1];
-  const bool lraw = !odd && !S.ll_band;
-  auto lo_of = [&](int32_t v) { return lraw ? __int_as_float(v) : __fmul_rn(__int2float_rn(v), ql); };
-  auto hi_of = [&](int32_t v) { return __fmul_rn(__int2float_rn(v), qh); };
-  auto at = [&](int j) {
-    j = fold97(j, w);
-    return (j & 1) ? hi_of(__ldg(Hr + (j >> 1))) : lo_of(__ldg(Lr + (j >> 1)));
-  };
-  const int c = 2 * b;
-  Raw97 R;
-  if (S.vec && c + 3 < w) {
-    const int2 l = __ldg(reinterpret_cast<const int2*>(Lr + b));
-    const int2 h = __ldg(reinterpret_cast<const int2*>(Hr + b));
-    R.e0 = lo_of(l.x);
-    R.o0 = hi_of(h.x);
-    R.e1 = lo_of(l.y);
-    R.o1 = hi_of(h.y);
-  } else {
-    R.e0 = at(c);
-    R.o0 = at(c + 1);
-    R.e1 = at(c + 2);
-    R.o1 = at(c + 3);
+  lo = ((y & 1) ? S.lh : S.ll) + (size_t)r * ((S.w + 1) >> 1);
+  hi = ((y & 1) ? S.hh : S.hl) + (size_t)r * (S.w >> 1);
+}
+
+// c: the lane's first column (even).
+__device__ __forceinline__ Raw97 load97(const Src97& S, int y, int c) {
+  const int32_t *lo, *hi;
+  row_bands(S, y, lo, hi);
+  if (S.fast) {
+    const int2 l = __ldg(reinterpret_cast<const int2*>(lo + (c >> 1)));
+    const int2 h = __ldg(reinterpret_cast<const int2*>(hi + (c >> 1)));
+    return Raw97{l.x, h.x, l.y, h.y};
   }
-  R.h0 = R.h1 = R.h2 = R.h3 = 0.0f;
-  if (lane == 0) {
-    R.h0 = at(c - 3);
-    R.h1 = at(c - 2);
-    R.h2 = at(c - 1);
-  } else if (lane == kLanes - 1) {
-    R.h0 = at(c + 4);
-    R.h1 = at(c + 5);
-    R.h2 = at(c + 6);
-    R.h3 = at(c + 7);
-  }
-  return R;
+  // Reflection keeps a column's parity, so even columns stay in the low band.
+  const int w = S.w;
+  return Raw97{__ldg(lo + (fold97(c, w) >> 1)), __ldg(hi + (fold97(c + 1, w) >> 1)), __ldg(lo + (fold97(c + 2, w) >> 1)),
+               __ldg(hi + (fold97(c + 3, w) >> 1))};
 }
 
 __device__ __forceinline__ float lstep(float l, float r, float c, float x) { return fmaf(__fadd_rn(l, r), c, x); }
 
-// Horizontal 9/7 synthesis of a loaded row: columns c .. c+3.
-__device__ __forceinline__ float4 lift97(const Raw97& R, int w, int lane, float K, float IK) {
-  if (w == 1) return make_float4(R.e0, 0.0f, 0.0f, 0.0f);
-  const float e0 = __fmul_rn(R.e0, K), o0 = __fmul_rn(R.o0, IK), e1 = __fmul_rn(R.e1, K), o1 = __fmul_rn(R.o1, IK);
-  // Halo, scaled by the parity of its columns.
-  const bool left = lane == 0;
-  const float h0 = __fmul_rn(R.h0, left ? IK : K), h1 = __fmul_rn(R.h1, left ? K : IK);
-  const float h2 = __fmul_rn(R.h2, left ? IK : K), h3 = __fmul_rn(R.h3, IK);
-  // delta: even columns.
-  float om1 = __shfl_up_sync(0xFFFFFFFFu, o1, 1);  // X[c-1]
-  if (left) om1 = h2;
-  const float e0a = lstep(om1, o0, kNegDelta97, e0);
-  const float e1a = lstep(o0, o1, kNegDelta97, e1);
-  // gamma: odd columns.
-  float ep4a = __shfl_down_sync(0xFFFFFFFFu, e0a, 1);  // E[c+4]
-  if (lane == kLanes - 1) ep4a = lstep(o1, h1, kNegDelta97, h0);
-  const float o0b = lstep(e0a, e1a, kNegGamma97, o0);
-  const float o1b = lstep(e1a, ep4a, kNegGamma97, o1);
-  // beta: even columns.
-  float om1b = __shfl_up_sync(0xFFFFFFFFu, o1b, 1);  // O[c-1]
-  if (left) {
-    const float em2a = lstep(h0, h2, kNegDelta97, h1);  // E[c-2] after delta
-    om1b = lstep(em2a, e0a, kNegGamma97, h2);
+// Dequantises (or reinterprets) a loaded row and runs the horizontal 9/7
+// synthesis: the lane's four columns (exact on lanes 1..30).
+__device__ __forceinline__ float4 lift97(const Src97& S, int y, const Raw97& R, float K, float IK) {
+  const bool odd = fold97(y, S.h) & 1;
+  const float ql = odd ? S.q[2] : S.q[0], qh = odd ? S.q[3] : S.q[1];
+  float e0, e1;
+  if (!odd && !S.ll_band) {
+    e0 = __int_as_float(R.e0);
+    e1 = __int_as_float(R.e1);
+  } else {
+    e0 = __fmul_rn(__int2float_rn(R.e0), ql);
+    e1 = __fmul_rn(__int2float_rn(R.e1), ql);
   }
-  const float e0c = lstep(om1b, o0b, kNegBeta97, e0a);
-  const float e1c = lstep(o0b, o1b, kNegBeta97, e1a);
-  // alpha: odd columns.
-  float ep4c = __shfl_down_sync(0xFFFFFFFFu, e0c, 1);  // E[c+4]
-  if (lane == kLanes - 1) {
-    const float ep6a = lstep(h1, h3, kNegDelta97, h2);   // E[c+6] after delta
-    const float op5b = lstep(ep4a, ep6a, kNegGamma97, h1);  // O[c+5] after gamma
-    ep4c = lstep(o1b, op5b, kNegBeta97, ep4a);
-  }
-  const float o0d = lstep(e0c, e1c, kNegAlpha97, o0b);
-  const float o1d = lstep(e1c, ep4c, kNegAlpha97, o1b);
-  return make_float4(e0c, o0d, e1c, o1d);
+  float o0 = __fmul_rn(__int2float_rn(R.o0), qh), o1 = __fmul_rn(__int2float_rn(R.o1), qh);
+  if (S.w == 1) return make_float4(e0, 0.0f, 0.0f, 0.0f);
+  e0 = __fmul_rn(e0, K);
+  e1 = __fmul_rn(e1, K);
+  o0 = __fmul_rn(o0, IK);
+  o1 = __fmul_rn(o1, IK);
+  // delta: even columns; gamma: odd; beta: even; alpha: odd.
+  const float om1 = __shfl_up_sync(0xFFFFFFFFu, o1, 1);
+  const float e0a = lstep(om1, o0, kNegDelta97, e0), e1a = lstep(o0, o1, kNegDelta97, e1);
+  const float ep4a = __shfl_down_sync(0xFFFFFFFFu, e0a, 1);
+  const float o0b = lstep(e0a, e1a, kNegGamma97, o0), o1b = lstep(e1a, ep4a, kNegGamma97, o1);
+  const float om1b = __shfl_up_sync(0xFFFFFFFFu, o1b, 1);
+  const float e0c = lstep(om1b, o0b, kNegBeta97, e0a), e1c = lstep(o0b, o1b, kNegBeta97, e1a);
+  const float ep4c = __shfl_down_sync(0xFFFFFFFFu, e0c, 1);
+  return make_float4(e0c, lstep(e0c, e1c, kNegAlpha97, o0b), e1c, lstep(e1c, ep4c, kNegAlpha97, o1b));
 }
 
 __device__ __forceinline__ float4 scale4(float4 v, float k) {
@@ -704,45 +683,81 @@ __device__ __forceinline__ float4 lstep4(float4 a, float4 b, float c, float4 x) 
 }
 
 // Vertical 9/7 stream over rows [ys, ye) (ys even) of NC level images.
-// row(c, y) returns the horizontally lifted row y of component c (any y,
-// reflected inside); st(c, k) is the component's lifting state k (0 the
-// last odd input row, 1..3 the last rows after delta, gamma, beta);
-// emit(y, v[NC]) receives each finished row.
-template <int NC, typename Row, typename State, typename Emit>
-__device__ __forceinline__ void stream97(Row row, int h, int ys, int ye, float K, float IK, State st, Emit emit) {
-  float4 od[NC], ev[NC];
+// col is the lane's first column; src(c) gives component c's bands;
+// st(c, k) is its lifting state (k 0: the
+// last odd input row, 1..3: the last rows after delta, gamma, beta; 4, 5:
+// the finished odd and even rows of the step); emit(y, v[NC]) receives each
+// finished row.  Components are lifted one at a time while the next
+// component's (or the next step's) rows load.
+template <int NC, typename SrcOf, typename State, typename Emit>
+__device__ __forceinline__ void stream97(SrcOf src, int h, int col, int ys, int ye, float K, float IK, State st,
+                                         Emit emit) {
+  float4 v[NC];
   if (h == 1) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c) ev[c] = row(c, 0);
-    emit(0, ev);
+    for (int c = 0; c < NC; ++c) {
+      const Src97& S = src(c);
+      v[c] = lift97(S, 0, load97(S, 0, col), K, IK);
+    }
+    emit(0, v);
     return;
   }
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-#pragma unroll
+#pragma unroll 1
   for (int c = 0; c < NC; ++c) {
-    st(c, 0) = scale4(row(c, ys - 3), IK);
+    const Src97& S = src(c);
+    st(c, 0) = scale4(lift97(S, ys - 3, load97(S, ys - 3, col), K, IK), IK);
     st(c, 1) = zero;
     st(c, 2) = zero;
     st(c, 3) = zero;
   }
-  for (int m = (ys >> 1) - 2; m <= (ye >> 1); ++m) {
-#pragma unroll
+  const int m0 = (ys >> 1) - 2, m1 = ye >> 1;
+  Raw97 re, ro;
+  {
+    const Src97& S = src(0);
+    re = load97(S, 2 * m0 + 2, col);
+    ro = load97(S, 2 * m0 + 3, col);
+  }
+  for (int m = m0; m <= m1; ++m) {
+#pragma unroll 1
     for (int c = 0; c < NC; ++c) {
-      const float4 xe = scale4(row(c, 2 * m + 2), K), xo = scale4(row(c, 2 * m + 3), IK);
+      // Loads of the next component's rows, or of the next step's first one.
+      Raw97 ne = re, no = ro;
+      if (c + 1 < NC) {
+        const Src97& N = src(c + 1);
+        ne = load97(N, 2 * m + 2, col);
+        no = load97(N, 2 * m + 3, col);
+      } else if (m < m1) {
+        const Src97& N = src(0);
+        ne = load97(N, 2 * m + 4, col);
+        no = load97(N, 2 * m + 5, col);
+      }
+      const Src97& S = src(c);
+      const float4 xe = scale4(lift97(S, 2 * m + 2, re, K, IK), K);
+      const float4 xo = scale4(lift97(S, 2 * m + 3, ro, K, IK), IK);
+      re = ne;
+      ro = no;
       const float4 xp = st(c, 0), s1p = st(c, 1), s2p = st(c, 2), s3p = st(c, 3);
-      const float4 s1 = lstep4(xp, xo, kNegDelta97, xe);    // row 2m+2
-      const float4 s2 = lstep4(s1p, s1, kNegGamma97, xp);   // row 2m+1
-      const float4 s3 = lstep4(s2p, s2, kNegBeta97, s1p);   // row 2m, final
-      od[c] = lstep4(s3p, s3, kNegAlpha97, s2p);            // row 2m-1, final
-      ev[c] = s3;
+      const float4 s1 = lstep4(xp, xo, kNegDelta97, xe);   // row 2m+2
+      const float4 s2 = lstep4(s1p, s1, kNegGamma97, xp);  // row 2m+1
+      const float4 s3 = lstep4(s2p, s2, kNegBeta97, s1p);  // row 2m, final
+      st(c, 4) = lstep4(s3p, s3, kNegAlpha97, s2p);        // row 2m-1, final
       st(c, 0) = xo;
       st(c, 1) = s1;
       st(c, 2) = s2;
       st(c, 3) = s3;
     }
     const int yo = 2 * m - 1, yv = 2 * m;
-    if (yo >= ys && yo < ye) emit(yo, od);
-    if (yv >= ys && yv < ye) emit(yv, ev);
+    if (yo >= ys && yo < ye) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = st(c, 4);
+      emit(yo, v);
+    }
+    if (yv >= ys && yv < ye) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[c] = st(c, 3);
+      emit(yv, v);
+    }
   }
 }
 
@@ -750,18 +765,21 @@ __device__ __forceinline__ void idwt97_unit(const IdwtJob* __restrict__ jobs, ui
   const int lane = threadIdx.x & 31;
   const IdwtJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
-  const int x0 = (int)(local % job.strips) * kIdwtStripW;
+  const int x0 = (int)(local % job.strips) * kStrip97;
   const int ys = (int)(local / job.strips) * (int)job.seg;
   const int w = (int)job.w, h = (int)job.h;
   const int ye = min(ys + (int)job.seg, h);
-  const Src97 S = make_src97(job.ll, job.hl, job.lh, job.hh, job.step, job.ll_band != 0, w, h);
-  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
+  const int col = x0 - 4 + 4 * lane;
+  const Src97 S = make_src97(job.ll, job.hl, job.lh, job.hh, job.step, job.ll_band != 0, w, h, x0 - 4);
   float* out = reinterpret_cast<float*>(job.out);
+  const bool mine = lane >= 1 && lane <= kLanes - 2;
   const bool vec_out = (w & 3) == 0 && (((uintptr_t)out) & 15) == 0;
-  float4 state[4];
-  stream97<1>([&](int, int y) { return lift97(load97(S, y, b, lane), w, lane, kKappa97, IK); }, h, ys, ye,
-              kKappa97, IK, [&](int, int k) -> float4& { return state[k]; },
+  float4 state[6];
+  const Src97* sp = &S;
+  stream97<1>([sp](int) -> const Src97& { return *sp; }, h, col, ys, ye, kKappa97, IK,
+              [&](int, int k) -> float4& { return state[k]; },
               [&](int y, const float4* v) {
+                if (!mine) return;
                 float* rowp = out + (size_t)y * w;
                 if (vec_out && col + 3 < w) {
                   *reinterpret_cast<float4*>(rowp + col) = v[0];
@@ -858,20 +876,20 @@ __device__ __forceinline__ void put_pixel97(uint32_t* wds, int p, float c0, floa
   }
 }
 
-// Slots of a lane's 9/7 lifting state in shared memory: 4 per component.
-constexpr int kSlots97 = 4 * 3;
+// Shared-memory slots of a lane's three-component 9/7 stream: 6 per component.
+constexpr int kSlots97 = 6 * 3;
 
 template <int NC, int FMT>
 __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
-                                            float4* st, float IK) {
+                                            float4* st, Src97* tab, float IK) {
   constexpr int BPP = pack_bpp<FMT>();
   const int w = (int)job.w, h = (int)job.h;
   const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
   const uint32_t bd = job.bit_depth, reg = job.region_conv;
   const float shift = (float)(1u << (bd - 1));
   const bool ict = NC == 3 && job.mct;
-  const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
-  const int xs = max(x0, cx0), xe = min(x0 + kIdwtStripW, cx1);
+  const int col = x0 - 4 + 4 * lane;
+  const int xs = max(x0, cx0), xe = min(x0 + kStrip97, cx1);
   const int nbytes = (xe - xs) * BPP;
   auto emit = [&](int y, const float4* v) {
     if (y < cy0 || y >= cy1) return;  // warp-uniform
@@ -899,19 +917,26 @@ __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, 
       c0 = __fadd_rn(c0, shift);
       put_pixel97<FMT>(wds, p, c0, c1, c2, bd, reg);
     }
-    store_row<BPP>(job, y, x0, xs, nbytes, lane, rowbuf, wds);
-  };
-  auto src = [&](int c) {
-    return make_src97(job.ll[c], job.hl[c], job.lh[c], job.hh[c], job.step[c], job.ll_band != 0, w, h);
+    // Lane k's words are columns x0 - 4 + 4k ..: the row starts at x0 - 4.
+    store_row<BPP>(job, y, x0 - 4, xs, nbytes, lane, rowbuf, wds);
   };
   if (job.lifting) {
-    auto row = [&](int c, int y) { return lift97(load97(src(c), y, b, lane), w, lane, kKappa97, IK); };
     if (NC == 3) {
-      stream97<3>(row, h, ys, ye, kKappa97, IK, [&](int c, int k) -> float4& { return st[(c * 4 + k) * kLanes + lane]; },
-                  emit);
+      // The components' band descriptors, read from the job once per unit.
+      if (lane < 3)
+        tab[lane] = make_src97(job.ll[lane], job.hl[lane], job.lh[lane], job.hh[lane], job.step[lane],
+                               job.ll_band != 0, w, h, x0 - 4);
+      __syncwarp();
+      stream97<3>([&](int c) -> const Src97& { return tab[c]; }, h, col, ys, ye, kKappa97, IK,
+                  [&](int c, int k) -> float4& { return st[(c * 6 + k) * kLanes + lane]; }, emit);
+      __syncwarp();
     } else {
-      float4 state[4];
-      stream97<1>(row, h, ys, ye, kKappa97, IK, [&](int, int k) -> float4& { return state[k]; }, emit);
+      const Src97 S = make_src97(job.ll[0], job.hl[0], job.lh[0], job.hh[0], job.step[0], job.ll_band != 0, w, h,
+                                 x0 - 4);
+      float4 state[6];
+      const Src97* sp = &S;
+      stream97<1>([sp](int) -> const Src97& { return *sp; }, h, col, ys, ye, kKappa97, IK,
+                  [&](int, int k) -> float4& { return state[k]; }, emit);
     }
   } else {
     // Nothing to lift: the image is the LL band itself (dequantised).
@@ -921,7 +946,10 @@ __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, 
       for (int c = 0; c < NC; ++c) {
         const int32_t* rowp = job.ll[c] + (size_t)y * w;
         const float q = job.step[c][0];
-        auto at = [&](int k) { return col + k < w ? __fmul_rn(__int2float_rn(__ldg(rowp + col + k)), q) : 0.0f; };
+        auto at = [&](int k) {
+          const int x = col + k;
+          return x >= 0 && x < w ? __fmul_rn(__int2float_rn(__ldg(rowp + x)), q) : 0.0f;
+        };
         v[c] = make_float4(at(0), at(1), at(2), at(3));
       }
       emit(y, v);
@@ -936,18 +964,20 @@ __global__ void __launch_bounds__(kWarps97 * 32) pack97_kernel(const PackJob* __
                                                                uint32_t nunits, uint32_t* queue) {
   __shared__ __align__(16) uint32_t rowbufs[kWarps97][kRowWords];
   __shared__ float4 states[kWarps97][kSlots97 * kLanes];
+  __shared__ Src97 tabs[kWarps97][3];
   const float IK = __fdiv_rn(1.0f, kKappa97);
   uint32_t* rowbuf = rowbufs[threadIdx.x >> 5];
   float4* st = states[threadIdx.x >> 5];
+  Src97* tab = tabs[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   auto one = [&](uint32_t unit) {
     const PackJob& job = find_job(jobs, njobs, unit);
     const uint32_t local = unit - job.unit_begin;
-    const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
+    const int x0 = (int)(job.cx - job.cx % kStrip97) + (int)(local % job.strips) * kStrip97;
     const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
     const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
-    if (job.ncomp >= 3) pack97_unit<3, FMT>(job, x0, ys, ye, lane, rowbuf, st, IK);
-    else pack97_unit<1, FMT>(job, x0, ys, ye, lane, rowbuf, st, IK);
+    if (job.ncomp >= 3) pack97_unit<3, FMT>(job, x0, ys, ye, lane, rowbuf, st, tab, IK);
+    else pack97_unit<1, FMT>(job, x0, ys, ye, lane, rowbuf, st, tab, IK);
   };
   if (!QUEUE) {
     const uint32_t unit = blockIdx.x * kWarps97 + (threadIdx.x >> 5);

@@ -116,10 +116,14 @@ def _pool():
     return ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1)))
 
 
-def _he_tile(widx: int, i: int, side: int, sigma: float, levels: int, cb_exp: int, keep: bool, blank=False) -> Tile:
+def _he_tile(widx: int, i: int, side: int, sigma: float, levels: int, cb_exp: int, keep: bool, blank=False,
+             lossy_step: float | None = None) -> Tile:
     seed = _mix(MASTER_SEED, widx, i)
     px = blank_rgb8(seed, side, side) if blank else he_rgb8(seed, side, side, sigma)
-    cs = encode_lossless(px, side, side, 3, 8, levels=levels, cb_exp=cb_exp)
+    if lossy_step is None:
+        cs = encode_lossless(px, side, side, 3, 8, levels=levels, cb_exp=cb_exp)
+    else:
+        cs = encode_irreversible(px, side, side, 3, 8, lossy_step, levels=levels, cb_exp=cb_exp)
     return Tile(cs, side, side, 3, 8, levels, 1 << (cb_exp + 2), "blank" if blank else "he", px if keep else None)
 
 
@@ -133,6 +137,14 @@ def config1(n=256, side=512, keep_pixels=False) -> Workload:
     with _pool() as ex:
         tiles = list(ex.map(lambda i: _he_tile(1, i, side, 6.0, 5, 4, keep_pixels), range(n)))
     return Workload(f"c1_rgb8_{n}x{side}x{side}", tiles)
+
+
+def config1_irreversible(n=256, side=512, step=1 / 256, keep_pixels=False) -> Workload:
+    """The uniform batch of config1 coded lossy: ICT, 9/7, 5 levels, 64x64
+    blocks, every band quantised with relative step `step`."""
+    with _pool() as ex:
+        tiles = list(ex.map(lambda i: _he_tile(5, i, side, 6.0, 5, 4, keep_pixels, lossy_step=step), range(n)))
+    return Workload(f"c1i_rgb8_{n}x{side}x{side}_97", tiles)
 
 
 def config2(n=1024, keep_pixels=False) -> Workload:

@@ -168,7 +168,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
       j.out = lvl[c * 2 + (r & 1)].data();
       j.w = res_dim(r, true);
       j.h = res_dim(r, false);
-      j.strips = (j.w + kIdwtStripW - 1) / kIdwtStripW;
+      const uint32_t sw = irr ? kStrip97 : kIdwtStripW;
+      j.strips = (j.w + sw - 1) / sw;
       j.seg = idwt_segment_rows(j.h) * (irr ? 2 : 1);
       j.ll_band = r == 1;
       j.step[0] = T.bands[b0].step;
@@ -212,7 +213,7 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     pj.mct = T.mct && nc >= 3;
     pj.bit_depth = T.bit_depth;
     pj.fmt = fmt;
-    pj.strips = (W + kIdwtStripW - 1) / kIdwtStripW;
+    pj.strips = (W + (irr ? kStrip97 : kIdwtStripW) - 1) / (irr ? kStrip97 : kIdwtStripW);
     pj.seg = idwt_segment_rows(H) * (irr ? 2 : 1);
     pj.ll_band = R <= 1;
     const uint32_t units = pj.strips * ((H + pj.seg - 1) / pj.seg);
