@@ -180,6 +180,15 @@ void* sgn_ctx_stream(sgn_ctx* ctx);
  * reference's ht_tables.rs. */
 void sgn_ht_lookup_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1);
 
+/* Diagnostics (no counterpart in the reference): the classic Tier-1 tables
+ * the kernels decode with, as the reference lays them out: zero-coding
+ * contexts for LL/LH, HL and HH bands and the sign-coding (label, xor)
+ * pairs, 256 entries each over the neighbour-significance byte, and the MQ
+ * probability table as 47 little-endian (u16 qe, u8 nmps, u8 nlps,
+ * u8 switch) records (235 bytes), so tests can pin them to the reference. */
+void sgn_ebcot_tables(uint8_t* zc_ll_lh, uint8_t* zc_hl, uint8_t* zc_hh, uint8_t* sc_label, uint8_t* sc_xor,
+                      uint8_t* qe_records);
+
 /* One HT code block for the block-level entry points below: where its
  * cleanup segment starts in a segment buffer (the refinement segment, if
  * any, follows it), where its first sample goes in an int32 coefficient

@@ -1,10 +1,10 @@
 // TEST INFRASTRUCTURE ONLY — the parity oracle (see oracle_internal.h).
 //
-// Codestream parsing, tile geometry, packet parsing, the per-sub-band HT
-// driver, the inverse 5/3 DWT, inverse RCT, DC shift and the pixel-format
-// conversions, restated from crates/signinum-j2k-native and
-// crates/signinum-j2k.  Scope: raw J2K codestreams, HT block coding,
-// reversible 5/3; classic EBCOT, 9/7, PPM/PPT and sub-sampled components are
+// Codestream parsing, tile geometry, packet parsing (HT and classic), the
+// per-sub-band block decode drivers, dequantisation, the inverse 5/3 and 9/7
+// DWTs, inverse RCT and ICT, DC shift and the pixel-format conversions,
+// restated from crates/signinum-j2k-native and crates/signinum-j2k.  Scope:
+// raw J2K codestreams and JP2 files; PPM/PPT and sub-sampled components are
 // reported as unsupported here.
 #include <algorithm>
 #include <array>
@@ -133,7 +133,6 @@ struct BitReader {
 // ---------------------------------------------------------------------------
 // Main header, crates/signinum-j2k-native/src/j2c/codestream.rs.
 enum Prog { LRCP = 0, RLCP = 1, RPCL = 2, PCRL = 3, CPRL = 4 };
-enum SbType { LL = 0, HL = 1, LH = 2, HH = 3 };
 enum QStyle { QNONE = 0, QDERIVED = 1, QEXPOUNDED = 2 };
 
 struct StepSize { uint16_t mantissa, exponent; };
@@ -725,7 +724,7 @@ static bool read_tag(size_t ni, uint32_t x, uint32_t y, BitReader& r, uint32_t p
 
 // ---------------------------------------------------------------------------
 // Build, crates/signinum-j2k-native/src/j2c/build.rs.
-struct Segment { uint8_t idx; uint32_t len; const uint8_t* data; };
+struct Segment { uint8_t idx; uint32_t len; const uint8_t* data; uint8_t passes = 0; };
 struct CodeBlock {
   IntRect rect;
   uint32_t xi, yi;
@@ -963,6 +962,114 @@ static bool resolve_ht(size_t band, const Prg& pg, BitReader& r, Storage& st) {
   return true;
 }
 
+// decode_num_classic_coding_passes (Table B.4), segment.rs:482-506: prefix
+// codes are matched by peeking, longest first.
+static bool classic_num_passes(BitReader& r, uint32_t& np) {
+  auto peek = [&](uint32_t n, uint32_t want) {
+    BitReader c = r;
+    uint32_t v;
+    return c.read_bits_stuffed(n, &v) && v == want;
+  };
+  uint32_t v;
+  if (peek(9, 0x1FF)) {
+    r.read_bits_stuffed(9, &v);
+    if (!r.read_bits_stuffed(7, &v)) return false;
+    np = v + 37;
+  } else if (peek(4, 0xF)) {
+    r.read_bits_stuffed(4, &v);
+    if (!r.read_bits_stuffed(5, &v)) return false;
+    np = v + 6;
+  } else if (peek(4, 0xE)) {
+    r.read_bits_stuffed(4, &v);
+    np = 5;
+  } else if (peek(4, 0xD)) {
+    r.read_bits_stuffed(4, &v);
+    np = 4;
+  } else if (peek(4, 0xC)) {
+    r.read_bits_stuffed(4, &v);
+    np = 3;
+  } else if (peek(2, 0x2)) {
+    r.read_bits_stuffed(2, &v);
+    np = 2;
+  } else if (peek(1, 0)) {
+    r.read_bits_stuffed(1, &v);
+    np = 1;
+  } else {
+    return false;
+  }
+  return true;
+}
+
+// segment_idx_for_bypass, segment.rs:585-591.
+static uint32_t bypass_segment(uint32_t p) { return p < 10 ? 0 : 1 + 2 * ((p - 10) / 3) + ((p - 10) % 3 == 2 ? 1 : 0); }
+
+// resolve_classic_segments, segment.rs:168-302.
+static bool resolve_classic(size_t band, const Prg& pg, BitReader& r, Storage& st, uint8_t style) {
+  const SubBand& sb = st.bands[band];
+  if (pg.prec >= sb.precincts.size()) return false;
+  Precinct& pr = st.precs[sb.precincts[pg.prec]];
+  for (size_t cbi : pr.cbs) {
+    CodeBlock& cb = st.cbs[cbi];
+    bool first = !cb.included;
+    bool inc;
+    if (cb.included) {
+      uint32_t b;
+      if (!r.read_bits_stuffed(1, &b)) return false;
+      inc = b == 1;
+    } else {
+      uint32_t v;
+      if (!read_tag(pr.incl_tree, cb.xi, cb.yi, r, 0, (uint32_t)pg.layer + 1, st.nodes, v)) return false;
+      inc = v <= pg.layer;
+    }
+    if (!inc) continue;
+    if (first) {
+      uint32_t v;
+      if (!read_tag(pr.zbp_tree, cb.xi, cb.yi, r, 0, UINT32_MAX, st.nodes, v)) return false;
+      cb.missing = (uint8_t)v;
+    }
+    cb.included = true;
+    uint32_t added;
+    if (!classic_num_passes(r, added)) return false;
+    uint32_t inc_l = 0, b;
+    for (;;) {
+      if (!r.read_bits_stuffed(1, &b)) return false;
+      if (b == 0) break;
+      ++inc_l;
+    }
+    cb.lblock += inc_l;
+    const uint32_t prev = cb.passes, cum = prev + added;
+    if (cum > 1 + 3 * 31) return false;
+    auto seg_idx = [&](uint32_t p) -> uint32_t {
+      if (style & 0x04) return p;
+      if (style & 0x01) return bypass_segment(p);
+      return cb.nonempty;
+    };
+    std::vector<Segment>& segs = cb.layers[pg.layer];
+    auto push = [&](uint32_t idx, uint32_t count) {
+      uint32_t bits = cb.lblock + (31 - (uint32_t)__builtin_clz(count)), len;
+      if (bits > 32 || !r.read_bits_stuffed(bits, &len)) return false;
+      segs.push_back({(uint8_t)idx, len, nullptr, (uint8_t)count});
+      return true;
+    };
+    uint32_t last = seg_idx(prev), count = 0;
+    for (uint32_t p = prev; p < cum; ++p) {
+      const uint32_t s = seg_idx(p);
+      if (s != last) {
+        if (!push(last, count)) return false;
+        last = s;
+        count = 1;
+      } else {
+        ++count;
+      }
+    }
+    if (count > 0 && !push(last, count)) return false;
+    cb.has_layer[pg.layer] = true;
+    cb.passes = (uint8_t)cum;
+    cb.nonempty = (uint8_t)(cb.nonempty + 1);
+  }
+  return true;
+}
+
 // parse_inner, segment.rs:53-148 (merged tile parts only).
 static bool parse_part(BitReader& r, const std::vector<Prg>& prog, size_t& pi, const Tile& t, Storage& st) {
   while (!r.at_end()) {
@@ -980,7 +1087,7 @@ static bool parse_part(BitReader& r, const std::vector<Prg>& prog, size_t& pi, c
     bool zero = b == 0;
     if (!zero)
       for (size_t bi : bands)
-        if (!resolve_ht(bi, pg, r, st)) return false;
+        if (!(ci.ht() ? resolve_ht(bi, pg, r, st) : resolve_classic(bi, pg, r, st, ci.cp.cbstyle))) return false;
     r.align();
     if (ci.flags & 4) {
       if (!r.read_marker(&m) || m != 0x92) return false;
@@ -1177,7 +1284,6 @@ static int32_t coefficient_to_i32(uint32_t v, uint8_t kmax) {
 // decode.rs:1117-1171, :1682-1716; ht_block_decode::decode_with_stats :236-300.
 static void decode_band(Storage& st, size_t bi, uint8_t res, const CompInfo& ci, const Header& h) {
   SubBand& sb = st.bands[bi];
-  if (!ci.ht()) fail(ERR_UNSUPPORTED, "classic block coding is outside the oracle's scope");
   auto em = ci.exponent_mantissa(sb.type, res);
   // Dequantisation step (decode.rs:1130-1151): 2^(R_b - exponent) * (1 + mantissa / 2048),
   // R_b = precision + log2 gain of the band (LL 0, HL/LH 1, HH 2); pow2i, math.rs:550-556.
@@ -1192,6 +1298,42 @@ static void decode_band(Storage& st, size_t bi, uint8_t res, const CompInfo& ci,
   if (nb < 0) fail(ERR_DECODE, "invalid bitplane count");
   if (nb > 32) fail(ERR_DECODE, "too many bitplanes");
   uint8_t num_bitplanes = (uint8_t)nb;
+  if (!ci.ht()) {
+    // Classic code blocks (decode_sub_band_bitplanes, decode.rs:1290-1345):
+    // the layers' segments are combined as in decode_inner (bitplane.rs:90-128).
+    std::vector<int32_t> blk;
+    for (size_t pi : sb.precincts)
+      for (size_t cbi : st.precs[pi].cbs) {
+        CodeBlock& cb = st.cbs[cbi];
+        uint32_t w = cb.rect.width(), hh = cb.rect.height();
+        std::vector<uint8_t> data;
+        std::vector<size_t> seg_start{0};
+        std::vector<uint32_t> seg_pass{0};
+        uint32_t last = 0, passes = 0;
+        for (size_t l = 0; l < cb.layers.size(); ++l) {
+          if (!cb.has_layer[l]) continue;
+          for (const Segment& s : cb.layers[l]) {
+            if (s.idx != last) {
+              seg_start.push_back(data.size());
+              seg_pass.push_back(passes);
+              last = s.idx;
+            }
+            if (s.len) data.insert(data.end(), s.data, s.data + s.len);
+            passes += s.passes;
+          }
+        }
+        seg_start.push_back(data.size());
+        seg_pass.push_back(passes);
+        blk.assign((size_t)w * hh, 0);
+        classic_block_decode(data.data(), seg_start, seg_pass, w, hh, cb.missing, cb.passes, num_bitplanes, sb.type,
+                             ci.cp.cbstyle, blk.data(), w);
+        uint32_t xo = cb.rect.x0 - sb.rect.x0, yo = cb.rect.y0 - sb.rect.y0;
+        for (uint32_t y = 0; y < hh; ++y)
+          for (uint32_t x = 0; x < w; ++x)
+            sb.coef[(size_t)(yo + y) * sb.rect.width() + xo + x] = (float)blk[(size_t)y * w + x] * step;
+      }
+    return;
+  }
   std::vector<uint32_t> buf;
   for (size_t pi : sb.precincts) {
     for (size_t cbi : st.precs[pi].cbs) {

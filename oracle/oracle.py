@@ -54,6 +54,7 @@ def lib():
         L.oracle_subband_coefficients.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32,
                                                   ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_tables.argtypes = [ctypes.c_void_p] * 4
+        L.oracle_ebcot_tables.argtypes = [ctypes.c_void_p] * 6
         L.oracle_decode_batch.restype = ctypes.c_long
         L.oracle_decode_batch.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
                                           ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
@@ -97,6 +98,14 @@ def tables():
     u1 = np.zeros(256, np.uint16)
     lib().oracle_tables(v0.ctypes.data, v1.ctypes.data, u0.ctypes.data, u1.ctypes.data)
     return v0, v1, u0, u1
+
+
+def ebcot_tables():
+    """Classic Tier-1 tables: zero-coding (LL/LH, HL, HH), sign label, sign
+    xor (256 u8 each) and the MQ probability records (235 bytes)."""
+    bufs = [np.zeros(256, np.uint8) for _ in range(5)] + [np.zeros(235, np.uint8)]
+    lib().oracle_ebcot_tables(*[b.ctypes.data for b in bufs])
+    return bufs
 
 
 def decode_batch(datas, fmt, workers=0):

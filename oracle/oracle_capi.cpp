@@ -87,6 +87,12 @@ long oracle_subband_coefficients(const uint8_t* data, size_t len, uint32_t comp,
   }
 }
 
+void oracle_ebcot_tables(uint8_t* zc_ll_lh, uint8_t* zc_hl, uint8_t* zc_hh, uint8_t* sc_label, uint8_t* sc_xor,
+                         uint8_t* qe_records) {
+  ebcot_tables(zc_ll_lh, zc_hl, zc_hh, sc_label, sc_xor);
+  ebcot_qe_records(qe_records);
+}
+
 void oracle_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1) {
   std::memcpy(vlc0, vlc_table(0), 1024 * 2);
   std::memcpy(vlc1, vlc_table(1), 1024 * 2);

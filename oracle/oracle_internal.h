@@ -49,6 +49,9 @@ struct IntRect {
 enum PixelFormat : int { FMT_GRAY8 = 0, FMT_RGB8 = 1, FMT_RGBA8 = 2, FMT_GRAY16 = 3, FMT_RGB16 = 4, FMT_RGBA16 = 5 };
 int bytes_per_pixel(int fmt);
 
+// Sub-band types (SubBandType).
+enum SbType { LL = 0, HL = 1, LH = 2, HH = 3 };
+
 enum RequestKind : int { REQ_FULL = 0, REQ_REGION = 1, REQ_SCALED = 2, REQ_REGION_SCALED = 3 };
 
 struct Request {
@@ -82,6 +85,23 @@ void decode(const uint8_t* data, size_t len, int fmt, const Request& req,
 bool ht_block_decode(const uint8_t* cleanup, size_t lcup, const uint8_t* refinement, size_t lref,
                      uint32_t missing_msbs, uint32_t num_passes, uint32_t width, uint32_t height,
                      uint32_t stride, bool stripe_causal, uint32_t* out);
+
+// Classic (EBCOT) Tier-1 decode of one code block (oracle_ebcot.cpp;
+// bitplane.rs:90-185 and the passes it calls).  `data` holds the block's
+// codeword segments back to back: segment k covers bytes [seg_start[k],
+// seg_start[k+1]) and coding passes [seg_pass[k], seg_pass[k+1]).  `band`
+// is the sub-band type (LL 0, HL 1, LH 2, HH 3), `style` the code-block style
+// byte of COD/COC.  Writes w x h int32 coefficients (stride out_stride).
+bool classic_block_decode(const uint8_t* data, const std::vector<size_t>& seg_start,
+                          const std::vector<uint32_t>& seg_pass, uint32_t w, uint32_t h, uint32_t missing,
+                          uint32_t num_passes, uint32_t total_bitplanes, int band, uint8_t style, int32_t* out,
+                          size_t out_stride);
+
+// The zero-coding (Table D.1, per band class) and sign-coding (Table D.3)
+// context tables over all 256 neighbour-significance patterns.
+void ebcot_tables(uint8_t* zc_ll_lh, uint8_t* zc_hl, uint8_t* zc_hh, uint8_t* sc_label, uint8_t* sc_xor);
+// The MQ probability table (Table C.2) as 47 (u16 qe LE, nmps, nlps, switch) records.
+void ebcot_qe_records(uint8_t* out);
 
 // Sub-band coefficients of component `comp` (after HT decode, before IDWT),
 // concatenated in the reference's sub-band order (LL, then HL, LH, HH for each

@@ -124,6 +124,7 @@ CUDA_SIGNATURES = {
     "sgn_plan_destroy": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "sgn_ctx_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "sgn_ht_lookup_tables": (None, [ctypes.c_void_p] * 4),
+    "sgn_ebcot_tables": (None, [ctypes.c_void_p] * 6),
     "sgn_j2k_ht_block_table": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                                 ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_uint64)]),
     "sgn_plan_tile_coefficients": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
@@ -141,6 +142,10 @@ ENCODE_SIGNATURES = {
     "sgn_j2k_encode_irreversible": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                                    ctypes.c_uint32, ctypes.POINTER(SgnEncodeOptions), ctypes.c_double,
                                                    ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_j2k_encode_classic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_uint32, ctypes.POINTER(SgnEncodeOptions), ctypes.c_uint32,
+                                              ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t,
+                                              ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_synth_he_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p]),
     "sgn_synth_blank_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
     "sgn_synth_fluor_gray16": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),

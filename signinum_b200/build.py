@@ -33,6 +33,7 @@ CUDA_SOURCES = [
 ]
 ENCODE_SOURCES = [
     CSRC / "encode" / "j2k_encode.cpp",
+    CSRC / "encode" / "classic_encode.cpp",
     CSRC / "encode" / "synth.cpp",
     CSRC / "encode" / "encode_capi.cpp",
 ]

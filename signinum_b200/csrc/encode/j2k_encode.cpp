@@ -26,6 +26,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../ebcot.h"
 #include "../ht_tables.h"
 #include "j2k_encode.h"
 
@@ -423,6 +424,8 @@ struct TagTree {
 
 struct CodeBlockOut {
   std::vector<uint8_t> bytes;
+  ClassicBlockOut classic;  // classic Tier-1 segments (bytes unused then)
+  bool empty() const { return bytes.empty() && classic.passes == 0; }
 };
 
 struct Band {
@@ -596,7 +599,8 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
       }
     }
     const uint32_t cw = lw[L], ch = lhh[L];
-    auto make_band = [&](const std::vector<int32_t>& data, uint32_t w, uint32_t h, uint32_t gain) -> int {
+    auto make_band = [&](const std::vector<int32_t>& data, uint32_t w, uint32_t h, uint32_t gain,
+                         uint8_t band_class) -> int {
       Band b;
       b.w = w;
       b.h = h;
@@ -609,20 +613,26 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
         for (uint32_t bx = 0; bx < b.ncx; ++bx) {
           uint32_t x0 = bx * cbw, y0 = by * cbh, bw = std::min(cbw, w - x0), bh = std::min(cbh, h - y0);
           CodeBlockOut cb;
-          if (encode_ht_block(&data[(size_t)y0 * w + x0], w, bw, bh, b.mb, cb.bytes) != 0) return -3;
+          if (P.classic) {
+            if (encode_classic_block(&data[(size_t)y0 * w + x0], w, bw, bh, b.mb, band_class, P.cb_style,
+                                     cb.classic) != 0)
+              return -3;
+          } else if (encode_ht_block(&data[(size_t)y0 * w + x0], w, bw, bh, b.mb, cb.bytes) != 0) {
+            return -3;
+          }
           b.blocks.push_back(std::move(cb));
         }
       bands[c].push_back(std::move(b));
       return 0;
     };
-    if (make_band(cur, cw, ch, 0) != 0) return -3;
+    if (make_band(cur, cw, ch, 0, ebcot::kLlLh) != 0) return -3;
     for (uint32_t r = 1; r <= L; ++r) {
       uint32_t d = L + 1 - r;  // decomposition level of resolution r
       uint32_t pw = lw[d - 1], ph = lhh[d - 1];
       uint32_t lwd = (pw + 1) / 2, hwd = pw / 2, lhd = (ph + 1) / 2, hhd = ph / 2;
-      if (make_band(hl[d], hwd, lhd, 1) != 0) return -3;
-      if (make_band(lh[d], lwd, hhd, 1) != 0) return -3;
-      if (make_band(hh[d], hwd, hhd, 2) != 0) return -3;
+      if (make_band(hl[d], hwd, lhd, 1, ebcot::kHl) != 0) return -3;
+      if (make_band(lh[d], lwd, hhd, 1, ebcot::kLlLh) != 0) return -3;
+      if (make_band(hh[d], hwd, hhd, 2, ebcot::kHh) != 0) return -3;
     }
   }
   // Packets: one layer, one precinct per resolution.
@@ -632,7 +642,7 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     size_t b0 = r == 0 ? 0 : 1 + (size_t)(r - 1) * 3, nb = r == 0 ? 1 : 3;
     bool any = false;
     for (size_t bi = b0; bi < b0 + nb; ++bi)
-      for (auto& cb : bands[c][bi].blocks) any = any || !cb.bytes.empty();
+      for (auto& cb : bands[c][bi].blocks) any = any || !cb.empty();
     if (P.sop_eph) {
       tile.push_back(0xFF); tile.push_back(0x91);
       put16(tile, 4);
@@ -648,16 +658,40 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
         if (b.ncx == 0 || b.ncy == 0) continue;
         std::vector<uint32_t> incl(b.blocks.size()), zbp(b.blocks.size());
         for (size_t i = 0; i < b.blocks.size(); ++i) {
-          incl[i] = b.blocks[i].bytes.empty() ? 1 : 0;
-          zbp[i] = b.blocks[i].bytes.empty() ? 0xFFFFu : b.mb - 1;  // empty leaves never coded
+          const bool empty = b.blocks[i].empty();
+          incl[i] = empty ? 1 : 0;
+          // Empty leaves are never coded.
+          zbp[i] = empty ? 0xFFFFu : (P.classic ? b.blocks[i].classic.zero_planes : b.mb - 1);
         }
         TagTree ti(b.ncx, b.ncy, incl), tz(b.ncx, b.ncy, zbp);
         for (uint32_t y = 0; y < b.ncy; ++y)
           for (uint32_t x = 0; x < b.ncx; ++x) {
             const auto& cb = b.blocks[(size_t)y * b.ncx + x];
             ti.encode(x, y, 1, hw);
-            if (cb.bytes.empty()) continue;
+            if (cb.empty()) continue;
             tz.encode(x, y, UINT32_MAX, hw);
+            if (P.classic) {
+              // Number of coding passes (Table B.4), Lblock increment, then
+              // one length per codeword segment of Lblock + floor(log2(passes))
+              // bits (B.10.6-B.10.7).
+              const ClassicBlockOut& k = cb.classic;
+              const uint32_t np = k.passes;
+              if (np == 1) hw.bit(0);
+              else if (np == 2) hw.bits(0x2, 2);
+              else if (np <= 5) hw.bits(0xC | (np - 3), 4);
+              else if (np <= 36) { hw.bits(0xF, 4); hw.bits(np - 6, 5); }
+              else { hw.bits(0x1FF, 9); hw.bits(np - 37, 7); }
+              uint32_t inc = 0;
+              for (size_t sgi = 0; sgi < k.seg_len.size(); ++sgi) {
+                const uint32_t lg = bitlen(k.seg_passes[sgi]) - 1, need = bitlen(k.seg_len[sgi]);
+                if (need > 3 + lg) inc = std::max(inc, need - 3 - lg);
+              }
+              for (uint32_t i = 0; i < inc; ++i) hw.bit(1);
+              hw.bit(0);
+              for (size_t sgi = 0; sgi < k.seg_len.size(); ++sgi)
+                hw.bits(k.seg_len[sgi], 3 + inc + bitlen(k.seg_passes[sgi]) - 1);
+              continue;
+            }
             hw.bit(0);  // one coding pass
             uint32_t len = (uint32_t)cb.bytes.size();
             uint32_t need = bitlen(len);
@@ -673,7 +707,10 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     if (P.sop_eph) { tile.push_back(0xFF); tile.push_back(0x92); }
     if (any)
       for (size_t bi = b0; bi < b0 + nb; ++bi)
-        for (auto& cb : bands[c][bi].blocks) tile.insert(tile.end(), cb.bytes.begin(), cb.bytes.end());
+        for (auto& cb : bands[c][bi].blocks) {
+          const std::vector<uint8_t>& bytes = P.classic ? cb.classic.bytes : cb.bytes;
+          tile.insert(tile.end(), bytes.begin(), bytes.end());
+        }
   };
   if (P.progression == 3 || P.progression == 4) {
     for (uint32_t c = 0; c < C; ++c)
@@ -687,15 +724,15 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   out.push_back(0xFF); out.push_back(0x4F);  // SOC
   out.push_back(0xFF); out.push_back(0x51);  // SIZ
   put16(out, 38 + 3 * C);
-  put16(out, 0x4000);  // Rsiz: HTJ2K
+  put16(out, P.classic ? 0 : 0x4000);  // Rsiz: HTJ2K unless classic
   put32(out, W); put32(out, H); put32(out, 0); put32(out, 0);
   put32(out, W); put32(out, H); put32(out, 0); put32(out, 0);
   put16(out, C);
   for (uint32_t c = 0; c < C; ++c) { out.push_back((uint8_t)(bd - 1)); out.push_back(1); out.push_back(1); }
-  out.push_back(0xFF); out.push_back(0x50);  // CAP
-  put16(out, 8);
-  put32(out, 0x00020000);
-  {
+  if (!P.classic) {
+    out.push_back(0xFF); out.push_back(0x50);  // CAP
+    put16(out, 8);
+    put32(out, 0x00020000);
     uint32_t mbits = bd - 1;
     uint32_t bp = mbits <= 8 ? 0 : (mbits < 28 ? mbits - 8 : 13 + (mbits >> 2));
     put16(out, bp);
@@ -709,7 +746,7 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   out.push_back((uint8_t)L);
   out.push_back((uint8_t)P.cbw_exp);
   out.push_back((uint8_t)P.cbh_exp);
-  out.push_back(0x40);
+  out.push_back(P.classic ? (uint8_t)(P.cb_style & 0x3F) : 0x40);  // code-block style
   out.push_back(irr ? 0 : 1);  // wavelet: 0 = 9/7 irreversible, 1 = 5/3 reversible
   out.push_back(0xFF); out.push_back(0x5C);  // QCD
   if (irr) {

@@ -17,7 +17,20 @@ struct EncodeParams {
   // with relative step rel_step of every band's nominal range.
   bool irreversible = false;
   double rel_step = 1.0 / 256;
+  // Classic (EBCOT) Tier-1 instead of HT, with code-block style bits
+  // (bypass 0x01, reset 0x02, termall 0x04, vcausal 0x08, segsym 0x20).
+  bool classic = false;
+  uint8_t cb_style = 0;
 };
+// One classic code block: its codeword segments back to back, each
+// segment's length and coding-pass count, and the block's zero bit-planes.
+struct ClassicBlockOut {
+  std::vector<uint8_t> bytes;
+  std::vector<uint32_t> seg_len, seg_passes;
+  uint32_t passes = 0, zero_planes = 0;
+};
+int encode_classic_block(const int32_t* c, size_t stride, uint32_t w, uint32_t h, uint32_t Mb, uint8_t band_class,
+                         uint8_t style, ClassicBlockOut& out);
 int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& out);
 int encode_ht_block(const int32_t* c, size_t stride, uint32_t w, uint32_t h, uint32_t Mb, std::vector<uint8_t>& out);
 }  // namespace enc

@@ -21,6 +21,7 @@
 
 #include "../../../include/signinum_j2k_cuda.h"
 #include "../device_plan.h"
+#include "../ebcot.h"
 #include "../ht_tables.h"
 #include "../kernels/kernels.h"
 #include "codestream.h"
@@ -711,6 +712,29 @@ void sgn_ctx_destroy(sgn_ctx* ctx) {
 uint64_t sgn_ctx_submissions(const sgn_ctx* ctx) { return ctx ? ctx->submissions.load() : 0; }
 
 void* sgn_ctx_stream(sgn_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+void sgn_ebcot_tables(uint8_t* zc_ll_lh, uint8_t* zc_hl, uint8_t* zc_hh, uint8_t* sc_label, uint8_t* sc_xor,
+                      uint8_t* qe_records) {
+  using namespace sgn::ebcot;
+  for (int n = 0; n < 256; ++n) {
+    zc_ll_lh[n] = zc_context((uint8_t)n, kLlLh);
+    zc_hl[n] = zc_context((uint8_t)n, kHl);
+    zc_hh[n] = zc_context((uint8_t)n, kHh);
+    // Patterns with both bits of a neighbour's field set cannot occur; the
+    // reference's table holds (0, 0) there.
+    bool possible = true;
+    for (int sh = 0; sh < 8; sh += 2) possible = possible && ((n >> sh) & 3) != 3;
+    sc_label[n] = sc_xor[n] = 0;
+    if (possible) sc_context((uint8_t)n, sc_label[n], sc_xor[n]);
+  }
+  for (int k = 0; k < 47; ++k) {
+    qe_records[5 * k] = (uint8_t)(kQe[k] & 0xFF);
+    qe_records[5 * k + 1] = (uint8_t)(kQe[k] >> 8);
+    qe_records[5 * k + 2] = kNmps[k];
+    qe_records[5 * k + 3] = kNlps[k];
+    qe_records[5 * k + 4] = kSwitch[k];
+  }
+}
 
 void sgn_ht_lookup_tables(uint16_t* vlc0, uint16_t* vlc1, uint16_t* uvlc0, uint16_t* uvlc1) {
   HtDecodeTables t;

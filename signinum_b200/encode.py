@@ -69,6 +69,25 @@ def encode_irreversible(pixels: np.ndarray, width: int, height: int, components:
     return out[: n.value].tobytes()
 
 
+def encode_classic(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int, style: int = 0,
+                   irreversible: bool = False, relative_step: float = 1.0 / 256, levels: int = 5, cb_exp: int = 4,
+                   use_mct: bool = True, progression: int = 0, cb_exp_h: int | None = None) -> bytes:
+    """Classic (EBCOT Tier-1) codestream with code-block style bits `style`,
+    lossless 5/3 or (irreversible) lossy 9/7; same sample layout as
+    encode_lossless."""
+    px = np.ascontiguousarray(pixels)
+    opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression, 0, 0)
+    cap = px.nbytes * 3 + 65536
+    out = np.zeros(cap, np.uint8)
+    n = ctypes.c_size_t()
+    rc = _native.encode_lib().sgn_j2k_encode_classic(px.ctypes.data, width, height, components, bit_depth,
+                                                     ctypes.byref(opts), style, int(irreversible), relative_step,
+                                                     out.ctypes.data, cap, ctypes.byref(n))
+    if rc != 0:
+        raise ValueError(f"encode failed ({rc})")
+    return out[: n.value].tobytes()
+
+
 def he_rgb8(seed: int, width: int, height: int, sigma: float = 6.0) -> np.ndarray:
     out = np.zeros(width * height * 3, np.uint8)
     _native.encode_lib().sgn_synth_he_rgb8(seed, width, height, sigma, out.ctypes.data)
