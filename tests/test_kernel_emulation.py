@@ -28,7 +28,8 @@ def emu(tmp_path_factory):
     flags = ["g++", "-std=c++20", "-O1", "-fsanitize=address", "-ffp-contract=off", f"-I{EMU}", f"-I{CSRC}",
              f"-I{ROOT / 'oracle'}"]
     units = [out / "ht_decode_emu.cpp", out / "idwt_pack_emu.cpp", EMU / "emu_main.cpp", CSRC / "host" / "codestream.cpp",
-             ROOT / "oracle" / "oracle.cpp", ROOT / "oracle" / "oracle_ht.cpp", ROOT / "oracle" / "oracle_capi.cpp"]
+             ROOT / "oracle" / "oracle.cpp", ROOT / "oracle" / "oracle_ht.cpp", ROOT / "oracle" / "oracle_ebcot.cpp",
+             ROOT / "oracle" / "oracle_capi.cpp"]
     procs = [subprocess.Popen(flags + ["-c", str(u), "-o", str(out / (u.stem + ".o"))]) for u in units]
     assert all(p.wait() == 0 for p in procs)
     subprocess.run(flags + ["-o", str(out / "emu")] + [str(out / (u.stem + ".o")) for u in units] + ["-lpthread"],
