@@ -25,6 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = [
     CSRC / "kernels" / "ht_decode.cu",
     CSRC / "kernels" / "idwt_pack.cu",
+    CSRC / "kernels" / "classic_decode.cu",
     CSRC / "host" / "runtime.cu",
     CSRC / "host" / "noalloc.cu",
     CSRC / "host" / "server.cu",

@@ -62,6 +62,34 @@ __host__ __device__
 #endif
 inline uint32_t sym_words(uint32_t w, uint32_t h) { return (sym_row_stride(w) * ((h + 1) / 2) + 3) & ~3u; }
 
+// One classic (EBCOT Tier-1) code block: its codeword segments lie back to
+// back in the input arena from `src` (classic_block_decode's `data`), the
+// segment table entries [seg, seg + nseg) give each segment's bytes and
+// coding passes.  passes == 0: an all-zero block.
+struct ClassicJob {
+  uint64_t src;        // byte offset of the block's first segment in the input arena
+  uint64_t dst;        // element offset of the block's first sample in the coefficient arena
+  uint32_t seg;        // first segment-table entry
+  uint32_t tile;       // batch index of the tile (status reporting)
+  uint32_t stride;     // band row stride in elements
+  uint16_t w, h;
+  uint8_t nseg, passes;
+  uint8_t bitplanes;   // the band's bit-planes minus the block's missing ones (> 0 when passes > 0)
+  uint8_t band_class;  // zero-coding rule: 0 LL/LH, 1 HL, 2 HH
+  uint8_t style;       // code-block style bits
+  uint8_t pad[3];
+};
+static_assert(sizeof(ClassicJob) == 40, "ClassicJob layout");
+
+struct ClassicSeg {
+  uint32_t len;     // bytes
+  uint32_t passes;  // coding passes
+};
+
+// Flag words per thread of the classic kernel: (w + 2) (h + 2) for the
+// largest code block (w h <= 4096, w, h <= 1024).
+constexpr uint32_t kClassicSlotMax = 6160;
+
 // Irreversible (9/7) levels use the same tables: band pointers hold int32
 // coefficients that the kernel dequantises with `step`, level images (the
 // ll input after the first level, and `out`) hold f32 samples.

@@ -316,9 +316,43 @@ struct BlockState {
   bool included = false;
   uint8_t missing = 0, passes = 0;
   uint32_t lblock = 3;
-  uint32_t lcup = 0, lref = 0;
+  uint32_t lcup = 0, lref = 0;  // classic: lcup = bytes of all segments
   int64_t cleanup_off = -1, ref_off = -1;
+  std::vector<ClassicSegment> segs;  // classic
 };
+
+// Number of coding passes of a classic block (Table B.4,
+// decode_num_classic_coding_passes, segment.rs:482-506): prefixes matched by
+// peeking, longest first.
+bool classic_passes(Reader& r, uint32_t& np) {
+  auto peek = [&](uint32_t n, uint32_t want) {
+    Reader c = r;
+    uint32_t v;
+    return c.bits(n, v) && v == want;
+  };
+  uint32_t v;
+  if (peek(9, 0x1FF)) {
+    r.bits(9, v);
+    if (!r.bits(7, v)) return false;
+    np = v + 37;
+  } else if (peek(4, 0xF)) {
+    r.bits(4, v);
+    if (!r.bits(5, v)) return false;
+    np = v + 6;
+  } else if (peek(4, 0xE) || peek(4, 0xD) || peek(4, 0xC)) {
+    r.bits(4, v);
+    np = v - 0xC + 3;
+  } else if (peek(2, 0x2)) {
+    r.bits(2, v);
+    np = 2;
+  } else if (peek(1, 0)) {
+    r.bits(1, v);
+    np = 1;
+  } else {
+    return false;
+  }
+  return true;
+}
 
 struct Packet {  // one (component, resolution, precinct)
   uint8_t comp, res;
@@ -591,7 +625,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   const Comp& c0 = h.comps[0];
   for (auto& c : h.comps) {
     if (c.xr != 1 || c.yr != 1) fail(ST_UNSUPPORTED, "sub-sampled components are not supported by the CUDA path");
-    if (!(c.cs.cbstyle & 0x40)) fail(ST_UNSUPPORTED, "classic (non-HT) block coding is not supported by the CUDA path");
+    if (c.cs.cbstyle != c0.cs.cbstyle) fail(ST_UNSUPPORTED, "components with different code-block styles");
     if (c.cs.transform != c0.cs.transform) fail(ST_UNSUPPORTED, "components with different wavelet transforms");
     // The reversible path is integer arithmetic: a quantised 5/3 codestream
     // (non-integer dequantised samples) is outside it.
@@ -603,7 +637,9 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     if (n == 0) fail(ST_DECODE, "missing step sizes");
     if (c.q.style != 1 && max_res != 0 && 1 + (max_res - 1) * 3 + 2 >= n) fail(ST_DECODE, "insufficient exponents");
   }
-  if (h.layers > 1) fail(ST_UNSUPPORTED, "multi-layer HTJ2K packet assembly");
+  const bool classic = !(c0.cs.cbstyle & 0x40);
+  if (h.layers > 1 && !classic) fail(ST_UNSUPPORTED, "multi-layer HTJ2K packet assembly");
+  if (h.layers > 1) fail(ST_UNSUPPORTED, "multi-layer classic codestreams are not supported by the CUDA path");
   const uint32_t W = h.gw, H = h.gh, L = c0.cs.ndecomp;
   T = TileLayout();
   T.width = W;
@@ -614,6 +650,8 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   T.mct = h.mct;
   T.reversible = c0.cs.transform == 1;
   T.causal = (c0.cs.cbstyle & 0x08) != 0;
+  T.classic = classic;
+  T.cbstyle = c0.cs.cbstyle;
   uint32_t skipped = 0;
   if (target) {
     uint32_t wr = W / target[0], hr = H / target[1];
@@ -793,6 +831,39 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
             }
             bs.included = true;
             if (!first || bs.passes != 0) { ok = false; break; }
+            if (classic) {
+              // resolve_classic_segments (segment.rs:168-302), one layer:
+              // segments by pass (termination on every pass), by the bypass
+              // rule, or one for the block.
+              uint32_t np, b, incr = 0;
+              if (!classic_passes(pr, np) || np > 1 + 3 * 31) { ok = false; break; }
+              for (;;) {
+                if (!pr.bits(1, b)) { ok = false; break; }
+                if (!b) break;
+                ++incr;
+              }
+              if (!ok) break;
+              bs.lblock += incr;
+              const uint8_t st = cs.cbstyle;
+              auto seg_of = [&](uint32_t p) -> uint32_t {
+                return (st & 0x04) ? p : (st & 0x01) ? (p < 10 ? 0 : 1 + 2 * ((p - 10) / 3) + ((p - 10) % 3 == 2)) : 0;
+              };
+              uint32_t total = 0, count = 0;
+              for (uint32_t p = 0; ok && p <= np; ++p) {
+                if (p == np || (p > 0 && seg_of(p) != seg_of(p - 1))) {
+                  uint32_t len, nbits = bs.lblock + (31 - (uint32_t)__builtin_clz(count));
+                  if (nbits > 32 || !pr.bits(nbits, len) || total + (uint64_t)len > 0x7FFFFFFF) { ok = false; break; }
+                  bs.segs.push_back({len, (uint8_t)count});
+                  total += len;
+                  count = 0;
+                }
+                ++count;
+              }
+              if (!ok) break;
+              bs.passes = (uint8_t)np;
+              bs.lcup = total;
+              continue;
+            }
             uint32_t np = 1, b;
             if (!pr.bits(1, b)) { ok = false; break; }
             if (b) {
@@ -851,7 +922,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
           size_t at = part.first + pr.pos();
           if (!pr.skip(bs.lcup)) { ok = false; break; }
           bs.cleanup_off = (int64_t)at;
-          if (bs.passes > 1) {
+          if (bs.passes > 1 && !classic) {
             size_t at2 = part.first + pr.pos();
             if (!pr.skip(bs.lref)) { ok = false; break; }
             bs.ref_off = (int64_t)at2;
@@ -879,6 +950,23 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     uint32_t nbp = b.nbp;
     uint32_t actual = nbp > bs.missing ? nbp - bs.missing : 0;
     if (nbp > 31) fail(ST_DECODE, "too many bitplanes");
+    if (classic) {
+      // Classic blocks keep every pass; the kernel decodes the first
+      // 1 + 3 (bitplanes - 1) of them (reset_for_job, bitplane.rs:493-548).
+      if (nbp == 0 || bs.passes == 0 || actual == 0) {
+        cb.passes = 0;
+      } else {
+        if (bs.cleanup_off < 0) fail(ST_DECODE, "code-block decode failure: missing segment data");
+        cb.cleanup_off = (uint32_t)bs.cleanup_off;
+        cb.lcup = bs.lcup;
+        cb.seg_begin = (uint32_t)T.segments.size();
+        cb.nseg = (uint8_t)bs.segs.size();
+        if (bs.segs.size() > 255) fail(ST_DECODE, "too many codeword segments");
+        T.segments.insert(T.segments.end(), bs.segs.begin(), bs.segs.end());
+      }
+      T.blocks.push_back(cb);
+      continue;
+    }
     if (nbp == 0 || bs.passes == 0 || actual == 0) {
       cb.passes = 0;  // all-zero block
     } else {

@@ -45,11 +45,19 @@ struct CodeBlock {
   uint32_t band;        // index into TileLayout::bands
   uint32_t x0, y0;      // position inside the band
   uint16_t w, h;
-  uint32_t cleanup_off; // byte offset of the cleanup segment in the codestream
-  uint32_t lcup;
+  uint32_t cleanup_off; // byte offset of the cleanup segment in the codestream (classic: of the first segment)
+  uint32_t lcup;        // classic: the bytes of all segments, back to back
   uint32_t ref_off;     // byte offset of the refinement segment (when lref > 0)
   uint32_t lref;
   uint8_t missing_msbs, passes;
+  uint32_t seg_begin = 0;  // classic: first entry in TileLayout::segments
+  uint8_t nseg = 0;        // classic: codeword segments of the block
+};
+
+// A classic code block's codeword segment: its bytes and coding passes.
+struct ClassicSegment {
+  uint32_t len;
+  uint8_t passes;
 };
 
 struct TileLayout {
@@ -60,6 +68,9 @@ struct TileLayout {
   bool mct = false;
   bool reversible = true;          // 5/3 (integer path); false: 9/7 with dequantisation
   bool causal = false;             // vertically causal context (code-block style bit 3)
+  bool classic = false;            // classic (EBCOT) Tier-1 code blocks instead of HT
+  uint8_t cbstyle = 0;             // code-block style byte of COD/COC
+  std::vector<ClassicSegment> segments;  // classic: per block, in block order
   uint32_t skipped = 0;            // resolution levels dropped for a reduced decode
   uint32_t out_w = 0, out_h = 0;   // dimensions of the decoded (possibly reduced) image
   std::vector<Band> bands;         // per component: LL, then HL/LH/HH per resolution

@@ -248,12 +248,20 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     uint64_t sym = 0;
     uint32_t nref = 0, ms_words = 8, max_w = 1;
     uint32_t hist[kLenBuckets];
+    uint32_t ncls = 0, nseg = 0, slot = 0;  // classic tiles
   };
   std::vector<TileHt> th(n);
   ctx->workers->parallel_for(n, [&](size_t i) {
     TileHt& t = th[i];
     std::fill(t.hist, t.hist + kLenBuckets, 0u);
     if (plan->status[i] != SGN_OK) return;
+    if (work[i].L->classic) {
+      t.ncls = (uint32_t)work[i].L->blocks.size();
+      t.nseg = (uint32_t)work[i].L->segments.size();
+      for (const CodeBlock& cb : work[i].L->blocks)
+        if (cb.passes) t.slot = std::max<uint32_t>(t.slot, (uint32_t)(cb.w + 2) * (cb.h + 2));
+      return;
+    }
     for (const CodeBlock& cb : work[i].L->blocks) {
       ++t.hist[len_bucket(cb.lcup)];
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
@@ -272,6 +280,15 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   std::vector<uint32_t> ref_off(n, 0), start((size_t)kLenBuckets * n, 0);
   uint64_t sym_total = 0;
   uint32_t nht = 0, nref = 0, ms_words = 8, max_w = 1;
+  std::vector<uint32_t> cls_off(n, 0), cseg_off(n, 0);
+  uint32_t ncls = 0, ncseg = 0, cslot = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cls_off[i] = ncls;
+    ncls += th[i].ncls;
+    cseg_off[i] = ncseg;
+    ncseg += th[i].nseg;
+    cslot = std::max(cslot, th[i].slot);
+  }
   for (size_t i = 0; i < n; ++i) {
     sym_off[i] = sym_total;
     sym_total += th[i].sym;
@@ -410,6 +427,16 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   packs.insert(packs.end(), packs97.begin(), packs97.end());
   if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
   if ((e = dalloc(&plan->d_refine, nref, s)) != cudaSuccess) return cuda_status(e, "refine list");
+  plan->nclassic = ncls;
+  if (ncls) {
+    plan->classic_slot = std::max<uint32_t>(cslot, 1);
+    const uint32_t per = classic_threads_per_cta();
+    plan->classic_ctas = std::min<uint32_t>((ncls + per - 1) / per, (uint32_t)ctx->sm_count * 2);
+    if ((e = dalloc(&plan->d_classic, ncls, s)) != cudaSuccess) return cuda_status(e, "classic jobs");
+    if ((e = dalloc(&plan->d_csegs, std::max<uint32_t>(ncseg, 1), s)) != cudaSuccess) return cuda_status(e, "classic segments");
+    if ((e = dalloc(&plan->d_cscratch, (size_t)plan->classic_ctas * per * plan->classic_slot, s)) != cudaSuccess)
+      return cuda_status(e, "classic scratch");
+  }
   if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
   if ((e = dalloc(&plan->d_pack, packs.size(), s)) != cudaSuccess) return cuda_status(e, "pack jobs");
 
@@ -419,7 +446,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   const size_t at_ref = at_ht + up16((size_t)nht * sizeof(HtJob));
   const size_t at_idwt = at_ref + up16((size_t)nref * 4);
   const size_t at_pack = at_idwt + up16(idwt.size() * sizeof(IdwtJob));
-  const size_t stage_bytes = at_pack + up16(packs.size() * sizeof(PackJob));
+  const size_t at_cls = at_pack + up16(packs.size() * sizeof(PackJob));
+  const size_t at_cseg = at_cls + up16((size_t)ncls * sizeof(ClassicJob));
+  const size_t stage_bytes = at_cseg + up16((size_t)ncseg * sizeof(ClassicSeg));
   if ((e = staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
   uint8_t* st = staging.p;
   HtJob* ht = reinterpret_cast<HtJob*>(st + at_ht);
@@ -430,6 +459,31 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (plan->status[i] != SGN_OK) return;
     if (!direct) std::memcpy(st + in_off[i], datas[i], lens[i]);
     const TileLayout& L = *work[i].L;
+    if (L.classic) {
+      // Classic blocks: one job each (all-zero blocks too, so that every
+      // block's samples are written), segments after the tile's offset.
+      ClassicJob* cj = reinterpret_cast<ClassicJob*>(st + at_cls) + cls_off[i];
+      ClassicSeg* cs = reinterpret_cast<ClassicSeg*>(st + at_cseg) + cseg_off[i];
+      for (size_t k = 0; k < L.segments.size(); ++k) cs[k] = ClassicSeg{L.segments[k].len, L.segments[k].passes};
+      for (const CodeBlock& cb : L.blocks) {
+        const Band& b = L.bands[cb.band];
+        ClassicJob& j = *cj++;
+        std::memset(&j, 0, sizeof(j));
+        j.src = in_off[i] + cb.cleanup_off;
+        j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+        j.seg = cseg_off[i] + cb.seg_begin;
+        j.tile = (uint32_t)i;
+        j.stride = b.w;
+        j.w = cb.w;
+        j.h = cb.h;
+        j.nseg = cb.nseg;
+        j.passes = cb.passes;
+        j.bitplanes = (uint8_t)(b.nbp > cb.missing_msbs ? b.nbp - cb.missing_msbs : 0);
+        j.band_class = b.type == BAND_HL ? ebcot::kHl : b.type == BAND_HH ? ebcot::kHh : ebcot::kLlLh;
+        j.style = L.cbstyle;
+      }
+      return;
+    }
     uint32_t cursor[kLenBuckets];
     for (uint32_t b = 0; b < kLenBuckets; ++b) cursor[b] = start[(size_t)b * n + i];
     uint64_t sym = sym_off[i];
@@ -467,7 +521,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
              {plan->d_ht, at_ht, (size_t)nht * sizeof(HtJob)},
              {plan->d_refine, at_ref, (size_t)nref * 4},
              {plan->d_idwt, at_idwt, idwt.size() * sizeof(IdwtJob)},
-             {plan->d_pack, at_pack, packs.size() * sizeof(PackJob)}};
+             {plan->d_pack, at_pack, packs.size() * sizeof(PackJob)},
+             {plan->d_classic, at_cls, (size_t)ncls * sizeof(ClassicJob)},
+             {plan->d_csegs, at_cseg, (size_t)ncseg * sizeof(ClassicSeg)}};
   for (auto& u : ups) {
     if (!u.bytes) continue;
     if ((e = cudaMemcpyAsync(u.d, st + u.at, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
@@ -476,12 +532,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // The staging buffer is reused by the next call: finish the copies now
   // (callers that reuse it only after the plan has run pass sync_uploads false).
   if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
-  plan->launches =
-      (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + plan->rounds.size() + (plan->npack ? 1 : 0) + (plan->npack97 ? 1 : 0);
+  plan->launches = (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + (plan->nclassic ? 1 : 0) + plan->rounds.size() +
+                   (plan->npack ? 1 : 0) + (plan->npack97 ? 1 : 0);
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
   // Work-queue counters and the launch shape (an autotuned one when this
   // context has tuned a plan of the same signature).
-  plan->nqueues = (uint32_t)plan->rounds.size() + 3;
+  plan->nqueues = (uint32_t)plan->rounds.size() + 4;
   if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
   LaunchConfig cfg;
   {
@@ -526,6 +582,11 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
   return SGN_OK;
 }
 
+cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s) {
+  return launch_classic(p->d_classic, p->d_csegs, p->nclassic, p->d_input, p->d_coef, p->d_cscratch, p->classic_slot,
+                        p->classic_ctas, p->d_queue + p->rounds.size() + 3, s);
+}
+
 cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas) {
   const RoundInfo& r = p->rounds[k];
   uint32_t* q = queued ? p->d_queue + 1 + k : nullptr;
@@ -549,7 +610,7 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
   if (p->d_queue) cudaFreeAsync(p->d_queue, s);
   p->d_queue = nullptr;
   void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
-                  p->d_refine, p->d_idwt, p->d_pack, p->d_status};
+                  p->d_refine, p->d_idwt, p->d_pack, p->d_status, p->d_classic, p->d_csegs, p->d_cscratch};
   for (void* q : ptrs)
     if (q) cudaFreeAsync(q, s);
   p->d_input = nullptr;
@@ -557,6 +618,9 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
   p->d_symbols = nullptr;
   p->d_ht = nullptr;
   p->d_refine = nullptr;
+  p->d_classic = nullptr;
+  p->d_csegs = nullptr;
+  p->d_cscratch = nullptr;
   p->d_idwt = nullptr;
   p->d_pack = nullptr;
   p->d_status = nullptr;
@@ -583,6 +647,7 @@ sgn_status execute(sgn_plan* p, cudaStream_t s) {
     return cuda_status(e, "HT MagSgn launch");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
+  if ((e = launch_classic_blocks(p, s)) != cudaSuccess) return cuda_status(e, "classic block launch");
   for (size_t k = 0; k < p->rounds.size(); ++k)
     if ((e = launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas)) != cudaSuccess) return cuda_status(e, "IDWT launch");
   if ((e = launch_packs(p, s, c.pack_queue != 0, c.pack_ctas)) != cudaSuccess) return cuda_status(e, "pack launch");
@@ -816,6 +881,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
                        c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas));
   chk(cudaEventRecord(ev[2], s));
   chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
+  chk(launch_classic_blocks(p, s));
   chk(cudaEventRecord(ev[3], s));
   for (size_t k = 0; k < p->rounds.size(); ++k) chk(launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas));
   chk(cudaEventRecord(ev[4], s));

@@ -159,6 +159,8 @@ struct RoundInfo {
 struct sgn_plan {
   using HtJob = sgn::HtJob;
   using IdwtJob = sgn::IdwtJob;
+  using ClassicJob = sgn::ClassicJob;
+  using ClassicSeg = sgn::ClassicSeg;
   using PackJob = sgn::PackJob;
   using RoundInfo = ::RoundInfo;
   size_t n = 0;
@@ -173,6 +175,11 @@ struct sgn_plan {
   uint32_t* d_symbols = nullptr;
   HtJob* d_ht = nullptr;
   uint32_t* d_refine = nullptr;
+  // Classic (EBCOT) code blocks: jobs, segment table, per-thread flag scratch.
+  ClassicJob* d_classic = nullptr;
+  ClassicSeg* d_csegs = nullptr;
+  uint16_t* d_cscratch = nullptr;
+  uint32_t nclassic = 0, classic_ctas = 0, classic_slot = 0;
   IdwtJob* d_idwt = nullptr;
   PackJob* d_pack = nullptr;
   uint32_t* d_status = nullptr;
@@ -184,8 +191,8 @@ struct sgn_plan {
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
   // Launch shape and the device work-queue counters (one per queued launch:
-  // MagSgn, each IDWT round, pack, 9/7 pack), zeroed at the start of every
-  // execution.
+  // MagSgn, each IDWT round, pack, 9/7 pack, classic blocks), zeroed at the
+  // start of every execution.
   LaunchConfig cfg;
   uint32_t* d_queue = nullptr;
   uint32_t nqueues = 0;
@@ -226,6 +233,8 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& cfg);
 // IDWT round k (the 5/3 or the 9/7 kernel) and the pack launches, with the
 // plan's work-queue counters when `queued`, on persistent grids of `ctas`.
 cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas);
+// The classic (EBCOT) code-block kernel over the plan's classic jobs.
+cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s);
 cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas);
 // Workload signature for the autotuner cache: pixel format, job counts and
 // block shape classes.

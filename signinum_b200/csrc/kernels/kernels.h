@@ -43,6 +43,14 @@ cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nuni
 cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
                         uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
 cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm);
+// Classic (EBCOT Tier-1) code blocks: a persistent grid of `ctas` CTAs whose
+// threads each take blocks from the zeroed counter `queue` and decode them
+// with their own slot of `slot_words` 16-bit flag words in `scratch`
+// (ctas x classic_threads_per_cta() slots).
+cudaError_t launch_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t njobs, const uint8_t* arena,
+                           int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas, uint32_t* queue,
+                           cudaStream_t stream);
+uint32_t classic_threads_per_cta();
 // Irreversible (9/7) forms of the two launches above, same arguments; the
 // pack units of launch_pack97 run four warps per CTA.
 cudaError_t launch_idwt97_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,

@@ -136,10 +136,12 @@ def _pool():
 
 
 def _he_tile(widx: int, i: int, side: int, sigma: float, levels: int, cb_exp: int, keep: bool, blank=False,
-             lossy_step: float | None = None) -> Tile:
+             lossy_step: float | None = None, classic_style: int | None = None) -> Tile:
     seed = _mix(MASTER_SEED, widx, i)
     px = blank_rgb8(seed, side, side) if blank else he_rgb8(seed, side, side, sigma)
-    if lossy_step is None:
+    if classic_style is not None:
+        cs = encode_classic(px, side, side, 3, 8, style=classic_style, levels=levels, cb_exp=cb_exp)
+    elif lossy_step is None:
         cs = encode_lossless(px, side, side, 3, 8, levels=levels, cb_exp=cb_exp)
     else:
         cs = encode_irreversible(px, side, side, 3, 8, lossy_step, levels=levels, cb_exp=cb_exp)
@@ -164,6 +166,14 @@ def config1_irreversible(n=256, side=512, step=1 / 256, keep_pixels=False) -> Wo
     with _pool() as ex:
         tiles = list(ex.map(lambda i: _he_tile(5, i, side, 6.0, 5, 4, keep_pixels, lossy_step=step), range(n)))
     return Workload(f"c1i_rgb8_{n}x{side}x{side}_97", tiles)
+
+
+def config1_classic(n=256, side=512, style=0, keep_pixels=False) -> Workload:
+    """The uniform batch of config1 coded with classic (EBCOT) Tier-1 code
+    blocks (code-block style bits `style`), lossless 5/3, RCT."""
+    with _pool() as ex:
+        tiles = list(ex.map(lambda i: _he_tile(6, i, side, 6.0, 5, 4, keep_pixels, classic_style=style), range(n)))
+    return Workload(f"c1c_rgb8_{n}x{side}x{side}_ebcot", tiles)
 
 
 def config2(n=1024, keep_pixels=False) -> Workload:

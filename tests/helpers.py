@@ -83,3 +83,25 @@ def random_irreversible(rng, max_side=80):
                                     levels=int(rng.integers(0, 7)), cb_exp=cbw, cb_exp_h=cbh,
                                     use_mct=bool(rng.integers(0, 4)), progression=int(rng.choice([0, 1, 2, 3, 4])))
     return cs, px, w, h, comps, bd
+
+
+CLASSIC_STYLES = [0, 0x01, 0x02, 0x04, 0x08, 0x20, 0x05, 0x0D, 0x2F]
+
+
+def random_classic(rng, max_side=80):
+    """A seeded classic (EBCOT) codestream: random code-block style, lossless
+    5/3 or lossy 9/7."""
+    w = int(rng.integers(1, max_side))
+    h = int(rng.integers(1, max_side))
+    comps = int(rng.choice([1, 3]))
+    bd = int(rng.choice([8, 8, 12, 16])) if comps == 1 else int(rng.choice([8, 8, 8, 10]))
+    px = random_tile(rng, w, h, comps, bd, int(rng.integers(0, 3)))
+    cbw = int(rng.integers(0, 5))
+    cbh = min(int(rng.integers(0, 5)), 8 - cbw)
+    irr = bool(rng.integers(0, 2))
+    cs = encode.encode_classic(px.reshape(-1).view(np.uint8), w, h, comps, bd,
+                               style=int(rng.choice(CLASSIC_STYLES)), irreversible=irr,
+                               relative_step=float(rng.choice([1 / 64, 1 / 256, 1 / 1000])),
+                               levels=int(rng.integers(0, 7)), cb_exp=cbw, cb_exp_h=cbh,
+                               use_mct=bool(rng.integers(0, 4)), progression=int(rng.choice([0, 1, 2, 3, 4])))
+    return cs, px, w, h, comps, bd

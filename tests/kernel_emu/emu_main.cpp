@@ -32,6 +32,8 @@ void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t
 void emu_idwt(bool, const IdwtJob*, uint32_t, uint32_t);
 void emu_pack(bool, int, const PackJob*, uint32_t, uint32_t);
 int emu_pack_warps(bool);
+void emu_classic(const ClassicJob*, const ClassicSeg*, uint32_t, const uint8_t*, int32_t*, uint16_t*, uint32_t,
+                 uint32_t*);
 size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps);
 }
 extern "C" int oracle_decode(const uint8_t*, size_t, int, int, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
@@ -83,6 +85,54 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
   std::vector<uint8_t> arena((d.size() + 15) & ~(size_t)15, 0);
   std::memcpy(arena.data(), d.data(), d.size());
   std::vector<int32_t> coef(T.coef_per_comp * nc, 0x7F7F7F7F), ref(T.coef_per_comp * nc, 0);
+  std::vector<uint32_t> status(1, 0);
+  uint32_t n = 0, nr = 0;
+  if (T.classic) {
+    // Classic jobs (build_plan_impl, one tile): every block, zero ones too.
+    std::vector<ClassicJob> cj;
+    std::vector<ClassicSeg> cs;
+    for (const auto& sg : T.segments) cs.push_back(ClassicSeg{sg.len, sg.passes});
+    uint32_t slot = 1;
+    for (const CodeBlock& cb : T.blocks) {
+      const Band& b = T.bands[cb.band];
+      ClassicJob j;
+      std::memset(&j, 0, sizeof(j));
+      j.src = cb.cleanup_off;
+      j.dst = (uint64_t)b.comp * T.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
+      j.seg = cb.seg_begin;
+      j.stride = b.w;
+      j.w = cb.w;
+      j.h = cb.h;
+      j.nseg = cb.nseg;
+      j.passes = cb.passes;
+      j.bitplanes = (uint8_t)(b.nbp > cb.missing_msbs ? b.nbp - cb.missing_msbs : 0);
+      j.band_class = b.type == BAND_HL ? 1 : b.type == BAND_HH ? 2 : 0;
+      j.style = T.cbstyle;
+      cj.push_back(j);
+      if (cb.passes) slot = std::max<uint32_t>(slot, (uint32_t)(cb.w + 2) * (cb.h + 2));
+      // Oracle block decode of the same segments.
+      std::vector<size_t> seg_start{0};
+      std::vector<uint32_t> seg_pass{0};
+      for (uint32_t k = 0; k < cb.nseg; ++k) {
+        seg_start.push_back(seg_start.back() + T.segments[cb.seg_begin + k].len);
+        seg_pass.push_back(seg_pass.back() + T.segments[cb.seg_begin + k].passes);
+      }
+      std::vector<int32_t> blk((size_t)cb.w * cb.h, 0);
+      if (cb.passes)
+        oracle::classic_block_decode(d.data() + cb.cleanup_off, seg_start, seg_pass, cb.w, cb.h, cb.missing_msbs,
+                                     cb.passes, b.nbp, b.type, T.cbstyle, blk.data(), cb.w);
+      for (uint32_t y = 0; y < cb.h; ++y)
+        for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = blk[(size_t)y * cb.w + x];
+    }
+    n = (uint32_t)cj.size();
+    const uint32_t ctas = std::min<uint32_t>((n + 127) / 128, 2);
+    std::vector<uint16_t> scratch((size_t)std::max<uint32_t>(ctas, 1) * 128 * slot, 0xABCD);
+    std::vector<uint32_t> queue(1, 0);
+    if (n)
+      launch(ctas, 128, [&] {
+        emu_classic(cj.data(), cs.data(), n, arena.data(), coef.data(), scratch.data(), slot, queue.data());
+      });
+  } else {
   // HT jobs (runtime passes A/B for one tile).
   std::vector<HtJob> jobs;
   std::vector<uint32_t> refine;
@@ -132,16 +182,16 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
       for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = to_i32(buf[(size_t)y * cb.w + x], b.nbp);
   }
   std::vector<uint32_t> symbols(std::max<uint64_t>(sym, 1), 0xDEADBEEF);
-  std::vector<uint32_t> status(1, 0);
-  const uint32_t n = (uint32_t)jobs.size();
+  n = (uint32_t)jobs.size();
   launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols.data()); });
   const size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, 8);
   if (smem > sizeof(g_dyn_smem)) { printf("smem too large\n"); return 2; }
   launch((n + 7) / 8, 256, [&] {
     emu_magsgn(jobs.data(), n, arena.data(), symbols.data(), coef.data(), status.data(), ms_words, max_w);
   });
-  const uint32_t nr = (uint32_t)refine.size();
+  nr = (uint32_t)refine.size();
   if (nr) launch((nr + 63) / 64, 64, [&] { emu_refine(jobs.data(), refine.data(), nr, arena.data(), coef.data(), status.data()); });
+  }
   size_t cdiff = 0;
   for (size_t i = 0; i < coef.size(); ++i) cdiff += coef[i] != ref[i];
   // IDWT levels and pack (runtime plan for one tile, full image).
@@ -227,8 +277,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     size_t nd = 0, first = SIZE_MAX;
     for (size_t i = 0; i < (size_t)W * H * bpp; ++i)
       if (out[i] != want[i]) { ++nd; if (first == SIZE_MAX) first = i; }
-    printf("%ux%u nc %u bd %u L %u %s fmt %d blocks %u refine %u status %u: coef diffs %zu, pixel diffs %zu", W, H, nc,
-           T.bit_depth, L, irr ? "9/7" : "5/3", fmt, n, nr, status[0], cdiff, nd);
+    printf("%ux%u nc %u bd %u L %u %s %s fmt %d blocks %u refine %u status %u: coef diffs %zu, pixel diffs %zu", W,
+           H, nc, T.bit_depth, L, irr ? "9/7" : "5/3", T.classic ? "classic" : "HT", fmt, n, nr, status[0], cdiff, nd);
     if (nd) printf(" (first at %zu: got %u want %u)", first, out[first], want[first]);
     printf("\n");
     nd_total += nd;

@@ -23,6 +23,19 @@ void emu_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8
 }  // namespace sgn
 """
 
+CLASSIC_WRAPPERS = """
+namespace sgn {
+void emu_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t n, const uint8_t* arena, int32_t* coef,
+                 uint16_t* scratch, uint32_t slot, uint32_t* queue) {
+  QeTable qt;
+  for (int i = 0; i < 47; ++i)
+    qt.e[i] = ebcot::kQe[i] | ((uint32_t)ebcot::kNmps[i] << 16) | ((uint32_t)ebcot::kNlps[i] << 23) |
+              ((uint32_t)ebcot::kSwitch[i] << 30);
+  classic_kernel(jobs, segs, n, arena, coef, scratch, slot, queue, qt);
+}
+}  // namespace sgn
+"""
+
 IP_WRAPPERS = """
 namespace sgn {
 void emu_idwt(bool irr, const IdwtJob* jobs, uint32_t n, uint32_t units) {
@@ -73,6 +86,12 @@ def main(out_dir):
                                                                                    '#include "cuda_shim.h"')
     src = strip_functions(src, r"launch_\w+|idwt_pack_occupancy")
     (out / "idwt_pack_emu.cpp").write_text(src + IP_WRAPPERS)
+    src = (CSRC / "kernels" / "classic_decode.cu").read_text()
+    src = src.replace('#include "../device_plan.h"', inc("device_plan.h")).replace('#include "../ebcot.h"', inc("ebcot.h"))
+    src = src.replace('#include "kernels.h"', '#include "cuda_shim.h"')
+    src = strip_functions(src, r"launch_\w+")
+    src = re.sub(r"^uint32_t classic_threads_per_cta\(\) \{[^}]*\}", "", src, flags=re.M)
+    (out / "classic_emu.cpp").write_text(src + CLASSIC_WRAPPERS)
 
 
 if __name__ == "__main__":

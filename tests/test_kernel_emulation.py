@@ -1,6 +1,6 @@
 """The decode kernels' CUDA source run on CPU threads (tests/kernel_emu):
-every HT, IDWT and pack kernel on the golden fixtures and on seeded random
-reversible and irreversible codestreams, built with AddressSanitizer, and
+every HT, classic (EBCOT), IDWT and pack kernel on the golden fixtures and
+on seeded random reversible, irreversible and classic codestreams, built with AddressSanitizer, and
 compared with the oracle (coefficients per code block, then pixels, exact).
 Out-of-bounds accesses and parity breaks show up here without a GPU."""
 import json
@@ -12,7 +12,7 @@ import sys
 import numpy as np
 import pytest
 
-from tests.helpers import random_codestream, random_irreversible
+from tests.helpers import random_classic, random_codestream, random_irreversible
 
 EMU = pathlib.Path(__file__).parent / "kernel_emu"
 ROOT = EMU.parents[1]
@@ -27,7 +27,8 @@ def emu(tmp_path_factory):
     subprocess.run([sys.executable, str(EMU / "make_sources.py"), str(out)], check=True)
     flags = ["g++", "-std=c++20", "-O1", "-fsanitize=address", "-ffp-contract=off", f"-I{EMU}", f"-I{CSRC}",
              f"-I{ROOT / 'oracle'}"]
-    units = [out / "ht_decode_emu.cpp", out / "idwt_pack_emu.cpp", EMU / "emu_main.cpp", CSRC / "host" / "codestream.cpp",
+    units = [out / "ht_decode_emu.cpp", out / "idwt_pack_emu.cpp", out / "classic_emu.cpp", EMU / "emu_main.cpp",
+             CSRC / "host" / "codestream.cpp",
              ROOT / "oracle" / "oracle.cpp", ROOT / "oracle" / "oracle_ht.cpp", ROOT / "oracle" / "oracle_ebcot.cpp",
              ROOT / "oracle" / "oracle_capi.cpp"]
     procs = [subprocess.Popen(flags + ["-c", str(u), "-o", str(out / (u.stem + ".o"))]) for u in units]
@@ -53,10 +54,10 @@ def test_golden_fixtures_through_emulated_kernels(emu):
     run(emu, "03", [bytes.fromhex(f["j2k_hex"]) for f in fx.values()])
 
 
-@pytest.mark.parametrize("kind", ["reversible", "irreversible"])
+@pytest.mark.parametrize("kind", ["reversible", "irreversible", "classic"])
 def test_random_codestreams_through_emulated_kernels(emu, kind):
-    rng = np.random.default_rng(31 if kind == "reversible" else 97)
-    make = random_codestream if kind == "reversible" else random_irreversible
+    rng = np.random.default_rng({"reversible": 31, "irreversible": 97, "classic": 7}[kind])
+    make = {"reversible": random_codestream, "irreversible": random_irreversible, "classic": random_classic}[kind]
     by_comps = {1: [], 3: []}
     while len(by_comps[1]) < 4 or len(by_comps[3]) < 4:
         cs, _, _, _, comps, _ = make(rng, max_side=100)
