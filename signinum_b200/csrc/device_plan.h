@@ -86,9 +86,16 @@ struct ClassicSeg {
   uint32_t passes;  // coding passes
 };
 
-// Flag words per thread of the classic kernel: (w + 2) (h + 2) for the
-// largest code block (w h <= 4096, w, h <= 1024).
-constexpr uint32_t kClassicSlotMax = 6160;
+// 16-bit scratch words a classic block needs: blocks of at most 64 x 64
+// keep four 64-bit planes of rows -1 .. h+3 (69 rows); larger ones one flag
+// word per sample padded by one on every side.  A multiple of 4, so slots
+// stay 8-byte aligned.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline uint32_t classic_slot_words(uint32_t w, uint32_t h) {
+  return (w <= 64 && h <= 64) ? 4u * 69u * 4u : (((w + 2) * (h + 2) + 3) & ~3u);
+}
 
 // Irreversible (9/7) levels use the same tables: band pointers hold int32
 // coefficients that the kernel dequantises with `step`, level images (the

@@ -259,7 +259,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       t.ncls = (uint32_t)work[i].L->blocks.size();
       t.nseg = (uint32_t)work[i].L->segments.size();
       for (const CodeBlock& cb : work[i].L->blocks)
-        if (cb.passes) t.slot = std::max<uint32_t>(t.slot, (uint32_t)(cb.w + 2) * (cb.h + 2));
+        if (cb.passes) t.slot = std::max<uint32_t>(t.slot, classic_slot_words(cb.w, cb.h));
       return;
     }
     for (const CodeBlock& cb : work[i].L->blocks) {
@@ -431,7 +431,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   if (ncls) {
     plan->classic_slot = std::max<uint32_t>(cslot, 1);
     const uint32_t per = classic_threads_per_cta();
-    plan->classic_ctas = std::min<uint32_t>((ncls + per - 1) / per, (uint32_t)ctx->sm_count * 2);
+    // As many resident threads as the kernel's occupancy allows (every block
+    // a thread of its own where possible: the slowest block sets the time).
+    plan->classic_ctas = std::min<uint32_t>((ncls + per - 1) / per, (uint32_t)ctx->sm_count * classic_ctas_per_sm());
     if ((e = dalloc(&plan->d_classic, ncls, s)) != cudaSuccess) return cuda_status(e, "classic jobs");
     if ((e = dalloc(&plan->d_csegs, std::max<uint32_t>(ncseg, 1), s)) != cudaSuccess) return cuda_status(e, "classic segments");
     if ((e = dalloc(&plan->d_cscratch, (size_t)plan->classic_ctas * per * plan->classic_slot, s)) != cudaSuccess)

@@ -263,6 +263,186 @@ struct Block {
   }
 };
 
+// Blocks of at most 64 x 64 samples: per row four 64-bit planes (bit x =
+// column x) in the thread's scratch slot, rows -1 .. h+3 with zero padding:
+// significant, sign, refined, coded in this bit-plane.  A pass walks the
+// stripes; the six rows around a stripe live in registers while its columns
+// are scanned (the neighbour-significance byte of a sample is assembled from
+// three-bit windows of the rows above, at and below it), and the four rows
+// of the stripe go back at its end.  Magnitude and sign bits are OR-ed into
+// the coefficient words with reductions that nothing waits on.
+constexpr uint32_t kSmallRows = 64 + 5;
+static_assert(4 * kSmallRows * 4 == 1104, "small-block slot of classic_slot_words");
+
+struct Small {
+  uint64_t* P;  // sig, sgn, ref, cod planes of kSmallRows rows; row y at y + 1
+  uint32_t* out;
+  uint32_t w, h, stride, pos;
+  uint8_t band, style;
+  Tables* t;
+  int tid;
+  __device__ __forceinline__ uint8_t& cx(int label) { return t->cx[label][tid]; }
+  __device__ __forceinline__ uint64_t* plane(int k) { return P + k * kSmallRows; }
+  // Bits x-1, x, x+1 of a row (columns outside the block read 0).
+  __device__ static __forceinline__ uint32_t w3(uint64_t r, uint32_t x) {
+    return (uint32_t)(x ? (r >> (x - 1)) : (r << 1)) & 7u;
+  }
+  __device__ static __forceinline__ uint32_t bit_at(uint64_t r, uint32_t x) { return (uint32_t)(r >> x) & 1u; }
+  __device__ __forceinline__ void reset_contexts() {
+    for (int k = 0; k < 19; ++k) cx(k) = initial_index(k);
+  }
+
+  template <int KIND, typename D>
+  __device__ void pass(D& dec, bool raw) {
+    uint64_t* S = plane(0);
+    uint64_t* G = plane(1);
+    uint64_t* R = plane(2);
+    uint64_t* C = plane(3);
+    const bool vcausal = style & kVCausal;
+    for (uint32_t y0 = 0; y0 < h; y0 += 4) {
+      const uint32_t nr = min(4u, h - y0);
+      uint64_t s[6], g[6], c[4], r[4];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        s[k] = S[y0 + k];
+        g[k] = G[y0 + k];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        c[k] = C[y0 + 1 + k];
+        r[k] = R[y0 + 1 + k];
+      }
+      // Vertically causal: the stripe's last row ignores the row below it.
+      const bool cut = vcausal && y0 + 4 < h;
+      for (uint32_t x = 0; x < w; ++x) {
+        const uint64_t bx = 1ull << x;
+        auto nbr = [&](int k) -> uint32_t {
+          const uint32_t u = w3(s[k], x), m = w3(s[k + 1], x), d = (cut && k == 3) ? 0u : w3(s[k + 2], x);
+          return ((u & 1) << 7) | ((u & 2) << 5) | ((u & 4) << 3) | ((m & 1) << 4) | ((d & 1) << 3) | (m & 4) |
+                 ((d & 4) >> 1) | ((d & 2) >> 1);
+        };
+        auto sign = [&](int k, uint32_t n) {
+          const uint32_t sg = n & 0x55;
+          const uint32_t top = bit_at(g[k], x), left = x ? bit_at(g[k + 1], x - 1) : 0u;
+          const uint32_t right = x < 63 ? bit_at(g[k + 1], x + 1) : 0u;
+          const uint32_t bottom = (cut && k == 3) ? 0u : bit_at(g[k + 2], x);
+          const uint32_t signs = (top << 6) | (left << 4) | (right << 2) | bottom;
+          const uint8_t e = t->sc[(uint8_t)(((sg & signs) << 1) | (sg & ~signs))];
+          uint32_t b = dec.decode(cx(e & 0x7F), t->qe);
+          if (!raw) b ^= e >> 7;
+          return b;
+        };
+        uint32_t* col = out + (size_t)y0 * stride + x;
+        // A sample turning significant: its magnitude bit, sign, and state.
+        auto significant = [&](int k, uint32_t n) {
+          const uint32_t sb = sign(k, n);
+          atomicOr(col + (size_t)k * stride, (1u << pos) | (sb << 31));
+          s[k + 1] |= bx;
+          if (sb) g[k + 1] |= bx;
+        };
+        if (KIND == 0) {
+          int first = 0;
+          if (nr == 4) {
+            bool run = true;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) run = run && !((s[k + 1] | c[k]) & bx) && nbr(k) == 0;
+            if (run) {
+              if (dec.decode(cx(17), t->qe) == 0) continue;
+              uint32_t f = dec.decode(cx(18), t->qe) << 1;
+              f |= dec.decode(cx(18), t->qe);
+#pragma unroll
+              for (int k = 0; k < 4; ++k)
+                if ((uint32_t)k == f) significant(k, nbr(k));
+              first = (int)f + 1;
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (k < first || (uint32_t)k >= nr || ((s[k + 1] | c[k]) & bx)) continue;
+            const uint32_t n = nbr(k);
+            if (dec.decode(cx(t->zc[band][n]), t->qe)) significant(k, n);
+          }
+        } else if (KIND == 1) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if ((uint32_t)k >= nr || (s[k + 1] & bx)) continue;
+            const uint32_t n = nbr(k);
+            if (n == 0) continue;
+            c[k] |= bx;
+            if (dec.decode(cx(t->zc[band][n]), t->qe)) significant(k, n);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if ((uint32_t)k >= nr || !(s[k + 1] & bx) || (c[k] & bx)) continue;
+            const uint32_t b = dec.decode(cx(mr_context((r[k] & bx) != 0, nbr(k))), t->qe);
+            if (b) atomicOr(col + (size_t)k * stride, 1u << pos);
+            r[k] |= bx;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if ((uint32_t)k >= nr) continue;
+        S[y0 + 1 + k] = s[k + 1];
+        G[y0 + 1 + k] = g[k + 1];
+        R[y0 + 1 + k] = r[k];
+        C[y0 + 1 + k] = KIND == 0 ? 0ull : c[k];  // the cleanup pass ends the bit-plane
+      }
+    }
+  }
+
+  template <typename D>
+  __device__ void passes(uint32_t start, uint32_t end, uint32_t bitplanes, D& dec, bool raw) {
+    for (uint32_t p = start; p < end; ++p) {
+      pos = bitplanes - 1 - (p + 2) / 3;
+      const uint32_t kind = p % 3;
+      if (kind == 0) {
+        pass<0>(dec, raw);
+        if (style & kSegSym)
+          for (int k = 0; k < 4; ++k) dec.decode(cx(18), t->qe);
+      } else if (kind == 1) {
+        pass<1>(dec, raw);
+      } else {
+        pass<2>(dec, raw);
+      }
+      if (style & kReset) reset_contexts();
+    }
+  }
+};
+
+__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
+                               const uint8_t* __restrict__ arena, uint32_t* out, uint16_t* slot, Tables* t);
+
+template <typename B>
+__device__ __forceinline__ void run_passes(B& b, const ClassicJob& job, const ClassicSeg* __restrict__ segs,
+                                           const uint8_t* data) {
+  const uint32_t max_passes = 1 + 3 * ((uint32_t)job.bitplanes - 1);
+  if (!(job.style & (kBypass | kTermAll))) {
+    uint32_t total = 0;
+    for (uint32_t k = 0; k < job.nseg; ++k) total += segs[job.seg + k].len;
+    MqDec dec;
+    dec.init(data, total);
+    b.passes(0, min((uint32_t)job.passes, max_passes), job.bitplanes, dec, false);
+    return;
+  }
+  uint32_t start = 0, off = 0;
+  for (uint32_t k = 0; k < job.nseg; ++k) {
+    const ClassicSeg s = segs[job.seg + k];
+    const uint32_t end = min(start + s.passes, max_passes);
+    if (segment_is_arithmetic(job.style, start)) {
+      MqDec dec;
+      dec.init(data + off, s.len);
+      b.passes(start, end, job.bitplanes, dec, false);
+    } else {
+      RawDec dec{data + off, s.len, 0};
+      b.passes(start, end, job.bitplanes, dec, true);
+    }
+    start += s.passes;
+    off += s.len;
+  }
+}
+
 __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
                              const uint8_t* __restrict__ arena, int32_t* __restrict__ coef, uint16_t* slot, Tables* t) {
   const uint32_t w = job.w, h = job.h, stride = job.stride;
@@ -270,6 +450,37 @@ __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict
   for (uint32_t y = 0; y < h; ++y)
     for (uint32_t x = 0; x < w; ++x) out[(size_t)y * stride + x] = 0;
   if (job.passes == 0 || job.bitplanes == 0) return;
+  if (w <= 64 && h <= 64) {
+    Small b;
+    b.P = reinterpret_cast<uint64_t*>(slot);
+    b.out = out;
+    b.w = w;
+    b.h = h;
+    b.stride = stride;
+    b.pos = 0;
+    b.band = job.band_class;
+    b.style = job.style;
+    b.t = t;
+    b.tid = threadIdx.x;
+    for (uint32_t i = 0; i < 4 * kSmallRows; ++i) b.P[i] = 0;
+    b.reset_contexts();
+    run_passes(b, job, segs, arena + job.src);
+  } else {
+    decode_general(job, segs, arena, out, slot, t);
+  }
+  // The magnitude and sign bits arrived by reductions in L2: read them there.
+  for (uint32_t y = 0; y < h; ++y)
+    for (uint32_t x = 0; x < w; ++x) {
+      const uint32_t v = __ldcg(out + (size_t)y * stride + x);
+      const int32_t m = (int32_t)(v & 0x7FFFFFFFu);
+      out[(size_t)y * stride + x] = (uint32_t)((v >> 31) ? -m : m);
+    }
+}
+
+// Blocks wider or taller than 64: one 16-bit flag word per padded sample.
+__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
+                               const uint8_t* __restrict__ arena, uint32_t* out, uint16_t* slot, Tables* t) {
+  const uint32_t w = job.w, h = job.h, stride = job.stride;
   Block b;
   b.f = slot;
   b.out = out;
@@ -284,37 +495,7 @@ __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict
   b.tid = threadIdx.x;
   for (uint32_t i = 0; i < (w + 2) * (h + 2); ++i) slot[i] = 0;
   b.reset_contexts();
-  const uint32_t max_passes = 1 + 3 * ((uint32_t)job.bitplanes - 1);
-  const uint8_t* data = arena + job.src;
-  if (!(job.style & (kBypass | kTermAll))) {
-    uint32_t total = 0;
-    for (uint32_t k = 0; k < job.nseg; ++k) total += segs[job.seg + k].len;
-    MqDec dec;
-    dec.init(data, total);
-    b.passes(0, min((uint32_t)job.passes, max_passes), job.bitplanes, dec, false);
-  } else {
-    uint32_t start = 0, off = 0;
-    for (uint32_t k = 0; k < job.nseg; ++k) {
-      const ClassicSeg s = segs[job.seg + k];
-      const uint32_t end = min(start + s.passes, max_passes);
-      if (segment_is_arithmetic(job.style, start)) {
-        MqDec dec;
-        dec.init(data + off, s.len);
-        b.passes(start, end, job.bitplanes, dec, false);
-      } else {
-        RawDec dec{data + off, s.len, 0};
-        b.passes(start, end, job.bitplanes, dec, true);
-      }
-      start += s.passes;
-      off += s.len;
-    }
-  }
-  for (uint32_t y = 0; y < h; ++y)
-    for (uint32_t x = 0; x < w; ++x) {
-      const uint32_t v = out[(size_t)y * stride + x];
-      const int32_t m = (int32_t)(v & 0x7FFFFFFFu);
-      out[(size_t)y * stride + x] = (uint32_t)((v >> 31) ? -m : m);
-    }
+  run_passes(b, job, segs, arena + job.src);
 }
 
 }  // namespace
@@ -362,5 +543,12 @@ cudaError_t launch_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint3
 }
 
 uint32_t classic_threads_per_cta() { return kClassicThreads; }
+
+uint32_t classic_ctas_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, classic_kernel, kClassicThreads, 0) != cudaSuccess || n < 1)
+    n = 1;
+  return (uint32_t)n;
+}
 
 }  // namespace sgn

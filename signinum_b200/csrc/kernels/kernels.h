@@ -51,6 +51,7 @@ cudaError_t launch_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint3
                            int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas, uint32_t* queue,
                            cudaStream_t stream);
 uint32_t classic_threads_per_cta();
+uint32_t classic_ctas_per_sm();  // resident CTAs per SM of the classic kernel
 // Irreversible (9/7) forms of the two launches above, same arguments; the
 // pack units of launch_pack97 run four warps per CTA.
 cudaError_t launch_idwt97_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,

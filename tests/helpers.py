@@ -96,8 +96,8 @@ def random_classic(rng, max_side=80):
     comps = int(rng.choice([1, 3]))
     bd = int(rng.choice([8, 8, 12, 16])) if comps == 1 else int(rng.choice([8, 8, 8, 10]))
     px = random_tile(rng, w, h, comps, bd, int(rng.integers(0, 3)))
-    cbw = int(rng.integers(0, 5))
-    cbh = min(int(rng.integers(0, 5)), 8 - cbw)
+    cbw = int(rng.integers(0, 9))  # classic blocks up to 1024 wide (w h <= 4096)
+    cbh = min(int(rng.integers(0, 9)), 8 - cbw)
     irr = bool(rng.integers(0, 2))
     cs = encode.encode_classic(px.reshape(-1).view(np.uint8), w, h, comps, bd,
                                style=int(rng.choice(CLASSIC_STYLES)), irreversible=irr,

@@ -109,7 +109,7 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
       j.band_class = b.type == BAND_HL ? 1 : b.type == BAND_HH ? 2 : 0;
       j.style = T.cbstyle;
       cj.push_back(j);
-      if (cb.passes) slot = std::max<uint32_t>(slot, (uint32_t)(cb.w + 2) * (cb.h + 2));
+      if (cb.passes) slot = std::max<uint32_t>(slot, classic_slot_words(cb.w, cb.h));
       // Oracle block decode of the same segments.
       std::vector<size_t> seg_start{0};
       std::vector<uint32_t> seg_pass{0};

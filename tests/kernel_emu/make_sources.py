@@ -91,6 +91,7 @@ def main(out_dir):
     src = src.replace('#include "kernels.h"', '#include "cuda_shim.h"')
     src = strip_functions(src, r"launch_\w+")
     src = re.sub(r"^uint32_t classic_threads_per_cta\(\) \{[^}]*\}", "", src, flags=re.M)
+    src = src[:src.index("uint32_t classic_ctas_per_sm()")] + "}  // namespace sgn\n"
     (out / "classic_emu.cpp").write_text(src + CLASSIC_WRAPPERS)
 
 
