@@ -63,13 +63,14 @@ int sgn_j2k_encode_irreversible(const uint8_t* pixels, uint32_t width, uint32_t 
  * (0x01 arithmetic-coding bypass, 0x02 context reset, 0x04 termination on
  * every pass, 0x08 vertically causal context, 0x20 segmentation symbols);
  * irreversible selects the lossy mode of sgn_j2k_encode_irreversible with
- * relative_step, else the transform is lossless 5/3.  Like the irreversible
+ * relative_step, else the transform is lossless 5/3; layers (>= 1) quality
+ * layers split every block's coding passes evenly.  Like the irreversible
  * mode it has no counterpart in the reference's public encoder.  Returns as
  * sgn_j2k_encode_lossless. */
 int sgn_j2k_encode_classic(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
                            uint32_t bit_depth, const sgn_encode_options* options, uint32_t code_block_style,
-                           uint32_t irreversible, double relative_step, uint8_t* out, size_t out_cap,
-                           size_t* out_len);
+                           uint32_t irreversible, double relative_step, uint32_t layers, uint8_t* out,
+                           size_t out_cap, size_t* out_len);
 
 /* Seeded synthetic tiles (tight, interleaved). */
 void sgn_synth_he_rgb8(uint64_t seed, uint32_t width, uint32_t height, double noise_sigma, uint8_t* out);

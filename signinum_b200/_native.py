@@ -144,8 +144,8 @@ ENCODE_SIGNATURES = {
                                                    ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_j2k_encode_classic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                               ctypes.c_uint32, ctypes.POINTER(SgnEncodeOptions), ctypes.c_uint32,
-                                              ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t,
-                                              ctypes.POINTER(ctypes.c_size_t)]),
+                                              ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32, ctypes.c_void_p,
+                                              ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_synth_he_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p]),
     "sgn_synth_blank_rgb8": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),
     "sgn_synth_fluor_gray16": (None, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]),

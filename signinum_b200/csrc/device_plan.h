@@ -81,6 +81,10 @@ struct ClassicJob {
 };
 static_assert(sizeof(ClassicJob) == 40, "ClassicJob layout");
 
+// ClassicJob::src with this bit set: an offset in the plan's gather area
+// (multi-layer blocks, their parts copied back to back) instead of the input.
+constexpr uint64_t kClassicGathered = 1ull << 63;
+
 struct ClassicSeg {
   uint32_t len;     // bytes
   uint32_t passes;  // coding passes

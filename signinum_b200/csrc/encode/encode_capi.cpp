@@ -11,12 +11,15 @@ extern "C" {
 
 static int encode_with(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
                        uint32_t bit_depth, const sgn_encode_options* o, bool irreversible, double rel_step,
-                       uint8_t* out, size_t out_cap, size_t* out_len, bool classic = false, uint32_t style = 0) {
+                       uint8_t* out, size_t out_cap, size_t* out_len, bool classic = false, uint32_t style = 0,
+                       uint32_t layers = 1) {
   sgn::enc::EncodeParams p;
   p.irreversible = irreversible;
   p.rel_step = rel_step;
   p.classic = classic;
   p.cb_style = (uint8_t)(style & 0x2F);
+  p.layers = layers;
+  if (layers == 0 || layers > 64) return -2;
   p.width = width;
   p.height = height;
   p.comps = components;
@@ -56,10 +59,10 @@ int sgn_j2k_encode_irreversible(const uint8_t* pixels, uint32_t width, uint32_t 
 
 int sgn_j2k_encode_classic(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t components,
                            uint32_t bit_depth, const sgn_encode_options* o, uint32_t code_block_style,
-                           uint32_t irreversible, double relative_step, uint8_t* out, size_t out_cap,
-                           size_t* out_len) {
+                           uint32_t irreversible, double relative_step, uint32_t layers, uint8_t* out,
+                           size_t out_cap, size_t* out_len) {
   return encode_with(pixels, width, height, components, bit_depth, o, irreversible != 0, relative_step, out, out_cap,
-                     out_len, true, code_block_style);
+                     out_len, true, code_block_style, layers);
 }
 
 void sgn_synth_he_rgb8(uint64_t seed, uint32_t w, uint32_t h, double sigma, uint8_t* out) {

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "../ebcot.h"
@@ -638,86 +639,160 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   // Packets: one layer, one precinct per resolution.
   std::vector<uint8_t> tile;
   uint32_t sop_seq = 0;
-  auto packet = [&](uint32_t c, uint32_t r) {
+  // Quality layers (classic only): block passes are split evenly over the
+  // layers, the bytes of a codeword segment in proportion to its passes
+  // (a decoder joins a segment's parts from all layers back together).
+  const uint32_t NL = P.classic ? std::max<uint32_t>(P.layers, 1) : 1;
+  auto layer_first = [&](uint32_t np, uint32_t l) { return (uint32_t)((uint64_t)np * l / NL); };
+  struct Part {
+    uint32_t off, len, passes;
+  };
+  auto layer_parts = [&](const ClassicBlockOut& k, uint32_t l) {
+    std::vector<Part> parts;
+    const uint32_t a = layer_first(k.passes, l), z = layer_first(k.passes, l + 1);
+    uint32_t s0 = 0, o0 = 0;
+    for (size_t i = 0; i < k.seg_len.size(); ++i) {
+      const uint32_t s1 = s0 + k.seg_passes[i], len = k.seg_len[i];
+      const uint32_t pa = std::max(a, s0), pz = std::min(z, s1);
+      if (pa < pz) {
+        auto at = [&](uint32_t t) { return o0 + (uint32_t)((uint64_t)len * (t - s0) / (s1 - s0)); };
+        parts.push_back({at(pa), at(pz) - at(pa), pz - pa});
+      }
+      s0 = s1;
+      o0 += len;
+    }
+    return parts;
+  };
+  // Packet state that lasts over the layers: per band the inclusion (leaf:
+  // first layer with passes) and zero-bit-plane tag trees, per block whether
+  // it was included and its Lblock.
+  struct BandState {
+    std::unique_ptr<TagTree> ti, tz;
+    std::vector<uint8_t> included;
+    std::vector<uint32_t> lblock;
+  };
+  std::vector<std::vector<BandState>> bstate(C);
+  for (uint32_t c = 0; c < C; ++c)
+    for (Band& b : bands[c]) {
+      BandState st;
+      std::vector<uint32_t> incl(b.blocks.size()), zbp(b.blocks.size());
+      for (size_t i = 0; i < b.blocks.size(); ++i) {
+        const CodeBlockOut& cb = b.blocks[i];
+        uint32_t first = 0xFFFFu;  // never included
+        if (!cb.empty()) {
+          first = 0;
+          if (P.classic)
+            while (layer_first(cb.classic.passes, first + 1) == layer_first(cb.classic.passes, first)) ++first;
+        }
+        incl[i] = first;
+        // Empty leaves are never coded.
+        zbp[i] = cb.empty() ? 0xFFFFu : (P.classic ? cb.classic.zero_planes : b.mb - 1);
+      }
+      if (b.ncx && b.ncy) {
+        st.ti.reset(new TagTree(b.ncx, b.ncy, incl));
+        st.tz.reset(new TagTree(b.ncx, b.ncy, zbp));
+      }
+      st.included.assign(b.blocks.size(), 0);
+      st.lblock.assign(b.blocks.size(), 3);
+      bstate[c].push_back(std::move(st));
+    }
+  auto passes_in = [&](const CodeBlockOut& cb, uint32_t l) -> uint32_t {
+    if (cb.empty()) return 0;
+    if (!P.classic) return l == 0 ? 1 : 0;
+    return layer_first(cb.classic.passes, l + 1) - layer_first(cb.classic.passes, l);
+  };
+  auto packet = [&](uint32_t c, uint32_t r, uint32_t l) {
     size_t b0 = r == 0 ? 0 : 1 + (size_t)(r - 1) * 3, nb = r == 0 ? 1 : 3;
     bool any = false;
     for (size_t bi = b0; bi < b0 + nb; ++bi)
-      for (auto& cb : bands[c][bi].blocks) any = any || !cb.empty();
+      for (auto& cb : bands[c][bi].blocks) any = any || passes_in(cb, l) > 0;
     if (P.sop_eph) {
       tile.push_back(0xFF); tile.push_back(0x91);
       put16(tile, 4);
       put16(tile, sop_seq++ & 0xFFFF);
     }
     HeaderWriter hw;
+    std::vector<std::pair<const uint8_t*, uint32_t>> body;
     if (!any) {
       hw.bit(0);
     } else {
       hw.bit(1);
       for (size_t bi = b0; bi < b0 + nb; ++bi) {
         Band& b = bands[c][bi];
+        BandState& st = bstate[c][bi];
         if (b.ncx == 0 || b.ncy == 0) continue;
-        std::vector<uint32_t> incl(b.blocks.size()), zbp(b.blocks.size());
-        for (size_t i = 0; i < b.blocks.size(); ++i) {
-          const bool empty = b.blocks[i].empty();
-          incl[i] = empty ? 1 : 0;
-          // Empty leaves are never coded.
-          zbp[i] = empty ? 0xFFFFu : (P.classic ? b.blocks[i].classic.zero_planes : b.mb - 1);
-        }
-        TagTree ti(b.ncx, b.ncy, incl), tz(b.ncx, b.ncy, zbp);
         for (uint32_t y = 0; y < b.ncy; ++y)
           for (uint32_t x = 0; x < b.ncx; ++x) {
-            const auto& cb = b.blocks[(size_t)y * b.ncx + x];
-            ti.encode(x, y, 1, hw);
-            if (cb.empty()) continue;
-            tz.encode(x, y, UINT32_MAX, hw);
+            const size_t i = (size_t)y * b.ncx + x;
+            const auto& cb = b.blocks[i];
+            const uint32_t np = passes_in(cb, l);
+            if (!st.included[i]) {
+              st.ti->encode(x, y, l + 1, hw);
+              if (np == 0) continue;
+              st.tz->encode(x, y, UINT32_MAX, hw);
+              st.included[i] = 1;
+            } else {
+              hw.bit(np > 0 ? 1 : 0);
+              if (np == 0) continue;
+            }
             if (P.classic) {
               // Number of coding passes (Table B.4), Lblock increment, then
-              // one length per codeword segment of Lblock + floor(log2(passes))
-              // bits (B.10.6-B.10.7).
-              const ClassicBlockOut& k = cb.classic;
-              const uint32_t np = k.passes;
+              // one length per codeword segment part of Lblock +
+              // floor(log2(passes)) bits (B.10.6-B.10.7).
               if (np == 1) hw.bit(0);
               else if (np == 2) hw.bits(0x2, 2);
               else if (np <= 5) hw.bits(0xC | (np - 3), 4);
               else if (np <= 36) { hw.bits(0xF, 4); hw.bits(np - 6, 5); }
               else { hw.bits(0x1FF, 9); hw.bits(np - 37, 7); }
+              const std::vector<Part> parts = layer_parts(cb.classic, l);
               uint32_t inc = 0;
-              for (size_t sgi = 0; sgi < k.seg_len.size(); ++sgi) {
-                const uint32_t lg = bitlen(k.seg_passes[sgi]) - 1, need = bitlen(k.seg_len[sgi]);
-                if (need > 3 + lg) inc = std::max(inc, need - 3 - lg);
+              for (const Part& pt : parts) {
+                const uint32_t lg = bitlen(pt.passes) - 1, need = bitlen(pt.len);
+                if (need > st.lblock[i] + lg) inc = std::max(inc, need - st.lblock[i] - lg);
               }
-              for (uint32_t i = 0; i < inc; ++i) hw.bit(1);
+              for (uint32_t k = 0; k < inc; ++k) hw.bit(1);
               hw.bit(0);
-              for (size_t sgi = 0; sgi < k.seg_len.size(); ++sgi)
-                hw.bits(k.seg_len[sgi], 3 + inc + bitlen(k.seg_passes[sgi]) - 1);
+              st.lblock[i] += inc;
+              for (const Part& pt : parts) {
+                hw.bits(pt.len, st.lblock[i] + bitlen(pt.passes) - 1);
+                body.push_back({cb.classic.bytes.data() + pt.off, pt.len});
+              }
               continue;
             }
             hw.bit(0);  // one coding pass
             uint32_t len = (uint32_t)cb.bytes.size();
             uint32_t need = bitlen(len);
             uint32_t k = need > 3 ? need - 3 : 0;
-            for (uint32_t i = 0; i < k; ++i) hw.bit(1);
+            for (uint32_t n = 0; n < k; ++n) hw.bit(1);
             hw.bit(0);
             hw.bits(len, 3 + k);
+            body.push_back({cb.bytes.data(), len});
           }
       }
     }
     hw.flush();
     tile.insert(tile.end(), hw.buf.begin(), hw.buf.end());
     if (P.sop_eph) { tile.push_back(0xFF); tile.push_back(0x92); }
-    if (any)
-      for (size_t bi = b0; bi < b0 + nb; ++bi)
-        for (auto& cb : bands[c][bi].blocks) {
-          const std::vector<uint8_t>& bytes = P.classic ? cb.classic.bytes : cb.bytes;
-          tile.insert(tile.end(), bytes.begin(), bytes.end());
-        }
+    for (auto& part : body) tile.insert(tile.end(), part.first, part.first + part.second);
   };
-  if (P.progression == 3 || P.progression == 4) {
-    for (uint32_t c = 0; c < C; ++c)
-      for (uint32_t r = 0; r <= L; ++r) packet(c, r);
-  } else {
+  // Packet order (one precinct per resolution): LRCP l r c; RLCP r l c;
+  // RPCL r c l; PCRL and CPRL c r l.
+  if (P.progression == 0) {
+    for (uint32_t l = 0; l < NL; ++l)
+      for (uint32_t r = 0; r <= L; ++r)
+        for (uint32_t c = 0; c < C; ++c) packet(c, r, l);
+  } else if (P.progression == 1) {
     for (uint32_t r = 0; r <= L; ++r)
-      for (uint32_t c = 0; c < C; ++c) packet(c, r);
+      for (uint32_t l = 0; l < NL; ++l)
+        for (uint32_t c = 0; c < C; ++c) packet(c, r, l);
+  } else if (P.progression == 2) {
+    for (uint32_t r = 0; r <= L; ++r)
+      for (uint32_t c = 0; c < C; ++c)
+        for (uint32_t l = 0; l < NL; ++l) packet(c, r, l);
+  } else {
+    for (uint32_t c = 0; c < C; ++c)
+      for (uint32_t r = 0; r <= L; ++r)
+        for (uint32_t l = 0; l < NL; ++l) packet(c, r, l);
   }
   // Codestream.
   out.clear();
@@ -741,7 +816,7 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   put16(out, 12);
   out.push_back(P.sop_eph ? 0x06 : 0x00);
   out.push_back((uint8_t)P.progression);
-  put16(out, 1);
+  put16(out, NL);
   out.push_back(mct ? 1 : 0);
   out.push_back((uint8_t)L);
   out.push_back((uint8_t)P.cbw_exp);

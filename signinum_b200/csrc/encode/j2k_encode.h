@@ -21,6 +21,7 @@ struct EncodeParams {
   // (bypass 0x01, reset 0x02, termall 0x04, vcausal 0x08, segsym 0x20).
   bool classic = false;
   uint8_t cb_style = 0;
+  uint32_t layers = 1;  // quality layers (classic only)
 };
 // One classic code block: its codeword segments back to back, each
 // segment's length and coding-pass count, and the block's zero bit-planes.

@@ -316,9 +316,16 @@ struct BlockState {
   bool included = false;
   uint8_t missing = 0, passes = 0;
   uint32_t lblock = 3;
-  uint32_t lcup = 0, lref = 0;  // classic: lcup = bytes of all segments
+  uint32_t lcup = 0, lref = 0;
   int64_t cleanup_off = -1, ref_off = -1;
-  std::vector<ClassicSegment> segs;  // classic
+  // Classic: the codeword-segment parts of every layer in stream order
+  // (segment index, bytes, passes, offset in the codestream).
+  struct Part {
+    uint32_t idx, len, passes;
+    int64_t off;
+  };
+  std::vector<Part> parts;
+  uint32_t nonempty = 0;  // layers that contributed to the block
 };
 
 // Number of coding passes of a classic block (Table B.4,
@@ -354,8 +361,9 @@ bool classic_passes(Reader& r, uint32_t& np) {
   return true;
 }
 
-struct Packet {  // one (component, resolution, precinct)
+struct Packet {  // one (layer, component, resolution, precinct)
   uint8_t comp, res;
+  uint16_t layer;
   uint32_t precinct;
   uint32_t pb_begin, pb_count;
   uint64_t sort_py, sort_px;
@@ -495,9 +503,15 @@ void parse_tile(const uint8_t* data, size_t len, const uint32_t* target, TileLay
     if (c.colr != -1 && !((c.colr == 16 && T.ncomp == 3) || (c.colr == 17 && T.ncomp == 1)))
       fail(ST_UNSUPPORTED, "backend color space cannot be mapped to the requested pixel format");
   }
-  for (CodeBlock& cb : T.blocks) {
-    cb.cleanup_off += (uint32_t)c.off;
-    if (cb.passes > 1) cb.ref_off += (uint32_t)c.off;
+  // Offsets into the file rather than the codestream (gathered classic
+  // blocks address their gather area instead).
+  if (T.gathered) {
+    for (auto& op : T.gather) op.first += (uint32_t)c.off;
+  } else {
+    for (CodeBlock& cb : T.blocks) {
+      cb.cleanup_off += (uint32_t)c.off;
+      if (cb.passes > 1 && !T.classic) cb.ref_off += (uint32_t)c.off;
+    }
   }
 }
 
@@ -639,7 +653,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   }
   const bool classic = !(c0.cs.cbstyle & 0x40);
   if (h.layers > 1 && !classic) fail(ST_UNSUPPORTED, "multi-layer HTJ2K packet assembly");
-  if (h.layers > 1) fail(ST_UNSUPPORTED, "multi-layer classic codestreams are not supported by the CUDA path");
+  const uint32_t nlayers = h.layers;
   const uint32_t W = h.gw, H = h.gh, L = c0.cs.ndecomp;
   T = TileLayout();
   T.width = W;
@@ -652,6 +666,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   T.causal = (c0.cs.cbstyle & 0x08) != 0;
   T.classic = classic;
   T.cbstyle = c0.cs.cbstyle;
+  T.gathered = classic && nlayers > 1;
   uint32_t skipped = 0;
   if (target) {
     uint32_t wr = W / target[0], hr = H / target[1];
@@ -736,6 +751,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
           Packet pk;
           pk.comp = (uint8_t)c;
           pk.res = (uint8_t)res;
+          pk.layer = 0;
           pk.precinct = py * npx + px;
           pk.pb_begin = (uint32_t)pbs.size();
           pk.pb_count = nb;
@@ -777,19 +793,33 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     }
     T.coef_per_comp = off;
   }
-  // Packet order (progression.rs:114-338), one layer.
+  // Packet order (progression.rs:114-338): every (component, resolution,
+  // precinct) once per layer; LRCP and RLCP place the layer first and second,
+  // the position orders innermost.
+  if (nlayers > 1) {
+    const size_t n1 = packets.size();
+    for (uint32_t l = 1; l < nlayers; ++l)
+      for (size_t i = 0; i < n1; ++i) {
+        Packet pk = packets[i];
+        pk.layer = (uint16_t)l;
+        packets.push_back(pk);
+      }
+  }
   std::vector<uint32_t> order(packets.size());
   for (size_t i = 0; i < order.size(); ++i) order[i] = (uint32_t)i;
   auto key = [&](const Packet& p) {
+    const uint64_t l = p.layer;
     switch (h.prog) {
-      case 0: case 1:  // LRCP / RLCP with one layer: resolution, component, precinct
-        return std::make_tuple((uint64_t)p.res, (uint64_t)p.comp, (uint64_t)0, (uint64_t)0, (uint64_t)p.precinct);
+      case 0:  // LRCP: layer, resolution, component, precinct
+        return std::make_tuple(l, (uint64_t)p.res, (uint64_t)p.comp, (uint64_t)0, (uint64_t)p.precinct, (uint64_t)0);
+      case 1:  // RLCP: resolution, layer, component, precinct
+        return std::make_tuple((uint64_t)p.res, l, (uint64_t)p.comp, (uint64_t)0, (uint64_t)p.precinct, (uint64_t)0);
       case 2:  // RPCL
-        return std::make_tuple((uint64_t)p.res, p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.precinct);
+        return std::make_tuple((uint64_t)p.res, p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.precinct, l);
       case 3:  // PCRL
-        return std::make_tuple(p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.res, (uint64_t)p.precinct);
+        return std::make_tuple(p.sort_py, p.sort_px, (uint64_t)p.comp, (uint64_t)p.res, (uint64_t)p.precinct, l);
       default:  // CPRL
-        return std::make_tuple((uint64_t)p.comp, p.sort_py, p.sort_px, (uint64_t)p.res, (uint64_t)p.precinct);
+        return std::make_tuple((uint64_t)p.comp, p.sort_py, p.sort_px, (uint64_t)p.res, (uint64_t)p.precinct, l);
     }
   };
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key(packets[a]) < key(packets[b]); });
@@ -801,6 +831,8 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     while (ok && !pr.end()) {
       if (next_packet >= order.size()) { ok = false; break; }
       const Packet& pk = packets[order[next_packet++]];
+      // Classic blocks with parts in this packet: (block, first new part).
+      std::vector<std::pair<BlockState*, size_t>> fresh;
       const CodingStyle& cs = h.comps[pk.comp].cs;
       uint8_t mk;
       if ((cs.flags & 2) && pr.peek_marker(mk) && mk == 0x91) {
@@ -821,8 +853,9 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
               if (!pr.bits(1, v)) { ok = false; break; }
               inc = v == 1;
             } else {
-              if (!pb.incl.read(xi, yi, 1, pr, v)) { ok = false; break; }
-              inc = v == 0;
+              // Included in this layer when its first layer is at most pk.layer.
+              if (!pb.incl.read(xi, yi, (uint32_t)pk.layer + 1, pr, v)) { ok = false; break; }
+              inc = v <= pk.layer;
             }
             if (!inc) continue;
             if (first) {
@@ -830,13 +863,13 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
               bs.missing = (uint8_t)v;
             }
             bs.included = true;
-            if (!first || bs.passes != 0) { ok = false; break; }
             if (classic) {
-              // resolve_classic_segments (segment.rs:168-302), one layer:
-              // segments by pass (termination on every pass), by the bypass
-              // rule, or one for the block.
+              // resolve_classic_segments (segment.rs:168-302): this layer's
+              // passes continue the block's; a new part starts where the
+              // segment index changes (every pass with termination on each
+              // pass, the bypass rule, else one per contributing layer).
               uint32_t np, b, incr = 0;
-              if (!classic_passes(pr, np) || np > 1 + 3 * 31) { ok = false; break; }
+              if (!classic_passes(pr, np)) { ok = false; break; }
               for (;;) {
                 if (!pr.bits(1, b)) { ok = false; break; }
                 if (!b) break;
@@ -844,26 +877,35 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
               }
               if (!ok) break;
               bs.lblock += incr;
+              const uint32_t prev = bs.passes, cum = prev + np;
+              if (cum > 1 + 3 * 31) { ok = false; break; }
               const uint8_t st = cs.cbstyle;
               auto seg_of = [&](uint32_t p) -> uint32_t {
-                return (st & 0x04) ? p : (st & 0x01) ? (p < 10 ? 0 : 1 + 2 * ((p - 10) / 3) + ((p - 10) % 3 == 2)) : 0;
+                return (st & 0x04) ? p
+                       : (st & 0x01) ? (p < 10 ? 0 : 1 + 2 * ((p - 10) / 3) + ((p - 10) % 3 == 2))
+                                     : bs.nonempty;
               };
-              uint32_t total = 0, count = 0;
-              for (uint32_t p = 0; ok && p <= np; ++p) {
-                if (p == np || (p > 0 && seg_of(p) != seg_of(p - 1))) {
-                  uint32_t len, nbits = bs.lblock + (31 - (uint32_t)__builtin_clz(count));
-                  if (nbits > 32 || !pr.bits(nbits, len) || total + (uint64_t)len > 0x7FFFFFFF) { ok = false; break; }
-                  bs.segs.push_back({len, (uint8_t)count});
-                  total += len;
+              fresh.push_back({&bs, bs.parts.size()});
+              uint32_t last = seg_of(prev), count = 0;
+              for (uint32_t p = prev; ok && p <= cum; ++p) {
+                if (p == cum || seg_of(p) != last) {
+                  if (count) {
+                    uint32_t len, nbits = bs.lblock + (31 - (uint32_t)__builtin_clz(count));
+                    if (nbits > 32 || !pr.bits(nbits, len) || len > 0x7FFFFFFF) { ok = false; break; }
+                    bs.parts.push_back({last, len, count, -1});
+                  }
+                  if (p == cum) break;
+                  last = seg_of(p);
                   count = 0;
                 }
                 ++count;
               }
               if (!ok) break;
-              bs.passes = (uint8_t)np;
-              bs.lcup = total;
+              bs.passes = (uint8_t)cum;
+              ++bs.nonempty;
               continue;
             }
+            if (!first || bs.passes != 0) { ok = false; break; }
             uint32_t np = 1, b;
             if (!pr.bits(1, b)) { ok = false; break; }
             if (b) {
@@ -914,7 +956,13 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
       if (cs.flags & 4) {
         if (!pr.marker(mk) || mk != 0x92) { ok = false; break; }
       }
-      for (uint32_t k = 0; nz && ok && k < pk.pb_count; ++k) {
+      for (auto& f : fresh)
+        for (size_t k = f.second; ok && k < f.first->parts.size(); ++k) {
+          auto& part_k = f.first->parts[k];
+          part_k.off = (int64_t)(part.first + pr.pos());
+          if (!pr.skip(part_k.len)) ok = false;
+        }
+      for (uint32_t k = 0; nz && ok && !classic && k < pk.pb_count; ++k) {
         PrecinctBand& pb = pbs[pk.pb_begin + k];
         for (uint32_t i = 0; ok && i < pb.ncx * pb.ncy; ++i) {
           BlockState& bs = blocks[pb.first_block + i];
@@ -953,16 +1001,38 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     if (classic) {
       // Classic blocks keep every pass; the kernel decodes the first
       // 1 + 3 (bitplanes - 1) of them (reset_for_job, bitplane.rs:493-548).
+      // Parts of one segment index form one codeword segment (decode_inner,
+      // bitplane.rs:90-128).  With one layer a block's parts lie back to back
+      // in its packet; with several they are gathered into one run.
       if (nbp == 0 || bs.passes == 0 || actual == 0) {
         cb.passes = 0;
       } else {
-        if (bs.cleanup_off < 0) fail(ST_DECODE, "code-block decode failure: missing segment data");
-        cb.cleanup_off = (uint32_t)bs.cleanup_off;
-        cb.lcup = bs.lcup;
         cb.seg_begin = (uint32_t)T.segments.size();
-        cb.nseg = (uint8_t)bs.segs.size();
-        if (bs.segs.size() > 255) fail(ST_DECODE, "too many codeword segments");
-        T.segments.insert(T.segments.end(), bs.segs.begin(), bs.segs.end());
+        uint64_t total = 0;
+        for (size_t k = 0; k < bs.parts.size(); ++k) {
+          const auto& pt = bs.parts[k];
+          if (pt.off < 0) fail(ST_DECODE, "code-block decode failure: missing segment data");
+          if (k > 0 && pt.idx == bs.parts[k - 1].idx) {
+            T.segments.back().len += pt.len;
+            T.segments.back().passes = (uint8_t)(T.segments.back().passes + pt.passes);
+          } else {
+            T.segments.push_back({pt.len, (uint8_t)pt.passes});
+          }
+          total += pt.len;
+        }
+        if (T.segments.size() - cb.seg_begin > 255) fail(ST_DECODE, "too many codeword segments");
+        if (total > 0x7FFFFFFF) fail(ST_DECODE, "code-block data too long");
+        cb.nseg = (uint8_t)(T.segments.size() - cb.seg_begin);
+        cb.lcup = (uint32_t)total;
+        if (!T.gathered) {
+          cb.cleanup_off = bs.parts.empty() ? 0 : (uint32_t)bs.parts[0].off;
+        } else {
+          cb.cleanup_off = (uint32_t)T.gather_bytes;
+          for (const auto& pt : bs.parts) {
+            T.gather.push_back({(uint32_t)pt.off, pt.len});
+            T.gather_bytes += pt.len;
+          }
+        }
       }
       T.blocks.push_back(cb);
       continue;

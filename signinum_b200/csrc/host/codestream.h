@@ -71,6 +71,12 @@ struct TileLayout {
   bool classic = false;            // classic (EBCOT) Tier-1 code blocks instead of HT
   uint8_t cbstyle = 0;             // code-block style byte of COD/COC
   std::vector<ClassicSegment> segments;  // classic: per block, in block order
+  // Multi-layer classic: the blocks' parts (codestream offset, bytes) to copy
+  // back to back into a gather area; CodeBlock::cleanup_off is then an offset
+  // in that area (gather_bytes long) instead of the codestream.
+  bool gathered = false;
+  std::vector<std::pair<uint32_t, uint32_t>> gather;
+  uint64_t gather_bytes = 0;
   uint32_t skipped = 0;            // resolution levels dropped for a reduced decode
   uint32_t out_w = 0, out_h = 0;   // dimensions of the decoded (possibly reduced) image
   std::vector<Band> bands;         // per component: LL, then HL/LH/HH per resolution

@@ -249,6 +249,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     uint32_t nref = 0, ms_words = 8, max_w = 1;
     uint32_t hist[kLenBuckets];
     uint32_t ncls = 0, nseg = 0, slot = 0;  // classic tiles
+    uint64_t gather = 0;                    // multi-layer classic tiles
   };
   std::vector<TileHt> th(n);
   ctx->workers->parallel_for(n, [&](size_t i) {
@@ -258,6 +259,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (work[i].L->classic) {
       t.ncls = (uint32_t)work[i].L->blocks.size();
       t.nseg = (uint32_t)work[i].L->segments.size();
+      t.gather = work[i].L->gather_bytes;
       for (const CodeBlock& cb : work[i].L->blocks)
         if (cb.passes) t.slot = std::max<uint32_t>(t.slot, classic_slot_words(cb.w, cb.h));
       return;
@@ -281,8 +283,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   uint64_t sym_total = 0;
   uint32_t nht = 0, nref = 0, ms_words = 8, max_w = 1;
   std::vector<uint32_t> cls_off(n, 0), cseg_off(n, 0);
+  std::vector<uint64_t> gather_off(n, 0);
   uint32_t ncls = 0, ncseg = 0, cslot = 0;
+  uint64_t gather_total = 0;
   for (size_t i = 0; i < n; ++i) {
+    gather_off[i] = gather_total;
+    gather_total += (th[i].gather + 15) & ~(uint64_t)15;
     cls_off[i] = ncls;
     ncls += th[i].ncls;
     cseg_off[i] = ncseg;
@@ -438,6 +444,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if ((e = dalloc(&plan->d_csegs, std::max<uint32_t>(ncseg, 1), s)) != cudaSuccess) return cuda_status(e, "classic segments");
     if ((e = dalloc(&plan->d_cscratch, (size_t)plan->classic_ctas * per * plan->classic_slot, s)) != cudaSuccess)
       return cuda_status(e, "classic scratch");
+    if (gather_total && (e = dalloc(&plan->d_gather, gather_total, s)) != cudaSuccess)
+      return cuda_status(e, "classic gather area");
   }
   if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
   if ((e = dalloc(&plan->d_pack, packs.size(), s)) != cudaSuccess) return cuda_status(e, "pack jobs");
@@ -450,7 +458,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   const size_t at_pack = at_idwt + up16(idwt.size() * sizeof(IdwtJob));
   const size_t at_cls = at_pack + up16(packs.size() * sizeof(PackJob));
   const size_t at_cseg = at_cls + up16((size_t)ncls * sizeof(ClassicJob));
-  const size_t stage_bytes = at_cseg + up16((size_t)ncseg * sizeof(ClassicSeg));
+  const size_t at_gather = at_cseg + up16((size_t)ncseg * sizeof(ClassicSeg));
+  const size_t stage_bytes = at_gather + up16(gather_total);
   if ((e = staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
   uint8_t* st = staging.p;
   HtJob* ht = reinterpret_cast<HtJob*>(st + at_ht);
@@ -467,11 +476,16 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       ClassicJob* cj = reinterpret_cast<ClassicJob*>(st + at_cls) + cls_off[i];
       ClassicSeg* cs = reinterpret_cast<ClassicSeg*>(st + at_cseg) + cseg_off[i];
       for (size_t k = 0; k < L.segments.size(); ++k) cs[k] = ClassicSeg{L.segments[k].len, L.segments[k].passes};
+      uint8_t* g = st + at_gather + gather_off[i];
+      for (const auto& op : L.gather) {
+        std::memcpy(g, datas[i] + op.first, op.second);
+        g += op.second;
+      }
       for (const CodeBlock& cb : L.blocks) {
         const Band& b = L.bands[cb.band];
         ClassicJob& j = *cj++;
         std::memset(&j, 0, sizeof(j));
-        j.src = in_off[i] + cb.cleanup_off;
+        j.src = L.gathered ? (kClassicGathered | (gather_off[i] + cb.cleanup_off)) : in_off[i] + cb.cleanup_off;
         j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
         j.seg = cseg_off[i] + cb.seg_begin;
         j.tile = (uint32_t)i;
@@ -525,7 +539,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
              {plan->d_idwt, at_idwt, idwt.size() * sizeof(IdwtJob)},
              {plan->d_pack, at_pack, packs.size() * sizeof(PackJob)},
              {plan->d_classic, at_cls, (size_t)ncls * sizeof(ClassicJob)},
-             {plan->d_csegs, at_cseg, (size_t)ncseg * sizeof(ClassicSeg)}};
+             {plan->d_csegs, at_cseg, (size_t)ncseg * sizeof(ClassicSeg)},
+             {plan->d_gather, at_gather, (size_t)gather_total}};
   for (auto& u : ups) {
     if (!u.bytes) continue;
     if ((e = cudaMemcpyAsync(u.d, st + u.at, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
@@ -585,8 +600,8 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
 }
 
 cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s) {
-  return launch_classic(p->d_classic, p->d_csegs, p->nclassic, p->d_input, p->d_coef, p->d_cscratch, p->classic_slot,
-                        p->classic_ctas, p->d_queue + p->rounds.size() + 3, s);
+  return launch_classic(p->d_classic, p->d_csegs, p->nclassic, p->d_input, p->d_gather, p->d_coef, p->d_cscratch,
+                        p->classic_slot, p->classic_ctas, p->d_queue + p->rounds.size() + 3, s);
 }
 
 cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas) {
@@ -612,7 +627,8 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
   if (p->d_queue) cudaFreeAsync(p->d_queue, s);
   p->d_queue = nullptr;
   void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
-                  p->d_refine, p->d_idwt, p->d_pack, p->d_status, p->d_classic, p->d_csegs, p->d_cscratch};
+                  p->d_refine, p->d_idwt, p->d_pack, p->d_status, p->d_classic, p->d_csegs, p->d_cscratch,
+                  p->d_gather};
   for (void* q : ptrs)
     if (q) cudaFreeAsync(q, s);
   p->d_input = nullptr;
@@ -623,6 +639,7 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
   p->d_classic = nullptr;
   p->d_csegs = nullptr;
   p->d_cscratch = nullptr;
+  p->d_gather = nullptr;
   p->d_idwt = nullptr;
   p->d_pack = nullptr;
   p->d_status = nullptr;

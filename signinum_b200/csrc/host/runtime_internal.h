@@ -179,6 +179,7 @@ struct sgn_plan {
   ClassicJob* d_classic = nullptr;
   ClassicSeg* d_csegs = nullptr;
   uint16_t* d_cscratch = nullptr;
+  uint8_t* d_gather = nullptr;  // multi-layer classic blocks' data, gathered per block
   uint32_t nclassic = 0, classic_ctas = 0, classic_slot = 0;
   IdwtJob* d_idwt = nullptr;
   PackJob* d_pack = nullptr;

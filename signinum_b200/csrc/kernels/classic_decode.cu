@@ -411,8 +411,8 @@ struct Small {
   }
 };
 
-__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
-                               const uint8_t* __restrict__ arena, uint32_t* out, uint16_t* slot, Tables* t);
+__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs, const uint8_t* data,
+                               uint32_t* out, uint16_t* slot, Tables* t);
 
 template <typename B>
 __device__ __forceinline__ void run_passes(B& b, const ClassicJob& job, const ClassicSeg* __restrict__ segs,
@@ -444,8 +444,12 @@ __device__ __forceinline__ void run_passes(B& b, const ClassicJob& job, const Cl
 }
 
 __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
-                             const uint8_t* __restrict__ arena, int32_t* __restrict__ coef, uint16_t* slot, Tables* t) {
+                             const uint8_t* __restrict__ input, const uint8_t* __restrict__ gather,
+                             int32_t* __restrict__ coef, uint16_t* slot, Tables* t) {
   const uint32_t w = job.w, h = job.h, stride = job.stride;
+  // The block's segments, in the input or (multi-layer) in the gather area.
+  const uint8_t* data =
+      (job.src & kClassicGathered) ? gather + (job.src & ~kClassicGathered) : input + job.src;
   uint32_t* out = reinterpret_cast<uint32_t*>(coef + job.dst);
   for (uint32_t y = 0; y < h; ++y)
     for (uint32_t x = 0; x < w; ++x) out[(size_t)y * stride + x] = 0;
@@ -464,9 +468,9 @@ __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict
     b.tid = threadIdx.x;
     for (uint32_t i = 0; i < 4 * kSmallRows; ++i) b.P[i] = 0;
     b.reset_contexts();
-    run_passes(b, job, segs, arena + job.src);
+    run_passes(b, job, segs, data);
   } else {
-    decode_general(job, segs, arena, out, slot, t);
+    decode_general(job, segs, data, out, slot, t);
   }
   // The magnitude and sign bits arrived by reductions in L2: read them there.
   for (uint32_t y = 0; y < h; ++y)
@@ -478,8 +482,8 @@ __device__ void decode_block(const ClassicJob& job, const ClassicSeg* __restrict
 }
 
 // Blocks wider or taller than 64: one 16-bit flag word per padded sample.
-__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs,
-                               const uint8_t* __restrict__ arena, uint32_t* out, uint16_t* slot, Tables* t) {
+__device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restrict__ segs, const uint8_t* data,
+                               uint32_t* out, uint16_t* slot, Tables* t) {
   const uint32_t w = job.w, h = job.h, stride = job.stride;
   Block b;
   b.f = slot;
@@ -495,7 +499,7 @@ __device__ void decode_general(const ClassicJob& job, const ClassicSeg* __restri
   b.tid = threadIdx.x;
   for (uint32_t i = 0; i < (w + 2) * (h + 2); ++i) slot[i] = 0;
   b.reset_contexts();
-  run_passes(b, job, segs, arena + job.src);
+  run_passes(b, job, segs, data);
 }
 
 }  // namespace
@@ -509,6 +513,7 @@ struct QeTable {
 __global__ void __launch_bounds__(kClassicThreads) classic_kernel(const ClassicJob* __restrict__ jobs,
                                                                   const ClassicSeg* __restrict__ segs, uint32_t njobs,
                                                                   const uint8_t* __restrict__ arena,
+                                                                  const uint8_t* __restrict__ gather,
                                                                   int32_t* __restrict__ coef, uint16_t* scratch,
                                                                   uint32_t slot_words, uint32_t* queue, QeTable qt) {
   __shared__ Tables t;
@@ -526,19 +531,20 @@ __global__ void __launch_bounds__(kClassicThreads) classic_kernel(const ClassicJ
   for (;;) {
     const uint32_t j = atomicAdd(queue, 1u);
     if (j >= njobs) break;
-    decode_block(jobs[j], segs, arena, coef, slot, &t);
+    decode_block(jobs[j], segs, arena, gather, coef, slot, &t);
   }
 }
 
 cudaError_t launch_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t njobs, const uint8_t* arena,
-                           int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas, uint32_t* queue,
-                           cudaStream_t stream) {
+                           const uint8_t* gather, int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas,
+                           uint32_t* queue, cudaStream_t stream) {
   if (njobs == 0) return cudaSuccess;
   if (!scratch || !queue || ctas == 0) return cudaErrorInvalidValue;
   QeTable qt;
   for (int i = 0; i < 47; ++i)
     qt.e[i] = kQe[i] | ((uint32_t)kNmps[i] << 16) | ((uint32_t)kNlps[i] << 23) | ((uint32_t)kSwitch[i] << 30);
-  classic_kernel<<<ctas, kClassicThreads, 0, stream>>>(jobs, segs, njobs, arena, coef, scratch, slot_words, queue, qt);
+  classic_kernel<<<ctas, kClassicThreads, 0, stream>>>(jobs, segs, njobs, arena, gather, coef, scratch, slot_words,
+                                                       queue, qt);
   return cudaGetLastError();
 }
 

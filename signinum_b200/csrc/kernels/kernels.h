@@ -48,8 +48,8 @@ cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_c
 // with their own slot of `slot_words` 16-bit flag words in `scratch`
 // (ctas x classic_threads_per_cta() slots).
 cudaError_t launch_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t njobs, const uint8_t* arena,
-                           int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas, uint32_t* queue,
-                           cudaStream_t stream);
+                           const uint8_t* gather, int32_t* coef, uint16_t* scratch, uint32_t slot_words, uint32_t ctas,
+                           uint32_t* queue, cudaStream_t stream);
 uint32_t classic_threads_per_cta();
 uint32_t classic_ctas_per_sm();  // resident CTAs per SM of the classic kernel
 // Irreversible (9/7) forms of the two launches above, same arguments; the

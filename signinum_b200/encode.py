@@ -71,10 +71,10 @@ def encode_irreversible(pixels: np.ndarray, width: int, height: int, components:
 
 def encode_classic(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int, style: int = 0,
                    irreversible: bool = False, relative_step: float = 1.0 / 256, levels: int = 5, cb_exp: int = 4,
-                   use_mct: bool = True, progression: int = 0, cb_exp_h: int | None = None) -> bytes:
+                   use_mct: bool = True, progression: int = 0, cb_exp_h: int | None = None, layers: int = 1) -> bytes:
     """Classic (EBCOT Tier-1) codestream with code-block style bits `style`,
-    lossless 5/3 or (irreversible) lossy 9/7; same sample layout as
-    encode_lossless."""
+    lossless 5/3 or (irreversible) lossy 9/7, `layers` quality layers; same
+    sample layout as encode_lossless."""
     px = np.ascontiguousarray(pixels)
     opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression, 0, 0)
     cap = px.nbytes * 3 + 65536
@@ -82,7 +82,7 @@ def encode_classic(pixels: np.ndarray, width: int, height: int, components: int,
     n = ctypes.c_size_t()
     rc = _native.encode_lib().sgn_j2k_encode_classic(px.ctypes.data, width, height, components, bit_depth,
                                                      ctypes.byref(opts), style, int(irreversible), relative_step,
-                                                     out.ctypes.data, cap, ctypes.byref(n))
+                                                     layers, out.ctypes.data, cap, ctypes.byref(n))
     if rc != 0:
         raise ValueError(f"encode failed ({rc})")
     return out[: n.value].tobytes()

@@ -103,5 +103,6 @@ def random_classic(rng, max_side=80):
                                style=int(rng.choice(CLASSIC_STYLES)), irreversible=irr,
                                relative_step=float(rng.choice([1 / 64, 1 / 256, 1 / 1000])),
                                levels=int(rng.integers(0, 7)), cb_exp=cbw, cb_exp_h=cbh,
-                               use_mct=bool(rng.integers(0, 4)), progression=int(rng.choice([0, 1, 2, 3, 4])))
+                               use_mct=bool(rng.integers(0, 4)), progression=int(rng.choice([0, 1, 2, 3, 4])),
+                               layers=int(rng.choice([1, 1, 2, 3, 5])))
     return cs, px, w, h, comps, bd

@@ -32,8 +32,8 @@ void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t
 void emu_idwt(bool, const IdwtJob*, uint32_t, uint32_t);
 void emu_pack(bool, int, const PackJob*, uint32_t, uint32_t);
 int emu_pack_warps(bool);
-void emu_classic(const ClassicJob*, const ClassicSeg*, uint32_t, const uint8_t*, int32_t*, uint16_t*, uint32_t,
-                 uint32_t*);
+void emu_classic(const ClassicJob*, const ClassicSeg*, uint32_t, const uint8_t*, const uint8_t*, int32_t*, uint16_t*,
+                 uint32_t, uint32_t*);
 size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps);
 }
 extern "C" int oracle_decode(const uint8_t*, size_t, int, int, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
@@ -92,12 +92,16 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     std::vector<ClassicJob> cj;
     std::vector<ClassicSeg> cs;
     for (const auto& sg : T.segments) cs.push_back(ClassicSeg{sg.len, sg.passes});
+    // Multi-layer: the blocks' parts gathered back to back.
+    std::vector<uint8_t> gather;
+    for (const auto& op : T.gather) gather.insert(gather.end(), d.begin() + op.first, d.begin() + op.first + op.second);
+    gather.resize(((gather.size() + 15) & ~(size_t)15) + 16, 0);
     uint32_t slot = 1;
     for (const CodeBlock& cb : T.blocks) {
       const Band& b = T.bands[cb.band];
       ClassicJob j;
       std::memset(&j, 0, sizeof(j));
-      j.src = cb.cleanup_off;
+      j.src = T.gathered ? (kClassicGathered | cb.cleanup_off) : cb.cleanup_off;
       j.dst = (uint64_t)b.comp * T.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;
       j.seg = cb.seg_begin;
       j.stride = b.w;
@@ -119,8 +123,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
       }
       std::vector<int32_t> blk((size_t)cb.w * cb.h, 0);
       if (cb.passes)
-        oracle::classic_block_decode(d.data() + cb.cleanup_off, seg_start, seg_pass, cb.w, cb.h, cb.missing_msbs,
-                                     cb.passes, b.nbp, b.type, T.cbstyle, blk.data(), cb.w);
+        oracle::classic_block_decode((T.gathered ? gather.data() : d.data()) + cb.cleanup_off, seg_start, seg_pass,
+                                     cb.w, cb.h, cb.missing_msbs, cb.passes, b.nbp, b.type, T.cbstyle, blk.data(), cb.w);
       for (uint32_t y = 0; y < cb.h; ++y)
         for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = blk[(size_t)y * cb.w + x];
     }
@@ -130,7 +134,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     std::vector<uint32_t> queue(1, 0);
     if (n)
       launch(ctas, 128, [&] {
-        emu_classic(cj.data(), cs.data(), n, arena.data(), coef.data(), scratch.data(), slot, queue.data());
+        emu_classic(cj.data(), cs.data(), n, arena.data(), gather.data(), coef.data(), scratch.data(), slot,
+                    queue.data());
       });
   } else {
   // HT jobs (runtime passes A/B for one tile).

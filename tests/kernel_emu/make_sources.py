@@ -25,13 +25,13 @@ void emu_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8
 
 CLASSIC_WRAPPERS = """
 namespace sgn {
-void emu_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t n, const uint8_t* arena, int32_t* coef,
-                 uint16_t* scratch, uint32_t slot, uint32_t* queue) {
+void emu_classic(const ClassicJob* jobs, const ClassicSeg* segs, uint32_t n, const uint8_t* arena,
+                 const uint8_t* gather, int32_t* coef, uint16_t* scratch, uint32_t slot, uint32_t* queue) {
   QeTable qt;
   for (int i = 0; i < 47; ++i)
     qt.e[i] = ebcot::kQe[i] | ((uint32_t)ebcot::kNmps[i] << 16) | ((uint32_t)ebcot::kNlps[i] << 23) |
               ((uint32_t)ebcot::kSwitch[i] << 30);
-  classic_kernel(jobs, segs, n, arena, coef, scratch, slot, queue, qt);
+  classic_kernel(jobs, segs, n, arena, gather, coef, scratch, slot, queue, qt);
 }
 }  // namespace sgn
 """

@@ -58,6 +58,19 @@ def test_classic_round_trip_through_oracle(style):
         assert got == px.tobytes(), (style, w, h, c, bd)
 
 
+@pytest.mark.parametrize("layers", [2, 3, 5])
+def test_multi_layer_classic_round_trip_through_oracle(layers):
+    # Quality layers: a block's passes split over several packets, its
+    # codeword segments continued across them (segment.rs:168-302).
+    rng = np.random.default_rng(2000 + layers)
+    for style in (0, 0x01, 0x04, 0x05, 0x2F):
+        for prog in range(5):
+            px = rng.integers(0, 256, size=70 * 50 * 3).astype(np.uint8)
+            cs = encode.encode_classic(px, 70, 50, 3, 8, style=style, levels=3, cb_exp=3, progression=prog,
+                                       layers=layers)
+            assert oracle.decode(cs, 1)[0] == px.tobytes(), (style, prog)
+
+
 def test_lossy_classic_decodes_like_lossy_ht():
     # Same quantised coefficients, two block coders: the same pixels.
     px = encode.he_rgb8(7, 96, 80)

@@ -69,3 +69,15 @@ def test_batch_mixing_ht_and_classic_tiles():
         want, wd = cpu(cs, PixelFormat.Rgb8)
         assert s.dimensions() == wd
         assert s.to_bytes() == want
+
+
+@pytest.mark.parametrize("layers", [2, 5])
+def test_multi_layer_classic_tiles(layers):
+    # Quality layers: the host gathers each block's parts from all packets.
+    for style, prog in ((0, 0), (0x01, 1), (0x04, 2), (0x2F, 3), (0x05, 4)):
+        px = encode.he_rgb8(21 + style, 384, 256)
+        cs = encode.encode_classic(px, 384, 256, 3, 8, style=style, levels=4, progression=prog, layers=layers)
+        got, dims = gpu(cs, PixelFormat.Rgb8)
+        assert dims == (384, 256)
+        assert got == px.tobytes()
+        assert got == cpu(cs, PixelFormat.Rgb8)[0]
