@@ -172,6 +172,9 @@ bool is_pinned(const void* p) {
 // take blocks in.  Exact order inside a bucket does not matter.
 constexpr uint32_t kLenBuckets = 64;
 inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<uint32_t>(lcup >> 6, kLenBuckets - 1); }
+// Classic blocks by coding passes (0 .. 94), most passes first.
+constexpr uint32_t kPassBuckets = 96;
+inline uint32_t pass_bucket(uint32_t passes) { return kPassBuckets - 1 - std::min<uint32_t>(passes, kPassBuckets - 1); }
 
 sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const uint8_t* const* datas,
                            const size_t* lens, size_t n, uint32_t fmt, const sgn_request* reqs, sgn_plan* plan,
@@ -250,18 +253,22 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     uint32_t hist[kLenBuckets];
     uint32_t ncls = 0, nseg = 0, slot = 0;  // classic tiles
     uint64_t gather = 0;                    // multi-layer classic tiles
+    uint32_t chist[kPassBuckets];           // classic blocks per coding-pass count
   };
   std::vector<TileHt> th(n);
   ctx->workers->parallel_for(n, [&](size_t i) {
     TileHt& t = th[i];
     std::fill(t.hist, t.hist + kLenBuckets, 0u);
+    std::fill(t.chist, t.chist + kPassBuckets, 0u);
     if (plan->status[i] != SGN_OK) return;
     if (work[i].L->classic) {
       t.ncls = (uint32_t)work[i].L->blocks.size();
       t.nseg = (uint32_t)work[i].L->segments.size();
       t.gather = work[i].L->gather_bytes;
-      for (const CodeBlock& cb : work[i].L->blocks)
+      for (const CodeBlock& cb : work[i].L->blocks) {
+        ++t.chist[pass_bucket(cb.passes)];
         if (cb.passes) t.slot = std::max<uint32_t>(t.slot, classic_slot_words(cb.w, cb.h));
+      }
       return;
     }
     for (const CodeBlock& cb : work[i].L->blocks) {
@@ -282,19 +289,25 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   std::vector<uint32_t> ref_off(n, 0), start((size_t)kLenBuckets * n, 0);
   uint64_t sym_total = 0;
   uint32_t nht = 0, nref = 0, ms_words = 8, max_w = 1;
-  std::vector<uint32_t> cls_off(n, 0), cseg_off(n, 0);
+  // Classic jobs: bucket-major by coding passes (most first), tile-minor, so
+  // that the lanes of a warp take blocks of similar work and the longest
+  // blocks start first.
+  std::vector<uint32_t> cseg_off(n, 0), cstart((size_t)kPassBuckets * n, 0);
   std::vector<uint64_t> gather_off(n, 0);
   uint32_t ncls = 0, ncseg = 0, cslot = 0;
   uint64_t gather_total = 0;
   for (size_t i = 0; i < n; ++i) {
     gather_off[i] = gather_total;
     gather_total += (th[i].gather + 15) & ~(uint64_t)15;
-    cls_off[i] = ncls;
-    ncls += th[i].ncls;
     cseg_off[i] = ncseg;
     ncseg += th[i].nseg;
     cslot = std::max(cslot, th[i].slot);
   }
+  for (uint32_t b = 0; b < kPassBuckets; ++b)
+    for (size_t i = 0; i < n; ++i) {
+      cstart[(size_t)b * n + i] = ncls;
+      ncls += th[i].chist[b];
+    }
   for (size_t i = 0; i < n; ++i) {
     sym_off[i] = sym_total;
     sym_total += th[i].sym;
@@ -473,7 +486,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (L.classic) {
       // Classic blocks: one job each (all-zero blocks too, so that every
       // block's samples are written), segments after the tile's offset.
-      ClassicJob* cj = reinterpret_cast<ClassicJob*>(st + at_cls) + cls_off[i];
+      ClassicJob* cjobs = reinterpret_cast<ClassicJob*>(st + at_cls);
+      uint32_t ccur[kPassBuckets];
+      for (uint32_t b = 0; b < kPassBuckets; ++b) ccur[b] = cstart[(size_t)b * n + i];
       ClassicSeg* cs = reinterpret_cast<ClassicSeg*>(st + at_cseg) + cseg_off[i];
       for (size_t k = 0; k < L.segments.size(); ++k) cs[k] = ClassicSeg{L.segments[k].len, L.segments[k].passes};
       uint8_t* g = st + at_gather + gather_off[i];
@@ -483,7 +498,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       }
       for (const CodeBlock& cb : L.blocks) {
         const Band& b = L.bands[cb.band];
-        ClassicJob& j = *cj++;
+        ClassicJob& j = cjobs[ccur[pass_bucket(cb.passes)]++];
         std::memset(&j, 0, sizeof(j));
         j.src = L.gathered ? (kClassicGathered | (gather_off[i] + cb.cleanup_off)) : in_off[i] + cb.cleanup_off;
         j.dst = coef_off[i] + (uint64_t)b.comp * L.coef_per_comp + b.coef_off + (uint64_t)cb.y0 * b.w + cb.x0;

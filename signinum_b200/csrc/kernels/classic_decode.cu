@@ -96,12 +96,15 @@ struct MqDec {
         cx = (uint8_t)(((e >> 23) & 0x7F) | ((mps ^ ((e >> 30) & 1)) << 7));
       }
     }
-    do {
+    // RENORMD (C.3.3), shifting as many bits at once as A needs and the
+    // byte buffer holds (as the reference's renormalize does).
+    while ((a & 0x8000) == 0) {
       if (ct == 0) bytein();
-      a <<= 1;
-      c <<= 1;
-      --ct;
-    } while ((a & 0x8000) == 0);
+      const uint32_t sh = min((uint32_t)__clz(a) - 16, ct);
+      a <<= sh;
+      c <<= sh;
+      ct -= sh;
+    }
     return dbit;
   }
 };
