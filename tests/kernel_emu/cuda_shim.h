@@ -88,6 +88,7 @@ inline unsigned __funnelshift_lc(unsigned lo, unsigned hi, unsigned sh) {
 }
 inline int __clz(unsigned v) { return v ? __builtin_clz(v) : 32; }
 inline int __ffs(unsigned v) { return v ? __builtin_ctz(v) + 1 : 0; }
+inline int __ffsll(long long v) { return v ? __builtin_ctzll((unsigned long long)v) + 1 : 0; }
 inline unsigned __byte_perm(unsigned x, unsigned y, unsigned s) {
   uint8_t b[8];
   for (int i = 0; i < 4; ++i) { b[i] = (uint8_t)(x >> (8 * i)); b[4 + i] = (uint8_t)(y >> (8 * i)); }
