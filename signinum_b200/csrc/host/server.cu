@@ -35,6 +35,7 @@ struct ResidentTile {
   std::vector<uint8_t> host;  // for header parsing
   uint64_t offset = 0;        // in the device arena (16-byte aligned)
   uint32_t width = 0, height = 0, ncomp = 0;
+  bool classic = false;  // classic (EBCOT) code blocks: per-thread scratch instead of quad symbols
   // Packet-header parse per resolution (downscale 1, 2, 4, 8), made by the
   // dispatcher the first time a request needs it and reused afterwards.
   std::unique_ptr<TileLayout> layout[4];
@@ -76,7 +77,10 @@ struct Slot {
 
 // Device bytes one request needs while its batch is in flight: coefficient
 // arena, level buffers and quad symbols of the decoded resolution, the output
-// surface and the job tables (about 48 bytes per code block).
+// surface and the job tables (about 48 bytes per code block).  Classic tiles
+// need no quad symbols but per-thread flag scratch (at most (w+2)(h+2) 16-bit
+// words per block) and, with several layers, a gathered copy of their data:
+// 3 bytes per sample covers both.
 uint64_t estimate_bytes(const ResidentTile& t, uint32_t format, const sgn_request& r) {
   const uint64_t d = (r.kind == SGN_REQ_SCALED || r.kind == SGN_REQ_REGION_SCALED) ? std::max(1u, r.downscale) : 1;
   const uint64_t w = (t.width + d - 1) / d, h = (t.height + d - 1) / d;
@@ -86,7 +90,8 @@ uint64_t estimate_bytes(const ResidentTile& t, uint32_t format, const sgn_reques
     out_w = (r.w + d - 1) / d + 1;
     out_h = (r.h + d - 1) / d + 1;
   }
-  const uint64_t coef = samples * 4, levels = samples * 2, symbols = samples, jobs = samples / 64 + 4096;
+  const uint64_t coef = samples * 4, levels = samples * 2, symbols = samples * (t.classic ? 3 : 1),
+                 jobs = samples / 64 + 4096;
   return coef + levels + symbols + jobs + out_w * out_h * bytes_per_pixel(format) + 4096;
 }
 
@@ -331,6 +336,7 @@ sgn_status sgn_server_register(sgn_server* sv, const uint8_t* data, size_t len, 
     t->width = info.width;
     t->height = info.height;
     t->ncomp = info.components;
+    t->classic = !info.ht;
   } catch (const ParseError& pe) {
     return set_error(pe.status, pe.message.c_str());
   }

@@ -113,3 +113,24 @@ def test_submit_validation(pool):
         assert e.value.is_unsupported()
         with pytest.raises(Error):
             server.submit(tid + 5, PixelFormat.Rgb8)
+
+
+def test_serving_mixes_ht_lossy_and_classic_tiles():
+    # The serving loop batches whatever is registered: HT lossless, lossy 9/7
+    # and classic (multi-layer) tiles side by side, each exact.
+    px = [encode.he_rgb8(40 + k, 256, 192) for k in range(3)]
+    tiles = [encode.encode_lossless(px[0], 256, 192, 3, 8, levels=4),
+             encode.encode_irreversible(px[1], 256, 192, 3, 8, 1 / 256, levels=4),
+             encode.encode_classic(px[2], 256, 192, 3, 8, style=0x05, levels=4, layers=3)]
+
+    class T:
+        def __init__(self, cs):
+            self.codestream, self.width, self.height = cs, 256, 192
+
+    pool = [T(cs) for cs in tiles]
+    with Server(max_batch_tiles=8, slots=2) as server:
+        ids = [server.register(t.codestream) for t in pool]
+        reqs = [(i, None, None) for i in range(3)] * 3 + [(2, Rect(32, 16, 128, 96), None), (1, None, Downscale.Half)]
+        for (i, roi, scale), (b, dims, _) in zip(reqs, _run(server, ids, reqs)):
+            want, w, h = _oracle(pool[i], roi, scale)
+            assert dims == (w, h) and b == want
