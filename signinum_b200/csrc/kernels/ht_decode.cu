@@ -708,9 +708,14 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
   }
   if (ok) {
     const uint32_t ms_len = lcup - scup;
-    unstuff_magsgn(src, ms_len, W, ms_words);
-    const bool bad = job.w <= 64 ? magsgn_rows<true>(job, W, ms_words, Ebase, cols, sym, dst)
-                                 : magsgn_rows<false>(job, W, ms_words, Ebase, cols, sym, dst);
+    // The block's own words of the bit array (at most ms_words, checked
+    // above): they are zeroed, filled and padded with ones past the stream,
+    // and reads beyond them return ones, so bits past the end still read as
+    // the reference's 0xFF padding.
+    const uint32_t words = (ms_len + 15) / 4 + 2;
+    unstuff_magsgn(src, ms_len, W, words);
+    const bool bad = job.w <= 64 ? magsgn_rows<true>(job, W, words, Ebase, cols, sym, dst)
+                                 : magsgn_rows<false>(job, W, words, Ebase, cols, sym, dst);
     ok = !bad;
   }
   if (!ok) {
