@@ -120,6 +120,16 @@ struct IdwtJob {
 
 enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
 
+// Kernel variant of a reversible tile's pack job: 0 RGB with samples that
+// convert by a clamp alone (8-bit samples to 8-bit formats, deeper ones to
+// 16-bit formats), 1 RGB rescaled, 2 gray by a clamp, 3 gray rescaled.
+constexpr uint32_t kPackVariants = 4;
+inline uint32_t pack_variant(uint32_t fmt, uint32_t ncomp, uint32_t bit_depth) {
+  const bool u8 = fmt == PACK_GRAY8 || fmt == PACK_RGB8 || fmt == PACK_RGBA8;
+  const bool direct = u8 ? bit_depth == 8 : bit_depth > 8;
+  return (ncomp >= 3 ? 0u : 2u) + (direct ? 0u : 1u);
+}
+
 struct PackJob {
   const int32_t* ll[3];
   const int32_t* hl[3];

@@ -334,7 +334,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // Rounds 0 .. max_rounds-1 hold 5/3 levels, the next max_rounds the 9/7
   // levels (each round is one launch of the kernel of its transform).
   std::vector<std::vector<IdwtJob>> rounds(2 * (size_t)max_rounds);
-  std::vector<PackJob> packs, packs97;
+  std::vector<PackJob> packs_v[kPackVariants], packs97;
   auto band_ptr = [&](size_t i, uint32_t c, uint32_t bi) -> int32_t* {
     const TileLayout& L = *work[i].L;
     return plan->d_coef + coef_off[i] + (uint64_t)c * L.coef_per_comp + L.bands[bi].coef_off;
@@ -423,11 +423,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     pj.seg = idwt_segment_rows(tw.crop_h) * (L.reversible ? 1 : 2);
     pj.ll_band = R <= 1 ? 1 : 0;
     uint32_t segs = (tw.crop_y + tw.crop_h - ay + pj.seg - 1) / pj.seg;
-    uint32_t& units = L.reversible ? plan->pack_ctas : plan->pack97_ctas;
+    const uint32_t v = pack_variant(fmt, L.ncomp, L.bit_depth);
+    uint32_t& units = L.reversible ? plan->pack_units_v[v] : plan->pack97_ctas;
     pj.unit_begin = units;
     pj.tile = (uint32_t)i;
     units += pj.strips * segs;
-    (L.reversible ? packs : packs97).push_back(pj);
+    (L.reversible ? packs_v[v] : packs97).push_back(pj);
   }
   // Flatten the rounds.
   std::vector<IdwtJob> idwt;
@@ -440,6 +441,13 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       idwt.push_back(j);
     }
     if (ri.njobs) plan->rounds.push_back(ri);
+  }
+  std::vector<PackJob> packs;
+  for (uint32_t v = 0; v < kPackVariants; ++v) {
+    plan->pack_begin[v] = (uint32_t)packs.size();
+    plan->npack_v[v] = (uint32_t)packs_v[v].size();
+    plan->pack_ctas += plan->pack_units_v[v];
+    packs.insert(packs.end(), packs_v[v].begin(), packs_v[v].end());
   }
   plan->npack = (uint32_t)packs.size();
   plan->npack97 = (uint32_t)packs97.size();
@@ -565,11 +573,12 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // (callers that reuse it only after the plan has run pass sync_uploads false).
   if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
   plan->launches = (plan->nht ? 2 : 0) + (plan->nref ? 1 : 0) + (plan->nclassic ? 1 : 0) + plan->rounds.size() +
-                   (plan->npack ? 1 : 0) + (plan->npack97 ? 1 : 0);
+                   (plan->npack97 ? 1 : 0);
+  for (uint32_t v = 0; v < kPackVariants; ++v) plan->launches += plan->npack_v[v] ? 1 : 0;
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
   // Work-queue counters and the launch shape (an autotuned one when this
   // context has tuned a plan of the same signature).
-  plan->nqueues = (uint32_t)plan->rounds.size() + 4;
+  plan->nqueues = (uint32_t)plan->rounds.size() + 3 + kPackVariants;
   if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
   LaunchConfig cfg;
   {
@@ -616,7 +625,7 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
 
 cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s) {
   return launch_classic(p->d_classic, p->d_csegs, p->nclassic, p->d_input, p->d_gather, p->d_coef, p->d_cscratch,
-                        p->classic_slot, p->classic_ctas, p->d_queue + p->rounds.size() + 3, s);
+                        p->classic_slot, p->classic_ctas, p->d_queue + p->rounds.size() + 2 + kPackVariants, s);
 }
 
 cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas) {
@@ -627,10 +636,15 @@ cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queue
 }
 
 cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas) {
+  // Counters: one per reversible variant, then the 9/7 pack.
   uint32_t* q = queued ? p->d_queue + 1 + p->rounds.size() : nullptr;
-  cudaError_t e = launch_pack(p->d_pack, p->npack, p->pack_ctas, p->format, s, q, ctas);
+  cudaError_t e = cudaSuccess;
+  for (uint32_t v = 0; v < kPackVariants && e == cudaSuccess; ++v)
+    e = launch_pack(p->d_pack + p->pack_begin[v], p->npack_v[v], p->pack_units_v[v], p->format, v, s,
+                    q ? q + v : nullptr, ctas);
   if (e == cudaSuccess)
-    e = launch_pack97(p->d_pack + p->npack, p->npack97, p->pack97_ctas, p->format, s, q ? q + 1 : nullptr, ctas);
+    e = launch_pack97(p->d_pack + p->npack, p->npack97, p->pack97_ctas, p->format, s,
+                      q ? q + kPackVariants : nullptr, ctas);
   return e;
 }
 
@@ -1168,21 +1182,24 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
   std::lock_guard<std::mutex> g(ctx->mu);
   cudaSetDevice(ctx->device);
   ctx->submissions.fetch_add(1);
-  // Pipelined: large batches are cut into up to four chunks of about equal
-  // coded bytes, each a plan on its own stream with its own staging, built
-  // and launched in turn, so the upload of chunk c overlaps the kernels of
-  // chunk c - 1 and the host parse of chunk c + 1.
+  // Pipelined: large batches are cut into up to four chunks by coded bytes,
+  // each a plan on its own stream with its own staging, built and launched
+  // in turn, so the upload of chunk c overlaps the kernels of chunk c - 1 and
+  // the host parse of chunk c + 1.  The last chunk carries half the bytes of
+  // each of the others: only its kernels run after the last upload.
   uint64_t total = 0;
   for (size_t i = 0; i < n; ++i) total += lens[i];
   const size_t K = std::min<size_t>(total >= (48ull << 20) ? 4 : total >= (12ull << 20) ? 2 : 1, std::max<size_t>(1, n / 2));
   std::vector<size_t> cut(K + 1, n);
   cut[0] = 0;
   {
+    // Chunk c < K - 1 ends at 2c / (2K - 1) of the bytes (weights 2, .., 2, 1).
     uint64_t acc = 0;
     size_t c = 1;
+    const uint64_t parts = K > 1 ? 2 * K - 1 : 1;
     for (size_t i = 0; i < n && c < K; ++i) {
       acc += lens[i];
-      if (acc * K >= total * c) cut[c++] = i + 1;
+      if (acc * parts >= total * 2 * c) cut[c++] = i + 1;
     }
   }
   std::vector<sgn_plan*> plans(K, nullptr);

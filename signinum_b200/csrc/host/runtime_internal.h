@@ -185,15 +185,20 @@ struct sgn_plan {
   PackJob* d_pack = nullptr;
   uint32_t* d_status = nullptr;
   uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
-  // Pack jobs of irreversible tiles follow the npack reversible ones.
+  // Reversible pack jobs grouped by kernel variant (pack_variant): variant v
+  // has npack_v[v] jobs from d_pack + pack_begin[v] covering pack_units_v[v]
+  // units; npack and pack_ctas are their totals.  Pack jobs of irreversible
+  // tiles follow the npack reversible ones.
+  uint32_t pack_begin[sgn::kPackVariants] = {}, npack_v[sgn::kPackVariants] = {},
+           pack_units_v[sgn::kPackVariants] = {};
   uint32_t npack97 = 0, pack97_ctas = 0;
   std::vector<RoundInfo> rounds;
   uint64_t launches = 0;
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
   // Launch shape and the device work-queue counters (one per queued launch:
-  // MagSgn, each IDWT round, pack, 9/7 pack, classic blocks), zeroed at the
-  // start of every execution.
+  // MagSgn, each IDWT round, each pack variant, 9/7 pack, classic blocks),
+  // zeroed at the start of every execution.
   LaunchConfig cfg;
   uint32_t* d_queue = nullptr;
   uint32_t nqueues = 0;

@@ -700,6 +700,11 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
   }
   const uint32_t* sym = symbols + job.sym;
   const uint8_t* src = arena + job.src;
+  // The block's cleanup bytes and quad symbols are requested from HBM before
+  // the first of them is loaded: the unstuffing steps and the quad rows then
+  // read them from L2.
+  prefetch_l2_range(src, job.lcup, lane, 32);
+  prefetch_l2_range(sym, (size_t)sym_row_stride(w) * ((h + 1) / 2) * 4, lane, 32);
   bool ok = sym[0] != kSymFailed;
   uint32_t lcup = job.lcup, scup = 0;
   if (ok) {

@@ -205,12 +205,14 @@ constexpr int kStreamSlots = 9;
 
 // Vertical 5/3 stream over rows [ys, ye) of three level images, one
 // component at a time: the lifting state lives in the lane's own
-// shared-memory slots `st` (slot k at st[k * 32 + lane]), so only one
+// shared-memory slots `st` (slot k at st[k * 32 + lane]) and the components'
+// band descriptors in the warp's shared table `tab`, so only one
 // component's rows are in registers at once.  emit(y, v[3]) as stream_rows.
 template <typename Emit>
-__device__ __forceinline__ void stream_rows3(const PackJob& job, int w, int h, int b, int lane, int ys, int ye,
-                                             int4* st, Emit emit) {
-  auto bands = [&](int c) { return make_bands(job.ll[c], job.hl[c], job.lh[c], job.hh[c], w, h); };
+__device__ __forceinline__ void stream_rows3(const Bands* tab, int b, int lane, int ys, int ye, int4* st,
+                                             Emit emit) {
+  const int w = tab[0].w, h = tab[0].h;
+  auto bands = [&](int c) -> const Bands& { return tab[c]; };
   auto slot = [&](int k) -> int4& { return st[k * kLanes + lane]; };
   int4 v[3];
   if (h == 1) {
@@ -234,11 +236,11 @@ __device__ __forceinline__ void stream_rows3(const PackJob& job, int w, int h, i
     for (int c = 0; c < 3; ++c) {
       RawRow ne = re, no = ro;
       if (c < 2) {
-        const Bands N = bands(c + 1);
+        const Bands& N = bands(c + 1);
         ne = load_row(N, ye_row, b, lane);
         no = load_row(N, yo_row, b, lane);
       } else if (more) {
-        const Bands N = bands(0);
+        const Bands& N = bands(0);
         ne = load_row(N, ye_row + 2, b, lane);
         no = load_row(N, yo_row + 2, b, lane);
       }
@@ -449,7 +451,7 @@ __device__ __forceinline__ void store_row(const PackJob& job, int y, int x0, int
 
 template <int NC, int FMT, bool DIRECT>
 __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
-                                          int4* st) {
+                                          int4* st, Bands* tab) {
   constexpr int BPP = pack_bpp<FMT>();
   const int w = (int)job.w;
   const int cx0 = (int)job.cx, cy0 = (int)job.cy, cx1 = cx0 + (int)job.cw, cy1 = cy0 + (int)job.ch;
@@ -487,7 +489,11 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
   };
   if (job.lifting) {
     if (NC == 3) {
-      stream_rows3(job, w, (int)job.h, b, lane, ys, ye, st, emit);
+      // The components' band descriptors, read from the job once per unit.
+      if (lane < 3) tab[lane] = make_bands(job.ll[lane], job.hl[lane], job.lh[lane], job.hh[lane], w, (int)job.h);
+      __syncwarp();
+      stream_rows3(tab, b, lane, ys, ye, st, emit);
+      __syncwarp();  // the table is rewritten by the warp's next unit
     } else {
       const Bands B = make_bands(job.ll[0], job.hl[0], job.lh[0], job.hh[0], w, (int)job.h);
       stream_rows<1, true>(&B, b, lane, ys, ye, emit);
@@ -511,40 +517,41 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
 
 }  // namespace
 
-template <int FMT>
+template <int FMT, int NC, bool DIRECT>
 __device__ __forceinline__ void pack_one(const PackJob* __restrict__ jobs, uint32_t njobs, uint32_t unit,
-                                         uint32_t* rowbuf, int4* st) {
+                                         uint32_t* rowbuf, int4* st, Bands* tab) {
   const int lane = threadIdx.x & 31;
   const PackJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
   const int x0 = (int)(job.cx & ~(uint32_t)(kIdwtStripW - 1)) + (int)(local % job.strips) * kIdwtStripW;
   const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
   const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
-  constexpr bool kU8 = FMT == PACK_GRAY8 || FMT == PACK_RGB8 || FMT == PACK_RGBA8;
-  const bool direct = kU8 ? job.bit_depth == 8 : job.bit_depth > 8;
-  if (job.ncomp >= 3) {
-    if (direct) pack_unit<3, FMT, true>(job, x0, ys, ye, lane, rowbuf, st);
-    else pack_unit<3, FMT, false>(job, x0, ys, ye, lane, rowbuf, st);
-  } else {
-    if (direct) pack_unit<1, FMT, true>(job, x0, ys, ye, lane, rowbuf, st);
-    else pack_unit<1, FMT, false>(job, x0, ys, ye, lane, rowbuf, st);
-  }
+  pack_unit<NC, FMT, DIRECT>(job, x0, ys, ye, lane, rowbuf, st, tab);
 }
 
-template <int FMT, bool QUEUE>
-__global__ void __launch_bounds__(kIdwtWarps * 32, 4) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
+// One kernel per (pixel format, components, conversion) variant, with the
+// jobs of a launch all of that variant (pack_variant): each variant gets the
+// registers it needs and none of the others' code.  NC 3: RGB tiles, 1: gray;
+// DIRECT: samples convert with a clamp alone.  The gray stream keeps its
+// lifting state in registers (the RGB one in shared memory), so it runs
+// three CTAs per SM with room for it instead of four.
+template <int FMT, int NC, bool DIRECT, bool QUEUE>
+__global__ void __launch_bounds__(kIdwtWarps * 32, NC == 3 ? 4 : 3) pack_kernel(const PackJob* __restrict__ jobs, uint32_t njobs,
                                                                uint32_t nunits, uint32_t* queue) {
   __shared__ __align__(16) uint32_t rowbufs[kIdwtWarps][kRowWords];
   __shared__ int4 states[kIdwtWarps][kStreamSlots * kLanes];
+  __shared__ Bands tabs[kIdwtWarps][3];
   uint32_t* rowbuf = rowbufs[threadIdx.x >> 5];
   int4* st = states[threadIdx.x >> 5];
+  Bands* tab = tabs[threadIdx.x >> 5];
   if (!QUEUE) {
     const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
-    if (unit < nunits) pack_one<FMT>(jobs, njobs, unit, rowbuf, st);
+    if (unit < nunits) pack_one<FMT, NC, DIRECT>(jobs, njobs, unit, rowbuf, st, tab);
     return;
   }
   bool first = true;
-  for (uint32_t unit; next_unit(queue, nunits, first, unit);) pack_one<FMT>(jobs, njobs, unit, rowbuf, st);
+  for (uint32_t unit; next_unit(queue, nunits, first, unit);)
+    pack_one<FMT, NC, DIRECT>(jobs, njobs, unit, rowbuf, st, tab);
 }
 
 // ---------------------------------------------------------------------------
@@ -685,8 +692,9 @@ __device__ __forceinline__ float4 lstep4(float4 a, float4 b, float c, float4 x) 
 // Vertical 9/7 stream over rows [ys, ye) (ys even) of NC level images.
 // col is the lane's first column; src(c) gives component c's bands;
 // st(c, k) is its lifting state (k 0: the
-// last odd input row, 1..3: the last rows after delta, gamma, beta; 4, 5:
-// the finished odd and even rows of the step); emit(y, v[NC]) receives each
+// last odd input row, 1..3: the last rows after delta, gamma, beta, the
+// beta row being the step's finished even row; 4: its finished odd row);
+// emit(y, v[NC]) receives each
 // finished row.  Components are lifted one at a time while the next
 // component's (or the next step's) rows load.
 template <int NC, typename SrcOf, typename State, typename Emit>
@@ -774,7 +782,7 @@ __device__ __forceinline__ void idwt97_unit(const IdwtJob* __restrict__ jobs, ui
   float* out = reinterpret_cast<float*>(job.out);
   const bool mine = lane >= 1 && lane <= kLanes - 2;
   const bool vec_out = (w & 3) == 0 && (((uintptr_t)out) & 15) == 0;
-  float4 state[6];
+  float4 state[5];
   const Src97* sp = &S;
   stream97<1>([sp](int) -> const Src97& { return *sp; }, h, col, ys, ye, kKappa97, IK,
               [&](int, int k) -> float4& { return state[k]; },
@@ -876,8 +884,9 @@ __device__ __forceinline__ void put_pixel97(uint32_t* wds, int p, float c0, floa
   }
 }
 
-// Shared-memory slots of a lane's three-component 9/7 stream: 6 per component.
-constexpr int kSlots97 = 6 * 3;
+// Shared-memory slots of a lane's three-component 9/7 stream: 5 per component
+// (the stream's st(c, 0..4)).
+constexpr int kSlots97 = 5 * 3;
 
 template <int NC, int FMT>
 __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, int ye, int lane, uint32_t* rowbuf,
@@ -928,12 +937,12 @@ __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, 
                                job.ll_band != 0, w, h, x0 - 4);
       __syncwarp();
       stream97<3>([&](int c) -> const Src97& { return tab[c]; }, h, col, ys, ye, kKappa97, IK,
-                  [&](int c, int k) -> float4& { return st[(c * 6 + k) * kLanes + lane]; }, emit);
+                  [&](int c, int k) -> float4& { return st[(c * 5 + k) * kLanes + lane]; }, emit);
       __syncwarp();
     } else {
       const Src97 S = make_src97(job.ll[0], job.hl[0], job.lh[0], job.hh[0], job.step[0], job.ll_band != 0, w, h,
                                  x0 - 4);
-      float4 state[6];
+      float4 state[5];
       const Src97* sp = &S;
       stream97<1>([sp](int) -> const Src97& { return *sp; }, h, col, ys, ye, kKappa97, IK,
                   [&](int, int k) -> float4& { return state[k]; }, emit);
@@ -976,8 +985,10 @@ __global__ void __launch_bounds__(kWarps97 * 32) pack97_kernel(const PackJob* __
     const int x0 = (int)(job.cx - job.cx % kStrip97) + (int)(local % job.strips) * kStrip97;
     const int ys = (int)(job.cy & ~1u) + (int)(local / job.strips) * (int)job.seg;
     const int ye = min(ys + (int)job.seg, (int)(job.cy + job.ch));
-    if (job.ncomp >= 3) pack97_unit<3, FMT>(job, x0, ys, ye, lane, rowbuf, st, tab, IK);
-    else pack97_unit<1, FMT>(job, x0, ys, ye, lane, rowbuf, st, tab, IK);
+    // RGB formats take RGB tiles, gray formats gray ones (the host maps them
+    // so), so the format fixes the component count.
+    constexpr int NC = (FMT == PACK_GRAY8 || FMT == PACK_GRAY16) ? 1 : 3;
+    pack97_unit<NC, FMT>(job, x0, ys, ye, lane, rowbuf, st, tab, IK);
   };
   if (!QUEUE) {
     const uint32_t unit = blockIdx.x * kWarps97 + (threadIdx.x >> 5);
@@ -1031,44 +1042,66 @@ cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nuni
   return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
-                        uint32_t* queue, uint32_t persistent_ctas) {
+namespace {
+
+template <int F, int NC, bool D>
+cudaError_t launch_pack_variant(const PackJob* jobs, uint32_t njobs, uint32_t nunits, dim3 grid, cudaStream_t stream,
+                                uint32_t* queue) {
+  if (queue) pack_kernel<F, NC, D, true><<<grid, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, queue);
+  else pack_kernel<F, NC, D, false><<<grid, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, nullptr);
+  return cudaGetLastError();
+}
+
+// RGB formats take RGB tiles (variants 0, 1), gray formats gray ones (2, 3).
+template <int F>
+cudaError_t launch_pack_format(uint32_t variant, const PackJob* jobs, uint32_t njobs, uint32_t nunits, dim3 grid,
+                               cudaStream_t stream, uint32_t* queue) {
+  if constexpr (F == PACK_GRAY8 || F == PACK_GRAY16) {
+    if (variant == 2) return launch_pack_variant<F, 1, true>(jobs, njobs, nunits, grid, stream, queue);
+    if (variant == 3) return launch_pack_variant<F, 1, false>(jobs, njobs, nunits, grid, stream, queue);
+  } else {
+    if (variant == 0) return launch_pack_variant<F, 3, true>(jobs, njobs, nunits, grid, stream, queue);
+    if (variant == 1) return launch_pack_variant<F, 3, false>(jobs, njobs, nunits, grid, stream, queue);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, uint32_t variant,
+                        cudaStream_t stream, uint32_t* queue, uint32_t persistent_ctas) {
   if (njobs == 0 || nunits == 0) return cudaSuccess;
   uint32_t ctas = (nunits + kIdwtWarps - 1) / kIdwtWarps;
   if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
-  const dim3 grid(ctas), block(kIdwtWarps * 32);
-#define SGN_PACK_LAUNCH(F)                                                                   \
-  case F:                                                                                     \
-    if (queue) pack_kernel<F, true><<<grid, block, 0, stream>>>(jobs, njobs, nunits, queue); \
-    else pack_kernel<F, false><<<grid, block, 0, stream>>>(jobs, njobs, nunits, nullptr);    \
-    break;
+  const dim3 grid(ctas);
   switch (fmt) {
-    SGN_PACK_LAUNCH(PACK_GRAY8)
-    SGN_PACK_LAUNCH(PACK_RGB8)
-    SGN_PACK_LAUNCH(PACK_RGBA8)
-    SGN_PACK_LAUNCH(PACK_GRAY16)
-    SGN_PACK_LAUNCH(PACK_RGB16)
+    case PACK_GRAY8: return launch_pack_format<PACK_GRAY8>(variant, jobs, njobs, nunits, grid, stream, queue);
+    case PACK_RGB8: return launch_pack_format<PACK_RGB8>(variant, jobs, njobs, nunits, grid, stream, queue);
+    case PACK_RGBA8: return launch_pack_format<PACK_RGBA8>(variant, jobs, njobs, nunits, grid, stream, queue);
+    case PACK_GRAY16: return launch_pack_format<PACK_GRAY16>(variant, jobs, njobs, nunits, grid, stream, queue);
+    case PACK_RGB16: return launch_pack_format<PACK_RGB16>(variant, jobs, njobs, nunits, grid, stream, queue);
     default: return cudaErrorInvalidValue;
   }
-#undef SGN_PACK_LAUNCH
-  return cudaGetLastError();
 }
 
 cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm) {
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(idwt_ctas_per_sm, idwt_level_kernel<true>,
                                                                 kIdwtWarps * 32, 0);
   if (e != cudaSuccess) return e;
+  // Every variant has the same launch bounds and shared memory; the direct
+  // one of the format stands for them.
   switch (fmt) {
-    case PACK_GRAY8:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_GRAY8, true>, kIdwtWarps * 32, 0);
-    case PACK_RGB8:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGB8, true>, kIdwtWarps * 32, 0);
-    case PACK_RGBA8:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGBA8, true>, kIdwtWarps * 32, 0);
-    case PACK_GRAY16:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_GRAY16, true>, kIdwtWarps * 32, 0);
-    case PACK_RGB16:
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(pack_ctas_per_sm, pack_kernel<PACK_RGB16, true>, kIdwtWarps * 32, 0);
+#define SGN_PACK_OCC(F)                                                                                    \
+    case F:                                                                                                 \
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                                 \
+          pack_ctas_per_sm, pack_kernel<F, (F == PACK_GRAY8 || F == PACK_GRAY16) ? 1 : 3, true, true>,     \
+          kIdwtWarps * 32, 0);
+    SGN_PACK_OCC(PACK_GRAY8)
+    SGN_PACK_OCC(PACK_RGB8)
+    SGN_PACK_OCC(PACK_RGBA8)
+    SGN_PACK_OCC(PACK_GRAY16)
+    SGN_PACK_OCC(PACK_RGB16)
+#undef SGN_PACK_OCC
     default: return cudaErrorInvalidValue;
   }
 }

@@ -11,6 +11,25 @@
 
 namespace sgn {
 
+#ifdef __CUDACC__
+// L2 prefetch hint for the 128-byte line holding p (a global address the
+// caller may read).  No register waits for it: the bytes a warp will load
+// later are requested from HBM early and its loads then hit L2.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(p)));
+}
+
+// Prefetches every line of the n bytes at p, `step` lines apart starting at
+// line `first` (lanes of a warp pass their lane index and 32).  Every
+// address passed to the hint lies inside [p, p + n).
+__device__ __forceinline__ void prefetch_l2_range(const void* p, size_t n, uint32_t first, uint32_t step) {
+  if (n == 0) return;
+  const uintptr_t a = (uintptr_t)p, end = a + n, line0 = a & ~(uintptr_t)127;
+  for (uintptr_t q = line0 + (uintptr_t)first * 128; q < end; q += (uintptr_t)step * 128)
+    prefetch_l2(reinterpret_cast<const void*>(q < a ? a : q));
+}
+#endif
+
 cudaError_t ht_kernels_init();
 // Uploads the HT tables and sets kernel attributes on `device` (current) once.
 cudaError_t ensure_device_init(int device);
@@ -39,9 +58,10 @@ cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n
 // at most persistent_ctas CTAs whose warps take units from the counter.
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
                               uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
-// All jobs of one launch share the pixel format fmt (a PackFormat).
-cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, cudaStream_t stream,
-                        uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
+// All jobs of one launch share the pixel format fmt (a PackFormat) and the
+// kernel variant (pack_variant of their components and bit depth).
+cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, uint32_t variant,
+                        cudaStream_t stream, uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
 cudaError_t idwt_pack_occupancy(uint32_t fmt, int* idwt_ctas_per_sm, int* pack_ctas_per_sm);
 // Classic (EBCOT Tier-1) code blocks: a persistent grid of `ctas` CTAs whose
 // threads each take blocks from the zeroed counter `queue` and decode them

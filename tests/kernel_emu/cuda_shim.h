@@ -46,6 +46,18 @@ inline unsigned __vcmpeq4(unsigned a, unsigned b) {
 inline int4 make_int4(int a, int b, int c, int d) { return {a, b, c, d}; }
 inline float4 make_float4(float a, float b, float c, float d) { return {a, b, c, d}; }
 template <class T> inline T __ldg(const T* p) { return *p; }
+// L2 prefetch hints have no effect on the host; the range form still checks
+// that every hinted address lies inside the range it was given.
+inline void prefetch_l2(const void*) {}
+inline void prefetch_l2_range(const void* p, size_t n, uint32_t first, uint32_t step) {
+  if (n == 0) return;
+  const uintptr_t a = (uintptr_t)p, end = a + n, line0 = a & ~(uintptr_t)127;
+  for (uintptr_t q = line0 + (uintptr_t)first * 128; q < end; q += (uintptr_t)step * 128) {
+    const uintptr_t h = q < a ? a : q;
+    if (h < a || h >= end) std::abort();
+    (void)*reinterpret_cast<const volatile uint8_t*>(h);  // under ASan: the byte must be addressable
+  }
+}
 template <class T> inline T __ldcg(const T* p) { return *p; }
 inline float __fmul_rn(float a, float b) { return a * b; }
 inline float __fadd_rn(float a, float b) { return a + b; }

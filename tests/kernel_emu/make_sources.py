@@ -42,8 +42,16 @@ void emu_idwt(bool irr, const IdwtJob* jobs, uint32_t n, uint32_t units) {
   if (irr) idwt97_level_kernel<false>(jobs, n, units, nullptr);
   else idwt_level_kernel<false>(jobs, n, units, nullptr);
 }
+template <int F>
+void emu_pack_fmt(bool irr, const PackJob* jobs, uint32_t n, uint32_t units) {
+  if (irr) return pack97_kernel<F, false>(jobs, n, units, nullptr);
+  constexpr int NC = (F == PACK_GRAY8 || F == PACK_GRAY16) ? 1 : 3;
+  // The launch's variant: every job of these launches has the first one's.
+  if (pack_variant(F, jobs[0].ncomp, jobs[0].bit_depth) & 1) pack_kernel<F, NC, false, false>(jobs, n, units, nullptr);
+  else pack_kernel<F, NC, true, false>(jobs, n, units, nullptr);
+}
 void emu_pack(bool irr, int fmt, const PackJob* jobs, uint32_t n, uint32_t units) {
-#define K(F) case F: if (irr) pack97_kernel<F, false>(jobs, n, units, nullptr); else pack_kernel<F, false>(jobs, n, units, nullptr); break;
+#define K(F) case F: emu_pack_fmt<F>(irr, jobs, n, units); break;
   switch (fmt) { K(PACK_GRAY8) K(PACK_RGB8) K(PACK_RGBA8) K(PACK_GRAY16) K(PACK_RGB16) }
 #undef K
 }
@@ -54,7 +62,8 @@ int emu_pack_warps(bool irr) { return irr ? kWarps97 : kIdwtWarps; }
 
 def strip_functions(src, names):
     out, i = [], 0
-    pat = re.compile(r"^(cudaError_t|size_t) (%s)\(" % names, re.M)
+    # A template header line directly above a launcher goes with it.
+    pat = re.compile(r"^(template <[^>\n]*>\n)?(cudaError_t|size_t) (%s)\(" % names, re.M)
     while True:
         m = pat.search(src, i)
         if not m:
