@@ -22,8 +22,9 @@ constexpr int kIdwtStripW = 128;
 constexpr int kStrip97 = 120;
 
 // Rows per work unit: long segments for big levels (less halo re-reading),
-// short ones for small levels (more warps in flight).
-inline uint32_t idwt_segment_rows(uint32_t h) { return h >= 256 ? 64 : (h >= 64 ? 32 : 16); }
+// short ones for small levels, whose few units otherwise each stream many
+// rows one after another (more, shorter units finish sooner).
+inline uint32_t idwt_segment_rows(uint32_t h) { return h >= 256 ? 64 : h >= 128 ? 16 : h >= 64 ? 8 : 4; }
 constexpr int kIdwtWarps = 8;  // warps (units) per CTA
 
 struct HtJob {
