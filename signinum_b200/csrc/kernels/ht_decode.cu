@@ -537,13 +537,18 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t* W, uint32_t nwords, 
 // neighbouring lanes by shuffles, otherwise they are kept per column in
 // shared memory (Ebase, two rows of `cols` bytes).  Returns true (on every
 // lane) when the stream is invalid.
-template <bool NARROW>
+template <bool NARROW, bool RAW>
 __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_words, uint8_t* Ebase, uint32_t cols,
                             const uint32_t* __restrict__ sym, int32_t* __restrict__ dst) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t w = job.w, h = job.h, stride = job.stride;
   const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
-  const bool raw = job.passes > 1;
+  // Window reads start at most at bit `lim`, so that words wi .. wi + 2 lie
+  // in the array (it holds at least 5 words).  The array ends with at least
+  // 64 bits of ones past the stream (its padding), and `lim` lies beyond
+  // those bits' start, so a clamped read returns the ones an unclamped one
+  // would have seen past the end of the stream.
+  const uint32_t lim = 32 * (ms_words - 3);
   const bool pairs = ((job.dst | stride) & 1) == 0;  // 8-byte aligned sample pairs
   const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
   uint8_t* Eprev = Ebase;  // wide blocks: bit lengths of v_n per column + 1, row above
@@ -609,10 +614,12 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
       // samples (independent funnel shifts); otherwise each sample reads its
       // own 32 bits.
       const uint32_t cs[4] = {0u, m[0], m[0] + m[1], m[0] + m[1] + m[2]};
-      uint32_t lo = 0, hi = 0;
-      if (inf & 0xF0) {
-        lo = bits_at(W, ms_words, off);
-        hi = bits_at(W, ms_words, off + 32);
+      uint32_t lo, hi;
+      {
+        const uint32_t o = min(off, lim), wi = o >> 5, sh = o & 31;
+        const uint32_t a0 = W[wi], a1 = W[wi + 1], a2 = W[wi + 2];
+        lo = __funnelshift_r(a0, a1, sh);
+        hi = __funnelshift_r(a1, a2, sh);
       }
       uint32_t msv[4];
 #pragma unroll
@@ -634,7 +641,7 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
       }
       if (active) {
         const uint32_t x = 2 * q;
-        auto cv = [&](uint32_t vv) { return raw ? (int32_t)vv : to_i32(vv, nbp); };
+        auto cv = [&](uint32_t vv) { return RAW ? (int32_t)vv : to_i32(vv, nbp); };
         if (pairs && x + 1 < w) {
           *reinterpret_cast<int2*>(row0 + x) = make_int2(cv(val[0]), cv(val[2]));
           if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(cv(val[1]), cv(val[3]));
@@ -719,8 +726,12 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
     // the reference's 0xFF padding.
     const uint32_t words = (ms_len + 15) / 4 + 2;
     unstuff_magsgn(src, ms_len, W, words);
-    const bool bad = job.w <= 64 ? magsgn_rows<true>(job, W, words, Ebase, cols, sym, dst)
-                                 : magsgn_rows<false>(job, W, words, Ebase, cols, sym, dst);
+    // Blocks with refinement passes keep the sign-magnitude words for them.
+    const bool raw = job.passes > 1;
+    const bool bad = job.w <= 64 ? (raw ? magsgn_rows<true, true>(job, W, words, Ebase, cols, sym, dst)
+                                        : magsgn_rows<true, false>(job, W, words, Ebase, cols, sym, dst))
+                                 : (raw ? magsgn_rows<false, true>(job, W, words, Ebase, cols, sym, dst)
+                                        : magsgn_rows<false, false>(job, W, words, Ebase, cols, sym, dst));
     ok = !bad;
   }
   if (!ok) {
