@@ -564,7 +564,9 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
     const bool initial = y == 0, second = y + 1 < h;
     int32_t* row0 = dst + (size_t)y * stride;
     int32_t* row1 = row0 + stride;
-    for (uint32_t c0 = 0; c0 < nq; c0 += 32) {
+    // NARROW rows have at most 32 quads: one pass, known at compile time.
+    const uint32_t c0_end = NARROW ? 1u : nq;
+    for (uint32_t c0 = 0; c0 < c0_end; c0 += 32) {
       const uint32_t q = c0 + lane;
       const bool active = q < nq;
       const uint32_t s = active ? sym[(size_t)r * qs + q] : 0;
