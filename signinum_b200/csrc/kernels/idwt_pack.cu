@@ -755,16 +755,20 @@ __device__ __forceinline__ void stream97(SrcOf src, int h, int col, int ys, int 
       st(c, 2) = s2;
       st(c, 3) = s3;
     }
-    const int yo = 2 * m - 1, yv = 2 * m;
-    if (yo >= ys && yo < ye) {
+    // The step's finished odd row 2m - 1, then its even row 2m, through one
+    // call site of emit (its pixel conversions are long: one copy of them
+    // in the loop keeps the code small).
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+      const int y = 2 * m - 1 + k;
+      if (y >= ys && y < ye) {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = st(c, 4);
-      emit(yo, v);
-    }
-    if (yv >= ys && yv < ye) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = st(c, 3);
-      emit(yv, v);
+        for (int c = 0; c < NC; ++c) {
+          const float4 odd = st(c, 4), even = st(c, 3);
+          v[c] = k ? even : odd;
+        }
+        emit(y, v);
+      }
     }
   }
 }
