@@ -420,7 +420,10 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     const uint32_t sw = L.reversible ? kIdwtStripW : kStrip97;
     uint32_t ax = tw.crop_x - tw.crop_x % sw, ay = tw.crop_y & ~1u;
     pj.strips = (tw.crop_x + tw.crop_w - ax + sw - 1) / sw;
-    pj.seg = idwt_segment_rows(tw.crop_h) * (L.reversible ? 1 : 2);
+    // The 9/7 pack keeps the 5/3 segment length although its units re-read
+    // seven rows: 128-row segments left a batch of 512^2 tiles at 1.4 waves
+    // of units, 64-row ones fill the last wave far better.
+    pj.seg = idwt_segment_rows(tw.crop_h);
     pj.ll_band = R <= 1 ? 1 : 0;
     uint32_t segs = (tw.crop_y + tw.crop_h - ay + pj.seg - 1) / pj.seg;
     const uint32_t v = pack_variant(fmt, L.ncomp, L.bit_depth);
