@@ -37,6 +37,24 @@ def random_codestream(rng, max_side=80):
     return cs, px, w, h, comps, bd
 
 
+# Code-block shapes beyond 64 on a side (exponents over the 4-sample base),
+# within JPEG 2000's limits (at most 1024 on a side, w h <= 4096).
+WIDE_BLOCKS = [(5, 3), (6, 2), (7, 1), (8, 0), (3, 5), (0, 8), (5, 1)]
+
+
+def wide_block_codestream(rng, cb, max_w=300, max_h=140):
+    """A seeded lossless HT codestream whose code blocks have the exponents
+    cb = (width, height): 128x32 .. 1024x4 and 4x1024 blocks."""
+    w = int(rng.integers(40, max_w))
+    h = int(rng.integers(12, max_h))
+    comps = int(rng.choice([1, 3]))
+    bd = int(rng.choice([8, 12, 16])) if comps == 1 else 8
+    px = random_tile(rng, w, h, comps, bd, int(rng.integers(0, 2)))
+    cs = encode.encode_lossless(px.reshape(-1).view(np.uint8), w, h, comps, bd, levels=int(rng.integers(0, 4)),
+                                cb_exp=cb[0], cb_exp_h=cb[1], progression=int(rng.choice([0, 2, 4])))
+    return cs, px, w, h, comps, bd
+
+
 def _box(btype: bytes, payload: bytes, form: str = "short") -> bytes:
     """One JP2 box: 'short' (32-bit length), 'long' (extended 64-bit length)
     or 'to_end' (length 0: the box runs to the end of the file)."""

@@ -13,7 +13,7 @@ from oracle import oracle
 from signinum_b200 import (BackendKind, BackendRequest, Codec, CudaSession, Downscale, Error, J2kDecoder, PixelFormat,
                            Rect, TileBatchError, encode)
 from signinum_b200.j2k_cuda import _request
-from tests.helpers import random_codestream
+from tests.helpers import WIDE_BLOCKS, random_codestream, wide_block_codestream
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +67,25 @@ def test_random_tiles_match_oracle(seed):
             got, gd = gpu(cs, fmt)
             assert gd == wd == (w, h)
             assert got == want, (w, h, comps, bd, fmt)
+
+
+@pytest.mark.parametrize("cb", WIDE_BLOCKS)
+def test_wide_code_blocks_match_oracle(cb):
+    """Blocks wider than 64 take the kernels' wide paths (VLC context read
+    back from the symbol table, MagSgn exponents kept per column in shared
+    memory); 4x1024 blocks the long narrow ones."""
+    rng = np.random.default_rng(4100 + 16 * cb[0] + cb[1])
+    for _ in range(3):
+        cs, px, w, h, comps, bd = wide_block_codestream(rng, cb)
+        fmts = [PixelFormat.Rgb8, PixelFormat.Rgb16] if comps == 3 else [PixelFormat.Gray8, PixelFormat.Gray16]
+        for fmt in fmts:
+            want, wd = cpu(cs, fmt)
+            got, gd = gpu(cs, fmt)
+            assert gd == wd == (w, h)
+            assert got == want, (cb, w, h, comps, bd, fmt)
+        roi = Rect(w // 5, h // 4, max(1, w // 2), max(1, h // 2))
+        fmt = fmts[0]
+        assert gpu(cs, fmt, 1, roi)[0] == cpu(cs, fmt, 1, roi)[0]
 
 
 @pytest.mark.parametrize("seed", range(3))

@@ -12,7 +12,7 @@ import sys
 import numpy as np
 import pytest
 
-from tests.helpers import random_classic, random_codestream, random_irreversible
+from tests.helpers import WIDE_BLOCKS, random_classic, random_codestream, random_irreversible, wide_block_codestream
 
 EMU = pathlib.Path(__file__).parent / "kernel_emu"
 ROOT = EMU.parents[1]
@@ -64,3 +64,17 @@ def test_random_codestreams_through_emulated_kernels(emu, kind):
         by_comps[comps].append(cs)
     run(emu, "03", by_comps[1])  # Gray8, Gray16
     run(emu, "124", by_comps[3])  # Rgb8, Rgba8, Rgb16
+
+
+def test_wide_code_blocks_through_emulated_kernels(emu):
+    """HT blocks wider or higher than 64 (the VLC and MagSgn kernels' wide
+    paths) under AddressSanitizer."""
+    rng = np.random.default_rng(4200)
+    by_comps = {1: [], 3: []}
+    for cb in WIDE_BLOCKS:
+        cs, _, _, _, comps, _ = wide_block_codestream(rng, cb, max_w=160, max_h=72)
+        by_comps[comps].append(cs)
+    if by_comps[1]:
+        run(emu, "03", by_comps[1])
+    if by_comps[3]:
+        run(emu, "124", by_comps[3])

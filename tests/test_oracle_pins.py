@@ -10,7 +10,7 @@ import pytest
 
 from oracle import oracle
 from signinum_b200 import encode
-from tests.helpers import random_codestream
+from tests.helpers import WIDE_BLOCKS, random_codestream, wide_block_codestream
 
 GOLDEN = pathlib.Path(__file__).parent / "golden"
 
@@ -71,6 +71,19 @@ def test_encoder_roundtrip_through_oracle(seed):
         if bd not in (8, 16):
             want = np.clip(px.astype(np.int64), 0, (1 << bd) - 1).astype("<u2").tobytes()
         assert got == want
+
+
+@pytest.mark.parametrize("cb", WIDE_BLOCKS)
+def test_wide_code_blocks_roundtrip_through_oracle(cb):
+    """Code blocks wider or higher than 64 (up to 1024x4 and 4x1024) decode
+    losslessly: the oracle's HT decoder has no 64-sample limit."""
+    rng = np.random.default_rng(4000 + 16 * cb[0] + cb[1])
+    for _ in range(3):
+        cs, px, w, h, comps, bd = wide_block_codestream(rng, cb)
+        fmt = (1 if comps == 3 else 0) if bd == 8 else (4 if comps == 3 else 3)
+        got, ow, oh = oracle.decode(cs, fmt)
+        assert (ow, oh) == (w, h)
+        assert got == px.tobytes()
 
 
 def test_workload_tile_is_lossless():
