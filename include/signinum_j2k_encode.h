@@ -35,6 +35,8 @@ typedef struct sgn_encode_options {
   uint32_t progression;              /* sgn_progression */
   uint32_t write_tlm;
   uint32_t sop_eph;                  /* emit SOP/EPH packet markers */
+  uint32_t precinct_width_exp;       /* PPx of every resolution, 1..15; 0 (with height 0): no precincts */
+  uint32_t precinct_height_exp;      /* PPy */
 } sgn_encode_options;
 
 /* pixels: interleaved samples, 1 byte each for bit_depth <= 8, else u16 LE.

@@ -6,7 +6,10 @@
 // reversible colour transform, forward 5/3 with vertical then horizontal
 // lifting per level, no quantisation (exponents bit_depth + band gain, guard
 // bits raised to 2 with RCT), HT cleanup-only code blocks, one layer, one
-// precinct per resolution, SIZ/CAP/COD/QCD/[TLM]/SOT/SOD/EOC markers.
+// precinct per resolution unless precinct exponents are given (then the
+// resolutions are cut into precincts, code blocks clipped to them, packets
+// per precinct in the progression's order), SIZ/CAP/COD/QCD/[TLM]/SOT/SOD/EOC
+// markers.
 //
 // The irreversible mode produces lossy inputs for the 9/7 decode path (it
 // has no counterpart in the reference, which encodes losslessly only): DC
@@ -21,6 +24,7 @@
 // magnitude/sign bits in a forward stream, ending in the Scup trailer.  Every
 // context and exponent predictor mirrors what the decoder recomputes.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -576,7 +580,20 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   }
   // Per component: bands[0] = LL, then HL, LH, HH per resolution 1..L.
   std::vector<std::vector<Band>> bands(C);
-  const uint32_t cbw = 1u << (P.cbw_exp + 2), cbh = 1u << (P.cbh_exp + 2);
+  // Precincts (B.6): resolution r is cut into 2^PPx x 2^PPy precincts; in
+  // its sub-bands that is 2^(PPx-1) x 2^(PPy-1) samples (2^PPx x 2^PPy in
+  // the LL band of resolution 0), and code blocks are clipped to that size
+  // (B.7: xcb' = min(xcb, PPx - 1), or PPx at resolution 0).
+  const bool precincts = P.ppx || P.ppy;
+  if (precincts && (P.ppx < 1 || P.ppy < 1 || P.ppx > 15 || P.ppy > 15)) return -2;
+  auto band_pp = [&](uint32_t pp, uint32_t r) { return r == 0 ? pp : pp - 1; };
+  auto cb_w = [&](uint32_t r) {
+    return 1u << (precincts ? std::min(P.cbw_exp + 2, band_pp(P.ppx, r)) : P.cbw_exp + 2);
+  };
+  auto cb_h = [&](uint32_t r) {
+    return 1u << (precincts ? std::min(P.cbh_exp + 2, band_pp(P.ppy, r)) : P.cbh_exp + 2);
+  };
+  std::vector<uint32_t> res_w(L + 1), res_h(L + 1);  // resolution sizes
   auto band_mb = [&](uint32_t gain) { return irr ? guard + q_eps - 1 : guard + bd + gain - 1; };
   for (uint32_t c = 0; c < C; ++c) {
     std::vector<int32_t> cur;
@@ -601,7 +618,7 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     }
     const uint32_t cw = lw[L], ch = lhh[L];
     auto make_band = [&](const std::vector<int32_t>& data, uint32_t w, uint32_t h, uint32_t gain,
-                         uint8_t band_class) -> int {
+                         uint8_t band_class, uint32_t cbw, uint32_t cbh) -> int {
       Band b;
       b.w = w;
       b.h = h;
@@ -626,14 +643,19 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
       bands[c].push_back(std::move(b));
       return 0;
     };
-    if (make_band(cur, cw, ch, 0, ebcot::kLlLh) != 0) return -3;
+    if (c == 0)
+      for (uint32_t r = 0; r <= L; ++r) {
+        res_w[r] = lw[L - r];
+        res_h[r] = lhh[L - r];
+      }
+    if (make_band(cur, cw, ch, 0, ebcot::kLlLh, cb_w(0), cb_h(0)) != 0) return -3;
     for (uint32_t r = 1; r <= L; ++r) {
       uint32_t d = L + 1 - r;  // decomposition level of resolution r
       uint32_t pw = lw[d - 1], ph = lhh[d - 1];
       uint32_t lwd = (pw + 1) / 2, hwd = pw / 2, lhd = (ph + 1) / 2, hhd = ph / 2;
-      if (make_band(hl[d], hwd, lhd, 1, ebcot::kHl) != 0) return -3;
-      if (make_band(lh[d], lwd, hhd, 1, ebcot::kLlLh) != 0) return -3;
-      if (make_band(hh[d], hwd, hhd, 2, ebcot::kHh) != 0) return -3;
+      if (make_band(hl[d], hwd, lhd, 1, ebcot::kHl, cb_w(r), cb_h(r)) != 0) return -3;
+      if (make_band(lh[d], lwd, hhd, 1, ebcot::kLlLh, cb_w(r), cb_h(r)) != 0) return -3;
+      if (make_band(hh[d], hwd, hhd, 2, ebcot::kHh, cb_w(r), cb_h(r)) != 0) return -3;
     }
   }
   // Packets: one layer, one precinct per resolution.
@@ -663,34 +685,63 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     }
     return parts;
   };
-  // Packet state that lasts over the layers: per band the inclusion (leaf:
-  // first layer with passes) and zero-bit-plane tag trees, per block whether
-  // it was included and its Lblock.
-  struct BandState {
+  // Precinct grid of resolution r: npx x npy precincts of 2^PPx x 2^PPy.
+  auto n_prec = [&](uint32_t r, bool x) -> uint32_t {
+    const uint32_t n = x ? res_w[r] : res_h[r], pp = x ? P.ppx : P.ppy;
+    return !precincts ? 1u : (n + (1u << pp) - 1) >> pp;
+  };
+  auto res_of = [](size_t bi) -> uint32_t { return bi == 0 ? 0u : (uint32_t)((bi - 1) / 3 + 1); };
+  // The code blocks of precinct p of a band: block columns [x0, x1) and
+  // rows [y0, y1) of the band's block grid.
+  struct Range {
+    uint32_t x0, x1, y0, y1;
+  };
+  auto prec_blocks = [&](const Band& b, size_t bi, uint32_t p) -> Range {
+    if (!precincts) return {0, b.ncx, 0, b.ncy};
+    const uint32_t r = res_of(bi), npx = n_prec(r, true);
+    const uint32_t px = p % npx, py = p / npx;
+    const uint32_t bpw = 1u << band_pp(P.ppx, r), bph = 1u << band_pp(P.ppy, r);  // band precinct size
+    const uint32_t kx = bpw / b.cbw, ky = bph / b.cbh;                              // blocks per precinct side
+    return {std::min(px * kx, b.ncx), std::min((px + 1) * kx, b.ncx), std::min(py * ky, b.ncy),
+            std::min((py + 1) * ky, b.ncy)};
+  };
+  // Packet state that lasts over the layers: per (band, precinct) the
+  // inclusion (leaf: first layer with passes) and zero-bit-plane tag trees;
+  // per block whether it was included and its Lblock.
+  struct PrecState {
     std::unique_ptr<TagTree> ti, tz;
+  };
+  struct BandState {
+    std::vector<PrecState> prec;
     std::vector<uint8_t> included;
     std::vector<uint32_t> lblock;
   };
   std::vector<std::vector<BandState>> bstate(C);
   for (uint32_t c = 0; c < C; ++c)
-    for (Band& b : bands[c]) {
+    for (size_t bi = 0; bi < bands[c].size(); ++bi) {
+      Band& b = bands[c][bi];
       BandState st;
-      std::vector<uint32_t> incl(b.blocks.size()), zbp(b.blocks.size());
-      for (size_t i = 0; i < b.blocks.size(); ++i) {
-        const CodeBlockOut& cb = b.blocks[i];
-        uint32_t first = 0xFFFFu;  // never included
-        if (!cb.empty()) {
-          first = 0;
-          if (P.classic)
-            while (layer_first(cb.classic.passes, first + 1) == layer_first(cb.classic.passes, first)) ++first;
-        }
-        incl[i] = first;
-        // Empty leaves are never coded.
-        zbp[i] = cb.empty() ? 0xFFFFu : (P.classic ? cb.classic.zero_planes : b.mb - 1);
-      }
-      if (b.ncx && b.ncy) {
-        st.ti.reset(new TagTree(b.ncx, b.ncy, incl));
-        st.tz.reset(new TagTree(b.ncx, b.ncy, zbp));
+      const uint32_t r = res_of(bi), np = n_prec(r, true) * n_prec(r, false);
+      st.prec.resize(np);
+      for (uint32_t p = 0; p < np; ++p) {
+        const Range R = prec_blocks(b, bi, p);
+        if (R.x1 <= R.x0 || R.y1 <= R.y0) continue;
+        std::vector<uint32_t> incl, zbp;
+        for (uint32_t y = R.y0; y < R.y1; ++y)
+          for (uint32_t x = R.x0; x < R.x1; ++x) {
+            const CodeBlockOut& cb = b.blocks[(size_t)y * b.ncx + x];
+            uint32_t first = 0xFFFFu;  // never included
+            if (!cb.empty()) {
+              first = 0;
+              if (P.classic)
+                while (layer_first(cb.classic.passes, first + 1) == layer_first(cb.classic.passes, first)) ++first;
+            }
+            incl.push_back(first);
+            // Empty leaves are never coded.
+            zbp.push_back(cb.empty() ? 0xFFFFu : (P.classic ? cb.classic.zero_planes : b.mb - 1));
+          }
+        st.prec[p].ti.reset(new TagTree(R.x1 - R.x0, R.y1 - R.y0, incl));
+        st.prec[p].tz.reset(new TagTree(R.x1 - R.x0, R.y1 - R.y0, zbp));
       }
       st.included.assign(b.blocks.size(), 0);
       st.lblock.assign(b.blocks.size(), 3);
@@ -701,11 +752,15 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     if (!P.classic) return l == 0 ? 1 : 0;
     return layer_first(cb.classic.passes, l + 1) - layer_first(cb.classic.passes, l);
   };
-  auto packet = [&](uint32_t c, uint32_t r, uint32_t l) {
+  auto packet = [&](uint32_t c, uint32_t r, uint32_t l, uint32_t p) {
     size_t b0 = r == 0 ? 0 : 1 + (size_t)(r - 1) * 3, nb = r == 0 ? 1 : 3;
     bool any = false;
-    for (size_t bi = b0; bi < b0 + nb; ++bi)
-      for (auto& cb : bands[c][bi].blocks) any = any || passes_in(cb, l) > 0;
+    for (size_t bi = b0; bi < b0 + nb; ++bi) {
+      const Band& b = bands[c][bi];
+      const Range R = prec_blocks(b, bi, p);
+      for (uint32_t y = R.y0; y < R.y1; ++y)
+        for (uint32_t x = R.x0; x < R.x1; ++x) any = any || passes_in(b.blocks[(size_t)y * b.ncx + x], l) > 0;
+    }
     if (P.sop_eph) {
       tile.push_back(0xFF); tile.push_back(0x91);
       put16(tile, 4);
@@ -720,16 +775,18 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
       for (size_t bi = b0; bi < b0 + nb; ++bi) {
         Band& b = bands[c][bi];
         BandState& st = bstate[c][bi];
-        if (b.ncx == 0 || b.ncy == 0) continue;
-        for (uint32_t y = 0; y < b.ncy; ++y)
-          for (uint32_t x = 0; x < b.ncx; ++x) {
+        const Range R = prec_blocks(b, bi, p);
+        if (R.x1 <= R.x0 || R.y1 <= R.y0) continue;
+        PrecState& ps = st.prec[p];
+        for (uint32_t y = R.y0; y < R.y1; ++y)
+          for (uint32_t x = R.x0; x < R.x1; ++x) {
             const size_t i = (size_t)y * b.ncx + x;
             const auto& cb = b.blocks[i];
             const uint32_t np = passes_in(cb, l);
             if (!st.included[i]) {
-              st.ti->encode(x, y, l + 1, hw);
+              ps.ti->encode(x - R.x0, y - R.y0, l + 1, hw);
               if (np == 0) continue;
-              st.tz->encode(x, y, UINT32_MAX, hw);
+              ps.tz->encode(x - R.x0, y - R.y0, UINT32_MAX, hw);
               st.included[i] = 1;
             } else {
               hw.bit(np > 0 ? 1 : 0);
@@ -775,25 +832,40 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     if (P.sop_eph) { tile.push_back(0xFF); tile.push_back(0x92); }
     for (auto& part : body) tile.insert(tile.end(), part.first, part.first + part.second);
   };
-  // Packet order (one precinct per resolution): LRCP l r c; RLCP r l c;
-  // RPCL r c l; PCRL and CPRL c r l.
-  if (P.progression == 0) {
-    for (uint32_t l = 0; l < NL; ++l)
-      for (uint32_t r = 0; r <= L; ++r)
-        for (uint32_t c = 0; c < C; ++c) packet(c, r, l);
-  } else if (P.progression == 1) {
-    for (uint32_t r = 0; r <= L; ++r)
-      for (uint32_t l = 0; l < NL; ++l)
-        for (uint32_t c = 0; c < C; ++c) packet(c, r, l);
-  } else if (P.progression == 2) {
-    for (uint32_t r = 0; r <= L; ++r)
-      for (uint32_t c = 0; c < C; ++c)
-        for (uint32_t l = 0; l < NL; ++l) packet(c, r, l);
-  } else {
-    for (uint32_t c = 0; c < C; ++c)
-      for (uint32_t r = 0; r <= L; ++r)
-        for (uint32_t l = 0; l < NL; ++l) packet(c, r, l);
-  }
+  // Packet order (B.12.1).  LRCP and RLCP nest layer, resolution,
+  // component and precinct (raster order) as named.  The position-driven
+  // orders walk the tile's sample grid (y outer, x inner) and take, at each
+  // position, the precincts whose top-left corner lies there: with zero
+  // image and tile origins and no sub-sampling, precinct (px, py) of
+  // resolution r starts at (px, py) * 2^(PP + levels - r) on that grid.
+  // RPCL: r, then position, then component; PCRL: position, component, r;
+  // CPRL: component, position, r; the layers innermost.
+  struct Pk {
+    std::array<uint64_t, 5> key;
+    uint32_t c, r, l, p;
+  };
+  std::vector<Pk> order;
+  for (uint32_t c = 0; c < C; ++c)
+    for (uint32_t r = 0; r <= L; ++r) {
+      const uint32_t npx = n_prec(r, true), npy = n_prec(r, false);
+      for (uint32_t p = 0; p < npx * npy; ++p) {
+        const uint64_t ty = precincts ? (uint64_t)(p / npx) << (P.ppy + L - r) : 0;
+        const uint64_t tx = precincts ? (uint64_t)(p % npx) << (P.ppx + L - r) : 0;
+        for (uint32_t l = 0; l < NL; ++l) {
+          std::array<uint64_t, 5> k{};
+          switch (P.progression) {
+            case 0: k = {l, r, c, p, 0}; break;
+            case 1: k = {r, l, c, p, 0}; break;
+            case 2: k = {r, ty, tx, c, l}; break;
+            case 3: k = {ty, tx, c, r, l}; break;
+            default: k = {c, ty, tx, r, l}; break;
+          }
+          order.push_back({k, c, r, l, p});
+        }
+      }
+    }
+  std::sort(order.begin(), order.end(), [](const Pk& a, const Pk& b) { return a.key < b.key; });
+  for (const Pk& k : order) packet(k.c, k.r, k.l, k.p);
   // Codestream.
   out.clear();
   out.push_back(0xFF); out.push_back(0x4F);  // SOC
@@ -813,8 +885,8 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
     put16(out, bp);
   }
   out.push_back(0xFF); out.push_back(0x52);  // COD
-  put16(out, 12);
-  out.push_back(P.sop_eph ? 0x06 : 0x00);
+  put16(out, 12 + (precincts ? L + 1 : 0));
+  out.push_back((P.sop_eph ? 0x06 : 0x00) | (precincts ? 0x01 : 0x00));
   out.push_back((uint8_t)P.progression);
   put16(out, NL);
   out.push_back(mct ? 1 : 0);
@@ -823,6 +895,8 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
   out.push_back((uint8_t)P.cbh_exp);
   out.push_back(P.classic ? (uint8_t)(P.cb_style & 0x3F) : 0x40);  // code-block style
   out.push_back(irr ? 0 : 1);  // wavelet: 0 = 9/7 irreversible, 1 = 5/3 reversible
+  if (precincts)
+    for (uint32_t r = 0; r <= L; ++r) out.push_back((uint8_t)((P.ppy << 4) | P.ppx));
   out.push_back(0xFF); out.push_back(0x5C);  // QCD
   if (irr) {
     put16(out, 3 + 2 * (1 + 3 * L));

@@ -22,6 +22,9 @@ struct EncodeParams {
   bool classic = false;
   uint8_t cb_style = 0;
   uint32_t layers = 1;  // quality layers (classic only)
+  // Precinct exponents (PPx, PPy) of every resolution, 1..15; 0 = one
+  // precinct per resolution (no precinct partition signalled).
+  uint32_t ppx = 0, ppy = 0;
 };
 // One classic code block: its codeword segments back to back, each
 // segment's length and coding-pass count, and the block's zero bit-planes.

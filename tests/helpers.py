@@ -55,6 +55,31 @@ def wide_block_codestream(rng, cb, max_w=300, max_h=140):
     return cs, px, w, h, comps, bd
 
 
+def precinct_codestream(rng, kind, max_side=200):
+    """A seeded codestream cut into precincts of 2^PPx x 2^PPy (2 .. 256) in
+    any progression: kind "ht" (lossless), "classic" (lossless, 1-3 layers,
+    random code-block styles) or "lossy" (9/7).  Returns the codestream, the
+    pixels, width, height and components."""
+    w = int(rng.integers(1, max_side))
+    h = int(rng.integers(1, max_side))
+    comps = int(rng.choice([1, 3]))
+    px = random_tile(rng, w, h, comps, 8, int(rng.integers(0, 2)))
+    pp = (int(rng.integers(1, 9)), int(rng.integers(1, 9)))
+    cbw = int(rng.integers(0, 5))
+    cbh = min(int(rng.integers(0, 5)), 8 - cbw)
+    kw = dict(levels=int(rng.integers(0, 6)), cb_exp=cbw, cb_exp_h=cbh, progression=int(rng.integers(0, 5)),
+              precincts=pp)
+    flat = px.reshape(-1)
+    if kind == "ht":
+        cs = encode.encode_lossless(flat, w, h, comps, 8, **kw)
+    elif kind == "classic":
+        cs = encode.encode_classic(flat, w, h, comps, 8, style=int(rng.choice([0, 0x01, 0x04, 0x05, 0x2F])),
+                                   layers=int(rng.integers(1, 4)), **kw)
+    else:
+        cs = encode.encode_irreversible(flat, w, h, comps, 8, **kw)
+    return cs, px, w, h, comps
+
+
 def _box(btype: bytes, payload: bytes, form: str = "short") -> bytes:
     """One JP2 box: 'short' (32-bit length), 'long' (extended 64-bit length)
     or 'to_end' (length 0: the box runs to the end of the file)."""

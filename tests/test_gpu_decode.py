@@ -13,7 +13,7 @@ from oracle import oracle
 from signinum_b200 import (BackendKind, BackendRequest, Codec, CudaSession, Downscale, Error, J2kDecoder, PixelFormat,
                            Rect, TileBatchError, encode)
 from signinum_b200.j2k_cuda import _request
-from tests.helpers import WIDE_BLOCKS, random_codestream, wide_block_codestream
+from tests.helpers import WIDE_BLOCKS, precinct_codestream, random_codestream, wide_block_codestream
 
 pytestmark = pytest.mark.gpu
 
@@ -86,6 +86,22 @@ def test_wide_code_blocks_match_oracle(cb):
         roi = Rect(w // 5, h // 4, max(1, w // 2), max(1, h // 2))
         fmt = fmts[0]
         assert gpu(cs, fmt, 1, roi)[0] == cpu(cs, fmt, 1, roi)[0]
+
+
+@pytest.mark.parametrize("kind", ["ht", "classic", "lossy"])
+def test_precinct_partitions_match_oracle(kind):
+    """Codestreams cut into precincts (2 .. 256 samples a side) in every
+    progression: HT, multi-layer classic and lossy 9/7 code blocks."""
+    rng = np.random.default_rng({"ht": 4500, "classic": 4501, "lossy": 4502}[kind])
+    for _ in range(12):
+        cs, px, w, h, comps = precinct_codestream(rng, kind)
+        fmt = PixelFormat.Rgb8 if comps == 3 else PixelFormat.Gray8
+        want, wd = cpu(cs, fmt)
+        got, gd = gpu(cs, fmt)
+        assert gd == wd == (w, h)
+        assert got == want, (kind, w, h, comps)
+        if kind != "lossy":
+            assert got == px.tobytes()
 
 
 @pytest.mark.parametrize("seed", range(3))

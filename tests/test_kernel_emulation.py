@@ -12,7 +12,8 @@ import sys
 import numpy as np
 import pytest
 
-from tests.helpers import WIDE_BLOCKS, random_classic, random_codestream, random_irreversible, wide_block_codestream
+from tests.helpers import (WIDE_BLOCKS, precinct_codestream, random_classic, random_codestream, random_irreversible,
+                           wide_block_codestream)
 
 EMU = pathlib.Path(__file__).parent / "kernel_emu"
 ROOT = EMU.parents[1]
@@ -78,3 +79,16 @@ def test_wide_code_blocks_through_emulated_kernels(emu):
         run(emu, "03", by_comps[1])
     if by_comps[3]:
         run(emu, "124", by_comps[3])
+
+
+@pytest.mark.parametrize("kind", ["ht", "classic", "lossy"])
+def test_precinct_partitions_through_emulated_kernels(emu, kind):
+    """Precinct partitions through the product's host parser (which builds
+    the job tables) and the emulated kernels."""
+    rng = np.random.default_rng({"ht": 4400, "classic": 4401, "lossy": 4402}[kind])
+    by_comps = {1: [], 3: []}
+    while len(by_comps[1]) < 3 or len(by_comps[3]) < 3:
+        cs, _, _, _, comps = precinct_codestream(rng, kind, max_side=90)
+        by_comps[comps].append(cs)
+    run(emu, "03", by_comps[1])
+    run(emu, "124", by_comps[3])

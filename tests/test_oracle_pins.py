@@ -10,7 +10,7 @@ import pytest
 
 from oracle import oracle
 from signinum_b200 import encode
-from tests.helpers import WIDE_BLOCKS, random_codestream, wide_block_codestream
+from tests.helpers import WIDE_BLOCKS, precinct_codestream, random_codestream, wide_block_codestream
 
 GOLDEN = pathlib.Path(__file__).parent / "golden"
 
@@ -82,6 +82,19 @@ def test_wide_code_blocks_roundtrip_through_oracle(cb):
         cs, px, w, h, comps, bd = wide_block_codestream(rng, cb)
         fmt = (1 if comps == 3 else 0) if bd == 8 else (4 if comps == 3 else 3)
         got, ow, oh = oracle.decode(cs, fmt)
+        assert (ow, oh) == (w, h)
+        assert got == px.tobytes()
+
+
+@pytest.mark.parametrize("kind", ["ht", "classic"])
+def test_precinct_partitions_roundtrip_through_oracle(kind):
+    """Resolutions cut into precincts (code blocks clipped to them, packets
+    per precinct in every progression, the position-driven ones included)
+    decode losslessly: the encoder's packet order and the oracle's agree."""
+    rng = np.random.default_rng({"ht": 4300, "classic": 4301}[kind])
+    for _ in range(30):
+        cs, px, w, h, comps = precinct_codestream(rng, kind)
+        got, ow, oh = oracle.decode(cs, 1 if comps == 3 else 0)
         assert (ow, oh) == (w, h)
         assert got == px.tobytes()
 
