@@ -37,6 +37,7 @@ typedef struct sgn_encode_options {
   uint32_t sop_eph;                  /* emit SOP/EPH packet markers */
   uint32_t precinct_width_exp;       /* PPx of every resolution, 1..15; 0 (with height 0): no precincts */
   uint32_t precinct_height_exp;      /* PPy */
+  uint32_t tile_parts;               /* tile-parts the packets are split into (0 or 1: one) */
 } sgn_encode_options;
 
 /* pixels: interleaved samples, 1 byte each for bit_depth <= 8, else u16 LE.

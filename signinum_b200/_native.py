@@ -42,7 +42,7 @@ class SgnHtBlock(ctypes.Structure):
 class SgnEncodeOptions(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("max_decomposition_levels", "code_block_width_exp", "code_block_height_exp", "use_mct",
-                 "progression", "write_tlm", "sop_eph", "precinct_width_exp", "precinct_height_exp")]
+                 "progression", "write_tlm", "sop_eph", "precinct_width_exp", "precinct_height_exp", "tile_parts")]
 
 
 class SgnServerConfig(ctypes.Structure):

@@ -33,6 +33,7 @@ static int encode_with(const uint8_t* pixels, uint32_t width, uint32_t height, u
   p.sop_eph = o ? o->sop_eph != 0 : false;
   p.ppx = o ? o->precinct_width_exp : 0;
   p.ppy = o ? o->precinct_height_exp : 0;
+  p.tile_parts = o && o->tile_parts ? o->tile_parts : 1;
   // Code blocks up to 1024 wide or high with w h <= 4096 (exponents of 4).
   const uint32_t max_exp = 8;
   if (p.cbw_exp > max_exp || p.cbh_exp > max_exp || p.cbw_exp + p.cbh_exp > 8 || p.progression < 0 ||

@@ -865,7 +865,20 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
       }
     }
   std::sort(order.begin(), order.end(), [](const Pk& a, const Pk& b) { return a.key < b.key; });
-  for (const Pk& k : order) packet(k.c, k.r, k.l, k.p);
+  std::vector<size_t> pkt_end;  // end offset in `tile` of each packet
+  for (const Pk& k : order) {
+    packet(k.c, k.r, k.l, k.p);
+    pkt_end.push_back(tile.size());
+  }
+  // Tile-parts: the packets in order, cut into nearly equal runs.
+  const uint32_t NT = std::max<uint32_t>(1, std::min<uint32_t>(P.tile_parts, (uint32_t)std::max<size_t>(1, order.size())));
+  if (NT > 255) return -2;
+  std::vector<size_t> part_end(NT);
+  for (uint32_t t = 0; t < NT; ++t) {
+    const size_t k = (size_t)((uint64_t)order.size() * (t + 1) / NT);
+    part_end[t] = k == 0 ? 0 : pkt_end[k - 1];
+  }
+  part_end[NT - 1] = tile.size();
   // Codestream.
   out.clear();
   out.push_back(0xFF); out.push_back(0x4F);  // SOC
@@ -912,23 +925,32 @@ int encode(const uint8_t* pixels, const EncodeParams& P, std::vector<uint8_t>& o
       out.push_back((uint8_t)((bd + 2) << 3));
     }
   }
-  uint32_t psot = 12 + 2 + (uint32_t)tile.size();
+  auto psot = [&](uint32_t t) {
+    const size_t b = t == 0 ? 0 : part_end[t - 1];
+    return (uint32_t)(12 + 2 + (part_end[t] - b));
+  };
   if (P.write_tlm) {
+    // One entry per tile-part: Stlm 0x60 = 16-bit Ttlm, 32-bit Ptlm.
     out.push_back(0xFF); out.push_back(0x55);
-    put16(out, 10);
+    put16(out, 4 + 6 * NT);
     out.push_back(0);
-    out.push_back(0x22);
-    put16(out, 0);
-    put32(out, psot);
+    out.push_back(0x60);
+    for (uint32_t t = 0; t < NT; ++t) {
+      put16(out, 0);
+      put32(out, psot(t));
+    }
   }
-  out.push_back(0xFF); out.push_back(0x90);  // SOT
-  put16(out, 10);
-  put16(out, 0);
-  put32(out, psot);
-  out.push_back(0);
-  out.push_back(1);
-  out.push_back(0xFF); out.push_back(0x93);  // SOD
-  out.insert(out.end(), tile.begin(), tile.end());
+  for (uint32_t t = 0; t < NT; ++t) {
+    out.push_back(0xFF); out.push_back(0x90);  // SOT
+    put16(out, 10);
+    put16(out, 0);
+    put32(out, psot(t));
+    out.push_back((uint8_t)t);   // TPsot
+    out.push_back((uint8_t)NT);  // TNsot
+    out.push_back(0xFF); out.push_back(0x93);  // SOD
+    const size_t b = t == 0 ? 0 : part_end[t - 1];
+    out.insert(out.end(), tile.begin() + (long)b, tile.begin() + (long)part_end[t]);
+  }
   out.push_back(0xFF); out.push_back(0xD9);  // EOC
   return 0;
 }

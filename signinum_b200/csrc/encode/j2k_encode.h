@@ -25,6 +25,8 @@ struct EncodeParams {
   // Precinct exponents (PPx, PPy) of every resolution, 1..15; 0 = one
   // precinct per resolution (no precinct partition signalled).
   uint32_t ppx = 0, ppy = 0;
+  // Tile-parts the packets are split into (at packet boundaries), >= 1.
+  uint32_t tile_parts = 1;
 };
 // One classic code block: its codeword segments back to back, each
 // segment's length and coding-pass count, and the block's zero bit-planes.

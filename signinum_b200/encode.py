@@ -53,25 +53,27 @@ def _encode(call, cap: int) -> bytes:
 def encode_lossless(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int,
                     levels: int = 5, cb_exp: int = 4, use_mct: bool = True, progression: int = 0,
                     sop_eph: bool = False, write_tlm: bool = False, cb_exp_h: int | None = None,
-                    precincts: tuple = (0, 0)) -> bytes:
+                    precincts: tuple = (0, 0), tile_parts: int = 1) -> bytes:
     """Encodes interleaved samples (u8, or little-endian u16 for depths > 8).
     precincts: (PPx, PPy) exponents of every resolution, (0, 0) for one
-    precinct per resolution."""
+    precinct per resolution; tile_parts: tile-parts the packets are split
+    into."""
     px = np.ascontiguousarray(pixels)
     opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression,
-                            int(write_tlm), int(sop_eph), precincts[0], precincts[1])
+                            int(write_tlm), int(sop_eph), precincts[0], precincts[1], tile_parts)
     return _encode(lambda out, cap, n: _native.encode_lib().sgn_j2k_encode_lossless(
         px.ctypes.data, width, height, components, bit_depth, ctypes.byref(opts), out, cap, n), px.nbytes * 2 + 65536)
 
 
 def encode_irreversible(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int,
                         relative_step: float = 1.0 / 256, levels: int = 5, cb_exp: int = 4, use_mct: bool = True,
-                        progression: int = 0, cb_exp_h: int | None = None, precincts: tuple = (0, 0)) -> bytes:
+                        progression: int = 0, cb_exp_h: int | None = None, precincts: tuple = (0, 0),
+                        tile_parts: int = 1) -> bytes:
     """Lossy 9/7 codestream (ICT, scalar expounded quantisation) for the
     irreversible decode path's tests; same sample layout as encode_lossless."""
     px = np.ascontiguousarray(pixels)
     opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression, 0, 0,
-                            precincts[0], precincts[1])
+                            precincts[0], precincts[1], tile_parts)
     return _encode(lambda out, cap, n: _native.encode_lib().sgn_j2k_encode_irreversible(
         px.ctypes.data, width, height, components, bit_depth, ctypes.byref(opts), relative_step, out, cap, n),
         px.nbytes * 2 + 65536)
@@ -80,13 +82,13 @@ def encode_irreversible(pixels: np.ndarray, width: int, height: int, components:
 def encode_classic(pixels: np.ndarray, width: int, height: int, components: int, bit_depth: int, style: int = 0,
                    irreversible: bool = False, relative_step: float = 1.0 / 256, levels: int = 5, cb_exp: int = 4,
                    use_mct: bool = True, progression: int = 0, cb_exp_h: int | None = None, layers: int = 1,
-                   precincts: tuple = (0, 0)) -> bytes:
+                   precincts: tuple = (0, 0), tile_parts: int = 1) -> bytes:
     """Classic (EBCOT Tier-1) codestream with code-block style bits `style`,
     lossless 5/3 or (irreversible) lossy 9/7, `layers` quality layers; same
     sample layout as encode_lossless."""
     px = np.ascontiguousarray(pixels)
     opts = SgnEncodeOptions(levels, cb_exp, cb_exp if cb_exp_h is None else cb_exp_h, int(use_mct), progression, 0, 0,
-                            precincts[0], precincts[1])
+                            precincts[0], precincts[1], tile_parts)
     return _encode(lambda out, cap, n: _native.encode_lib().sgn_j2k_encode_classic(
         px.ctypes.data, width, height, components, bit_depth, ctypes.byref(opts), style, int(irreversible),
         relative_step, layers, out, cap, n), px.nbytes * 3 + 65536)

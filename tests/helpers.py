@@ -57,9 +57,10 @@ def wide_block_codestream(rng, cb, max_w=300, max_h=140):
 
 def precinct_codestream(rng, kind, max_side=200):
     """A seeded codestream cut into precincts of 2^PPx x 2^PPy (2 .. 256) in
-    any progression: kind "ht" (lossless), "classic" (lossless, 1-3 layers,
-    random code-block styles) or "lossy" (9/7).  Returns the codestream, the
-    pixels, width, height and components."""
+    any progression, its packets split over 1-6 tile-parts: kind "ht"
+    (lossless, with or without TLM), "classic" (lossless, 1-3 layers, random
+    code-block styles) or "lossy" (9/7).  Returns the codestream, the pixels,
+    width, height and components."""
     w = int(rng.integers(1, max_side))
     h = int(rng.integers(1, max_side))
     comps = int(rng.choice([1, 3]))
@@ -68,10 +69,10 @@ def precinct_codestream(rng, kind, max_side=200):
     cbw = int(rng.integers(0, 5))
     cbh = min(int(rng.integers(0, 5)), 8 - cbw)
     kw = dict(levels=int(rng.integers(0, 6)), cb_exp=cbw, cb_exp_h=cbh, progression=int(rng.integers(0, 5)),
-              precincts=pp)
+              precincts=pp, tile_parts=int(rng.integers(1, 7)))
     flat = px.reshape(-1)
     if kind == "ht":
-        cs = encode.encode_lossless(flat, w, h, comps, 8, **kw)
+        cs = encode.encode_lossless(flat, w, h, comps, 8, write_tlm=bool(rng.integers(0, 2)), **kw)
     elif kind == "classic":
         cs = encode.encode_classic(flat, w, h, comps, 8, style=int(rng.choice([0, 0x01, 0x04, 0x05, 0x2F])),
                                    layers=int(rng.integers(1, 4)), **kw)

@@ -91,7 +91,8 @@ def test_wide_code_blocks_match_oracle(cb):
 @pytest.mark.parametrize("kind", ["ht", "classic", "lossy"])
 def test_precinct_partitions_match_oracle(kind):
     """Codestreams cut into precincts (2 .. 256 samples a side) in every
-    progression: HT, multi-layer classic and lossy 9/7 code blocks."""
+    progression, over several tile-parts: HT, multi-layer classic and lossy
+    9/7 code blocks."""
     rng = np.random.default_rng({"ht": 4500, "classic": 4501, "lossy": 4502}[kind])
     for _ in range(12):
         cs, px, w, h, comps = precinct_codestream(rng, kind)

@@ -89,8 +89,9 @@ def test_wide_code_blocks_roundtrip_through_oracle(cb):
 @pytest.mark.parametrize("kind", ["ht", "classic"])
 def test_precinct_partitions_roundtrip_through_oracle(kind):
     """Resolutions cut into precincts (code blocks clipped to them, packets
-    per precinct in every progression, the position-driven ones included)
-    decode losslessly: the encoder's packet order and the oracle's agree."""
+    per precinct in every progression, the position-driven ones included,
+    split over tile-parts) decode losslessly: the encoder's packet order and
+    the oracle's agree."""
     rng = np.random.default_rng({"ht": 4300, "classic": 4301}[kind])
     for _ in range(30):
         cs, px, w, h, comps = precinct_codestream(rng, kind)
