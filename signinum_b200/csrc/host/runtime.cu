@@ -172,6 +172,12 @@ bool is_pinned(const void* p) {
 // take blocks in.  Exact order inside a bucket does not matter.
 constexpr uint32_t kLenBuckets = 64;
 inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<uint32_t>(lcup >> 6, kLenBuckets - 1); }
+// HT job order: blocks the MagSgn pass decodes one per warp, then the narrow
+// ones it decodes two per warp (at most 32 wide, no refinement passes), each
+// group by coded length, longest first.
+constexpr uint32_t kHtBuckets = 2 * kLenBuckets;
+inline bool pairable(const CodeBlock& cb) { return cb.w <= 32 && cb.passes <= 1; }
+inline uint32_t ht_bucket(const CodeBlock& cb) { return (pairable(cb) ? kLenBuckets : 0) + len_bucket(cb.lcup); }
 // Classic blocks by coding passes (0 .. 94), most passes first.
 constexpr uint32_t kPassBuckets = 96;
 inline uint32_t pass_bucket(uint32_t passes) { return kPassBuckets - 1 - std::min<uint32_t>(passes, kPassBuckets - 1); }
@@ -249,8 +255,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // ceil(w/2) x ceil(h/2) words in the symbol scratch.
   struct TileHt {
     uint64_t sym = 0;
-    uint32_t nref = 0, ms_words = 8, max_w = 1;
-    uint32_t hist[kLenBuckets];
+    uint32_t nref = 0, ms_words = 8, ms_half = 0, max_w = 1;
+    uint32_t hist[kHtBuckets];
     uint32_t ncls = 0, nseg = 0, slot = 0;  // classic tiles
     uint64_t gather = 0;                    // multi-layer classic tiles
     uint32_t chist[kPassBuckets];           // classic blocks per coding-pass count
@@ -258,7 +264,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   std::vector<TileHt> th(n);
   ctx->workers->parallel_for(n, [&](size_t i) {
     TileHt& t = th[i];
-    std::fill(t.hist, t.hist + kLenBuckets, 0u);
+    std::fill(t.hist, t.hist + kHtBuckets, 0u);
     std::fill(t.chist, t.chist + kPassBuckets, 0u);
     if (plan->status[i] != SGN_OK) return;
     if (work[i].L->classic) {
@@ -272,7 +278,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       return;
     }
     for (const CodeBlock& cb : work[i].L->blocks) {
-      ++t.hist[len_bucket(cb.lcup)];
+      ++t.hist[ht_bucket(cb)];
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
       if (!cb.passes) continue;
       t.sym += sym_words(cb.w, cb.h);
@@ -280,15 +286,19 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       if (cb.lcup >= 2) {
         const uint8_t* seg = datas[i] + cb.cleanup_off;
         uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
-        if (scup <= cb.lcup) t.ms_words = std::max<uint32_t>(t.ms_words, (cb.lcup - scup + 15) / 4 + 2);
+        if (scup <= cb.lcup) {
+          const uint32_t words = (cb.lcup - scup + 15) / 4 + 2;
+          t.ms_words = std::max(t.ms_words, words);
+          if (pairable(cb)) t.ms_half = std::max(t.ms_half, words);
+        }
       }
     }
   });
   // Bucket-major, tile-minor start positions; symbol and refinement offsets.
   std::vector<uint64_t> sym_off(n, 0);
-  std::vector<uint32_t> ref_off(n, 0), start((size_t)kLenBuckets * n, 0);
+  std::vector<uint32_t> ref_off(n, 0), start((size_t)kHtBuckets * n, 0);
   uint64_t sym_total = 0;
-  uint32_t nht = 0, nref = 0, ms_words = 8, max_w = 1;
+  uint32_t nht = 0, nref = 0, ms_words = 8, ms_half = 0, max_w = 1;
   // Classic jobs: bucket-major by coding passes (most first), tile-minor, so
   // that the lanes of a warp take blocks of similar work and the longest
   // blocks start first.
@@ -314,18 +324,22 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     ref_off[i] = nref;
     nref += th[i].nref;
     ms_words = std::max(ms_words, th[i].ms_words);
+    ms_half = std::max(ms_half, th[i].ms_half);
     max_w = std::max(max_w, th[i].max_w);
   }
-  for (uint32_t b = 0; b < kLenBuckets; ++b)
+  for (uint32_t b = 0; b < kHtBuckets; ++b) {
+    if (b == kLenBuckets) plan->nsingle = nht;
     for (size_t i = 0; i < n; ++i) {
       start[(size_t)b * n + i] = nht;
       nht += th[i].hist[b];
     }
+  }
   plan->nht = nht;
-  plan->ms_words = ms_words;
+  // Each warp's bit array holds one block, or two narrow ones in its halves.
+  plan->ms_words = std::max(ms_words, 2 * ms_half);
   plan->max_w = max_w;
   plan->nref = nref;
-  if (ht_magsgn_smem_bytes(ms_words, max_w) > 227 * 1024)
+  if (ht_magsgn_smem_bytes(plan->ms_words, max_w) > 227 * 1024)
     return set_error(SGN_ERR_UNSUPPORTED, "code-block segment too long for the MagSgn staging buffer");
   if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
     return cuda_status(e, "symbol scratch");
@@ -526,13 +540,13 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       }
       return;
     }
-    uint32_t cursor[kLenBuckets];
-    for (uint32_t b = 0; b < kLenBuckets; ++b) cursor[b] = start[(size_t)b * n + i];
+    uint32_t cursor[kHtBuckets];
+    for (uint32_t b = 0; b < kHtBuckets; ++b) cursor[b] = start[(size_t)b * n + i];
     uint64_t sym = sym_off[i];
     uint32_t rk = ref_off[i];
     for (const CodeBlock& cb : L.blocks) {
       const Band& b = L.bands[cb.band];
-      const uint32_t pos = cursor[len_bucket(cb.lcup)]++;
+      const uint32_t pos = cursor[ht_bucket(cb)]++;
       HtJob& j = ht[pos];
       std::memset(&j, 0, sizeof(j));
       j.src = in_off[i] + cb.cleanup_off;
@@ -694,7 +708,8 @@ sgn_status execute(sgn_plan* p, cudaStream_t s) {
   if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads)) != cudaSuccess)
     return cuda_status(e, "HT VLC launch");
   if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
-                            s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas)) != cudaSuccess)
+                            s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas, p->nsingle)) !=
+      cudaSuccess)
     return cuda_status(e, "HT MagSgn launch");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
@@ -929,7 +944,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   chk(launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads));
   chk(cudaEventRecord(ev[1], s));
   chk(launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s,
-                       c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas));
+                       c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas, p->nsingle));
   chk(cudaEventRecord(ev[2], s));
   chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
   chk(launch_classic_blocks(p, s));
@@ -1027,7 +1042,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
       cudaError_t x = cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s);
       if (x != cudaSuccess) return x;
       return launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words,
-                              p->max_w, s, m.warps, m.gran ? p->d_queue : nullptr, m.gran, ctas);
+                              p->max_w, s, m.warps, m.gran ? p->d_queue : nullptr, m.gran, ctas, p->nsingle);
     }, e);
     if (m.warps == 8 && m.gran == 0) rep.ms_ms_default = ms;
     if (e == cudaSuccess && ms < best_ms) best_ms = ms, ms_warps = m.warps, ms_gran = m.gran;

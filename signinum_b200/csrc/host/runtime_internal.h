@@ -185,6 +185,7 @@ struct sgn_plan {
   PackJob* d_pack = nullptr;
   uint32_t* d_status = nullptr;
   uint32_t nht = 0, ms_words = 8, max_w = 1, nref = 0, npack = 0, pack_ctas = 0;
+  uint32_t nsingle = 0;  // HT jobs before the narrow ones the MagSgn pass decodes two per warp
   // Reversible pack jobs grouped by kernel variant (pack_variant): variant v
   // has npack_v[v] jobs from d_pack + pack_begin[v] covering pack_units_v[v]
   // units; npack and pack_ctas are their totals.  Pack jobs of irreversible

@@ -684,6 +684,178 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
 }
 }  // namespace
 
+// Narrow blocks (at most 32 wide: 16 quads a row) would leave half of a
+// warp idle, so a warp takes two of them, one per half-warp (lanes 0-15 and
+// 16-31).  The functions below are unstuff_magsgn and magsgn_rows for that
+// case: every shuffle, ballot and scan runs on all 32 lanes with the
+// half-warp as its segment, and both halves run the longer block's loop
+// trip counts (a half past its own work idles), so no warp-synchronous
+// operation sits in a branch that one half skips.
+
+// unstuff_magsgn for the calling half-warp's stream: 64 bytes per step.
+__device__ uint32_t unstuff_half(const uint8_t* src, uint32_t len, uint32_t* W, uint32_t nwords) {
+  const uint32_t lane = threadIdx.x & 31, gl = lane & 15, gsh = lane & 16;
+  for (uint32_t i = gl; i < nwords; i += 16) W[i] = 0;
+  __syncwarp();
+  const uint32_t steps = (len + 63) / 64;
+  const uint32_t nsteps = max(steps, __shfl_xor_sync(0xFFFFFFFFu, steps, 16));
+  uint32_t ff_total = 0;  // 0xFF bytes among bytes [0, base)
+  uint32_t prev_ff = 0;   // byte base - 1 is 0xFF
+  for (uint32_t k = 0; k < nsteps; ++k) {
+    const uint32_t base = 64 * k, i0 = base + 4 * gl;
+    uint32_t x = 0;
+    if (i0 < len) {
+      const uintptr_t addr = (uintptr_t)(src + i0);
+      const uint32_t* wp = reinterpret_cast<const uint32_t*>(addr & ~(uintptr_t)3);
+      const uint32_t sh = (uint32_t)(addr & 3);
+      const uint32_t nvalid = min(4u, len - i0);
+      const uint32_t lo = __ldg(wp);
+      const uint32_t hi = sh + nvalid > 4 ? __ldg(wp + 1) : 0u;
+      x = __funnelshift_r(lo, hi, 8 * sh);
+      if (nvalid < 4) x &= 0xFFFFFFFFu >> (8 * (4 - nvalid));
+    }
+    const uint32_t fm = i0 < len ? __vcmpeq4(x, 0xFFFFFFFFu) : 0u;
+    const uint32_t f0 = fm & 1, f1 = (fm >> 8) & 1, f2 = (fm >> 16) & 1, f3 = (fm >> 24) & 1;
+    const uint32_t b0 = (__ballot_sync(0xFFFFFFFFu, f0) >> gsh) & 0xFFFFu;
+    const uint32_t b1 = (__ballot_sync(0xFFFFFFFFu, f1) >> gsh) & 0xFFFFu;
+    const uint32_t b2 = (__ballot_sync(0xFFFFFFFFu, f2) >> gsh) & 0xFFFFu;
+    const uint32_t b3 = (__ballot_sync(0xFFFFFFFFu, f3) >> gsh) & 0xFFFFu;
+    const uint32_t xn = __shfl_down_sync(0xFFFFFFFFu, x, 1, 16);
+    uint32_t pf = __shfl_up_sync(0xFFFFFFFFu, f3, 1, 16);
+    if (base < len) {
+      if (base + 64 <= len && !prev_ff && (b0 | b1 | b2 | b3) == 0) {
+        const uint32_t P = 8 * base - ff_total;
+        const uint32_t s = P & 31, wb = P >> 5;
+        if (gl < 15) W[wb + gl + 1] = __funnelshift_l(x, xn, s);
+        if (gl == 0) atomicOr(&W[wb], x << s);
+        if (gl == 15 && s) atomicOr(&W[wb + 16], x >> (32 - s));
+      } else {
+        const uint32_t lt = (1u << gl) - 1;
+        const uint32_t F = ff_total + __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
+        if (gl == 0) pf = prev_ff;
+        const uint32_t ffb[4] = {F - pf, F, F + f0, F + f0 + f1};
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          if (i0 + j < len) {
+            const uint32_t pos = 8 * (i0 + j) - ffb[j];
+            const uint32_t byte = (x >> (8 * j)) & 0xFF;
+            atomicOr(&W[pos >> 5], byte << (pos & 31));
+            if ((pos & 31) > 24) atomicOr(&W[(pos >> 5) + 1], byte >> (32 - (pos & 31)));
+          }
+        }
+      }
+      ff_total += __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
+      const uint32_t last = min(base + 64, len) - 1 - base;  // last byte of the step
+      const uint32_t lb = last >> 2, lj = last & 3;
+      const uint32_t lf = lj == 0 ? b0 : lj == 1 ? b1 : lj == 2 ? b2 : b3;
+      prev_ff = (lf >> lb) & 1;
+    }
+  }
+  const uint32_t end_bits = len ? 8 * len - (ff_total - prev_ff) : 0;
+  __syncwarp();
+  for (uint32_t wi = gl; wi < nwords; wi += 16) {
+    uint32_t lo = wi * 32;
+    if (lo >= end_bits) W[wi] = 0xFFFFFFFFu;
+    else if (lo + 32 > end_bits) W[wi] |= 0xFFFFFFFFu << (end_bits - lo);
+  }
+  __syncwarp();
+  return end_bits;
+}
+
+// magsgn_rows<true, false> for the calling half-warp's block (live) over
+// hmax rows, the taller of the two blocks' heights.  Returns true on the
+// half's lanes when its stream is invalid.
+__device__ bool magsgn_rows_half(const HtJob& job, bool live, const uint32_t* W, uint32_t ms_words, uint32_t hmax,
+                                 const uint32_t* __restrict__ sym, int32_t* __restrict__ dst) {
+  const uint32_t lane = threadIdx.x & 31, gl = lane & 15, gsh = lane & 16;
+  const uint32_t w = live ? job.w : 0, h = live ? job.h : 0, stride = job.stride;
+  const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
+  // As in magsgn_rows: clamped window reads stay in the half's words.
+  const uint32_t lim = live ? 32 * (ms_words - 3) : 0;
+  const bool pairs = ((job.dst | stride) & 1) == 0;
+  const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
+  uint32_t e_left = 0, e_right = 0, rowbase = 0;
+  bool bad = false;
+  for (uint32_t y = 0, r = 0; y < hmax; y += 2, ++r) {
+    const bool initial = y == 0, second = y + 1 < h;
+    const uint32_t q = gl;
+    const bool active = y < h && q < nq;
+    const uint32_t s = active ? sym[(size_t)r * qs + q] : 0;
+    const uint32_t inf = s & 0xFFFF;
+    uint32_t U = s >> 16;
+    if (!initial) {
+      uint32_t l = __shfl_up_sync(0xFFFFFFFFu, e_right, 1, 16);
+      uint32_t rr = __shfl_down_sync(0xFFFFFFFFu, e_left, 1, 16);
+      if (gl == 0) l = 0;
+      if (gl == 15) rr = 0;
+      const uint32_t e = max(max(l, e_left), max(e_right, rr));
+      uint32_t gamma = inf & 0xF0;
+      gamma &= gamma - 0x10;
+      if (active) U += gamma != 0 ? max(e, 2u) - 1 : 1;
+    }
+    bad |= active && U > mmsbp2;
+    uint32_t m[4], tot = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
+      tot += m[i];
+    }
+    uint32_t inc = tot;
+#pragma unroll
+    for (int d = 1; d < 16; d <<= 1) {
+      uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d, 16);
+      if (gl >= (uint32_t)d) inc += v;
+    }
+    const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 15, 16);
+    const uint32_t off = rowbase + inc - tot;
+    rowbase += chunk_bits;
+    const uint32_t cs[4] = {0u, m[0], m[0] + m[1], m[0] + m[1] + m[2]};
+    uint32_t lo, hi;
+    {
+      const uint32_t o = min(off, lim), wi = o >> 5, sh = o & 31;
+      const uint32_t a0 = W[wi], a1 = W[wi + 1], a2 = W[wi + 2];
+      lo = __funnelshift_r(a0, a1, sh);
+      hi = __funnelshift_r(a1, a2, sh);
+    }
+    uint32_t msv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) msv[i] = cs[i] < 32 ? __funnelshift_r(lo, hi, cs[i]) : hi >> (cs[i] - 32);
+    if (tot >= 64) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) msv[i] = bits_at(W, ms_words, off + cs[i]);
+    }
+    uint32_t val[4], E[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const bool sig = (inf >> (4 + i)) & 1;
+      const uint32_t mn = m[i];
+      const uint32_t mask = __funnelshift_lc(0xFFFFFFFFu, 0u, mn);
+      const uint32_t v = (msv[i] & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
+      val[i] = sig ? (msv[i] << 31) | ((v + 2) << (p - 1)) : 0u;
+      E[i] = sig ? 32 - __clz(v) : 0u;
+    }
+    if (active) {
+      int32_t* row0 = dst + (size_t)y * stride;
+      int32_t* row1 = row0 + stride;
+      const uint32_t x = 2 * q;
+      if (pairs && x + 1 < w) {
+        *reinterpret_cast<int2*>(row0 + x) = make_int2(to_i32(val[0], nbp), to_i32(val[2], nbp));
+        if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(to_i32(val[1], nbp), to_i32(val[3], nbp));
+      } else {
+        row0[x] = to_i32(val[0], nbp);
+        if (second) row1[x] = to_i32(val[1], nbp);
+        if (x + 1 < w) {
+          row0[x + 1] = to_i32(val[2], nbp);
+          if (second) row1[x + 1] = to_i32(val[3], nbp);
+        }
+      }
+    }
+    e_left = active ? E[1] : 0;
+    e_right = active && 2 * q + 1 < w ? E[3] : 0;
+  }
+  return ((__ballot_sync(0xFFFFFFFFu, bad) >> gsh) & 0xFFFFu) != 0;
+}
+
 // Pass 2: one warp per code block decodes magnitudes and signs
 // (decode_magnitude_sign_phase, ht_block_decode.rs:1435-1561).  Per quad row
 // the lanes take one quad each: the exponent bound kappa comes from the four
@@ -745,6 +917,50 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
   __syncwarp();  // the warp's shared buffers are reused by its next block
 }
 
+// Two narrow blocks, jobs[a] on lanes 0-15 and jobs[b] on lanes 16-31 (b ==
+// UINT32_MAX: none), each with half of the warp's bit array (half_words
+// words); both at most 32 wide with no refinement passes (the host orders
+// such blocks after the others).  Same results as magsgn_block on each.
+__device__ void magsgn_pair(const HtJob* __restrict__ jobs, uint32_t a, uint32_t b, const uint8_t* __restrict__ arena,
+                            const uint32_t* __restrict__ symbols, int32_t* __restrict__ coef,
+                            uint32_t* __restrict__ tile_status, uint32_t half_words, uint32_t* W) {
+  const uint32_t lane = threadIdx.x & 31, g = lane >> 4, gl = lane & 15;
+  const bool present = g == 0 || b != 0xFFFFFFFFu;
+  const HtJob job = jobs[present ? (g ? b : a) : a];
+  uint32_t* Wg = W + g * half_words;
+  int32_t* dst = coef + job.dst;
+  const uint32_t* sym = symbols + job.sym;
+  const uint8_t* src = arena + job.src;
+  const bool coded = present && job.passes != 0;
+  bool ok = coded;
+  if (ok) {
+    prefetch_l2_range(src, job.lcup, gl, 16);
+    prefetch_l2_range(sym, (size_t)sym_row_stride(job.w) * ((job.h + 1) / 2) * 4, gl, 16);
+    ok = sym[0] != kSymFailed;
+  }
+  uint32_t ms_len = 0, words = 0;
+  if (ok) {
+    const uint32_t lcup = job.lcup;
+    const uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
+    ok = (lcup - scup + 15) / 4 + 2 <= half_words;
+    if (ok) {
+      ms_len = lcup - scup;
+      words = (ms_len + 15) / 4 + 2;
+    }
+  }
+  unstuff_half(src, ms_len, Wg, words);
+  const uint32_t hh = ok ? job.h : 0;
+  const uint32_t hmax = max(hh, __shfl_xor_sync(0xFFFFFFFFu, hh, 16));
+  const bool bad = magsgn_rows_half(job, ok, Wg, words, hmax, sym, dst);
+  if (present && (!ok || bad)) {
+    // No coded passes: zeros; an invalid stream: zeros and the tile's status.
+    for (uint32_t y = 0; y < job.h; ++y)
+      for (uint32_t x = gl; x < job.w; x += 16) dst[(size_t)y * job.stride + x] = 0;
+    if (coded && gl == 0) atomicOr(&tile_status[job.tile], kStatusDecode);
+  }
+  __syncwarp();  // the warp's shared buffers are reused by its next work item
+}
+
 }  // namespace
 
 // Pass 2: one warp per code block decodes magnitudes and signs
@@ -753,6 +969,10 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
 // a persistent grid whose warps take `gran` consecutive blocks at a time
 // from the device work queue (an atomic counter over the job table, which is
 // ordered by coded length, longest first).
+//
+// Work items: jobs [0, nsingle) one per warp; the narrow jobs after them
+// (at most 32 wide, no refinement passes) two per warp, item nsingle + k
+// taking jobs nsingle + 2k and nsingle + 2k + 1.
 template <bool QUEUE>
 __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
                                                                   const uint8_t* __restrict__ arena,
@@ -760,24 +980,32 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
                                                                   int32_t* __restrict__ coef,
                                                                   uint32_t* __restrict__ tile_status,
                                                                   uint32_t ms_words, uint32_t max_w, uint32_t* queue,
-                                                                  uint32_t gran) {
+                                                                  uint32_t gran, uint32_t nsingle) {
   extern __shared__ __align__(16) uint8_t smem[];
   const uint32_t nw = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t cols = max_w + 4;
   uint32_t* W = reinterpret_cast<uint32_t*>(smem) + (size_t)warp * ms_words;
   uint8_t* Ebase = smem + (size_t)nw * ms_words * 4 + (size_t)warp * 2 * cols;
+  const uint32_t nitems = nsingle + (njobs - nsingle + 1) / 2;
+  auto item = [&](uint32_t it) {
+    if (it < nsingle) {
+      magsgn_block(jobs[it], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+    } else {
+      const uint32_t a = nsingle + 2 * (it - nsingle);
+      magsgn_pair(jobs, a, a + 1 < njobs ? a + 1 : 0xFFFFFFFFu, arena, symbols, coef, tile_status, ms_words / 2, W);
+    }
+  };
   if constexpr (!QUEUE) {
-    const uint32_t j = blockIdx.x * nw + warp;
-    if (j < njobs) magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+    const uint32_t it = blockIdx.x * nw + warp;
+    if (it < nitems) item(it);
   } else {
     for (;;) {
       uint32_t base = 0;
       if (lane == 0) base = atomicAdd(queue, gran);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
-      if (base >= njobs) break;
-      const uint32_t end = min(base + gran, njobs);
-      for (uint32_t j = base; j < end; ++j)
-        magsgn_block(jobs[j], arena, symbols, coef, tile_status, ms_words, cols, W, Ebase);
+      if (base >= nitems) break;
+      const uint32_t end = min(base + gran, nitems);
+      for (uint32_t it = base; it < end; ++it) item(it);
     }
   }
 }
@@ -984,22 +1212,24 @@ cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* aren
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                              cudaStream_t stream, uint32_t warps, uint32_t* queue, uint32_t gran,
-                             uint32_t persistent_ctas) {
+                             uint32_t persistent_ctas, uint32_t nsingle) {
   if (njobs == 0) return cudaSuccess;
   if (warps == 0 || warps > kMsWarps) warps = kMsWarps;
+  nsingle = std::min(nsingle, njobs);
   size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, warps);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  uint32_t ctas = (njobs + warps - 1) / warps;
+  const uint32_t nitems = nsingle + (njobs - nsingle + 1) / 2;
+  uint32_t ctas = (nitems + warps - 1) / warps;
   if (queue) {
     if (gran == 0) gran = 1;
     ctas = std::max(1u, std::min(ctas, persistent_ctas));
   }
   if (queue)
     ht_magsgn_kernel<true><<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status,
-                                                               ms_words, max_w, queue, gran);
+                                                               ms_words, max_w, queue, gran, nsingle);
   else
     ht_magsgn_kernel<false><<<ctas, warps * 32, smem, stream>>>(jobs, njobs, arena, symbols, coef, tile_status,
-                                                                ms_words, max_w, nullptr, 0);
+                                                                ms_words, max_w, nullptr, 0, nsingle);
   return cudaGetLastError();
 }
 
@@ -1015,7 +1245,7 @@ cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* 
   cudaError_t e = launch_ht_vlc(jobs, njobs, arena, symbols, stream, kHtThreads);
   if (e != cudaSuccess) return e;
   return launch_ht_magsgn(jobs, njobs, arena, symbols, coef, tile_status, ms_words, max_w, stream, kMsWarps, nullptr,
-                          0, 0);
+                          0, 0, njobs);
 }
 
 cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8_t* arena, int32_t* coef,

@@ -40,13 +40,15 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps = 
 // unstuffed MagSgn capacity per block in 32-bit words; max_w: widest code
 // block of the launch.  With `queue` (a zeroed device counter) the MagSgn pass
 // runs as a persistent grid of at most persistent_ctas CTAs whose warps take
-// `gran` blocks per grab.
+// `gran` blocks per grab.  Jobs from nsingle on are narrow (at most 32 wide,
+// no refinement passes) and decode two per warp, each with half of the
+// warp's ms_words (default: none).
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                           cudaStream_t stream, uint32_t threads = 128);
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                              cudaStream_t stream, uint32_t warps = 8, uint32_t* queue = nullptr, uint32_t gran = 0,
-                             uint32_t persistent_ctas = 0);
+                             uint32_t persistent_ctas = 0, uint32_t nsingle = 0xFFFFFFFFu);
 cudaError_t ht_magsgn_occupancy(uint32_t ms_words, uint32_t max_w, uint32_t warps, int* ctas_per_sm);
 cudaError_t launch_ht_cleanup(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                               int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,

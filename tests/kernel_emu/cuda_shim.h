@@ -121,15 +121,24 @@ template <class T> inline T shfl_from(T v, int src_of_lane_fn_lane, bool ok) {
   g_warp->bar.arrive_and_wait();
   return r;
 }
-template <class T> inline T __shfl_up_sync(unsigned, T v, int d) {
+// Shuffles over segments of `width` lanes (a power of two, 32 by default):
+// a source outside the caller's segment leaves the caller's own value.
+template <class T> inline T __shfl_up_sync(unsigned, T v, int d, int width = 32) {
   const int lane = threadIdx.x & 31;
-  return shfl_from(v, lane - d, lane - d >= 0);
+  return shfl_from(v, lane - d, (lane & (width - 1)) - d >= 0);
 }
-template <class T> inline T __shfl_down_sync(unsigned, T v, int d) {
+template <class T> inline T __shfl_down_sync(unsigned, T v, int d, int width = 32) {
   const int lane = threadIdx.x & 31;
-  return shfl_from(v, lane + d, lane + d < 32);
+  return shfl_from(v, lane + d, (lane & (width - 1)) + d < width);
 }
-template <class T> inline T __shfl_sync(unsigned, T v, int src) { return shfl_from(v, src & 31, true); }
+template <class T> inline T __shfl_sync(unsigned, T v, int src, int width = 32) {
+  const int lane = threadIdx.x & 31;
+  return shfl_from(v, (lane & ~(width - 1)) + (src & (width - 1)), true);
+}
+template <class T> inline T __shfl_xor_sync(unsigned, T v, int m, int width = 32) {
+  const int lane = threadIdx.x & 31, src = lane ^ m;
+  return shfl_from(v, src & 31, (src & ~(width - 1)) == (lane & ~(width - 1)));
+}
 inline void __syncwarp() { g_warp->bar.arrive_and_wait(); }
 inline unsigned atomicAdd(unsigned* p, unsigned v) {
   unsigned o = __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);

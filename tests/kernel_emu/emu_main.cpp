@@ -27,7 +27,8 @@ alignas(16) uint8_t g_dyn_smem[232448];
 namespace sgn {
 void emu_tables();
 void emu_vlc(const HtJob*, uint32_t, const uint8_t*, uint32_t*);
-void emu_magsgn(const HtJob*, uint32_t, const uint8_t*, const uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t);
+void emu_magsgn(const HtJob*, uint32_t, const uint8_t*, const uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t,
+                uint32_t);
 void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t*, uint32_t*);
 void emu_idwt(bool, const IdwtJob*, uint32_t, uint32_t);
 void emu_pack(bool, int, const PackJob*, uint32_t, uint32_t);
@@ -142,7 +143,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
   std::vector<HtJob> jobs;
   std::vector<uint32_t> refine;
   uint64_t sym = 0;
-  uint32_t ms_words = 8, max_w = 1;
+  uint32_t ms_words = 8, ms_half = 0, max_w = 1;
+  auto pairable = [](const HtJob& j) { return j.w <= 32 && j.passes <= 1; };
   for (const CodeBlock& cb : T.blocks) {
     const Band& b = T.bands[cb.band];
     max_w = std::max<uint32_t>(max_w, cb.w);
@@ -167,7 +169,11 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     if (cb.passes && cb.lcup >= 2) {
       const uint8_t* seg = d.data() + cb.cleanup_off;
       uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
-      if (scup <= cb.lcup) ms_words = std::max<uint32_t>(ms_words, (cb.lcup - scup + 15) / 4 + 2);
+      if (scup <= cb.lcup) {
+        const uint32_t words = (cb.lcup - scup + 15) / 4 + 2;
+        ms_words = std::max(ms_words, words);
+        if (pairable(j)) ms_half = std::max(ms_half, words);
+      }
     }
     if (cb.passes && cb.lref && cb.ref_off != cb.cleanup_off + cb.lcup) printf("refinement not contiguous\n");
     jobs.push_back(j);
@@ -186,13 +192,22 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
     for (uint32_t y = 0; y < cb.h; ++y)
       for (uint32_t x = 0; x < cb.w; ++x) ref[j.dst + (size_t)y * b.w + x] = to_i32(buf[(size_t)y * cb.w + x], b.nbp);
   }
+  // The runtime's order: blocks decoded one per warp, then the narrow ones
+  // decoded two per warp, whose halves of the bit array must hold them.
+  std::stable_partition(jobs.begin(), jobs.end(), [&](const HtJob& j) { return !pairable(j); });
+  const uint32_t nsingle = (uint32_t)std::count_if(jobs.begin(), jobs.end(), [&](const HtJob& j) { return !pairable(j); });
+  refine.clear();
+  for (size_t k = 0; k < jobs.size(); ++k)
+    if (jobs[k].passes > 1) refine.push_back((uint32_t)k);
+  ms_words = std::max(ms_words, 2 * ms_half);
   std::vector<uint32_t> symbols(std::max<uint64_t>(sym, 1), 0xDEADBEEF);
   n = (uint32_t)jobs.size();
   launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols.data()); });
   const size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, 8);
   if (smem > sizeof(g_dyn_smem)) { printf("smem too large\n"); return 2; }
-  launch((n + 7) / 8, 256, [&] {
-    emu_magsgn(jobs.data(), n, arena.data(), symbols.data(), coef.data(), status.data(), ms_words, max_w);
+  const uint32_t nitems = nsingle + (n - nsingle + 1) / 2;
+  launch((nitems + 7) / 8, 256, [&] {
+    emu_magsgn(jobs.data(), n, arena.data(), symbols.data(), coef.data(), status.data(), ms_words, max_w, nsingle);
   });
   nr = (uint32_t)refine.size();
   if (nr) launch((nr + 63) / 64, 64, [&] { emu_refine(jobs.data(), refine.data(), nr, arena.data(), coef.data(), status.data()); });
