@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
-    ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000",
+    ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000,160000,200000",
                     help="c4: arrival rates, tiles/s")
     ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate")
     ap.add_argument("--slots", type=int, default=4, help="c4: batches in flight")

@@ -1048,6 +1048,11 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
       cb.passes = (uint8_t)passes;
       cb.cleanup_off = (uint32_t)bs.cleanup_off;
       cb.lcup = bs.lcup;
+      if ((uint64_t)bs.cleanup_off + bs.lcup <= len) {
+        const uint8_t* seg = data + bs.cleanup_off;
+        const uint32_t scup = ((uint32_t)seg[bs.lcup - 1] << 4) + (seg[bs.lcup - 2] & 0x0F);
+        if (scup <= bs.lcup) cb.ms_words = (uint16_t)std::min<uint32_t>((bs.lcup - scup + 15) / 4 + 2, 0xFFFFu);
+      }
       if (passes > 1) {
         cb.ref_off = (uint32_t)bs.ref_off;
         cb.lref = bs.lref;

@@ -50,6 +50,10 @@ struct CodeBlock {
   uint32_t ref_off;     // byte offset of the refinement segment (when lref > 0)
   uint32_t lref;
   uint8_t missing_msbs, passes;
+  // HT: 32-bit words of the unstuffed MagSgn stream the decode stages
+  // ((Lcup - Scup + 15) / 4 + 2, Scup from the segment's last two bytes);
+  // 0 when Scup exceeds Lcup or the block has no coded passes.
+  uint16_t ms_words = 0;
   uint32_t seg_begin = 0;  // classic: first entry in TileLayout::segments
   uint8_t nseg = 0;        // classic: codeword segments of the block
 };

@@ -283,14 +283,9 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       if (!cb.passes) continue;
       t.sym += sym_words(cb.w, cb.h);
       if (cb.passes > 1) ++t.nref;
-      if (cb.lcup >= 2) {
-        const uint8_t* seg = datas[i] + cb.cleanup_off;
-        uint32_t scup = ((uint32_t)seg[cb.lcup - 1] << 4) + (seg[cb.lcup - 2] & 0x0F);
-        if (scup <= cb.lcup) {
-          const uint32_t words = (cb.lcup - scup + 15) / 4 + 2;
-          t.ms_words = std::max(t.ms_words, words);
-          if (pairable(cb)) t.ms_half = std::max(t.ms_half, words);
-        }
+      if (cb.ms_words) {  // from the parse (cached layouts carry it)
+        t.ms_words = std::max<uint32_t>(t.ms_words, cb.ms_words);
+        if (pairable(cb)) t.ms_half = std::max<uint32_t>(t.ms_half, cb.ms_words);
       }
     }
   });

@@ -104,12 +104,15 @@ class Workers {
 struct PinnedBuffer {
   uint8_t* p = nullptr;
   size_t cap = 0;
+  // Grows geometrically: freeing pinned memory waits for the device, so a
+  // buffer reused by calls of slowly growing sizes must not be replaced on
+  // every call.
   cudaError_t ensure(size_t n) {
     if (n <= cap) return cudaSuccess;
+    const size_t c = std::max<size_t>(n, cap * 2);
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    size_t c = std::max<size_t>(n, cap * 2);
     cudaError_t e = cudaMallocHost((void**)&p, c);
     if (e == cudaSuccess) cap = c;
     return e;
