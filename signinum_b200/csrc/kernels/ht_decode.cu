@@ -13,7 +13,8 @@
 //  2. ht_magsgn_kernel: one warp per code block decodes magnitudes and signs,
 //     a quad per lane, with a warp prefix scan of per-quad bit counts over the
 //     block's unstuffed MagSgn stream staged in shared memory, and writes
-//     whole rows with coalesced stores.
+//     whole rows with coalesced stores; blocks at most 32 wide without
+//     refinement passes go two per warp, one per half-warp.
 // Refinement passes (SigProp/MagRef) run in ht_refine_kernel for the few
 // blocks that carry them.
 #include <algorithm>
