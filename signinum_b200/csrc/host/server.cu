@@ -310,6 +310,16 @@ sgn_status sgn_server_create(sgn_ctx* ctx, const sgn_server_config* config, sgn_
     if (e == cudaSuccess) e = cudaFreeAsync(warm, sv->free_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(sv->free_stream);
   }
+  // Pinned staging for each slot's job tables, sized once for a full batch
+  // (about 64 bytes per 1024 decoded samples: an HT job per 32x32 block and
+  // the smaller IDWT and pack tables), so that growing it (pinning memory,
+  // which waits for the device) does not land between batches.
+  if (e == cudaSuccess) {
+    const uint64_t samples = sv->cfg.max_batch_samples ? sv->cfg.max_batch_samples : (96ull << 20);
+    const size_t bytes = (size_t)std::min<uint64_t>(samples / 1024 * 64 + (1u << 20), 64ull << 20);
+    for (auto& sl : sv->slots)
+      if (e == cudaSuccess) e = sl.staging.ensure(bytes);
+  }
   if (e != cudaSuccess) {
     sgn_status st = cuda_status(e, "server set-up");
     for (auto& sl : sv->slots) {
