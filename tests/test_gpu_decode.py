@@ -13,7 +13,7 @@ from oracle import oracle
 from signinum_b200 import (BackendKind, BackendRequest, Codec, CudaSession, Downscale, Error, J2kDecoder, PixelFormat,
                            Rect, TileBatchError, encode)
 from signinum_b200.j2k_cuda import _request
-from tests.helpers import WIDE_BLOCKS, precinct_codestream, random_codestream, wide_block_codestream
+from tests.helpers import WIDE_BLOCKS, precinct_codestream, random_codestream, random_tile, wide_block_codestream
 
 pytestmark = pytest.mark.gpu
 
@@ -170,6 +170,59 @@ def test_corrupt_code_block_is_an_error_not_a_fault():
         except oracle.OracleError:
             return
         assert got == want
+
+
+@pytest.mark.parametrize("seed", range(2))
+@pytest.mark.parametrize("where", ["magsgn", "vlc"])
+def test_damaged_narrow_blocks_stay_in_their_tile(seed, where):
+    """Code blocks at most 32 wide decode two per warp, and the two may come
+    from different tiles of the batch.  Damage in a tile's MagSgn bits must
+    give the oracle's (different) values; damage in its VLC bits must fail
+    that tile alone; the tiles decoded beside it must come out exact."""
+    from signinum_b200.plan import Plan
+
+    rng = np.random.default_rng(4700 + seed)
+    pixels, inputs = [], []
+    for _ in range(5):
+        px = random_tile(rng, 96, 80, 3, 8, 1)
+        pixels.append(px)
+        inputs.append(encode.encode_lossless(px.reshape(-1), 96, 80, 3, 8, levels=2, cb_exp=3))
+    # Damage the cleanup segments of some of tile 2's coded blocks (packet
+    # headers intact): near the start (MagSgn bits) or near the end (VLC).
+    import ctypes
+
+    from signinum_b200 import _native
+    from signinum_b200._native import SgnHtBlock
+
+    lib = _native.cuda_lib()
+    arr = np.frombuffer(inputs[2], np.uint8)
+    count, elems = ctypes.c_size_t(), ctypes.c_size_t()
+    lib.sgn_j2k_ht_block_table(arr.ctypes.data, arr.nbytes, None, 0, ctypes.byref(count), ctypes.byref(elems))
+    blocks = (SgnHtBlock * count.value)()
+    assert lib.sgn_j2k_ht_block_table(arr.ctypes.data, arr.nbytes, blocks, count.value, ctypes.byref(count),
+                                      ctypes.byref(elems)) == 0
+    coded = [b for b in blocks if b.passes == 1 and b.lcup >= 16 and b.w <= 32]
+    assert coded
+    cs = bytearray(inputs[2])
+    for b in coded[:: max(1, len(coded) // 8)]:
+        cs[b.src + (1 if where == "magsgn" else b.lcup - 4)] ^= 0x5A
+    inputs[2] = bytes(cs)
+    plan = Plan(inputs, PixelFormat.Rgb8)
+    plan.execute_async()
+    _, per = plan.wait()
+    for i in (0, 1, 3, 4):
+        assert per[i] == 0
+        assert plan.download(i) == pixels[i].tobytes()
+    if where == "magsgn":
+        want = cpu(inputs[2], PixelFormat.Rgb8)[0]
+        assert want != pixels[2].tobytes()
+        assert per[2] == 0
+        assert plan.download(2) == want
+    else:
+        with pytest.raises(oracle.OracleError):
+            cpu(inputs[2], PixelFormat.Rgb8)
+        assert per[2] in (3, 4)
+    plan.destroy()
 
 
 def test_unsupported_format_rejected_before_device_work():
