@@ -378,7 +378,10 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
         j.ll_band = r == 1 ? 1 : 0;
         j.step[0] = L.bands[b0].step;
         for (uint32_t k = 0; k < 3; ++k) j.step[1 + k] = L.bands[b0 + 1 + (r - 1) * 3 + k].step;
-        if (!L.reversible) j.seg *= 2;  // 9/7 units re-read seven rows: longer segments
+        // 9/7 units re-read seven rows: longer segments, except on levels of
+        // 256 rows and more, where doubled units left the last wave mostly
+        // idle (1.3 waves for 512^2 tiles).
+        if (!L.reversible && j.h < 256) j.seg *= 2;
         if (j.w == 0 || j.h == 0) continue;
         rounds[L.reversible ? r - 1 : max_rounds + r - 1].push_back(j);
       }
