@@ -638,13 +638,13 @@ def main():
         assert rc == 0, rc
         return outs
 
-    for _ in range(min(args.warmup, 2)):
+    for _ in range(max(3, args.warmup)):
         outs = e2e_step()
         for i in range(n):
             lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
     barrier()
     e2e_ms_list = []
-    for _ in range(max(1, min(args.steps, 5))):
+    for _ in range(max(1, min(args.steps, 10))):
         c0 = torch.cuda.Event(enable_timing=True)
         c1 = torch.cuda.Event(enable_timing=True)
         c0.record(stream)
