@@ -1,29 +1,44 @@
 """Benchmark: decoded Mpixel/s of the HTJ2K tile-batch decode path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c1i|c1c|c2|c3|c4] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c1i|c1c|c3|c4] [--impl ours|reference]
 
-A step is one decode of the whole workload batch.  Default workload: 256
-tiles of 512x512 RGB8 (H&E-like, 5 levels, 64x64 code blocks, RCT), seeded
-synthetic data; c1i is the same batch coded lossy (9/7, ICT, quantised),
-c1c the same batch with classic (EBCOT) code blocks.
-Prints one JSON line (rank 0):
+A step is one decode of the whole workload batch.  Default workload: the
+uneven batch (1024 RGB8 tiles, sides 128..1024, 3..6 levels, 32x32 / 64x64
+code blocks, 20% near-blank), the configuration the batched-versus-plain
+target is quoted on; seeded synthetic data.  c1 is 256 tiles of 512x512, c3
+128 gray u16 tiles of 2048x2048, c1i the c1 batch coded lossy (9/7, ICT,
+quantised), c1c the c1 batch with classic (EBCOT) code blocks, c4 the full
+serving sweep.  Prints one JSON line (rank 0):
 
-  value        batched decode, codestreams resident in HBM (one plan: HT
-               cleanup over all code blocks ordered by coded length, IDWT
-               rounds, fused last level + RCT + pack), timed with CUDA events
-               on the library's stream;
-  plain_*      the plain per-tile path (one tile per call) on the same tiles;
-  e2e          sgn_j2k_decode_tiles_to_device from pinned host codestreams:
-               host parse, H2D copy, kernels, status read-back;
-  roofline     dominant kernel: (codestream + output bytes) / its duration;
-  cpu_baseline the oracle (C++ restatement of the reference CPU tile batch)
-               on the host cores, bounded sample.
+  value          batched decode, codestreams resident in HBM (one plan: HT
+                 cleanup over all code blocks ordered by coded length, IDWT
+                 rounds, fused last level + RCT + pack), CUDA-graph replays
+                 timed with CUDA events on the library's stream;
+  e2e            sgn_j2k_decode_tiles_to_device from pinned host codestreams:
+                 host parse, H2D copy, kernels, status read-back;
+  e2e_pageable   the same call from one pageable host buffer per tile (what
+                 a caller passing separate slices hands in);
+  plain_*        the plain per-tile drop-in (one tile per call) on the same
+                 tiles: device-resident replays and sgn_j2k_decode_to_device
+                 end to end;
+  parity         every tile of the timed batch against the oracle;
+  roofline       dominant kernel: (codestream + output bytes) / its duration;
+  cpu_baseline   the oracle (C++ restatement of the reference CPU tile batch)
+                 on the host cores, bounded sample;
+  other_configs  (N = 1) the c1 and c3 batches: batched, plain, e2e, parity;
+  serving        (N = 1) the c4 request stream: closed-loop peak, then
+                 Poisson arrivals at fractions of it, p50/p99 per rate.
 
-With --gpus N > 1 (torchrun) every rank decodes its own replica of the
-workload (independent tiles, no data-path collective) and rank 0 reports the
-total over the max per-rank time.
+With --gpus N > 1 (torchrun) the global tile list (N times the workload's
+tiles for the uneven batch, tiles independent, no data-path collective) is
+partitioned over the ranks by coded bytes; each rank decodes its shard and
+rank 0 reports all tiles' pixels over the slowest rank's time.
+
+The reference arm (--impl reference) times the oracle's CPU tile batch on
+all host cores over the same workload, whole batches per step.
 """
 import argparse
+import ctypes
 import json
 import os
 import pathlib
@@ -37,6 +52,7 @@ sys.path.insert(0, str(ROOT))
 
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "decoded Mpixel/s"
 
 
 def parse_args():
@@ -44,34 +60,22 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=["c1", "c1i", "c1c", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c1i", "c1c", "c2", "c3", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other configs and the serving summary")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
     ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000,160000,200000",
                     help="c4: arrival rates, tiles/s")
-    ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate")
+    ap.add_argument("--min-requests", type=int, default=10000, help="c4: requests per rate, at least")
+    ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate, at least")
     ap.add_argument("--slots", type=int, default=4, help="c4: batches in flight")
     ap.add_argument("--max-batch", type=int, default=512, help="c4: requests per batch")
     ap.add_argument("--max-batch-samples", type=int, default=96000000,
                     help="c4: decoded samples per batch (0: unbounded)")
     return ap.parse_args()
-
-
-def build_workload(name):
-    from signinum_b200 import encode
-
-    if name == "c1":
-        return encode.config1(), "rgb8"
-    if name == "c1i":
-        return encode.config1_irreversible(), "rgb8"
-    if name == "c1c":
-        return encode.config1_classic(), "rgb8"
-    if name == "c2":
-        return encode.config2(), "rgb8"
-    return encode.config3(), "gray16"
 
 
 WORKLOAD_CONFIG = {
@@ -88,10 +92,27 @@ WORKLOAD_CONFIG = {
 }
 
 
+def build_workload(name, n=None, indices=None):
+    """(tiles, output format) of a workload; c2 with n / indices gives part
+    of a larger list of the same distribution."""
+    from signinum_b200 import encode
+
+    if name == "c1":
+        return encode.config1().tiles, 1
+    if name == "c1i":
+        return encode.config1_irreversible().tiles, 1
+    if name == "c1c":
+        return encode.config1_classic().tiles, 1
+    if name == "c2":
+        return encode.config2(n or 1024, indices=indices).tiles, 1
+    return encode.config3().tiles, 3
+
+
 class Clocks:
     """SM clock, power and clock-event reasons sampled from NVML (read-only
-    queries) every millisecond during the timed region; each sample is also
-    written to gpurun_out/clocks_<pid>.csv."""
+    queries) every millisecond during a timed region.  With the environment
+    variable SGN_BENCH_CLOCKS_DIR set, every sample is also written to
+    <dir>/clocks_<pid>.csv."""
 
     REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
@@ -101,7 +122,8 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.rows = []
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        d = os.environ.get("SGN_BENCH_CLOCKS_DIR")
+        self.path = pathlib.Path(d) / f"clocks_{os.getpid()}.csv" if d else None
         self.stop = None
         self.thread = None
 
@@ -166,14 +188,15 @@ class Clocks:
                 self._sample()
             except Exception:
                 pass
-            try:
-                self.path.parent.mkdir(exist_ok=True)
-                with open(self.path, "w") as f:
-                    f.write("t_s,sm_mhz,sm_max_mhz,power_w,reasons\n")
-                    for t, sm, mx, pw, act in self.rows:
-                        f.write(f"{t:.6f},{sm},{mx},{pw:.1f},{'|'.join(act)}\n")
-            except Exception:
-                pass
+            if self.path:
+                try:
+                    self.path.parent.mkdir(parents=True, exist_ok=True)
+                    with open(self.path, "w") as f:
+                        f.write("t_s,sm_mhz,sm_max_mhz,power_w,reasons\n")
+                        for t, sm, mx, pw, act in self.rows:
+                            f.write(f"{t:.6f},{sm},{mx},{pw:.1f},{'|'.join(act)}\n")
+                except Exception:
+                    pass
 
     def summary(self):
         if not self.rows:
@@ -184,19 +207,33 @@ class Clocks:
                 "samples": len(self.rows), "source": "NVML, 1 ms polling during the timed region"}
 
 
+def _oracle_outputs(tiles, fmt, workers):
+    from oracle import oracle
+
+    outs, first = oracle.decode_batch([t.codestream for t in tiles], fmt, workers=workers)
+    return outs, first
+
+
 def cpu_baseline(tiles, fmt, budget_s=12.0):
     """The oracle's CPU tile batch (all host threads) over a bounded sample of
-    the workload: whole passes over its tiles until about budget_s seconds."""
+    the workload: whole passes over its first tiles until about budget_s
+    seconds."""
     from oracle import oracle
 
     cores = os.cpu_count() or 1
-    # One single-threaded probe decode sizes the sample.
+    # One single-threaded probe decode per tile size class sizes the sample.
     t0 = time.perf_counter()
-    oracle.decode(tiles[0].codestream, fmt)
-    per_tile = max(time.perf_counter() - t0, 1e-4)
-    k = int(max(1, min(len(tiles), budget_s * cores / per_tile)))
-    sample = [t.codestream for t in tiles[:k]]
+    probe = tiles[: min(8, len(tiles))]
+    for t in probe:
+        oracle.decode(t.codestream, fmt)
+    per_px = max(time.perf_counter() - t0, 1e-4) / sum(t.width * t.height for t in probe)
+    k, px = 0, 0
+    while k < len(tiles) and (px + tiles[k].width * tiles[k].height) * per_px <= budget_s * cores / 2:
+        px += tiles[k].width * tiles[k].height
+        k += 1
+    k = max(k, 1)
     px = sum(t.width * t.height for t in tiles[:k])
+    sample = [t.codestream for t in tiles[:k]]
     passes, dt, ok = 0, 0.0, True
     while passes == 0 or dt < budget_s:
         t0 = time.perf_counter()
@@ -211,75 +248,348 @@ def cpu_baseline(tiles, fmt, budget_s=12.0):
 
 
 def run_reference(args):
-    """--impl reference: the CPU restatement of the reference's tile batch."""
+    """--impl reference: the CPU restatement of the reference's tile batch
+    (decode_tiles_into, crates/signinum-j2k/src/batch.rs:110-147) on all host
+    threads, over the same workload as the GPU arm: the whole batch per step,
+    or (when K + W whole batches would not end within about three minutes) a
+    prefix of it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w, kind = build_workload(args.workload)
-    fmt = 1 if kind == "rgb8" else 3
+    if args.workload == "c4":
+        print(json.dumps({"impl": "reference", "unavailable": "the serving sweep has no CPU counterpart in the "
+                                                                "reference (its adapter decodes one call at a time)"}))
+        return
+    tiles, fmt = build_workload(args.workload)
     from oracle import oracle
 
     cores = os.cpu_count() or 1
-    # Each step: a bounded sample (~2 s of CPU work per step at one thread).
+    budget_s = 180.0
+    # Probe one batch of the first tiles to estimate a whole batch's time.
+    probe = tiles[: min(32, len(tiles))]
     t0 = time.perf_counter()
-    oracle.decode(w.tiles[0].codestream, fmt)
-    per_tile = max(time.perf_counter() - t0, 1e-4)
-    k = int(max(1, min(len(w.tiles), 2.0 * cores / per_tile / max(args.steps, 1))))
-    sample = [t.codestream for t in w.tiles[:k]]
-    px = sum(t.width * t.height for t in w.tiles[:k])
+    oracle.decode_batch([t.codestream for t in probe], fmt, workers=cores)
+    per_px = (time.perf_counter() - t0) / sum(t.width * t.height for t in probe)
+    total_px = sum(t.width * t.height for t in tiles)
+    steps = max(args.steps + args.warmup, 1)
+    k = len(tiles)
+    if per_px * total_px * steps > budget_s:
+        px, k = 0, 0
+        while k < len(tiles) and (px + tiles[k].width * tiles[k].height) * per_px * steps <= budget_s:
+            px += tiles[k].width * tiles[k].height
+            k += 1
+        k = max(k, 1)
+    sample = [t.codestream for t in tiles[:k]]
+    px = sum(t.width * t.height for t in tiles[:k])
     for _ in range(args.warmup):
         oracle.decode_batch(sample, fmt, workers=cores)
     times = []
+    ok = True
     for _ in range(args.steps):
         t0 = time.perf_counter()
         _, first = oracle.decode_batch(sample, fmt, workers=cores)
         times.append(time.perf_counter() - t0)
+        ok = ok and first == -1
     ms = 1000.0 * float(np.mean(times))
     v = px / (ms / 1000.0) / 1e6
-    line = {"impl": "reference", "metric": "decoded Mpixel/s", "value": v, "unit": "Mpixel/s",
+    what = "the whole batch" if k == len(tiles) else f"the first {k} of {len(tiles)} tiles"
+    cfg = dict(WORKLOAD_CONFIG[args.workload], parallelism="host threads")
+    if k != len(tiles):
+        cfg["sample_tiles"] = k
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpixel/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic (seeded)", "config": dict(WORKLOAD_CONFIG[args.workload], sample_tiles=k),
+            "data": "synthetic (seeded)", "config": cfg, "decode_ok": ok,
             "cpu_baseline": {"value": v, "unit": "Mpixel/s", "cores": cores, "kind": "port",
-                             "sample": f"first {k} tiles of the workload per step, {cores} threads; C++ "
-                                       "restatement of the reference CPU tile batch (Rust toolchain absent)"},
+                             "sample": f"{what} per step, {cores} threads; C++ restatement of the reference CPU "
+                                       "tile batch (Rust toolchain absent)"},
             "e2e": {"value": v, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args):
-    """Serving: open-loop Poisson arrivals over a resident pool of uneven tiles
-    (60% full RGB8, 25% quarter resolution, 15% 256x256 region), continuous
-    batching in the native server, p50/p99 latency and throughput per rate."""
-    import ctypes
-    import threading
-
+def reduce_max(dist, x, device):
+    """Max of a per-rank scalar over all ranks (the timed region's duration is
+    the slowest rank's); identity without a process group."""
+    if not dist:
+        return x
     import torch
 
-    from signinum_b200 import _native, encode
-    from signinum_b200._native import SgnRequest, SgnServerResult
-    from signinum_b200.server import Server
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    pool = encode.config4_pool(args.pool).tiles
-    coded = sum(len(t.codestream) for t in pool)
-    from signinum_b200 import j2k_cuda
 
-    ctx = j2k_cuda._Context.open(local)
-    server = Server(ctx, device_budget_bytes=16 << 30, resident_capacity_bytes=coded + 64 * len(pool) + (1 << 20),
-                    max_batch_tiles=args.max_batch, slots=args.slots, max_batch_samples=args.max_batch_samples)
-    ids = [server.register(t.codestream) for t in pool]
+def replica_throughput(world, units_per_rank, ms):
+    """Whole-job rate (units/s, in millions) of `world` replicas that each
+    processed units_per_rank in `ms` milliseconds (max over ranks)."""
+    return world * units_per_rank / (ms / 1000.0) / 1e6
+
+
+def job_throughput(units_total, ms):
+    """Whole-job rate (units/s, in millions): all ranks' units over the
+    slowest rank's milliseconds."""
+    return units_total / (ms / 1000.0) / 1e6
+
+
+def traffic_for(workload, kernel):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    p = ROOT / "profiles" / "dram_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
+            return float(parts[2])
+    return None
+
+
+class Batch:
+    """One workload's tiles in pinned, contiguous host memory (16-byte
+    aligned, the layout the batched call uploads in one copy)."""
+
+    def __init__(self, tiles, fmt):
+        import torch
+
+        self.tiles = tiles
+        self.fmt = fmt
+        self.n = len(tiles)
+        self.bpp = 3 if fmt == 1 else 2
+        self.pixels = sum(t.width * t.height for t in tiles)
+        self.coded = sum(len(t.codestream) for t in tiles)
+        self.out_bytes = self.pixels * self.bpp
+        self.offs, pos = [], 0
+        for t in tiles:
+            self.offs.append(pos)
+            pos += (len(t.codestream) + 15) & ~15
+        self.pinned_bytes = pos
+        self.pinned = torch.empty(max(pos, 16), dtype=torch.uint8, pin_memory=True)
+        self.host = self.pinned.numpy()
+        for o, t in zip(self.offs, tiles):
+            self.host[o:o + len(t.codestream)] = np.frombuffer(t.codestream, np.uint8)
+        self.lens = [len(t.codestream) for t in tiles]
+
+
+def measure_batched(ctx, stream, b, args, dist=None, clocks_index=None):
+    """Device-resident batched plan: autotune, per-stage times, then K timed
+    CUDA-graph replays after W warm-ups.  Returns (plan, results)."""
+    import torch
+
+    from signinum_b200.plan import Plan
+
+    plan = Plan(b.lens, b.fmt, ctx=ctx, contiguous=b.host, offsets=b.offs)
+    tune = None if args.no_autotune else plan.autotune(5)
+    stages = [plan.execute_timed() for _ in range(3)]
+    # The first execution runs eagerly, the second captures the plan as a
+    # CUDA graph; timed steps replay the graph.
+    for _ in range(max(args.warmup, 3)):
+        plan.execute_async()
+    st, per = plan.wait()
+    assert st == 0, f"decode failed: {st}"
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(clocks_index if clocks_index is not None else torch.cuda.current_device())
+    with clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            plan.execute_async()
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = reduce_max(dist, ev0.elapsed_time(ev1) / args.steps, "cuda")
+    stage = np.mean(np.array(stages), axis=0)  # VLC, MagSgn, refine, IDWT, pack, total
+    return plan, {"ms": ms, "stage": stage, "tune": tune, "launches": plan.launches, "clocks": clk.summary()}
+
+
+def parity_all(plan, b, workers):
+    """Every tile of the batch against the oracle, in chunks of tiles."""
+    ok, checked = True, 0
+    chunk = 64
+    for s in range(0, b.n, chunk):
+        part = b.tiles[s:s + chunk]
+        want, first = _oracle_outputs(part, b.fmt, workers)
+        ok = ok and first == -1
+        for i, w in enumerate(want):
+            got = plan.download(s + i)
+            ok = ok and got == w[: len(got)].tobytes() and len(got) == part[i].width * part[i].height * b.bpp
+            checked += 1
+    return {"tiles_checked": checked, "tiles": b.n, "bit_exact": bool(ok), "against": "oracle (all tiles)"}
+
+
+def measure_plain(ctx, stream, b, dist=None):
+    """The plain per-tile path on the batch's tiles: one plan per tile
+    (device-resident, warmed until its CUDA graph is captured, then one timed
+    replay each) and the drop-in call sgn_j2k_decode_to_device end to end
+    from pinned host memory."""
+    import torch
+
+    from signinum_b200 import _native
+    from signinum_b200._native import SgnRequest, SgnSurface
+    from signinum_b200.plan import Plan
+
+    n = b.n
+    tplans = [Plan([b.lens[i]], b.fmt, ctx=ctx, contiguous=b.host[b.offs[i]:b.offs[i] + ((b.lens[i] + 15) & ~15)],
+                   offsets=[0]) for i in range(n)]
+    for p in tplans:
+        p.execute_async()
+        p.execute_async()  # captures the tile's graph
+    tplans[-1].wait()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for p, (e0, e1) in zip(tplans, evs):
+        e0.record(stream)
+        p.execute_async()
+        e1.record(stream)
+        p.wait()
+    a1.record(stream)
+    a1.synchronize()
+    lat = [e0.elapsed_time(e1) for e0, e1 in evs]
+    plain_ms = reduce_max(dist, a0.elapsed_time(a1), "cuda")
+    for p in tplans:
+        p.destroy()
     lib = _native.cuda_lib()
-    h = server._h
+    req = SgnRequest(0, 0, 0, 0, 0, 1)
+    for i in range(min(8, n)):
+        s = SgnSurface()
+        assert lib.sgn_j2k_decode_to_device(ctx.handle, b.host.ctypes.data + b.offs[i], b.lens[i], b.fmt,
+                                            ctypes.byref(req), 3, ctypes.byref(s)) == 0
+        lib.sgn_surface_free(ctx.handle, ctypes.byref(s))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e2e_lat = []
+    t_all = time.perf_counter()
+    for i in range(n):
+        s = SgnSurface()
+        t0 = time.perf_counter()
+        rc = lib.sgn_j2k_decode_to_device(ctx.handle, b.host.ctypes.data + b.offs[i], b.lens[i], b.fmt,
+                                          ctypes.byref(req), 3, ctypes.byref(s))
+        e2e_lat.append((time.perf_counter() - t0) * 1000.0)
+        assert rc == 0
+        lib.sgn_surface_free(ctx.handle, ctypes.byref(s))
+    plain_e2e_ms = reduce_max(dist, (time.perf_counter() - t_all) * 1000.0, "cuda")
+    return {"plain_ms": plain_ms, "plain_e2e_ms": plain_e2e_ms,
+            "plain_tile_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "plain_e2e_tile_latency_ms": {"p50": float(np.percentile(e2e_lat, 50)),
+                                          "p99": float(np.percentile(e2e_lat, 99))}}
 
-    def make_requests(n, seed):
+
+def measure_e2e(ctx, stream, b, args, dist=None, pageable=False):
+    """sgn_j2k_decode_tiles_to_device from host codestreams, timed with CUDA
+    events on the context stream around the whole call (H2D, parse, plan,
+    kernels, status read-back); pinned contiguous buffers, or one pageable
+    buffer per tile.  Mean of up to ten calls after at least three warm-ups."""
+    import torch
+
+    from signinum_b200 import _native
+    from signinum_b200._native import SgnSurface
+
+    lib = _native.cuda_lib()
+    n = b.n
+    if pageable:
+        bufs = [np.frombuffer(bytearray(t.codestream), np.uint8) for t in b.tiles]
+        ptrs = (ctypes.c_void_p * n)(*[x.ctypes.data for x in bufs])
+    else:
+        ptrs = (ctypes.c_void_p * n)(*[b.host.ctypes.data + o for o in b.offs])
+    clens = (ctypes.c_size_t * n)(*b.lens)
+    per_tile = (ctypes.c_int32 * n)()
+    first = ctypes.c_size_t()
+
+    def step():
+        outs = (SgnSurface * n)()
+        rc = lib.sgn_j2k_decode_tiles_to_device(ctx.handle, ptrs, clens, n, b.fmt, None, 3, outs, per_tile,
+                                                ctypes.byref(first))
+        assert rc == 0, rc
+        return outs
+
+    def release(outs):
+        for i in range(n):
+            lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
+
+    for _ in range(max(3, args.warmup)):
+        release(step())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    times = []
+    for _ in range(max(1, min(args.steps, 10))):
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        outs = step()
+        c1.record(stream)
+        c1.synchronize()
+        times.append(c0.elapsed_time(c1))
+        release(outs)
+    ms = reduce_max(dist, float(np.mean(times)), "cuda")
+    return {"ms": ms, "h2d_bytes_per_step": int(sum(b.lens) if pageable else b.pinned_bytes),
+            "d2h_bytes_per_step": 4 * n}
+
+
+def config_summary(ctx, stream, name, args):
+    """Batched, plain and e2e figures of another config, with every tile
+    checked against the oracle (N = 1 only)."""
+    tiles, fmt = build_workload(name)
+    b = Batch(tiles, fmt)
+    plan, r = measure_batched(ctx, stream, b, args)
+    par = parity_all(plan, b, os.cpu_count() or 1)
+    plan.destroy()
+    pl = measure_plain(ctx, stream, b)
+    e = measure_e2e(ctx, stream, b, args)
+    v = job_throughput(b.pixels, r["ms"])
+    return {"workload": WORKLOAD_CONFIG[name]["workload"], "value": v, "unit": "Mpixel/s",
+            "ms_per_step": r["ms"], "stage_ms": dict(zip(["ht_vlc", "ht_magsgn", "ht_refine", "idwt_levels",
+                                                          "last_level_pack", "total"], map(float, r["stage"]))),
+            "e2e": {"value": job_throughput(b.pixels, e["ms"]), "unit": "Mpixel/s", "ms_per_step": e["ms"]},
+            "plain_mpix_s": job_throughput(b.pixels, pl["plain_ms"]),
+            "plain_e2e_mpix_s": job_throughput(b.pixels, pl["plain_e2e_ms"]),
+            "plain_tile_latency_ms": pl["plain_tile_latency_ms"],
+            "batched_over_plain": pl["plain_ms"] / r["ms"], "parity": par, "autotune": r["tune"],
+            "clocks": r["clocks"]}
+
+
+# ---------------------------------------------------------------------------
+# Serving (c4): continuous batching over a resident pool of uneven tiles.
+
+class ServingRun:
+    """A native server over a resident pool of uneven tiles (60% full RGB8,
+    25% quarter resolution, 15% 256x256 region requests), driven open loop:
+    requests go in at their Poisson arrival times, a poller thread collects
+    results; latency is the server's submit-to-publication time."""
+
+    def __init__(self, ctx, pool, args):
+        from signinum_b200 import _native
+        from signinum_b200.server import Server
+
+        self.ctx = ctx
+        self.pool = pool
+        coded = sum(len(t.codestream) for t in pool)
+        self.coded = coded
+        self.server = Server(ctx, device_budget_bytes=16 << 30,
+                             resident_capacity_bytes=coded + 64 * len(pool) + (1 << 20),
+                             max_batch_tiles=args.max_batch, slots=args.slots,
+                             max_batch_samples=args.max_batch_samples)
+        self.ids = [self.server.register(t.codestream) for t in pool]
+        self.lib = _native.cuda_lib()
+        self.h = self.server._h
+
+    def make_requests(self, n, seed):
+        from signinum_b200._native import SgnRequest
+
         rng = np.random.default_rng(seed)
         reqs, px = [], []
         for _ in range(n):
-            i = int(rng.integers(len(pool)))
-            t = pool[i]
+            i = int(rng.integers(len(self.pool)))
+            t = self.pool[i]
             u = rng.uniform()
             r = SgnRequest(0, 0, 0, 0, 0, 1)
             if u < 0.60:
@@ -293,14 +603,20 @@ def run_serving(args):
                 r.x = int(rng.integers(0, t.width - side + 1))
                 r.y = int(rng.integers(0, t.height - side + 1))
                 px.append(side * side)
-            reqs.append((ids[i], r, i))
+            reqs.append((self.ids[i], r, i))
         return reqs, px
 
-    def run(reqs, gaps, check=0):
+    def run(self, reqs, gaps, check=0):
         """Submits reqs at the given inter-arrival gaps (seconds), every request
         whose arrival time has passed going in with one sgn_server_submit_many
         call; returns latencies (ms), wall seconds from first submit to last
-        result, and the parity of `check` sampled results against the oracle."""
+        result, and (checked, all equal) for `check` sampled results against
+        the oracle."""
+        import threading
+
+        from signinum_b200._native import SgnRequest, SgnServerResult, SgnSurface
+
+        lib, h, ctx = self.lib, self.h, self.ctx
         n = len(reqs)
         chunks = []
         done = threading.Event()
@@ -309,8 +625,6 @@ def run_serving(args):
         first = []
 
         def poller():
-            from signinum_b200._native import SgnSurface
-
             cap = 8192
             buf = (SgnServerResult * cap)()
             view = np.frombuffer(buf, dtype=np.dtype({
@@ -371,61 +685,115 @@ def run_serving(args):
         done.wait(120)
         wall = time.perf_counter() - t0
         th.join(5)
+        sys.setswitchinterval(5e-3)
         res = np.concatenate(chunks) if chunks else np.zeros(0)
         lat = res["latency"]
         assert len(res) == n and np.all(res["status"] == 0), "a request failed"
-        ok = None
+        parity = None
         if check:
             from oracle import oracle
 
             ok = len(kept) > 0
-            for kk, b in kept.items():
+            for kk, bts in kept.items():
                 tid, r, i = reqs[kk]
-                want, _, _ = oracle.decode(pool[i].codestream, 1, r.kind, (r.x, r.y, r.w, r.h), r.downscale)
-                ok = ok and (want == b)
-        return lat, wall, ok
+                want, _, _ = oracle.decode(self.pool[i].codestream, 1, r.kind, (r.x, r.y, r.w, r.h), r.downscale)
+                ok = ok and (want == bts)
+            parity = {"checked": len(kept), "bit_exact": bool(ok)}
+        return lat, wall, parity
 
-    # Warm-up, then the closed-loop peak: every request submitted at once.
-    warm, _ = make_requests(2000, 11)
-    run(warm, np.zeros(len(warm)))
-    peak_reqs, peak_px = make_requests(20000, 12)
-    s0 = server.stats()
-    with Clocks(local) as clk_peak:
-        _, peak_wall, ok_peak = run(peak_reqs, np.zeros(len(peak_reqs)), check=16)
-    peak_tps = len(peak_reqs) / peak_wall
-    s1 = server.stats()
+    def stats(self):
+        return self.server.stats()
 
-    def per_batch(a, b):
-        nb = max(1, b["batches"] - a["batches"])
-        return {"batches": b["batches"] - a["batches"], "tiles_per_batch": (b["completed"] - a["completed"]) / nb,
-                "build_us": (b["build_us_total"] - a["build_us_total"]) / nb,
-                "gpu_us": (b["gpu_us_total"] - a["gpu_us_total"]) / nb,
-                "flight_us": (b["flight_us_total"] - a["flight_us_total"]) / nb}
+    def close(self):
+        self.server.close()
 
-    rates = [float(x) for x in args.rates.split(",") if x]
-    per_rate = []
-    for k, lam in enumerate(rates):
-        n = int(max(200, min(lam * args.seconds, 40000)))
-        reqs, px = make_requests(n, 100 + k)
-        gaps = np.random.default_rng(200 + k).exponential(1.0 / lam, size=n)
-        gaps[0] = 0.0
-        sa = server.stats()
-        with Clocks(local) as clk:
-            lat, wall, ok = run(reqs, gaps, check=8)
-        sb = server.stats()
-        tps = n / wall
-        per_rate.append({"rate_tiles_s": lam, "requests": n, "throughput_tiles_s": tps,
-                         "throughput_mpix_s": sum(px) / wall / 1e6,
-                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "max_ms": float(lat.max()), "parity_sample_ok": ok, "clocks": clk.summary(),
-                         "per_batch": per_batch(sa, sb)})
-    # Peak batched throughput: the larger of the closed-loop run and the best
-    # rate the open-loop sweep sustained.
-    peak_ref = max([peak_tps] + [r["throughput_tiles_s"] for r in per_rate])
+
+def _per_batch(a, b):
+    nb = max(1, b["batches"] - a["batches"])
+    return {"batches": b["batches"] - a["batches"], "tiles_per_batch": (b["completed"] - a["completed"]) / nb,
+            "build_us": (b["build_us_total"] - a["build_us_total"]) / nb,
+            "gpu_us": (b["gpu_us_total"] - a["gpu_us_total"]) / nb,
+            "flight_us": (b["flight_us_total"] - a["flight_us_total"]) / nb}
+
+
+def serving_rate(sr, lam, k, args, check):
+    """One open-loop rate: at least args.min_requests requests and
+    args.seconds of arrivals (at most 60,000 requests)."""
+    n = int(min(max(args.min_requests, lam * args.seconds), max(args.min_requests, 60000)))
+    reqs, px = sr.make_requests(n, 100 + k)
+    gaps = np.random.default_rng(200 + k).exponential(1.0 / lam, size=n)
+    gaps[0] = 0.0
+    sa = sr.stats()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        lat, wall, par = sr.run(reqs, gaps, check=check)
+    sb = sr.stats()
+    return {"rate_tiles_s": lam, "requests": n, "throughput_tiles_s": n / wall,
+            "throughput_mpix_s": sum(px) / wall / 1e6,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99_samples": int(n // 100), "max_ms": float(lat.max()), "parity": par, "clocks": clk.summary(),
+            "per_batch": _per_batch(sa, sb)}
+
+
+def serving_peak(sr, check=16):
+    warm, _ = sr.make_requests(2000, 11)
+    sr.run(warm, np.zeros(len(warm)))
+    peak_reqs, peak_px = sr.make_requests(20000, 12)
+    s0 = sr.stats()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        _, wall, par = sr.run(peak_reqs, np.zeros(len(peak_reqs)), check=check)
+    s1 = sr.stats()
+    return {"throughput_tiles_s": len(peak_reqs) / wall, "throughput_mpix_s": sum(peak_px) / wall / 1e6,
+            "requests": len(peak_reqs), "parity": par, "per_batch": _per_batch(s0, s1), "clocks": clk.summary()}
+
+
+def serving_summary(ctx, args):
+    """The c4 stream in brief for the default line: closed-loop peak, then
+    Poisson arrivals at 50, 80 and 90 % of it."""
+    from signinum_b200 import encode
+
+    pool = encode.config4_pool(args.pool).tiles
+    sr = ServingRun(ctx, pool, args)
+    try:
+        peak = serving_peak(sr)
+        rates = []
+        for k, f in enumerate((0.5, 0.8, 0.9)):
+            rates.append(serving_rate(sr, peak["throughput_tiles_s"] * f, k, args, check=64))
+        ref = max([peak["throughput_tiles_s"]] + [r["throughput_tiles_s"] for r in rates])
+        for r in rates:
+            r["frac_of_peak"] = r["throughput_tiles_s"] / ref
+        good = [r for r in rates if r["frac_of_peak"] >= 0.8 and r["p99_ms"] <= 5.0]
+        best = max(good, key=lambda r: r["throughput_tiles_s"]) if good else None
+    finally:
+        sr.close()
+    return {"workload": f"serving pool of {len(pool)} uneven RGB8 tiles, requests 60% full / 25% quarter "
+                        "resolution / 15% 256x256 region, Poisson arrivals, 16 GiB budget",
+            "peak_tiles_s": ref, "peak_closed_loop": peak,
+            "at_80pct_of_peak": ({"rate_tiles_s": best["rate_tiles_s"], "throughput_tiles_s": best["throughput_tiles_s"],
+                                  "frac_of_peak": best["frac_of_peak"], "p50_ms": best["p50_ms"],
+                                  "p99_ms": best["p99_ms"], "requests": best["requests"]} if best else None),
+            "rates": rates}
+
+
+def run_serving(args):
+    """--workload c4: the full serving sweep over args.rates."""
+    import torch
+
+    from signinum_b200 import encode, j2k_cuda
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pool = encode.config4_pool(args.pool).tiles
+    ctx = j2k_cuda._Context.open(local)
+    sr = ServingRun(ctx, pool, args)
+    peak = serving_peak(sr)
+    per_rate = [serving_rate(sr, float(x), k, args, check=8)
+                for k, x in enumerate([x for x in args.rates.split(",") if x])]
+    peak_ref = max([peak["throughput_tiles_s"]] + [r["throughput_tiles_s"] for r in per_rate])
     for r in per_rate:
         r["frac_of_peak"] = r["throughput_tiles_s"] / peak_ref
-    st = server.stats()
-    server.close()
+    st = sr.stats()
+    sr.close()
     if rank == 0:
         best = [r for r in per_rate if r["p99_ms"] <= 5.0]
         line = {
@@ -436,48 +804,14 @@ def run_serving(args):
             "config": {"workload": f"serving pool of {len(pool)} uneven RGB8 tiles (sides 128..1024), requests 60% "
                                    "full RGB8 / 25% quarter resolution / 15% 256x256 region, Poisson arrivals, "
                                    "16 GiB admission budget, codestreams resident on the device",
-                       "pool_coded_bytes": coded, "slots": args.slots, "max_batch_tiles": args.max_batch,
+                       "pool_coded_bytes": sr.coded, "slots": args.slots, "max_batch_tiles": args.max_batch,
                        "max_batch_samples": args.max_batch_samples},
-            "peak_tiles_s": peak_ref,
-            "peak_closed_loop": {"throughput_tiles_s": peak_tps, "throughput_mpix_s": sum(peak_px) / peak_wall / 1e6,
-                                 "requests": len(peak_reqs), "parity_sample_ok": ok_peak,
-                                 "per_batch": per_batch(s0, s1),
-                                 "clocks": clk_peak.summary()},
-            "per_rate": per_rate,
-            "server_stats": st,
+            "peak_tiles_s": peak_ref, "peak_closed_loop": peak, "per_rate": per_rate, "server_stats": st,
         }
         print(json.dumps(line), flush=True)
 
 
-def reduce_max(dist, x, device):
-    """Max of a per-rank scalar over all ranks (the timed region's duration is
-    the slowest replica's); identity without a process group."""
-    if not dist:
-        return x
-    import torch
-
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def replica_throughput(world, units_per_rank, ms):
-    """Whole-job rate (units/s, in millions) of `world` replicas that each
-    processed units_per_rank in `ms` milliseconds (max over ranks)."""
-    return world * units_per_rank / (ms / 1000.0) / 1e6
-
-
-def traffic_for(workload, kernel):
-    """dram bytes per launch of `kernel` from the committed ncu summary."""
-    p = ROOT / "profiles" / "dram_traffic.txt"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        parts = line.split()
-        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
-            return float(parts[2])
-    return None
-
+# ---------------------------------------------------------------------------
 
 def main():
     args = parse_args()
@@ -499,165 +833,42 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from signinum_b200 import j2k_cuda
-    from signinum_b200.plan import Plan
 
     ctx = j2k_cuda._Context.open(local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
-    w, kind = build_workload(args.workload)
-    fmt = 1 if kind == "rgb8" else 3
-    bpp = 3 if kind == "rgb8" else 2
-    tiles = w.tiles
-    n = len(tiles)
-    pixels = w.pixels()
-    coded = w.coded_bytes()
-    out_bytes = sum(t.width * t.height * bpp for t in tiles)
-    # Pinned, contiguous codestreams (16-byte aligned) for the H2D path.
-    offs, pos = [], 0
-    for t in tiles:
-        offs.append(pos)
-        pos += (len(t.codestream) + 15) & ~15
-    pinned = torch.empty(pos, dtype=torch.uint8, pin_memory=True)
-    host = pinned.numpy()
-    for o, t in zip(offs, tiles):
-        host[o:o + len(t.codestream)] = np.frombuffer(t.codestream, np.uint8)
-    lens = [len(t.codestream) for t in tiles]
+    shard = None
+    if world > 1 and args.workload == "c2":
+        # The global list: world x 1024 uneven tiles, partitioned by coded bytes.
+        from signinum_b200.shard import shard_tiles
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
+        n_total = 1024 * world
+        _, tiles, shard = shard_tiles(dist, n_total, lambda idx: build_workload("c2", n_total, idx)[0])
+        fmt = 1
+    else:
+        tiles, fmt = build_workload(args.workload)
+    b = Batch(tiles, fmt)
+    if shard:
+        pixels_total = shard["pixels_total"]
+    else:
+        # Replicas of a workload that is not partitioned (every rank its own copy).
+        pixels_total = b.pixels * world
 
-    def max_over_ranks(x):
-        return reduce_max(dist, x, "cuda")
-
-    # ---- Batched, device-resident (value).
-    plan = Plan(lens, fmt, ctx=ctx, contiguous=host, offsets=offs)
-    # Launch shape chosen by the autotuner on this plan's data (untimed).
-    tune = None if args.no_autotune else plan.autotune(5)
-    # Per-stage breakdown with the tuned shape (events between stages; untimed).
-    stages = [plan.execute_timed() for _ in range(3)]
-    # Warm-up: the first execution runs eagerly, the second captures the plan
-    # as a CUDA graph; timed steps replay the graph.
-    for _ in range(args.warmup):
-        plan.execute_async()
-    st, per = plan.wait()
-    assert st == 0, f"decode failed: {st}"
-    barrier()
-    with Clocks(local) as clk:
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            plan.execute_async()
-        ev1.record(stream)
-        ev1.synchronize()
-    barrier()
-    batched_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-    stage = np.mean(np.array(stages), axis=0)  # VLC, MagSgn, refine, IDWT, pack, total
-    launches = plan.launches * args.steps
-    value = replica_throughput(world, pixels, batched_ms)
-    # Parity spot check of the benchmark output against the oracle.
-    check = None
-    if rank == 0:
-        from oracle import oracle
-
-        idx = [0, n // 2, n - 1]
-        check = all(plan.download(i) == oracle.decode(tiles[i].codestream, fmt)[0] for i in idx)
-
-    # ---- Plain per-tile path (one tile per call), device-resident and e2e.
+    plan, r = measure_batched(ctx, stream, b, args, dist, local)
+    value = job_throughput(pixels_total, r["ms"])
+    parity = parity_all(plan, b, os.cpu_count() or 1) if rank == 0 else None
     plain = {}
     if not args.no_plain:
-        tplans = [Plan([lens[i]], fmt, ctx=ctx, contiguous=host[offs[i]:offs[i] + ((lens[i] + 15) & ~15)],
-                       offsets=[0]) for i in range(n)]
-        for p in tplans[: min(8, n)]:
-            p.execute_async()
-            p.wait()
-        barrier()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for p, (e0, e1) in zip(tplans, evs):
-            e0.record(stream)
-            p.execute_async()
-            e1.record(stream)
-            p.wait()
-        a1.record(stream)
-        a1.synchronize()
-        lat = [e0.elapsed_time(e1) for e0, e1 in evs]
-        plain_ms = max_over_ranks(a0.elapsed_time(a1))
-        for p in tplans:
-            p.destroy()
-        # e2e plain: the drop-in call from pinned host memory, one tile per call.
-        import ctypes
-
-        from signinum_b200 import _native
-        from signinum_b200._native import SgnRequest, SgnSurface
-
-        lib = _native.cuda_lib()
-        req = SgnRequest(0, 0, 0, 0, 0, 1)
-        barrier()
-        b0 = torch.cuda.Event(enable_timing=True)
-        b1 = torch.cuda.Event(enable_timing=True)
-        e2e_lat = []
-        b0.record(stream)
-        for i in range(n):
-            s = SgnSurface()
-            t0 = time.perf_counter()
-            rc = lib.sgn_j2k_decode_to_device(ctx.handle, host.ctypes.data + offs[i], lens[i], fmt,
-                                              ctypes.byref(req), 3, ctypes.byref(s))
-            e2e_lat.append((time.perf_counter() - t0) * 1000.0)
-            assert rc == 0
-            lib.sgn_surface_free(ctx.handle, ctypes.byref(s))
-        b1.record(stream)
-        b1.synchronize()
-        plain_e2e_ms = max_over_ranks(b0.elapsed_time(b1))
-        plain = {"plain_mpix_s": world * pixels / (plain_ms / 1000.0) / 1e6,
-                 "plain_tile_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-                 "plain_e2e_mpix_s": world * pixels / (plain_e2e_ms / 1000.0) / 1e6,
-                 "plain_e2e_tile_latency_ms": {"p50": float(np.percentile(e2e_lat, 50)),
-                                               "p99": float(np.percentile(e2e_lat, 99))}}
+        pl = measure_plain(ctx, stream, b, dist)
+        plain = {"plain_mpix_s": job_throughput(pixels_total, pl["plain_ms"]),
+                 "plain_tile_latency_ms": pl["plain_tile_latency_ms"],
+                 "plain_e2e_mpix_s": job_throughput(pixels_total, pl["plain_e2e_ms"]),
+                 "plain_e2e_tile_latency_ms": pl["plain_e2e_tile_latency_ms"]}
         plain["batched_over_plain"] = value / plain["plain_mpix_s"]
-
-    # ---- e2e batched: decode_tiles_to_device from pinned host buffers.
-    import ctypes
-
-    from signinum_b200 import _native
-    from signinum_b200._native import SgnSurface
-
-    lib = _native.cuda_lib()
-    ptrs = (ctypes.c_void_p * n)(*[host.ctypes.data + o for o in offs])
-    clens = (ctypes.c_size_t * n)(*lens)
-    per_tile = (ctypes.c_int32 * n)()
-    first = ctypes.c_size_t()
-
-    def e2e_step():
-        outs = (SgnSurface * n)()
-        rc = lib.sgn_j2k_decode_tiles_to_device(ctx.handle, ptrs, clens, n, fmt, None, 3, outs, per_tile,
-                                                ctypes.byref(first))
-        assert rc == 0, rc
-        return outs
-
-    for _ in range(max(3, args.warmup)):
-        outs = e2e_step()
-        for i in range(n):
-            lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
-    barrier()
-    e2e_ms_list = []
-    for _ in range(max(1, min(args.steps, 10))):
-        c0 = torch.cuda.Event(enable_timing=True)
-        c1 = torch.cuda.Event(enable_timing=True)
-        c0.record(stream)
-        outs = e2e_step()
-        c1.record(stream)
-        c1.synchronize()
-        e2e_ms_list.append(c0.elapsed_time(c1))
-        for i in range(n):
-            lib.sgn_surface_free(ctx.handle, ctypes.byref(outs[i]))
-    e2e_ms = max_over_ranks(float(np.mean(e2e_ms_list)))
-    e2e_val = world * pixels / (e2e_ms / 1000.0) / 1e6
+    e2e = measure_e2e(ctx, stream, b, args, dist)
+    e2e_pg = measure_e2e(ctx, stream, b, args, dist, pageable=True)
 
     if rank == 0:
+        stage = r["stage"]
         names = ["ht_vlc_kernel", "ht_magsgn_kernel", "ht_refine_kernel", "idwt_level_kernel", "pack_kernel"]
         if args.workload == "c1i":
             names[3:] = ["idwt97_level_kernel", "pack97_kernel"]
@@ -666,40 +877,57 @@ def main():
         dom = int(np.argmax(stage[:5]))
         peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
         peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
-        algo = coded + out_bytes
+        algo = b.coded + b.out_bytes
         achieved = algo / (stage[dom] / 1000.0) / 1e9
         traffic = traffic_for(args.workload, names[dom])
-        cpu = None if args.no_cpu else cpu_baseline(tiles, fmt)
+        cpu = None if args.no_cpu else cpu_baseline(b.tiles, fmt)
+        cfg = dict(WORKLOAD_CONFIG[args.workload],
+                   parallelism=(f"dp{world}: tile list partitioned by coded bytes" if shard else
+                                f"replicas{world}" if world > 1 else "1 GPU"),
+                   l2="inputs larger than L2 (coded + coefficient arenas), no flush",
+                   coded_bytes=b.coded, output_bytes=b.out_bytes, pixels=b.pixels)
+        if shard:
+            cfg["shards"] = shard
         line = {
-            "metric": "decoded Mpixel/s (batched persistent form; plain per-tile beside it)",
+            "metric": METRIC,
             "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int32 (HT), f32 (9/7, ICT)" if args.workload == "c1i" else "int32", "data": "synthetic (seeded)",
-            "config": dict(WORKLOAD_CONFIG[args.workload], parallelism=f"replicas{world}",
-                           l2="inputs larger than L2 (coded + coefficient arenas), no flush",
-                           coded_bytes=coded, output_bytes=out_bytes, pixels=pixels),
-            "compressed_MB_s": world * coded / (batched_ms / 1000.0) / 1e6,
-            "hbm_roofline_frac_path": (world * algo / (batched_ms / 1000.0) / 1e9) / peak,
+            "config": cfg,
+            "form": "batched persistent form (one plan, CUDA graph replay); the plain per-tile drop-in beside it",
+            "compressed_MB_s": b.coded * (pixels_total / b.pixels) / (r["ms"] / 1000.0) / 1e6,
+            "hbm_roofline_frac_path": (algo / (r["ms"] / 1000.0) / 1e9) / peak,
             "stage_ms": {"ht_vlc": stage[0], "ht_magsgn": stage[1],
-                         ("classic_blocks" if args.workload == "c1c" else "ht_refine"): stage[2], "idwt_levels": stage[3],
-                         "last_level_pack": stage[4], "total": stage[5]},
+                         ("classic_blocks" if args.workload == "c1c" else "ht_refine"): stage[2],
+                         "idwt_levels": stage[3], "last_level_pack": stage[4], "total": stage[5]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": names[dom],
-                         "peak_source": "measured" if PEAKS.exists() else "fallback",
+                         "peak_source": "measured (burst copy)" if PEAKS.exists() else "fallback",
                          "algorithmic_bytes_per_launch": algo},
-            "e2e": {"value": e2e_val, "unit": "Mpixel/s", "h2d_bytes_per_step": pos,
-                    "d2h_bytes_per_step": 4 * n, "ms_per_step": e2e_ms},
-            "gpu_launches": int(launches),
-            "autotune": tune,
+            "e2e": {"value": job_throughput(pixels_total, e2e["ms"]), "unit": "Mpixel/s",
+                    "h2d_bytes_per_step": e2e["h2d_bytes_per_step"], "d2h_bytes_per_step": e2e["d2h_bytes_per_step"],
+                    "ms_per_step": e2e["ms"], "input": "pinned host memory, codestreams back to back"},
+            "e2e_pageable": {"value": job_throughput(pixels_total, e2e_pg["ms"]), "unit": "Mpixel/s",
+                             "h2d_bytes_per_step": e2e_pg["h2d_bytes_per_step"],
+                             "d2h_bytes_per_step": e2e_pg["d2h_bytes_per_step"], "ms_per_step": e2e_pg["ms"],
+                             "input": "one pageable host buffer per tile"},
+            "gpu_launches": int(r["launches"] * args.steps),
+            "autotune": r["tune"],
             "execution": "CUDA graph replay of the autotuned plan",
-            "clocks": clk.summary(),
-            "parity_spot_check": check,
+            "clocks": r["clocks"],
+            "parity": parity,
         }
         line.update(plain)
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_extra and args.workload == "c2":
+            plan.destroy()
+            plan = None
+            line["other_configs"] = {name: config_summary(ctx, stream, name, args) for name in ("c1", "c3")}
+            line["serving"] = serving_summary(ctx, args)
         print(json.dumps(line), flush=True)
-    plan.destroy()
+    if plan is not None:
+        plan.destroy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

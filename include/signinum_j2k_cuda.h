@@ -11,7 +11,10 @@
  *   SGN_ERR_UNSUPPORTED / SGN_ERR_UNSUPPORTED_BACKEND / SGN_ERR_CUDA_UNAVAILABLE
  *       -> is_unsupported();   SGN_ERR_BUFFER -> is_buffer_error();
  *   SGN_ERR_TRUNCATED -> is_truncated();  SGN_ERR_REGION -> J2kError::InvalidRegion;
- *   SGN_ERR_DECODE -> other decode errors;  SGN_ERR_CUDA_RUNTIME -> CudaRuntime{message}.
+ *   SGN_ERR_DECODE -> other decode errors;  SGN_ERR_CUDA_RUNTIME -> CudaRuntime{message};
+ *   SGN_ERR_HOST_BACKEND -> not an error in the reference: the adapter's host
+ *       branch for BackendRequest::Cpu / ::Auto, which this library leaves
+ *       to the caller.
  */
 #ifndef SIGNINUM_J2K_CUDA_H
 #define SIGNINUM_J2K_CUDA_H
@@ -35,7 +38,12 @@ enum {
   SGN_ERR_CUDA_RUNTIME = 7,
   SGN_ERR_UNSUPPORTED_BACKEND = 8,
   SGN_ERR_INVALID_ARGUMENT = 9,
-  SGN_ERR_OUT_OF_MEMORY = 10
+  SGN_ERR_OUT_OF_MEMORY = 10,
+  /* BackendRequest::Cpu or ::Auto: the request belongs to the adapter's host
+   * branch (wrap_surface returns a host Surface of the CPU decoder's bytes,
+   * crates/signinum-j2k-cuda/src/runtime.rs:19-48).  Returned before any
+   * CUDA call; no context is needed or created. */
+  SGN_ERR_HOST_BACKEND = 11
 };
 
 /* signinum_core::PixelFormat (crates/signinum-core/src/types.rs). */
@@ -49,8 +57,11 @@ typedef enum sgn_pixel_format {
 } sgn_pixel_format;
 
 /* signinum_core::BackendRequest (crates/signinum-core/src/backend.rs:15-22).
- * CUDA and AUTO decode on the GPU; CPU and METAL are rejected with
- * SGN_ERR_UNSUPPORTED_BACKEND (this library has no host decoder). */
+ * Only CUDA decodes here.  CPU and AUTO return SGN_ERR_HOST_BACKEND before
+ * any CUDA call: the reference serves both with a host surface and never
+ * initialises CUDA for them (runtime.rs:19-48, session.rs:32-38), so the
+ * adapter keeps that branch and routes only CUDA to this library.  METAL is
+ * SGN_ERR_UNSUPPORTED_BACKEND (validate_surface_request, runtime.rs:52-57). */
 typedef enum sgn_backend_request {
   SGN_BACKEND_AUTO = 0,
   SGN_BACKEND_CPU = 1,
@@ -224,30 +235,42 @@ sgn_status sgn_plan_tile_coefficients(sgn_ctx* ctx, const sgn_plan* plan, size_t
                                       size_t* count);
 
 /* HT code-block decode that allocates nothing (no counterpart in the
- * reference).
+ * reference: its adapter has no block-level entry point).
  *
- * For callers that cannot call cudaMalloc: code running inside CUDA graph
- * capture or an externally owned device memory arena, real-time loops that
- * must not allocate (nor synchronise the device through the allocator) once
- * they run, and frameworks whose own allocator owns all device memory.  The
- * caller passes device memory for the inputs (`segments`, the buffer the
- * blocks' src offsets point into) and the outputs (`coefficients`, and
- * `tile_status` with n_tiles words, set to nonzero for tiles with a block that
- * failed to decode); `blocks` is a host array.  The scratch the HT kernels
- * need lives in a fixed static device array (16 MiB of quad symbols; 4096
- * blocks of at most 4096 samples per call; cleanup segments up to about 27 KB),
- * and larger requests are rejected with SGN_ERR_INVALID_ARGUMENT or
- * SGN_ERR_UNSUPPORTED before any device work.
+ * For callers of this code that cannot allocate device memory: a host
+ * framework whose caching allocator owns all of the GPU's memory (a
+ * cudaMalloc beside it fails or fragments that pool), a decoder plugin that
+ * is handed its input and output buffers by its host and may create none of
+ * its own, and real-time loops that must not allocate, nor wait on the
+ * allocator's implicit synchronisation, once they run.  The caller passes
+ * device memory for the inputs (`segments`, segments_len bytes, the buffer
+ * the blocks' src offsets point into) and the outputs (`coefficients`,
+ * coefficients_len int32 elements, 8-byte aligned; `tile_status`, n_tiles
+ * words, set to nonzero for tiles with a block that failed to decode);
+ * `blocks` is a host array.  Every block's reads must lie inside
+ * segments[0, segments_len) and its writes inside
+ * coefficients[0, coefficients_len), else the call returns SGN_ERR_BUFFER
+ * before any device work.
+ *
+ * The scratch the HT kernels need lives in fixed static device arrays
+ * (16 MiB of quad symbols plus the device copy of the block table, about
+ * 16.4 MiB in all): at most 4096 blocks of at most 4096 samples per call,
+ * cleanup segments up to about 27 KB; larger requests are rejected with
+ * SGN_ERR_INVALID_ARGUMENT or SGN_ERR_UNSUPPORTED before any device work.
+ * The arrays stay reserved on every device where the library's module that
+ * holds them is loaded (with CUDA's default lazy loading: from this entry
+ * point's first call on that device) until the process exits.
  *
  * Runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
- * stream) on the current device.  The first call on a device looks up the
- * static arrays' device addresses; make that first call before any stream
- * capture.  All calls on a device share the static arrays and leave the last
- * call's contents there: calls that overlap on the GPU race and must be
- * serialised by the caller.  tile_status is cleared by the call. */
+ * stream) on the current device.  The first call on a device does the
+ * per-device set-up (it looks up the static arrays' device addresses with
+ * cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the static arrays and leave the last call's
+ * contents there: calls that overlap on the GPU race and must be serialised
+ * by the caller.  tile_status is cleared by the call. */
 sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, const uint8_t* segments,
-                                        int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
-                                        void* stream);
+                                        size_t segments_len, int32_t* coefficients, size_t coefficients_len,
+                                        uint32_t* tile_status, uint32_t n_tiles, void* stream);
 
 /* ---- DICOM input: extract_dicom_encapsulated_frames_with_limit
  * (crates/signinum-j2k-metal/src/dicom.rs:22-95).  Extracts up to `limit`

@@ -6,7 +6,8 @@ mirrors the reference's signinum-j2k-cuda adapter; j2k_cuda is its Python
 face.
 """
 from .j2k_cuda import (BackendKind, BackendRequest, Codec, CudaSession, CudaSurface, Downscale, Error, J2kDecoder,
-                       PixelFormat, Rect, Surface, TileBatchError, dicom_frames, inspect)
+                       PixelFormat, Rect, Surface, TileBatchError, dicom_frames, inspect, set_host_decoder)
 
 __all__ = ["BackendKind", "BackendRequest", "Codec", "CudaSession", "CudaSurface", "Downscale", "Error",
-           "J2kDecoder", "PixelFormat", "Rect", "Surface", "TileBatchError", "dicom_frames", "inspect"]
+           "J2kDecoder", "PixelFormat", "Rect", "Surface", "TileBatchError", "dicom_frames", "inspect",
+           "set_host_decoder"]

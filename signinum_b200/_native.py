@@ -131,8 +131,8 @@ CUDA_SIGNATURES = {
                                                     ctypes.c_void_p, ctypes.c_size_t,
                                                     ctypes.POINTER(ctypes.c_size_t)]),
     "sgn_ht_decode_blocks_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
-                                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
-                                                      ctypes.c_void_p]),
+                                                      ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                                      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
 }
 
 ENCODE_SIGNATURES = {

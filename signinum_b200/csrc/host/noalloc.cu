@@ -1,17 +1,23 @@
 // HT code-block decode that allocates nothing.
 //
-// For callers that cannot call cudaMalloc: code that runs inside CUDA graph
-// capture or an externally owned memory arena, real-time decode loops that
-// must not allocate (or synchronise the device through the allocator) once
-// running, and host frameworks whose allocator owns all device memory.  They
-// hand in device inputs and outputs; the scratch the HT kernels need (one
-// 32-bit symbol per quad, written by the VLC pass and read by the MagSgn
-// pass), the device copy of the block descriptors and the refinement list
-// live in file-scope static device arrays of fixed size, so this entry point
-// calls no cudaMalloc, cudaFree or allocating library routine.
+// Some callers of this code cannot allocate device memory: a host
+// framework whose own caching allocator owns all of the GPU's memory (a
+// cudaMalloc beside it would fail or fragment its pool), a decoder plugin
+// that is handed its input and output buffers by its host and may not
+// create any of its own, and a real-time loop that must not allocate, nor
+// wait on the allocator's implicit synchronisation, once it runs.  They hand
+// in device inputs and outputs; the scratch the HT kernels need (one 32-bit
+// symbol per quad, written by the VLC pass and read by the MagSgn pass), the
+// device copy of the block descriptors and the refinement list live in
+// file-scope static device arrays of fixed size, so this entry point calls
+// no cudaMalloc, cudaFree or allocating library routine.
 //
-// The arrays are shared by every call on a device and keep the last call's
-// contents; calls that overlap on the GPU (different streams, or host
+// The arrays (about 16.4 MiB) are reserved on every device where this
+// file's CUDA module is loaded, until the process exits: under CUDA's
+// default lazy module loading that is the first call of this entry point on
+// the device, under CUDA_MODULE_LOADING=EAGER the library's first use of the
+// device.  They are shared by every call on a device and keep the last
+// call's contents; calls that overlap on the GPU (different streams, or host
 // threads racing) race on them and must be serialised by the caller.
 #include <cuda_runtime.h>
 
@@ -73,6 +79,14 @@ sgn_status fail(sgn_status s, const char* m) {
   return s;
 }
 
+// The coding passes the kernels run for a descriptor, as the codestream
+// parser settles them: a refinement pass needs refinement bytes, and with 29
+// missing MSBs only the cleanup pass has a bit-plane left.
+__host__ __device__ inline uint32_t effective_passes(uint32_t passes, uint32_t lref, uint32_t missing_msbs) {
+  if (passes > 1 && (lref == 0 || missing_msbs == 29)) return 1;
+  return passes;
+}
+
 // Device addresses of the static arrays for the current device: taken once
 // per device with cudaGetSymbolAddress (host code must not use the arrays'
 // names as device addresses).
@@ -98,13 +112,15 @@ sgn_status setup(int device, DeviceArrays** out) {
   return SGN_OK;
 }
 
-// Gives every block its slice of the symbol scratch and lists the blocks
-// that carry refinement passes.
+// Gives every block its slice of the symbol scratch, settles its passes and
+// lists the blocks that carry refinement passes.
 __global__ void noalloc_prepare_kernel(HtJob* jobs, uint32_t n, uint32_t* refine, uint32_t* refine_count) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  jobs[j].sym = (uint64_t)j * kNoAllocSymbolsPerBlock;
-  if (jobs[j].passes > 1) refine[atomicAdd(refine_count, 1u)] = j;
+  HtJob& job = jobs[j];
+  job.sym = (uint64_t)j * kNoAllocSymbolsPerBlock;
+  job.passes = (uint8_t)effective_passes(job.passes, job.lref, job.mmsb);
+  if (job.passes > 1) refine[atomicAdd(refine_count, 1u)] = j;
 }
 
 }  // namespace
@@ -112,13 +128,21 @@ __global__ void noalloc_prepare_kernel(HtJob* jobs, uint32_t n, uint32_t* refine
 extern "C" {
 
 sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, const uint8_t* segments,
-                                        int32_t* coefficients, uint32_t* tile_status, uint32_t n_tiles,
-                                        void* stream) {
+                                        size_t segments_len, int32_t* coefficients, size_t coefficients_len,
+                                        uint32_t* tile_status, uint32_t n_tiles, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (n > kNoAllocMaxBlocks) return fail(SGN_ERR_INVALID_ARGUMENT, "more than 4096 code blocks in one call");
   if ((n && (!blocks || !segments || !coefficients)) || (n_tiles && !tile_status))
     return fail(SGN_ERR_INVALID_ARGUMENT, "null argument");
-  // Validate the descriptors on the host before any device work.
+  // The kernels store sample pairs with 8-byte stores wherever a block's
+  // first sample and row stride are even, which assumes an 8-byte aligned
+  // coefficient buffer.
+  if (((uintptr_t)coefficients & 7) != 0)
+    return fail(SGN_ERR_INVALID_ARGUMENT, "coefficients must be 8-byte aligned");
+  if (((uintptr_t)tile_status & 3) != 0) return fail(SGN_ERR_INVALID_ARGUMENT, "tile_status must be 4-byte aligned");
+  // Validate the descriptors on the host before any device work: every read
+  // stays inside segments[0, segments_len) and every write inside
+  // coefficients[0, coefficients_len).
   uint32_t max_w = 1, max_lcup = 0, nref = 0;
   for (uint32_t j = 0; j < n; ++j) {
     const sgn_ht_block& b = blocks[j];
@@ -128,9 +152,15 @@ sgn_status sgn_ht_decode_blocks_noalloc(const sgn_ht_block* blocks, uint32_t n, 
     if (b.passes > 3 || (b.passes && (b.lcup < 2 || b.missing_msbs >= 30)) || b.tile >= n_tiles ||
         b.stride < b.w)
       return fail(SGN_ERR_INVALID_ARGUMENT, "invalid code-block descriptor");
+    if (b.dst > coefficients_len || (uint64_t)(b.h - 1) * b.stride + b.w > coefficients_len - b.dst)
+      return fail(SGN_ERR_BUFFER, "code block outside the coefficient buffer");
+    const uint32_t passes = effective_passes(b.passes, b.lref, b.missing_msbs);
+    const uint64_t span = passes == 0 ? 0 : (uint64_t)b.lcup + (passes > 1 ? b.lref : 0);
+    if (b.src > segments_len || span > segments_len - b.src)
+      return fail(SGN_ERR_BUFFER, "code-block segment outside the segment buffer");
     if (b.w > max_w) max_w = b.w;
-    if (b.passes && b.lcup > max_lcup) max_lcup = b.lcup;
-    if (b.passes > 1) ++nref;
+    if (passes && b.lcup > max_lcup) max_lcup = b.lcup;
+    if (passes > 1) ++nref;
   }
   uint32_t ms_words = (max_lcup + 15) / 4 + 2;
   if (ht_magsgn_smem_bytes(ms_words, max_w) > 227 * 1024)

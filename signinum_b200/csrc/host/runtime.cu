@@ -885,10 +885,18 @@ sgn_status sgn_j2k_inspect(const uint8_t* data, size_t len, sgn_info* out) {
   }
 }
 
+// Backend routing of wrap_surface / validate_surface_request
+// (crates/signinum-j2k-cuda/src/runtime.rs:19-57): Cuda decodes here; Cpu and
+// Auto are the adapter's host-surface branch, which never initialises CUDA
+// (session.rs:32-38), so they return before any CUDA call; Metal is an
+// unsupported backend.
 static sgn_status check_backend(uint32_t backend) {
-  if (backend == SGN_BACKEND_CUDA || backend == SGN_BACKEND_AUTO) return SGN_OK;
-  if (backend == SGN_BACKEND_CPU || backend == SGN_BACKEND_METAL)
-    return set_error(SGN_ERR_UNSUPPORTED_BACKEND, "backend request is not supported by this CUDA decoder");
+  if (backend == SGN_BACKEND_CUDA) return SGN_OK;
+  if (backend == SGN_BACKEND_CPU || backend == SGN_BACKEND_AUTO)
+    return set_error(SGN_ERR_HOST_BACKEND,
+                     "Cpu and Auto requests take the adapter's host-surface branch; this library decodes on CUDA only");
+  if (backend == SGN_BACKEND_METAL)
+    return set_error(SGN_ERR_UNSUPPORTED_BACKEND, "backend request Metal is not supported by signinum-j2k-cuda");
   return set_error(SGN_ERR_INVALID_ARGUMENT, "unknown backend request");
 }
 
@@ -1189,9 +1197,10 @@ extern "C" {
 sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
                                           uint32_t format, const sgn_request* requests, uint32_t backend,
                                           sgn_surface* outs, sgn_status* per_tile, size_t* first_failing) {
-  if (!ctx || (n && (!datas || !lens || !outs))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  // The backend decides first: Cpu / Auto need no context and touch no CUDA.
   sgn_status bs = check_backend(backend);
   if (bs != SGN_OK) return bs;
+  if (!ctx || (n && (!datas || !lens || !outs))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   if (first_failing) *first_failing = SIZE_MAX;
   for (size_t i = 0; i < n; ++i) outs[i] = sgn_surface{};
   if (n == 0) return SGN_OK;
@@ -1300,6 +1309,8 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
 
 sgn_status sgn_j2k_decode_to_device(sgn_ctx* ctx, const uint8_t* data, size_t len, uint32_t format,
                                     const sgn_request* request, uint32_t backend, sgn_surface* out) {
+  sgn_status bs = check_backend(backend);
+  if (bs != SGN_OK) return bs;
   if (!ctx || !data || !out) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   sgn_status tile_status = SGN_OK;
   size_t first = 0;

@@ -182,9 +182,11 @@ def config1_classic(n=256, side=512, style=0, keep_pixels=False) -> Workload:
     return Workload(f"c1c_rgb8_{n}x{side}x{side}_ebcot", tiles)
 
 
-def config2(n=1024, keep_pixels=False) -> Workload:
+def config2(n=1024, keep_pixels=False, indices=None) -> Workload:
     """1024 uneven RGB8 tiles: sides {128,256,512,1024}, noise sigma U[0,30],
-    20% near-blank, levels 3..6 by side, 32x32 or 64x64 blocks."""
+    20% near-blank, levels 3..6 by side, 32x32 or 64x64 blocks.  With
+    `indices`, only those tiles of the n-tile list (each tile is a pure
+    function of n and its index)."""
     rng = np.random.default_rng(_mix(MASTER_SEED, 2) & 0xFFFFFFFF)
     sides = rng.choice([128, 256, 512, 1024], size=n)
     sigmas = rng.uniform(0, 30, size=n)
@@ -197,7 +199,7 @@ def config2(n=1024, keep_pixels=False) -> Workload:
         return _he_tile(2, i, s, float(sigmas[i]), lv[s], int(cbs[i]), keep_pixels, bool(blank[i]))
 
     with _pool() as ex:
-        tiles = list(ex.map(one, range(n)))
+        tiles = list(ex.map(one, range(n) if indices is None else indices))
     return Workload(f"c2_rgb8_uneven_{n}", tiles)
 
 

@@ -7,16 +7,21 @@ signinum-j2k-cuda adapter (crates/signinum-j2k-cuda/src/lib.rs:21-27).
 Names, argument meaning and error predicates follow the reference:
 J2kDecoder (decoder.rs:17-280), Codec (codec.rs:18-210), CudaSession
 (session.rs:11-39), Surface / CudaSurface (surface.rs:19-127), Error
-(error.rs:7-41).  Decoding always runs on the GPU through the C ABI of
-libsigninum_j2k_cuda.so; Cpu and Metal requests are rejected with an
-unsupported-backend error because this package carries no host decoder.
+(error.rs:7-41).  BackendRequest.Cuda decodes on the GPU through the C ABI
+of libsigninum_j2k_cuda.so.  Cpu and Auto keep the reference adapter's
+host-surface branch (wrap_surface, crates/signinum-j2k-cuda/src/runtime.rs:19-48):
+the caller's host decoder (the reference's own CPU J2kDecoder, registered
+with set_host_decoder) produces the bytes and the surface is a host one;
+no CUDA context is created for them.  This package carries no host decoder
+of its own, so without a registered one Cpu and Auto raise an Error whose
+is_host_backend() is true.  Metal is an unsupported backend.
 """
 from __future__ import annotations
 
 import ctypes
 import enum
 from dataclasses import dataclass
-from typing import Optional, Sequence
+from typing import Callable, Optional, Sequence
 
 import numpy as np
 
@@ -34,6 +39,7 @@ ERR_CUDA_RUNTIME = 7
 ERR_UNSUPPORTED_BACKEND = 8
 ERR_INVALID_ARGUMENT = 9
 ERR_OUT_OF_MEMORY = 10
+ERR_HOST_BACKEND = 11
 
 
 class BackendRequest(enum.IntEnum):
@@ -117,6 +123,11 @@ class Error(Exception):
 
     def is_invalid_region(self) -> bool:
         return self.status == ERR_REGION
+
+    def is_host_backend(self) -> bool:
+        """Cpu / Auto request with no host decoder registered: the adapter's
+        host branch, which this package does not implement."""
+        return self.status == ERR_HOST_BACKEND
 
 
 def _check(status: int):
@@ -207,14 +218,25 @@ class CudaSurface:
 
 
 class Surface:
-    """A decoded tile in device memory (surface.rs:55-127); tight rows."""
+    """A decoded tile (surface.rs:55-127); tight rows.  Device storage for
+    BackendRequest.Cuda, host storage for the Cpu / Auto branch."""
 
-    def __init__(self, raw: SgnSurface, ctx: _Context):
+    def __init__(self, raw: SgnSurface, ctx: Optional[_Context], host: Optional[bytes] = None):
         self._raw = raw
         self._ctx = ctx
+        self._host = host
+
+    @classmethod
+    def from_host(cls, data: bytes, dims, fmt: PixelFormat) -> "Surface":
+        raw = SgnSurface()
+        raw.width, raw.height = dims
+        raw.format = int(fmt)
+        raw.backend = int(BackendKind.Cpu)
+        raw.pitch_bytes = dims[0] * PixelFormat(fmt).bytes_per_pixel()
+        return cls(raw, None, bytes(data))
 
     def backend_kind(self) -> BackendKind:
-        return BackendKind.Cuda
+        return BackendKind.Cpu if self._host is not None else BackendKind.Cuda
 
     def dimensions(self):
         return (self._raw.width, self._raw.height)
@@ -229,23 +251,34 @@ class Surface:
         return self._raw.pitch_bytes * self._raw.height
 
     def as_host_bytes(self):
-        return None
+        return self._host
 
-    def cuda_surface(self) -> CudaSurface:
-        return CudaSurface(self)
+    def cuda_surface(self) -> Optional[CudaSurface]:
+        return CudaSurface(self) if self._host is None else None
 
     def download_into(self, out, stride: int):
         buf = out if isinstance(out, np.ndarray) else np.frombuffer(out, dtype=np.uint8)
+        if self._host is not None:
+            # Surface::download_into for host storage (surface.rs:78-92).
+            row, h = self.pitch_bytes(), self._raw.height
+            if h and (stride < row or buf.nbytes < stride * (h - 1) + row):
+                raise Error(ERR_BUFFER, "output buffer too small for the surface")
+            src = np.frombuffer(self._host, np.uint8)
+            for y in range(h):
+                buf[y * stride:y * stride + row] = src[y * row:(y + 1) * row]
+            return
         _check(_native.cuda_lib().sgn_surface_download(self._ctx.handle, ctypes.byref(self._raw),
                                                         buf.ctypes.data, buf.nbytes, stride))
 
     def to_bytes(self) -> bytes:
+        if self._host is not None:
+            return self._host
         out = np.zeros(self.byte_len(), dtype=np.uint8)
         self.download_into(out, self.pitch_bytes())
         return out.tobytes()
 
     def free(self):
-        if self._raw.device_ptr:
+        if self._host is None and self._raw.device_ptr:
             _native.cuda_lib().sgn_surface_free(self._ctx.handle, ctypes.byref(self._raw))
 
     def __del__(self):
@@ -253,6 +286,33 @@ class Surface:
             self.free()
         except Exception:
             pass
+
+
+# The host decoder of the Cpu / Auto branch: a callable
+# (codestream bytes, PixelFormat, SgnRequest) -> (pixels bytes, (width, height)).
+HostDecoder = Callable[[bytes, PixelFormat, SgnRequest], tuple]
+_host_decoder: Optional[HostDecoder] = None
+
+
+def set_host_decoder(fn: Optional[HostDecoder]) -> Optional[HostDecoder]:
+    """Registers the decoder that serves BackendRequest.Cpu and .Auto (the
+    reference's CPU J2kDecoder in a signinum process); returns the previous
+    one.  None removes it."""
+    global _host_decoder
+    prev, _host_decoder = _host_decoder, fn
+    return prev
+
+
+def _host_branch(data, fmt: PixelFormat, req: SgnRequest, backend: BackendRequest) -> Surface:
+    """wrap_surface's Cpu | Auto arm (runtime.rs:19-48): host bytes in a host
+    surface; CUDA is not touched."""
+    if PixelFormat(fmt) == PixelFormat.Rgba16:
+        raise Error(ERR_UNSUPPORTED, "Rgba16 output is not supported")
+    if _host_decoder is None:
+        raise Error(ERR_HOST_BACKEND, f"backend request {backend.name} takes the host-surface branch and no host "
+                                      "decoder is registered (set_host_decoder); this package decodes on CUDA only")
+    pixels, dims = _host_decoder(bytes(_as_u8(data)), PixelFormat(fmt), req)
+    return Surface.from_host(pixels, dims, PixelFormat(fmt))
 
 
 def _request(kind=0, roi: Optional[Rect] = None, scale: Optional[Downscale] = None) -> SgnRequest:
@@ -273,8 +333,13 @@ def _decode_one(ctx: _Context, data, fmt: PixelFormat, req: SgnRequest, backend:
 
 
 def _validate_backend(backend: BackendRequest):
-    if backend in (BackendRequest.Cpu, BackendRequest.Metal):
-        raise Error(ERR_UNSUPPORTED_BACKEND, f"backend request {backend.name} is not supported by this CUDA decoder")
+    """validate_surface_request (runtime.rs:52-57)."""
+    if BackendRequest(backend) == BackendRequest.Metal:
+        raise Error(ERR_UNSUPPORTED_BACKEND, "backend request Metal is not supported by signinum-j2k-cuda")
+
+
+def _is_host(backend: BackendRequest) -> bool:
+    return BackendRequest(backend) in (BackendRequest.Cpu, BackendRequest.Auto)
 
 
 @dataclass
@@ -307,27 +372,26 @@ class J2kDecoder:
     def info(self) -> Info:
         return self._info
 
-    def _ctx(self, session: Optional[CudaSession]):
+    def _decode(self, fmt, req: SgnRequest, backend, session: Optional[CudaSession]) -> Surface:
+        _validate_backend(backend)
         if session is not None:
             session.record_submit()
-            return session.cuda_context()
-        return _Context.default()
+        if _is_host(backend):
+            return _host_branch(self._data, fmt, req, backend)
+        ctx = session.cuda_context() if session is not None else _Context.default()
+        return _decode_one(ctx, self._data, fmt, req, backend)
 
     def decode_to_device(self, fmt: PixelFormat, backend: BackendRequest, session: Optional[CudaSession] = None):
-        _validate_backend(backend)
-        return _decode_one(self._ctx(session), self._data, fmt, _request(0), backend)
+        return self._decode(fmt, _request(0), backend, session)
 
     def decode_region_to_device(self, fmt, roi: Rect, backend, session=None):
-        _validate_backend(backend)
-        return _decode_one(self._ctx(session), self._data, fmt, _request(1, roi), backend)
+        return self._decode(fmt, _request(1, roi), backend, session)
 
     def decode_scaled_to_device(self, fmt, scale: Downscale, backend, session=None):
-        _validate_backend(backend)
-        return _decode_one(self._ctx(session), self._data, fmt, _request(2, None, scale), backend)
+        return self._decode(fmt, _request(2, None, scale), backend, session)
 
     def decode_region_scaled_to_device(self, fmt, roi: Rect, scale: Downscale, backend, session=None):
-        _validate_backend(backend)
-        return _decode_one(self._ctx(session), self._data, fmt, _request(3, roi, scale), backend)
+        return self._decode(fmt, _request(3, roi, scale), backend, session)
 
     # ImageDecodeSubmit: the submission is ready when the call returns.
     def submit_to_device(self, session: CudaSession, fmt, backend):
@@ -369,6 +433,15 @@ class Codec:
         input, order preserved; raises TileBatchError for the lowest failing
         index."""
         _validate_backend(backend)
+        if _is_host(backend):
+            surfaces = []
+            for i, d in enumerate(inputs):
+                try:
+                    surfaces.append(_host_branch(d, fmt, requests[i] if requests is not None else _request(0),
+                                                 backend))
+                except Error as e:
+                    raise TileBatchError(i, e.status, e.message) from e
+            return surfaces
         ctx = session.cuda_context() if session is not None else _Context.default()
         arrs = [_as_u8(d) for d in inputs]
         n = len(arrs)

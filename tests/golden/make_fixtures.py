@@ -19,7 +19,7 @@ Writes:
   LICENSE.OpenHTJ2K     the licence that travels with the conformance data.
 
 Run only where the reference checkout exists:
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <frames-sg/signinum checkout>
 """
 import hashlib
 import json
@@ -31,7 +31,9 @@ import sys
 
 
 def main():
-    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <frames-sg/signinum checkout>")
+    ref = pathlib.Path(sys.argv[1])
     here = pathlib.Path(__file__).parent
     fx = ref / "crates/signinum-j2k-native/fixtures/htj2k"
     out = {

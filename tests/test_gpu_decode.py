@@ -233,14 +233,6 @@ def test_unsupported_format_rejected_before_device_work():
     assert e.value.is_unsupported()
 
 
-def test_cpu_and_metal_backends_are_unsupported():
-    t = encode.config0().tiles[0]
-    for b in (BackendRequest.Cpu, BackendRequest.Metal):
-        with pytest.raises(Error) as e:
-            J2kDecoder(t.codestream).decode_to_device(PixelFormat.Rgb8, b)
-        assert e.value.is_unsupported()
-
-
 def test_invalid_region_rejected():
     t = encode.config0().tiles[0]
     with pytest.raises(Error) as e:

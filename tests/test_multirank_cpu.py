@@ -1,7 +1,8 @@
 """CPU tests of bench.py's multi-rank logic with the gloo backend, world
 size 2: every rank takes the same collective steps, the timed region is the
-max over ranks, the job value sums the replicas, and only rank 0 runs and
-prints the reference arm."""
+max over ranks, the tile list is partitioned over the ranks by coded bytes
+(every tile on exactly one rank), and only rank 0 runs and prints the
+reference arm."""
 import json
 import os
 import socket
@@ -68,3 +69,52 @@ def test_reference_arm_prints_only_on_rank_zero():
                         "--warmup", "0"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_tile_list_partition_by_coded_bytes_with_gloo():
+    """Two ranks shard a global list of uneven tiles: each encodes its
+    round-robin candidates, the coded sizes are all-gathered, both compute
+    the same balanced shards; every tile lands on exactly one rank, each
+    rank holds exactly the codestreams of its shard, and the ranks' coded
+    bytes differ by less than the largest tile."""
+    outs = _run_ranks("""
+        import datetime, json
+        import torch.distributed as dist
+        import bench
+        from signinum_b200.shard import shard_tiles
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        n_total = 24
+        idx, tiles, summary = shard_tiles(dist, n_total, lambda ix: bench.build_workload("c2", n_total, ix)[0])
+        ref = bench.build_workload("c2", n_total, idx)[0]
+        same = all(a.codestream == b.codestream for a, b in zip(tiles, ref))
+        print(json.dumps({"rank": dist.get_rank(), "idx": idx, "same": same, "summary": summary,
+                          "bytes": sum(len(t.codestream) for t in tiles)}))
+        dist.destroy_process_group()
+    """, timeout=300)
+    rows = [json.loads(o.strip().splitlines()[-1]) for o in outs]
+    idx = sorted(i for r in rows for i in r["idx"])
+    assert idx == list(range(24)), "every tile exactly once"
+    assert all(r["same"] for r in rows)
+    assert rows[0]["summary"] == rows[1]["summary"], "both ranks agree on the shards"
+    loads = rows[0]["summary"]["coded_bytes_per_rank"]
+    assert [r["bytes"] for r in sorted(rows, key=lambda r: r["rank"])] == loads
+    from signinum_b200 import encode
+
+    largest = max(len(t.codestream) for t in encode.config2(24).tiles)
+    assert abs(loads[0] - loads[1]) < largest
+
+
+def test_balance_by_coded_bytes_bounds_and_determinism():
+    import numpy as np
+
+    from signinum_b200.shard import balance_by_coded_bytes
+
+    rng = np.random.default_rng(5)
+    for world in (2, 3, 8):
+        sizes = [int(x) for x in rng.integers(1, 1 << 20, size=500)]
+        shards = balance_by_coded_bytes(sizes, world)
+        assert sorted(i for s in shards for i in s) == list(range(500))
+        loads = [sum(sizes[i] for i in s) for s in shards]
+        assert max(loads) - min(loads) < max(sizes)
+        assert shards == balance_by_coded_bytes(sizes, world)
+    assert balance_by_coded_bytes([0, 0, 0], 2) == [[0, 2], [1]]

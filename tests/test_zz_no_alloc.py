@@ -1,13 +1,16 @@
 """The HT decode entry point that allocates nothing, checked against the
 existing decode path.
 
-Some callers cannot call cudaMalloc (work recorded inside CUDA graph capture,
-a device arena owned by another framework, real-time loops that must not
-allocate once running).  sgn_ht_decode_blocks_noalloc serves them: inputs and
-outputs are the caller's device memory and its scratch is a fixed static
-device array.  Its coefficients must equal, bit for bit, the HT stage output
-of the regular plan path for the same codestream, on two calls in a row that
-share that static scratch.
+Some callers of this library cannot call cudaMalloc: a host framework whose
+caching allocator owns all of the GPU's memory, a decoder plugin that is
+handed its input and output buffers and may create none of its own, and
+real-time loops that must not allocate once they run.
+sgn_ht_decode_blocks_noalloc serves them: inputs and outputs are the
+caller's device memory and its scratch is a fixed static device array.  Its
+coefficients must equal, bit for bit (the reversible path is integer
+arithmetic, so the tolerance is zero), the HT stage output of the regular
+plan path for the same codestream, on two calls in a row that share that
+static scratch.
 
 This file is named to be collected last, so a failing run that stops at the
 first failure has already run every other test.
@@ -80,8 +83,8 @@ def test_noalloc_matches_existing_path_on_two_calls(name, cs, fmt):
     for call in range(2):
         # Poison the output so a block the call skipped would show up.
         coef.fill_(-123456789)
-        st = lib.sgn_ht_decode_blocks_noalloc(blocks, n, segments.data_ptr(), coef.data_ptr(), status.data_ptr(), 1,
-                                              ctypes.c_void_p(stream.cuda_stream))
+        st = lib.sgn_ht_decode_blocks_noalloc(blocks, n, segments.data_ptr(), segments.numel(), coef.data_ptr(),
+                                              coef.numel(), status.data_ptr(), 1, ctypes.c_void_p(stream.cuda_stream))
         assert st == 0, _native.last_error()
         torch.cuda.synchronize(dev)
         assert int(status.item()) == 0, f"call {call}: block decode failure reported"
@@ -89,14 +92,65 @@ def test_noalloc_matches_existing_path_on_two_calls(name, cs, fmt):
         assert np.array_equal(got, want), f"call {call}: coefficients differ from the existing path"
 
 
+def test_noalloc_clamps_refinement_passes_as_the_parser_does():
+    """A descriptor with 29 missing MSBs has one bit-plane left: the kernels
+    run its cleanup pass only (as the codestream parser settles it), so it
+    decodes exactly as the same descriptor with passes = 1."""
+    import torch
+
+    fx = json.loads((GOLDEN / "openhtj2k.json").read_text())["fixtures"]["openhtj2k_ds0_ht_12_b11"]
+    cs = bytes.fromhex(fx["j2k_hex"])
+    blocks, n, elems = _block_table(cs)
+    assert any(b.passes > 1 for b in blocks[:n])
+    dev = torch.device("cuda", 0)
+    segments = torch.tensor(np.frombuffer(cs, np.uint8).copy(), device=dev)
+    lib = _native.cuda_lib()
+    outs = []
+    for passes in (None, 1):
+        tbl = (SgnHtBlock * n)()
+        ctypes.memmove(tbl, blocks, ctypes.sizeof(SgnHtBlock) * n)
+        for b in tbl:
+            if b.passes > 1:
+                b.missing_msbs = 29
+                if passes is not None:
+                    b.passes = passes
+        coef = torch.full((elems,), -7, dtype=torch.int32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        st = lib.sgn_ht_decode_blocks_noalloc(tbl, n, segments.data_ptr(), segments.numel(), coef.data_ptr(),
+                                              coef.numel(), status.data_ptr(), 1, None)
+        assert st == 0, _native.last_error()
+        torch.cuda.synchronize(dev)
+        outs.append((coef.cpu().numpy(), int(status.item())))
+    assert np.array_equal(outs[0][0], outs[1][0]) and outs[0][1] == outs[1][1]
+
+
 def test_noalloc_rejects_requests_beyond_its_limit():
+    """Every rejection happens on the host, before any device work: too many
+    blocks, a block too large, a misaligned coefficient buffer, and blocks
+    reaching outside the caller's buffers."""
     lib = _native.cuda_lib()
     blocks = (SgnHtBlock * 4097)()
-    st = lib.sgn_ht_decode_blocks_noalloc(blocks, 4097, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), 1,
-                                          None)
-    assert st == 9  # SGN_ERR_INVALID_ARGUMENT, before any device work
+    st = lib.sgn_ht_decode_blocks_noalloc(blocks, 4097, ctypes.c_void_p(16), 1 << 20, ctypes.c_void_p(16), 1 << 20,
+                                          ctypes.c_void_p(16), 1, None)
+    assert st == 9  # SGN_ERR_INVALID_ARGUMENT
     assert "4096" in _native.last_error()
     one = (SgnHtBlock * 1)()
     one[0].w, one[0].h, one[0].stride, one[0].passes, one[0].lcup = 128, 64, 128, 1, 10
-    st = lib.sgn_ht_decode_blocks_noalloc(one, 1, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_void_p(1), 1, None)
+    st = lib.sgn_ht_decode_blocks_noalloc(one, 1, ctypes.c_void_p(16), 1 << 20, ctypes.c_void_p(16), 1 << 20,
+                                          ctypes.c_void_p(16), 1, None)
     assert st == 9
+    one[0].w, one[0].h, one[0].stride = 64, 64, 64
+    # A coefficient buffer offset by one element (4-byte aligned only).
+    st = lib.sgn_ht_decode_blocks_noalloc(one, 1, ctypes.c_void_p(16), 1 << 20, ctypes.c_void_p(20), 1 << 20,
+                                          ctypes.c_void_p(16), 1, None)
+    assert st == 9 and "aligned" in _native.last_error()
+    # The cleanup segment ends past the segment buffer.
+    one[0].src = 100
+    st = lib.sgn_ht_decode_blocks_noalloc(one, 1, ctypes.c_void_p(16), 109, ctypes.c_void_p(16), 1 << 20,
+                                          ctypes.c_void_p(16), 1, None)
+    assert st == 2  # SGN_ERR_BUFFER
+    # The block's last row ends past the coefficient buffer.
+    one[0].src, one[0].dst = 0, 10
+    st = lib.sgn_ht_decode_blocks_noalloc(one, 1, ctypes.c_void_p(16), 1 << 20, ctypes.c_void_p(16), 64 * 64 + 9,
+                                          ctypes.c_void_p(16), 1, None)
+    assert st == 2
