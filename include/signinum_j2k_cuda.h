@@ -228,6 +228,14 @@ typedef struct sgn_ht_block {
  * SGN_ERR_BUFFER). */
 sgn_status sgn_j2k_ht_block_table(const uint8_t* data, size_t len, sgn_ht_block* out, size_t cap, size_t* count,
                                   uint64_t* coef_elems);
+/* Diagnostics (no counterpart in the reference's interface; host only, no
+ * CUDA): the code blocks a decode of `request` (NULL: full image) at pixel
+ * format `format` decodes (*decoded) out of the blocks of the decoded
+ * resolutions (*total).  Region requests decode only the blocks their region
+ * needs (RoiPlan::code_block_required,
+ * crates/signinum-j2k-native/src/j2c/roi.rs:108-113); other requests all. */
+sgn_status sgn_j2k_request_blocks(const uint8_t* data, size_t len, uint32_t format, const sgn_request* request,
+                                  uint64_t* decoded, uint64_t* total);
 /* Diagnostics: copies tile `tile`'s sub-band coefficients (the HT stage
  * output, same layout as sgn_j2k_ht_block_table) of an executed plan to host
  * memory; *count receives the element count. */

@@ -130,6 +130,9 @@ CUDA_SIGNATURES = {
     "sgn_plan_tile_coefficients": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                                     ctypes.c_void_p, ctypes.c_size_t,
                                                     ctypes.POINTER(ctypes.c_size_t)]),
+    "sgn_j2k_request_blocks": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32,
+                                                ctypes.POINTER(SgnRequest), ctypes.POINTER(ctypes.c_uint64),
+                                                ctypes.POINTER(ctypes.c_uint64)]),
     "sgn_ht_decode_blocks_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                                       ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                                       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),

@@ -58,17 +58,31 @@ def _run(cmd):
 
 
 def build_cuda(force=False):
+    """Compiles every source to an object in parallel, then links the
+    library.  No --use_fast_math: the pack conversions call the IEEE
+    intrinsics (__fdiv_rn, __fmul_rn) explicitly and nothing else on the
+    path needs it."""
+    from concurrent.futures import ThreadPoolExecutor
+
     target = OUT / "libsigninum_j2k_cuda.so"
-    if not force and not _stale(target, _deps()):
+    deps = _deps()
+    if not force and not _stale(target, deps):
         return target
-    OUT.mkdir(exist_ok=True)
-    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--use_fast_math", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-o", target, "-I", ROOT / "include", *CUDA_SOURCES]
-    # --use_fast_math is not wanted for the pack conversions: they call the
-    # IEEE intrinsics (__fdiv_rn, __fmul_rn) explicitly, and no other float
-    # arithmetic runs on the path.
-    cmd.remove("--use_fast_math")
-    _run(cmd)
+    objdir = OUT / "obj"
+    objdir.mkdir(parents=True, exist_ok=True)
+    common = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-I", ROOT / "include"]
+
+    def compile_one(src):
+        obj = objdir / (src.stem + src.suffix.replace(".", "_") + ".o")
+        if force or _stale(obj, deps):
+            _run([NVCC, *common, "-c", "-o", obj, src])
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(CUDA_SOURCES)) as ex:
+        objs = list(ex.map(compile_one, CUDA_SOURCES))
+    tmp = target.with_suffix(".so.tmp")
+    _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs])
+    os.replace(tmp, target)  # a reader never sees a half-written library
     return target
 
 

@@ -117,7 +117,13 @@ struct IdwtJob {
   uint32_t seg;         // output rows per work unit (even)
   uint32_t ll_band;     // 9/7: ll is the LL band (dequantise) rather than a level image
   float step[4];        // 9/7: dequantisation steps of ll, hl, lh, hh
+  // Window of the level the units cover: columns from x_begin (a multiple of
+  // the strip width) over `strips` strips, rows [y_begin, y_end) with y_begin
+  // even.  The whole level (0, 0, h) unless a region request prunes it.
+  uint32_t x_begin, y_begin, y_end;
+  uint32_t pad;
 };
+static_assert(sizeof(IdwtJob) == 96, "IdwtJob layout");
 
 enum PackFormat : uint32_t { PACK_GRAY8 = 0, PACK_RGB8 = 1, PACK_RGBA8 = 2, PACK_GRAY16 = 3, PACK_RGB16 = 4 };
 

@@ -25,6 +25,7 @@
 #include "../ht_tables.h"
 #include "../kernels/kernels.h"
 #include "codestream.h"
+#include "roi.h"
 #include "runtime_internal.h"
 
 using namespace sgn;
@@ -191,12 +192,18 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   plan->status.assign(n, SGN_OK);
   plan->surfaces.assign(n, sgn_surface{});
   std::vector<TileWork> work(n);
+  // Region requests: the code blocks and IDWT windows the region needs
+  // (RoiPlan, crates/signinum-j2k-native/src/j2c/roi.rs:18-270).
+  std::vector<RoiWindows> rois(n);
   ctx->workers->parallel_for(n, [&](size_t i) {
     if (!datas[i] && lens[i]) {
       work[i].status = SGN_ERR_INVALID_ARGUMENT;
       return;
     }
     prepare_tile(datas[i], lens[i], fmt, reqs ? &reqs[i] : nullptr, work[i], layouts ? layouts[i] : nullptr);
+    const TileWork& tw = work[i];
+    if (tw.status == SGN_OK && tw.region_conv)
+      build_roi_windows(*tw.L, tw.crop_x, tw.crop_y, tw.crop_w, tw.crop_h, rois[i]);
   });
   // Arena layout.
   std::vector<uint64_t> in_off(n, 0), coef_off(n, 0), lvl_off(n, 0), lvl_size(n, 0);
@@ -268,16 +275,18 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     std::fill(t.chist, t.chist + kPassBuckets, 0u);
     if (plan->status[i] != SGN_OK) return;
     if (work[i].L->classic) {
-      t.ncls = (uint32_t)work[i].L->blocks.size();
       t.nseg = (uint32_t)work[i].L->segments.size();
       t.gather = work[i].L->gather_bytes;
       for (const CodeBlock& cb : work[i].L->blocks) {
+        if (!block_required(rois[i], cb)) continue;
+        ++t.ncls;
         ++t.chist[pass_bucket(cb.passes)];
         if (cb.passes) t.slot = std::max<uint32_t>(t.slot, classic_slot_words(cb.w, cb.h));
       }
       return;
     }
     for (const CodeBlock& cb : work[i].L->blocks) {
+      if (!block_required(rois[i], cb)) continue;
       ++t.hist[ht_bucket(cb)];
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
       if (!cb.passes) continue;
@@ -383,6 +392,18 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
         // idle (1.3 waves for 512^2 tiles).
         if (!L.reversible && j.h < 256) j.seg *= 2;
         if (j.w == 0 || j.h == 0) continue;
+        j.x_begin = j.y_begin = j.pad = 0;
+        j.y_end = j.h;
+        if (rois[i].active) {
+          // Only the level's window: whole strips from the one holding its
+          // first column, rows from an even one.
+          const Window& wnd = rois[i].level[r];
+          if (wnd.empty()) continue;
+          j.x_begin = wnd.x0 - wnd.x0 % sw;
+          j.strips = (wnd.x1 - j.x_begin + sw - 1) / sw;
+          j.y_begin = wnd.y0 & ~1u;
+          j.y_end = wnd.y1;
+        }
         rounds[L.reversible ? r - 1 : max_rounds + r - 1].push_back(j);
       }
     }
@@ -452,7 +473,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     RoundInfo ri{(uint32_t)idwt.size(), (uint32_t)rj.size(), 0, k >= max_rounds ? 1u : 0u};
     for (IdwtJob& j : rj) {
       j.unit_begin = ri.ctas;
-      ri.ctas += j.strips * ((j.h + j.seg - 1) / j.seg);
+      ri.ctas += j.strips * ((j.y_end - j.y_begin + j.seg - 1) / j.seg);
       idwt.push_back(j);
     }
     if (ri.njobs) plan->rounds.push_back(ri);
@@ -520,6 +541,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
         g += op.second;
       }
       for (const CodeBlock& cb : L.blocks) {
+        if (!block_required(rois[i], cb)) continue;
         const Band& b = L.bands[cb.band];
         ClassicJob& j = cjobs[ccur[pass_bucket(cb.passes)]++];
         std::memset(&j, 0, sizeof(j));
@@ -543,6 +565,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     uint64_t sym = sym_off[i];
     uint32_t rk = ref_off[i];
     for (const CodeBlock& cb : L.blocks) {
+      if (!block_required(rois[i], cb)) continue;
       const Band& b = L.bands[cb.band];
       const uint32_t pos = cursor[ht_bucket(cb)]++;
       HtJob& j = ht[pos];
@@ -1168,6 +1191,21 @@ sgn_status sgn_j2k_ht_block_table(const uint8_t* data, size_t len, sgn_ht_block*
   } catch (const ParseError& e) {
     return set_error(e.status, e.message.c_str());
   }
+}
+
+sgn_status sgn_j2k_request_blocks(const uint8_t* data, size_t len, uint32_t format, const sgn_request* request,
+                                  uint64_t* decoded, uint64_t* total) {
+  if (!data || !decoded || !total) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  TileWork tw;
+  prepare_tile(data, len, format, request, tw, nullptr);
+  if (tw.status != SGN_OK) return set_error(tw.status, "request rejected");
+  RoiWindows roi;
+  if (tw.region_conv) build_roi_windows(*tw.L, tw.crop_x, tw.crop_y, tw.crop_w, tw.crop_h, roi);
+  uint64_t k = 0;
+  for (const CodeBlock& cb : tw.L->blocks) k += block_required(roi, cb) ? 1 : 0;
+  *decoded = k;
+  *total = tw.L->blocks.size();
+  return SGN_OK;
 }
 
 void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan) {

@@ -303,10 +303,10 @@ __device__ __forceinline__ void idwt_unit(const IdwtJob* __restrict__ jobs, uint
   const int lane = threadIdx.x & 31;
   const IdwtJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
-  const int x0 = (int)(local % job.strips) * kIdwtStripW;
-  const int ys = (int)(local / job.strips) * (int)job.seg;
+  const int x0 = (int)job.x_begin + (int)(local % job.strips) * kIdwtStripW;
+  const int ys = (int)job.y_begin + (int)(local / job.strips) * (int)job.seg;
   const int w = (int)job.w, h = (int)job.h;
-  const int ye = min(ys + (int)job.seg, h);
+  const int ye = min(ys + (int)job.seg, (int)job.y_end);
   const Bands B = make_bands(job.ll, job.hl, job.lh, job.hh, w, h);
   const int b = (x0 >> 1) + 2 * lane, col = 2 * b;
   int32_t* out = job.out;
@@ -777,10 +777,10 @@ __device__ __forceinline__ void idwt97_unit(const IdwtJob* __restrict__ jobs, ui
   const int lane = threadIdx.x & 31;
   const IdwtJob& job = find_job(jobs, njobs, unit);
   const uint32_t local = unit - job.unit_begin;
-  const int x0 = (int)(local % job.strips) * kStrip97;
-  const int ys = (int)(local / job.strips) * (int)job.seg;
+  const int x0 = (int)job.x_begin + (int)(local % job.strips) * kStrip97;
+  const int ys = (int)job.y_begin + (int)(local / job.strips) * (int)job.seg;
   const int w = (int)job.w, h = (int)job.h;
-  const int ye = min(ys + (int)job.seg, h);
+  const int ye = min(ys + (int)job.seg, (int)job.y_end);
   const int col = x0 - 4 + 4 * lane;
   const Src97 S = make_src97(job.ll, job.hl, job.lh, job.hh, job.step, job.ll_band != 0, w, h, x0 - 4);
   float* out = reinterpret_cast<float*>(job.out);

@@ -245,6 +245,8 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
       j.step[0] = T.bands[b0].step;
       for (int k = 0; k < 3; ++k) j.step[1 + k] = T.bands[b0 + 1 + (r - 1) * 3 + k].step;
       j.unit_begin = units;
+      j.x_begin = j.y_begin = 0;
+      j.y_end = j.h;
       if (j.w == 0 || j.h == 0) continue;
       units += j.strips * ((j.h + j.seg - 1) / j.seg);
       ij.push_back(j);
