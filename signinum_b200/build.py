@@ -31,6 +31,7 @@ CUDA_SOURCES = [
     CSRC / "host" / "server.cu",
     CSRC / "host" / "dicom.cpp",
     CSRC / "host" / "codestream.cpp",
+    CSRC / "host" / "profile.cpp",
 ]
 ENCODE_SOURCES = [
     CSRC / "encode" / "j2k_encode.cpp",

@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +27,7 @@
 #include "../ht_tables.h"
 #include "../kernels/kernels.h"
 #include "codestream.h"
+#include "profile.h"
 #include "roi.h"
 #include "runtime_internal.h"
 
@@ -261,7 +264,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // staging bound.  Each coded block gets a quad-symbol table of
   // ceil(w/2) x ceil(h/2) words in the symbol scratch.
   struct TileHt {
-    uint64_t sym = 0;
+    uint64_t sym = 0, bytes = 0;
     uint32_t nref = 0, ms_words = 8, ms_half = 0, max_w = 1;
     uint32_t hist[kHtBuckets];
     uint32_t ncls = 0, nseg = 0, slot = 0;  // classic tiles
@@ -291,6 +294,7 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
       t.max_w = std::max<uint32_t>(t.max_w, cb.w);
       if (!cb.passes) continue;
       t.sym += sym_words(cb.w, cb.h);
+      t.bytes += cb.lcup;
       if (cb.passes > 1) ++t.nref;
       if (cb.ms_words) {  // from the parse (cached layouts carry it)
         t.ms_words = std::max<uint32_t>(t.ms_words, cb.ms_words);
@@ -343,6 +347,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   plan->ms_words = std::max(ms_words, 2 * ms_half);
   plan->max_w = max_w;
   plan->nref = nref;
+  plan->ht_cleanup_bytes = 0;
+  for (size_t i = 0; i < n; ++i) plan->ht_cleanup_bytes += th[i].bytes;
   if (ht_magsgn_smem_bytes(plan->ms_words, max_w) > 227 * 1024)
     return set_error(SGN_ERR_UNSUPPORTED, "code-block segment too long for the MagSgn staging buffer");
   if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
@@ -719,25 +725,32 @@ void release_plan(sgn_plan* p, cudaStream_t s) {
   free_plan_buffers(p, s);
 }
 
-sgn_status execute(sgn_plan* p, cudaStream_t s) {
+sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev) {
   cudaError_t e;
   const LaunchConfig& c = p->cfg;
+  auto mark = [&](int k) { return ev ? cudaEventRecord(ev[k], s) : cudaSuccess; };
   if (p->n && (e = cudaMemsetAsync(p->d_status, 0, p->n * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "status reset");
   if (p->d_queue && (e = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "work queue reset");
+  if ((e = mark(0)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads)) != cudaSuccess)
     return cuda_status(e, "HT VLC launch");
+  if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
                             s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas, p->nsingle)) !=
       cudaSuccess)
     return cuda_status(e, "HT MagSgn launch");
+  if ((e = mark(2)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
   if ((e = launch_classic_blocks(p, s)) != cudaSuccess) return cuda_status(e, "classic block launch");
+  if ((e = mark(3)) != cudaSuccess) return cuda_status(e, "event record");
   for (size_t k = 0; k < p->rounds.size(); ++k)
     if ((e = launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas)) != cudaSuccess) return cuda_status(e, "IDWT launch");
+  if ((e = mark(4)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_packs(p, s, c.pack_queue != 0, c.pack_ctas)) != cudaSuccess) return cuda_status(e, "pack launch");
+  if ((e = mark(5)) != cudaSuccess) return cuda_status(e, "event record");
   return SGN_OK;
 }
 
@@ -959,35 +972,16 @@ sgn_status sgn_plan_execute_async(sgn_ctx* ctx, sgn_plan* plan) {
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* p, float* stage_ms) {
   if (!ctx || !p || !stage_ms) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   cudaSetDevice(ctx->device);
-  cudaStream_t s = ctx->stream;
   cudaEvent_t ev[6];
   for (auto& e : ev) cudaEventCreate(&e);
-  cudaError_t e = cudaSuccess;
-  auto chk = [&](cudaError_t x) {
-    if (e == cudaSuccess) e = x;
-  };
-  const LaunchConfig& c = p->cfg;
-  chk(cudaMemsetAsync(p->d_status, 0, std::max<size_t>(p->n, 1) * sizeof(uint32_t), s));
-  if (p->d_queue) chk(cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s));
-  chk(cudaEventRecord(ev[0], s));
-  chk(launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads));
-  chk(cudaEventRecord(ev[1], s));
-  chk(launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w, s,
-                       c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas, p->nsingle));
-  chk(cudaEventRecord(ev[2], s));
-  chk(launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s));
-  chk(launch_classic_blocks(p, s));
-  chk(cudaEventRecord(ev[3], s));
-  for (size_t k = 0; k < p->rounds.size(); ++k) chk(launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas));
-  chk(cudaEventRecord(ev[4], s));
-  chk(launch_packs(p, s, c.pack_queue != 0, c.pack_ctas));
-  chk(cudaEventRecord(ev[5], s));
-  chk(cudaEventSynchronize(ev[5]));
-  if (e == cudaSuccess) {
+  sgn_status st = execute(p, ctx->stream, ev);
+  cudaError_t e = st == SGN_OK ? cudaEventSynchronize(ev[5]) : cudaSuccess;
+  if (st == SGN_OK && e == cudaSuccess) {
     for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
     cudaEventElapsedTime(&stage_ms[5], ev[0], ev[5]);
   }
   for (auto& x : ev) cudaEventDestroy(x);
+  if (st != SGN_OK) return st;
   return cuda_status(e, "timed execute");
 }
 
@@ -1232,13 +1226,101 @@ void sgn_surface_free_locked(sgn_ctx* ctx, sgn_surface* sf) {
 
 extern "C" {
 
+}  // extern "C"
+
+namespace {
+
+const char* backend_name(uint32_t b) {
+  static const char* const names[] = {"Auto", "Cpu", "Metal", "Cuda"};
+  return b < 4 ? names[b] : "Unknown";
+}
+
+const char* format_name(uint32_t f) {
+  static const char* const names[] = {"Gray8", "Rgb8", "Rgba8", "Gray16", "Rgb16", "Rgba16"};
+  return f < 6 ? names[f] : "Unknown";
+}
+
+const char* request_op(const sgn_request* r) {
+  static const char* const names[] = {"full", "region", "scaled", "region_scaled"};
+  return (r && r->kind < 4) ? names[r->kind] : "full";
+}
+
+// A GPU route row (SIGNINUM_GPU_ROUTE_PROFILE) for a call that did not reach
+// the device: the adapter's host branch for Cpu / Auto, or an unsupported
+// backend.  Dimensions come from a host parse of the header.
+void route_not_decoded(const char* op, uint32_t backend, uint32_t format, const uint8_t* data, size_t len,
+                       sgn_status st, size_t tiles) {
+  if (prof::route_mode() == prof::Mode::Disabled) return;
+  prof::Fields f{{"op", op}, {"request", backend_name(backend)}, {"fmt", format_name(format)}};
+  if (tiles != 1) {
+    f.emplace_back("tiles", std::to_string(tiles));
+  } else if (data) {
+    try {
+      Info i = inspect_codestream(data, len);
+      f.emplace_back("width", std::to_string(i.width));
+      f.emplace_back("height", std::to_string(i.height));
+    } catch (const ParseError&) {
+    }
+  }
+  f.emplace_back("decision", st == SGN_ERR_HOST_BACKEND ? "host_surface" : "unsupported_backend");
+  prof::emit_route("j2k", "cuda", f);
+}
+
+// Device stage times of a call's plans (SIGNINUM_J2K_PROFILE_STAGES).
+struct StageTimes {
+  bool on = false;
+  uint64_t build_us = 0, blocks = 0, refine_blocks = 0, cleanup_bytes = 0;
+  double ms[5] = {0, 0, 0, 0, 0};  // VLC, MagSgn, refinement + classic, IDWT, pack
+};
+
+sgn_status decode_tiles_impl(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
+                             uint32_t format, const sgn_request* requests, sgn_surface* outs, sgn_status* per_tile,
+                             size_t* first_failing, StageTimes& prof_st);
+
+}  // namespace
+
+extern "C" {
+
 sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
                                           uint32_t format, const sgn_request* requests, uint32_t backend,
                                           sgn_surface* outs, sgn_status* per_tile, size_t* first_failing) {
   // The backend decides first: Cpu / Auto need no context and touch no CUDA.
   sgn_status bs = check_backend(backend);
-  if (bs != SGN_OK) return bs;
+  if (bs != SGN_OK) {
+    route_not_decoded("tile_batch", backend, format, nullptr, 0, bs, n);
+    return bs;
+  }
   if (!ctx || (n && (!datas || !lens || !outs))) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  const auto t0 = std::chrono::steady_clock::now();
+  StageTimes pst;
+  pst.on = prof::stage_mode() != prof::Mode::Disabled;
+  sgn_status st = decode_tiles_impl(ctx, datas, lens, n, format, requests, outs, per_tile, first_failing, pst);
+  if (pst.on && n) {
+    const uint64_t total_us =
+        (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+    auto us = [](double ms) { return std::to_string((uint64_t)(ms * 1000.0 + 0.5)); };
+    prof::emit_stages("j2k", "decode", "cuda",
+                      {{"tiles", std::to_string(n)}, {"build_us", std::to_string(pst.build_us)},
+                       {"ht_blocks", std::to_string(pst.blocks)}, {"ht_refinement_blocks", std::to_string(pst.refine_blocks)},
+                       {"ht_cleanup_bytes", std::to_string(pst.cleanup_bytes)},
+                       {"ht_cleanup_us", us(pst.ms[0] + pst.ms[1])}, {"ht_vlc_us", us(pst.ms[0])},
+                       {"ht_mag_sgn_us", us(pst.ms[1])}, {"ht_refine_us", us(pst.ms[2])}, {"idwt_us", us(pst.ms[3])},
+                       {"pack_us", us(pst.ms[4])}, {"total_us", std::to_string(total_us)}});
+  }
+  if (n > 1 && prof::route_mode() != prof::Mode::Disabled)
+    prof::emit_route("j2k", "cuda",
+                     {{"op", "tile_batch"}, {"request", "Cuda"}, {"fmt", format_name(format)},
+                      {"tiles", std::to_string(n)}, {"decision", st == SGN_OK ? "cuda_decode" : "cuda_error"}});
+  return st;
+}
+
+}  // extern "C"
+
+namespace {
+
+sgn_status decode_tiles_impl(sgn_ctx* ctx, const uint8_t* const* datas, const size_t* lens, size_t n,
+                             uint32_t format, const sgn_request* requests, sgn_surface* outs, sgn_status* per_tile,
+                             size_t* first_failing, StageTimes& pst) {
   if (first_failing) *first_failing = SIZE_MAX;
   for (size_t i = 0; i < n; ++i) outs[i] = sgn_surface{};
   if (n == 0) return SGN_OK;
@@ -1266,6 +1348,7 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     }
   }
   std::vector<sgn_plan*> plans(K, nullptr);
+  std::vector<std::array<cudaEvent_t, 6>> events(K);
   std::vector<sgn_status> statuses(n, SGN_OK);
   sgn_status st = SGN_OK;
   // Pinned codestreams laid out back to back (16-byte padded): every chunk's
@@ -1294,6 +1377,7 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     const size_t b = cut[c], m = cut[c + 1] - b;
     if (m == 0) continue;
     plans[c] = new sgn_plan();
+    const auto tb = std::chrono::steady_clock::now();
     try {
       st = build_plan(ctx, ctx->lanes[c], ctx->lane_staging[c], datas + b, lens + b, m, format,
                       requests ? requests + b : nullptr, plans[c], arenas[c], up_front ? roffs[c].data() : nullptr,
@@ -1301,7 +1385,12 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     } catch (const std::bad_alloc&) {
       st = set_error(SGN_ERR_OUT_OF_MEMORY, "host allocation failed");
     }
-    if (st == SGN_OK) st = execute(plans[c], ctx->lanes[c]);
+    if (pst.on) {
+      pst.build_us += (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(
+                          std::chrono::steady_clock::now() - tb).count();
+      for (auto& e : events[c]) cudaEventCreate(&e);
+    }
+    if (st == SGN_OK) st = execute(plans[c], ctx->lanes[c], pst.on ? events[c].data() : nullptr);
   }
   sgn_status wst = SGN_OK;
   size_t first = SIZE_MAX;
@@ -1311,6 +1400,16 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     size_t f = SIZE_MAX;
     if (st == SGN_OK) {
       wait_plan(plans[c], ctx->lanes[c], statuses.data() + b, &f);
+      if (pst.on) {
+        for (int k = 0; k < 5; ++k) {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, events[c][k], events[c][k + 1]) == cudaSuccess) pst.ms[k] += ms;
+        }
+        cudaGetLastError();
+        pst.blocks += plans[c]->nht + plans[c]->nclassic;
+        pst.refine_blocks += plans[c]->nref;
+        pst.cleanup_bytes += plans[c]->ht_cleanup_bytes;
+      }
       if (f != SIZE_MAX && first == SIZE_MAX) {
         first = b + f;
         wst = statuses[b + f];
@@ -1325,6 +1424,8 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
     }
     release_plan(plans[c], ctx->lanes[c]);
     delete plans[c];
+    if (pst.on)
+      for (auto& e : events[c]) cudaEventDestroy(e);
   }
   for (size_t c = 0; c < K; ++c)
     if (arenas[c]) {
@@ -1345,17 +1446,36 @@ sgn_status sgn_j2k_decode_tiles_to_device(sgn_ctx* ctx, const uint8_t* const* da
   return wst;
 }
 
+}  // namespace
+
+extern "C" {
+
 sgn_status sgn_j2k_decode_to_device(sgn_ctx* ctx, const uint8_t* data, size_t len, uint32_t format,
                                     const sgn_request* request, uint32_t backend, sgn_surface* out) {
   sgn_status bs = check_backend(backend);
-  if (bs != SGN_OK) return bs;
+  if (bs != SGN_OK) {
+    route_not_decoded(request_op(request), backend, format, data, len, bs, 1);
+    return bs;
+  }
   if (!ctx || !data || !out) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   sgn_status tile_status = SGN_OK;
   size_t first = 0;
   sgn_status st = sgn_j2k_decode_tiles_to_device(ctx, &data, &len, 1, format, request, backend, out, &tile_status,
                                                  &first);
-  if (st != SGN_OK) return st;
-  return tile_status;
+  if (st == SGN_OK) st = tile_status;
+  if (prof::route_mode() != prof::Mode::Disabled) {
+    prof::Fields f{{"op", request_op(request)}, {"request", "Cuda"}, {"fmt", format_name(format)}};
+    if (st == SGN_OK) {
+      f.emplace_back("width", std::to_string(out->width));
+      f.emplace_back("height", std::to_string(out->height));
+      f.emplace_back("decision", "cuda_decode");
+      f.emplace_back("kernel_dispatches", std::to_string(out->kernel_dispatches));
+    } else {
+      f.emplace_back("decision", "cuda_error");
+    }
+    prof::emit_route("j2k", "cuda", f);
+  }
+  return st;
 }
 
 sgn_status sgn_surface_download(sgn_ctx* ctx, const sgn_surface* sf, uint8_t* out, size_t out_len, size_t stride) {

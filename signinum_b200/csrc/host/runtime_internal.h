@@ -198,6 +198,7 @@ struct sgn_plan {
   uint32_t npack97 = 0, pack97_ctas = 0;
   std::vector<RoundInfo> rounds;
   uint64_t launches = 0;
+  uint64_t ht_cleanup_bytes = 0;  // cleanup segment bytes of the HT jobs (profiling rows)
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
   // Launch shape and the device work-queue counters (one per queued launch:
@@ -233,7 +234,10 @@ sgn_status build_plan(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, const
                       const uint8_t* resident_arena = nullptr, const uint64_t* resident_off = nullptr,
                       const TileLayout* const* layouts = nullptr, bool sync_uploads = true);
 // Enqueues the plan's kernels on s.
-sgn_status execute(sgn_plan* p, cudaStream_t s);
+// Launches the plan's kernels on s.  With `ev` (6 events), records ev[0]
+// before the HT VLC pass and ev[k] after stage k: VLC, MagSgn, refinement
+// and classic blocks, IDWT levels, packs (ev[5] after the last).
+sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev = nullptr);
 // Reads the per-tile device status (synchronising s) and merges host statuses.
 sgn_status wait_plan(sgn_plan* p, cudaStream_t s, sgn_status* per_tile, size_t* first_failing);
 void free_plan_buffers(sgn_plan* p, cudaStream_t s);
