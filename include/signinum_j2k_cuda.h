@@ -166,19 +166,25 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms)
  * (VLC lanes per CTA; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
  * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
- * IDWT levels, bit 1 = pack), keeps the fastest per
+ * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
+ * the base rows per unit scaled by 2^shift, shift -1, 0 or 1), keeps the fastest per
  * stage for the plan and for later plans of the same shape on this context,
  * and re-executes the plan so its surfaces hold the decode.  Synchronous. */
 typedef struct sgn_tune_report {
   uint32_t vlc_threads, ms_warps, ms_blocks_per_grab, dwt_queue;  /* chosen shape */
   float vlc_ms, ms_ms, dwt_ms;                                     /* its stage times */
   float vlc_ms_default, ms_ms_default, dwt_ms_default;             /* the default shape's */
+  int32_t idwt_seg_shift, pack_seg_shift;                          /* chosen DWT tile shape (rows x 2^shift) */
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;
  * vlc_threads 32..128 in steps of 32, ms_warps 1..8, dwt_queue 0..3). */
 sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_threads, uint32_t ms_warps,
                                      uint32_t ms_blocks_per_grab, uint32_t dwt_queue);
+/* Sets the DWT tile shape by hand: rows per work unit of the IDWT levels and
+ * of the last level + pack, the base rule scaled by 2^shift (shift -1, 0 or
+ * 1; strips stay 128 columns wide).  Re-uploads the plan's job tables. */
+sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* plan, int32_t idwt_seg_shift, int32_t pack_seg_shift);
 /* Launches issued by one execute of the plan. */
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);
 void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan);

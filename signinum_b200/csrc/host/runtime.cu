@@ -494,6 +494,17 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   plan->npack = (uint32_t)packs.size();
   plan->npack97 = (uint32_t)packs97.size();
   packs.insert(packs.end(), packs97.begin(), packs97.end());
+  // The launch shape: an autotuned one when this context has tuned a plan of
+  // the same signature (computed on the base tile shapes); its rows per
+  // unit are applied to the job tables before they go up.
+  LaunchConfig cfg;
+  plan->sig = plan_signature(plan);
+  {
+    std::lock_guard<std::mutex> g(ctx->tune_mu);
+    for (auto& t : ctx->tuned)
+      if (t.first == plan->sig) cfg = t.second;
+  }
+  if (cfg.idwt_seg_shift || cfg.pack_seg_shift) set_segments(plan, idwt, packs, cfg.idwt_seg_shift, cfg.pack_seg_shift);
   if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
   if ((e = dalloc(&plan->d_refine, nref, s)) != cudaSuccess) return cuda_status(e, "refine list");
   plan->nclassic = ncls;
@@ -624,13 +635,8 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // context has tuned a plan of the same signature).
   plan->nqueues = (uint32_t)plan->rounds.size() + 3 + kPackVariants;
   if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
-  LaunchConfig cfg;
-  {
-    const uint64_t sig = plan_signature(plan);
-    std::lock_guard<std::mutex> g(ctx->tune_mu);
-    for (auto& t : ctx->tuned)
-      if (t.first == sig) cfg = t.second;
-  }
+  plan->h_idwt = std::move(idwt);
+  plan->h_pack = std::move(packs);
   return apply_config(ctx, plan, cfg);
 }
 
@@ -648,6 +654,49 @@ uint64_t plan_signature(const sgn_plan* p) {
   return (uint64_t)p->format | (lg(p->nht + 1) << 4) | (lg(p->max_w) << 10) | (lg(p->ms_words) << 14) |
          (lg(p->pack_ctas + 1) << 20) | ((uint64_t)p->rounds.size() << 26) | ((uint64_t)(p->nref > 0) << 31) |
          ((uint64_t)lg(p->pack97_ctas + 1) << 32);
+}
+
+namespace {
+
+uint32_t scaled_seg(uint32_t base, int shift) {
+  uint32_t s = shift > 0 ? base << shift : shift < 0 ? base >> -shift : base;
+  return std::max<uint32_t>(2, s & ~1u);
+}
+
+}  // namespace
+
+void set_segments(sgn_plan* p, std::vector<IdwtJob>& idwt, std::vector<PackJob>& packs, int ishift, int pshift) {
+  for (RoundInfo& r : p->rounds) {
+    r.ctas = 0;
+    for (uint32_t k = r.job_begin; k < r.job_begin + r.njobs; ++k) {
+      IdwtJob& j = idwt[k];
+      // The build's rule: 9/7 units re-read seven rows, so levels under 256
+      // rows take doubled segments.
+      const uint32_t base = idwt_segment_rows(j.h) * (r.irreversible && j.h < 256 ? 2 : 1);
+      j.seg = scaled_seg(base, ishift);
+      j.unit_begin = r.ctas;
+      r.ctas += j.strips * ((j.y_end - j.y_begin + j.seg - 1) / j.seg);
+    }
+  }
+  auto units = [](PackJob& j) { return j.strips * ((j.cy + j.ch - (j.cy & ~1u) + j.seg - 1) / j.seg); };
+  p->pack_ctas = 0;
+  for (uint32_t v = 0; v < kPackVariants; ++v) {
+    p->pack_units_v[v] = 0;
+    for (uint32_t k = p->pack_begin[v]; k < p->pack_begin[v] + p->npack_v[v]; ++k) {
+      PackJob& j = packs[k];
+      j.seg = scaled_seg(idwt_segment_rows(j.ch), pshift);
+      j.unit_begin = p->pack_units_v[v];
+      p->pack_units_v[v] += units(j);
+    }
+    p->pack_ctas += p->pack_units_v[v];
+  }
+  p->pack97_ctas = 0;
+  for (uint32_t k = p->npack; k < p->npack + p->npack97; ++k) {
+    PackJob& j = packs[k];
+    j.seg = scaled_seg(idwt_segment_rows(j.ch), pshift);
+    j.unit_begin = p->pack97_ctas;
+    p->pack97_ctas += units(j);
+  }
 }
 
 sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
@@ -1024,6 +1073,30 @@ sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_thr
   c.ms_gran = ms_blocks_per_grab;
   c.idwt_queue = dwt_queue & 1;
   c.pack_queue = (dwt_queue >> 1) & 1;
+  // The tile shape stays the one the plan's job tables were built with.
+  c.idwt_seg_shift = p->cfg.idwt_seg_shift;
+  c.pack_seg_shift = p->cfg.pack_seg_shift;
+  return apply_config(ctx, p, c);
+}
+
+sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* p, int32_t idwt_seg_shift, int32_t pack_seg_shift) {
+  if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  if (idwt_seg_shift < -1 || idwt_seg_shift > 1 || pack_seg_shift < -1 || pack_seg_shift > 1)
+    return set_error(SGN_ERR_INVALID_ARGUMENT, "tile shape shift out of range");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  set_segments(p, p->h_idwt, p->h_pack, idwt_seg_shift, pack_seg_shift);
+  cudaError_t e = cudaSuccess;
+  if (!p->h_idwt.empty())
+    e = cudaMemcpyAsync(p->d_idwt, p->h_idwt.data(), p->h_idwt.size() * sizeof(IdwtJob), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !p->h_pack.empty())
+    e = cudaMemcpyAsync(p->d_pack, p->h_pack.data(), p->h_pack.size() * sizeof(PackJob), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "tile shape upload");
+  LaunchConfig c = p->cfg;
+  c.idwt_seg_shift = idwt_seg_shift;
+  c.pack_seg_shift = pack_seg_shift;
   return apply_config(ctx, p, c);
 }
 
@@ -1070,32 +1143,52 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     if (m.warps == 8 && m.gran == 0) rep.ms_ms_default = ms;
     if (e == cudaSuccess && ms < best_ms) best_ms = ms, ms_warps = m.warps, ms_gran = m.gran;
   }
-  // IDWT levels and pack, each: one unit per warp, or persistent warps on a queue.
+  // IDWT levels and pack, each: one unit per warp or persistent warps on a
+  // queue, and the DWT tile shape (rows per unit: the base rule scaled by
+  // 2^shift, shift -1, 0 or 1; the strip is 128 columns, four per lane).
+  auto set_shape = [&](int is, int ps) {
+    set_segments(p, p->h_idwt, p->h_pack, is, ps);
+    cudaError_t x = cudaSuccess;
+    if (!p->h_idwt.empty())
+      x = cudaMemcpyAsync(p->d_idwt, p->h_idwt.data(), p->h_idwt.size() * sizeof(IdwtJob), cudaMemcpyHostToDevice, s);
+    if (x == cudaSuccess && !p->h_pack.empty())
+      x = cudaMemcpyAsync(p->d_pack, p->h_pack.data(), p->h_pack.size() * sizeof(PackJob), cudaMemcpyHostToDevice, s);
+    if (x == cudaSuccess) x = cudaStreamSynchronize(s);
+    return x;
+  };
   float best_idwt = 1e30f, best_pack = 1e30f, idwt_default = 0.f, pack_default = 0.f;
   uint32_t idwt_queue = 0, pack_queue = 0;
-  for (uint32_t q = 0; q < 2; ++q) {
-    const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
-    float ms = time_stage(s, reps, [&] {
-      cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
-      for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, q != 0, ictas);
-      return x;
-    }, e);
-    if (q == 0) idwt_default = ms;
-    if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q;
-    ms = time_stage(s, reps, [&] {
-      cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
-      if (x == cudaSuccess) x = launch_packs(p, s, q != 0, pctas);
-      return x;
-    }, e);
-    if (q == 0) pack_default = ms;
-    if (e == cudaSuccess && ms < best_pack) best_pack = ms, pack_queue = q;
+  int idwt_shift = 0, pack_shift = 0;
+  const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
+  for (int sh = -1; sh <= 1 && e == cudaSuccess; ++sh) {
+    if ((e = set_shape(sh, sh)) != cudaSuccess) break;
+    for (uint32_t q = 0; q < 2; ++q) {
+      float ms = time_stage(s, reps, [&] {
+        cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
+        for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, q != 0, ictas);
+        return x;
+      }, e);
+      if (q == 0 && sh == 0) idwt_default = ms;
+      if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q, idwt_shift = sh;
+      ms = time_stage(s, reps, [&] {
+        cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
+        if (x == cudaSuccess) x = launch_packs(p, s, q != 0, pctas);
+        return x;
+      }, e);
+      if (q == 0 && sh == 0) pack_default = ms;
+      if (e == cudaSuccess && ms < best_pack) best_pack = ms, pack_queue = q, pack_shift = sh;
+    }
   }
   rep.dwt_ms_default = idwt_default + pack_default;
   const float best_dwt = best_idwt + best_pack;
+  if (e == cudaSuccess) e = set_shape(idwt_shift, pack_shift);
   if (e != cudaSuccess) {
+    set_shape(base.idwt_seg_shift, base.pack_seg_shift);
     apply_config(ctx, p, base);
     return cuda_status(e, "autotune");
   }
+  cfg.idwt_seg_shift = idwt_shift;
+  cfg.pack_seg_shift = pack_shift;
   cfg.vlc_threads = vlc_threads;
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
@@ -1108,7 +1201,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   st = execute(p, s);
   if (st == SGN_OK) st = cuda_status(cudaStreamSynchronize(s), "autotune");
   {
-    const uint64_t sig = plan_signature(p);
+    const uint64_t sig = p->sig;
     std::lock_guard<std::mutex> tg(ctx->tune_mu);
     bool found = false;
     for (auto& t : ctx->tuned)
@@ -1119,6 +1212,8 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
   rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);
+  rep.idwt_seg_shift = cfg.idwt_seg_shift;
+  rep.pack_seg_shift = cfg.pack_seg_shift;
   rep.vlc_ms = best_vlc;
   rep.ms_ms = best_ms;
   rep.dwt_ms = best_dwt;

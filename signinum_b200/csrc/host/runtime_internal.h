@@ -132,6 +132,9 @@ struct LaunchConfig {
   uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
   uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue
   uint32_t pack_queue = 0;     // the same for the last level + pack
+  // DWT tile shape: rows per work unit of the IDWT levels and of the pack,
+  // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -1..1.
+  int32_t idwt_seg_shift = 0, pack_seg_shift = 0;
   // Persistent grid sizes (SMs x resident CTAs), derived from the above.
   uint32_t ms_ctas = 0, idwt_ctas = 0, pack_ctas = 0;
 };
@@ -197,7 +200,12 @@ struct sgn_plan {
            pack_units_v[sgn::kPackVariants] = {};
   uint32_t npack97 = 0, pack97_ctas = 0;
   std::vector<RoundInfo> rounds;
+  // Host copies of the IDWT and pack job tables (as uploaded), so that the
+  // autotuner can change their rows per unit.
+  std::vector<IdwtJob> h_idwt;
+  std::vector<PackJob> h_pack;
   uint64_t launches = 0;
+  uint64_t sig = 0;  // plan_signature on the base tile shapes (the autotuner's cache key)
   uint64_t ht_cleanup_bytes = 0;  // cleanup segment bytes of the HT jobs (profiling rows)
   std::vector<uint32_t> h_status;
   std::vector<uint64_t> tile_coef_off, tile_coef_elems;  // per tile, in d_coef
@@ -250,6 +258,11 @@ cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queue
 // The classic (EBCOT) code-block kernel over the plan's classic jobs.
 cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s);
 cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas);
+// Rows per work unit of the plan's IDWT jobs and pack jobs: the base rule of
+// each job scaled by 2^ishift / 2^pshift (at least 2 rows, even), with the
+// units of every job, round and pack launch recomputed to match.
+void set_segments(sgn_plan* p, std::vector<sgn::IdwtJob>& idwt, std::vector<sgn::PackJob>& packs, int ishift,
+                  int pshift);
 // Workload signature for the autotuner cache: pixel format, job counts and
 // block shape classes.
 uint64_t plan_signature(const sgn_plan* p);

@@ -66,6 +66,11 @@ class Plan:
         _check(_native.cuda_lib().sgn_plan_set_launch_shape(self.ctx.handle, self.handle, vlc_threads, ms_warps,
                                                             ms_blocks_per_grab, dwt_queue))
 
+    def set_tile_shape(self, idwt_seg_shift=0, pack_seg_shift=0):
+        """Rows per IDWT / pack work unit: the base rule scaled by 2^shift."""
+        _check(_native.cuda_lib().sgn_plan_set_tile_shape(self.ctx.handle, self.handle, idwt_seg_shift,
+                                                          pack_seg_shift))
+
     def execute_timed(self):
         """Per-stage milliseconds: HT VLC pass, HT MagSgn pass, HT refinement, IDWT levels,
         last level + pack, total."""

@@ -54,3 +54,40 @@ def test_autotune_keeps_output_and_is_reused(batch):
     st, _ = plan.wait()
     assert st == 0 and [plan.download(i) for i in range(len(batch))] == want
     plan.destroy()
+
+
+@pytest.mark.parametrize("shift", [(-1, -1), (1, 1), (-1, 1), (1, 0)])
+def test_dwt_tile_shapes_are_bit_exact(shift):
+    """Rows per IDWT / pack unit halved or doubled, on reversible and
+    irreversible tiles and on pruned region decodes (windowed levels)."""
+    from signinum_b200.j2k_cuda import Rect, _request
+
+    tiles = encode.config2(n=6).tiles
+    lossy = encode.encode_irreversible(encode.he_rgb8(5, 300, 200, 9.0), 300, 200, 3, 8, 1 / 256, levels=4, cb_exp=4)
+    big = tiles[[t.width for t in tiles].index(max(t.width for t in tiles))]
+    roi = Rect(big.width // 3, big.height // 4, 77, 45)
+    inputs = [t.codestream for t in tiles] + [lossy, big.codestream]
+    reqs = [_request(0)] * (len(inputs) - 1) + [_request(1, roi)]
+    want = [oracle.decode(c, int(PixelFormat.Rgb8))[0] for c in inputs[:-1]]
+    want.append(oracle.decode(big.codestream, int(PixelFormat.Rgb8), 1, (roi.x, roi.y, roi.w, roi.h), 1)[0])
+    plan = Plan(inputs, int(PixelFormat.Rgb8), requests=reqs)
+    plan.set_tile_shape(*shift)
+    for _ in range(3):
+        plan.execute_async()
+        st, _ = plan.wait()
+        assert st == 0
+        assert [plan.download(i) for i in range(len(inputs))] == want
+    plan.destroy()
+
+
+def test_autotuned_tile_shape_applies_to_the_next_plan_of_the_same_shape(batch):
+    want = _want(batch)
+    a = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
+    rep = a.autotune(2)
+    assert rep["idwt_seg_shift"] in (-1, 0, 1) and rep["pack_seg_shift"] in (-1, 0, 1)
+    a.destroy()
+    b = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
+    b.execute_async()
+    st, _ = b.wait()
+    assert st == 0 and [b.download(i) for i in range(len(batch))] == want
+    b.destroy()
