@@ -163,11 +163,11 @@ sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n);
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms);
 /* Autotuner (no counterpart in the reference).  Times the plan's stages on
  * its own data over `reps` runs each (0: 5) for every candidate launch shape
- * (VLC lanes per CTA; MagSgn warps per CTA, one block per warp or persistent
+ * (VLC threads per CTA and code blocks per VLC warp; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
  * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
  * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
- * the base rows per unit scaled by 2^shift, shift -1, 0 or 1), keeps the fastest per
+ * the base rows per unit scaled by 2^shift, shift -2 to 1), keeps the fastest per
  * stage for the plan and for later plans of the same shape on this context,
  * and re-executes the plan so its surfaces hold the decode.  Synchronous. */
 typedef struct sgn_tune_report {
@@ -175,6 +175,7 @@ typedef struct sgn_tune_report {
   float vlc_ms, ms_ms, dwt_ms;                                     /* its stage times */
   float vlc_ms_default, ms_ms_default, dwt_ms_default;             /* the default shape's */
   int32_t idwt_seg_shift, pack_seg_shift;                          /* chosen DWT tile shape (rows x 2^shift) */
+  uint32_t vlc_lanes;                                              /* chosen code blocks per VLC warp */
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;
@@ -182,8 +183,8 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tu
 sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_threads, uint32_t ms_warps,
                                      uint32_t ms_blocks_per_grab, uint32_t dwt_queue);
 /* Sets the DWT tile shape by hand: rows per work unit of the IDWT levels and
- * of the last level + pack, the base rule scaled by 2^shift (shift -1, 0 or
- * 1; strips stay 128 columns wide).  Re-uploads the plan's job tables. */
+ * of the last level + pack, the base rule scaled by 2^shift (shift -2 to 1;
+ * strips stay 128 columns wide).  Re-uploads the plan's job tables. */
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* plan, int32_t idwt_seg_shift, int32_t pack_seg_shift);
 /* Launches issued by one execute of the plan. */
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);

@@ -499,10 +499,22 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   // unit are applied to the job tables before they go up.
   LaunchConfig cfg;
   plan->sig = plan_signature(plan);
+  bool found_cfg = false;
   {
     std::lock_guard<std::mutex> g(ctx->tune_mu);
     for (auto& t : ctx->tuned)
-      if (t.first == plan->sig) cfg = t.second;
+      if (t.first == plan->sig) cfg = t.second, found_cfg = true;
+  }
+  if (!found_cfg) {
+    // Untuned plans: a plan whose last level (or largest IDWT round) has
+    // fewer units than twice the SMs (one tile, a small batch) takes
+    // shorter segments, so that more warps share its rows.
+    const uint32_t sms = (uint32_t)std::max(1, ctx->sm_count);
+    auto shift_for = [&](uint32_t units) { return units < sms ? -2 : units < 2 * sms ? -1 : 0; };
+    uint32_t round_units = 0;
+    for (const RoundInfo& r : plan->rounds) round_units = std::max(round_units, r.ctas);
+    if (!plan->rounds.empty()) cfg.idwt_seg_shift = shift_for(round_units);
+    if (plan->pack_ctas + plan->pack97_ctas) cfg.pack_seg_shift = shift_for(plan->pack_ctas + plan->pack97_ctas);
   }
   if (cfg.idwt_seg_shift || cfg.pack_seg_shift) set_segments(plan, idwt, packs, cfg.idwt_seg_shift, cfg.pack_seg_shift);
   if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
@@ -705,6 +717,15 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
   cudaError_t e = ht_magsgn_occupancy(p->ms_words, p->max_w, c.ms_warps ? c.ms_warps : 8, &ms);
   if (e == cudaSuccess) e = idwt_pack_occupancy(p->format < 5 ? p->format : 1, &idwt, &pack);
   if (e != cudaSuccess) return cuda_status(e, "occupancy query");
+  if (c.vlc_lanes == 0) {
+    // Blocks per VLC warp by default: 32 once the batch has that many blocks
+    // for every scheduler (four per SM), fewer for smaller plans, so each
+    // block's serial chain runs in a warp with fewer other blocks' paths.
+    const uint64_t per_sched = p->nht / (4ull * (uint64_t)std::max(1, ctx->sm_count));
+    uint32_t lanes = 1;
+    while (lanes < 32 && (uint64_t)lanes * 2 <= per_sched) lanes *= 2;
+    c.vlc_lanes = lanes;
+  }
   c.ms_ctas = (uint32_t)std::max(1, ms * ctx->sm_count);
   c.idwt_ctas = (uint32_t)std::max(1, idwt * ctx->sm_count);
   c.pack_ctas = (uint32_t)std::max(1, pack * ctx->sm_count);
@@ -783,7 +804,7 @@ sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev) {
   if (p->d_queue && (e = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "work queue reset");
   if ((e = mark(0)) != cudaSuccess) return cuda_status(e, "event record");
-  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads)) != cudaSuccess)
+  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads, c.vlc_lanes)) != cudaSuccess)
     return cuda_status(e, "HT VLC launch");
   if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
@@ -1081,7 +1102,7 @@ sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_thr
 
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* p, int32_t idwt_seg_shift, int32_t pack_seg_shift) {
   if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
-  if (idwt_seg_shift < -1 || idwt_seg_shift > 1 || pack_seg_shift < -1 || pack_seg_shift > 1)
+  if (idwt_seg_shift < -2 || idwt_seg_shift > 1 || pack_seg_shift < -2 || pack_seg_shift > 1)
     return set_error(SGN_ERR_INVALID_ARGUMENT, "tile shape shift out of range");
   std::lock_guard<std::mutex> g(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -1113,15 +1134,18 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   const LaunchConfig base = p->cfg;
   sgn_tune_report rep;
   std::memset(&rep, 0, sizeof(rep));
-  // VLC pass: lanes per CTA.
+  // VLC pass: threads per CTA and code blocks per warp.
   const uint32_t vlc_c[] = {64, 128};
   float best_vlc = 1e30f;
-  uint32_t vlc_threads = base.vlc_threads;
-  for (uint32_t t : vlc_c) {
-    float ms = time_stage(s, reps, [&] { return launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, t); }, e);
-    if (t == 128) rep.vlc_ms_default = ms;
-    if (e == cudaSuccess && ms < best_vlc) best_vlc = ms, vlc_threads = t;
-  }
+  uint32_t vlc_threads = base.vlc_threads, vlc_lanes = p->cfg.vlc_lanes;
+  for (uint32_t t : vlc_c)
+    for (uint32_t l = 32; l >= 1; l /= 2) {
+      if (l < 32 && (uint64_t)l * 64 > p->nht) continue;  // fewer blocks per warp only pays for small plans
+      float ms = time_stage(s, reps, [&] { return launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, t, l); },
+                            e);
+      if (t == 128 && l == p->cfg.vlc_lanes) rep.vlc_ms_default = ms;
+      if (e == cudaSuccess && ms < best_vlc) best_vlc = ms, vlc_threads = t, vlc_lanes = l;
+    }
   // MagSgn pass: warps per CTA, grid or queue (blocks per grab).
   struct MsC {
     uint32_t warps, gran;
@@ -1145,7 +1169,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   }
   // IDWT levels and pack, each: one unit per warp or persistent warps on a
   // queue, and the DWT tile shape (rows per unit: the base rule scaled by
-  // 2^shift, shift -1, 0 or 1; the strip is 128 columns, four per lane).
+  // 2^shift, shift -2 to 1; the strip is 128 columns, four per lane).
   auto set_shape = [&](int is, int ps) {
     set_segments(p, p->h_idwt, p->h_pack, is, ps);
     cudaError_t x = cudaSuccess;
@@ -1160,7 +1184,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   uint32_t idwt_queue = 0, pack_queue = 0;
   int idwt_shift = 0, pack_shift = 0;
   const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
-  for (int sh = -1; sh <= 1 && e == cudaSuccess; ++sh) {
+  for (int sh = -2; sh <= 1 && e == cudaSuccess; ++sh) {
     if ((e = set_shape(sh, sh)) != cudaSuccess) break;
     for (uint32_t q = 0; q < 2; ++q) {
       float ms = time_stage(s, reps, [&] {
@@ -1168,14 +1192,14 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
         for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, q != 0, ictas);
         return x;
       }, e);
-      if (q == 0 && sh == 0) idwt_default = ms;
+      if (q == 0 && sh == base.idwt_seg_shift) idwt_default = ms;
       if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q, idwt_shift = sh;
       ms = time_stage(s, reps, [&] {
         cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
         if (x == cudaSuccess) x = launch_packs(p, s, q != 0, pctas);
         return x;
       }, e);
-      if (q == 0 && sh == 0) pack_default = ms;
+      if (q == 0 && sh == base.pack_seg_shift) pack_default = ms;
       if (e == cudaSuccess && ms < best_pack) best_pack = ms, pack_queue = q, pack_shift = sh;
     }
   }
@@ -1190,6 +1214,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   cfg.idwt_seg_shift = idwt_shift;
   cfg.pack_seg_shift = pack_shift;
   cfg.vlc_threads = vlc_threads;
+  cfg.vlc_lanes = vlc_lanes;
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
   cfg.idwt_queue = idwt_queue;
@@ -1209,6 +1234,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     if (!found) ctx->tuned.emplace_back(sig, p->cfg);
   }
   rep.vlc_threads = cfg.vlc_threads;
+  rep.vlc_lanes = cfg.vlc_lanes;
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
   rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);

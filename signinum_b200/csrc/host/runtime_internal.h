@@ -127,13 +127,14 @@ struct PinnedBuffer {
 
 // Launch shape of a plan's kernels, chosen by the autotuner.
 struct LaunchConfig {
-  uint32_t vlc_threads = 128;  // lanes (code blocks) per CTA of the VLC pass
+  uint32_t vlc_threads = 128;  // threads per CTA of the VLC pass
+  uint32_t vlc_lanes = 0;      // code blocks per VLC warp (1..32, a power of two; 0: chosen by block count)
   uint32_t ms_warps = 8;       // warps (code blocks in flight) per CTA of the MagSgn pass
   uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
   uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue
   uint32_t pack_queue = 0;     // the same for the last level + pack
   // DWT tile shape: rows per work unit of the IDWT levels and of the pack,
-  // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -1..1.
+  // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -2..1.
   int32_t idwt_seg_shift = 0, pack_seg_shift = 0;
   // Persistent grid sizes (SMs x resident CTAs), derived from the above.
   uint32_t ms_ctas = 0, idwt_ctas = 0, pack_ctas = 0;

@@ -411,10 +411,16 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
 
 }  // namespace
 
-// Pass 1: one lane per code block runs the VLC chain.
+// Pass 1: one lane per code block runs the VLC chain, `lanes` (a power of
+// two up to 32) code blocks per warp: warp k takes blocks k * lanes ..
+// k * lanes + lanes - 1 on its first lanes.  The lanes of a warp follow
+// different blocks' branches, and a warp pays for every path any of its
+// lanes takes at each step; fewer blocks per warp make each chain step
+// shorter, which a plan with few blocks (one tile) wants, while a large
+// batch fills the SMs with 32 blocks per warp.
 __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
                                                             const uint8_t* __restrict__ arena,
-                                                            uint32_t* __restrict__ symbols) {
+                                                            uint32_t* __restrict__ symbols, uint32_t lanes) {
   __shared__ SmemTables T;
   __shared__ uint2 stage[16 * kHtThreads];  // per lane: the pairs of one row of a 64-wide block
   {
@@ -423,7 +429,9 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
     for (uint32_t i = threadIdx.x; i < sizeof(SmemTables) / 4; i += blockDim.x) d[i] = src[i];
   }
   __syncthreads();
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  if (lane >= lanes) return;
+  const uint32_t j = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * lanes + lane;
   if (j >= njobs) return;
   const HtJob job = jobs[j];
   if (job.passes == 0) return;
@@ -527,6 +535,87 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t* W, uint32_t nwords, 
   return __funnelshift_r(lo, hi, sh);
 }
 
+// Per-quad magnitude/sign arithmetic of the row loops below, with the quad's
+// four samples as the four bytes of one word (byte i = sample i, the order
+// of the quad's bits in the stream: (0,0), (0,1), (1,0), (1,1) by column
+// pairs).  A bit count m_n is at most 31 and a quad's total at most 124, so
+// bytewise sums never carry and a multiply by 0x01010101 forms every
+// sample's inclusive prefix inside the quad at once.
+
+// Byte i = bit i of the nibble x.
+__device__ __forceinline__ uint32_t spread4(uint32_t x) { return (x * 0x00204081u) & 0x01010101u; }
+
+struct QuadBits {
+  uint32_t m;    // m_n per sample: U - e_k when significant, else 0
+  uint32_t cs;   // per sample, the bits of the samples before it in the quad
+  uint32_t tot;  // the quad's bits
+};
+
+// U is the quad's u_q (plus the exponent bound kappa after the first row);
+// U > mmsb + 2 marks an invalid stream, which the caller flags and whose
+// block comes out as zeros, so clamping U to 31 here (the bytes then cannot
+// carry) changes no valid result.
+__device__ __forceinline__ QuadBits quad_bits(uint32_t inf, uint32_t U) {
+  const uint32_t sig = spread4((inf >> 4) & 0xFu), k = spread4(inf >> 12);
+  const uint32_t m = (min(U, 31u) * 0x01010101u - k) & (sig * 0xFFu);
+  const uint32_t incl = m * 0x01010101u;
+  return QuadBits{m, incl - m, incl >> 24};
+}
+
+// The 32 stream bits from bit c (< 64) of the 64-bit window hi:lo.
+__device__ __forceinline__ uint32_t window_bits(uint32_t lo, uint32_t hi, uint32_t c) {
+  return (uint32_t)((((uint64_t)hi << 32) | lo) >> c);
+}
+
+// Sample i's coefficient from its bits msv (sign first, then the magnitude
+// bits below the implied ones), bit count m, known-1 bit e1 and
+// significance: decode_mag_sgn_sample_with_vn's v_n (ht_block_decode.rs:1010-1032)
+// gives the sign-magnitude word sign << 31 | (v + 2) << (p - 1) in 32-bit
+// arithmetic (whose top bit, in the largest valid magnitudes, the shift can
+// set as well); RAW returns that word, otherwise coefficient_to_i32
+// (:225-234) of it: (word & 0x7FFFFFFF) >> (31 - nbp), negated when the top
+// bit is set, computed as (word << 1) >> rs with rs = 32 - nbp (1 when
+// nbp >= 31; the shift clamps at 32).  E receives the bit length of v (0
+// when insignificant), the exponent the row below needs.
+template <bool RAW>
+__device__ __forceinline__ int32_t sample_value(uint32_t msv, uint32_t m, uint32_t e1, bool sig, uint32_t p,
+                                                uint32_t rs, uint32_t& E) {
+  const uint32_t mask = __funnelshift_lc(0xFFFFFFFFu, 0u, m);
+  const uint32_t v = (msv & mask) | (e1 << m) | 1u;
+  E = sig ? 32 - __clz(v) : 0u;
+  const uint32_t word = (msv << 31) | ((v + 2) << (p - 1));
+  if (RAW) return sig ? (int32_t)word : 0;
+  const int32_t mag = (int32_t)__funnelshift_rc(word << 1, 0u, rs);
+  return sig ? ((int32_t)word < 0 ? -mag : mag) : 0;
+}
+
+// The four samples of a quad whose stream bits start at `off`: one clamped
+// three-word window read serves all four when the quad holds fewer than 64
+// bits; otherwise each sample reads its own 32 bits.
+template <bool RAW>
+__device__ __forceinline__ void quad_samples(const uint32_t* W, uint32_t ms_words, uint32_t lim, uint32_t off,
+                                             uint32_t inf, const QuadBits& qb, uint32_t p, uint32_t rs,
+                                             int32_t val[4], uint32_t E[4]) {
+  uint32_t lo, hi;
+  {
+    const uint32_t o = min(off, lim), wi = o >> 5, sh = o & 31;
+    const uint32_t a0 = W[wi], a1 = W[wi + 1], a2 = W[wi + 2];
+    lo = __funnelshift_r(a0, a1, sh);
+    hi = __funnelshift_r(a1, a2, sh);
+  }
+  uint32_t msv[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) msv[i] = window_bits(lo, hi, (qb.cs >> (8 * i)) & 0xFFu);
+  if (qb.tot >= 64) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) msv[i] = bits_at(W, ms_words, off + ((qb.cs >> (8 * i)) & 0xFFu));
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    val[i] = sample_value<RAW>(msv[i], (qb.m >> (8 * i)) & 0xFFu, (inf >> (8 + i)) & 1u, (inf >> (4 + i)) & 1u, p,
+                               rs, E[i]);
+}
+
 
 // The magnitude/sign rows of one block (decode_magnitude_sign_phase,
 // ht_block_decode.rs:1435-1561) for the calling warp.  Per quad row the lanes
@@ -544,6 +633,7 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t w = job.w, h = job.h, stride = job.stride;
   const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
+  const uint32_t rs = nbp >= 31 ? 1u : 32u - nbp;
   // Window reads start at most at bit `lim`, so that words wi .. wi + 2 lie
   // in the array (it holds at least 5 words).  The array ends with at least
   // 64 bits of ones past the stream (its padding), and `lim` lies beyond
@@ -595,65 +685,31 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
         if (active) U += gamma != 0 ? max(e, 2u) - 1 : 1;
       }
       bad |= active && U > mmsbp2;
-      // m_n per sample (0 when insignificant) and the quad's bit count.
-      uint32_t m[4], tot = 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
-        tot += m[i];
-      }
+      const QuadBits qb = quad_bits(inf, U);
       // Warp inclusive scan of the bit counts.
-      uint32_t inc = tot;
+      uint32_t inc = qb.tot;
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
         uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
         if (lane >= (uint32_t)d) inc += v;
       }
       const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 31);
-      uint32_t off = rowbase + inc - tot;
+      const uint32_t off = rowbase + inc - qb.tot;
       rowbase += chunk_bits;
-      // Sample i's bits start at off + c_i, c_i = m_0 + .. + m_{i-1}.  When the
-      // quad holds fewer than 64 bits one 64-bit window read serves all four
-      // samples (independent funnel shifts); otherwise each sample reads its
-      // own 32 bits.
-      const uint32_t cs[4] = {0u, m[0], m[0] + m[1], m[0] + m[1] + m[2]};
-      uint32_t lo, hi;
-      {
-        const uint32_t o = min(off, lim), wi = o >> 5, sh = o & 31;
-        const uint32_t a0 = W[wi], a1 = W[wi + 1], a2 = W[wi + 2];
-        lo = __funnelshift_r(a0, a1, sh);
-        hi = __funnelshift_r(a1, a2, sh);
-      }
-      uint32_t msv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) msv[i] = cs[i] < 32 ? __funnelshift_r(lo, hi, cs[i]) : hi >> (cs[i] - 32);
-      if (tot >= 64) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) msv[i] = bits_at(W, ms_words, off + cs[i]);
-      }
-      uint32_t val[4], E[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const bool sig = (inf >> (4 + i)) & 1;
-        const uint32_t mn = m[i];
-        // (1 << mn) - 1, saturating at 32 bits.
-        const uint32_t mask = __funnelshift_lc(0xFFFFFFFFu, 0u, mn);
-        const uint32_t v = (msv[i] & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
-        val[i] = sig ? (msv[i] << 31) | ((v + 2) << (p - 1)) : 0u;
-        E[i] = sig ? 32 - __clz(v) : 0u;
-      }
+      int32_t val[4];
+      uint32_t E[4];
+      quad_samples<RAW>(W, ms_words, lim, off, inf, qb, p, rs, val, E);
       if (active) {
         const uint32_t x = 2 * q;
-        auto cv = [&](uint32_t vv) { return RAW ? (int32_t)vv : to_i32(vv, nbp); };
         if (pairs && x + 1 < w) {
-          *reinterpret_cast<int2*>(row0 + x) = make_int2(cv(val[0]), cv(val[2]));
-          if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(cv(val[1]), cv(val[3]));
+          *reinterpret_cast<int2*>(row0 + x) = make_int2(val[0], val[2]);
+          if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(val[1], val[3]);
         } else {
-          row0[x] = cv(val[0]);
-          if (second) row1[x] = cv(val[1]);
+          row0[x] = val[0];
+          if (second) row1[x] = val[1];
           if (x + 1 < w) {
-            row0[x + 1] = cv(val[2]);
-            if (second) row1[x + 1] = cv(val[3]);
+            row0[x + 1] = val[2];
+            if (second) row1[x + 1] = val[3];
           }
         }
         if (!NARROW) {
@@ -771,6 +827,7 @@ __device__ bool magsgn_rows_half(const HtJob& job, bool live, const uint32_t* W,
   const uint32_t lane = threadIdx.x & 31, gl = lane & 15, gsh = lane & 16;
   const uint32_t w = live ? job.w : 0, h = live ? job.h : 0, stride = job.stride;
   const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
+  const uint32_t rs = nbp >= 31 ? 1u : 32u - nbp;
   // As in magsgn_rows: clamped window reads stay in the half's words.
   const uint32_t lim = live ? 32 * (ms_words - 3) : 0;
   const bool pairs = ((job.dst | stride) & 1) == 0;
@@ -795,59 +852,32 @@ __device__ bool magsgn_rows_half(const HtJob& job, bool live, const uint32_t* W,
       if (active) U += gamma != 0 ? max(e, 2u) - 1 : 1;
     }
     bad |= active && U > mmsbp2;
-    uint32_t m[4], tot = 0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      m[i] = (inf >> (4 + i)) & 1 ? U - ((inf >> (12 + i)) & 1) : 0;
-      tot += m[i];
-    }
-    uint32_t inc = tot;
+    const QuadBits qb = quad_bits(inf, U);
+    uint32_t inc = qb.tot;
 #pragma unroll
     for (int d = 1; d < 16; d <<= 1) {
       uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, d, 16);
       if (gl >= (uint32_t)d) inc += v;
     }
     const uint32_t chunk_bits = __shfl_sync(0xFFFFFFFFu, inc, 15, 16);
-    const uint32_t off = rowbase + inc - tot;
+    const uint32_t off = rowbase + inc - qb.tot;
     rowbase += chunk_bits;
-    const uint32_t cs[4] = {0u, m[0], m[0] + m[1], m[0] + m[1] + m[2]};
-    uint32_t lo, hi;
-    {
-      const uint32_t o = min(off, lim), wi = o >> 5, sh = o & 31;
-      const uint32_t a0 = W[wi], a1 = W[wi + 1], a2 = W[wi + 2];
-      lo = __funnelshift_r(a0, a1, sh);
-      hi = __funnelshift_r(a1, a2, sh);
-    }
-    uint32_t msv[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) msv[i] = cs[i] < 32 ? __funnelshift_r(lo, hi, cs[i]) : hi >> (cs[i] - 32);
-    if (tot >= 64) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) msv[i] = bits_at(W, ms_words, off + cs[i]);
-    }
-    uint32_t val[4], E[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const bool sig = (inf >> (4 + i)) & 1;
-      const uint32_t mn = m[i];
-      const uint32_t mask = __funnelshift_lc(0xFFFFFFFFu, 0u, mn);
-      const uint32_t v = (msv[i] & mask) | (((inf >> (8 + i)) & 1) << mn) | 1;
-      val[i] = sig ? (msv[i] << 31) | ((v + 2) << (p - 1)) : 0u;
-      E[i] = sig ? 32 - __clz(v) : 0u;
-    }
+    int32_t val[4];
+    uint32_t E[4];
+    quad_samples<false>(W, ms_words, lim, off, inf, qb, p, rs, val, E);
     if (active) {
       int32_t* row0 = dst + (size_t)y * stride;
       int32_t* row1 = row0 + stride;
       const uint32_t x = 2 * q;
       if (pairs && x + 1 < w) {
-        *reinterpret_cast<int2*>(row0 + x) = make_int2(to_i32(val[0], nbp), to_i32(val[2], nbp));
-        if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(to_i32(val[1], nbp), to_i32(val[3], nbp));
+        *reinterpret_cast<int2*>(row0 + x) = make_int2(val[0], val[2]);
+        if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(val[1], val[3]);
       } else {
-        row0[x] = to_i32(val[0], nbp);
-        if (second) row1[x] = to_i32(val[1], nbp);
+        row0[x] = val[0];
+        if (second) row1[x] = val[1];
         if (x + 1 < w) {
-          row0[x + 1] = to_i32(val[2], nbp);
-          if (second) row1[x + 1] = to_i32(val[3], nbp);
+          row0[x + 1] = val[2];
+          if (second) row1[x + 1] = val[3];
         }
       }
     }
@@ -1203,10 +1233,12 @@ cudaError_t ht_kernels_init() {
 }
 
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                          cudaStream_t stream, uint32_t threads) {
+                          cudaStream_t stream, uint32_t threads, uint32_t lanes) {
   if (njobs == 0) return cudaSuccess;
   if (threads == 0 || threads > kHtThreads || threads % 32) threads = kHtThreads;
-  ht_vlc_kernel<<<(njobs + threads - 1) / threads, threads, 0, stream>>>(jobs, njobs, arena, symbols);
+  if (lanes == 0 || lanes > 32 || (lanes & (lanes - 1))) lanes = 32;
+  const uint32_t warps = (njobs + lanes - 1) / lanes, per_cta = threads / 32;
+  ht_vlc_kernel<<<(warps + per_cta - 1) / per_cta, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
   return cudaGetLastError();
 }
 

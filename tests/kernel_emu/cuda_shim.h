@@ -98,6 +98,12 @@ inline unsigned __funnelshift_lc(unsigned lo, unsigned hi, unsigned sh) {
   sh = sh > 32 ? 32 : sh;
   return (unsigned)((v << sh) >> 32);
 }
+// The clamping right funnel shift: the low word of (hi:lo) >> min(sh, 32).
+inline unsigned __funnelshift_rc(unsigned lo, unsigned hi, unsigned sh) {
+  uint64_t v = ((uint64_t)hi << 32) | lo;
+  sh = sh > 32 ? 32 : sh;
+  return (unsigned)(v >> sh);
+}
 inline int __clz(unsigned v) { return v ? __builtin_clz(v) : 32; }
 inline int __ffs(unsigned v) { return v ? __builtin_ctz(v) + 1 : 0; }
 inline int __ffsll(long long v) { return v ? __builtin_ctzll((unsigned long long)v) + 1 : 0; }

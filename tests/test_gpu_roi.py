@@ -38,9 +38,9 @@ def _regions(w, h, rng, n):
     out = [Rect(0, 0, 1, 1), Rect(0, 0, 64, 64), Rect(w // 2, h // 3, 64, 64), Rect(w - 65, h - 65, 64, 64),
            Rect(17, h // 2, 255, 3), Rect(w // 3, 5, 1, 200)]
     for _ in range(n):
-        rw, rh = int(rng.integers(1, 300)), int(rng.integers(1, 300))
-        out.append(Rect(int(rng.integers(0, w - rw)), int(rng.integers(0, h - rh)), rw, rh))
-    return out
+        rw, rh = int(rng.integers(1, min(300, w))), int(rng.integers(1, min(300, h)))
+        out.append(Rect(int(rng.integers(0, w - rw + 1)), int(rng.integers(0, h - rh + 1)), rw, rh))
+    return [r for r in out if r.x + r.w <= w and r.y + r.h <= h]
 
 
 @pytest.mark.parametrize("name", list(TILES))
