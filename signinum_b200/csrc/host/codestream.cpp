@@ -57,16 +57,21 @@ struct Reader {
     return true;
   }
   void align() { bit = (bit + 7) & ~(size_t)7; }
+  // read_bits_with_stuffing (reader.rs:129-160): cnt bits, most significant
+  // first; after the last bit of an 0xFF byte the next byte's top bit is a
+  // stuffed zero (a one there is an error) and is skipped.  Takes the bits
+  // of one byte per step.
   bool bits(uint32_t cnt, uint32_t& out) {
     uint32_t v = 0;
-    for (uint32_t i = 0; i < cnt; ++i) {
-      size_t p = bit >> 3;
+    while (cnt) {
+      const size_t p = bit >> 3;
       if (p >= n) return false;
-      uint32_t bp = bit & 7;
-      bool stuff = bp == 7 && d[p] == 0xFF;
-      v = (v << 1) | ((d[p] >> (7 - bp)) & 1);
-      ++bit;
-      if (stuff) {
+      const uint32_t avail = 8 - (uint32_t)(bit & 7), take = cnt < avail ? cnt : avail;
+      const uint32_t byte = d[p];
+      v = (v << take) | ((byte >> (avail - take)) & ((1u << take) - 1));
+      bit += take;
+      cnt -= take;
+      if (take == avail && byte == 0xFF) {
         if ((bit >> 3) >= n) return false;
         if ((d[bit >> 3] >> 7) & 1) return false;
         ++bit;
@@ -253,18 +258,22 @@ MainHeader read_main_header(const uint8_t* data, size_t len) {
   return h;
 }
 
+// Node values of every tag tree of a tile, in one pool (a node's known flag
+// in bit 31 of its value), so that a precinct band's trees cost no
+// allocation of their own.
+struct TagPool {
+  std::vector<uint32_t> nodes;
+};
+
 struct TagTree {
   uint32_t levels = 0;
-  uint32_t lw[17], lh[17];
-  size_t base[17];
-  std::vector<uint32_t> val;
-  std::vector<uint8_t> known;
-  void init(uint32_t w, uint32_t h) {
+  uint32_t lw[17];
+  size_t base[17];  // first node of each level in the pool
+  void init(uint32_t w, uint32_t h, TagPool& pool) {
     levels = 0;
-    size_t total = 0;
+    size_t total = pool.nodes.size();
     for (;;) {
       lw[levels] = w;
-      lh[levels] = h;
       base[levels] = total;
       total += (size_t)w * h;
       ++levels;
@@ -272,32 +281,34 @@ struct TagTree {
       w = (w + 1) / 2;
       h = (h + 1) / 2;
     }
-    val.assign(total, 0);
-    known.assign(total, 0);
+    pool.nodes.resize(total, 0);
   }
   // read_tag_node, tag_tree.rs:118-190, unrolled over levels.
-  bool read(uint32_t x, uint32_t y, uint32_t threshold, Reader& r, uint32_t& out) {
+  bool read(uint32_t x, uint32_t y, uint32_t threshold, Reader& r, uint32_t& out, TagPool& pool) {
+    constexpr uint32_t kKnown = 1u << 31;
     uint32_t parent = 0;
     for (uint32_t l = levels; l-- > 0;) {
-      size_t i = base[l] + (size_t)(y >> l) * lw[l] + (x >> l);
-      if (!known[i]) {
-        uint32_t v = std::max(parent, val[i]);
+      uint32_t& node = pool.nodes[base[l] + (size_t)(y >> l) * lw[l] + (x >> l)];
+      if (!(node & kKnown)) {
+        uint32_t v = std::max(parent, node);
+        bool known = false;
         while (v < threshold) {
           uint32_t b;
           if (!r.bits(1, b)) return false;
           if (b == 0) ++v;
           else {
-            known[i] = 1;
+            known = true;
             break;
           }
         }
-        val[i] = v;
+        node = v | (known ? kKnown : 0u);
       }
-      if (val[i] >= threshold || l == 0) {
-        out = val[i];
+      const uint32_t val = node & ~kKnown;
+      if (val >= threshold || l == 0) {
+        out = val;
         return true;
       }
-      parent = val[i];
+      parent = val;
     }
     out = parent;
     return true;
@@ -318,6 +329,7 @@ struct BlockState {
   uint32_t lblock = 3;
   uint32_t lcup = 0, lref = 0;
   int64_t cleanup_off = -1, ref_off = -1;
+  uint16_t ms_words = 0;  // HT: CodeBlock::ms_words, from the segment's last two bytes
   // Classic: the codeword-segment parts of every layer in stream order
   // (segment index, bytes, passes, offset in the codestream).
   struct Part {
@@ -681,6 +693,16 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
   std::vector<Packet> packets;
   std::vector<PrecinctBand> pbs;
   std::vector<BlockState> blocks;
+  TagPool tags;
+  {
+    // Room for every block of every band (and its tag-tree nodes) up front.
+    const uint64_t cbs = (1ull << (h.comps[0].cs.cbw + h.comps[0].cs.cbh));
+    const uint64_t est = (uint64_t)nc * ((uint64_t)W * H / std::max<uint64_t>(cbs, 1) + 8ull * (L + 1)) * 4 / 3 + 16;
+    if (est < (1u << 22)) {
+      blocks.reserve(est);
+      tags.nodes.reserve(est * 3);
+    }
+  }
   T.comp_band_begin.resize(nc);
   for (uint32_t c = 0; c < nc; ++c) {
     const CodingStyle& cs = h.comps[c].cs;
@@ -784,8 +806,8 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
                 bs.h = std::min<uint32_t>(bs.y0 + cbh, b.h) - bs.y0;
                 blocks.push_back(bs);
               }
-            pbd.incl.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1));
-            pbd.zbp.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1));
+            pbd.incl.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1), tags);
+            pbd.zbp.init(std::max<uint32_t>(pbd.ncx, 1), std::max<uint32_t>(pbd.ncy, 1), tags);
             pbs.push_back(std::move(pbd));
           }
           packets.push_back(pk);
@@ -854,12 +876,12 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
               inc = v == 1;
             } else {
               // Included in this layer when its first layer is at most pk.layer.
-              if (!pb.incl.read(xi, yi, (uint32_t)pk.layer + 1, pr, v)) { ok = false; break; }
+              if (!pb.incl.read(xi, yi, (uint32_t)pk.layer + 1, pr, v, tags)) { ok = false; break; }
               inc = v <= pk.layer;
             }
             if (!inc) continue;
             if (first) {
-              if (!pb.zbp.read(xi, yi, UINT32_MAX, pr, v)) { ok = false; break; }
+              if (!pb.zbp.read(xi, yi, UINT32_MAX, pr, v, tags)) { ok = false; break; }
               bs.missing = (uint8_t)v;
             }
             bs.included = true;
@@ -970,6 +992,13 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
           size_t at = part.first + pr.pos();
           if (!pr.skip(bs.lcup)) { ok = false; break; }
           bs.cleanup_off = (int64_t)at;
+          if (bs.lcup >= 2) {
+            // Scup from the segment's last two bytes, read here while the
+            // walk is at the segment (the bodies are visited in stream order).
+            const uint8_t* seg = data + at;
+            const uint32_t scup = ((uint32_t)seg[bs.lcup - 1] << 4) + (seg[bs.lcup - 2] & 0x0F);
+            if (scup <= bs.lcup) bs.ms_words = (uint16_t)std::min<uint32_t>((bs.lcup - scup + 15) / 4 + 2, 0xFFFFu);
+          }
           if (bs.passes > 1 && !classic) {
             size_t at2 = part.first + pr.pos();
             if (!pr.skip(bs.lref)) { ok = false; break; }
@@ -980,6 +1009,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
     }
   }
   // Segment table for the decoded resolutions (decode.rs:1554-1718 checks).
+  T.blocks.reserve(blocks.size());
   for (const BlockState& bs : blocks) {
     const Band& b = T.bands[bs.band];
     if (b.res >= nres_dec || bs.w == 0 || bs.h == 0) continue;
@@ -1048,11 +1078,7 @@ void parse_tile_raw(const uint8_t* data, size_t len, const uint32_t* target, Til
       cb.passes = (uint8_t)passes;
       cb.cleanup_off = (uint32_t)bs.cleanup_off;
       cb.lcup = bs.lcup;
-      if ((uint64_t)bs.cleanup_off + bs.lcup <= len) {
-        const uint8_t* seg = data + bs.cleanup_off;
-        const uint32_t scup = ((uint32_t)seg[bs.lcup - 1] << 4) + (seg[bs.lcup - 2] & 0x0F);
-        if (scup <= bs.lcup) cb.ms_words = (uint16_t)std::min<uint32_t>((bs.lcup - scup + 15) / 4 + 2, 0xFFFFu);
-      }
+      cb.ms_words = bs.ms_words;
       if (passes > 1) {
         cb.ref_off = (uint32_t)bs.ref_off;
         cb.lref = bs.lref;

@@ -251,9 +251,6 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (direct && (e = cudaMemcpyAsync(plan->d_input, datas[0], in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
       return cuda_status(e, "input upload");
   }
-  if ((e = dalloc(&plan->d_coef, coef_total, s)) != cudaSuccess) return cuda_status(e, "coefficient arena");
-  if ((e = dalloc(&plan->d_levels, lvl_total, s)) != cudaSuccess) return cuda_status(e, "level buffers");
-  if ((e = dalloc(&plan->d_status, std::max<size_t>(n, 1), s)) != cudaSuccess) return cuda_status(e, "status");
   plan->tile_coef_off = coef_off;
   plan->tile_coef_elems.assign(n, 0);
   for (size_t i = 0; i < n; ++i)
@@ -351,8 +348,20 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   for (size_t i = 0; i < n; ++i) plan->ht_cleanup_bytes += th[i].bytes;
   if (ht_magsgn_smem_bytes(plan->ms_words, max_w) > 227 * 1024)
     return set_error(SGN_ERR_UNSUPPORTED, "code-block segment too long for the MagSgn staging buffer");
-  if ((e = dalloc(&plan->d_symbols, std::max<uint64_t>(sym_total, 1), s)) != cudaSuccess)
-    return cuda_status(e, "symbol scratch");
+  {
+    // One work arena: coefficients, level planes, quad symbols, tile status
+    // (256-byte aligned parts).
+    auto up256 = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t at_lvl = up256(coef_total * 4), at_sym = at_lvl + up256(lvl_total * 4);
+    const size_t at_st = at_sym + up256(std::max<uint64_t>(sym_total, 1) * 4);
+    const size_t bytes = at_st + up256(std::max<size_t>(n, 1) * 4);
+    if ((e = cudaMallocAsync(&plan->d_work, bytes, s)) != cudaSuccess) return cuda_status(e, "work arena");
+    uint8_t* base = static_cast<uint8_t*>(plan->d_work);
+    plan->d_coef = reinterpret_cast<int32_t*>(base);
+    plan->d_levels = reinterpret_cast<int32_t*>(base + at_lvl);
+    plan->d_symbols = reinterpret_cast<uint32_t*>(base + at_sym);
+    plan->d_status = reinterpret_cast<uint32_t*>(base + at_st);
+  }
 
   // IDWT rounds: round r-1 holds resolution r of every tile that has it.
   // Rounds 0 .. max_rounds-1 hold 5/3 levels, the next max_rounds the 9/7
@@ -517,24 +526,17 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
     if (plan->pack_ctas + plan->pack97_ctas) cfg.pack_seg_shift = shift_for(plan->pack_ctas + plan->pack97_ctas);
   }
   if (cfg.idwt_seg_shift || cfg.pack_seg_shift) set_segments(plan, idwt, packs, cfg.idwt_seg_shift, cfg.pack_seg_shift);
-  if ((e = dalloc(&plan->d_ht, nht, s)) != cudaSuccess) return cuda_status(e, "ht jobs");
-  if ((e = dalloc(&plan->d_refine, nref, s)) != cudaSuccess) return cuda_status(e, "refine list");
   plan->nclassic = ncls;
+  size_t cscratch_bytes = 0;
   if (ncls) {
     plan->classic_slot = std::max<uint32_t>(cslot, 1);
     const uint32_t per = classic_threads_per_cta();
     // As many resident threads as the kernel's occupancy allows (every block
     // a thread of its own where possible: the slowest block sets the time).
     plan->classic_ctas = std::min<uint32_t>((ncls + per - 1) / per, (uint32_t)ctx->sm_count * classic_ctas_per_sm());
-    if ((e = dalloc(&plan->d_classic, ncls, s)) != cudaSuccess) return cuda_status(e, "classic jobs");
-    if ((e = dalloc(&plan->d_csegs, std::max<uint32_t>(ncseg, 1), s)) != cudaSuccess) return cuda_status(e, "classic segments");
-    if ((e = dalloc(&plan->d_cscratch, (size_t)plan->classic_ctas * per * plan->classic_slot, s)) != cudaSuccess)
-      return cuda_status(e, "classic scratch");
-    if (gather_total && (e = dalloc(&plan->d_gather, gather_total, s)) != cudaSuccess)
-      return cuda_status(e, "classic gather area");
+    cscratch_bytes = (size_t)plan->classic_ctas * per * plan->classic_slot * sizeof(uint16_t);
   }
-  if ((e = dalloc(&plan->d_idwt, idwt.size(), s)) != cudaSuccess) return cuda_status(e, "idwt jobs");
-  if ((e = dalloc(&plan->d_pack, packs.size(), s)) != cudaSuccess) return cuda_status(e, "pack jobs");
+  plan->nqueues = (uint32_t)plan->rounds.size() + 3 + kPackVariants;
 
   // Pinned staging: [codestreams unless direct] [HT jobs] [refine] [IDWT] [pack].
   auto up16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
@@ -547,6 +549,23 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   const size_t at_gather = at_cseg + up16((size_t)ncseg * sizeof(ClassicSeg));
   const size_t stage_bytes = at_gather + up16(gather_total);
   if ((e = staging.ensure(stage_bytes)) != cudaSuccess) return cuda_status(e, "pinned staging");
+  {
+    // One table arena: the job tables in their staging layout (uploaded by
+    // one copy), then the work-queue counters and the classic scratch.
+    const size_t tab = stage_bytes - at_ht, at_q = up16(tab), at_cs = at_q + up16((size_t)plan->nqueues * 4);
+    if ((e = cudaMallocAsync(&plan->d_tables, at_cs + std::max<size_t>(cscratch_bytes, 16), s)) != cudaSuccess)
+      return cuda_status(e, "table arena");
+    uint8_t* base = static_cast<uint8_t*>(plan->d_tables);
+    plan->d_ht = nht ? reinterpret_cast<HtJob*>(base) : nullptr;
+    plan->d_refine = nref ? reinterpret_cast<uint32_t*>(base + (at_ref - at_ht)) : nullptr;
+    plan->d_idwt = idwt.empty() ? nullptr : reinterpret_cast<IdwtJob*>(base + (at_idwt - at_ht));
+    plan->d_pack = packs.empty() ? nullptr : reinterpret_cast<PackJob*>(base + (at_pack - at_ht));
+    plan->d_classic = ncls ? reinterpret_cast<ClassicJob*>(base + (at_cls - at_ht)) : nullptr;
+    plan->d_csegs = ncls ? reinterpret_cast<ClassicSeg*>(base + (at_cseg - at_ht)) : nullptr;
+    plan->d_gather = gather_total ? base + (at_gather - at_ht) : nullptr;
+    plan->d_queue = reinterpret_cast<uint32_t*>(base + at_q);
+    plan->d_cscratch = cscratch_bytes ? reinterpret_cast<uint16_t*>(base + at_cs) : nullptr;
+  }
   uint8_t* st = staging.p;
   HtJob* ht = reinterpret_cast<HtJob*>(st + at_ht);
   uint32_t* refine = reinterpret_cast<uint32_t*>(st + at_ref);
@@ -620,22 +639,13 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   });
   if (!idwt.empty()) std::memcpy(st + at_idwt, idwt.data(), idwt.size() * sizeof(IdwtJob));
   if (!packs.empty()) std::memcpy(st + at_pack, packs.data(), packs.size() * sizeof(PackJob));
-  struct Up {
-    void* d;
-    size_t at, bytes;
-  } ups[] = {{plan->d_input, 0, direct ? 0 : in_total},
-             {plan->d_ht, at_ht, (size_t)nht * sizeof(HtJob)},
-             {plan->d_refine, at_ref, (size_t)nref * 4},
-             {plan->d_idwt, at_idwt, idwt.size() * sizeof(IdwtJob)},
-             {plan->d_pack, at_pack, packs.size() * sizeof(PackJob)},
-             {plan->d_classic, at_cls, (size_t)ncls * sizeof(ClassicJob)},
-             {plan->d_csegs, at_cseg, (size_t)ncseg * sizeof(ClassicSeg)},
-             {plan->d_gather, at_gather, (size_t)gather_total}};
-  for (auto& u : ups) {
-    if (!u.bytes) continue;
-    if ((e = cudaMemcpyAsync(u.d, st + u.at, u.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_status(e, "plan upload");
-  }
+  // Uploads: the codestreams (unless they went up directly) and every job
+  // table in one copy.
+  if (!direct && in_total && (e = cudaMemcpyAsync(plan->d_input, st, in_total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e, "plan upload");
+  if (stage_bytes > at_ht &&
+      (e = cudaMemcpyAsync(plan->d_tables, st + at_ht, stage_bytes - at_ht, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e, "plan upload");
   // The staging buffer is reused by the next call: finish the copies now
   // (callers that reuse it only after the plan has run pass sync_uploads false).
   if (sync_uploads && (e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e, "plan upload");
@@ -645,8 +655,6 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   for (auto& sf : plan->surfaces) sf.kernel_dispatches = plan->launches;
   // Work-queue counters and the launch shape (an autotuned one when this
   // context has tuned a plan of the same signature).
-  plan->nqueues = (uint32_t)plan->rounds.size() + 3 + kPackVariants;
-  if ((e = dalloc(&plan->d_queue, plan->nqueues, s)) != cudaSuccess) return cuda_status(e, "work queues");
   plan->h_idwt = std::move(idwt);
   plan->h_pack = std::move(packs);
   return apply_config(ctx, plan, cfg);
@@ -767,16 +775,14 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
     cudaGraphExecDestroy(p->graph);
     p->graph = nullptr;
   }
-  if (p->d_queue) cudaFreeAsync(p->d_queue, s);
-  p->d_queue = nullptr;
-  void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_coef, p->d_levels, p->d_symbols, p->d_ht,
-                  p->d_refine, p->d_idwt, p->d_pack, p->d_status, p->d_classic, p->d_csegs, p->d_cscratch,
-                  p->d_gather};
+  void* ptrs[] = {p->owns_input ? p->d_input : nullptr, p->d_work, p->d_tables};
   for (void* q : ptrs)
     if (q) cudaFreeAsync(q, s);
   p->d_input = nullptr;
+  p->d_work = p->d_tables = nullptr;
   p->d_coef = p->d_levels = nullptr;
   p->d_symbols = nullptr;
+  p->d_status = nullptr;
   p->d_ht = nullptr;
   p->d_refine = nullptr;
   p->d_classic = nullptr;
@@ -785,7 +791,7 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s) {
   p->d_gather = nullptr;
   p->d_idwt = nullptr;
   p->d_pack = nullptr;
-  p->d_status = nullptr;
+  p->d_queue = nullptr;
 }
 
 void release_plan(sgn_plan* p, cudaStream_t s) {

@@ -174,7 +174,12 @@ struct sgn_plan {
   uint32_t format = 0;
   std::vector<sgn_status> status;  // host-side (parse/request) status per tile
   std::vector<sgn_surface> surfaces;
-  // Device allocations (stream-ordered pool).
+  // Device allocations (stream-ordered pool): the input arena, and two
+  // arenas the buffers below are parts of: d_work (coefficients, level
+  // planes, quad symbols, tile status) and d_tables (job tables, work-queue
+  // counters, classic scratch).
+  void* d_work = nullptr;
+  void* d_tables = nullptr;
   uint8_t* d_input = nullptr;
   bool owns_input = true;  // false: codestreams live in a caller-owned resident arena
   int32_t* d_coef = nullptr;

@@ -42,6 +42,36 @@ struct SmemTables {
 
 __device__ __forceinline__ uint8_t ld8(const uint8_t* p) { return __ldg(p); }
 
+// MEL bit-buffer refill, out of line (it runs once every several runs, and
+// inlined its byte loop would sit in every step of the VLC chain): appends
+// bytes until more than 56 bits are buffered.  After a 0xFF byte the next
+// byte carries 7 bits; the last byte is ORed with 0x0F and the stream
+// continues with 0xFF bytes.  State passed and returned by value, so it
+// stays in registers.
+struct MelFill {
+  uint64_t buf;
+  uint32_t pos, remaining, unstuff;
+  int bits;
+};
+__device__ __noinline__ MelFill mel_refill(const uint8_t* data, MelFill f) {
+  while (f.bits <= 56) {
+    uint32_t b;
+    if (f.remaining > 0) {
+      b = __ldg(data + f.pos);
+      ++f.pos;
+      --f.remaining;
+    } else {
+      b = 0xFF;
+    }
+    if (f.remaining == 0) b |= 0x0F;
+    const int nb = 8 - (int)f.unstuff;
+    f.buf |= (uint64_t)(b & ((1u << nb) - 1)) << (64 - f.bits - nb);
+    f.bits += nb;
+    f.unstuff = b == 0xFF;
+  }
+  return f;
+}
+
 // MEL run decoder (ht_block_decode.rs:782-880).  The reference decodes runs
 // into a small queue; here each run is decoded when it is needed, from a
 // 64-bit buffer of unstuffed MEL bits (most significant bit first), with no
@@ -61,25 +91,13 @@ struct Mel {
     bits = 0;
     k = 0;
   }
-  // Appends bytes until more than 56 bits are buffered.  After a 0xFF byte
-  // the next byte carries 7 bits; the last byte is ORed with 0x0F and the
-  // stream continues with 0xFF bytes.
-  __device__ void refill() {
-    while (bits <= 56) {
-      uint32_t b;
-      if (remaining > 0) {
-        b = ld8(data + pos);
-        ++pos;
-        --remaining;
-      } else {
-        b = 0xFF;
-      }
-      if (remaining == 0) b |= 0x0F;
-      const int nb = 8 - (int)unstuff;
-      buf |= (uint64_t)(b & ((1u << nb) - 1)) << (64 - bits - nb);
-      bits += nb;
-      unstuff = b == 0xFF;
-    }
+  __device__ __forceinline__ void refill() {
+    const MelFill f = mel_refill(data, MelFill{buf, pos, remaining, unstuff, bits});
+    buf = f.buf;
+    pos = f.pos;
+    remaining = f.remaining;
+    unstuff = f.unstuff;
+    bits = f.bits;
   }
   __device__ __forceinline__ int get_run() {
     if (bits < 6) refill();
@@ -97,6 +115,26 @@ struct Mel {
     return first ? ((1 << e) - 1) << 1 : (int)((v << 1) | 1);
   }
 };
+
+// Four bytes (highest address first) into the backward VLC reader's bit
+// buffer one at a time, for words with a byte whose low 7 bits are all ones
+// (after a byte above 0x8F such a byte loses its top bit to stuffing).  Out
+// of line: it is the rare case of a refill.
+struct VlcPush {
+  uint64_t tmp;
+  uint32_t bits, unstuff;
+};
+__device__ __noinline__ VlcPush vlc_push4(uint32_t wv, uint64_t tmp, uint32_t bits, uint32_t unstuff) {
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    const uint32_t b = (wv >> (8 * k)) & 0xFF;
+    const uint32_t db = 8 - ((unstuff && (b & 0x7F) == 0x7F) ? 1 : 0);
+    tmp |= (uint64_t)b << bits;
+    bits += db;
+    unstuff = b > 0x8F;
+  }
+  return VlcPush{tmp, bits, unstuff};
+}
 
 // Backward VLC reader (ht_block_decode.rs:932-1000, new_vlc).
 struct Vlc {
@@ -174,10 +212,10 @@ struct Vlc {
           bits += 32;
           unstuff = (wv & 0xFF) > 0x8F;
         } else {
-          push(wv >> 24);
-          push((wv >> 16) & 0xFF);
-          push((wv >> 8) & 0xFF);
-          push(wv & 0xFF);
+          const VlcPush r = vlc_push4(wv, tmp, bits, unstuff);
+          tmp = r.tmp;
+          bits = r.bits;
+          unstuff = r.unstuff;
         }
       } else {
         uint32_t b = 0;
