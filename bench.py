@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the other configs and the serving summary")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
+    ap.add_argument("--tiles", type=int, default=0,
+                    help="c1/c2/c3: the workload drawn with this many tiles instead (smaller profiling cases)")
     ap.add_argument("--pool", type=int, default=4096, help="c4: tiles in the serving pool")
     ap.add_argument("--rates", default="2000,5000,10000,20000,35000,50000,70000,90000,110000,130000,160000,200000",
                     help="c4: arrival rates, tiles/s")
@@ -93,19 +95,19 @@ WORKLOAD_CONFIG = {
 
 
 def build_workload(name, n=None, indices=None):
-    """(tiles, output format) of a workload; c2 with n / indices gives part
-    of a larger list of the same distribution."""
+    """(tiles, output format) of a workload, drawn with n tiles when given
+    (c2 with indices: part of a larger list of the same distribution)."""
     from signinum_b200 import encode
 
     if name == "c1":
-        return encode.config1().tiles, 1
+        return encode.config1(n or 256).tiles, 1
     if name == "c1i":
-        return encode.config1_irreversible().tiles, 1
+        return encode.config1_irreversible(n or 256).tiles, 1
     if name == "c1c":
-        return encode.config1_classic().tiles, 1
+        return encode.config1_classic(n or 256).tiles, 1
     if name == "c2":
         return encode.config2(n or 1024, indices=indices).tiles, 1
-    return encode.config3().tiles, 3
+    return encode.config3(n or 128).tiles, 3
 
 
 class Clocks:
@@ -845,7 +847,7 @@ def main():
         _, tiles, shard = shard_tiles(dist, n_total, lambda idx: build_workload("c2", n_total, idx)[0])
         fmt = 1
     else:
-        tiles, fmt = build_workload(args.workload)
+        tiles, fmt = build_workload(args.workload, args.tiles or None)
     b = Batch(tiles, fmt)
     if shard:
         pixels_total = shard["pixels_total"]
@@ -881,7 +883,7 @@ def main():
         achieved = algo / (stage[dom] / 1000.0) / 1e9
         traffic = traffic_for(args.workload, names[dom])
         cpu = None if args.no_cpu else cpu_baseline(b.tiles, fmt)
-        cfg = dict(WORKLOAD_CONFIG[args.workload],
+        cfg = dict(WORKLOAD_CONFIG[args.workload], **({"tiles": b.n} if args.tiles else {}),
                    parallelism=(f"dp{world}: tile list partitioned by coded bytes" if shard else
                                 f"replicas{world}" if world > 1 else "1 GPU"),
                    l2="inputs larger than L2 (coded + coefficient arenas), no flush",
