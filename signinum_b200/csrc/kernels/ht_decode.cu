@@ -483,6 +483,25 @@ namespace {
 
 constexpr int kMsWarps = 8;  // warps (code blocks in flight) per CTA of the MagSgn pass
 
+// The lane's four stream bytes x (byte j at 8 j; zero past the segment) as
+// one bit string from the position of its first byte: byte j sits at
+// r_j = 8 j minus the 0xFF bytes among the lane's bytes before byte j - 1
+// and the byte before the lane (pf).  Bytes that follow an 0xFF carry 7 bits
+// (their top bit, a stuffed zero, overlaps the next byte and is ORed in as
+// the reference's reader does).  At most 32 bits: r_3 <= 24.
+__device__ __forceinline__ uint32_t lane_bits(uint32_t x, uint32_t pf, uint32_t f0, uint32_t f1) {
+  const uint32_t r1 = 8 - pf, r2 = r1 + 8 - f0, r3 = r2 + 8 - f1;
+  return (x & 0xFFu) | (((x >> 8) & 0xFFu) << r1) | (((x >> 16) & 0xFFu) << r2) | ((x >> 24) << r3);
+}
+
+// ORs a lane's bit string v into the bit array W at bit position pos (two
+// words at most).
+__device__ __forceinline__ void or_bits(uint32_t* W, uint32_t pos, uint32_t v) {
+  const uint32_t wi = pos >> 5, sh = pos & 31;
+  atomicOr(&W[wi], v << sh);
+  if (sh && (v >> (32 - sh))) atomicOr(&W[wi + 1], v >> (32 - sh));
+}
+
 // Unstuffs the forward MagSgn byte stream [0, len) into a bit array W
 // (bit k of the stream = bit k%32 of W[k/32]): each byte contributes 8 bits,
 // or 7 after a 0xFF byte, ORed in at its offset exactly as the reference's
@@ -536,17 +555,9 @@ __device__ uint32_t unstuff_magsgn(const uint8_t* src, uint32_t len, uint32_t* W
     const uint32_t F = ff_total + __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
     uint32_t pf = __shfl_up_sync(0xFFFFFFFFu, f3, 1);
     if (lane == 0) pf = prev_ff;
-    // Byte i0 + j is shortened by the 0xFF bytes among [0, i0 + j - 1).
-    const uint32_t ffb[4] = {F - pf, F, F + f0, F + f0 + f1};
-#pragma unroll
-    for (uint32_t j = 0; j < 4; ++j) {
-      if (i0 + j < len) {
-        const uint32_t pos = 8 * (i0 + j) - ffb[j];
-        const uint32_t byte = (x >> (8 * j)) & 0xFF;
-        atomicOr(&W[pos >> 5], byte << (pos & 31));
-        if ((pos & 31) > 24) atomicOr(&W[(pos >> 5) + 1], byte >> (32 - (pos & 31)));
-      }
-    }
+    // Byte i0 is shortened by the 0xFF bytes among [0, i0 - 1); the lane's
+    // other bytes follow it (lane_bits).
+    if (x) or_bits(W, 8 * i0 - (F - pf), lane_bits(x, pf, f0, f1));
     ff_total += __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
     const uint32_t last = min(base + 128, len) - 1 - base;  // last byte of the step
     const uint32_t lb = last >> 2, lj = last & 3;
@@ -689,16 +700,17 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
   uint32_t e_left = 0, e_right = 0;  // NARROW: bottom-row bit lengths of this lane's quad
   uint32_t rowbase = 0;
   bool bad = false;
-  for (uint32_t y = 0, r = 0; y < h; y += 2, ++r) {
+  // Running pointers: sample row y of the block and quad row r of its symbols.
+  int32_t* row0 = dst;
+  const uint32_t* srow = sym;
+  for (uint32_t y = 0; y < h; y += 2, row0 += 2 * (size_t)stride, srow += qs) {
     const bool initial = y == 0, second = y + 1 < h;
-    int32_t* row0 = dst + (size_t)y * stride;
-    int32_t* row1 = row0 + stride;
     // NARROW rows have at most 32 quads: one pass, known at compile time.
     const uint32_t c0_end = NARROW ? 1u : nq;
     for (uint32_t c0 = 0; c0 < c0_end; c0 += 32) {
       const uint32_t q = c0 + lane;
       const bool active = q < nq;
-      const uint32_t s = active ? sym[(size_t)r * qs + q] : 0;
+      const uint32_t s = active ? srow[q] : 0;
       const uint32_t inf = s & 0xFFFF;
       uint32_t U = s >> 16;
       if (!initial) {
@@ -739,15 +751,16 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
       quad_samples<RAW>(W, ms_words, lim, off, inf, qb, p, rs, val, E);
       if (active) {
         const uint32_t x = 2 * q;
+        int32_t* p0 = row0 + x;
         if (pairs && x + 1 < w) {
-          *reinterpret_cast<int2*>(row0 + x) = make_int2(val[0], val[2]);
-          if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(val[1], val[3]);
+          *reinterpret_cast<int2*>(p0) = make_int2(val[0], val[2]);
+          if (second) *reinterpret_cast<int2*>(p0 + stride) = make_int2(val[1], val[3]);
         } else {
-          row0[x] = val[0];
-          if (second) row1[x] = val[1];
+          p0[0] = val[0];
+          if (second) p0[stride] = val[1];
           if (x + 1 < w) {
-            row0[x + 1] = val[2];
-            if (second) row1[x + 1] = val[3];
+            p0[1] = val[2];
+            if (second) p0[stride + 1] = val[3];
           }
         }
         if (!NARROW) {
@@ -828,16 +841,7 @@ __device__ uint32_t unstuff_half(const uint8_t* src, uint32_t len, uint32_t* W, 
         const uint32_t lt = (1u << gl) - 1;
         const uint32_t F = ff_total + __popc(b0 & lt) + __popc(b1 & lt) + __popc(b2 & lt) + __popc(b3 & lt);
         if (gl == 0) pf = prev_ff;
-        const uint32_t ffb[4] = {F - pf, F, F + f0, F + f0 + f1};
-#pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
-          if (i0 + j < len) {
-            const uint32_t pos = 8 * (i0 + j) - ffb[j];
-            const uint32_t byte = (x >> (8 * j)) & 0xFF;
-            atomicOr(&W[pos >> 5], byte << (pos & 31));
-            if ((pos & 31) > 24) atomicOr(&W[(pos >> 5) + 1], byte >> (32 - (pos & 31)));
-          }
-        }
+        if (x) or_bits(W, 8 * i0 - (F - pf), lane_bits(x, pf, f0, f1));
       }
       ff_total += __popc(b0) + __popc(b1) + __popc(b2) + __popc(b3);
       const uint32_t last = min(base + 64, len) - 1 - base;  // last byte of the step
@@ -872,11 +876,17 @@ __device__ bool magsgn_rows_half(const HtJob& job, bool live, const uint32_t* W,
   const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
   uint32_t e_left = 0, e_right = 0, rowbase = 0;
   bool bad = false;
-  for (uint32_t y = 0, r = 0; y < hmax; y += 2, ++r) {
+  // Per lane, invariant over the rows: its quad column, whether it holds a
+  // quad, whether the quad has a right column and whether the pair goes out
+  // in one 8-byte store; running pointers to its samples and its symbols.
+  const uint32_t q = gl;
+  const bool lane_q = q < nq, has_right = 2 * q + 1 < w, pair_store = pairs && has_right;
+  int32_t* lp = dst + 2 * q;
+  const uint32_t* sp = sym + q;
+  for (uint32_t y = 0; y < hmax; y += 2, lp += 2 * (size_t)stride, sp += qs) {
     const bool initial = y == 0, second = y + 1 < h;
-    const uint32_t q = gl;
-    const bool active = y < h && q < nq;
-    const uint32_t s = active ? sym[(size_t)r * qs + q] : 0;
+    const bool active = y < h && lane_q;
+    const uint32_t s = active ? *sp : 0;
     const uint32_t inf = s & 0xFFFF;
     uint32_t U = s >> 16;
     if (!initial) {
@@ -904,23 +914,20 @@ __device__ bool magsgn_rows_half(const HtJob& job, bool live, const uint32_t* W,
     uint32_t E[4];
     quad_samples<false>(W, ms_words, lim, off, inf, qb, p, rs, val, E);
     if (active) {
-      int32_t* row0 = dst + (size_t)y * stride;
-      int32_t* row1 = row0 + stride;
-      const uint32_t x = 2 * q;
-      if (pairs && x + 1 < w) {
-        *reinterpret_cast<int2*>(row0 + x) = make_int2(val[0], val[2]);
-        if (second) *reinterpret_cast<int2*>(row1 + x) = make_int2(val[1], val[3]);
+      if (pair_store) {
+        *reinterpret_cast<int2*>(lp) = make_int2(val[0], val[2]);
+        if (second) *reinterpret_cast<int2*>(lp + stride) = make_int2(val[1], val[3]);
       } else {
-        row0[x] = val[0];
-        if (second) row1[x] = val[1];
-        if (x + 1 < w) {
-          row0[x + 1] = val[2];
-          if (second) row1[x + 1] = val[3];
+        lp[0] = val[0];
+        if (second) lp[stride] = val[1];
+        if (has_right) {
+          lp[1] = val[2];
+          if (second) lp[stride + 1] = val[3];
         }
       }
     }
     e_left = active ? E[1] : 0;
-    e_right = active && 2 * q + 1 < w ? E[3] : 0;
+    e_right = active && has_right ? E[3] : 0;
   }
   return ((__ballot_sync(0xFFFFFFFFu, bad) >> gsh) & 0xFFFFu) != 0;
 }
