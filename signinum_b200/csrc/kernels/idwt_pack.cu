@@ -420,11 +420,26 @@ constexpr int kRowWords = (16 + kIdwtStripW * 6) / 4;
 // pixels of BPP bytes) are staged in the warp's row buffer so that the copied
 // range has the destination's alignment mod 16, then columns [xs, xe) go out
 // as the bytes up to the first 16-byte boundary, 16-byte vectors and a tail.
+// g: the destination of column xs in the row; lane k's words hold columns
+// x0 + 4k .. x0 + 4k + 3.  When the destination is 4-byte aligned and the
+// columns [xs, xs + nbytes / BPP) start and end on lane boundaries (whole
+// strips of a tile, the common case), every lane inside writes its BPP words
+// itself: four pixels of BPP bytes are BPP 32-bit words at a 4-byte aligned
+// place.  Otherwise the row goes through the warp's buffer as below.
 template <int BPP>
-__device__ __forceinline__ void store_row(const PackJob& job, int y, int x0, int xs, int nbytes, int lane,
-                                          uint32_t* rowbuf, const uint32_t* wds) {
+__device__ __forceinline__ void store_row(uint8_t* g, int x0, int xs, int nbytes, int lane, uint32_t* rowbuf,
+                                          const uint32_t* wds) {
+  const int xe = xs + nbytes / BPP;
+  if ((((uintptr_t)g & 3) | ((xs - x0) & 3) | ((xe - x0) & 3)) == 0) {  // warp-uniform
+    const int c = x0 + 4 * lane;
+    if (c >= xs && c < xe) {
+      uint32_t* d = reinterpret_cast<uint32_t*>(g + (size_t)(c - xs) * BPP);
+#pragma unroll
+      for (int k = 0; k < BPP; ++k) d[k] = wds[k];
+    }
+    return;
+  }
   uint8_t* rowbytes = reinterpret_cast<uint8_t*>(rowbuf);
-  uint8_t* g = job.out + (uint64_t)(y - (int)job.cy) * job.pitch + (uint64_t)(xs - (int)job.cx) * BPP;
   const int sh = (int)(((uintptr_t)g - (uintptr_t)((xs - x0) * BPP)) & 15);
   if ((sh & 3) == 0) {
     uint32_t* dst = rowbuf + (sh >> 2) + lane * BPP;
@@ -485,7 +500,8 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
       c0 += shift;
       put_pixel<FMT, DIRECT>(wds, p, c0, c1, c2, bd, reg);
     }
-    store_row<BPP>(job, y, x0, xs, nbytes, lane, rowbuf, wds);
+    store_row<BPP>(job.out + (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * BPP, x0, xs, nbytes, lane,
+                   rowbuf, wds);
   };
   if (job.lifting) {
     if (NC == 3) {
@@ -931,7 +947,8 @@ __device__ __forceinline__ void pack97_unit(const PackJob& job, int x0, int ys, 
       put_pixel97<FMT>(wds, p, c0, c1, c2, bd, reg);
     }
     // Lane k's words are columns x0 - 4 + 4k ..: the row starts at x0 - 4.
-    store_row<BPP>(job, y, x0 - 4, xs, nbytes, lane, rowbuf, wds);
+    store_row<BPP>(job.out + (uint64_t)(y - cy0) * job.pitch + (uint64_t)(xs - cx0) * BPP, x0 - 4, xs, nbytes,
+                   lane, rowbuf, wds);
   };
   if (job.lifting) {
     if (NC == 3) {
