@@ -116,47 +116,6 @@ struct Mel {
   }
 };
 
-// The MEL symbols of a block, decoded ahead of the VLC chain.  Each MEL
-// codeword (Mel::get_run) expands into its symbols, first symbol in the
-// lowest bit: a 1 codeword into 2^e zero symbols, a 0 codeword with its
-// e-bit value v into v zeros and a one.  The VLC chain takes one symbol
-// where the reference decrements its run counter by two and tests it for -1
-// (decode_cleanup_symbols, ht_block_decode.rs:1056-1205), so it sees the same
-// symbols in the same order; taking one is a shift, and codewords are decoded
-// in batches (at least 32 symbols at a time) between pair steps.
-struct MelSymbols {
-  Mel mel;
-  uint64_t sb;  // buffered symbols
-  int sn;       // how many
-  __device__ void init(const uint8_t* d, uint32_t lcup, uint32_t scup) {
-    mel.init(d, lcup, scup);
-    sb = 0;
-    sn = 0;
-  }
-  __device__ __forceinline__ void fill_ahead() {
-    while (sn <= 32) {
-      const int r = mel.get_run();
-      // r = 2 z: z + 1 = 2^e zeros; r = 2 v + 1: v zeros, then a one.
-      if (r & 1) {
-        sb |= 1ull << (sn + (r >> 1));
-        sn += (r >> 1) + 1;
-      } else {
-        sn += (r >> 1) + 1;
-      }
-    }
-  }
-  // Every pair step takes at most three symbols.
-  __device__ __forceinline__ void ensure3() {
-    if (sn < 3) fill_ahead();
-  }
-  __device__ __forceinline__ uint32_t take() {
-    const uint32_t v = (uint32_t)sb & 1u;
-    sb >>= 1;
-    --sn;
-    return v;
-  }
-};
-
 // Four bytes (highest address first) into the backward VLC reader's bit
 // buffer one at a time, for words with a byte whose low 7 bits are all ones
 // (after a byte above 0x8F such a byte loses its top bit to stuffing).  Out
@@ -339,10 +298,11 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
   if (lcup < 2) return false;
   uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
   if (scup < 2 || scup > lcup || scup > 4079) return false;
-  MelSymbols mel;
+  Mel mel;
   mel.init(src, lcup, scup);
   Vlc vlc;
   vlc.init(src, lcup, scup);
+  int run = mel.get_run();
   const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
   uint32_t* row = sym;
   // REG blocks whose rows hold a multiple of 4 symbols stage each row's
@@ -369,10 +329,13 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
   {
     uint32_t c_q = 0;
     for (uint32_t q = 0; q < nq; q += 2) {
-      mel.ensure3();
       uint32_t v = vlc.fetch();
       uint32_t t0 = T.vlc0[c_q + (v & 0x7F)];
-      if (c_q == 0) t0 = mel.take() ? t0 : 0;
+      if (c_q == 0) {
+        run -= 2;
+        t0 = run == -1 ? t0 : 0;
+        if (run < 0) run = mel.get_run();
+      }
       c_q = ((t0 & 0x10) << 3) | ((t0 & 0xE0) << 2);
       // The pair's bits (at most 30) are read from the 32-bit window v with
       // 32-bit shifts; the reader advances once, by their sum, at the end.
@@ -380,13 +343,21 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       v >>= l0;
       const bool hasB = q + 1 < nq;
       uint32_t t1 = T.vlc0[c_q + (v & 0x7F)];
-      if (c_q == 0 && hasB) t1 = mel.take() ? t1 : 0;
+      if (c_q == 0 && hasB) {
+        run -= 2;
+        t1 = run == -1 ? t1 : 0;
+        if (run < 0) run = mel.get_run();
+      }
       if (!hasB) t1 = 0;
       c_q = ((t1 & 0x10) << 3) | ((t1 & 0xE0) << 2);
       const uint32_t l1 = t1 & 7;
       v >>= l1;
       uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
-      if (mode == 0xC0 && mel.take()) mode += 0x40;
+      if (mode == 0xC0) {
+        run -= 2;
+        if (run == -1) mode += 0x40;
+        if (run < 0) run = mel.get_run();
+      }
       uint32_t ue = T.uvlc0[mode + (v & 0x3F)];
       const uint32_t lp = ue & 7;
       v >>= lp;
@@ -430,10 +401,13 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       }
       c_q |= (pq0 & 0xA0) << 2;
       c_q |= (pq1 & 0x20) << 4;
-      mel.ensure3();
       uint32_t v = vlc.fetch();
       uint32_t t0 = T.vlc1[c_q + (v & 0x7F)];
-      if (c_q == 0) t0 = mel.take() ? t0 : 0;
+      if (c_q == 0) {
+        run -= 2;
+        t0 = run == -1 ? t0 : 0;
+        if (run < 0) run = mel.get_run();
+      }
       c_q = ((t0 & 0x40) << 2) | ((t0 & 0x80) << 1);
       c_q |= pq0 & 0x80;
       c_q |= (pq1 & 0xA0) << 2;
@@ -442,7 +416,11 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       v >>= l0;
       const bool hasB = q + 1 < nq;
       uint32_t t1 = T.vlc1[c_q + (v & 0x7F)];
-      if (c_q == 0 && hasB) t1 = mel.take() ? t1 : 0;
+      if (c_q == 0 && hasB) {
+        run -= 2;
+        t1 = run == -1 ? t1 : 0;
+        if (run < 0) run = mel.get_run();
+      }
       if (!hasB) t1 = 0;
       c_q = ((t1 & 0x40) << 2) | ((t1 & 0x80) << 1);
       c_q |= pq1 & 0x80;
