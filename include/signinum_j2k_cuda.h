@@ -163,7 +163,8 @@ sgn_status sgn_plan_surfaces(const sgn_plan* plan, sgn_surface* outs, size_t n);
 sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms);
 /* Autotuner (no counterpart in the reference).  Times the plan's stages on
  * its own data over `reps` runs each (0: 5) for every candidate launch shape
- * (VLC threads per CTA and code blocks per VLC warp; MagSgn warps per CTA, one block per warp or persistent
+ * (VLC threads per CTA, code blocks per VLC warp and its bit-reader refills
+ * inline or out of line; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
  * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
  * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
@@ -176,6 +177,7 @@ typedef struct sgn_tune_report {
   float vlc_ms_default, ms_ms_default, dwt_ms_default;             /* the default shape's */
   int32_t idwt_seg_shift, pack_seg_shift;                          /* chosen DWT tile shape (rows x 2^shift) */
   uint32_t vlc_lanes;                                              /* chosen code blocks per VLC warp */
+  uint32_t vlc_outline; /* 1: the VLC pass's bit-reader refills out of line, 0: inline */
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;

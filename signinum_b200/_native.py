@@ -68,7 +68,7 @@ class SgnTuneReport(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("vlc_threads", "ms_warps", "ms_blocks_per_grab", "dwt_queue")] + \
                [(n, ctypes.c_float) for n in ("vlc_ms", "ms_ms", "dwt_ms", "vlc_ms_default", "ms_ms_default",
                                               "dwt_ms_default")] + \
-               [(n, ctypes.c_int32) for n in ("idwt_seg_shift", "pack_seg_shift")] + [("vlc_lanes", ctypes.c_uint32)]
+               [(n, ctypes.c_int32) for n in ("idwt_seg_shift", "pack_seg_shift")] + [("vlc_lanes", ctypes.c_uint32), ("vlc_outline", ctypes.c_uint32)]
 
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.

@@ -810,7 +810,8 @@ sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev) {
   if (p->d_queue && (e = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "work queue reset");
   if ((e = mark(0)) != cudaSuccess) return cuda_status(e, "event record");
-  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads, c.vlc_lanes)) != cudaSuccess)
+  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads, c.vlc_lanes,
+                         c.vlc_outline != 0)) != cudaSuccess)
     return cuda_status(e, "HT VLC launch");
   if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
@@ -1140,18 +1141,21 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   const LaunchConfig base = p->cfg;
   sgn_tune_report rep;
   std::memset(&rep, 0, sizeof(rep));
-  // VLC pass: threads per CTA and code blocks per warp.
+  // VLC pass: threads per CTA, code blocks per warp, and the bit readers'
+  // refills inline or out of line (inline suits batches of few blocks per
+  // lane, out of line the large ones, whose warps diverge more).
   const uint32_t vlc_c[] = {64, 128};
   float best_vlc = 1e30f;
-  uint32_t vlc_threads = base.vlc_threads, vlc_lanes = p->cfg.vlc_lanes;
-  for (uint32_t t : vlc_c)
-    for (uint32_t l = 32; l >= 1; l /= 2) {
-      if (l < 32 && (uint64_t)l * 64 > p->nht) continue;  // fewer blocks per warp only pays for small plans
-      float ms = time_stage(s, reps, [&] { return launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, t, l); },
-                            e);
-      if (t == 128 && l == p->cfg.vlc_lanes) rep.vlc_ms_default = ms;
-      if (e == cudaSuccess && ms < best_vlc) best_vlc = ms, vlc_threads = t, vlc_lanes = l;
-    }
+  uint32_t vlc_threads = base.vlc_threads, vlc_lanes = p->cfg.vlc_lanes, vlc_outline = base.vlc_outline;
+  for (uint32_t o = 0; o < 2; ++o)
+    for (uint32_t t : vlc_c)
+      for (uint32_t l = 32; l >= 1; l /= 2) {
+        if (l < 32 && (uint64_t)l * 64 > p->nht) continue;  // fewer blocks per warp only pays for small plans
+        float ms = time_stage(
+            s, reps, [&] { return launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, t, l, o != 0); }, e);
+        if (t == 128 && l == p->cfg.vlc_lanes && o == base.vlc_outline) rep.vlc_ms_default = ms;
+        if (e == cudaSuccess && ms < best_vlc) best_vlc = ms, vlc_threads = t, vlc_lanes = l, vlc_outline = o;
+      }
   // MagSgn pass: warps per CTA, grid or queue (blocks per grab).
   struct MsC {
     uint32_t warps, gran;
@@ -1221,6 +1225,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   cfg.pack_seg_shift = pack_shift;
   cfg.vlc_threads = vlc_threads;
   cfg.vlc_lanes = vlc_lanes;
+  cfg.vlc_outline = vlc_outline;
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
   cfg.idwt_queue = idwt_queue;
@@ -1241,6 +1246,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   }
   rep.vlc_threads = cfg.vlc_threads;
   rep.vlc_lanes = cfg.vlc_lanes;
+  rep.vlc_outline = cfg.vlc_outline;
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
   rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);

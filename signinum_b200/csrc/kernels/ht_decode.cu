@@ -77,7 +77,8 @@ __device__ __noinline__ MelFill mel_refill(const uint8_t* data, MelFill f) {
 // 64-bit buffer of unstuffed MEL bits (most significant bit first), with no
 // inner loop: lanes of a warp decode different blocks, so a short fixed
 // sequence per run diverges far less than a queue refill.
-struct Mel {
+template <bool OUTLINE>
+struct MelT {
   const uint8_t* data;
   uint32_t pos, remaining, unstuff;
   uint64_t buf;  // unread bits, left-aligned
@@ -91,13 +92,33 @@ struct Mel {
     bits = 0;
     k = 0;
   }
+  // OUTLINE: the refill is the out-of-line mel_refill; otherwise its loop
+  // is inlined (which is faster depends on the batch: the autotuner picks).
   __device__ __forceinline__ void refill() {
-    const MelFill f = mel_refill(data, MelFill{buf, pos, remaining, unstuff, bits});
-    buf = f.buf;
-    pos = f.pos;
-    remaining = f.remaining;
-    unstuff = f.unstuff;
-    bits = f.bits;
+    if constexpr (OUTLINE) {
+      const MelFill f = mel_refill(data, MelFill{buf, pos, remaining, unstuff, bits});
+      buf = f.buf;
+      pos = f.pos;
+      remaining = f.remaining;
+      unstuff = f.unstuff;
+      bits = f.bits;
+    } else {
+      while (bits <= 56) {
+        uint32_t b;
+        if (remaining > 0) {
+          b = ld8(data + pos);
+          ++pos;
+          --remaining;
+        } else {
+          b = 0xFF;
+        }
+        if (remaining == 0) b |= 0x0F;
+        const int nb = 8 - (int)unstuff;
+        buf |= (uint64_t)(b & ((1u << nb) - 1)) << (64 - bits - nb);
+        bits += nb;
+        unstuff = b == 0xFF;
+      }
+    }
   }
   __device__ __forceinline__ int get_run() {
     if (bits < 6) refill();
@@ -137,7 +158,8 @@ __device__ __noinline__ VlcPush vlc_push4(uint32_t wv, uint64_t tmp, uint32_t bi
 }
 
 // Backward VLC reader (ht_block_decode.rs:932-1000, new_vlc).
-struct Vlc {
+template <bool OUTLINE>
+struct VlcT {
   const uint8_t* data;
   int pos;
   uint32_t remaining;
@@ -211,11 +233,16 @@ struct Vlc {
           tmp |= (uint64_t)__byte_perm(wv, 0, 0x0123) << bits;
           bits += 32;
           unstuff = (wv & 0xFF) > 0x8F;
-        } else {
+        } else if constexpr (OUTLINE) {
           const VlcPush r = vlc_push4(wv, tmp, bits, unstuff);
           tmp = r.tmp;
           bits = r.bits;
           unstuff = r.unstuff;
+        } else {
+          push(wv >> 24);
+          push((wv >> 16) & 0xFF);
+          push((wv >> 8) & 0xFF);
+          push(wv & 0xFF);
         }
       } else {
         uint32_t b = 0;
@@ -238,6 +265,10 @@ struct Vlc {
     return (uint32_t)tmp;
   }
 };
+
+// The refinement passes use the out-of-line forms.
+using Mel = MelT<true>;
+using Vlc = VlcT<true>;
 
 // Forward reader with 0xFF stuffing (ht_block_decode.rs:888-930).
 template <uint32_t PAD>
@@ -291,16 +322,16 @@ __device__ __forceinline__ uint32_t ctx_entry(uint32_t b) { return ((b & 1) << 5
 // quad rows of nq entries.  The row above gives the context: with REG (blocks
 // at most 64 wide, nq <= 32) its two context bits per quad live in a 64-bit
 // register, otherwise they are read back from the symbol table.
-template <bool REG>
+template <bool REG, bool OUTLINE>
 __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T,
                            uint2* __restrict__ stage) {
   const uint32_t lcup = job.lcup, w = job.w, h = job.h;
   if (lcup < 2) return false;
   uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
   if (scup < 2 || scup > lcup || scup > 4079) return false;
-  Mel mel;
+  MelT<OUTLINE> mel;
   mel.init(src, lcup, scup);
-  Vlc vlc;
+  VlcT<OUTLINE> vlc;
   vlc.init(src, lcup, scup);
   int run = mel.get_run();
   const uint32_t nq = (w + 1) / 2, qs = sym_row_stride(w);
@@ -455,7 +486,9 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
 // different blocks' branches, and a warp pays for every path any of its
 // lanes takes at each step; fewer blocks per warp make each chain step
 // shorter, which a plan with few blocks (one tile) wants, while a large
-// batch fills the SMs with 32 blocks per warp.
+// batch fills the SMs with 32 blocks per warp.  OUTLINE: the bit readers'
+// rare refill paths as out-of-line calls (MelT, VlcT).
+template <bool OUTLINE>
 __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restrict__ jobs, uint32_t njobs,
                                                             const uint8_t* __restrict__ arena,
                                                             uint32_t* __restrict__ symbols, uint32_t lanes) {
@@ -474,8 +507,8 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
   const HtJob job = jobs[j];
   if (job.passes == 0) return;
   uint32_t* sym = symbols + job.sym;
-  const bool ok = job.w <= 64 ? decode_vlc<true>(job, arena + job.src, sym, T, stage)
-                              : decode_vlc<false>(job, arena + job.src, sym, T, stage);
+  const bool ok = job.w <= 64 ? decode_vlc<true, OUTLINE>(job, arena + job.src, sym, T, stage)
+                              : decode_vlc<false, OUTLINE>(job, arena + job.src, sym, T, stage);
   if (!ok) sym[0] = kSymFailed;
 }
 
@@ -823,6 +856,22 @@ __device__ uint32_t unstuff_half(const uint8_t* src, uint32_t len, uint32_t* W, 
       if (nvalid < 4) x &= 0xFFFFFFFFu >> (8 * (4 - nvalid));
     }
     const uint32_t fm = i0 < len ? __vcmpeq4(x, 0xFFFFFFFFu) : 0u;
+    // One vote first: a step in which neither half has an 0xFF byte (and no
+    // 0xFF byte just before it) is a plain shift of the input in both, and
+    // needs neither the per-byte votes nor the 0xFF counts.
+    const uint32_t any_ff = (__ballot_sync(0xFFFFFFFFu, fm != 0) >> gsh) & 0xFFFFu;  // every lane votes
+    const bool plain = base >= len || (base + 64 <= len && !prev_ff && any_ff == 0);
+    if (__all_sync(0xFFFFFFFFu, plain)) {
+      const uint32_t xn = __shfl_down_sync(0xFFFFFFFFu, x, 1, 16);
+      if (base < len) {
+        const uint32_t P = 8 * base - ff_total;
+        const uint32_t s = P & 31, wb = P >> 5;
+        if (gl < 15) W[wb + gl + 1] = __funnelshift_l(x, xn, s);
+        if (gl == 0) atomicOr(&W[wb], x << s);
+        if (gl == 15 && s) atomicOr(&W[wb + 16], x >> (32 - s));
+      }
+      continue;
+    }
     const uint32_t f0 = fm & 1, f1 = (fm >> 8) & 1, f2 = (fm >> 16) & 1, f3 = (fm >> 24) & 1;
     const uint32_t b0 = (__ballot_sync(0xFFFFFFFFu, f0) >> gsh) & 0xFFFFu;
     const uint32_t b1 = (__ballot_sync(0xFFFFFFFFu, f1) >> gsh) & 0xFFFFu;
@@ -1278,12 +1327,14 @@ cudaError_t ht_kernels_init() {
 }
 
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                          cudaStream_t stream, uint32_t threads, uint32_t lanes) {
+                          cudaStream_t stream, uint32_t threads, uint32_t lanes, bool outline) {
   if (njobs == 0) return cudaSuccess;
   if (threads == 0 || threads > kHtThreads || threads % 32) threads = kHtThreads;
   if (lanes == 0 || lanes > 32 || (lanes & (lanes - 1))) lanes = 32;
   const uint32_t warps = (njobs + lanes - 1) / lanes, per_cta = threads / 32;
-  ht_vlc_kernel<<<(warps + per_cta - 1) / per_cta, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
+  const uint32_t grid = (warps + per_cta - 1) / per_cta;
+  if (outline) ht_vlc_kernel<true><<<grid, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
+  else ht_vlc_kernel<false><<<grid, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
   return cudaGetLastError();
 }
 

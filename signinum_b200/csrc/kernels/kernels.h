@@ -44,9 +44,9 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps = 
 // no refinement passes) and decode two per warp, each with half of the
 // warp's ms_words (default: none).
 // The VLC pass: `threads` per CTA, `lanes` code blocks per warp (a power of
-// two, 1..32).
+// two, 1..32); `outline`: the bit readers' rare refill paths out of line.
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
-                          cudaStream_t stream, uint32_t threads = 128, uint32_t lanes = 32);
+                          cudaStream_t stream, uint32_t threads = 128, uint32_t lanes = 32, bool outline = true);
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                              cudaStream_t stream, uint32_t warps = 8, uint32_t* queue = nullptr, uint32_t gran = 0,

@@ -85,6 +85,7 @@ inline unsigned vote(bool p, int mode) {
 }
 inline unsigned __ballot_sync(unsigned, bool p) { return vote(p, 0); }
 inline int __any_sync(unsigned, bool p) { return (int)vote(p, 1); }
+inline int __all_sync(unsigned, bool p) { return vote(p, 0) == 0xFFFFFFFFu; }
 inline unsigned __funnelshift_r(unsigned lo, unsigned hi, unsigned sh) {
   uint64_t v = ((uint64_t)hi << 32) | lo;
   return (unsigned)(v >> (sh & 31));

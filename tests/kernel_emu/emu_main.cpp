@@ -26,7 +26,7 @@ alignas(16) uint8_t g_dyn_smem[232448];
 
 namespace sgn {
 void emu_tables();
-void emu_vlc(const HtJob*, uint32_t, const uint8_t*, uint32_t*);
+void emu_vlc(const HtJob*, uint32_t, const uint8_t*, uint32_t*, bool);
 void emu_magsgn(const HtJob*, uint32_t, const uint8_t*, const uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t,
                 uint32_t);
 void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t*, uint32_t*);
@@ -202,7 +202,15 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
   ms_words = std::max(ms_words, 2 * ms_half);
   std::vector<uint32_t> symbols(std::max<uint64_t>(sym, 1), 0xDEADBEEF);
   n = (uint32_t)jobs.size();
-  launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols.data()); });
+  // Both forms of the VLC pass (bit-reader refills inline and out of line)
+  // must write the same symbols.
+  std::vector<uint32_t> symbols_inline(symbols);
+  launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols.data(), true); });
+  launch((n + 127) / 128, 128, [&] { emu_vlc(jobs.data(), n, arena.data(), symbols_inline.data(), false); });
+  if (symbols_inline != symbols) {
+    printf("VLC pass forms disagree\n");
+    return 1;
+  }
   const size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, 8);
   if (smem > sizeof(g_dyn_smem)) { printf("smem too large\n"); return 2; }
   const uint32_t nitems = nsingle + (n - nsingle + 1) / 2;

@@ -11,7 +11,10 @@ CSRC = pathlib.Path(__file__).resolve().parents[2] / "signinum_b200" / "csrc"
 HT_WRAPPERS = """
 namespace sgn {
 void emu_tables() { build_decode_tables(g_ht_tables); }
-void emu_vlc(const HtJob* jobs, uint32_t n, const uint8_t* arena, uint32_t* sym) { ht_vlc_kernel(jobs, n, arena, sym, 32); }
+void emu_vlc(const HtJob* jobs, uint32_t n, const uint8_t* arena, uint32_t* sym, bool outline) {
+  if (outline) ht_vlc_kernel<true>(jobs, n, arena, sym, 32);
+  else ht_vlc_kernel<false>(jobs, n, arena, sym, 32);
+}
 void emu_magsgn(const HtJob* jobs, uint32_t n, const uint8_t* arena, const uint32_t* sym, int32_t* coef,
                 uint32_t* status, uint32_t ms_words, uint32_t max_w, uint32_t nsingle) {
   ht_magsgn_kernel<false>(jobs, n, arena, sym, coef, status, ms_words, max_w, nullptr, 0, nsingle);
