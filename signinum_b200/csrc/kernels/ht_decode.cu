@@ -53,8 +53,26 @@ struct MelFill {
   uint32_t pos, remaining, unstuff;
   int bits;
 };
-__device__ __noinline__ MelFill mel_refill(const uint8_t* data, MelFill f) {
+// The out-of-line refill loop.  While 32 bits or fewer are buffered, four
+// bytes that are not the segment's last, after a byte that is not 0xFF and
+// with no 0xFF among their first three (each then carries 8 bits) go in as
+// one word from four independent loads; other bytes one at a time.  (The
+// inline form keeps the byte loop alone: the word step measured slower
+// inlined in the chain.)
+__device__ __forceinline__ void mel_fill(const uint8_t* data, MelFill& f) {
   while (f.bits <= 56) {
+    if (f.bits <= 32 && f.remaining >= 5 && !f.unstuff) {
+      const uint8_t* p = data + f.pos;
+      const uint32_t b0 = __ldg(p), b1 = __ldg(p + 1), b2 = __ldg(p + 2), b3 = __ldg(p + 3);
+      if (b0 != 0xFF && b1 != 0xFF && b2 != 0xFF) {
+        f.buf |= (uint64_t)((b0 << 24) | (b1 << 16) | (b2 << 8) | b3) << (32 - f.bits);
+        f.bits += 32;
+        f.pos += 4;
+        f.remaining -= 4;
+        f.unstuff = b3 == 0xFF;
+        continue;
+      }
+    }
     uint32_t b;
     if (f.remaining > 0) {
       b = __ldg(data + f.pos);
@@ -69,6 +87,9 @@ __device__ __noinline__ MelFill mel_refill(const uint8_t* data, MelFill f) {
     f.bits += nb;
     f.unstuff = b == 0xFF;
   }
+}
+__device__ __noinline__ MelFill mel_refill(const uint8_t* data, MelFill f) {
+  mel_fill(data, f);
   return f;
 }
 
@@ -310,11 +331,26 @@ __device__ __forceinline__ int32_t to_i32(uint32_t v, uint32_t nbp) {
   return (v & 0x80000000u) ? -m : m;
 }
 
-// Significance of the two bottom samples of a quad (entry bits 5 and 7), the
-// only part of a quad the row below takes its context from, as two bits.
-__device__ __forceinline__ uint32_t ctx_bits(uint32_t t) { return ((t >> 5) & 1) | ((t >> 6) & 2); }
-// The same two bits spread back to their entry positions.
-__device__ __forceinline__ uint32_t ctx_entry(uint32_t b) { return ((b & 1) << 5) | ((b & 2) << 6); }
+// Row-above context of blocks at most 64 wide (REG): the significance of
+// the two bottom samples of each quad (entry bits 5 and 7, the only part of
+// a quad the row below takes its context from) in one 64-bit mask S, four
+// bits per quad pair k at bits 4k .. 4k+3: {first quad's bit 5, second
+// quad's bit 5, first quad's bit 7, second quad's bit 7}.  In that order a
+// quad's two context bits from above (entry bits 7 and 9 of c_q: the left
+// quad's bit 7 or its own bit 5; its own bit 7 or the right quad's bit 5)
+// are ORs of adjacent bits of S: with Q = S | S >> 1, quad 2k takes
+// Q[4k-1] and Q[4k+1], quad 2k+1 Q[4k+1] and Q[4k+3].
+__device__ __forceinline__ uint32_t pair_nibble(uint32_t t0, uint32_t t1) {
+  return (t0 & 0xA0u) | ((t1 & 0xA0u) << 1);  // the pair's four bits at bits 5 .. 8
+}
+// Appends a pair's nibble to the row mask under construction (pairs enter
+// at the top and move down four bits per pair; the row's end aligns them).
+__device__ __forceinline__ uint64_t push_nibble(uint64_t S, uint32_t nib) {
+  return (S >> 4) | ((uint64_t)nib << 55);
+}
+// Context bit 8 of a quad from its left neighbour t in the same row (not
+// the initial row): either of the neighbour's right-column samples.
+__device__ __forceinline__ uint32_t left_ctx(uint32_t t) { return ((t & 0xC0u) + 0xC0u) & 0x100u; }
 
 // CxtVLC / MEL / UVLC pass of one block (decode_cleanup_symbols,
 // ht_block_decode.rs:1056-1205): the serial chain of the cleanup pass.  Writes
@@ -355,7 +391,10 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       }
     }
   };
-  uint64_t ctx = 0;  // REG: context bits of the row above, 2 per quad
+  // REG: the finished row's context mask S (pair_nibble); pairs enter it at
+  // the top, so the row's end shifts it down by 4 bits per absent pair.
+  uint64_t S = 0;
+  const uint32_t row_align = 64 - 4 * ((nq + 1) / 2);
   // Initial quad row.
   {
     uint32_t c_q = 0;
@@ -400,8 +439,9 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       len = ue & 7;
       ue >>= 3;
       put(q, t0 | ((1 + (ue & 7) + (tmp & ~(0xFFu << len))) << 16), t1 | ((1 + (ue >> 3) + (tmp >> len)) << 16));
-      if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
+      if (REG) S = push_nibble(S, pair_nibble(t0, t1));
     }
+    if (REG) S >>= row_align;
     flush();
   }
   // Other quad rows: context from the row above (quads q, q+1, q+2).
@@ -409,29 +449,33 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
     const uint32_t* prev = row;
     row += qs;
     uint32_t c_q = 0;
-    const uint64_t above = ctx;
-    ctx = 0;
-    uint32_t pq0, pq1;
+    // REG: Qc = (S | S >> 1) >> (4k + 1) for pair k (bits 0 and 2: Q[4k+1],
+    // Q[4k+3]); up7 = Q[4k-1] at bit 7 (Q[-1] = S[0]).
+    uint64_t Qc = 0;
+    uint32_t up7 = 0;
+    uint32_t pq0 = 0, pq1 = 0;
     if (REG) {
-      pq0 = ctx_entry((uint32_t)above);
-      pq1 = ctx_entry((uint32_t)above >> 2);
+      Qc = (S | (S >> 1)) >> 1;
+      up7 = ((uint32_t)S & 1u) << 7;
+      S = 0;
     } else {
       pq0 = prev[0] & 0xFFFF;
       pq1 = nq > 1 ? prev[1] & 0xFFFF : 0;
     }
     for (uint32_t q = 0; q < nq; q += 2) {
-      uint32_t pq2, pq3;
+      uint32_t pq2 = 0, pq3 = 0, a1 = 0;
       if (REG) {
-        // Bits past the row's last quad are zero.
-        const uint32_t a = (uint32_t)(above >> (2 * q)) >> 4;  // 2q <= 60
-        pq2 = ctx_entry(a);
-        pq3 = ctx_entry(a >> 2);
+        const uint32_t qc = (uint32_t)Qc;
+        c_q |= up7 | ((qc & 1u) << 9);  // quad q
+        a1 = (qc & 5u) << 7;             // quad q + 1
+        up7 = (qc & 4u) << 5;
+        Qc >>= 4;
       } else {
         pq2 = q + 2 < nq ? prev[q + 2] & 0xFFFF : 0;
         pq3 = q + 3 < nq ? prev[q + 3] & 0xFFFF : 0;
+        c_q |= (pq0 & 0xA0) << 2;
+        c_q |= (pq1 & 0x20) << 4;
       }
-      c_q |= (pq0 & 0xA0) << 2;
-      c_q |= (pq1 & 0x20) << 4;
       uint32_t v = vlc.fetch();
       uint32_t t0 = T.vlc1[c_q + (v & 0x7F)];
       if (c_q == 0) {
@@ -439,10 +483,9 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
         t0 = run == -1 ? t0 : 0;
         if (run < 0) run = mel.get_run();
       }
-      c_q = ((t0 & 0x40) << 2) | ((t0 & 0x80) << 1);
-      c_q |= pq0 & 0x80;
-      c_q |= (pq1 & 0xA0) << 2;
-      c_q |= (pq2 & 0x20) << 4;
+      c_q = left_ctx(t0);
+      if (REG) c_q |= a1;
+      else c_q |= (pq0 & 0x80) | ((pq1 & 0xA0) << 2) | ((pq2 & 0x20) << 4);
       const uint32_t l0 = t0 & 7;
       v >>= l0;
       const bool hasB = q + 1 < nq;
@@ -453,8 +496,8 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
         if (run < 0) run = mel.get_run();
       }
       if (!hasB) t1 = 0;
-      c_q = ((t1 & 0x40) << 2) | ((t1 & 0x80) << 1);
-      c_q |= pq1 & 0x80;
+      c_q = left_ctx(t1);
+      if (!REG) c_q |= pq1 & 0x80;
       const uint32_t l1 = t1 & 7;
       v >>= l1;
       uint32_t mode = ((t0 & 8) << 3) | ((t1 & 8) << 4);
@@ -469,10 +512,14 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
       len = ue & 7;
       ue >>= 3;
       put(q, t0 | (((ue & 7) + (tmp & ~(0xFFu << len))) << 16), t1 | (((ue >> 3) + (tmp >> len)) << 16));
-      if (REG) ctx |= (uint64_t)(ctx_bits(t0) | (ctx_bits(t1) << 2)) << (2 * q);
-      pq0 = pq2;
-      pq1 = pq3;
+      if (REG) {
+        S = push_nibble(S, pair_nibble(t0, t1));
+      } else {
+        pq0 = pq2;
+        pq1 = pq3;
+      }
     }
+    if (REG) S >>= row_align;
     flush();
   }
   return true;
@@ -1321,6 +1368,15 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps) {
 }
 
 cudaError_t ht_kernels_init() {
+  // The VLC pass's lanes read their blocks' bytes a few at a time over the
+  // whole chain, so its L1 hit rate matters more than a ninth resident CTA:
+  // left to itself the driver sizes shared memory for the CTAs that the
+  // registers allow (228 KB, 28 KB of L1); 72 % (164 KB, 7 CTAs of 21.6 KB)
+  // leaves 92 KB of L1 (C2 VLC pass 0.96 -> 0.88 ms).
+  for (const void* k : {(const void*)ht_vlc_kernel<true>, (const void*)ht_vlc_kernel<false>}) {
+    const cudaError_t c = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 72);
+    if (c != cudaSuccess) return c;
+  }
   cudaError_t e = cudaFuncSetAttribute(ht_magsgn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(ht_magsgn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);

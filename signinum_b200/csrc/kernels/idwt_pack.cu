@@ -74,6 +74,15 @@ struct RawRow {
   int x2;                  // lane 31: high band at column b + 2
 };
 
+// INTERIOR: the strip starts at column 128 or later and ends at least two
+// columns before the level's right edge (interior_strip), so every lane's
+// columns and the edge lanes' extra samples lie inside the level and no
+// column needs a bounds test or a mirror.
+__device__ __forceinline__ bool interior_strip(int x0, int w) {
+  return x0 >= (int)kIdwtStripW && x0 + (int)kIdwtStripW + 2 <= w;
+}
+
+template <bool INTERIOR = false>
 __device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lane) {
   y = fold(y, B.h);
   const int r = y >> 1;
@@ -81,6 +90,24 @@ __device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lan
   const int32_t* Lr = ((y & 1) ? B.lh : B.ll) + (size_t)r * lw;
   const int32_t* Hr = ((y & 1) ? B.hh : B.hl) + (size_t)r * hw;
   RawRow R;
+  if (INTERIOR) {
+    if (B.vec) {
+      const int2 l = __ldg(reinterpret_cast<const int2*>(Lr + b));
+      const int2 h = __ldg(reinterpret_cast<const int2*>(Hr + b));
+      R.lo0 = l.x;
+      R.lo1 = l.y;
+      R.hi0 = h.x;
+      R.hi1 = h.y;
+    } else {
+      R.lo0 = __ldg(Lr + b);
+      R.lo1 = __ldg(Lr + b + 1);
+      R.hi0 = __ldg(Hr + b);
+      R.hi1 = __ldg(Hr + b + 1);
+    }
+    R.x1 = lane == 0 ? __ldg(Hr + b - 1) : lane == kLanes - 1 ? __ldg(Lr + b + 2) : 0;
+    R.x2 = lane == kLanes - 1 ? __ldg(Hr + b + 2) : 0;
+    return R;
+  }
   if (B.vec && b + 1 < hw) {
     // b is even and both band widths are even: one 8-byte load per band.
     const int2 l = __ldg(reinterpret_cast<const int2*>(Lr + b));
@@ -103,7 +130,18 @@ __device__ __forceinline__ RawRow load_row(const Bands& B, int y, int b, int lan
 // Horizontal lifting of a loaded row: samples of image columns 2b .. 2b+3
 // (x: 2b, y: 2b+1, z: 2b+2, w: 2b+3).  Columns past the right edge return
 // garbage.  X[-1] mirrors X[1] and X[w] mirrors X[w-2].
+template <bool INTERIOR = false>
 __device__ __forceinline__ int4 lift_row(const RawRow& R, int w, int b, int lane) {
+  if (INTERIOR) {
+    int hm1 = __shfl_up_sync(0xFFFFFFFFu, R.hi1, 1);  // X[c-1]
+    if (lane == 0) hm1 = R.x1;
+    const int h0 = R.hi0, h1 = R.hi1;                  // X[c+1], X[c+3]
+    const int e0 = R.lo0 - ((hm1 + h0 + 2) >> 2);      // X[c]
+    const int e1 = R.lo1 - ((h0 + h1 + 2) >> 2);       // X[c+2]
+    int e2 = __shfl_down_sync(0xFFFFFFFFu, e0, 1);     // X[c+4]
+    if (lane == kLanes - 1) e2 = R.x1 - ((h1 + R.x2 + 2) >> 2);
+    return make_int4(e0, h0 + ((e0 + e1) >> 1), e1, h1 + ((e1 + e2) >> 1));
+  }
   if (w == 1) return make_int4(R.lo0, 0, 0, 0);
   const int c = 2 * b;
   int hm1 = __shfl_up_sync(0xFFFFFFFFu, R.hi1, 1);  // X[c-1]
@@ -122,8 +160,9 @@ __device__ __forceinline__ int4 lift_row(const RawRow& R, int w, int b, int lane
   return make_int4(e0, h0 + ((e0 + e1) >> 1), e1, h1 + ((e1 + e2) >> 1));
 }
 
+template <bool INTERIOR = false>
 __device__ __forceinline__ int4 hrow(const Bands& B, int y, int b, int lane) {
-  return lift_row(load_row(B, y, b, lane), B.w, b, lane);
+  return lift_row<INTERIOR>(load_row<INTERIOR>(B, y, b, lane), B.w, b, lane);
 }
 
 __device__ __forceinline__ int4 vupdate(int4 xe, int4 a, int4 c) {
@@ -139,13 +178,13 @@ __device__ __forceinline__ int4 vpredict(int4 xo, int4 a, int4 c) {
 // at once; emit(y, v[NC]) receives each finished row (four columns per lane).
 // With PREFETCH the loads of row pair m + 1 are issued before row pair m is
 // lifted (more registers; used where a warp streams one component).
-template <int NC, bool PREFETCH, typename Emit>
+template <int NC, bool PREFETCH, bool INTERIOR, typename Emit>
 __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int ys, int ye, Emit emit) {
   const int h = B[0].h, w = B[0].w;
   int4 v[NC];
   if (h == 1) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c) v[c] = hrow(B[c], 0, b, lane);
+    for (int c = 0; c < NC; ++c) v[c] = hrow<INTERIOR>(B[c], 0, b, lane);
     emit(0, v);
     return;
   }
@@ -153,9 +192,9 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
   RawRow re[NC], ro[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    re[c] = load_row(B[c], ys, b, lane);
-    ro[c] = load_row(B[c], ys + 1, b, lane);
-    xo_prev[c] = hrow(B[c], ys - 1, b, lane);
+    re[c] = load_row<INTERIOR>(B[c], ys, b, lane);
+    ro[c] = load_row<INTERIOR>(B[c], ys + 1, b, lane);
+    xo_prev[c] = hrow<INTERIOR>(B[c], ys - 1, b, lane);
     ev_prev[c] = make_int4(0, 0, 0, 0);
   }
   for (int m = ys >> 1;; ++m) {
@@ -168,15 +207,15 @@ __device__ __forceinline__ void stream_rows(const Bands* B, int b, int lane, int
     for (int c = 0; c < NC; ++c) {
       // Without PREFETCH one component's rows are loaded at a time.
       if (!PREFETCH && !first) {
-        re[c] = load_row(B[c], ye_row, b, lane);
-        ro[c] = load_row(B[c], yo_row, b, lane);
+        re[c] = load_row<INTERIOR>(B[c], ye_row, b, lane);
+        ro[c] = load_row<INTERIOR>(B[c], yo_row, b, lane);
       }
       if (PREFETCH && more) {
-        ne[c] = load_row(B[c], ye_row + 2, b, lane);
-        no[c] = load_row(B[c], yo_row + 2, b, lane);
+        ne[c] = load_row<INTERIOR>(B[c], ye_row + 2, b, lane);
+        no[c] = load_row<INTERIOR>(B[c], yo_row + 2, b, lane);
       }
-      const int4 xe = lift_row(re[c], w, b, lane);
-      xo[c] = lift_row(ro[c], w, b, lane);
+      const int4 xe = lift_row<INTERIOR>(re[c], w, b, lane);
+      xo[c] = lift_row<INTERIOR>(ro[c], w, b, lane);
       ev[c] = vupdate(xe, xo_prev[c], xo[c]);
     }
     if (ye_row - 1 >= ys && ye_row - 1 < ye) {
@@ -208,7 +247,7 @@ constexpr int kStreamSlots = 9;
 // shared-memory slots `st` (slot k at st[k * 32 + lane]) and the components'
 // band descriptors in the warp's shared table `tab`, so only one
 // component's rows are in registers at once.  emit(y, v[3]) as stream_rows.
-template <typename Emit>
+template <bool INTERIOR, typename Emit>
 __device__ __forceinline__ void stream_rows3(const Bands* tab, int b, int lane, int ys, int ye, int4* st,
                                              Emit emit) {
   const int w = tab[0].w, h = tab[0].h;
@@ -217,18 +256,18 @@ __device__ __forceinline__ void stream_rows3(const Bands* tab, int b, int lane, 
   int4 v[3];
   if (h == 1) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) v[c] = hrow(bands(c), 0, b, lane);
+    for (int c = 0; c < 3; ++c) v[c] = hrow<INTERIOR>(bands(c), 0, b, lane);
     emit(0, v);
     return;
   }
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
-    slot(c) = hrow(bands(c), ys - 1, b, lane);
+    slot(c) = hrow<INTERIOR>(bands(c), ys - 1, b, lane);
     slot(3 + c) = make_int4(0, 0, 0, 0);
   }
   // The rows of the next component (or of the next row pair's first
   // component) are loaded while the current one is lifted.
-  RawRow re = load_row(bands(0), ys, b, lane), ro = load_row(bands(0), ys + 1, b, lane);
+  RawRow re = load_row<INTERIOR>(bands(0), ys, b, lane), ro = load_row<INTERIOR>(bands(0), ys + 1, b, lane);
   for (int m = ys >> 1;; ++m) {
     const int ye_row = 2 * m, yo_row = 2 * m + 1;
     const bool more = yo_row < ye;
@@ -237,15 +276,15 @@ __device__ __forceinline__ void stream_rows3(const Bands* tab, int b, int lane, 
       RawRow ne = re, no = ro;
       if (c < 2) {
         const Bands& N = bands(c + 1);
-        ne = load_row(N, ye_row, b, lane);
-        no = load_row(N, yo_row, b, lane);
+        ne = load_row<INTERIOR>(N, ye_row, b, lane);
+        no = load_row<INTERIOR>(N, yo_row, b, lane);
       } else if (more) {
         const Bands& N = bands(0);
-        ne = load_row(N, ye_row + 2, b, lane);
-        no = load_row(N, yo_row + 2, b, lane);
+        ne = load_row<INTERIOR>(N, ye_row + 2, b, lane);
+        no = load_row<INTERIOR>(N, yo_row + 2, b, lane);
       }
-      const int4 xe = lift_row(re, w, b, lane);
-      const int4 xo = lift_row(ro, w, b, lane);
+      const int4 xe = lift_row<INTERIOR>(re, w, b, lane);
+      const int4 xo = lift_row<INTERIOR>(ro, w, b, lane);
       re = ne;
       ro = no;
       const int4 xo_prev = slot(c), ev_prev = slot(3 + c);
@@ -312,7 +351,7 @@ __device__ __forceinline__ void idwt_unit(const IdwtJob* __restrict__ jobs, uint
   int32_t* out = job.out;
   // Rows of w int32 from a 16-byte aligned base: 16-byte stores when w % 4 == 0.
   const bool vec_out = (w & 3) == 0 && (((uintptr_t)out) & 15) == 0;
-  stream_rows<1, true>(&B, b, lane, ys, ye, [&](int y, const int4* v) {
+  auto emit = [&](int y, const int4* v) {
     int32_t* row = out + (size_t)y * w;
     if (vec_out && col + 3 < w) {
       *reinterpret_cast<int4*>(row + col) = v[0];
@@ -322,7 +361,9 @@ __device__ __forceinline__ void idwt_unit(const IdwtJob* __restrict__ jobs, uint
       if (col + 2 < w) row[col + 2] = v[0].z;
       if (col + 3 < w) row[col + 3] = v[0].w;
     }
-  });
+  };
+  if (interior_strip(x0, w)) stream_rows<1, true, true>(&B, b, lane, ys, ye, emit);
+  else stream_rows<1, true, false>(&B, b, lane, ys, ye, emit);
 }
 
 }  // namespace
@@ -508,11 +549,13 @@ __device__ __forceinline__ void pack_unit(const PackJob& job, int x0, int ys, in
       // The components' band descriptors, read from the job once per unit.
       if (lane < 3) tab[lane] = make_bands(job.ll[lane], job.hl[lane], job.lh[lane], job.hh[lane], w, (int)job.h);
       __syncwarp();
-      stream_rows3(tab, b, lane, ys, ye, st, emit);
+      if (interior_strip(x0, w)) stream_rows3<true>(tab, b, lane, ys, ye, st, emit);
+      else stream_rows3<false>(tab, b, lane, ys, ye, st, emit);
       __syncwarp();  // the table is rewritten by the warp's next unit
     } else {
       const Bands B = make_bands(job.ll[0], job.hl[0], job.lh[0], job.hh[0], w, (int)job.h);
-      stream_rows<1, true>(&B, b, lane, ys, ye, emit);
+      if (interior_strip(x0, w)) stream_rows<1, true, true>(&B, b, lane, ys, ye, emit);
+      else stream_rows<1, true, false>(&B, b, lane, ys, ye, emit);
     }
   } else {
     // Nothing left to lift: the image is the LL band itself.

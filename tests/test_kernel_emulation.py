@@ -92,3 +92,21 @@ def test_precinct_partitions_through_emulated_kernels(emu, kind):
         by_comps[comps].append(cs)
     run(emu, "03", by_comps[1])
     run(emu, "124", by_comps[3])
+
+
+def test_interior_strips_through_emulated_kernels(emu):
+    """Levels wide enough for strips with no edge column (the 5/3 lifting's
+    interior form: a strip from column 128 on that ends at least two columns
+    before the level's edge), lossless RGB and gray, under AddressSanitizer."""
+    from signinum_b200 import encode
+    from tests.helpers import random_tile
+
+    rng = np.random.default_rng(4500)
+    by_comps = {1: [], 3: []}
+    for w, h, comps, levels in [(300, 14, 3, 0), (390, 9, 3, 1), (517, 6, 1, 2), (640, 11, 3, 2), (259, 20, 1, 1)]:
+        bd = 8 if comps == 3 else 12
+        px = random_tile(rng, w, h, comps, bd, int(rng.integers(0, 2)))
+        by_comps[comps].append(encode.encode_lossless(px.reshape(-1).view(np.uint8), w, h, comps, bd, levels=levels,
+                                                      cb_exp=4, cb_exp_h=3))
+    run(emu, "03", by_comps[1])
+    run(emu, "124", by_comps[3])
