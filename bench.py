@@ -584,6 +584,21 @@ class ServingRun:
         self.lib = _native.cuda_lib()
         self.h = self.server._h
 
+    def warm_requests(self):
+        """Every pool tile at full and at quarter resolution once: the
+        server parses a tile's packet headers the first time a request
+        needs that resolution and keeps the layout, so after these the
+        timed requests see the steady state of a long-running server."""
+        from signinum_b200._native import SgnRequest
+
+        reqs = []
+        for kind, d in ((0, 1), (2, 4)):
+            for i in range(len(self.pool)):
+                r = SgnRequest(0, 0, 0, 0, 0, 1)
+                r.kind, r.downscale = kind, d
+                reqs.append((self.ids[i], r, i))
+        return reqs
+
     def make_requests(self, n, seed):
         from signinum_b200._native import SgnRequest
 
@@ -737,6 +752,8 @@ def serving_rate(sr, lam, k, args, check):
 
 
 def serving_peak(sr, check=16):
+    warm = sr.warm_requests()
+    sr.run(warm, np.zeros(len(warm)))
     warm, _ = sr.make_requests(2000, 11)
     sr.run(warm, np.zeros(len(warm)))
     peak_reqs, peak_px = sr.make_requests(20000, 12)
