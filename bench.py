@@ -73,7 +73,7 @@ def parse_args():
                     help="c4: arrival rates, tiles/s")
     ap.add_argument("--min-requests", type=int, default=10000, help="c4: requests per rate, at least")
     ap.add_argument("--seconds", type=float, default=1.0, help="c4: open-loop duration per rate, at least")
-    ap.add_argument("--slots", type=int, default=4, help="c4: batches in flight")
+    ap.add_argument("--slots", type=int, default=3, help="c4: batches in flight")
     ap.add_argument("--max-batch", type=int, default=512, help="c4: requests per batch")
     ap.add_argument("--max-batch-samples", type=int, default=96000000,
                     help="c4: decoded samples per batch (0: unbounded)")
