@@ -164,7 +164,8 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms)
 /* Autotuner (no counterpart in the reference).  Times the plan's stages on
  * its own data over `reps` runs each (0: 5) for every candidate launch shape
  * (VLC threads per CTA, code blocks per VLC warp and its bit-reader refills
- * inline or out of line; MagSgn warps per CTA, one block per warp or persistent
+ * inline or out of line; for plans of up to 8192 code blocks, both cleanup
+ * passes fused in one kernel against the best separate pair; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
  * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
  * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
@@ -178,6 +179,8 @@ typedef struct sgn_tune_report {
   int32_t idwt_seg_shift, pack_seg_shift;                          /* chosen DWT tile shape (rows x 2^shift) */
   uint32_t vlc_lanes;                                              /* chosen code blocks per VLC warp */
   uint32_t vlc_outline; /* 1: the VLC pass's bit-reader refills out of line, 0: inline */
+  uint32_t ht_fused;    /* 1: both cleanup passes in one kernel, a CTA per code block (small plans) */
+  float fused_ms;       /* that kernel's time (0: not tried) */
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;
@@ -188,6 +191,11 @@ sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_
  * of the last level + pack, the base rule scaled by 2^shift (shift -2 to 1;
  * strips stay 128 columns wide).  Re-uploads the plan's job tables. */
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* plan, int32_t idwt_seg_shift, int32_t pack_seg_shift);
+/* Sets the HT cleanup form by hand (no counterpart in the reference): 0, the
+ * VLC pass then the MagSgn pass over all blocks; 1, both passes of each block
+ * in one CTA, its MagSgn following its VLC chain row by row (the default for
+ * plans of few blocks); 2, chosen by block count.  Decodes are the same. */
+sgn_status sgn_plan_set_cleanup_form(sgn_ctx* ctx, sgn_plan* plan, uint32_t fused);
 /* Launches issued by one execute of the plan. */
 uint64_t sgn_plan_kernel_launches(const sgn_plan* plan);
 void sgn_plan_destroy(sgn_ctx* ctx, sgn_plan* plan);

@@ -68,7 +68,8 @@ class SgnTuneReport(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("vlc_threads", "ms_warps", "ms_blocks_per_grab", "dwt_queue")] + \
                [(n, ctypes.c_float) for n in ("vlc_ms", "ms_ms", "dwt_ms", "vlc_ms_default", "ms_ms_default",
                                               "dwt_ms_default")] + \
-               [(n, ctypes.c_int32) for n in ("idwt_seg_shift", "pack_seg_shift")] + [("vlc_lanes", ctypes.c_uint32), ("vlc_outline", ctypes.c_uint32)]
+               [(n, ctypes.c_int32) for n in ("idwt_seg_shift", "pack_seg_shift")] + \
+               [(n, ctypes.c_uint32) for n in ("vlc_lanes", "vlc_outline", "ht_fused")] + [("fused_ms", ctypes.c_float)]
 
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.
@@ -135,6 +136,7 @@ CUDA_SIGNATURES = {
                                                 ctypes.POINTER(SgnRequest), ctypes.POINTER(ctypes.c_uint64),
                                                 ctypes.POINTER(ctypes.c_uint64)]),
     "sgn_plan_set_tile_shape": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    "sgn_plan_set_cleanup_form": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     "sgn_ht_decode_blocks_noalloc": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                                       ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
                                                       ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),

@@ -182,6 +182,9 @@ inline uint32_t len_bucket(uint32_t lcup) { return kLenBuckets - 1 - std::min<ui
 constexpr uint32_t kHtBuckets = 2 * kLenBuckets;
 inline bool pairable(const CodeBlock& cb) { return cb.w <= 32 && cb.passes <= 1; }
 inline uint32_t ht_bucket(const CodeBlock& cb) { return (pairable(cb) ? kLenBuckets : 0) + len_bucket(cb.lcup); }
+// Largest plan (HT blocks) the autotuner tries the fused cleanup kernel on
+// (a CTA per block; each waits only on its own chain lane).
+constexpr uint32_t kFusedMaxBlocks = 8192;
 // Classic blocks by coding passes (0 .. 94), most passes first.
 constexpr uint32_t kPassBuckets = 96;
 inline uint32_t pass_bucket(uint32_t passes) { return kPassBuckets - 1 - std::min<uint32_t>(passes, kPassBuckets - 1); }
@@ -734,6 +737,15 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
     while (lanes < 32 && (uint64_t)lanes * 2 <= per_sched) lanes *= 2;
     c.vlc_lanes = lanes;
   }
+  if (c.ht_fused == 2) {
+    // Plans of one block per VLC warp (few blocks, a tile or a few) take the
+    // fused form: each block's MagSgn follows its own chain instead of the
+    // slowest chain of the plan.
+    c.ht_fused = c.vlc_lanes == 1 && p->nht <= kFusedMaxBlocks &&
+                         ht_magsgn_smem_bytes(p->ms_words, p->max_w, 1) <= 200 * 1024
+                     ? 1
+                     : 0;
+  }
   c.ms_ctas = (uint32_t)std::max(1, ms * ctx->sm_count);
   c.idwt_ctas = (uint32_t)std::max(1, idwt * ctx->sm_count);
   c.pack_ctas = (uint32_t)std::max(1, pack * ctx->sm_count);
@@ -810,14 +822,22 @@ sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev) {
   if (p->d_queue && (e = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s)) != cudaSuccess)
     return cuda_status(e, "work queue reset");
   if ((e = mark(0)) != cudaSuccess) return cuda_status(e, "event record");
-  if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads, c.vlc_lanes,
-                         c.vlc_outline != 0)) != cudaSuccess)
-    return cuda_status(e, "HT VLC launch");
-  if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
-  if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words, p->max_w,
-                            s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas, p->nsingle)) !=
-      cudaSuccess)
-    return cuda_status(e, "HT MagSgn launch");
+  if (c.ht_fused == 1) {
+    // Both cleanup passes in one launch (its time shows as the VLC stage).
+    if ((e = launch_ht_fused(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words,
+                             p->max_w, s, c.vlc_outline != 0)) != cudaSuccess)
+      return cuda_status(e, "HT cleanup launch");
+    if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
+  } else {
+    if ((e = launch_ht_vlc(p->d_ht, p->nht, p->d_input, p->d_symbols, s, c.vlc_threads, c.vlc_lanes,
+                           c.vlc_outline != 0)) != cudaSuccess)
+      return cuda_status(e, "HT VLC launch");
+    if ((e = mark(1)) != cudaSuccess) return cuda_status(e, "event record");
+    if ((e = launch_ht_magsgn(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words,
+                              p->max_w, s, c.ms_warps, c.ms_gran ? p->d_queue : nullptr, c.ms_gran, c.ms_ctas,
+                              p->nsingle)) != cudaSuccess)
+      return cuda_status(e, "HT MagSgn launch");
+  }
   if ((e = mark(2)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_ht_refine(p->d_ht, p->d_refine, p->nref, p->d_input, p->d_coef, p->d_status, s)) != cudaSuccess)
     return cuda_status(e, "HT refinement launch");
@@ -1107,6 +1127,18 @@ sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* p, uint32_t vlc_thr
   return apply_config(ctx, p, c);
 }
 
+sgn_status sgn_plan_set_cleanup_form(sgn_ctx* ctx, sgn_plan* p, uint32_t fused) {
+  if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
+  if (fused > 2) return set_error(SGN_ERR_INVALID_ARGUMENT, "cleanup form out of range");
+  if (fused == 1 && (p->nht > kFusedMaxBlocks || ht_magsgn_smem_bytes(p->ms_words, p->max_w, 1) > 200 * 1024))
+    return set_error(SGN_ERR_UNSUPPORTED, "plan too large for the fused cleanup form");
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cudaSetDevice(ctx->device);
+  LaunchConfig c = p->cfg;
+  c.ht_fused = fused;
+  return apply_config(ctx, p, c);
+}
+
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* p, int32_t idwt_seg_shift, int32_t pack_seg_shift) {
   if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
   if (idwt_seg_shift < -2 || idwt_seg_shift > 1 || pack_seg_shift < -2 || pack_seg_shift > 1)
@@ -1177,6 +1209,21 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     if (m.warps == 8 && m.gran == 0) rep.ms_ms_default = ms;
     if (e == cudaSuccess && ms < best_ms) best_ms = ms, ms_warps = m.warps, ms_gran = m.gran;
   }
+  // Both cleanup passes fused (a CTA per block) against the best separate
+  // pair, on plans small enough for it.
+  uint32_t ht_fused = 0, fused_outline = vlc_outline;
+  if (p->nht && p->nht <= kFusedMaxBlocks && ht_magsgn_smem_bytes(p->ms_words, p->max_w, 1) <= 200 * 1024) {
+    float best_fused = 1e30f;
+    for (uint32_t o = 0; o < 2; ++o) {
+      float ms = time_stage(s, reps, [&] {
+        return launch_ht_fused(p->d_ht, p->nht, p->d_input, p->d_symbols, p->d_coef, p->d_status, p->ms_words,
+                               p->max_w, s, o != 0);
+      }, e);
+      if (e == cudaSuccess && ms < best_fused) best_fused = ms, fused_outline = o;
+    }
+    if (best_fused < best_vlc + best_ms) ht_fused = 1;
+    rep.fused_ms = best_fused;
+  }
   // IDWT levels and pack, each: one unit per warp or persistent warps on a
   // queue, and the DWT tile shape (rows per unit: the base rule scaled by
   // 2^shift, shift -2 to 1; the strip is 128 columns, four per lane).
@@ -1225,7 +1272,8 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   cfg.pack_seg_shift = pack_shift;
   cfg.vlc_threads = vlc_threads;
   cfg.vlc_lanes = vlc_lanes;
-  cfg.vlc_outline = vlc_outline;
+  cfg.vlc_outline = ht_fused ? fused_outline : vlc_outline;
+  cfg.ht_fused = ht_fused;
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
   cfg.idwt_queue = idwt_queue;
@@ -1247,6 +1295,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   rep.vlc_threads = cfg.vlc_threads;
   rep.vlc_lanes = cfg.vlc_lanes;
   rep.vlc_outline = cfg.vlc_outline;
+  rep.ht_fused = cfg.ht_fused;
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
   rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);

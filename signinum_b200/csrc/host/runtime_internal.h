@@ -130,6 +130,9 @@ struct LaunchConfig {
   uint32_t vlc_threads = 128;  // threads per CTA of the VLC pass
   uint32_t vlc_lanes = 0;      // code blocks per VLC warp (1..32, a power of two; 0: chosen by block count)
   uint32_t vlc_outline = 1;    // 1: the VLC pass's bit readers refill out of line; 0: inline
+  // 1: both cleanup passes in one kernel, a CTA per block (small plans);
+  // 0: the VLC and MagSgn kernels; 2: chosen by block count.
+  uint32_t ht_fused = 2;
   uint32_t ms_warps = 8;       // warps (code blocks in flight) per CTA of the MagSgn pass
   uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
   uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue

@@ -358,9 +358,16 @@ __device__ __forceinline__ uint32_t left_ctx(uint32_t t) { return ((t & 0xC0u) +
 // quad rows of nq entries.  The row above gives the context: with REG (blocks
 // at most 64 wide, nq <= 32) its two context bits per quad live in a 64-bit
 // register, otherwise they are read back from the symbol table.
-template <bool REG, bool OUTLINE>
+// After each quad row is in the symbol table, row_done(rows written so far)
+// (the fused small-plan kernel publishes progress with it).  The row's pairs
+// are staged at stage[pair * stage_stride + stage_slot].
+struct NoRowHook {
+  __device__ void operator()(uint32_t) const {}
+};
+template <bool REG, bool OUTLINE, typename RowHook = NoRowHook>
 __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __restrict__ sym, const SmemTables& T,
-                           uint2* __restrict__ stage) {
+                           uint2* __restrict__ stage, uint32_t stage_stride, uint32_t stage_slot,
+                           RowHook row_done = RowHook()) {
   const uint32_t lcup = job.lcup, w = job.w, h = job.h;
   if (lcup < 2) return false;
   uint32_t scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
@@ -376,7 +383,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
   // pairs in the lane's shared-memory column and write the row with 16-byte
   // stores (far fewer scattered store requests than one per pair).
   const bool staged = REG && (qs & 3) == 0;
-  const uint32_t lanes = blockDim.x, tid = threadIdx.x;
+  const uint32_t lanes = stage_stride, tid = stage_slot;
   auto put = [&](uint32_t q, uint32_t a, uint32_t b) {
     if (staged) stage[(q >> 1) * lanes + tid] = make_uint2(a, b);
     else *reinterpret_cast<uint2*>(row + q) = make_uint2(a, b);  // q even, rows padded to even
@@ -443,6 +450,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
     }
     if (REG) S >>= row_align;
     flush();
+    row_done(1u);
   }
   // Other quad rows: context from the row above (quads q, q+1, q+2).
   for (uint32_t y = 2; y < h; y += 2) {
@@ -521,6 +529,7 @@ __device__ bool decode_vlc(const HtJob& job, const uint8_t* src, uint32_t* __res
     }
     if (REG) S >>= row_align;
     flush();
+    row_done(y / 2 + 1);
   }
   return true;
 }
@@ -554,8 +563,8 @@ __global__ void __launch_bounds__(kHtThreads) ht_vlc_kernel(const HtJob* __restr
   const HtJob job = jobs[j];
   if (job.passes == 0) return;
   uint32_t* sym = symbols + job.sym;
-  const bool ok = job.w <= 64 ? decode_vlc<true, OUTLINE>(job, arena + job.src, sym, T, stage)
-                              : decode_vlc<false, OUTLINE>(job, arena + job.src, sym, T, stage);
+  const bool ok = job.w <= 64 ? decode_vlc<true, OUTLINE>(job, arena + job.src, sym, T, stage, blockDim.x, threadIdx.x)
+                              : decode_vlc<false, OUTLINE>(job, arena + job.src, sym, T, stage, blockDim.x, threadIdx.x);
   if (!ok) sym[0] = kSymFailed;
 }
 
@@ -756,9 +765,16 @@ __device__ __forceinline__ void quad_samples(const uint32_t* W, uint32_t ms_word
 // neighbouring lanes by shuffles, otherwise they are kept per column in
 // shared memory (Ebase, two rows of `cols` bytes).  Returns true (on every
 // lane) when the stream is invalid.
-template <bool NARROW, bool RAW>
+// Rows are taken as they are: the two-pass form decodes symbols a kernel
+// earlier.
+struct NoRowWait {
+  static constexpr bool kLive = false;
+  __device__ bool operator()(uint32_t) const { return true; }
+};
+template <bool NARROW, bool RAW, typename RowWait = NoRowWait>
 __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_words, uint8_t* Ebase, uint32_t cols,
-                            const uint32_t* __restrict__ sym, int32_t* __restrict__ dst) {
+                            const uint32_t* __restrict__ sym, int32_t* __restrict__ dst,
+                            RowWait row_ready = RowWait()) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t w = job.w, h = job.h, stride = job.stride;
   const uint32_t mmsb = job.mmsb, p = 30 - mmsb, mmsbp2 = mmsb + 2, nbp = job.nbp;
@@ -784,13 +800,20 @@ __device__ bool magsgn_rows(const HtJob& job, const uint32_t* W, uint32_t ms_wor
   int32_t* row0 = dst;
   const uint32_t* srow = sym;
   for (uint32_t y = 0; y < h; y += 2, row0 += 2 * (size_t)stride, srow += qs) {
+    // The fused form waits for the quad row's symbols (warp-uniform result;
+    // false: the chain failed or the wait ran out, and the block is invalid).
+    if (!row_ready(y >> 1)) {
+      bad = true;
+      break;
+    }
     const bool initial = y == 0, second = y + 1 < h;
     // NARROW rows have at most 32 quads: one pass, known at compile time.
     const uint32_t c0_end = NARROW ? 1u : nq;
     for (uint32_t c0 = 0; c0 < c0_end; c0 += 32) {
       const uint32_t q = c0 + lane;
       const bool active = q < nq;
-      const uint32_t s = active ? srow[q] : 0;
+      // Symbols written by the same CTA's chain lane are read past L1.
+      const uint32_t s = active ? (RowWait::kLive ? __ldcg(srow + q) : srow[q]) : 0;
       const uint32_t inf = s & 0xFFFF;
       uint32_t U = s >> 16;
       if (!initial) {
@@ -1039,10 +1062,11 @@ namespace {
 
 // Magnitudes and signs of one code block by the calling warp; W and Ebase
 // are the warp's shared-memory bit array and exponent rows.
+template <typename RowWait = NoRowWait>
 __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena,
                              const uint32_t* __restrict__ symbols, int32_t* __restrict__ coef,
                              uint32_t* __restrict__ tile_status, uint32_t ms_words, uint32_t cols, uint32_t* W,
-                             uint8_t* Ebase) {
+                             uint8_t* Ebase, RowWait row_ready = RowWait()) {
   const uint32_t lane = threadIdx.x & 31;
   int32_t* dst = coef + job.dst;
   const uint32_t w = job.w, h = job.h, stride = job.stride;
@@ -1057,13 +1081,22 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
   // the first of them is loaded: the unstuffing steps and the quad rows then
   // read them from L2.
   prefetch_l2_range(src, job.lcup, lane, 32);
-  prefetch_l2_range(sym, (size_t)sym_row_stride(w) * ((h + 1) / 2) * 4, lane, 32);
-  bool ok = sym[0] != kSymFailed;
   uint32_t lcup = job.lcup, scup = 0;
-  if (ok) {
-    scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
-    ok = (lcup - scup + 15) / 4 + 2 <= ms_words;
+  bool ok;
+  if constexpr (RowWait::kLive) {
+    // The chain is still running: its failure arrives through row_ready, and
+    // the segment checks it starts with are repeated here.
+    ok = lcup >= 2;
+    if (ok) {
+      scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
+      ok = scup >= 2 && scup <= lcup && scup <= 4079;
+    }
+  } else {
+    prefetch_l2_range(sym, (size_t)sym_row_stride(w) * ((h + 1) / 2) * 4, lane, 32);
+    ok = sym[0] != kSymFailed;
+    if (ok) scup = ((uint32_t)ld8(src + lcup - 1) << 4) + (ld8(src + lcup - 2) & 0x0F);
   }
+  if (ok) ok = (lcup - scup + 15) / 4 + 2 <= ms_words;
   if (ok) {
     const uint32_t ms_len = lcup - scup;
     // The block's own words of the bit array (at most ms_words, checked
@@ -1074,10 +1107,11 @@ __device__ void magsgn_block(const HtJob& job, const uint8_t* __restrict__ arena
     unstuff_magsgn(src, ms_len, W, words);
     // Blocks with refinement passes keep the sign-magnitude words for them.
     const bool raw = job.passes > 1;
-    const bool bad = job.w <= 64 ? (raw ? magsgn_rows<true, true>(job, W, words, Ebase, cols, sym, dst)
-                                        : magsgn_rows<true, false>(job, W, words, Ebase, cols, sym, dst))
-                                 : (raw ? magsgn_rows<false, true>(job, W, words, Ebase, cols, sym, dst)
-                                        : magsgn_rows<false, false>(job, W, words, Ebase, cols, sym, dst));
+    const bool bad =
+        job.w <= 64 ? (raw ? magsgn_rows<true, true>(job, W, words, Ebase, cols, sym, dst, row_ready)
+                           : magsgn_rows<true, false>(job, W, words, Ebase, cols, sym, dst, row_ready))
+                    : (raw ? magsgn_rows<false, true>(job, W, words, Ebase, cols, sym, dst, row_ready)
+                           : magsgn_rows<false, false>(job, W, words, Ebase, cols, sym, dst, row_ready));
     ok = !bad;
   }
   if (!ok) {
@@ -1180,6 +1214,81 @@ __global__ void __launch_bounds__(kMsWarps * 32) ht_magsgn_kernel(const HtJob* _
       for (uint32_t it = base; it < end; ++it) item(it);
     }
   }
+}
+
+// Small plans: one CTA of two warps per code block runs both cleanup passes
+// at once.  Lane 0 of warp 0 runs the block's VLC chain (decode_vlc) and
+// publishes each finished quad row in shared memory; warp 1 unstuffs the
+// MagSgn stream meanwhile and decodes each quad row's magnitudes and signs as
+// soon as its symbols are out, so the block's MagSgn work hides behind its
+// own chain instead of waiting for the slowest chain of the plan (a plan of
+// one tile is as long as its longest block's chain).  Waits are bounded: a
+// row that does not arrive within kFusedSpinLimit polls (tens of
+// milliseconds, far beyond any chain) fails the block like an invalid
+// stream.
+namespace {
+
+constexpr uint32_t kFusedThreads = 64;
+constexpr uint32_t kRowsFailed = 0xFFFFFFFFu;
+constexpr uint32_t kFusedSpinLimit = 1u << 20;
+
+struct FusedRowWait {
+  static constexpr bool kLive = true;
+  const volatile uint32_t* progress;  // quad rows published, or kRowsFailed
+  __device__ bool operator()(uint32_t row) const {
+    uint32_t ready = 1;
+    if ((threadIdx.x & 31) == 0) {
+      uint32_t p = *progress;
+      for (uint32_t it = 0; p != kRowsFailed && p <= row && it < kFusedSpinLimit; ++it) {
+        __nanosleep(32);
+        p = *progress;
+      }
+      ready = p != kRowsFailed && p > row;
+    }
+    ready = __shfl_sync(0xFFFFFFFFu, ready, 0);
+    __threadfence_block();  // the row's symbols are read after its flag
+    return ready != 0;
+  }
+};
+
+}  // namespace
+
+template <bool OUTLINE>
+__global__ void __launch_bounds__(kFusedThreads) ht_cleanup_fused_kernel(
+    const HtJob* __restrict__ jobs, uint32_t njobs, const uint8_t* __restrict__ arena, uint32_t* __restrict__ symbols,
+    int32_t* __restrict__ coef, uint32_t* __restrict__ tile_status, uint32_t ms_words, uint32_t max_w) {
+  __shared__ SmemTables T;
+  __shared__ uint2 stage[16];  // the chain lane's pairs of one row of a 64-wide block
+  __shared__ uint32_t rows_done;
+  extern __shared__ __align__(16) uint8_t smem[];
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&g_ht_tables);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&T);
+    for (uint32_t i = threadIdx.x; i < sizeof(SmemTables) / 4; i += blockDim.x) d[i] = src[i];
+  }
+  if (threadIdx.x == 0) rows_done = 0;
+  __syncthreads();
+  if (blockIdx.x >= njobs) return;
+  const HtJob job = jobs[blockIdx.x];
+  volatile uint32_t* progress = &rows_done;
+  if (threadIdx.x < 32) {
+    if (threadIdx.x != 0 || job.passes == 0) return;
+    uint32_t* sym = symbols + job.sym;
+    auto publish = [progress](uint32_t rows) {
+      __threadfence_block();  // the row's symbols before its flag
+      *progress = rows;
+    };
+    const bool ok = job.w <= 64 ? decode_vlc<true, OUTLINE>(job, arena + job.src, sym, T, stage, 1, 0, publish)
+                                : decode_vlc<false, OUTLINE>(job, arena + job.src, sym, T, stage, 1, 0, publish);
+    if (!ok) {
+      __threadfence_block();
+      *progress = kRowsFailed;
+    }
+    return;
+  }
+  const uint32_t cols = max_w + 4;
+  magsgn_block(job, arena, symbols, coef, tile_status, ms_words, cols, reinterpret_cast<uint32_t*>(smem),
+               smem + (size_t)ms_words * 4, FusedRowWait{progress});
 }
 
 // ---------------------------------------------------------------------------
@@ -1377,6 +1486,10 @@ cudaError_t ht_kernels_init() {
     const cudaError_t c = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 72);
     if (c != cudaSuccess) return c;
   }
+  for (const void* k : {(const void*)ht_cleanup_fused_kernel<true>, (const void*)ht_cleanup_fused_kernel<false>}) {
+    const cudaError_t c = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (c != cudaSuccess) return c;
+  }
   cudaError_t e = cudaFuncSetAttribute(ht_magsgn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(ht_magsgn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -1391,6 +1504,21 @@ cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* aren
   const uint32_t grid = (warps + per_cta - 1) / per_cta;
   if (outline) ht_vlc_kernel<true><<<grid, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
   else ht_vlc_kernel<false><<<grid, threads, 0, stream>>>(jobs, njobs, arena, symbols, lanes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ht_fused(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols, int32_t* coef,
+                           uint32_t* tile_status, uint32_t ms_words, uint32_t max_w, cudaStream_t stream,
+                           bool outline) {
+  if (njobs == 0) return cudaSuccess;
+  const size_t smem = ht_magsgn_smem_bytes(ms_words, max_w, 1);
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  if (outline)
+    ht_cleanup_fused_kernel<true><<<njobs, kFusedThreads, smem, stream>>>(jobs, njobs, arena, symbols, coef,
+                                                                          tile_status, ms_words, max_w);
+  else
+    ht_cleanup_fused_kernel<false><<<njobs, kFusedThreads, smem, stream>>>(jobs, njobs, arena, symbols, coef,
+                                                                           tile_status, ms_words, max_w);
   return cudaGetLastError();
 }
 

@@ -47,6 +47,11 @@ size_t ht_magsgn_smem_bytes(uint32_t ms_words, uint32_t max_w, uint32_t warps = 
 // two, 1..32); `outline`: the bit readers' rare refill paths out of line.
 cudaError_t launch_ht_vlc(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols,
                           cudaStream_t stream, uint32_t threads = 128, uint32_t lanes = 32, bool outline = true);
+// Both cleanup passes of each block in one CTA (small plans): the VLC chain
+// on one lane, MagSgn on a second warp following it row by row.
+cudaError_t launch_ht_fused(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, uint32_t* symbols, int32_t* coef,
+                           uint32_t* tile_status, uint32_t ms_words, uint32_t max_w, cudaStream_t stream,
+                           bool outline);
 cudaError_t launch_ht_magsgn(const HtJob* jobs, uint32_t njobs, const uint8_t* arena, const uint32_t* symbols,
                              int32_t* coef, uint32_t* tile_status, uint32_t ms_words, uint32_t max_w,
                              cudaStream_t stream, uint32_t warps = 8, uint32_t* queue = nullptr, uint32_t gran = 0,

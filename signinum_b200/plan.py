@@ -71,6 +71,11 @@ class Plan:
         _check(_native.cuda_lib().sgn_plan_set_tile_shape(self.ctx.handle, self.handle, idwt_seg_shift,
                                                           pack_seg_shift))
 
+    def set_cleanup_form(self, fused=2):
+        """HT cleanup passes: 0 the VLC then the MagSgn kernel, 1 both in one
+        kernel (a CTA per code block), 2 chosen by block count."""
+        _check(_native.cuda_lib().sgn_plan_set_cleanup_form(self.ctx.handle, self.handle, fused))
+
     def execute_timed(self):
         """Per-stage milliseconds: HT VLC pass, HT MagSgn pass, HT refinement, IDWT levels,
         last level + pack, total."""

@@ -8,6 +8,8 @@
 // compiled with -ffp-contract=off so none is fused.
 #pragma once
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <barrier>
 #include <cmath>
 #include <cstdint>
@@ -147,6 +149,10 @@ template <class T> inline T __shfl_xor_sync(unsigned, T v, int m, int width = 32
   return shfl_from(v, src & 31, (src & ~(width - 1)) == (lane & ~(width - 1)));
 }
 inline void __syncwarp() { g_warp->bar.arrive_and_wait(); }
+// The fused kernel's producer and consumer warps meet through shared memory:
+// fences order the host threads' accesses, a sleep yields the thread.
+inline void __threadfence_block() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+inline void __nanosleep(unsigned) { std::this_thread::yield(); }
 inline unsigned atomicAdd(unsigned* p, unsigned v) {
   unsigned o = __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST);
   return o;

@@ -30,6 +30,7 @@ void emu_vlc(const HtJob*, uint32_t, const uint8_t*, uint32_t*, bool);
 void emu_magsgn(const HtJob*, uint32_t, const uint8_t*, const uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t,
                 uint32_t);
 void emu_refine(const HtJob*, const uint32_t*, uint32_t, const uint8_t*, int32_t*, uint32_t*);
+void emu_fused(const HtJob*, uint32_t, const uint8_t*, uint32_t*, int32_t*, uint32_t*, uint32_t, uint32_t, bool);
 void emu_idwt(bool, const IdwtJob*, uint32_t, uint32_t);
 void emu_pack(bool, int, const PackJob*, uint32_t, uint32_t);
 int emu_pack_warps(bool);
@@ -219,6 +220,27 @@ int run(const std::vector<uint8_t>& d, const std::vector<int>& fmts) {
   });
   nr = (uint32_t)refine.size();
   if (nr) launch((nr + 63) / 64, 64, [&] { emu_refine(jobs.data(), refine.data(), nr, arena.data(), coef.data(), status.data()); });
+  // The small-plan form (both cleanup passes of a block in one CTA, the
+  // MagSgn warp following the chain lane row by row) must give the same
+  // coefficients and status, with either VLC form (one form per codestream,
+  // on the first two codestreams of a run with at most 64 blocks: its one
+  // MagSgn warp per CTA runs CTA after CTA here, which is slow to emulate;
+  // the GPU tests run it on every small plan).
+  static int fused_checks = 0;
+  for (int form = fused_checks % 2; n <= 64 && fused_checks < 2 && form < 2; form += 2) {
+    ++fused_checks;
+    std::vector<int32_t> coef2(coef.size(), 0x7F7F7F7F);
+    std::vector<uint32_t> status2(1, 0), sym2(symbols.size(), 0xDEADBEEF);
+    if (ht_magsgn_smem_bytes(ms_words, max_w, 1) > sizeof(g_dyn_smem)) { printf("smem too large\n"); return 2; }
+    launch(n, 64, [&] {
+      emu_fused(jobs.data(), n, arena.data(), sym2.data(), coef2.data(), status2.data(), ms_words, max_w, form == 0);
+    });
+    if (nr) launch((nr + 63) / 64, 64, [&] { emu_refine(jobs.data(), refine.data(), nr, arena.data(), coef2.data(), status2.data()); });
+    if (coef2 != coef || status2 != status) {
+      printf("fused cleanup form disagrees\n");
+      return 1;
+    }
+  }
   }
   size_t cdiff = 0;
   for (size_t i = 0; i < coef.size(); ++i) cdiff += coef[i] != ref[i];

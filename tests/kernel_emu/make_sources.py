@@ -23,6 +23,11 @@ void emu_refine(const HtJob* jobs, const uint32_t* list, uint32_t n, const uint8
                 uint32_t* status) {
   ht_refine_kernel(jobs, list, n, arena, coef, status);
 }
+void emu_fused(const HtJob* jobs, uint32_t n, const uint8_t* arena, uint32_t* sym, int32_t* coef, uint32_t* status,
+               uint32_t ms_words, uint32_t max_w, bool outline) {
+  if (outline) ht_cleanup_fused_kernel<true>(jobs, n, arena, sym, coef, status, ms_words, max_w);
+  else ht_cleanup_fused_kernel<false>(jobs, n, arena, sym, coef, status, ms_words, max_w);
+}
 }  // namespace sgn
 """
 

@@ -174,11 +174,14 @@ def test_corrupt_code_block_is_an_error_not_a_fault():
 
 @pytest.mark.parametrize("seed", range(2))
 @pytest.mark.parametrize("where", ["magsgn", "vlc"])
-def test_damaged_narrow_blocks_stay_in_their_tile(seed, where):
-    """Code blocks at most 32 wide decode two per warp, and the two may come
-    from different tiles of the batch.  Damage in a tile's MagSgn bits must
-    give the oracle's (different) values; damage in its VLC bits must fail
-    that tile alone; the tiles decoded beside it must come out exact."""
+@pytest.mark.parametrize("form", [0, 1])
+def test_damaged_narrow_blocks_stay_in_their_tile(seed, where, form):
+    """Code blocks at most 32 wide decode two per warp in the two-pass form
+    (form 0), and the two may come from different tiles of the batch; the
+    fused form (1) decodes each in a CTA whose MagSgn warp waits on the
+    block's chain row by row.  Damage in a tile's MagSgn bits must give the
+    oracle's (different) values; damage in its VLC bits must fail that tile
+    alone; the tiles decoded beside it must come out exact."""
     from signinum_b200.plan import Plan
 
     rng = np.random.default_rng(4700 + seed)
@@ -208,6 +211,7 @@ def test_damaged_narrow_blocks_stay_in_their_tile(seed, where):
         cs[b.src + (1 if where == "magsgn" else b.lcup - 4)] ^= 0x5A
     inputs[2] = bytes(cs)
     plan = Plan(inputs, PixelFormat.Rgb8)
+    plan.set_cleanup_form(form)
     plan.execute_async()
     _, per = plan.wait()
     for i in (0, 1, 3, 4):

@@ -92,3 +92,38 @@ def test_autotuned_tile_shape_applies_to_the_next_plan_of_the_same_shape(batch):
     st, _ = b.wait()
     assert st == 0 and [b.download(i) for i in range(len(batch))] == want
     b.destroy()
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_cleanup_forms_are_bit_exact(form):
+    """The HT cleanup as two kernels over all blocks (0), as one kernel whose
+    MagSgn warp follows each block's VLC chain row by row (1), or chosen by
+    block count (2): refinement passes, blocks wider than 64 and narrow ones,
+    in eager runs and graph replays."""
+    import json
+    import pathlib
+
+    import numpy as np
+
+    from tests.helpers import random_codestream, wide_block_codestream
+
+    rng = np.random.default_rng(5300)
+    rgb, gray = [encode.config0().tiles[0].codestream], []
+    fx = json.loads((pathlib.Path(__file__).parent / "golden" / "openhtj2k.json").read_text())["fixtures"]
+    gray.append(bytes.fromhex(fx["openhtj2k_ds0_ht_12_b11"]["j2k_hex"]))
+    while len(rgb) < 5 or len(gray) < 4:
+        cs, _, _, _, comps, _ = random_codestream(rng)
+        (rgb if comps == 3 else gray).append(cs)
+    for cb in [(5, 3), (0, 8)]:  # 128x32 and 4x1024 blocks
+        cs, _, _, _, comps, _ = wide_block_codestream(rng, cb, max_w=200, max_h=90)
+        (rgb if comps == 3 else gray).append(cs)
+    for inputs, fmt in [(rgb, PixelFormat.Rgb8), (gray, PixelFormat.Gray8)]:
+        want = [oracle.decode(c, int(fmt))[0] for c in inputs]
+        plan = Plan(inputs, int(fmt))
+        plan.set_cleanup_form(form)
+        for rep in range(3):
+            plan.execute_async()
+            st, per = plan.wait()
+            assert st == 0 and per == [0] * len(inputs)
+            assert [plan.download(i) for i in range(len(inputs))] == want, f"form {form}, execution {rep}"
+        plan.destroy()
