@@ -738,10 +738,13 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
     c.vlc_lanes = lanes;
   }
   if (c.ht_fused == 2) {
-    // Plans of one block per VLC warp (few blocks, a tile or a few) take the
-    // fused form: each block's MagSgn follows its own chain instead of the
-    // slowest chain of the plan.
-    c.ht_fused = c.vlc_lanes == 1 && p->nht <= kFusedMaxBlocks &&
+    // Plans of at most three blocks per SM take the fused form: each block's
+    // MagSgn follows its own chain instead of the slowest chain of the plan.
+    // With more, the MagSgn warps take issue slots from the chains running
+    // beside them on the same SMs (a 1024^2 RGB tile, about 850 blocks:
+    // 0.118 ms in two kernels, 0.186 ms fused; a 512^2 one, 210 blocks:
+    // 0.192 -> 0.165 ms).
+    c.ht_fused = c.vlc_lanes == 1 && p->nht <= 3ull * (uint64_t)std::max(1, ctx->sm_count) &&
                          ht_magsgn_smem_bytes(p->ms_words, p->max_w, 1) <= 200 * 1024
                      ? 1
                      : 0;

@@ -15,6 +15,8 @@
 //     block's unstuffed MagSgn stream staged in shared memory, and writes
 //     whole rows with coalesced stores; blocks at most 32 wide without
 //     refinement passes go two per warp, one per half-warp.
+// Plans of few blocks run both passes in ht_cleanup_fused_kernel instead: a
+// CTA per block, whose MagSgn warp follows the block's VLC chain row by row.
 // Refinement passes (SigProp/MagRef) run in ht_refine_kernel for the few
 // blocks that carry them.
 #include <algorithm>
