@@ -169,7 +169,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms)
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
  * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
  * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
- * the base rows per unit scaled by 2^shift, shift -2 to 1), keeps the fastest per
+ * the base rows per unit scaled by 2^shift, shift -4 to 1), keeps the fastest per
  * stage for the plan and for later plans of the same shape on this context,
  * and re-executes the plan so its surfaces hold the decode.  Synchronous. */
 typedef struct sgn_tune_report {
@@ -188,7 +188,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tu
 sgn_status sgn_plan_set_launch_shape(sgn_ctx* ctx, sgn_plan* plan, uint32_t vlc_threads, uint32_t ms_warps,
                                      uint32_t ms_blocks_per_grab, uint32_t dwt_queue);
 /* Sets the DWT tile shape by hand: rows per work unit of the IDWT levels and
- * of the last level + pack, the base rule scaled by 2^shift (shift -2 to 1;
+ * of the last level + pack, the base rule scaled by 2^shift (shift -4 to 1;
  * strips stay 128 columns wide).  Re-uploads the plan's job tables. */
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* plan, int32_t idwt_seg_shift, int32_t pack_seg_shift);
 /* Sets the HT cleanup form by hand (no counterpart in the reference): 0, the

@@ -520,9 +520,13 @@ sgn_status build_plan_impl(sgn_ctx* ctx, cudaStream_t s, PinnedBuffer& staging, 
   if (!found_cfg) {
     // Untuned plans: a plan whose last level (or largest IDWT round) has
     // fewer units than twice the SMs (one tile, a small batch) takes
-    // shorter segments, so that more warps share its rows.
+    // shorter segments, so that more warps share its rows: down to 4 rows
+    // for a 512^2 tile (512 units; 16 rows: 0.165 ms plan latency, 4 rows:
+    // 0.146 ms).
     const uint32_t sms = (uint32_t)std::max(1, ctx->sm_count);
-    auto shift_for = [&](uint32_t units) { return units < sms ? -2 : units < 2 * sms ? -1 : 0; };
+    auto shift_for = [&](uint32_t units) {
+      return 4 * units < sms ? -4 : 2 * units < sms ? -3 : units < sms ? -2 : units < 2 * sms ? -1 : 0;
+    };
     uint32_t round_units = 0;
     for (const RoundInfo& r : plan->rounds) round_units = std::max(round_units, r.ctas);
     if (!plan->rounds.empty()) cfg.idwt_seg_shift = shift_for(round_units);
@@ -1144,7 +1148,7 @@ sgn_status sgn_plan_set_cleanup_form(sgn_ctx* ctx, sgn_plan* p, uint32_t fused) 
 
 sgn_status sgn_plan_set_tile_shape(sgn_ctx* ctx, sgn_plan* p, int32_t idwt_seg_shift, int32_t pack_seg_shift) {
   if (!ctx || !p) return set_error(SGN_ERR_INVALID_ARGUMENT, "null argument");
-  if (idwt_seg_shift < -2 || idwt_seg_shift > 1 || pack_seg_shift < -2 || pack_seg_shift > 1)
+  if (idwt_seg_shift < -4 || idwt_seg_shift > 1 || pack_seg_shift < -4 || pack_seg_shift > 1)
     return set_error(SGN_ERR_INVALID_ARGUMENT, "tile shape shift out of range");
   std::lock_guard<std::mutex> g(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -1229,7 +1233,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   }
   // IDWT levels and pack, each: one unit per warp or persistent warps on a
   // queue, and the DWT tile shape (rows per unit: the base rule scaled by
-  // 2^shift, shift -2 to 1; the strip is 128 columns, four per lane).
+  // 2^shift, shift -4 to 1; the strip is 128 columns, four per lane).
   auto set_shape = [&](int is, int ps) {
     set_segments(p, p->h_idwt, p->h_pack, is, ps);
     cudaError_t x = cudaSuccess;
@@ -1244,7 +1248,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   uint32_t idwt_queue = 0, pack_queue = 0;
   int idwt_shift = 0, pack_shift = 0;
   const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
-  for (int sh = -2; sh <= 1 && e == cudaSuccess; ++sh) {
+  for (int sh = -4; sh <= 1 && e == cudaSuccess; ++sh) {
     if ((e = set_shape(sh, sh)) != cudaSuccess) break;
     for (uint32_t q = 0; q < 2; ++q) {
       float ms = time_stage(s, reps, [&] {

@@ -138,7 +138,7 @@ struct LaunchConfig {
   uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue
   uint32_t pack_queue = 0;     // the same for the last level + pack
   // DWT tile shape: rows per work unit of the IDWT levels and of the pack,
-  // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -2..1.
+  // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -4..1.
   int32_t idwt_seg_shift = 0, pack_seg_shift = 0;
   // Persistent grid sizes (SMs x resident CTAs), derived from the above.
   uint32_t ms_ctas = 0, idwt_ctas = 0, pack_ctas = 0;

@@ -56,7 +56,7 @@ def test_autotune_keeps_output_and_is_reused(batch):
     plan.destroy()
 
 
-@pytest.mark.parametrize("shift", [(-2, -2), (-1, -1), (1, 1), (-1, 1), (1, 0)])
+@pytest.mark.parametrize("shift", [(-4, -4), (-3, -2), (-2, -2), (-1, -1), (1, 1), (-1, 1), (1, 0)])
 def test_dwt_tile_shapes_are_bit_exact(shift):
     """Rows per IDWT / pack unit quartered, halved or doubled, on reversible and
     irreversible tiles and on pruned region decodes (windowed levels)."""
@@ -84,7 +84,7 @@ def test_autotuned_tile_shape_applies_to_the_next_plan_of_the_same_shape(batch):
     want = _want(batch)
     a = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
     rep = a.autotune(2)
-    assert rep["idwt_seg_shift"] in (-2, -1, 0, 1) and rep["pack_seg_shift"] in (-2, -1, 0, 1)
+    assert rep["idwt_seg_shift"] in range(-4, 2) and rep["pack_seg_shift"] in range(-4, 2)
     assert rep["vlc_lanes"] in (1, 2, 4, 8, 16, 32) and rep["vlc_outline"] in (0, 1)
     a.destroy()
     b = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
