@@ -742,13 +742,14 @@ sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& in) {
     c.vlc_lanes = lanes;
   }
   if (c.ht_fused == 2) {
-    // Plans of at most three blocks per SM take the fused form: each block's
+    // Plans of at most six blocks per SM take the fused form: each block's
     // MagSgn follows its own chain instead of the slowest chain of the plan.
     // With more, the MagSgn warps take issue slots from the chains running
-    // beside them on the same SMs (a 1024^2 RGB tile, about 850 blocks:
-    // 0.118 ms in two kernels, 0.186 ms fused; a 512^2 one, 210 blocks:
-    // 0.192 -> 0.165 ms).
-    c.ht_fused = c.vlc_lanes == 1 && p->nht <= 3ull * (uint64_t)std::max(1, ctx->sm_count) &&
+    // beside them on the same SMs (one-tile plans, two kernels -> fused:
+    // 210 blocks 0.175 -> 0.138 ms, 777 blocks 0.087 -> 0.075 ms, 786
+    // 0.217 -> 0.209 ms; 1,027 blocks 0.224 -> 0.253 ms, 3,081 blocks 0.118
+    // -> 0.183 ms).
+    c.ht_fused = c.vlc_lanes == 1 && p->nht <= 6ull * (uint64_t)std::max(1, ctx->sm_count) &&
                          ht_magsgn_smem_bytes(p->ms_words, p->max_w, 1) <= 200 * 1024
                      ? 1
                      : 0;
