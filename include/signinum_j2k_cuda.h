@@ -167,7 +167,7 @@ sgn_status sgn_plan_execute_timed(sgn_ctx* ctx, sgn_plan* plan, float* stage_ms)
  * inline or out of line; for plans of up to 8192 code blocks, both cleanup
  * passes fused in one kernel against the best separate pair; MagSgn warps per CTA, one block per warp or persistent
  * warps taking 1 or 4 blocks per grab from the device work queue; IDWT and
- * pack, each, one unit per warp or persistent on a queue: dwt_queue bit 0 =
+ * pack, each, one unit per warp (for IDWT also at four CTAs per SM) or persistent on a queue: dwt_queue bit 0 =
  * IDWT levels, bit 1 = pack; and the DWT tile shape of each, 128 columns by
  * the base rows per unit scaled by 2^shift, shift -4 to 1), keeps the fastest per
  * stage for the plan and for later plans of the same shape on this context,
@@ -181,6 +181,7 @@ typedef struct sgn_tune_report {
   uint32_t vlc_outline; /* 1: the VLC pass's bit-reader refills out of line, 0: inline */
   uint32_t ht_fused;    /* 1: both cleanup passes in one kernel, a CTA per code block (small plans) */
   float fused_ms;       /* that kernel's time (0: not tried) */
+  uint32_t idwt_lean;   /* 1: the IDWT levels' grid form held to four CTAs per SM */
 } sgn_tune_report;
 sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* plan, uint32_t reps, sgn_tune_report* out);
 /* Sets the launch shape by hand (the fields of sgn_tune_report's first row;

@@ -69,7 +69,8 @@ class SgnTuneReport(ctypes.Structure):
                [(n, ctypes.c_float) for n in ("vlc_ms", "ms_ms", "dwt_ms", "vlc_ms_default", "ms_ms_default",
                                               "dwt_ms_default")] + \
                [(n, ctypes.c_int32) for n in ("idwt_seg_shift", "pack_seg_shift")] + \
-               [(n, ctypes.c_uint32) for n in ("vlc_lanes", "vlc_outline", "ht_fused")] + [("fused_ms", ctypes.c_float)]
+               [(n, ctypes.c_uint32) for n in ("vlc_lanes", "vlc_outline", "ht_fused")] + [("fused_ms", ctypes.c_float)] + \
+               [("idwt_lean", ctypes.c_uint32)]
 
 
 # Every entry point of include/signinum_j2k_cuda.h with its ctypes signature.

@@ -770,11 +770,11 @@ cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s) {
                         p->classic_slot, p->classic_ctas, p->d_queue + p->rounds.size() + 2 + kPackVariants, s);
 }
 
-cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas) {
+cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas, bool lean) {
   const RoundInfo& r = p->rounds[k];
   uint32_t* q = queued ? p->d_queue + 1 + k : nullptr;
   return r.irreversible ? launch_idwt97_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q, ctas)
-                        : launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q, ctas);
+                        : launch_idwt_level(p->d_idwt + r.job_begin, r.njobs, r.ctas, s, q, ctas, lean);
 }
 
 cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas) {
@@ -852,7 +852,8 @@ sgn_status execute(sgn_plan* p, cudaStream_t s, cudaEvent_t* ev) {
   if ((e = launch_classic_blocks(p, s)) != cudaSuccess) return cuda_status(e, "classic block launch");
   if ((e = mark(3)) != cudaSuccess) return cuda_status(e, "event record");
   for (size_t k = 0; k < p->rounds.size(); ++k)
-    if ((e = launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas)) != cudaSuccess) return cuda_status(e, "IDWT launch");
+    if ((e = launch_round(p, k, s, c.idwt_queue != 0, c.idwt_ctas, c.idwt_lean != 0)) != cudaSuccess)
+      return cuda_status(e, "IDWT launch");
   if ((e = mark(4)) != cudaSuccess) return cuda_status(e, "event record");
   if ((e = launch_packs(p, s, c.pack_queue != 0, c.pack_ctas)) != cudaSuccess) return cuda_status(e, "pack launch");
   if ((e = mark(5)) != cudaSuccess) return cuda_status(e, "event record");
@@ -1246,20 +1247,24 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
     return x;
   };
   float best_idwt = 1e30f, best_pack = 1e30f, idwt_default = 0.f, pack_default = 0.f;
-  uint32_t idwt_queue = 0, pack_queue = 0;
+  uint32_t idwt_queue = 0, pack_queue = 0, idwt_lean = 0;
   int idwt_shift = 0, pack_shift = 0;
   const uint32_t ictas = p->cfg.idwt_ctas, pctas = p->cfg.pack_ctas;
   for (int sh = -4; sh <= 1 && e == cudaSuccess; ++sh) {
     if ((e = set_shape(sh, sh)) != cudaSuccess) break;
-    for (uint32_t q = 0; q < 2; ++q) {
-      float ms = time_stage(s, reps, [&] {
+    // IDWT: grid form (at three and at four CTAs per SM) or queue.
+    for (uint32_t f = 0; f < 3; ++f) {
+      const bool queued = f == 2, lean = f == 1;
+      const float ms = time_stage(s, reps, [&] {
         cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
-        for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, q != 0, ictas);
+        for (size_t k = 0; k < p->rounds.size() && x == cudaSuccess; ++k) x = launch_round(p, k, s, queued, ictas, lean);
         return x;
       }, e);
-      if (q == 0 && sh == base.idwt_seg_shift) idwt_default = ms;
-      if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = q, idwt_shift = sh;
-      ms = time_stage(s, reps, [&] {
+      if (f == 0 && sh == base.idwt_seg_shift) idwt_default = ms;
+      if (e == cudaSuccess && ms < best_idwt) best_idwt = ms, idwt_queue = queued, idwt_lean = lean, idwt_shift = sh;
+    }
+    for (uint32_t q = 0; q < 2; ++q) {
+      float ms = time_stage(s, reps, [&] {
         cudaError_t x = cudaMemsetAsync(p->d_queue, 0, p->nqueues * sizeof(uint32_t), s);
         if (x == cudaSuccess) x = launch_packs(p, s, q != 0, pctas);
         return x;
@@ -1285,6 +1290,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   cfg.ms_warps = ms_warps;
   cfg.ms_gran = ms_gran;
   cfg.idwt_queue = idwt_queue;
+  cfg.idwt_lean = idwt_lean;
   cfg.pack_queue = pack_queue;
   st = apply_config(ctx, p, cfg);
   if (st != SGN_OK) return st;
@@ -1304,6 +1310,7 @@ sgn_status sgn_plan_autotune(sgn_ctx* ctx, sgn_plan* p, uint32_t reps, sgn_tune_
   rep.vlc_lanes = cfg.vlc_lanes;
   rep.vlc_outline = cfg.vlc_outline;
   rep.ht_fused = cfg.ht_fused;
+  rep.idwt_lean = cfg.idwt_lean;
   rep.ms_warps = cfg.ms_warps;
   rep.ms_blocks_per_grab = cfg.ms_gran;
   rep.dwt_queue = cfg.idwt_queue | (cfg.pack_queue << 1);

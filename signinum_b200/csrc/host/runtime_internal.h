@@ -136,6 +136,7 @@ struct LaunchConfig {
   uint32_t ms_warps = 8;       // warps (code blocks in flight) per CTA of the MagSgn pass
   uint32_t ms_gran = 0;        // 0: one block per warp; > 0: persistent warps take ms_gran blocks per grab
   uint32_t idwt_queue = 0;     // 0: one unit per warp; 1: persistent warps take IDWT units from a queue
+  uint32_t idwt_lean = 0;      // grid form: 1, the kernel held to four CTAs per SM
   uint32_t pack_queue = 0;     // the same for the last level + pack
   // DWT tile shape: rows per work unit of the IDWT levels and of the pack,
   // the base rule (idwt_segment_rows) scaled by 2^shift, shift in -4..1.
@@ -264,7 +265,7 @@ void free_plan_buffers(sgn_plan* p, cudaStream_t s);
 sgn_status apply_config(sgn_ctx* ctx, sgn_plan* p, const LaunchConfig& cfg);
 // IDWT round k (the 5/3 or the 9/7 kernel) and the pack launches, with the
 // plan's work-queue counters when `queued`, on persistent grids of `ctas`.
-cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas);
+cudaError_t launch_round(const sgn_plan* p, size_t k, cudaStream_t s, bool queued, uint32_t ctas, bool lean = false);
 // The classic (EBCOT) code-block kernel over the plan's classic jobs.
 cudaError_t launch_classic_blocks(const sgn_plan* p, cudaStream_t s);
 cudaError_t launch_packs(const sgn_plan* p, cudaStream_t s, bool queued, uint32_t ctas);

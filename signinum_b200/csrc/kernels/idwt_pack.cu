@@ -370,6 +370,16 @@ __device__ __forceinline__ void idwt_unit(const IdwtJob* __restrict__ jobs, uint
 
 // QUEUE: persistent grid taking units from the device counter `queue`;
 // otherwise one unit per warp.
+// The grid form held to four CTAs per SM (64 registers, a few bytes of
+// spills): more units in flight, which the large levels of uneven batches
+// want (C2 levels 0.728 -> 0.680 ms) and the uniform 512^2 batch does not
+// (0.158 -> 0.163 ms); the autotuner picks.
+__global__ void __launch_bounds__(kIdwtWarps * 32, 4) idwt_level_lean_kernel(const IdwtJob* __restrict__ jobs,
+                                                                            uint32_t njobs, uint32_t nunits) {
+  const uint32_t unit = blockIdx.x * kIdwtWarps + (threadIdx.x >> 5);
+  if (unit < nunits) idwt_unit(jobs, njobs, unit);
+}
+
 template <bool QUEUE>
 __global__ void __launch_bounds__(kIdwtWarps * 32) idwt_level_kernel(const IdwtJob* __restrict__ jobs,
                                                                      uint32_t njobs, uint32_t nunits,
@@ -1097,11 +1107,12 @@ cudaError_t launch_pack97(const PackJob* jobs, uint32_t njobs, uint32_t nunits, 
 }
 
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
-                              uint32_t* queue, uint32_t persistent_ctas) {
+                              uint32_t* queue, uint32_t persistent_ctas, bool lean) {
   if (njobs == 0 || nunits == 0) return cudaSuccess;
   uint32_t ctas = (nunits + kIdwtWarps - 1) / kIdwtWarps;
   if (queue) ctas = std::max(1u, std::min(ctas, persistent_ctas));
   if (queue) idwt_level_kernel<true><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, queue);
+  else if (lean) idwt_level_lean_kernel<<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits);
   else idwt_level_kernel<false><<<ctas, kIdwtWarps * 32, 0, stream>>>(jobs, njobs, nunits, nullptr);
   return cudaGetLastError();
 }

@@ -65,8 +65,9 @@ cudaError_t launch_ht_refine(const HtJob* jobs, const uint32_t* list, uint32_t n
 // nunits: work units (strip x row segment) of all jobs of the launch.  With
 // `queue` (a zeroed device counter) the kernels run as a persistent grid of
 // at most persistent_ctas CTAs whose warps take units from the counter.
+// lean: the grid form held to four CTAs per SM (no effect with a queue).
 cudaError_t launch_idwt_level(const IdwtJob* jobs, uint32_t njobs, uint32_t nunits, cudaStream_t stream,
-                              uint32_t* queue = nullptr, uint32_t persistent_ctas = 0);
+                              uint32_t* queue = nullptr, uint32_t persistent_ctas = 0, bool lean = false);
 // All jobs of one launch share the pixel format fmt (a PackFormat) and the
 // kernel variant (pack_variant of their components and bit depth).
 cudaError_t launch_pack(const PackJob* jobs, uint32_t njobs, uint32_t nunits, uint32_t fmt, uint32_t variant,
