@@ -86,6 +86,7 @@ def test_autotuned_tile_shape_applies_to_the_next_plan_of_the_same_shape(batch):
     rep = a.autotune(2)
     assert rep["idwt_seg_shift"] in range(-4, 2) and rep["pack_seg_shift"] in range(-4, 2)
     assert rep["vlc_lanes"] in (1, 2, 4, 8, 16, 32) and rep["vlc_outline"] in (0, 1)
+    assert rep["ht_fused"] in (0, 1) and rep["idwt_lean"] in (0, 1)
     a.destroy()
     b = Plan([t.codestream for t in batch], int(PixelFormat.Rgb8))
     b.execute_async()
