@@ -1244,8 +1244,9 @@ constexpr uint32_t kRowsFailed = 0xFFFFFFFFu;
 constexpr uint32_t kFusedSpinLimit = 1u << 20;
 
 // The chain lane's row hook: the row's symbols, then its flag.  Its pair
-// loop is unrolled twice (one chain per SM quarter or less: 0.146 -> 0.139
-// ms for a 512^2 tile; the two-pass VLC kernel is slower unrolled).
+// loop is unrolled twice (a fused plan runs few chains per SM, each on a
+// warp of its own: 0.146 -> 0.139 ms for a 512^2 tile; the two-pass VLC
+// kernel, 32 chains per warp, is slower unrolled).
 struct FusedPublish {
   static constexpr bool kUnroll2 = true;
   volatile uint32_t* progress;
